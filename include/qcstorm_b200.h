@@ -1,0 +1,146 @@
+/*
+ * qcstorm_b200 -- C ABI of the B200-native QC-STORM MLEbfgs localization path.
+ *
+ * This is the drop-in boundary for the path that the QC-STORM JNI layers
+ * (ImageJ "QC-STORM_ CPPDLL", Micro-Manager "QC-STORM CPPDLL") and the batch
+ * drivers drive through the reference's exported C++ classes
+ * (MLEbfgs/bfgs_MLE_dll x64/bfgsMLE_dll/x64/Release/bfgs_MLE_dll.h):
+ *
+ *   reference                                            this ABI
+ *   -------------------------------------------------    -------------------------------
+ *   LocalizationPara (bfgs_base.h:26-110)                 qcs_loc_para (same fields, order)
+ *   LocalizationPara::LocalizationPara() (bfgs_base.cu:18) qcs_loc_para_default
+ *   LDROIExtractData_TypeDef (LDROIExtraction.h)          qcs_extract_*
+ *   LDLocData_TypeDef (bfgs_top.h)                         qcs_loc_*
+ *   WLEParameterEstimation_TypeDef (WLEParaEstimation.h)  qcs_wle_estimate
+ *
+ * Every function returns a status code (QCS_OK == 0); the reference returns
+ * void and only prints CUDA errors, so a caller that ignores the status sees
+ * the reference's behaviour.  Plain pointers and sizes only; no C++ types.
+ *
+ * Record formats (identical to the reference):
+ *   ROI record   ROISize*(ROISize+1) uint16: ROISize^2 pixels (row-major, ADU)
+ *                then header words [x, y, frame%65536, frame/65536, detector
+ *                type] (LDROIExtraction_ROIExtraction.cu:280-298).
+ *   WLE record   6 float: [nearest-neighbour distance, sigmaL, sigmaR, sigmaU,
+ *                sigmaD, molecule type] (WLEParaEstimation_Parameters.h:20-28).
+ *   Loc record   12 float: [peak photon, x, y, z nm, sigma x, sigma y, total
+ *                photon, background, SNR, CRLB x nm, CRLB y nm, frame]
+ *                (bfgs_CommonPara.h:296-309).
+ */
+#ifndef QCSTORM_B200_H
+#define QCSTORM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define QCS_OK 0
+#define QCS_ERR_ARG 1          /* null pointer, negative count, bad enum      */
+#define QCS_ERR_ROISIZE 2      /* ROI size not supported by the fit kind      */
+#define QCS_ERR_CAPACITY 3     /* count above the context's capacity          */
+#define QCS_ERR_CUDA 4         /* CUDA runtime error (see qcs_last_error)     */
+#define QCS_ERR_NOMEM 5        /* host or device allocation failed            */
+#define QCS_ERR_STATE 6        /* context used after deinit / wrong order     */
+#define QCS_ERR_NOT_BUILT 7    /* library built without CUDA support          */
+
+/* ---- constants, same values as the reference ----------------------------- */
+/* localization type (bfgs_CommonPara.h:275-277) */
+#define QCS_LOCTYPE_GS2D 0
+#define QCS_LOCTYPE_AS3D 1
+#define QCS_LOCTYPE_DH3D 2
+/* image source of qcs_extract_molecules (bfgs_CommonPara.h:319-323) */
+#define QCS_IMAGE_SOURCE_GPU 0
+#define QCS_IMAGE_SOURCE_CPU_PINNED 1
+#define QCS_IMAGE_SOURCE_CPU_NORMAL 2
+/* record sizes and capacity (bfgs_CommonPara.h:292-316, WLEParaEstimation_Parameters.h:20) */
+#define QCS_OUT_PARA_NUM 12
+#define QCS_WLE_PARA_NUM 6
+#define QCS_MAX_POINT_NUM (20480 * 5)
+/* output columns (bfgs_CommonPara.h:298-309) */
+#define QCS_POS_PPHO 0
+#define QCS_POS_XPOS 1
+#define QCS_POS_YPOS 2
+#define QCS_POS_ZPOS 3
+#define QCS_POS_SIGX 4
+#define QCS_POS_SIGY 5
+#define QCS_POS_TPHO 6
+#define QCS_POS_BAKG 7
+#define QCS_POS_PSNR 8
+#define QCS_POS_CRBX 9
+#define QCS_POS_CRBY 10
+#define QCS_POS_FRME 11
+/* molecule type in WLE record column 5 (WLEParaEstimation_Parameters.h:32-34) */
+#define QCS_MOLECULE_MLEFIT 0
+#define QCS_MOLECULE_WLEFIT 1
+#define QCS_MOLECULE_MULTIFIT 2
+/* detector ROI type in record header word 4 (LDROIExtraction_Param.h:53-54) */
+#define QCS_ROITYPE_SINGLE 0
+#define QCS_ROITYPE_MULTI 1
+
+/*
+ * Localization parameters.  Field names, types and order are those of the
+ * reference's LocalizationPara (bfgs_base.h:26-99), so a JNI layer that fills
+ * LocalizationPara field by field (QC_STORM_CPPDLL.cpp:33-143) fills this
+ * struct the same way.  Fields outside the localization path (rendering,
+ * consecutive fit, double helix, spatial resolution) are carried, not used.
+ */
+typedef struct qcs_loc_para {
+    /* camera */
+    float Offset;       /* ADU */
+    float KAdc;         /* e-/ADU */
+    float QE;           /* e-/photon */
+    float ReadNoise_e;  /* e- */
+    /* localization */
+    int ROISize;
+    int LocType;
+    int MultiEmitterFitEn;
+    int WLEEn;
+    /* consecutive molecule filter (carried) */
+    float ConsecFit_DistanceTh_nm;
+    int ConsecFitEn;
+    /* rendering (PixelSize is used by the CRLB, the rest is carried) */
+    float PixelSize;
+    float PixelZoom;
+    float SNR_th;
+    int ColorMode_3D;
+    /* raw image size */
+    int ImageWidth;
+    int ImageHigh;
+    int TotalFrameNum;
+    int SRImageWidth;
+    int SRImageHigh;
+    /* astigmatic 3D calibration */
+    float MinZDepth;
+    float MaxZDepth;
+    float ZDepthCorrFactor;
+    float p4_XGY, p3_XGY, p2_XGY, p1_XGY, p0_XGY; /* sigma x >= sigma y */
+    float p4_XLY, p3_XLY, p2_XLY, p1_XLY, p0_XLY; /* sigma x <  sigma y */
+    /* double helix (carried) */
+    int DH_RotateType;
+    float DH_MeanDistance;
+    float DH_DistanceTh;
+    /* spatial resolution (carried) */
+    int ImagesPerGroup;
+    int IsHollowTube;
+    float StrucuteSize_2D;
+    int SpatialResolutionCalcEn;
+} qcs_loc_para;
+
+/* Fill with the reference's defaults (bfgs_base.cu:18-86). */
+void qcs_loc_para_default(qcs_loc_para *p);
+
+/* Text of the last error on the calling thread ("" if none). */
+const char *qcs_last_error(void);
+
+/* 1 if the library found a usable CUDA device, else 0. */
+int qcs_device_available(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QCSTORM_B200_H */

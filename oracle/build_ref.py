@@ -1,0 +1,132 @@
+#!/usr/bin/env python3
+"""TEST INFRASTRUCTURE ONLY: build the reference QC-STORM library for the host.
+
+Compiles the reference's own CUDA sources (MLEbfgs/bfgs_MLE_dll x64/bfgsMLE_dll/
+bfgsMLE_dll/) with g++ against the host shim in oracle/refshim/, links them with
+oracle/ref_harness.cpp and writes oracle/_ref/libqcs_ref_host.so.  The result
+runs the reference's fit kernels, WLE pre-pass, CRLB, cascade orchestration and
+ROI extraction on the CPU, one emulated CUDA block at a time; it is the checker
+the CPU oracle (oracle/qcs_oracle.c) is pinned against.
+
+Two mechanical rewrites are applied while the sources are read, into a
+temporary directory outside the repository that is deleted afterwards (no
+reference source text is kept in the repository):
+  1. kernel launches `k<<<cfg>>>(args)` become `qcs_emu_cfg(cfg).run((k), args)`,
+     because g++ has no launch syntax;
+  2. SplineInterpolation.h names a function-pointer parameter after an
+     enclosing template parameter (InputDataLen), which MSVC accepts and GCC
+     rejects; the parameter name is dropped (names in a function-pointer
+     parameter list have no meaning).
+Nothing else is changed.  Only the built .so lands in oracle/_ref/.
+
+Usage: python oracle/build_ref.py [--ref PATH] [--force]
+Exits 0 without building when the reference tree is absent (GPU hosts).
+"""
+import argparse
+import os
+import re
+import shutil
+import subprocess
+import sys
+import tempfile
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+DEFAULT_REF = "/root/reference/MLEbfgs/bfgs_MLE_dll x64/bfgsMLE_dll/bfgsMLE_dll"
+OUT_DIR = os.path.join(HERE, "_ref")
+OUT_SO = os.path.join(OUT_DIR, "libqcs_ref_host.so")
+
+# Reference sub-directories and translation units of the localization path.
+DIRS = ["bfgsMLE_Loc_LD", "bfgsMLE_Loc_HD", "bfgsMLE_Loc_top", "WLEParaEstimation",
+        "SubregionExtraction", "cudaWrapper"]
+UNITS = [
+    "bfgsMLE_Loc_LD/bfgs_base.cu",
+    "bfgsMLE_Loc_LD/bfgsMLE_Single_Emitter_Fit.cu",
+    "bfgsMLE_Loc_HD/bfgsMLE_Multi_Emitter_Fit.cu",
+    "bfgsMLE_Loc_top/bfgs_top.cu",
+    "bfgsMLE_Loc_top/bfgs_top_MoleculeClasify.cu",
+    "bfgsMLE_Loc_top/LocPrecCalc_GaussianCRLB.cu",
+    "bfgsMLE_Loc_top/ZeroLocalizationsRemove.cu",
+    "WLEParaEstimation/WLEParaEstimation.cpp",
+    "WLEParaEstimation/WLEParaEstimation_core.cu",
+    "SubregionExtraction/LDROIExtraction.cu",
+    "SubregionExtraction/LDROIExtraction_ImageFiltering.cu",
+    "SubregionExtraction/LDROIExtraction_ROIExtraction.cu",
+]
+
+LAUNCH = re.compile(
+    r"([A-Za-z_]\w*(?:\s*<[^<>;()]*>)?)\s*<<\s*<([^;]*?)>>\s*>\s*\(\s*(\)?)")
+FNPTR_PARAM = re.compile(
+    r"(\(\s*\*\s*FindPositionID\s*\)\s*\([^()]*?)int\s+InputDataLen\s*,")
+
+
+def rewrite(text):
+    def launch(m):
+        kernel, cfg, empty = m.group(1), m.group(2).strip(), m.group(3)
+        return "qcs_emu_cfg(%s).run((%s)%s" % (cfg, kernel, ")" if empty else ", ")
+    text, _ = LAUNCH.subn(launch, text)
+    text = FNPTR_PARAM.sub(r"\1int,", text)
+    return text
+
+
+def newest_mtime(paths):
+    return max(os.path.getmtime(p) for p in paths)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default=DEFAULT_REF)
+    ap.add_argument("--force", action="store_true")
+    args = ap.parse_args()
+    if not os.path.isdir(args.ref):
+        print("build_ref: reference tree not present, skipping")
+        return 0
+    ours = [os.path.join(HERE, "ref_harness.cpp"), os.path.join(HERE, "refshim", "cuda_runtime.h"),
+            os.path.join(HERE, "refshim", "simt_emu.cpp"), os.path.abspath(__file__),
+            os.path.join(HERE, "..", "include", "qcstorm_b200.h")]
+    if (not args.force and os.path.exists(OUT_SO)
+            and os.path.getmtime(OUT_SO) > newest_mtime(ours)):
+        print("build_ref: up to date")
+        return 0
+    os.makedirs(OUT_DIR, exist_ok=True)
+    tmp = tempfile.mkdtemp(prefix="qcs_refsrc_")
+    try:
+        for d in DIRS:
+            src = os.path.join(args.ref, d)
+            dst = os.path.join(tmp, d)
+            os.makedirs(dst, exist_ok=True)
+            for name in os.listdir(src):
+                if not name.endswith((".h", ".cu", ".cpp")):
+                    continue
+                with open(os.path.join(src, name), "r", encoding="latin-1") as f:
+                    text = f.read()
+                with open(os.path.join(dst, name), "w", encoding="latin-1") as f:
+                    f.write(rewrite(text))
+        incs = ["-I" + os.path.join(HERE, "refshim")] + ["-I" + os.path.join(tmp, d) for d in DIRS]
+        flags = ["-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-w", "-D__declspec(x)="]
+        objs = []
+        units = [os.path.join(tmp, u) for u in UNITS]
+        units += [os.path.join(HERE, "ref_harness.cpp"), os.path.join(HERE, "refshim", "simt_emu.cpp")]
+        procs = []
+        for i, u in enumerate(units):
+            o = os.path.join(tmp, "u%02d.o" % i)
+            objs.append(o)
+            cmd = ["g++", "-x", "c++"] + flags + incs + ["-c", u, "-o", o]
+            procs.append((u, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))
+        ok = True
+        for u, p in procs:
+            out, _ = p.communicate()
+            if p.returncode != 0:
+                ok = False
+                sys.stdout.write("build_ref: compile failed for %s\n%s\n" % (u, out.decode(errors="replace")[-4000:]))
+        if not ok:
+            return 1
+        cmd = ["g++", "-shared", "-o", OUT_SO] + objs
+        subprocess.check_call(cmd)
+        print("build_ref: wrote", OUT_SO)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,58 @@
+/*
+ * TEST INFRASTRUCTURE ONLY -- the CPU oracle of the QC-STORM MLEbfgs path.
+ *
+ * A plain-C restatement of the reference algorithm (file:line citations in
+ * qcs_oracle_impl.h), used by the tests as the parity checker and by
+ * bench.py as the timed CPU baseline.  It is never called by the product
+ * library.  The float build (suffix _f32) follows the reference's operation
+ * order so that, compiled with -ffp-contract=off against glibc expf/logf, it
+ * reproduces the host build of the reference bit for bit (pinned by
+ * tests/test_oracle_pin.py against oracle/_ref/libqcs_ref_host.so).  The
+ * double build (suffix _f64) runs the same fixed schedule in FP64 and gives
+ * the "error against FP64" of each result.
+ */
+#ifndef QCS_ORACLE_H
+#define QCS_ORACLE_H
+
+#include <stdint.h>
+#include "../include/qcstorm_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Number of OpenMP threads used by the batch entry points (0 = all cores). */
+void qcso_set_threads(int n);
+int qcso_get_threads(void);
+
+/* WLE pre-pass: PSF width, nearest neighbour, molecule type.  wle: n x 6. */
+int qcso_wle(const qcs_loc_para *p, const uint16_t *rois, int n, float *wle);
+
+/* Whole BFGS_MLELocalization: classify, single fit, 2E/3E cascade, CRLB.
+ * out: out_cap x 12; *n_valid = rows written; ratios: 7 floats or NULL. */
+int qcso_localize_f32(const qcs_loc_para *p, const uint16_t *rois, const float *wle, int n,
+                      float *out, int out_cap, int *n_valid, float *ratios);
+int qcso_localize_f64(const qcs_loc_para *p, const uint16_t *rois, const float *wle, int n,
+                      float *out, int out_cap, int *n_valid, float *ratios);
+
+/* One single-emitter fit pass over all n ROIs (kind 0 GS2D, 1 AS3D), no
+ * cascade and no CRLB: the kernel-level output. out: n x 12. */
+int qcso_fit_single_f32(int kind, const qcs_loc_para *p, const uint16_t *rois, const float *wle,
+                        int n, float *out);
+int qcso_fit_single_f64(int kind, const qcs_loc_para *p, const uint16_t *rois, const float *wle,
+                        int n, float *out);
+
+/* CRLB columns 9/10 over n rows, in place. */
+int qcso_crlb(const qcs_loc_para *p, float *loc, int n);
+
+/* ROI extraction over n_frames frames fed in batches of `batch` frames, as
+ * consecutive ExtractMolecules calls; rois_out cap x R(R+1), wle_out cap x 6. */
+int qcso_extract(const qcs_loc_para *p, const uint16_t *frames, int n_frames, int batch,
+                 int start_frame, uint16_t *rois_out, float *wle_out, int cap, int *n_roi,
+                 int *first_frame, int *end_frame);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,230 @@
+// TEST INFRASTRUCTURE ONLY -- never linked into the product library.
+//
+// extern "C" entry points over the reference QC-STORM library compiled for
+// the host (oracle/build_ref.py).  Everything below calls the reference's own
+// classes and kernels; this file only converts parameters and copies results.
+//   qcsref_localize    LDLocData_TypeDef::BFGS_MLELocalization (bfgs_top.cu:26-204)
+//   qcsref_fit_kernel  one fit kernel launched directly, e.g. bfgsMLELoc_AS3D<9,6>
+//                      (the reference dispatcher launches <8> for ROISize 9,
+//                      bfgsMLE_Single_Emitter_Fit.cu:96)
+//   qcsref_crlb        GaussianCRLB_Calc_top (LocPrecCalc_GaussianCRLB.h:65-128)
+//   qcsref_wle         WLEParameterEstimation_TypeDef::WLEParameterEstimate
+//                      (WLEParaEstimation.cpp:20-40)
+//   qcsref_extract     LDROIExtractData_TypeDef::ExtractMolecules (LDROIExtraction.cu:30-80)
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "bfgs_top.h"
+#include "LDROIExtraction.h"
+#include "WLEParaEstimation.h"
+#include "bfgsMLE_GS2D_core.h"
+#include "bfgsMLE_AS3D_core.h"
+#include "LocPrecCalc_GaussianCRLB.h"
+
+#include "../include/qcstorm_b200.h"
+
+// cudaWrapper.cu is not compiled (it only prints); these are its quiet stand-ins.
+void HandleErr(cudaError_t, const char *) {}
+
+namespace {
+
+void to_ref(const qcs_loc_para *p, LocalizationPara &r) {
+    r.Offset = p->Offset;
+    r.KAdc = p->KAdc;
+    r.QE = p->QE;
+    r.ReadNoise_e = p->ReadNoise_e;
+    r.ROISize = p->ROISize;
+    r.LocType = p->LocType;
+    r.MultiEmitterFitEn = p->MultiEmitterFitEn;
+    r.WLEEn = p->WLEEn;
+    r.ConsecFit_DistanceTh_nm = p->ConsecFit_DistanceTh_nm;
+    r.ConsecFitEn = p->ConsecFitEn;
+    r.PixelSize = p->PixelSize;
+    r.PixelZoom = p->PixelZoom;
+    r.SNR_th = p->SNR_th;
+    r.ColorMode_3D = p->ColorMode_3D;
+    r.ImageWidth = p->ImageWidth;
+    r.ImageHigh = p->ImageHigh;
+    r.TotalFrameNum = p->TotalFrameNum;
+    r.SRImageWidth = p->SRImageWidth;
+    r.SRImageHigh = p->SRImageHigh;
+    r.MinZDepth = p->MinZDepth;
+    r.MaxZDepth = p->MaxZDepth;
+    r.ZDepthCorrFactor = p->ZDepthCorrFactor;
+    r.p4_XGY = p->p4_XGY; r.p3_XGY = p->p3_XGY; r.p2_XGY = p->p2_XGY; r.p1_XGY = p->p1_XGY; r.p0_XGY = p->p0_XGY;
+    r.p4_XLY = p->p4_XLY; r.p3_XLY = p->p3_XLY; r.p2_XLY = p->p2_XLY; r.p1_XLY = p->p1_XLY; r.p0_XLY = p->p0_XLY;
+    r.DH_RotateType = p->DH_RotateType;
+    r.DH_MeanDistance = p->DH_MeanDistance;
+    r.DH_DistanceTh = p->DH_DistanceTh;
+    r.ImagesPerGroup = p->ImagesPerGroup;
+    r.IsHollowTube = p->IsHollowTube;
+    r.StrucuteSize_2D = p->StrucuteSize_2D;
+    r.SpatialResolutionCalcEn = p->SpatialResolutionCalcEn;
+}
+
+CoreFittingPara core_para(const LocalizationPara &r) {
+    CoreFittingPara c;
+    c.MultiEmitterFitEn = r.MultiEmitterFitEn;
+    c.WLEEn = r.WLEEn;
+    c.Offset = r.Offset;
+    c.KAdc = r.KAdc;
+    c.QE = r.QE;
+    c.ReadNoise_e = r.ReadNoise_e;
+    c.ZDepthCorrFactor = r.ZDepthCorrFactor;
+    c.p4_XGY = r.p4_XGY; c.p3_XGY = r.p3_XGY; c.p2_XGY = r.p2_XGY; c.p1_XGY = r.p1_XGY; c.p0_XGY = r.p0_XGY;
+    c.p4_XLY = r.p4_XLY; c.p3_XLY = r.p3_XLY; c.p2_XLY = r.p2_XLY; c.p1_XLY = r.p1_XLY; c.p0_XLY = r.p0_XLY;
+    return c;
+}
+
+}  // namespace
+
+extern "C" {
+
+// The reference's default LocalizationPara, field by field.
+void qcsref_default_para(qcs_loc_para *p) {
+    LocalizationPara r;
+    p->Offset = r.Offset; p->KAdc = r.KAdc; p->QE = r.QE; p->ReadNoise_e = r.ReadNoise_e;
+    p->ROISize = r.ROISize; p->LocType = r.LocType; p->MultiEmitterFitEn = r.MultiEmitterFitEn; p->WLEEn = r.WLEEn;
+    p->ConsecFit_DistanceTh_nm = r.ConsecFit_DistanceTh_nm; p->ConsecFitEn = r.ConsecFitEn;
+    p->PixelSize = r.PixelSize; p->PixelZoom = r.PixelZoom; p->SNR_th = r.SNR_th; p->ColorMode_3D = r.ColorMode_3D;
+    p->ImageWidth = r.ImageWidth; p->ImageHigh = r.ImageHigh; p->TotalFrameNum = r.TotalFrameNum;
+    p->SRImageWidth = r.SRImageWidth; p->SRImageHigh = r.SRImageHigh;
+    p->MinZDepth = r.MinZDepth; p->MaxZDepth = r.MaxZDepth; p->ZDepthCorrFactor = r.ZDepthCorrFactor;
+    p->p4_XGY = r.p4_XGY; p->p3_XGY = r.p3_XGY; p->p2_XGY = r.p2_XGY; p->p1_XGY = r.p1_XGY; p->p0_XGY = r.p0_XGY;
+    p->p4_XLY = r.p4_XLY; p->p3_XLY = r.p3_XLY; p->p2_XLY = r.p2_XLY; p->p1_XLY = r.p1_XLY; p->p0_XLY = r.p0_XLY;
+    p->DH_RotateType = r.DH_RotateType; p->DH_MeanDistance = r.DH_MeanDistance; p->DH_DistanceTh = r.DH_DistanceTh;
+    p->ImagesPerGroup = r.ImagesPerGroup; p->IsHollowTube = r.IsHollowTube; p->StrucuteSize_2D = r.StrucuteSize_2D;
+    p->SpatialResolutionCalcEn = r.SpatialResolutionCalcEn;
+}
+
+// LDLocData_TypeDef::BFGS_MLELocalization over n records.
+// out: capacity out_cap rows of 12 floats; ratios: 7 floats
+// [FitRatio_1E, 2E, 3E, Final_1E, Final_2E, Final_3E, Final_4E].
+int qcsref_localize(const qcs_loc_para *p, const unsigned short *rois, const float *wle, int n,
+                    float *out, int out_cap, int *n_valid, float *ratios) {
+    LocalizationPara r;
+    to_ref(p, r);
+    LDLocData_TypeDef loc;
+    loc.Init(r);
+    const int whole = r.ROISize * (r.ROISize + 1);
+    int m = n < MaxPointNum ? n : MaxPointNum;
+    std::vector<unsigned short> h_roi(rois, rois + (size_t)m * whole);
+    std::vector<float> h_wle(wle, wle + (size_t)m * WLE_ParaNumber);
+    loc.BFGS_MLELocalization(h_roi.data(), h_wle.data(), r, n, nullptr);
+    int nv = loc.oValidFluoNum;
+    if (nv > out_cap) nv = out_cap;
+    memcpy(out, loc.h_LocArry, sizeof(float) * OutParaNumGS2D * (size_t)nv);
+    *n_valid = loc.oValidFluoNum;
+    if (ratios) {
+        ratios[0] = loc.FitRatio_1E; ratios[1] = loc.FitRatio_2E; ratios[2] = loc.FitRatio_3E;
+        ratios[3] = loc.FitRatio_Final_1E; ratios[4] = loc.FitRatio_Final_2E;
+        ratios[5] = loc.FitRatio_Final_3E; ratios[6] = loc.FitRatio_Final_4E;
+    }
+    loc.Deinit(r);
+    return 0;
+}
+
+// One single-emitter fit kernel launched directly with MultiEmitterFitEn = 0
+// semantics for the queue (identity map).  kind 0 = GS2D, 1 = AS3D.
+// out: n rows of 12 floats (CRLB columns left as the kernel leaves them).
+int qcsref_fit_kernel(int kind, const qcs_loc_para *p, const unsigned short *rois, const float *wle,
+                      int n, float *out) {
+    LocalizationPara r;
+    to_ref(p, r);
+    CoreFittingPara c = core_para(r);
+    c.MultiEmitterFitEn = 0;
+    std::vector<int> single(n), q2(MaxPointNum), q3(MaxPointNum);
+    for (int i = 0; i < n; ++i) single[i] = i;
+    int n_single = n, n2 = 0, n3 = 0, rej = 0, added = n;
+    FitPosInf_TypeDef f;
+    memset(&f, 0, sizeof(f));
+    f.d_SingleFitFluoNum = &n_single;
+    f.d_SingleFitFluoPos = single.data();
+    f.d_MultiFitFluoNum_2E = &n2;
+    f.d_MultiFitFluoPos_2E = q2.data();
+    f.d_MultiFitFluoNum_3E = &n3;
+    f.d_MultiFitFluoPos_3E = q3.data();
+    f.d_RejectedFluoNum = &rej;
+    f.d_MultiFit_AddedFluoNum = &added;
+    const int whole = r.ROISize * (r.ROISize + 1);
+    std::vector<unsigned short> d_roi(rois, rois + (size_t)n * whole);
+    std::vector<float> d_wle(wle, wle + (size_t)n * WLE_ParaNumber);
+    std::vector<float> d_loc((size_t)n * OutParaNumGS2D, 0.0f);
+    qcs_emu_cfg cfg((n + ThreadsPerBlock - 1) / ThreadsPerBlock, ThreadsPerBlock);
+#define QCSREF_CASE(KIND, R, KERNEL)                                                              \
+    if (kind == KIND && r.ROISize == R) {                                                         \
+        cfg.run((KERNEL), d_loc.data(), d_roi.data(), d_wle.data(), n, &f, &c);                    \
+        memcpy(out, d_loc.data(), sizeof(float) * d_loc.size());                                  \
+        return 0;                                                                                 \
+    }
+    QCSREF_CASE(0, 5, (bfgsMLELoc_Gauss2D<5, FitParaNum_2D>))
+    QCSREF_CASE(0, 7, (bfgsMLELoc_Gauss2D<7, FitParaNum_2D>))
+    QCSREF_CASE(0, 9, (bfgsMLELoc_Gauss2D<9, FitParaNum_2D>))
+    QCSREF_CASE(0, 11, (bfgsMLELoc_Gauss2D<11, FitParaNum_2D>))
+    QCSREF_CASE(0, 13, (bfgsMLELoc_Gauss2D<13, FitParaNum_2D>))
+    QCSREF_CASE(1, 5, (bfgsMLELoc_AS3D<5, FitParaNum_AS3D>))
+    QCSREF_CASE(1, 7, (bfgsMLELoc_AS3D<7, FitParaNum_AS3D>))
+    QCSREF_CASE(1, 9, (bfgsMLELoc_AS3D<9, FitParaNum_AS3D>))
+    QCSREF_CASE(1, 11, (bfgsMLELoc_AS3D<11, FitParaNum_AS3D>))
+    QCSREF_CASE(1, 13, (bfgsMLELoc_AS3D<13, FitParaNum_AS3D>))
+#undef QCSREF_CASE
+    return 2;
+}
+
+// GaussianCRLB_Calc_top over n 12-float rows, in place.  The reference kernel
+// has no bounds guard, so rows are padded to a multiple of 32 here.
+int qcsref_crlb(const qcs_loc_para *p, float *loc, int n) {
+    LocalizationPara r;
+    to_ref(p, r);
+    const int blocks = (n + ThreadsPerBlock - 1) / ThreadsPerBlock;
+    std::vector<float> d_loc((size_t)blocks * ThreadsPerBlock * OutParaNumGS2D, 0.0f);
+    memcpy(d_loc.data(), loc, sizeof(float) * OutParaNumGS2D * (size_t)n);
+    LDLocData_TypeDef::LocPrecCalc_GaussianCRLB(d_loc.data(), r, n, nullptr);
+    memcpy(loc, d_loc.data(), sizeof(float) * OutParaNumGS2D * (size_t)n);
+    return 0;
+}
+
+// WLEParameterEstimate over n records; wle_out: n rows of 6 floats.
+int qcsref_wle(const qcs_loc_para *p, const unsigned short *rois, int n, float *wle_out) {
+    LocalizationPara r;
+    to_ref(p, r);
+    WLEParameterEstimation_TypeDef w;
+    w.Init(r);
+    const int whole = r.ROISize * (r.ROISize + 1);
+    std::vector<unsigned short> d_roi(rois, rois + (size_t)n * whole);
+    w.WLEParameterEstimate(d_roi.data(), r.LocType, r.MultiEmitterFitEn, r.ROISize, n, nullptr);
+    memcpy(wle_out, w.d_WLEPara, sizeof(float) * WLE_ParaNumber * (size_t)n);
+    w.Deinit();
+    return 0;
+}
+
+// ExtractMolecules over consecutive batches of frames (the JNI feeding
+// pattern), accumulating ROI records and WLE rows.  batch: frames per call.
+int qcsref_extract(const qcs_loc_para *p, const unsigned short *frames, int n_frames, int batch,
+                   int start_frame, unsigned short *rois_out, float *wle_out, int cap, int *n_roi,
+                   int *first_frame, int *end_frame) {
+    LocalizationPara r;
+    to_ref(p, r);
+    LDROIExtractData_TypeDef ex;
+    ex.Init(r);
+    ex.ResetROINum();
+    const size_t frame_px = (size_t)r.ImageWidth * r.ImageHigh;
+    for (int f = 0; f < n_frames; f += batch) {
+        int nb = (n_frames - f) < batch ? (n_frames - f) : batch;
+        std::vector<unsigned short> buf(frames + f * frame_px, frames + (f + nb) * frame_px);
+        ex.ExtractMolecules(buf.data(), ImageSource_CPU_Pinned, r, start_frame + f, nb, nullptr);
+    }
+    int n = ex.GetAccumulatedROINum();
+    *n_roi = n;
+    if (n > cap) n = cap;
+    const int whole = r.ROISize * (r.ROISize + 1);
+    memcpy(rois_out, ex.h_ImageROI, sizeof(unsigned short) * whole * (size_t)n);
+    memcpy(wle_out, ex.Get_h_WLEPara(), sizeof(float) * WLE_ParaNumber * (size_t)n);
+    *first_frame = ex.FirstFrame;
+    *end_frame = ex.EndFrame;
+    ex.Deinit();
+    return 0;
+}
+
+}  // extern "C"

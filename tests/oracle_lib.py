@@ -1,0 +1,82 @@
+"""Test-side binding of the CPU oracle (oracle/liboracle.so) and of the host
+build of the reference (oracle/_ref/libqcs_ref_host.so, present only where the
+reference tree was available at build time).  Checkers only."""
+import ctypes as C
+import os
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_SO = os.path.join(ROOT, "oracle", "liboracle.so")
+REF_SO = os.path.join(ROOT, "oracle", "_ref", "libqcs_ref_host.so")
+
+_lib = {}
+
+
+def _load(path):
+    if path not in _lib:
+        _lib[path] = C.CDLL(path) if os.path.exists(path) else None
+    return _lib[path]
+
+
+def oracle():
+    lib = _load(ORACLE_SO)
+    if lib is None:
+        raise RuntimeError("oracle/liboracle.so not built (make -C oracle)")
+    return lib
+
+
+def ref_host():
+    return _load(REF_SO)
+
+
+def _p(a):
+    return C.c_void_p(a.ctypes.data) if a is not None else None
+
+
+def wle(para, rec, lib="oracle"):
+    n = rec.shape[0]
+    out = np.zeros((n, 6), np.float32)
+    L = oracle() if lib == "oracle" else ref_host()
+    f = L.qcso_wle if lib == "oracle" else L.qcsref_wle
+    st = f(C.byref(para), _p(rec), n, _p(out))
+    assert st == 0, st
+    return out
+
+
+def localize(para, rec, wl, lib="oracle", precision="f32", out_cap=None):
+    n = rec.shape[0]
+    cap = out_cap or max(2 * n, 1)
+    out = np.zeros((cap, 12), np.float32)
+    nv = C.c_int(0)
+    ratios = np.zeros(7, np.float32)
+    if lib == "oracle":
+        f = getattr(oracle(), "qcso_localize_" + precision)
+    else:
+        f = ref_host().qcsref_localize
+    st = f(C.byref(para), _p(rec), _p(wl), n, _p(out), cap, C.byref(nv), _p(ratios))
+    assert st == 0, st
+    return out[:nv.value].copy(), ratios
+
+
+def fit_single(kind, para, rec, wl, lib="oracle", precision="f32"):
+    n = rec.shape[0]
+    out = np.zeros((n, 12), np.float32)
+    if lib == "oracle":
+        st = getattr(oracle(), "qcso_fit_single_" + precision)(kind, C.byref(para), _p(rec), _p(wl), n, _p(out))
+    else:
+        st = ref_host().qcsref_fit_kernel(kind, C.byref(para), _p(rec), _p(wl), n, _p(out))
+    assert st == 0, st
+    return out
+
+
+def crlb(para, loc, lib="oracle"):
+    out = np.ascontiguousarray(loc, np.float32).copy()
+    f = oracle().qcso_crlb if lib == "oracle" else ref_host().qcsref_crlb
+    st = f(C.byref(para), _p(out), out.shape[0])
+    assert st == 0, st
+    return out
+
+
+def set_threads(n):
+    oracle().qcso_set_threads(int(n))
