@@ -139,6 +139,83 @@ const char *qcs_last_error(void);
 /* 1 if the library found a usable CUDA device, else 0. */
 int qcs_device_available(void);
 
+/* ---- localization context: LDLocData_TypeDef --------------------------- */
+/*
+ * One context owns every buffer of the localization path for records of one
+ * ROI size, like LDLocData_TypeDef::Init (bfgs_top.cu:234-293).  Capacity is
+ * the largest record count one call accepts; the reference fixes it at
+ * MaxPointNum = 102400 (bfgs_CommonPara.h:316) and silently truncates larger
+ * calls (bfgs_top.cu:36), this ABI rejects them with QCS_ERR_CAPACITY.  Row
+ * capacity is 2 x capacity (records + appended second emitters).
+ */
+typedef struct qcs_loc_data qcs_loc_data;
+
+/* LDLocData_TypeDef::Init(LocalizationPara&) (bfgs_top.h:75, bfgs_top.cu:234). */
+int qcs_loc_init(const qcs_loc_para *p, qcs_loc_data **out);
+/* Same with an explicit record capacity (<= 0: QCS_MAX_POINT_NUM). */
+int qcs_loc_init_capacity(const qcs_loc_para *p, int capacity, qcs_loc_data **out);
+/* LDLocData_TypeDef::Deinit (bfgs_top.h:76, bfgs_top.cu:295). */
+int qcs_loc_deinit(qcs_loc_data *c);
+int qcs_loc_capacity(const qcs_loc_data *c);
+
+/*
+ * LDLocData_TypeDef::BFGS_MLELocalization(unsigned short *h_ImageROI,
+ * float *h_WLEPara, LocalizationPara&, int FluoNum, cudaStream_t)
+ * (bfgs_top.h:78, bfgs_top.cu:26-204).  Host records in; on return the rows
+ * are in qcs_loc_h_loc_arry() (h_LocArry), their count in
+ * qcs_loc_valid_num() (oValidFluoNum) and the fit ratios in
+ * qcs_loc_fit_ratios() (FitRatio_*).  Synchronous, like the reference.
+ * h_wle may be NULL: the WLE pre-pass then runs on the device from the
+ * records (the reference computes it during ROI extraction).  stream: a
+ * cudaStream_t or NULL for the context's own stream.
+ */
+int qcs_loc_bfgs_mle_localization(qcs_loc_data *c, const uint16_t *h_rois, const float *h_wle,
+                                  const qcs_loc_para *p, int n, void *stream);
+/* h_LocArry: valid until the next call on the context (bfgs_top.h:38). */
+const float *qcs_loc_h_loc_arry(const qcs_loc_data *c);
+/* oValidFluoNum (bfgs_top.h:42). */
+int qcs_loc_valid_num(const qcs_loc_data *c);
+/* [FitRatio_1E, FitRatio_2E, FitRatio_3E, FitRatio_Final_1E, FitRatio_Final_2E,
+ *  FitRatio_Final_3E, FitRatio_Final_4E] (bfgs_top.h:46-58). */
+int qcs_loc_fit_ratios(const qcs_loc_data *c, float *out7);
+
+/*
+ * Device-resident form of the same call: records (and optionally WLE rows)
+ * already in device memory, rows left in device memory
+ * (qcs_loc_device_rows, count at qcs_loc_device_valid_num), asynchronous on
+ * `stream` with no host synchronisation, so whole pipelines can be captured
+ * in a CUDA graph.  No counterpart in the reference (it always copies
+ * through pinned host memory, bfgs_top.cu:42-47, 201-202).
+ */
+int qcs_loc_localize_device(qcs_loc_data *c, const uint16_t *d_rois, const float *d_wle,
+                            const qcs_loc_para *p, int n, void *stream);
+const float *qcs_loc_device_rows(const qcs_loc_data *c);
+const int *qcs_loc_device_valid_num(const qcs_loc_data *c);
+/* The context's own device record / WLE buffers (capacity records). */
+uint16_t *qcs_loc_device_roi_buffer(qcs_loc_data *c);
+float *qcs_loc_device_wle_buffer(qcs_loc_data *c);
+
+/* ---- WLE pre-pass: WLEParameterEstimation_TypeDef ---------------------- */
+/* WLEParameterEstimation_TypeDef::WLEParameterEstimate (WLEParaEstimation.h:41,
+ * WLEParaEstimation.cpp:20-40): PSF width, same-frame nearest neighbour and
+ * molecule type of n records; host in, host out. */
+int qcs_wle_estimate(qcs_loc_data *c, const uint16_t *h_rois, int n, const qcs_loc_para *p, float *h_wle);
+/* Same on device pointers, asynchronous on `stream`. */
+int qcs_wle_estimate_device(qcs_loc_data *c, const uint16_t *d_rois, int n, const qcs_loc_para *p, float *d_wle,
+                            void *stream);
+
+/* ---- kernel-level entry points ----------------------------------------- */
+/* One single-emitter fit pass over n device records, identity queue, no
+ * cascade and no CRLB: LDLoc_BFGS_MLELocalizationGS2D / ...AS3D
+ * (bfgsMLE_Single_Emitter_Fit.h:10-13, .cu:31-119), dispatching the true ROI
+ * size (the reference launches the 8x8 kernel for ROISize 9 in AS3D, .cu:96).
+ * loc_type: QCS_LOCTYPE_*; rows: n x 12 in d_loc, CRLB columns left 0. */
+int qcs_fit_single_device(int loc_type, const qcs_loc_para *p, const uint16_t *d_rois, const float *d_wle, int n,
+                          float *d_loc, void *stream);
+/* LDLocData_TypeDef::LocPrecCalc_GaussianCRLB (bfgs_top.h:90,
+ * LocPrecCalc_GaussianCRLB.cu:23-40): CRLB columns of n device rows. */
+int qcs_crlb_device(const qcs_loc_para *p, float *d_loc, int n, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

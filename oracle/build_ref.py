@@ -19,7 +19,12 @@ reference source text is kept in the repository):
      parameter list have no meaning).
 Nothing else is changed.  Only the built .so lands in oracle/_ref/.
 
-Usage: python oracle/build_ref.py [--ref PATH] [--force]
+With --gpu the same sources are compiled unmodified by nvcc for sm_100a
+(only rewrite 2 applies) with oracle/ref_harness_gpu.cu into
+oracle/_ref/libqcs_ref_gpu.so: the reference's own CUDA code, run on the
+B200 as the bit-level checker of the product kernels.
+
+Usage: python oracle/build_ref.py [--ref PATH] [--force] [--gpu]
 Exits 0 without building when the reference tree is absent (GPU hosts).
 """
 import argparse
@@ -34,6 +39,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_REF = "/root/reference/MLEbfgs/bfgs_MLE_dll x64/bfgsMLE_dll/bfgsMLE_dll"
 OUT_DIR = os.path.join(HERE, "_ref")
 OUT_SO = os.path.join(OUT_DIR, "libqcs_ref_host.so")
+OUT_GPU_SO = os.path.join(OUT_DIR, "libqcs_ref_gpu.so")
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 # Reference sub-directories and translation units of the localization path.
 DIRS = ["bfgsMLE_Loc_LD", "bfgsMLE_Loc_HD", "bfgsMLE_Loc_top", "WLEParaEstimation",
@@ -59,13 +66,72 @@ FNPTR_PARAM = re.compile(
     r"(\(\s*\*\s*FindPositionID\s*\)\s*\([^()]*?)int\s+InputDataLen\s*,")
 
 
-def rewrite(text):
+def rewrite(text, launches=True):
     def launch(m):
         kernel, cfg, empty = m.group(1), m.group(2).strip(), m.group(3)
         return "qcs_emu_cfg(%s).run((%s)%s" % (cfg, kernel, ")" if empty else ", ")
-    text, _ = LAUNCH.subn(launch, text)
+    if launches:
+        text, _ = LAUNCH.subn(launch, text)
     text = FNPTR_PARAM.sub(r"\1int,", text)
     return text
+
+
+def stage_sources(ref, tmp, launches):
+    for d in DIRS:
+        src = os.path.join(ref, d)
+        dst = os.path.join(tmp, d)
+        os.makedirs(dst, exist_ok=True)
+        for name in os.listdir(src):
+            if not name.endswith((".h", ".cu", ".cpp")):
+                continue
+            with open(os.path.join(src, name), "r", encoding="latin-1") as f:
+                text = f.read()
+            with open(os.path.join(dst, name), "w", encoding="latin-1") as f:
+                f.write(rewrite(text, launches))
+
+
+def run_parallel(cmds):
+    procs = [(c, subprocess.Popen(c, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)) for c in cmds]
+    ok = True
+    for c, p in procs:
+        out, _ = p.communicate()
+        if p.returncode != 0:
+            ok = False
+            sys.stdout.write("build_ref: failed: %s\n%s\n" % (" ".join(c)[-300:], out.decode(errors="replace")[-4000:]))
+    return ok
+
+
+def build_gpu(args):
+    if not os.path.isdir(args.ref):
+        print("build_ref: reference tree not present, skipping")
+        return 0
+    ours = [os.path.join(HERE, "ref_harness_gpu.cu"), os.path.abspath(__file__),
+            os.path.join(HERE, "..", "include", "qcstorm_b200.h")]
+    if (not args.force and os.path.exists(OUT_GPU_SO)
+            and os.path.getmtime(OUT_GPU_SO) > newest_mtime(ours)):
+        print("build_ref: gpu build up to date")
+        return 0
+    os.makedirs(OUT_DIR, exist_ok=True)
+    tmp = tempfile.mkdtemp(prefix="qcs_refsrc_")
+    try:
+        stage_sources(args.ref, tmp, launches=False)
+        open(os.path.join(tmp, "stdafx.h"), "w").close()
+        incs = ["-I" + tmp] + ["-I" + os.path.join(tmp, d) for d in DIRS]
+        flags = ["-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-Xcompiler", "-fPIC",
+                 "-w", "-D__declspec(x)=", "-x", "cu", "-rdc=false"]
+        units = [os.path.join(tmp, u) for u in UNITS] + [os.path.join(HERE, "ref_harness_gpu.cu")]
+        objs, cmds = [], []
+        for i, u in enumerate(units):
+            o = os.path.join(tmp, "g%02d.o" % i)
+            objs.append(o)
+            cmds.append([NVCC] + flags + incs + ["-c", u, "-o", o])
+        if not run_parallel(cmds):
+            return 1
+        subprocess.check_call([NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", OUT_GPU_SO] + objs)
+        print("build_ref: wrote", OUT_GPU_SO)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    return 0
 
 
 def newest_mtime(paths):
@@ -76,7 +142,10 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default=DEFAULT_REF)
     ap.add_argument("--force", action="store_true")
+    ap.add_argument("--gpu", action="store_true")
     args = ap.parse_args()
+    if args.gpu:
+        return build_gpu(args)
     if not os.path.isdir(args.ref):
         print("build_ref: reference tree not present, skipping")
         return 0

@@ -1,0 +1,337 @@
+// C ABI of libqcstorm_b200 (include/qcstorm_b200.h): localization contexts
+// (LDLocData_TypeDef), the WLE pre-pass (WLEParameterEstimation_TypeDef) and
+// kernel-level entry points.  All device memory of a context is allocated
+// once at init for its record capacity; calls allocate nothing.
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <cuda_runtime.h>
+
+#include "../../include/qcstorm_b200.h"
+#include "qcs_cascade.h"
+#include "qcs_fit_math.cuh"
+#include "qcs_kernels.h"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char *what, cudaError_t e = cudaSuccess) {
+    g_err = what;
+    if (e != cudaSuccess) {
+        g_err += ": ";
+        g_err += cudaGetErrorString(e);
+    }
+    return code;
+}
+
+#define QCS_CUDA(call, what)                                  \
+    do {                                                      \
+        cudaError_t e_ = (call);                              \
+        if (e_ != cudaSuccess) return fail(QCS_ERR_CUDA, what, e_); \
+    } while (0)
+
+int check_para(const qcs_loc_para *p, bool multi_ok_sizes = true) {
+    if (!p) return fail(QCS_ERR_ARG, "null parameter struct");
+    if (p->LocType < QCS_LOCTYPE_GS2D || p->LocType > QCS_LOCTYPE_DH3D) return fail(QCS_ERR_ARG, "LocType out of range");
+    const int R = p->ROISize;
+    if (R < 5 || R > 17 || (R & 1) == 0) return fail(QCS_ERR_ROISIZE, "ROISize must be odd, 5..17");
+    if (multi_ok_sizes && p->MultiEmitterFitEn && R > 13)
+        return fail(QCS_ERR_ROISIZE, "multi-emitter fitting supports ROISize 5..13");
+    if (!(p->QE > 0.0f)) return fail(QCS_ERR_ARG, "QE must be positive");
+    return QCS_OK;
+}
+
+}  // namespace
+
+struct qcs_loc_data {
+    qcs_loc_para para;
+    int R, whole, capacity, max_rows;
+    uint16_t *d_rois = nullptr;
+    float *d_wle = nullptr;
+    float *d_loc = nullptr;
+    void *d_wle_scratch = nullptr;
+    size_t wle_scratch = 0;
+    qcs::CascadeState st{};
+    void *d_state = nullptr;
+    float *h_loc = nullptr;
+    int *h_counters = nullptr;
+    cudaStream_t stream = nullptr;
+    int valid = 0;
+    float ratios[7] = {0, 0, 0, 0, 0, 0, 0};
+};
+
+extern "C" {
+
+void qcs_loc_para_default(qcs_loc_para *p) {
+    if (!p) return;
+    memset(p, 0, sizeof(*p));
+    p->KAdc = 0.45f;
+    p->Offset = 100.0f;
+    p->QE = 0.72f;
+    p->ReadNoise_e = 1.3f;
+    p->ROISize = 7;
+    p->LocType = QCS_LOCTYPE_GS2D;
+    p->MultiEmitterFitEn = 0;
+    p->WLEEn = 1;
+    p->ConsecFit_DistanceTh_nm = 80.0f;
+    p->ConsecFitEn = 0;
+    p->PixelSize = 100.0f;
+    p->PixelZoom = 5.0f;
+    p->SNR_th = 5.0f;
+    p->ColorMode_3D = 0;
+    p->ImageWidth = 2048;
+    p->ImageHigh = 2048;
+    p->TotalFrameNum = 1;
+    p->MinZDepth = -500.0f;
+    p->MaxZDepth = 500.0f;
+    p->ZDepthCorrFactor = 1.0f;
+    p->p1_XGY = 1.0f;
+    p->p1_XLY = 1.0f;
+    p->DH_RotateType = 0;
+    p->DH_MeanDistance = 10.0f;
+    p->DH_DistanceTh = 2.0f;
+    p->ImagesPerGroup = 50;
+    p->IsHollowTube = 0;
+    p->StrucuteSize_2D = 40.0f;
+    p->SpatialResolutionCalcEn = 1;
+    p->SRImageWidth = ((int)(p->ImageWidth * p->PixelZoom) + 3) / 4 * 4;
+    p->SRImageHigh = ((int)(p->ImageHigh * p->PixelZoom) + 3) / 4 * 4;
+}
+
+const char *qcs_last_error(void) { return g_err.c_str(); }
+
+int qcs_device_available(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+    return n > 0;
+}
+
+int qcs_loc_deinit(qcs_loc_data *c) {
+    if (!c) return QCS_OK;
+    cudaFree(c->d_rois);
+    cudaFree(c->d_wle);
+    cudaFree(c->d_loc);
+    cudaFree(c->d_wle_scratch);
+    cudaFree(c->d_state);
+    cudaFreeHost(c->h_loc);
+    cudaFreeHost(c->h_counters);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return QCS_OK;
+}
+
+int qcs_loc_init_capacity(const qcs_loc_para *p, int capacity, qcs_loc_data **out) {
+    if (!out) return fail(QCS_ERR_ARG, "null output handle");
+    *out = nullptr;
+    int st = check_para(p, false);
+    if (st) return st;
+    if (capacity <= 0) capacity = QCS_MAX_POINT_NUM;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(QCS_ERR_CUDA, "no CUDA device: qcstorm_b200 has no CPU fallback");
+    qcs_loc_data *c = new qcs_loc_data();
+    c->para = *p;
+    c->R = p->ROISize;
+    c->whole = c->R * (c->R + 1);
+    c->capacity = capacity;
+    c->max_rows = 2 * capacity;
+    const size_t cap = (size_t)capacity;
+    auto A = [&](void **ptr, size_t bytes) { return cudaMalloc(ptr, bytes > 0 ? bytes : 1); };
+    cudaError_t e = cudaSuccess;
+    if (e == cudaSuccess) e = A((void **)&c->d_rois, cap * c->whole * sizeof(uint16_t));
+    if (e == cudaSuccess) e = A((void **)&c->d_wle, cap * QCS_WLE_PARA_NUM * sizeof(float));
+    if (e == cudaSuccess) e = A((void **)&c->d_loc, (size_t)c->max_rows * QCS_OUT_PARA_NUM * sizeof(float));
+    c->wle_scratch = qcs::wle_scratch_bytes(capacity);
+    if (e == cudaSuccess) e = A(&c->d_wle_scratch, c->wle_scratch);
+    // cascade state in one allocation
+    const size_t a_int = cap * sizeof(int), a_u8 = (cap + 255) / 256 * 256, a_row = cap * 12 * sizeof(float);
+    const size_t bytes = 3 * a_int + 3 * a_u8 + 2 * a_row + 256;
+    if (e == cudaSuccess) e = A(&c->d_state, bytes);
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&c->h_loc, (size_t)c->max_rows * QCS_OUT_PARA_NUM * sizeof(float));
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&c->h_counters, qcs::kCntNum * sizeof(int));
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        qcs_loc_deinit(c);
+        return fail(e == cudaErrorMemoryAllocation ? QCS_ERR_NOMEM : QCS_ERR_CUDA, "qcs_loc_init", e);
+    }
+    char *s = static_cast<char *>(c->d_state);
+    c->st.q_single = reinterpret_cast<int *>(s); s += a_int;
+    c->st.q2 = reinterpret_cast<int *>(s); s += a_int;
+    c->st.q3 = reinterpret_cast<int *>(s); s += a_int;
+    c->st.to2e = reinterpret_cast<uint8_t *>(s); s += a_u8;
+    c->st.res2 = reinterpret_cast<int8_t *>(s); s += a_u8;
+    c->st.res3 = reinterpret_cast<int8_t *>(s); s += a_u8;
+    c->st.extra2 = reinterpret_cast<float *>(s); s += a_row;
+    c->st.extra3 = reinterpret_cast<float *>(s); s += a_row;
+    c->st.counters = reinterpret_cast<int *>(s);
+    *out = c;
+    return QCS_OK;
+}
+
+int qcs_loc_init(const qcs_loc_para *p, qcs_loc_data **out) { return qcs_loc_init_capacity(p, QCS_MAX_POINT_NUM, out); }
+
+int qcs_loc_capacity(const qcs_loc_data *c) { return c ? c->capacity : 0; }
+
+static int check_call(qcs_loc_data *c, const qcs_loc_para *p, int n) {
+    if (!c) return fail(QCS_ERR_ARG, "null context");
+    int st = check_para(p);
+    if (st) return st;
+    if (p->ROISize != c->R) return fail(QCS_ERR_ROISIZE, "ROISize differs from the one the context was created with");
+    if (n < 0) return fail(QCS_ERR_ARG, "negative ROI count");
+    if (n > c->capacity) return fail(QCS_ERR_CAPACITY, "ROI count above the context capacity");
+    return QCS_OK;
+}
+
+int qcs_loc_localize_device(qcs_loc_data *c, const uint16_t *d_rois, const float *d_wle, const qcs_loc_para *p,
+                            int n, void *stream) {
+    int st = check_call(c, p, n);
+    if (st) return st;
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+    if (!d_rois && n > 0) return fail(QCS_ERR_ARG, "null ROI pointer");
+    const float *wle = d_wle;
+    if (!wle && n > 0) {
+        QCS_CUDA(qcs::launch_wle(d_rois, n, c->R, p->LocType, c->d_wle, c->d_wle_scratch, s), "WLE pre-pass");
+        wle = c->d_wle;
+    }
+    qcs::CascadeArgs a;
+    a.para = *p;
+    a.rois = d_rois;
+    a.wle = wle;
+    a.n = n;
+    a.loc = c->d_loc;
+    a.max_rows = c->max_rows;
+    a.stream = s;
+    QCS_CUDA(qcs::run_cascade(a, c->st), "localization cascade");
+    return QCS_OK;
+}
+
+const float *qcs_loc_device_rows(const qcs_loc_data *c) { return c ? c->d_loc : nullptr; }
+const int *qcs_loc_device_valid_num(const qcs_loc_data *c) { return c ? c->st.counters + qcs::kCntValid : nullptr; }
+uint16_t *qcs_loc_device_roi_buffer(qcs_loc_data *c) { return c ? c->d_rois : nullptr; }
+float *qcs_loc_device_wle_buffer(qcs_loc_data *c) { return c ? c->d_wle : nullptr; }
+
+static void compute_ratios(qcs_loc_data *c, const qcs_loc_para *p, int n) {
+    const int *k = c->h_counters;
+    const float div = (float)(n < 1 ? 1 : n);
+    for (int i = 0; i < 7; ++i) c->ratios[i] = 0;
+    if (n <= 0) return;
+    const int single = k[qcs::kCntSingle];
+    c->ratios[0] = (float)single / div;
+    c->ratios[3] = (float)single / div;
+    if (p->MultiEmitterFitEn) {
+        const int n2 = k[qcs::kCnt2E], n2c = k[qcs::kCnt2EClassify], n3 = k[qcs::kCnt3E], rej = k[qcs::kCntRejected];
+        c->ratios[1] = (float)n2 / div;
+        c->ratios[2] = (float)n3 / div;
+        c->ratios[3] = (float)(single - (n2 - n2c)) / div;
+        if (p->LocType == QCS_LOCTYPE_GS2D) {
+            c->ratios[4] = (float)(n2 - n3) / div;
+            c->ratios[5] = (float)(n3 - rej) / div;
+        } else {
+            c->ratios[4] = (float)(n2 - rej) / div;
+        }
+        c->ratios[6] = (float)rej / div;
+    }
+}
+
+int qcs_loc_bfgs_mle_localization(qcs_loc_data *c, const uint16_t *h_rois, const float *h_wle,
+                                  const qcs_loc_para *p, int n, void *stream) {
+    int st = check_call(c, p, n);
+    if (st) return st;
+    c->valid = 0;
+    for (int i = 0; i < 7; ++i) c->ratios[i] = 0;
+    if (n == 0) return QCS_OK;
+    if (!h_rois) return fail(QCS_ERR_ARG, "null ROI pointer");
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+    QCS_CUDA(cudaMemcpyAsync(c->d_rois, h_rois, (size_t)n * c->whole * sizeof(uint16_t), cudaMemcpyHostToDevice, s),
+             "copy ROI records");
+    if (h_wle)
+        QCS_CUDA(cudaMemcpyAsync(c->d_wle, h_wle, (size_t)n * QCS_WLE_PARA_NUM * sizeof(float),
+                                 cudaMemcpyHostToDevice, s),
+                 "copy WLE records");
+    st = qcs_loc_localize_device(c, c->d_rois, h_wle ? c->d_wle : nullptr, p, n, s);
+    if (st) return st;
+    QCS_CUDA(cudaMemcpyAsync(c->h_counters, c->st.counters, qcs::kCntNum * sizeof(int), cudaMemcpyDeviceToHost, s),
+             "read counters");
+    QCS_CUDA(cudaStreamSynchronize(s), "localization");
+    const int rows = c->h_counters[qcs::kCntValid];
+    if (rows > 0)
+        QCS_CUDA(cudaMemcpyAsync(c->h_loc, c->d_loc, (size_t)rows * QCS_OUT_PARA_NUM * sizeof(float),
+                                 cudaMemcpyDeviceToHost, s),
+                 "read localizations");
+    QCS_CUDA(cudaStreamSynchronize(s), "read localizations");
+    c->valid = rows;
+    compute_ratios(c, p, n);
+    return QCS_OK;
+}
+
+const float *qcs_loc_h_loc_arry(const qcs_loc_data *c) { return c ? c->h_loc : nullptr; }
+int qcs_loc_valid_num(const qcs_loc_data *c) { return c ? c->valid : 0; }
+
+int qcs_loc_fit_ratios(const qcs_loc_data *c, float *out7) {
+    if (!c || !out7) return fail(QCS_ERR_ARG, "null argument");
+    for (int i = 0; i < 7; ++i) out7[i] = c->ratios[i];
+    return QCS_OK;
+}
+
+int qcs_wle_estimate(qcs_loc_data *c, const uint16_t *h_rois, int n, const qcs_loc_para *p, float *h_wle) {
+    int st = check_call(c, p, n);
+    if (st) return st;
+    if (n == 0) return QCS_OK;
+    if (!h_rois || !h_wle) return fail(QCS_ERR_ARG, "null pointer");
+    cudaStream_t s = c->stream;
+    QCS_CUDA(cudaMemcpyAsync(c->d_rois, h_rois, (size_t)n * c->whole * sizeof(uint16_t), cudaMemcpyHostToDevice, s),
+             "copy ROI records");
+    QCS_CUDA(qcs::launch_wle(c->d_rois, n, c->R, p->LocType, c->d_wle, c->d_wle_scratch, s), "WLE pre-pass");
+    QCS_CUDA(cudaMemcpyAsync(h_wle, c->d_wle, (size_t)n * QCS_WLE_PARA_NUM * sizeof(float), cudaMemcpyDeviceToHost, s),
+             "read WLE records");
+    QCS_CUDA(cudaStreamSynchronize(s), "WLE pre-pass");
+    return QCS_OK;
+}
+
+int qcs_wle_estimate_device(qcs_loc_data *c, const uint16_t *d_rois, int n, const qcs_loc_para *p, float *d_wle,
+                            void *stream) {
+    int st = check_call(c, p, n);
+    if (st) return st;
+    if (n == 0) return QCS_OK;
+    if (!d_rois || !d_wle) return fail(QCS_ERR_ARG, "null pointer");
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+    QCS_CUDA(qcs::launch_wle(d_rois, n, c->R, p->LocType, d_wle, c->d_wle_scratch, s), "WLE pre-pass");
+    return QCS_OK;
+}
+
+int qcs_fit_single_device(int loc_type, const qcs_loc_para *p, const uint16_t *d_rois, const float *d_wle, int n,
+                          float *d_loc, void *stream) {
+    int st = check_para(p, false);
+    if (st) return st;
+    if (n < 0) return fail(QCS_ERR_ARG, "negative ROI count");
+    if (n == 0) return QCS_OK;
+    if (!d_rois || !d_wle || !d_loc) return fail(QCS_ERR_ARG, "null pointer");
+    qcs::FitLaunch f;
+    f.rois = d_rois;
+    f.wle = d_wle;
+    f.q = qcs::Queue{nullptr, nullptr, n};
+    f.max_count = n;
+    f.loc = d_loc;
+    f.to2e = nullptr;
+    f.mo = qcs::MultiOut{nullptr, nullptr};
+    qcs_loc_para q = *p;
+    q.MultiEmitterFitEn = 0;
+    f.para = qcs::core_para(q);
+    f.stream = static_cast<cudaStream_t>(stream);
+    QCS_CUDA(qcs::launch_fit(loc_type == QCS_LOCTYPE_AS3D ? qcs::kAS3D : qcs::kGS2D, p->ROISize, f), "fit launch");
+    return QCS_OK;
+}
+
+int qcs_crlb_device(const qcs_loc_para *p, float *d_loc, int n, void *stream) {
+    if (!p) return fail(QCS_ERR_ARG, "null parameter struct");
+    if (n < 0) return fail(QCS_ERR_ARG, "negative row count");
+    if (n == 0) return QCS_OK;
+    if (!d_loc) return fail(QCS_ERR_ARG, "null pointer");
+    QCS_CUDA(qcs::launch_crlb(d_loc, nullptr, n, n, p->LocType, p->ReadNoise_e, p->QE, p->PixelSize,
+                              static_cast<cudaStream_t>(stream)),
+             "CRLB launch");
+    return QCS_OK;
+}
+
+}  // extern "C"

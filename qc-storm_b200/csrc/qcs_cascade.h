@@ -1,0 +1,48 @@
+// Device-side cascade of the localization call (see qcs_cascade.cu).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/qcstorm_b200.h"
+
+namespace qcs {
+
+// Device counters of one localization call.
+enum {
+    kCntSingle = 0,      // single-emitter queue length
+    kCnt2E = 1,          // two-emitter queue length (classified + rejected singles)
+    kCnt2EClassify = 2,  // two-emitter queue entries that came from the classifier
+    kCnt3E = 3,          // three-emitter queue length
+    kCntRejected = 4,    // ROIs rejected by the last multi-emitter stage
+    kCntRows = 5,        // rows produced (records + appended second emitters)
+    kCntValid = 6,       // rows produced, capped at the row capacity
+    kCntNum = 8
+};
+
+// Scratch of one context, sized for `capacity` records.
+struct CascadeState {
+    int *q_single;   // capacity
+    int *q2;         // capacity
+    int *q3;         // capacity
+    uint8_t *to2e;   // capacity, indexed by record
+    int8_t *res2;    // capacity, indexed by 2E queue slot
+    int8_t *res3;    // capacity, indexed by 3E queue slot
+    float *extra2;   // capacity x 12
+    float *extra3;   // capacity x 12
+    int *counters;   // kCntNum
+};
+
+struct CascadeArgs {
+    qcs_loc_para para;
+    const uint16_t *rois;  // device, n records
+    const float *wle;      // device, n x 6
+    int n;
+    float *loc;            // device, max_rows x 12
+    int max_rows;
+    cudaStream_t stream;
+};
+
+cudaError_t run_cascade(const CascadeArgs &a, const CascadeState &st);
+
+}  // namespace qcs

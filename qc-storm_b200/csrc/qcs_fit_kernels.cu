@@ -1,0 +1,616 @@
+// Fit kernels: single-emitter GS2D / AS3D and multi-emitter GS2D-2E, GS2D-3E,
+// AS3D-2E.  One thread per ROI; a block stages its ROIs' pixels into shared
+// memory in a [pixel][thread] layout (conflict-free: thread t reads column t),
+// each thread then pre-estimates, fits with the fixed schedule of
+// qcs_fit_math.cuh and writes its 12-float row.  Queues come from device
+// memory, so the whole single -> 2E -> 3E cascade runs without host syncs.
+//
+// Reference kernels re-expressed (MLEbfgs/bfgs_MLE_dll x64/bfgsMLE_dll/bfgsMLE_dll/):
+//   bfgsMLE_Loc_LD/bfgsMLE_GS2D_core.h:57-310, 522-575   bfgsMLELoc_Gauss2D, PreEstimation_GS2D
+//   bfgsMLE_Loc_LD/bfgsMLE_AS3D_core.h:58-337, 548-607   bfgsMLELoc_AS3D, PreEstimation_AS3D
+//   bfgsMLE_Loc_HD/bfgsMLE_GS2D_2Emitter_core.h:75-371, 596-698
+//   bfgsMLE_Loc_HD/bfgsMLE_GS2D_3Emitter_core.h:77-362, 593-710
+//   bfgsMLE_Loc_HD/bfgsMLE_AS3D_2Emitter_core.h:78-422, 648-750
+// Differences in layout only: the reference writes second emitters through
+// an atomic counter (arbitrary order) and queues ROIs with atomics; here each
+// multi-emitter queue slot records its outcome and a compaction kernel
+// appends rows in queue order (qcs_cascade.cu), which is deterministic.
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "qcs_device.cuh"
+#include "qcs_fit_math.cuh"
+#include "qcs_kernels.h"
+
+#define rAScalFactor (1.0f / QCS_ASCALE)
+#define rBScalFactor (1.0f / QCS_BSCALE)
+#define rSScalFactor (1.0f / QCS_SSCALE)
+
+namespace qcs {
+namespace {
+
+constexpr int kTPB = 64;  // ROIs (threads) per block
+
+template <int R, int KIND>
+struct SmemLayout {
+    enum {
+        P = KindTraits<KIND>::P,
+        PIX = R * R,
+        IMG = 0,
+        W = PIX * kTPB,
+        D = W + (KindTraits<KIND>::WEIGHTED ? PIX * kTPB : 0),
+        TOTAL = D + P * P * kTPB,  // floats
+    };
+};
+
+// Stage the block's ROIs: element k of slot s at smem[k * kTPB + s].
+template <int R>
+__device__ __forceinline__ void stage_rois(float *s_img, const uint16_t *rois, const Queue &q, int base, int cnt,
+                                           float Offset, float KAdc) {
+    enum { PIX = R * R, WHOLE = R * (R + 1) };
+    for (int idx = threadIdx.x; idx < cnt * PIX; idx += kTPB) {
+        const int slot = idx / PIX;
+        const int k = idx - slot * PIX;
+        const int id = queue_at(q, base + slot);
+        const uint16_t u = __ldg(rois + (size_t)id * WHOLE + k);
+        s_img[k * kTPB + slot] = fmaxf((u - Offset) * KAdc, 1.0f);
+    }
+}
+
+__device__ __forceinline__ void store_row(float *loc, int id, const float (&v)[12]) {
+    float4 *dst = reinterpret_cast<float4 *>(loc + (size_t)id * 12);
+    dst[0] = make_float4(v[0], v[1], v[2], v[3]);
+    dst[1] = make_float4(v[4], v[5], v[6], v[7]);
+    dst[2] = make_float4(v[8], v[9], v[10], v[11]);
+}
+
+__device__ __forceinline__ void zero_row(float *loc, int id) {
+    float4 *dst = reinterpret_cast<float4 *>(loc + (size_t)id * 12);
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    dst[0] = z;
+    dst[1] = z;
+    dst[2] = z;
+}
+
+template <int R>
+__device__ __forceinline__ void edge_means(const float *img, float &Mean1, float &Mean2, float &Mean3, float &Mean4) {
+    Mean1 = 0;
+    Mean2 = 0;
+    Mean3 = 0;
+    Mean4 = 0;
+#pragma unroll
+    for (int cnt = 0; cnt < R; cnt++) {
+        Mean1 += img[(cnt * R + 0) * kTPB];
+        Mean2 += img[(cnt * R + R - 1) * kTPB];
+        Mean3 += img[(0 * R + cnt) * kTPB];
+        Mean4 += img[((R - 1) * R + cnt) * kTPB];
+    }
+}
+
+// Start positions of the extra emitters: the brightest (and for three
+// emitters also the second brightest) non-central block of a 3 x 3 tiling.
+template <int R>
+__device__ __forceinline__ void block_starts(const float *img, int nstart, float *xs, float *ys) {
+    const int ROISize_Half = R / 2;
+    const float ROICenter = R / 2.0f;
+    const int SumROILen = R / 3 + 1;
+    const int SumROILen_Half = SumROILen / 2;
+    int StartPos[3];
+    StartPos[0] = 0;
+    StartPos[1] = ROISize_Half - SumROILen_Half;
+    StartPos[2] = R - SumROILen;
+    float RegionPos[3];
+    RegionPos[0] = ROICenter - SumROILen / 2.0f;
+    RegionPos[1] = ROICenter;
+    RegionPos[2] = ROICenter + SumROILen / 2.0f;
+    float SumData[9];
+    for (int cnt = 0; cnt < 9; cnt++) {
+        float SumDat_t = 0;
+        const int XBias = StartPos[cnt % 3];
+        const int YBias = StartPos[cnt / 3];
+        for (int r = 0; r < SumROILen; r++)
+            for (int c = 0; c < SumROILen; c++) SumDat_t += img[((r + YBias) * R + c + XBias) * kTPB];
+        SumData[cnt] = SumDat_t;
+    }
+    SumData[9 / 2] = 0;
+    for (int e = 0; e < nstart; e++) {
+        int MaxPos = 0;
+        for (int cnt = 0; cnt < 9; cnt++)
+            if (SumData[cnt] > SumData[MaxPos]) MaxPos = cnt;
+        xs[e] = RegionPos[MaxPos % 3];
+        ys[e] = RegionPos[MaxPos / 3];
+        SumData[MaxPos] = 0;
+    }
+}
+
+__device__ __forceinline__ float zpoly(const CorePara &c, float SigmaDif) {
+    float CurZPos;
+    if (SigmaDif >= 0.0f)
+        CurZPos = c.p4_XGY * powf(SigmaDif, 4) + c.p3_XGY * powf(SigmaDif, 3) + c.p2_XGY * powf(SigmaDif, 2) +
+                  c.p1_XGY * SigmaDif + c.p0_XGY;
+    else
+        CurZPos = c.p4_XLY * powf(SigmaDif, 4) + c.p3_XLY * powf(SigmaDif, 3) + c.p2_XLY * powf(SigmaDif, 2) +
+                  c.p1_XLY * SigmaDif + c.p0_XLY;
+    return CurZPos * c.ZDepthCorrFactor;
+}
+
+// ------------------------------------------------------- single emitter ---
+template <int R, int KIND>
+__global__ void __launch_bounds__(kTPB) fit_single_kernel(const uint16_t *__restrict__ rois,
+                                                          const float *__restrict__ wle, Queue q,
+                                                          float *__restrict__ loc, uint8_t *__restrict__ to2e,
+                                                          CorePara c) {
+    typedef SmemLayout<R, KIND> L;
+    enum { P = KindTraits<KIND>::P, PIX = R * R, WHOLE = R * (R + 1), ROISize_Half = R / 2 };
+    extern __shared__ float smem[];
+    const int n = queue_len(q);
+    const int base = blockIdx.x * kTPB;
+    if (base >= n) return;
+    const int cnt = min(kTPB, n - base);
+    float *s_img = smem + L::IMG;
+    stage_rois<R>(s_img, rois, q, base, cnt, c.Offset, c.KAdc);
+    __syncthreads();
+    const int tid = threadIdx.x;
+    if (tid >= cnt) return;
+
+    const int CurFluoID = queue_at(q, base + tid);
+    const float *img = s_img + tid;
+    float *w = smem + L::W + tid;
+    float *D = smem + L::D + tid;
+    const uint16_t *hdr = rois + (size_t)CurFluoID * WHOLE + PIX;
+    const int XOffset = hdr[0];
+    const int YOffset = hdr[1];
+    const int CurFrame = hdr[2] + 65536 * hdr[3];
+    const float *pw = wle + (size_t)CurFluoID * QCS_WLE_PARA_NUM;
+
+    float Ininf[P];
+    const RoiRef roi{img, w, kTPB};
+    float row[12];
+    bool accepted;
+    float CurSNR;
+    int IsFittingValid;
+
+    if (KIND == kGS2D) {
+        const float XYLBound = R / 2.0f - 1.5f;
+        const float XYUBound = R / 2.0f + 1.5f;
+        float Simga_Max_Th = R / 1.5f / 2.35f;
+        if (c.MultiEmitterFitEn) Simga_Max_Th = R / 2.0f / 2.35f;
+        float SigmaL = pw[1], SigmaR = pw[2], SigmaU = pw[3], SigmaD = pw[4];
+        const int MoleculeType = pw[5];
+        SigmaL = fminf(SigmaL, SigmaR);
+        SigmaU = fminf(SigmaU, SigmaD);
+        float WLE_SigmaX = fminf(SigmaL, SigmaU);
+        WLE_SigmaX = fminf(WLE_SigmaX, R / 2.0f / 2.35f);
+        // PreEstimation_GS2D
+        {
+            const int CenterPos = R / 2;
+            float Mean1, Mean2, Mean3, Mean4;
+            edge_means<R>(img, Mean1, Mean2, Mean3, Mean4);
+            Mean1 = fminf(Mean1, Mean2);
+            Mean3 = fminf(Mean3, Mean4);
+            const float Bkg = (Mean1 + Mean3) / 2 / R;
+            const float Amp = img[(CenterPos * R + CenterPos) * kTPB] - Bkg;
+            const float SigmaX = WLE_SigmaX;
+            const float ParaSigma1 = (1.0f / (2.0f * SigmaX * SigmaX));
+            Ininf[0] = Amp * rAScalFactor;
+            Ininf[1] = (float)CenterPos + 0.5f;
+            Ininf[2] = (float)CenterPos + 0.5f;
+            Ininf[3] = ParaSigma1 * rSScalFactor;
+            Ininf[4] = Bkg * rBScalFactor;
+        }
+        if (MoleculeType != QCS_MOLECULE_MLEFIT) {
+            WLE_SigmaX = WLE_SigmaX / 1.2f;
+            WLE_SigmaX = fminf(WLE_SigmaX, R / 2.0f / 2.35f);
+        }
+        if (c.WLEEn == 0 && MoleculeType != QCS_MOLECULE_MULTIFIT) WLE_SigmaX = R;
+        wle_weights<R>(w, kTPB, WLE_SigmaX, WLE_SigmaX, MoleculeType);
+        mle_fit<R, kGS2D>(roi, Ininf, D, kTPB);
+
+        const float PeakPhoton = Ininf[0] * QCS_ASCALE / c.QE;
+        const float Background = Ininf[4] * QCS_BSCALE / c.QE;
+        float FittedXPos = Ininf[1];
+        float FittedYPos = Ininf[2];
+        float SimgaX = Ininf[3] * QCS_SSCALE;
+        SimgaX = sqrtf(0.5f / SimgaX);
+        FittedXPos = isnan(FittedXPos) ? -1 : FittedXPos;
+        FittedYPos = isnan(FittedYPos) ? -1 : FittedYPos;
+        SimgaX = isnan(SimgaX) ? -1 : SimgaX;
+        CurSNR = sqrtf(c.QE) * PeakPhoton / sqrtf(PeakPhoton + Background);
+        const float TotalPhoton = PeakPhoton * 2 * 3.141593f * SimgaX * SimgaX;
+        const float XPos = FittedXPos - ROISize_Half + XOffset;
+        const float YPos = FittedYPos - ROISize_Half + YOffset;
+        IsFittingValid = isnan(Background) ? 0 : 1;
+        accepted = IsFittingValid && (CurSNR > 4.0f) && (SimgaX <= Simga_Max_Th) && (SimgaX >= 0.6f) &&
+                   (FittedXPos > XYLBound) && (FittedXPos < XYUBound) && (FittedYPos > XYLBound) &&
+                   (FittedYPos < XYUBound);
+        row[0] = PeakPhoton;
+        row[1] = XPos;
+        row[2] = YPos;
+        row[3] = 0.0f;
+        row[4] = SimgaX;
+        row[5] = SimgaX;
+        row[6] = TotalPhoton;
+        row[7] = Background;
+        row[8] = CurSNR;
+        row[11] = CurFrame;
+    } else {  // kAS3D
+        const float XYLBound = R / 2.0f - 2.5f;
+        const float XYUBound = R / 2.0f + 2.5f;
+        float Simga_Max_Th = R / 1.5f / 2.35f;
+        if (c.MultiEmitterFitEn) Simga_Max_Th = R / 2.0f / 2.35f;
+        const float Simga_Min_Th = 0.8f;
+        const float SigmaL = pw[1], SigmaR = pw[2], SigmaU = pw[3], SigmaD = pw[4];
+        const int MoleculeType = pw[5];
+        float WLE_SigmaX = fminf(SigmaL, SigmaR);
+        float WLE_SigmaY = fminf(SigmaU, SigmaD);
+        // PreEstimation_AS3D
+        {
+            const int CenterPos = R / 2;
+            float Mean1, Mean2, Mean3, Mean4;
+            edge_means<R>(img, Mean1, Mean2, Mean3, Mean4);
+            Mean1 = fminf(Mean1, Mean2);
+            Mean3 = fminf(Mean3, Mean4);
+            const float Bkg = (Mean1 + Mean3) / 2 / R;
+            const float Amp = img[(CenterPos * R + CenterPos) * kTPB] - Bkg;
+            const float SigmaX = WLE_SigmaX;
+            const float SigmaY = WLE_SigmaY;
+            const float SigmaX1 = rSScalFactor * (0.5f / (SigmaX * SigmaX));
+            const float SigmaY1 = rSScalFactor * (0.5f / (SigmaY * SigmaY));
+            Ininf[0] = Amp * rAScalFactor;
+            Ininf[1] = (float)CenterPos + 0.5f;
+            Ininf[2] = (float)CenterPos + 0.5f;
+            Ininf[3] = SigmaX1;
+            Ininf[4] = SigmaY1;
+            Ininf[5] = Bkg * rBScalFactor;
+        }
+        if (MoleculeType != QCS_MOLECULE_MLEFIT) {
+            WLE_SigmaX = fminf(WLE_SigmaX, R / 1.6f / 2.35f);
+            WLE_SigmaY = fminf(WLE_SigmaY, R / 1.6f / 2.35f);
+        }
+        if (c.WLEEn == 0 && MoleculeType != QCS_MOLECULE_MULTIFIT) {
+            WLE_SigmaX = R;
+            WLE_SigmaY = R;
+        }
+        wle_weights<R>(w, kTPB, WLE_SigmaX, WLE_SigmaY, MoleculeType);
+        mle_fit<R, kAS3D>(roi, Ininf, D, kTPB);
+
+        float PeakPhoton = Ininf[0] * QCS_ASCALE;
+        float Background = Ininf[5] * QCS_BSCALE;
+        float FittedXPos = Ininf[1];
+        float FittedYPos = Ininf[2];
+        float SimgaX = Ininf[3] * QCS_SSCALE;
+        float SimgaY = Ininf[4] * QCS_SSCALE;
+        SimgaX = sqrtf(0.5f / SimgaX);
+        SimgaY = sqrtf(0.5f / SimgaY);
+        FittedXPos = isnan(FittedXPos) ? -1 : FittedXPos;
+        FittedYPos = isnan(FittedYPos) ? -1 : FittedYPos;
+        SimgaX = isnan(SimgaX) ? -1 : SimgaX;
+        SimgaY = isnan(SimgaY) ? -1 : SimgaY;
+        CurSNR = PeakPhoton / sqrtf(PeakPhoton + Background);
+        PeakPhoton = PeakPhoton / c.QE;
+        Background = Background / c.QE;
+        const float TotalPhoton = PeakPhoton * 2 * 3.141593f * SimgaX * SimgaY;
+        const float SigmaDif = SimgaX * SimgaX - SimgaY * SimgaY;
+        const float CurZPos = zpoly(c, SigmaDif);
+        const float XPos = FittedXPos - ROISize_Half + XOffset;
+        const float YPos = FittedYPos - ROISize_Half + YOffset;
+        const float MeanSigma = (SimgaX + SimgaY) / 2;
+        IsFittingValid = isnan(Background) ? 0 : 1;
+        accepted = IsFittingValid && (CurSNR > 3.5f) && (MeanSigma > Simga_Min_Th) && (MeanSigma < Simga_Max_Th) &&
+                   (FittedXPos > XYLBound) && (FittedXPos < XYUBound) && (FittedYPos > XYLBound) &&
+                   (FittedYPos < XYUBound);
+        row[0] = PeakPhoton;
+        row[1] = XPos;
+        row[2] = YPos;
+        row[3] = CurZPos;
+        row[4] = SimgaX;
+        row[5] = SimgaY;
+        row[6] = TotalPhoton;
+        row[7] = Background;
+        row[8] = CurSNR;
+        row[11] = CurFrame;
+    }
+    if (accepted) {
+        row[9] = 0.0f;
+        row[10] = 0.0f;
+        store_row(loc, CurFluoID, row);
+    } else {
+        zero_row(loc, CurFluoID);
+    }
+    if (to2e) to2e[CurFluoID] = (!accepted && c.MultiEmitterFitEn && IsFittingValid && (CurSNR > 6.0f)) ? 1 : 0;
+}
+
+// -------------------------------------------------------- multi emitter ---
+template <int R, int KIND>
+__global__ void __launch_bounds__(kTPB) fit_multi_kernel(const uint16_t *__restrict__ rois,
+                                                         const float *__restrict__ wle, Queue q,
+                                                         float *__restrict__ loc, MultiOut mo, CorePara c) {
+    typedef SmemLayout<R, KIND> L;
+    enum { P = KindTraits<KIND>::P, PIX = R * R, WHOLE = R * (R + 1), ROISize_Half = R / 2 };
+    extern __shared__ float smem[];
+    const int n = queue_len(q);
+    const int base = blockIdx.x * kTPB;
+    if (base >= n) return;
+    const int cnt = min(kTPB, n - base);
+    float *s_img = smem + L::IMG;
+    stage_rois<R>(s_img, rois, q, base, cnt, c.Offset, c.KAdc);
+    __syncthreads();
+    const int tid = threadIdx.x;
+    if (tid >= cnt) return;
+
+    const int slot = base + tid;
+    const int CurFluoID = queue_at(q, slot);
+    const float *img = s_img + tid;
+    float *w = smem + L::W + tid;
+    float *D = smem + L::D + tid;
+    const uint16_t *hdr = rois + (size_t)CurFluoID * WHOLE + PIX;
+    const int XOffset = hdr[0];
+    const int YOffset = hdr[1];
+    const int CurFrame = hdr[2] + 65536 * hdr[3];
+    const float ROICenter = R / 2.0f;
+    const float QE = c.QE;
+
+    float Ininf[P];
+    const RoiRef roi{img, w, kTPB};
+    float NearNeighborDistance = 1000;
+
+    if (KIND == k2E) {
+        float WLE_SigmaX = R / 1.8f / 2.35f;
+        NearNeighborDistance = wle[(size_t)CurFluoID * QCS_WLE_PARA_NUM + 0];
+        // PreEstimation_GS2D_2E
+        {
+            float Mean1, Mean2, Mean3, Mean4;
+            edge_means<R>(img, Mean1, Mean2, Mean3, Mean4);
+            Mean1 = fminf(Mean1, Mean2);
+            Mean3 = fminf(Mean3, Mean4);
+            Mean1 = fminf(Mean1, Mean3);
+            const float Bkg = Mean1 / R;
+            const float Amp = img[(ROISize_Half * R + ROISize_Half) * kTPB] - Bkg;
+            const float SigmaX = R / 2.2f / 2.35f;
+            const float SigmaX1 = (1.0f / (2.0f * SigmaX * SigmaX));
+            float xs[1], ys[1];
+            block_starts<R>(img, 1, xs, ys);
+            Ininf[0] = 0.8f * Amp * rAScalFactor;
+            Ininf[1] = ROICenter;
+            Ininf[2] = ROICenter;
+            Ininf[3] = 0.8f * Amp * rAScalFactor;
+            Ininf[4] = xs[0];
+            Ininf[5] = ys[0];
+            Ininf[6] = SigmaX1 * rSScalFactor;
+            Ininf[7] = 0.8f * Bkg * rBScalFactor;
+        }
+        if (c.WLEEn == 0) WLE_SigmaX = R;
+        wle_weights<R>(w, kTPB, WLE_SigmaX, WLE_SigmaX, QCS_MOLECULE_MULTIFIT);
+        mle_fit<R, k2E>(roi, Ininf, D, kTPB);
+    } else if (KIND == k3E) {
+        // PreEstimation_GS2D_3E
+        float Mean1, Mean2, Mean3, Mean4;
+        edge_means<R>(img, Mean1, Mean2, Mean3, Mean4);
+        Mean1 = fminf(Mean1, Mean2);
+        Mean3 = fminf(Mean3, Mean4);
+        const float Bkg = (Mean1 + Mean3) / 2 / R;
+        const float Amp = img[(ROISize_Half * R + ROISize_Half) * kTPB] - Bkg;
+        const float SigmaX = R / 2.2f / 2.35f;
+        const float SigmaX1 = (1.0f / (2.0f * SigmaX * SigmaX));
+        float xs[2], ys[2];
+        block_starts<R>(img, 2, xs, ys);
+        Ininf[0] = 0.7f * Amp * rAScalFactor;
+        Ininf[1] = ROICenter;
+        Ininf[2] = ROICenter;
+        Ininf[3] = 0.7f * Amp * rAScalFactor;
+        Ininf[4] = xs[0];
+        Ininf[5] = ys[0];
+        Ininf[6] = 0.3f * Amp * rAScalFactor;
+        Ininf[7] = xs[1];
+        Ininf[8] = ys[1];
+        Ininf[9] = SigmaX1 * rSScalFactor;
+        Ininf[10] = 0.8f * Bkg * rBScalFactor;
+        mle_fit<R, k3E>(roi, Ininf, D, kTPB);
+    } else {  // kAS3D2E
+        float Mean1, Mean2, Mean3, Mean4;
+        edge_means<R>(img, Mean1, Mean2, Mean3, Mean4);
+        Mean1 = fminf(Mean1, Mean2);
+        Mean3 = fminf(Mean3, Mean4);
+        const float Bkg = (Mean1 + Mean3) / 2 / R;
+        const float Amp = img[(ROISize_Half * R + ROISize_Half) * kTPB] - Bkg;
+        const float SigmaX = R / 2.2f / 2.35f;
+        const float SigmaY = R / 2.2f / 2.35f;
+        const float SigmaX1 = rSScalFactor * (0.5f / (SigmaX * SigmaX));
+        const float SigmaY1 = rSScalFactor * (0.5f / (SigmaY * SigmaY));
+        float xs[1], ys[1];
+        block_starts<R>(img, 1, xs, ys);
+        Ininf[0] = 0.7f * Amp * rAScalFactor;
+        Ininf[1] = ROICenter;
+        Ininf[2] = ROICenter;
+        Ininf[3] = SigmaX1;
+        Ininf[4] = SigmaY1;
+        Ininf[5] = 0.7f * Amp * rAScalFactor;
+        Ininf[6] = xs[0];
+        Ininf[7] = ys[0];
+        Ininf[8] = SigmaX1;
+        Ininf[9] = SigmaY1;
+        Ininf[10] = 0.8f * Bkg * rBScalFactor;
+        mle_fit<R, kAS3D2E>(roi, Ininf, D, kTPB);
+    }
+
+    // emitter selection (2Emitter_core.h:245-271, 3Emitter_core.h:247-280)
+    enum { NE = (KIND == k3E) ? 3 : 2, STRIDE = (KIND == kAS3D2E) ? 5 : 3 };
+    float row0[12], row1[12];
+    int result = 0;
+    if (KIND == kAS3D2E) {
+        Ininf[0] = Ininf[0] * QCS_ASCALE / QE;
+        Ininf[5] = Ininf[5] * QCS_ASCALE / QE;
+        Ininf[3] = sqrtf(0.5f / (Ininf[3] * QCS_SSCALE));
+        Ininf[4] = sqrtf(0.5f / (Ininf[4] * QCS_SSCALE));
+        Ininf[8] = sqrtf(0.5f / (Ininf[8] * QCS_SSCALE));
+        Ininf[9] = sqrtf(0.5f / (Ininf[9] * QCS_SSCALE));
+    } else if (KIND == k2E) {
+        Ininf[0] = Ininf[0] * QCS_ASCALE / QE;
+        Ininf[3] = Ininf[3] * QCS_ASCALE / QE;
+    } else {
+        Ininf[0] = Ininf[0] * QCS_ASCALE / QE;
+        Ininf[3] = Ininf[3] * QCS_ASCALE / QE;
+        Ininf[6] = Ininf[6] * QCS_ASCALE / QE;
+    }
+    const float Background = Ininf[P - 1] * QCS_BSCALE / QE;
+    const int IsFittingValid = isnan(Background) ? 0 : 1;
+    float Distance[NE];
+#pragma unroll
+    for (int e = 0; e < NE; e++) {
+        const float curPeak = Ininf[STRIDE * e + 0];
+        float curx = Ininf[STRIDE * e + 1];
+        float cury = Ininf[STRIDE * e + 2];
+        if (fabsf(curx - ROICenter) >= ROISize_Half) curx = -100;
+        if (fabsf(cury - ROICenter) >= ROISize_Half) cury = -100;
+        Distance[e] = sqrtf((curx - ROICenter) * (curx - ROICenter) + (cury - ROICenter) * (cury - ROICenter));
+        Distance[e] = curPeak * (R - Distance[e]);
+    }
+    int MoleculeSel0 = 0, MoleculeSel1 = 0;
+#pragma unroll
+    for (int e = 0; e < NE; e++)
+        if (Distance[e] > Distance[MoleculeSel0]) MoleculeSel0 = e;
+    if (NE == 2) {
+        MoleculeSel1 = 1 - MoleculeSel0;
+    } else {
+#pragma unroll
+        for (int e = 0; e < NE; e++)
+            if (e == MoleculeSel0) Distance[e] = -100;
+#pragma unroll
+        for (int e = 0; e < NE; e++)
+            if (Distance[e] > Distance[MoleculeSel1]) MoleculeSel1 = e;
+    }
+    // dynamic-index reads through a small switch keep Ininf in registers
+    auto get = [&](int i) {
+        float v = Ininf[0];
+#pragma unroll
+        for (int k = 1; k < P; k++)
+            if (k == i) v = Ininf[k];
+        return v;
+    };
+    const float PeakPhoton0 = get(STRIDE * MoleculeSel0 + 0);
+    const float XPos0_0 = get(STRIDE * MoleculeSel0 + 1);
+    const float YPos0_0 = get(STRIDE * MoleculeSel0 + 2);
+    const float PeakPhoton1 = get(STRIDE * MoleculeSel1 + 0);
+    const float XPos1_0 = get(STRIDE * MoleculeSel1 + 1);
+    const float YPos1_0 = get(STRIDE * MoleculeSel1 + 2);
+    const float Dist01 = sqrtf((XPos0_0 - XPos1_0) * (XPos0_0 - XPos1_0) + (YPos0_0 - YPos1_0) * (YPos0_0 - YPos1_0));
+
+    if (KIND == kAS3D2E) {
+        const float Simga_Max_Th = R / 1.9f / 2.35f;
+        const float Simga_Min_Th = 0.8f;
+        const float SimgaX0 = get(STRIDE * MoleculeSel0 + 3), SimgaY0 = get(STRIDE * MoleculeSel0 + 4);
+        const float SimgaX1 = get(STRIDE * MoleculeSel1 + 3), SimgaY1 = get(STRIDE * MoleculeSel1 + 4);
+        const float TotalPhoton0 = PeakPhoton0 * 2 * 3.141593f * SimgaX0 * SimgaY0;
+        const float CurSNR0 = sqrtf(QE) * PeakPhoton0 / sqrtf(PeakPhoton0 + Background);
+        const float CurZPos0 = zpoly(c, SimgaX0 * SimgaX0 - SimgaY0 * SimgaY0);
+        const float MeanSigma0 = (SimgaX0 + SimgaY0) / 2;
+        const float TotalPhoton1 = PeakPhoton1 * 2 * 3.141593f * SimgaX1 * SimgaY1;
+        const float CurSNR1 = sqrtf(QE) * PeakPhoton1 / sqrtf(PeakPhoton1 + Background);
+        const float CurZPos1 = zpoly(c, SimgaX1 * SimgaX1 - SimgaY1 * SimgaY1);
+        const float MeanSigma1 = (SimgaX1 + SimgaY1) / 2;
+        if (IsFittingValid && (CurSNR0 > 5.5f) && (MeanSigma0 > 0.6f) && (MeanSigma0 > Simga_Min_Th) &&
+            (MeanSigma0 <= Simga_Max_Th)) {
+            result = 1;
+            row0[0] = PeakPhoton0; row0[1] = XPos0_0 - ROISize_Half + XOffset; row0[2] = YPos0_0 - ROISize_Half + YOffset;
+            row0[3] = CurZPos0; row0[4] = SimgaX0; row0[5] = SimgaY0; row0[6] = TotalPhoton0; row0[7] = Background;
+            row0[8] = CurSNR0; row0[9] = 0.0f; row0[10] = 0.0f; row0[11] = CurFrame;
+            if ((Dist01 > 1.5f) && (CurSNR1 > 5.2f) && (NearNeighborDistance > ROICenter) && (MeanSigma1 > 0.6f) &&
+                (MeanSigma1 > Simga_Min_Th) && (MeanSigma1 <= Simga_Max_Th) && (PeakPhoton1 > PeakPhoton0 / 3.0f) &&
+                (XPos1_0 > 1) && (YPos1_0 > 1) && (XPos1_0 < R - 1) && (YPos1_0 < R - 1)) {
+                result = 2;
+                row1[0] = PeakPhoton1; row1[1] = XPos1_0 - ROISize_Half + XOffset; row1[2] = YPos1_0 - ROISize_Half + YOffset;
+                row1[3] = CurZPos1; row1[4] = SimgaX1; row1[5] = SimgaY1; row1[6] = TotalPhoton1; row1[7] = Background;
+                row1[8] = CurSNR1; row1[9] = 0.0f; row1[10] = 0.0f; row1[11] = CurFrame;
+            }
+        }
+    } else {
+        const float Simga_Max_Th = R / 2.0f / 2.35f;
+        const float SimgaX = sqrtf(0.5f / (Ininf[P - 2] * QCS_SSCALE));
+        const float TotalPhoton0 = PeakPhoton0 * 2 * 3.141593f * SimgaX * SimgaX;
+        const float CurSNR0 = sqrtf(QE) * PeakPhoton0 / sqrtf(PeakPhoton0 + Background);
+        const float TotalPhoton1 = PeakPhoton1 * 2 * 3.141593f * SimgaX * SimgaX;
+        const float CurSNR1 = sqrtf(QE) * PeakPhoton1 / sqrtf(PeakPhoton1 + Background);
+        if (IsFittingValid && (CurSNR0 > 5.5f) && (SimgaX > 0.6f) && (SimgaX <= Simga_Max_Th)) {
+            result = 1;
+            row0[0] = PeakPhoton0; row0[1] = XPos0_0 - ROISize_Half + XOffset; row0[2] = YPos0_0 - ROISize_Half + YOffset;
+            row0[3] = 0.0f; row0[4] = SimgaX; row0[5] = SimgaX; row0[6] = TotalPhoton0; row0[7] = Background;
+            row0[8] = CurSNR0; row0[9] = 0.0f; row0[10] = 0.0f; row0[11] = CurFrame;
+            const bool nn_ok = (KIND == k3E) ? (NearNeighborDistance > ROICenter) : (NearNeighborDistance >= ROICenter);
+            if ((Dist01 > 1.5f) && (CurSNR1 > 5.2f) && nn_ok && (PeakPhoton1 > PeakPhoton0 / 2.0f) && (XPos1_0 > 1) &&
+                (YPos1_0 > 1) && (XPos1_0 < R - 1) && (YPos1_0 < R - 1)) {
+                result = 2;
+                row1[0] = PeakPhoton1; row1[1] = XPos1_0 - ROISize_Half + XOffset; row1[2] = YPos1_0 - ROISize_Half + YOffset;
+                row1[3] = 0.0f; row1[4] = SimgaX; row1[5] = SimgaX; row1[6] = TotalPhoton1; row1[7] = Background;
+                row1[8] = CurSNR1; row1[9] = 0.0f; row1[10] = 0.0f; row1[11] = CurFrame;
+            }
+        }
+    }
+    if (result >= 1)
+        store_row(loc, CurFluoID, row0);
+    else
+        zero_row(loc, CurFluoID);
+    if (result == 2) store_row(mo.extra, slot, row1);
+    mo.result[slot] = (int8_t)result;
+}
+
+template <int R, int KIND>
+cudaError_t launch_single(const FitLaunch &a) {
+    const size_t smem = SmemLayout<R, KIND>::TOTAL * sizeof(float);
+    auto k = fit_single_kernel<R, KIND>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const int grid = (a.max_count + kTPB - 1) / kTPB;
+    if (grid == 0) return cudaSuccess;
+    k<<<grid, kTPB, smem, a.stream>>>(a.rois, a.wle, a.q, a.loc, a.to2e, a.para);
+    return cudaGetLastError();
+}
+
+template <int R, int KIND>
+cudaError_t launch_multi(const FitLaunch &a) {
+    const size_t smem = SmemLayout<R, KIND>::TOTAL * sizeof(float);
+    auto k = fit_multi_kernel<R, KIND>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const int grid = (a.max_count + kTPB - 1) / kTPB;
+    if (grid == 0) return cudaSuccess;
+    k<<<grid, kTPB, smem, a.stream>>>(a.rois, a.wle, a.q, a.loc, a.mo, a.para);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+// ROI sizes: odd 5..17 for single emitter, 5..13 for multi emitter (the
+// reference's shared-memory limit, bfgsMLE_Multi_Emitter_Fit.cu:62-70).
+cudaError_t launch_fit(int kind, int R, const FitLaunch &a) {
+#define QCS_SINGLE(RR)                                              \
+    case RR:                                                        \
+        return kind == kGS2D ? launch_single<RR, kGS2D>(a) : launch_single<RR, kAS3D>(a);
+#define QCS_MULTI(RR)                                                                        \
+    case RR:                                                                                 \
+        return kind == k2E ? launch_multi<RR, k2E>(a)                                        \
+                           : (kind == k3E ? launch_multi<RR, k3E>(a) : launch_multi<RR, kAS3D2E>(a));
+    if (kind == kGS2D || kind == kAS3D) {
+        switch (R) {
+            QCS_SINGLE(5)
+            QCS_SINGLE(7)
+            QCS_SINGLE(9)
+            QCS_SINGLE(11)
+            QCS_SINGLE(13)
+            QCS_SINGLE(15)
+            QCS_SINGLE(17)
+        }
+    } else {
+        switch (R) {
+            QCS_MULTI(5)
+            QCS_MULTI(7)
+            QCS_MULTI(9)
+            QCS_MULTI(11)
+            QCS_MULTI(13)
+        }
+    }
+#undef QCS_SINGLE
+#undef QCS_MULTI
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace qcs

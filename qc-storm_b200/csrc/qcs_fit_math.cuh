@@ -1,0 +1,288 @@
+// Device arithmetic of the MLEbfgs fit: losses, numerical gradient, BFGS
+// update and the fixed iteration schedule, one CUDA thread per ROI.
+//
+// Bit-level contract: every floating-point expression here has the operand
+// order and shape of the reference CUDA code (QC-STORM bfgsMLE_dll), and the
+// same __expf/__logf intrinsics, so that nvcc emits the same rounding and the
+// same fused multiply-adds and the results equal the reference kernels' bit
+// for bit on the same GPU.  The fixed-schedule optimiser with a numerical
+// gradient amplifies any rounding difference (a single fused multiply-add
+// more or less moves most fits by more than 1e-3 px), so this is the only way
+// to reproduce the reference's results rather than its statistics.
+// References (MLEbfgs/bfgs_MLE_dll x64/bfgsMLE_dll/bfgsMLE_dll/):
+//   loss        bfgsMLE_Loc_LD/bfgsMLE_GS2D_core.h:459-518, bfgsMLE_AS3D_core.h:485-544,
+//               bfgsMLE_Loc_HD/bfgsMLE_GS2D_2Emitter_core.h:519-592,
+//               bfgsMLE_GS2D_3Emitter_core.h:511-589, bfgsMLE_AS3D_2Emitter_core.h:570-644
+//   gradient    bfgsMLE_GS2D_core.h:430-454 (same in the other kinds)
+//   schedule    bfgsMLE_GS2D_core.h:313-426 (same in the other kinds)
+//   BFGS update bfgsMLE_Loc_LD/bfgsMLE_core.h:65-204
+#pragma once
+
+#include <cstdint>
+
+namespace qcs {
+
+enum FitKind { kGS2D = 0, kAS3D = 1, k2E = 2, k3E = 3, kAS3D2E = 4 };
+
+// parameters, iterations, loss clamp (0 or 0.01), weighted loss
+template <int KIND> struct KindTraits;
+template <> struct KindTraits<kGS2D> { enum { P = 5, IT = 8, CLAMP001 = 0, WEIGHTED = 1 }; };
+template <> struct KindTraits<kAS3D> { enum { P = 6, IT = 11, CLAMP001 = 1, WEIGHTED = 1 }; };
+template <> struct KindTraits<k2E> { enum { P = 8, IT = 13, CLAMP001 = 0, WEIGHTED = 1 }; };
+template <> struct KindTraits<k3E> { enum { P = 11, IT = 16, CLAMP001 = 0, WEIGHTED = 0 }; };
+template <> struct KindTraits<kAS3D2E> { enum { P = 11, IT = 16, CLAMP001 = 1, WEIGHTED = 0 }; };
+
+constexpr int kBisections = 11;
+
+// Scaled parameterisation: amplitude/128, background/64, 1/(2 sigma^2)/0.1
+// (bfgsMLE_core.h:52-60).
+#define QCS_ASCALE (128.0f)
+#define QCS_BSCALE (64.0f)
+#define QCS_SSCALE (0.1f)
+
+// One ROI's pixels as seen by its thread: element k at img[k * ld].
+struct RoiRef {
+    const float *img;  // photoelectrons, max((adu - offset) * gain, 1)
+    const float *w;    // weighted-MLE mask (read by the weighted kinds only)
+    int ld;
+};
+
+template <int R, int KIND>
+__device__ __forceinline__ float loss(const RoiRef &roi, float *Ininf) {
+    typedef KindTraits<KIND> T;
+#pragma unroll
+    for (int k = 0; k < T::P; k++) {
+        if (T::CLAMP001) {
+            if (Ininf[k] < 0.01f) Ininf[k] = 0.01f;
+        } else {
+            if (Ininf[k] < 0.0f) Ininf[k] = 0.0f;
+        }
+    }
+    float TotalLoss = 0;
+    for (int row = 0; row < R; row++) {
+        for (int col = 0; col < R; col++) {
+            const float pixval = roi.img[(row * R + col) * roi.ld];
+            const float rowpos = row + 0.5f;
+            const float colpos = col + 0.5f;
+            float Loss_t;
+            if (KIND == kGS2D) {
+                float tdat = -((colpos - Ininf[1]) * (colpos - Ininf[1]) + (rowpos - Ininf[2]) * (rowpos - Ininf[2])) *
+                             Ininf[3] * QCS_SSCALE;
+                float IVal = Ininf[0] * QCS_ASCALE * __expf(tdat) + Ininf[4] * QCS_BSCALE;
+                Loss_t = IVal - pixval - pixval * (__logf(IVal) - __logf(pixval));
+            } else if (KIND == kAS3D) {
+                float tdat = -((colpos - Ininf[1]) * (colpos - Ininf[1]) * Ininf[3] * QCS_SSCALE +
+                               (rowpos - Ininf[2]) * (rowpos - Ininf[2]) * Ininf[4] * QCS_SSCALE);
+                float IVal = Ininf[0] * QCS_ASCALE * __expf(tdat) + Ininf[5] * QCS_BSCALE;
+                Loss_t = IVal - pixval - pixval * (__logf(IVal) - __logf(pixval));
+            } else if (KIND == k2E) {
+                float IVal0 = Ininf[0] * QCS_ASCALE *
+                              __expf(-((colpos - Ininf[1]) * (colpos - Ininf[1]) + (rowpos - Ininf[2]) * (rowpos - Ininf[2])) *
+                                     Ininf[6] * QCS_SSCALE);
+                float IVal1 = Ininf[3] * QCS_ASCALE *
+                              __expf(-((colpos - Ininf[4]) * (colpos - Ininf[4]) + (rowpos - Ininf[5]) * (rowpos - Ininf[5])) *
+                                     Ininf[6] * QCS_SSCALE);
+                float IVal_all = IVal0 + IVal1 + Ininf[7] * QCS_BSCALE;
+                Loss_t = IVal_all - pixval - pixval * (__logf(IVal_all) - __logf(pixval));
+            } else if (KIND == k3E) {
+                float IVal0 = Ininf[0] * QCS_ASCALE *
+                              __expf(-((colpos - Ininf[1]) * (colpos - Ininf[1]) + (rowpos - Ininf[2]) * (rowpos - Ininf[2])) *
+                                     Ininf[9] * QCS_SSCALE);
+                float IVal1 = Ininf[3] * QCS_ASCALE *
+                              __expf(-((colpos - Ininf[4]) * (colpos - Ininf[4]) + (rowpos - Ininf[5]) * (rowpos - Ininf[5])) *
+                                     Ininf[9] * QCS_SSCALE);
+                float IVal2 = Ininf[6] * QCS_ASCALE *
+                              __expf(-((colpos - Ininf[7]) * (colpos - Ininf[7]) + (rowpos - Ininf[8]) * (rowpos - Ininf[8])) *
+                                     Ininf[9] * QCS_SSCALE);
+                float IVal_all = IVal0 + IVal1 + IVal2 + Ininf[10] * QCS_BSCALE;
+                Loss_t = IVal_all - pixval - pixval * (__logf(IVal_all) - __logf(pixval));
+            } else {  // kAS3D2E
+                float IVal0 = Ininf[0] * QCS_ASCALE *
+                              __expf(-((colpos - Ininf[1]) * (colpos - Ininf[1]) * Ininf[3] * QCS_SSCALE +
+                                       (rowpos - Ininf[2]) * (rowpos - Ininf[2]) * Ininf[4] * QCS_SSCALE));
+                float IVal1 = Ininf[5] * QCS_ASCALE *
+                              __expf(-((colpos - Ininf[6]) * (colpos - Ininf[6]) * Ininf[8] * QCS_SSCALE +
+                                       (rowpos - Ininf[7]) * (rowpos - Ininf[7]) * Ininf[9] * QCS_SSCALE));
+                float IVal_all = IVal0 + IVal1 + Ininf[10] * QCS_BSCALE;
+                Loss_t = IVal_all - pixval - pixval * (__logf(IVal_all) - __logf(pixval));
+            }
+            if (T::WEIGHTED)
+                TotalLoss = TotalLoss + roi.w[(row * R + col) * roi.ld] * Loss_t;
+            else
+                TotalLoss = TotalLoss + Loss_t;
+        }
+    }
+    return TotalLoss;
+}
+
+// Central difference on a working copy; each loss call clamps the copy in
+// place and later parameters see the clamped values, as in the reference.
+template <int R, int KIND>
+__device__ __forceinline__ void numerical_gradient(const RoiRef &roi, const float *Ininf, float *grad) {
+    enum { P = KindTraits<KIND>::P };
+    float tIninf[P];
+#pragma unroll
+    for (int cnt = 0; cnt < P; cnt++) tIninf[cnt] = Ininf[cnt];
+    for (int cnt = 0; cnt < P; cnt++) {
+        tIninf[cnt] = tIninf[cnt] - 0.002f;
+        float tgradn = loss<R, KIND>(roi, tIninf);
+        tIninf[cnt] = tIninf[cnt] + 0.004f;
+        float tgradp = loss<R, KIND>(roi, tIninf);
+        grad[cnt] = (tgradp - tgradn) * 250.0f;
+        tIninf[cnt] = tIninf[cnt] - 0.002f;
+    }
+}
+
+// D <- (I - s y'/(y's)) D (I - y s'/(y's)) + s s'/(y's); D is row-major P x P
+// at D[(r * P + c) * ld].
+template <int P>
+__device__ __forceinline__ void bfgs_update(float *D, int ld, const float *sk, const float *yk) {
+    float divdat = 0;
+#pragma unroll
+    for (int cnt = 0; cnt < P; cnt++) divdat += sk[cnt] * yk[cnt];
+    divdat = 1.0f / divdat;
+    float tdat10[P], tdat20[P];
+#pragma unroll
+    for (int cnt = 0; cnt < P; cnt++) {
+        tdat10[cnt] = yk[cnt] * divdat;
+        tdat20[cnt] = sk[cnt] * divdat;
+    }
+    float skyk[P][P], sksk[P][P], tD0[P][P];
+#pragma unroll
+    for (int row = 0; row < P; row++) {
+#pragma unroll
+        for (int col = 0; col < P; col++) {
+            if (row == col)
+                skyk[row][col] = 1.0f - sk[row] * tdat10[col];
+            else
+                skyk[row][col] = 0.0f - sk[row] * tdat10[col];
+            sksk[row][col] = sk[row] * tdat20[col];
+        }
+    }
+#pragma unroll
+    for (int row = 0; row < P; row++) {
+#pragma unroll
+        for (int col = 0; col < P; col++) {
+            tD0[row][col] = 0;
+#pragma unroll
+            for (int cnt = 0; cnt < P; cnt++) tD0[row][col] += skyk[row][cnt] * D[(cnt * P + col) * ld];
+        }
+    }
+#pragma unroll
+    for (int row = 0; row < P; row++) {
+#pragma unroll
+        for (int col = 0; col < P; col++) {
+            float acc = 0;
+#pragma unroll
+            for (int cnt = 0; cnt < P; cnt++) acc += tD0[row][cnt] * skyk[col][cnt];
+            D[(row * P + col) * ld] = acc;
+        }
+    }
+#pragma unroll
+    for (int row = 0; row < P; row++) {
+#pragma unroll
+        for (int cnt = 0; cnt < P; cnt++) D[(row * P + cnt) * ld] = D[(row * P + cnt) * ld] + sksk[row][cnt];
+    }
+}
+
+// Fixed schedule: IT quasi-Newton iterations, each with an 11-step bisection
+// of the step length in [1e-5, 1]; no convergence test.  D: P x P scratch.
+template <int R, int KIND>
+__device__ __forceinline__ void mle_fit(const RoiRef &roi, float *Ininf, float *D, int ld) {
+    enum { P = KindTraits<KIND>::P, IT = KindTraits<KIND>::IT };
+    float grad[P], d0[P], td0[P], sk[P], yk[P], tgrad[P];
+    float xd[P * 2];
+    float ddat[2], dpos[2];
+#pragma unroll
+    for (int r = 0; r < P; r++) {
+#pragma unroll
+        for (int c = 0; c < P; c++) D[(r * P + c) * ld] = (r == c) ? 1.0f : 0.0f;
+    }
+    numerical_gradient<R, KIND>(roi, Ininf, grad);
+#pragma unroll
+    for (int rcnt = 0; rcnt < P; rcnt++) d0[rcnt] = -grad[rcnt];
+
+    for (int itcnt = 0; itcnt < IT; itcnt++) {
+        float td0_total = 0;
+#pragma unroll
+        for (int rcnt = 0; rcnt < P; rcnt++) {
+            td0[rcnt] = fabsf(d0[rcnt]);
+            td0_total += td0[rcnt];
+        }
+        td0_total = ((float)P) / td0_total;
+#pragma unroll
+        for (int rcnt = 0; rcnt < P; rcnt++) d0[rcnt] = d0[rcnt] * td0_total;
+
+        dpos[0] = 0.00001f;
+        dpos[1] = 1.0f;
+#pragma unroll
+        for (int cnt = 0; cnt < P; cnt++) xd[cnt] = d0[cnt] * 0.0001f + Ininf[cnt];
+#pragma unroll
+        for (int cnt = 0; cnt < P; cnt++) xd[P + cnt] = d0[cnt] * 1.0f + Ininf[cnt];
+        ddat[0] = loss<R, KIND>(roi, &xd[0]);
+        ddat[1] = loss<R, KIND>(roi, &xd[P]);
+
+        for (int cnt = 0; cnt < kBisections; cnt++) {
+            const int xdsel = (ddat[0] < ddat[1]);
+            dpos[xdsel] = (dpos[0] + dpos[1]) * 0.5f;
+            if (cnt < kBisections - 1) {
+                // the selected half is rebuilt in place; written per slot so the
+                // array stays in registers
+                if (xdsel) {
+#pragma unroll
+                    for (int k = 0; k < P; k++) xd[P + k] = d0[k] * dpos[1] + Ininf[k];
+                    ddat[1] = loss<R, KIND>(roi, &xd[P]);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < P; k++) xd[k] = d0[k] * dpos[0] + Ininf[k];
+                    ddat[0] = loss<R, KIND>(roi, &xd[0]);
+                }
+            }
+        }
+        const float scale = (dpos[0] + dpos[1]) * 0.5f;
+#pragma unroll
+        for (int rcnt = 0; rcnt < P; rcnt++) {
+            sk[rcnt] = d0[rcnt] * scale;
+            Ininf[rcnt] = Ininf[rcnt] + sk[rcnt];
+        }
+#pragma unroll
+        for (int cnt = 0; cnt < P; cnt++)
+            if (Ininf[cnt] < 0.01f) Ininf[cnt] = 0.01f;
+
+        if (itcnt < IT - 1) {
+#pragma unroll
+            for (int rcnt = 0; rcnt < P; rcnt++) tgrad[rcnt] = grad[rcnt];
+            numerical_gradient<R, KIND>(roi, Ininf, grad);
+#pragma unroll
+            for (int rcnt = 0; rcnt < P; rcnt++) yk[rcnt] = grad[rcnt] - tgrad[rcnt];
+            bfgs_update<P>(D, ld, sk, yk);
+#pragma unroll
+            for (int row = 0; row < P; row++) {
+                d0[row] = 0;
+#pragma unroll
+                for (int cnt = 0; cnt < P; cnt++) d0[row] -= D[(row * P + cnt) * ld] * grad[cnt];
+            }
+        }
+    }
+}
+
+// Weighted-MLE mask (bfgsMLE_core.h:206-238).
+template <int R>
+__device__ __forceinline__ void wle_weights(float *w, int ld, float WLE_SigmaX, float WLE_SigmaY, int MoleculeType) {
+    const float ROICenter = R / 2.0f;
+    const float WLE_SigmaX1 = 1.0f / (2.0f * WLE_SigmaX * WLE_SigmaX);
+    const float WLE_SigmaY1 = 1.0f / (2.0f * WLE_SigmaY * WLE_SigmaY);
+    for (int row = 0; row < R; row++) {
+        for (int col = 0; col < R; col++) {
+            const float rowpos = row + 0.5f;
+            const float colpos = col + 0.5f;
+            if (MoleculeType == 0)
+                w[(row * R + col) * ld] = 1.0f;
+            else
+                w[(row * R + col) * ld] = __expf(-((colpos - ROICenter) * (colpos - ROICenter) * WLE_SigmaX1 +
+                                                   (rowpos - ROICenter) * (rowpos - ROICenter) * WLE_SigmaY1));
+        }
+    }
+}
+
+}  // namespace qcs

@@ -1,0 +1,38 @@
+// Host-side entry points of the qcstorm_b200 kernels (all asynchronous on a
+// caller-given stream; device pointers only).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "qcs_device.cuh"
+
+namespace qcs {
+
+struct FitLaunch {
+    const uint16_t *rois;  // records, R*(R+1) uint16 each
+    const float *wle;      // 6 floats per record
+    Queue q;               // which records this launch fits
+    int max_count;         // upper bound of the queue length (grid size)
+    float *loc;            // 12-float rows, indexed by record id
+    uint8_t *to2e;         // single-emitter kinds: per-record "send to 2E" flag (may be null)
+    MultiOut mo;           // multi-emitter kinds: per-slot result + second-emitter row
+    CorePara para;
+    cudaStream_t stream;
+};
+
+// kind: FitKind (qcs_fit_math.cuh); R: ROI size.
+cudaError_t launch_fit(int kind, int R, const FitLaunch &a);
+
+// CRLB columns 9/10 of rows [0, *n_dev) (or [0, n) when n_dev is null);
+// grid sized for max_rows.  LocPrecCalc_GaussianCRLB.h:65-243.
+cudaError_t launch_crlb(float *loc, const int *n_dev, int n, int max_rows, int loc_type, float ReadNoise_e, float QE,
+                        float PixelSize, cudaStream_t s);
+
+// WLE pre-pass over n records: PSF width, same-frame nearest neighbour and
+// molecule type into wle (6 floats per record).  scratch must hold
+// wle_scratch_bytes(n) bytes.
+size_t wle_scratch_bytes(int n);
+cudaError_t launch_wle(const uint16_t *rois, int n, int R, int loc_type, float *wle, void *scratch, cudaStream_t s);
+
+}  // namespace qcs

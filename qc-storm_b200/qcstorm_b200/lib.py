@@ -1,0 +1,141 @@
+"""ctypes binding of lib/libqcstorm_b200.so (include/qcstorm_b200.h).
+
+Thin: every call goes to the C ABI.  There is no CPU fallback; if the
+library or a CUDA device is missing the calls raise.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from .abi import LIB_PATH, LocPara
+
+_lib = None
+
+# name -> (restype, argtypes) of every exported function of the header
+_SIGS = {
+    "qcs_loc_para_default": (None, [C.POINTER(LocPara)]),
+    "qcs_last_error": (C.c_char_p, []),
+    "qcs_device_available": (C.c_int, []),
+    "qcs_loc_init": (C.c_int, [C.POINTER(LocPara), C.POINTER(C.c_void_p)]),
+    "qcs_loc_init_capacity": (C.c_int, [C.POINTER(LocPara), C.c_int, C.POINTER(C.c_void_p)]),
+    "qcs_loc_deinit": (C.c_int, [C.c_void_p]),
+    "qcs_loc_capacity": (C.c_int, [C.c_void_p]),
+    "qcs_loc_bfgs_mle_localization": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(LocPara), C.c_int,
+                                                C.c_void_p]),
+    "qcs_loc_h_loc_arry": (C.c_void_p, [C.c_void_p]),
+    "qcs_loc_valid_num": (C.c_int, [C.c_void_p]),
+    "qcs_loc_fit_ratios": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "qcs_loc_localize_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(LocPara), C.c_int,
+                                          C.c_void_p]),
+    "qcs_loc_device_rows": (C.c_void_p, [C.c_void_p]),
+    "qcs_loc_device_valid_num": (C.c_void_p, [C.c_void_p]),
+    "qcs_loc_device_roi_buffer": (C.c_void_p, [C.c_void_p]),
+    "qcs_loc_device_wle_buffer": (C.c_void_p, [C.c_void_p]),
+    "qcs_wle_estimate": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(LocPara), C.c_void_p]),
+    "qcs_wle_estimate_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(LocPara), C.c_void_p,
+                                          C.c_void_p]),
+    "qcs_fit_single_device": (C.c_int, [C.c_int, C.POINTER(LocPara), C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                        C.c_void_p]),
+    "qcs_crlb_device": (C.c_int, [C.POINTER(LocPara), C.c_void_p, C.c_int, C.c_void_p]),
+}
+
+
+class QcsError(RuntimeError):
+    def __init__(self, code, what):
+        super().__init__("qcstorm_b200 error %d: %s" % (code, what))
+        self.code = code
+
+
+def load(path=LIB_PATH):
+    """Load the library (once) and attach signatures."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(path):
+            raise OSError("qcstorm_b200 library not built: %s (run qc-storm_b200/build.py)" % path)
+        lib = C.CDLL(path)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def check(code):
+    if code != 0:
+        raise QcsError(code, load().qcs_last_error().decode())
+
+
+def _host(a, dtype):
+    a = np.ascontiguousarray(a, dtype=dtype)
+    return a, C.c_void_p(a.ctypes.data)
+
+
+class LocContext:
+    """LDLocData_TypeDef: buffers for records of one ROI size."""
+
+    def __init__(self, para, capacity=0):
+        self.lib = load()
+        self.para = para
+        h = C.c_void_p()
+        check(self.lib.qcs_loc_init_capacity(C.byref(para), int(capacity), C.byref(h)))
+        self.h = h
+        self.capacity = self.lib.qcs_loc_capacity(h)
+
+    def close(self):
+        if self.h:
+            self.lib.qcs_loc_deinit(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def localize(self, rois, wle=None, para=None):
+        """BFGS_MLELocalization on host arrays; returns (rows[n_valid, 12], ratios[7])."""
+        para = para or self.para
+        rois, pr = _host(rois, np.uint16)
+        n = rois.shape[0]
+        pw = None
+        if wle is not None:
+            wle, pw = _host(wle, np.float32)
+        check(self.lib.qcs_loc_bfgs_mle_localization(self.h, pr, pw, C.byref(para), n, None))
+        nv = self.lib.qcs_loc_valid_num(self.h)
+        ptr = self.lib.qcs_loc_h_loc_arry(self.h)
+        rows = np.ctypeslib.as_array((C.c_float * (12 * nv)).from_address(ptr)).reshape(nv, 12).copy() if nv else \
+            np.zeros((0, 12), np.float32)
+        ratios = np.zeros(7, np.float32)
+        check(self.lib.qcs_loc_fit_ratios(self.h, C.c_void_p(ratios.ctypes.data)))
+        return rows, ratios
+
+    def wle(self, rois, para=None):
+        """WLEParameterEstimate on host records; returns wle[n, 6]."""
+        para = para or self.para
+        rois, pr = _host(rois, np.uint16)
+        out = np.zeros((rois.shape[0], 6), np.float32)
+        check(self.lib.qcs_wle_estimate(self.h, pr, rois.shape[0], C.byref(para), C.c_void_p(out.ctypes.data)))
+        return out
+
+    # device-pointer forms (integers from torch.Tensor.data_ptr(), stream handles)
+    def localize_device(self, d_rois, n, d_wle=0, stream=0, para=None):
+        para = para or self.para
+        check(self.lib.qcs_loc_localize_device(self.h, C.c_void_p(d_rois), C.c_void_p(d_wle) if d_wle else None,
+                                               C.byref(para), int(n), C.c_void_p(stream) if stream else None))
+
+    def device_rows(self):
+        return self.lib.qcs_loc_device_rows(self.h)
+
+    def device_valid_num(self):
+        return self.lib.qcs_loc_device_valid_num(self.h)
+
+
+def fit_single_device(loc_type, para, d_rois, d_wle, n, d_loc, stream=0):
+    check(load().qcs_fit_single_device(int(loc_type), C.byref(para), C.c_void_p(d_rois), C.c_void_p(d_wle), int(n),
+                                       C.c_void_p(d_loc), C.c_void_p(stream) if stream else None))
+
+
+def crlb_device(para, d_loc, n, stream=0):
+    check(load().qcs_crlb_device(C.byref(para), C.c_void_p(d_loc), int(n), C.c_void_p(stream) if stream else None))

@@ -80,3 +80,45 @@ def crlb(para, loc, lib="oracle"):
 
 def set_threads(n):
     oracle().qcso_set_threads(int(n))
+
+
+REF_GPU_SO = os.path.join(ROOT, "oracle", "_ref", "libqcs_ref_gpu.so")
+
+
+def ref_gpu():
+    """The reference CUDA library built for sm_100a (checker on GPU hosts)."""
+    return _load(REF_GPU_SO)
+
+
+def ref_gpu_fit_kernel(kind, para, rec, wl):
+    n = rec.shape[0]
+    out = np.zeros((n, 12), np.float32)
+    ms = C.c_float(0)
+    st = ref_gpu().qcsrefg_fit_kernel(kind, C.byref(para), _p(rec), _p(wl), n, _p(out), C.byref(ms))
+    assert st == 0, st
+    return out, ms.value
+
+
+def ref_gpu_localize(para, rec, wl):
+    n = rec.shape[0]
+    cap = max(2 * n, 1)
+    out = np.zeros((cap, 12), np.float32)
+    nv = C.c_int(0)
+    ratios = np.zeros(7, np.float32)
+    st = ref_gpu().qcsrefg_localize(C.byref(para), _p(rec), _p(wl), n, _p(out), cap, C.byref(nv), _p(ratios))
+    assert st == 0, st
+    return out[:nv.value].copy(), ratios
+
+
+def ref_gpu_wle(para, rec):
+    out = np.zeros((rec.shape[0], 6), np.float32)
+    st = ref_gpu().qcsrefg_wle(C.byref(para), _p(rec), rec.shape[0], _p(out))
+    assert st == 0, st
+    return out
+
+
+def ref_gpu_crlb(para, loc):
+    out = np.ascontiguousarray(loc, np.float32).copy()
+    st = ref_gpu().qcsrefg_crlb(C.byref(para), _p(out), out.shape[0])
+    assert st == 0, st
+    return out
