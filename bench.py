@@ -1,0 +1,330 @@
+#!/usr/bin/env python3
+"""Throughput of the MLEbfgs localization path (GS2D 7x7 single-emitter fits/s).
+
+One step = one localization call over N = 100,000 synthetic 7x7 ROI records
+(the reference's per-call batch size, MaxPointNum = 102,400): WLE pre-pass
+(PSF width, nearest neighbour, molecule type) -> single-emitter fit with the
+reference's fixed schedule -> CRLB, all on the device through the C ABI
+(qcs_loc_localize_device).  Records: seeded synthetic config-0 ROIs (sigma
+U(1.0,1.6) px, photons log-U[500,5000], background U(20,100) e-/px, Poisson),
+16 distinct batches rotated across steps (179 MB of records, more than the
+126 MB L2).
+
+Printed JSON line (rank 0): `value` is device-timed fits/s with records
+resident in HBM; `e2e` is the same metric through the host-buffer call
+qcs_loc_bfgs_mle_localization (pinned host records in, rows out, copies
+inside the timed region); `roofline` is the fit kernel against the measured
+special-function-unit rate (the loss is exp/log bound, not HBM or tensor
+bound); `cpu_baseline` is the reference's own code compiled for the host
+(oracle/_ref) on all host cores.
+
+--impl reference times the reference's CPU implementation of the same step
+(oracle/_ref/libqcs_ref_host.so: the reference sources compiled for the CPU,
+WLE + localization + CRLB) on all host cores, rank 0 only.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "qc-storm_b200"))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "7x7 fits/s on 1 B200: learned-init vs plain MLEbfgs at equal RMSE/CRLB"
+UNIT = "fits/s"
+N_PER_STEP = 100_000
+BATCHES = 16
+R = 7
+PX_EVALS_PER_FIT = 176 * R * R  # reference schedule: 176 loss evaluations of R*R pixels
+MUFU_PER_PX_EVAL = 2            # exp of the model, log of the model (log of the data is invariant)
+
+
+def env_int(k, d):
+    try:
+        return int(os.environ.get(k, d))
+    except ValueError:
+        return d
+
+
+def start_clock_sampler(gpu_index):
+    f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+    q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+    try:
+        p = subprocess.Popen(["nvidia-smi", "--query-gpu=" + q, "--format=csv,noheader,nounits", "-i", str(gpu_index),
+                              "-lms", "200"], stdout=f, stderr=subprocess.DEVNULL)
+    except OSError:
+        p = None
+    return p, f.name
+
+
+def stop_clock_sampler(p, path):
+    out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+    if p is None:
+        return out
+    p.terminate()
+    try:
+        p.wait(timeout=5)
+    except subprocess.TimeoutExpired:
+        p.kill()
+    sm, mx, reasons = [], [], set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    with open(path) as fh:
+        for line in fh:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+    os.unlink(path)
+    if sm:
+        out = {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+               "samples": len(sm)}
+    return out
+
+
+def cpu_reference_rate(steps=1, per_thread=6000, threads=None):
+    """fits/s of the reference's own code compiled for the host (oracle/_ref),
+    WLE + localization + CRLB, one chunk of records per host thread; falls back
+    to the CPU oracle restatement when the reference build is absent."""
+    import oracle_lib as O
+    from qcstorm_b200 import synth
+    threads = threads or os.cpu_count() or 1
+    ref = O.ref_host()
+    kind = "reference" if ref is not None else "port"
+    lib = "ref" if ref is not None else "oracle"
+    if lib == "oracle":
+        O.set_threads(1)
+    chunks = []
+    for t in range(threads):
+        rec, para, _ = synth.gs2d_rois(per_thread, R=R, seed=9000 + t)
+        chunks.append((rec, para))
+    rates = []
+    for _ in range(steps):
+        done = [0] * threads
+
+        def work(i):
+            rec, para = chunks[i]
+            w = O.wle(para, rec, lib)
+            O.localize(para, rec, w, lib)
+            done[i] = rec.shape[0]
+
+        t0 = time.perf_counter()
+        ths = [threading.Thread(target=work, args=(i,)) for i in range(threads)]
+        for th in ths:
+            th.start()
+        for th in ths:
+            th.join()
+        dt = time.perf_counter() - t0
+        rates.append(sum(done) / dt)
+    return {"value": max(rates) if steps == 1 else statistics.median(rates), "unit": UNIT, "cores": threads,
+            "kind": kind,
+            "sample": "%d GS2D 7x7 records per host thread x %d threads per step (WLE + fit + CRLB)" % (
+                per_thread, threads)}, rates
+
+
+def run_reference_arm(args, rank):
+    if rank != 0:
+        return 0
+    base, rates = cpu_reference_rate(steps=args.warmup + args.steps)
+    rates = rates[args.warmup:]
+    v = statistics.median(rates)
+    base["value"] = v
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * N_PER_STEP / v,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": config_dict(args),
+        "cpu_baseline": base,
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def config_dict(args):
+    return {
+        "workload": "GS2D 7x7 single-emitter MLEbfgs, %d ROI records per call: WLE pre-pass + fit + CRLB "
+                    "(config-0 generator)" % N_PER_STEP,
+        "roi_size": R, "rois_per_step": N_PER_STEP, "mode": "plain MLEbfgs, reference schedule, bit-exact with "
+                                                          "the reference CUDA kernel",
+        "input_batches": BATCHES, "l2": "records rotate over %d batches (%.0f MB > 126 MB L2)" % (
+            BATCHES, BATCHES * N_PER_STEP * R * (R + 1) * 2 / 1e6),
+        "parallelism": "dp%d (independent frame batches per GPU)" % args.gpus,
+    }
+
+
+def profile_fit(n):
+    """Three launches of the single-emitter fit kernel over n records."""
+    import torch
+    from qcstorm_b200 import lib, synth
+    rec, para, _ = synth.gs2d_rois(n, R=R, seed=5)
+    d = torch.from_numpy(rec.view(np.int16)).cuda()
+    ctx = lib.LocContext(para, capacity=n)
+    w = torch.empty((n, 6), dtype=torch.float32, device="cuda")
+    sh = torch.cuda.current_stream().cuda_stream
+    lib.check(lib.load().qcs_wle_estimate_device(ctx.h, C.c_void_p(d.data_ptr()), n, C.byref(para),
+                                                 C.c_void_p(w.data_ptr()), C.c_void_p(sh)))
+    out = torch.empty((n, 12), dtype=torch.float32, device="cuda")
+    for _ in range(3):
+        lib.fit_single_device(0, para, d.data_ptr(), w.data_ptr(), n, out.data_ptr(), sh)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_fit": n, "accepted": float((out[:, 0] > 0).float().mean())}))
+    ctx.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-fit", type=int, default=0, metavar="N",
+                    help="only run the single-emitter fit kernel 3 times on N records (for ncu captures)")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = env_int("WORLD_SIZE", 1)
+    rank = env_int("RANK", 0)
+    local = env_int("LOCAL_RANK", 0)
+    if args.impl == "reference":
+        return run_reference_arm(args, rank)
+
+    import torch
+    from qcstorm_b200 import lib, synth
+
+    torch.cuda.set_device(local)
+    if args.profile_fit:
+        return profile_fit(args.profile_fit)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    # ---- inputs: BATCHES distinct batches resident in HBM, pinned host copies
+    d_batches, h_batches = [], []
+    para = None
+    for b in range(BATCHES):
+        rec, para, _ = synth.gs2d_rois(N_PER_STEP, R=R, seed=1000 * rank + b)
+        h = torch.from_numpy(rec.view(np.int16)).pin_memory()
+        h_batches.append(h)
+        d_batches.append(h.cuda())
+    ctx = lib.LocContext(para, capacity=N_PER_STEP)
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+
+    def step(k):
+        ctx.localize_device(d_batches[k % BATCHES].data_ptr(), N_PER_STEP, 0, sh)
+
+    launches_per_step = 8  # psf_width, nn_keys, nn_scan, classify, init_counters, fit, finish, crlb
+
+    # ---- device-timed steps
+    for k in range(args.warmup):
+        step(k)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler, spath = start_clock_sampler(local)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(args.steps):
+        step(k)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = stop_clock_sampler(sampler, spath)
+    if dist:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = args.steps * N_PER_STEP * world / (ms * 1e-3)
+
+    # ---- dominant kernel alone: the single-emitter fit (for the roofline)
+    wle_b = [torch.empty((N_PER_STEP, 6), dtype=torch.float32, device="cuda") for _ in range(BATCHES)]
+    for b in range(BATCHES):
+        lib.load().qcs_wle_estimate_device(ctx.h, C.c_void_p(d_batches[b].data_ptr()), N_PER_STEP, C.byref(para),
+                                           C.c_void_p(wle_b[b].data_ptr()), C.c_void_p(sh))
+    d_loc = torch.empty((N_PER_STEP, 12), dtype=torch.float32, device="cuda")
+    for k in range(3):
+        lib.fit_single_device(0, para, d_batches[k].data_ptr(), wle_b[k].data_ptr(), N_PER_STEP, d_loc.data_ptr(), sh)
+    torch.cuda.synchronize()
+    kt = []
+    for k in range(args.steps):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        lib.fit_single_device(0, para, d_batches[k % BATCHES].data_ptr(), wle_b[k % BATCHES].data_ptr(), N_PER_STEP,
+                              d_loc.data_ptr(), sh)
+        b.record(stream)
+        kt.append((a, b))
+    torch.cuda.synchronize()
+    fit_ms = statistics.mean(a.elapsed_time(b) for a, b in kt)
+    mufu_peak = lib.mufu_rate()
+    achieved = N_PER_STEP * PX_EVALS_PER_FIT * MUFU_PER_PX_EVAL / (fit_ms * 1e-3)
+
+    # ---- end to end through the host-buffer call (pinned records in, rows out)
+    e2e_steps = max(3, min(args.steps, 10))
+    for k in range(2):
+        ctx.localize(h_batches[k].numpy().view(np.uint16), None, stream=sh)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    rows = 0
+    for k in range(e2e_steps):
+        out, _ = ctx.localize(h_batches[k % BATCHES].numpy().view(np.uint16), None, stream=sh)
+        rows += out.shape[0]
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    e2e = {"value": e2e_steps * N_PER_STEP * world / e2e_s, "unit": UNIT,
+           "h2d_bytes_per_step": N_PER_STEP * R * (R + 1) * 2,
+           "d2h_bytes_per_step": int(rows / e2e_steps) * 48 + 32,
+           "call": "qcs_loc_bfgs_mle_localization (pinned host records, WLE on device, synchronous)"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cpu, _ = cpu_reference_rate(steps=1)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config_dict(args),
+            "e2e": e2e, "gpu_launches": launches_per_step * args.steps,
+            "roofline": {"bound": "sfu", "kernel": "fit_single_kernel<7,GS2D>", "achieved": achieved,
+                         "peak": mufu_peak, "unit": "MUFU op/s", "frac": achieved / mufu_peak, "traffic": None,
+                         "kernel_ms": fit_ms,
+                         "algorithmic": "%d px-evals x %d MUFU per fit; peak = measured __expf/__logf rate" % (
+                             PX_EVALS_PER_FIT, MUFU_PER_PX_EVAL)},
+            "cpu_baseline": cpu, "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -216,6 +216,12 @@ int qcs_fit_single_device(int loc_type, const qcs_loc_para *p, const uint16_t *d
  * LocPrecCalc_GaussianCRLB.cu:23-40): CRLB columns of n device rows. */
 int qcs_crlb_device(const qcs_loc_para *p, float *d_loc, int n, void *stream);
 
+/* ---- diagnostics --------------------------------------------------------- */
+/* Sustained special-function-unit rate of the loss's __expf/__logf pair on
+ * the current device: *ops MUFU operations in *ms milliseconds.  Used as the
+ * measured peak of the fit kernel's roofline; no counterpart in the reference. */
+int qcs_measure_mufu_rate(int iters, float *ms, double *ops);
+
 #ifdef __cplusplus
 }
 #endif

@@ -21,6 +21,10 @@
 #include "WLEParaEstimation.h"
 #include "bfgsMLE_GS2D_core.h"
 #include "bfgsMLE_AS3D_core.h"
+#include "bfgsMLE_GS2D_2Emitter_core.h"
+#include "bfgsMLE_GS2D_3Emitter_core.h"
+#include "bfgsMLE_AS3D_2Emitter_core.h"
+#include "LocPrecCalc_GaussianCRLB.h"
 
 #include "../include/qcstorm_b200.h"
 
@@ -148,6 +152,136 @@ int qcsrefg_fit_kernel(int kind, const qcs_loc_para *p, const unsigned short *ro
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaFree(d_roi); cudaFree(d_wle); cudaFree(d_loc); cudaFree(d_c); cudaFree(d_f); cudaFree(d_int);
+    return st;
+}
+
+// One multi-emitter fit kernel over all n records (queue 0..n-1): kind 2 =
+// GS2D 2E, 3 = GS2D 3E, 4 = AS3D 2E.  out: out_cap rows; first emitters (or
+// zero rows) at the record index, second emitters appended from row n in the
+// order of the reference's atomic counter; *n_rows = n + appended.
+int qcsrefg_fit_multi_kernel(int kind, const qcs_loc_para *p, const unsigned short *rois, const float *wle, int n,
+                             float *out, int out_cap, int *n_rows) {
+    LocalizationPara r;
+    to_ref(p, r);
+    if (n <= 0 || n > MaxPointNum / 2 || out_cap < 2 * n) return -1;
+    CoreFittingPara c;
+    c.MultiEmitterFitEn = 1; c.WLEEn = r.WLEEn; c.Offset = r.Offset; c.KAdc = r.KAdc; c.QE = r.QE;
+    c.ReadNoise_e = r.ReadNoise_e; c.ZDepthCorrFactor = r.ZDepthCorrFactor;
+    c.p4_XGY = r.p4_XGY; c.p3_XGY = r.p3_XGY; c.p2_XGY = r.p2_XGY; c.p1_XGY = r.p1_XGY; c.p0_XGY = r.p0_XGY;
+    c.p4_XLY = r.p4_XLY; c.p3_XLY = r.p3_XLY; c.p2_XLY = r.p2_XLY; c.p1_XLY = r.p1_XLY; c.p0_XLY = r.p0_XLY;
+    const int whole = r.ROISize * (r.ROISize + 1);
+    unsigned short *d_roi; float *d_wle, *d_loc; CoreFittingPara *d_c; FitPosInf_TypeDef *d_f; int *d_int;
+    cudaMalloc((void **)&d_roi, sizeof(unsigned short) * whole * (size_t)n);
+    cudaMalloc((void **)&d_wle, sizeof(float) * WLE_ParaNumber * (size_t)n);
+    cudaMalloc((void **)&d_loc, sizeof(float) * OutParaNumGS2D * (size_t)MaxPointNum);
+    cudaMalloc((void **)&d_c, sizeof(CoreFittingPara));
+    cudaMalloc((void **)&d_f, sizeof(FitPosInf_TypeDef));
+    cudaMalloc((void **)&d_int, sizeof(int) * (8 + 3 * (size_t)MaxPointNum));
+    cudaMemcpy(d_roi, rois, sizeof(unsigned short) * whole * (size_t)n, cudaMemcpyHostToDevice);
+    cudaMemcpy(d_wle, wle, sizeof(float) * WLE_ParaNumber * (size_t)n, cudaMemcpyHostToDevice);
+    cudaMemset(d_loc, 0, sizeof(float) * OutParaNumGS2D * (size_t)MaxPointNum);
+    cudaMemset(d_int, 0, sizeof(int) * (8 + 3 * (size_t)MaxPointNum));
+    cudaMemcpy(d_c, &c, sizeof(c), cudaMemcpyHostToDevice);
+    std::vector<int> ident(n);
+    for (int i = 0; i < n; ++i) ident[i] = i;
+    FitPosInf_TypeDef f;
+    memset(&f, 0, sizeof(f));
+    f.d_SingleFitFluoNum = d_int + 0;
+    f.d_MultiFitFluoNum_2E = d_int + 1;
+    f.d_MultiFitFluoNum_3E = d_int + 2;
+    f.d_RejectedFluoNum = d_int + 3;
+    f.d_MultiFit_AddedFluoNum = d_int + 4;
+    f.d_SingleFitFluoPos = d_int + 8;
+    f.d_MultiFitFluoPos_2E = d_int + 8 + MaxPointNum;
+    f.d_MultiFitFluoPos_3E = d_int + 8 + 2 * (size_t)MaxPointNum;
+    cudaMemcpy(kind == 3 ? f.d_MultiFitFluoPos_3E : f.d_MultiFitFluoPos_2E, ident.data(), sizeof(int) * n,
+               cudaMemcpyHostToDevice);
+    cudaMemcpy(f.d_MultiFit_AddedFluoNum, &n, sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemcpy(d_f, &f, sizeof(f), cudaMemcpyHostToDevice);
+    const int blocks = (n + ThreadsPerBlock - 1) / ThreadsPerBlock;
+    int st = 2;
+#define QCSREFG_MCASE(KIND, R, KERNEL)                                          \
+    if (kind == KIND && r.ROISize == R) {                                       \
+        KERNEL<<<blocks, ThreadsPerBlock>>>(d_loc, d_roi, d_wle, n, d_f, d_c);  \
+        st = check();                                                           \
+    }
+    QCSREFG_MCASE(2, 5, (bfgsMLELoc_Gauss2D_2E<5, FitParaNum_2D_2E>))
+    QCSREFG_MCASE(2, 7, (bfgsMLELoc_Gauss2D_2E<7, FitParaNum_2D_2E>))
+    QCSREFG_MCASE(2, 9, (bfgsMLELoc_Gauss2D_2E<9, FitParaNum_2D_2E>))
+    QCSREFG_MCASE(2, 11, (bfgsMLELoc_Gauss2D_2E<11, FitParaNum_2D_2E>))
+    QCSREFG_MCASE(2, 13, (bfgsMLELoc_Gauss2D_2E<13, FitParaNum_2D_2E>))
+    QCSREFG_MCASE(3, 5, (bfgsMLELoc_Gauss2D_3E<5, FitParaNum_2D_3E>))
+    QCSREFG_MCASE(3, 7, (bfgsMLELoc_Gauss2D_3E<7, FitParaNum_2D_3E>))
+    QCSREFG_MCASE(3, 9, (bfgsMLELoc_Gauss2D_3E<9, FitParaNum_2D_3E>))
+    QCSREFG_MCASE(3, 11, (bfgsMLELoc_Gauss2D_3E<11, FitParaNum_2D_3E>))
+    QCSREFG_MCASE(3, 13, (bfgsMLELoc_Gauss2D_3E<13, FitParaNum_2D_3E>))
+    QCSREFG_MCASE(4, 5, (bfgsMLELoc_AS3D_2E<5, FitParaNum_AS3D_2E>))
+    QCSREFG_MCASE(4, 7, (bfgsMLELoc_AS3D_2E<7, FitParaNum_AS3D_2E>))
+    QCSREFG_MCASE(4, 9, (bfgsMLELoc_AS3D_2E<9, FitParaNum_AS3D_2E>))
+    QCSREFG_MCASE(4, 11, (bfgsMLELoc_AS3D_2E<11, FitParaNum_AS3D_2E>))
+    QCSREFG_MCASE(4, 13, (bfgsMLELoc_AS3D_2E<13, FitParaNum_AS3D_2E>))
+#undef QCSREFG_MCASE
+    if (st == 0) {
+        int added = 0;
+        cudaMemcpy(&added, f.d_MultiFit_AddedFluoNum, sizeof(int), cudaMemcpyDeviceToHost);
+        if (added > out_cap) added = out_cap;
+        *n_rows = added;
+        cudaMemcpy(out, d_loc, sizeof(float) * OutParaNumGS2D * (size_t)added, cudaMemcpyDeviceToHost);
+    }
+    cudaFree(d_roi); cudaFree(d_wle); cudaFree(d_loc); cudaFree(d_c); cudaFree(d_f); cudaFree(d_int);
+    return st;
+}
+
+// Element-level probes of two reference device functions, one thread each:
+// the weighted-MLE mask WLEWeightsCalc<R> (bfgsMLE_core.h:206-238) and the
+// CRLB model image GaussianPSF_generate2D<G> (LocPrecCalc_GaussianCRLB.h:130-166).
+}  // extern "C"
+
+template <int R>
+__global__ void probe_weights_kernel(float *out, float sx, float sy, int type) {
+    float w[R * R];
+    WLEWeightsCalc<R>(w, sx, sy, type);
+    for (int k = 0; k < R * R; k++) out[k] = w[k];
+}
+
+template <int G>
+__global__ void probe_psf_kernel(float *out, const float *para) {
+    float p[GaussianCRLB_ParaNum], img[G * G];
+    for (int k = 0; k < GaussianCRLB_ParaNum; k++) p[k] = para[k];
+    GaussianPSF_generate2D<G>(img, p);
+    for (int k = 0; k < G * G; k++) out[k] = img[k];
+}
+
+extern "C" {
+
+int qcsrefg_probe_weights(int R, float sx, float sy, int type, float *out) {
+    float *d;
+    cudaMalloc((void **)&d, sizeof(float) * 17 * 17);
+    switch (R) {
+    case 5: probe_weights_kernel<5><<<1, 1>>>(d, sx, sy, type); break;
+    case 7: probe_weights_kernel<7><<<1, 1>>>(d, sx, sy, type); break;
+    case 9: probe_weights_kernel<9><<<1, 1>>>(d, sx, sy, type); break;
+    case 11: probe_weights_kernel<11><<<1, 1>>>(d, sx, sy, type); break;
+    case 13: probe_weights_kernel<13><<<1, 1>>>(d, sx, sy, type); break;
+    default: cudaFree(d); return -1;
+    }
+    int st = check();
+    cudaMemcpy(out, d, sizeof(float) * R * R, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    return st;
+}
+
+int qcsrefg_probe_psf(int G, const float *para6, float *out) {
+    float *d, *dp;
+    cudaMalloc((void **)&d, sizeof(float) * 15 * 15);
+    cudaMalloc((void **)&dp, sizeof(float) * 6);
+    cudaMemcpy(dp, para6, sizeof(float) * 6, cudaMemcpyHostToDevice);
+    if (G == 9) probe_psf_kernel<9><<<1, 1>>>(d, dp);
+    else probe_psf_kernel<15><<<1, 1>>>(d, dp);
+    int st = check();
+    cudaMemcpy(out, d, sizeof(float) * G * G, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    cudaFree(dp);
     return st;
 }
 

@@ -8,6 +8,7 @@
 // reference kernel lacks (:65-128) and reads the row count from the device.
 #include <cuda_runtime.h>
 
+#include "qcs_fit_math.cuh"
 #include "qcs_kernels.h"
 
 namespace qcs {
@@ -15,7 +16,24 @@ namespace {
 
 enum { kParaTPhn = 0, kParaBkgn = 1, kParaXPos = 2, kParaYPos = 3, kParaSigX = 4, kParaSigY = 5 };
 
+// Contraction of the PSF exponent x^2/(2 sx^2) + y^2/(2 sy^2) per grid size
+// (see SumMode in qcs_fit_math.cuh).
+// PEAK: peak * exp(.) + background; D2: f(+h) - 2 f(0) + f(-h);
+// FI: FI + (d2 - model * d2log).  0 = fused multiply-add, 1 = separately
+// rounded multiply and add, kCompiler = left to the compiler.
 template <int G>
+struct CrlbSpec {
+    enum { MODE = kCompiler, PEAK = kCompiler, D2 = kCompiler, FI = kCompiler };
+};
+
+template <int S>
+__device__ __forceinline__ float mul_add(float a, float b, float c) {
+    if (S == 0) return __fmaf_rn(a, b, c);
+    if (S == 1) return __fadd_rn(__fmul_rn(a, b), c);
+    return a * b + c;
+}
+
+template <int G, int MODE = CrlbSpec<G>::MODE, int PEAK = CrlbSpec<G>::PEAK>
 __device__ __forceinline__ void psf_generate(float *pPSFDat, const float *ParaArry) {
     enum { Half = G / 2 };
     const float TotalPhoton_e = ParaArry[kParaTPhn];
@@ -34,8 +52,10 @@ __device__ __forceinline__ void psf_generate(float *pPSFDat, const float *ParaAr
         for (int xcnt = 0; xcnt < G; xcnt++) {
             CurX = xcnt - Half;
             pPSFDat[ycnt * G + xcnt] =
-                PeakPn * __expf(-((CurX - x0) * (CurX - x0) * PSFSigma_ix + (CurY - y0) * (CurY - y0) * PSFSigma_iy)) +
-                Background_e;
+                mul_add<PEAK>(PeakPn,
+                              __expf(-sum_of_products<MODE>((CurX - x0) * (CurX - x0), PSFSigma_ix,
+                                                            (CurY - y0) * (CurY - y0), PSFSigma_iy)),
+                              Background_e);
         }
     }
 }
@@ -46,39 +66,50 @@ __device__ __forceinline__ void log_calc(const float *d, float *l) {
     for (int cnt = 0; cnt < N; cnt++) l[cnt] = logf(d[cnt]);
 }
 
-template <int N>
+template <int N, int D2>
 __device__ __forceinline__ void deriv2(float *Deriv2, const float *dat_0, const float *dat_p, const float *dat_n,
                                        float dh) {
 #pragma unroll
-    for (int cnt = 0; cnt < N; cnt++) Deriv2[cnt] = (dat_p[cnt] - 2 * dat_0[cnt] + dat_n[cnt]) / dh / dh;
+    for (int cnt = 0; cnt < N; cnt++) {
+        if (D2 == kCompiler)
+            Deriv2[cnt] = (dat_p[cnt] - 2 * dat_0[cnt] + dat_n[cnt]) / dh / dh;
+        else
+            Deriv2[cnt] = __fadd_rn(mul_add<D2>(-2.0f, dat_0[cnt], dat_p[cnt]), dat_n[cnt]) / dh / dh;
+    }
 }
 
-template <int G, int N>
+template <int G, int N, int MODE, int PEAK, int D2>
 __device__ __forceinline__ void derivative2(float *d2, float *d2log, float *ParaArry, int ParaID) {
     float t0[N], tl0[N], tp[N], tlp[N], tn[N], tln[N];
     const float dh = 0.02f;
-    psf_generate<G>(t0, ParaArry);
+    psf_generate<G, MODE, PEAK>(t0, ParaArry);
     log_calc<N>(t0, tl0);
     ParaArry[ParaID] += dh;
-    psf_generate<G>(tp, ParaArry);
+    psf_generate<G, MODE, PEAK>(tp, ParaArry);
     log_calc<N>(tp, tlp);
     ParaArry[ParaID] -= 2 * dh;
-    psf_generate<G>(tn, ParaArry);
+    psf_generate<G, MODE, PEAK>(tn, ParaArry);
     log_calc<N>(tn, tln);
     ParaArry[ParaID] += dh;
-    deriv2<N>(d2, t0, tp, tn, dh);
-    deriv2<N>(d2log, tl0, tlp, tln, dh);
+    deriv2<N, D2>(d2, t0, tp, tn, dh);
+    deriv2<N, D2>(d2log, tl0, tlp, tln, dh);
 }
 
-template <int N>
+template <int N, int FI>
 __device__ __forceinline__ float crlb_std(const float *model, const float *d2, const float *d2log) {
     float FishirInf = 0;
-    for (int cnt = 0; cnt < N; cnt++) FishirInf += (d2[cnt] - model[cnt] * d2log[cnt]);
+    for (int cnt = 0; cnt < N; cnt++) {
+        if (FI == kCompiler)
+            FishirInf += (d2[cnt] - model[cnt] * d2log[cnt]);
+        else
+            FishirInf = __fadd_rn(FishirInf, mul_add<FI>(-model[cnt], d2log[cnt], d2[cnt]));
+    }
     if (FishirInf == 0.0f) FishirInf = 1;
     return sqrtf(1 / FishirInf);
 }
 
-template <int G>
+template <int G, int MODE = CrlbSpec<G>::MODE, int PEAK = CrlbSpec<G>::PEAK, int D2 = CrlbSpec<G>::D2,
+          int FI = CrlbSpec<G>::FI>
 __global__ void crlb_kernel(float *__restrict__ loc, const int *__restrict__ n_dev, int n, float ReadNoise_e, float QE,
                             float PixelSize) {
     enum { N = G * G };
@@ -103,11 +134,11 @@ __global__ void crlb_kernel(float *__restrict__ loc, const int *__restrict__ n_d
         ParaArry[kParaYPos] = 0;
         ParaArry[kParaSigX] = PSFSigmaX;
         ParaArry[kParaSigY] = PSFSigmaY;
-        psf_generate<G>(model, ParaArry);
-        derivative2<G, N>(d2, d2log, ParaArry, kParaXPos);
-        ParaStdX = crlb_std<N>(model, d2, d2log);
-        derivative2<G, N>(d2, d2log, ParaArry, kParaYPos);
-        ParaStdY = crlb_std<N>(model, d2, d2log);
+        psf_generate<G, MODE, PEAK>(model, ParaArry);
+        derivative2<G, N, MODE, PEAK, D2>(d2, d2log, ParaArry, kParaXPos);
+        ParaStdX = crlb_std<N, FI>(model, d2, d2log);
+        derivative2<G, N, MODE, PEAK, D2>(d2, d2log, ParaArry, kParaYPos);
+        ParaStdY = crlb_std<N, FI>(model, d2, d2log);
         ParaStdX = ParaStdX * PixelSize;
         ParaStdY = ParaStdY * PixelSize;
     }

@@ -135,7 +135,7 @@ __device__ __forceinline__ float zpoly(const CorePara &c, float SigmaDif) {
 }
 
 // ------------------------------------------------------- single emitter ---
-template <int R, int KIND>
+template <int R, int KIND, int DIST = ArithSpec<KIND, R>::DIST, int MASK = ArithSpec<KIND, R>::MASK>
 __global__ void __launch_bounds__(kTPB) fit_single_kernel(const uint16_t *__restrict__ rois,
                                                           const float *__restrict__ wle, Queue q,
                                                           float *__restrict__ loc, uint8_t *__restrict__ to2e,
@@ -203,8 +203,8 @@ __global__ void __launch_bounds__(kTPB) fit_single_kernel(const uint16_t *__rest
             WLE_SigmaX = fminf(WLE_SigmaX, R / 2.0f / 2.35f);
         }
         if (c.WLEEn == 0 && MoleculeType != QCS_MOLECULE_MULTIFIT) WLE_SigmaX = R;
-        wle_weights<R>(w, kTPB, WLE_SigmaX, WLE_SigmaX, MoleculeType);
-        mle_fit<R, kGS2D>(roi, Ininf, D, kTPB);
+        wle_weights<R, MASK>(w, kTPB, WLE_SigmaX, WLE_SigmaX, MoleculeType);
+        mle_fit<R, kGS2D, DIST>(roi, Ininf, D, kTPB);
 
         const float PeakPhoton = Ininf[0] * QCS_ASCALE / c.QE;
         const float Background = Ininf[4] * QCS_BSCALE / c.QE;
@@ -271,8 +271,8 @@ __global__ void __launch_bounds__(kTPB) fit_single_kernel(const uint16_t *__rest
             WLE_SigmaX = R;
             WLE_SigmaY = R;
         }
-        wle_weights<R>(w, kTPB, WLE_SigmaX, WLE_SigmaY, MoleculeType);
-        mle_fit<R, kAS3D>(roi, Ininf, D, kTPB);
+        wle_weights<R, MASK>(w, kTPB, WLE_SigmaX, WLE_SigmaY, MoleculeType);
+        mle_fit<R, kAS3D, DIST>(roi, Ininf, D, kTPB);
 
         float PeakPhoton = Ininf[0] * QCS_ASCALE;
         float Background = Ininf[5] * QCS_BSCALE;
@@ -321,7 +321,8 @@ __global__ void __launch_bounds__(kTPB) fit_single_kernel(const uint16_t *__rest
 }
 
 // -------------------------------------------------------- multi emitter ---
-template <int R, int KIND>
+template <int R, int KIND, int DIST = ArithSpec<KIND, R>::DIST, int MASK = ArithSpec<KIND, R>::MASK,
+          int SUM2 = ArithSpec<KIND, R>::SUM2>
 __global__ void __launch_bounds__(kTPB) fit_multi_kernel(const uint16_t *__restrict__ rois,
                                                          const float *__restrict__ wle, Queue q,
                                                          float *__restrict__ loc, MultiOut mo, CorePara c) {
@@ -380,8 +381,8 @@ __global__ void __launch_bounds__(kTPB) fit_multi_kernel(const uint16_t *__restr
             Ininf[7] = 0.8f * Bkg * rBScalFactor;
         }
         if (c.WLEEn == 0) WLE_SigmaX = R;
-        wle_weights<R>(w, kTPB, WLE_SigmaX, WLE_SigmaX, QCS_MOLECULE_MULTIFIT);
-        mle_fit<R, k2E>(roi, Ininf, D, kTPB);
+        wle_weights<R, MASK>(w, kTPB, WLE_SigmaX, WLE_SigmaX, QCS_MOLECULE_MULTIFIT);
+        mle_fit<R, k2E, DIST, SUM2>(roi, Ininf, D, kTPB);
     } else if (KIND == k3E) {
         // PreEstimation_GS2D_3E
         float Mean1, Mean2, Mean3, Mean4;
@@ -405,7 +406,7 @@ __global__ void __launch_bounds__(kTPB) fit_multi_kernel(const uint16_t *__restr
         Ininf[8] = ys[1];
         Ininf[9] = SigmaX1 * rSScalFactor;
         Ininf[10] = 0.8f * Bkg * rBScalFactor;
-        mle_fit<R, k3E>(roi, Ininf, D, kTPB);
+        mle_fit<R, k3E, DIST, SUM2>(roi, Ininf, D, kTPB);
     } else {  // kAS3D2E
         float Mean1, Mean2, Mean3, Mean4;
         edge_means<R>(img, Mean1, Mean2, Mean3, Mean4);
@@ -430,7 +431,7 @@ __global__ void __launch_bounds__(kTPB) fit_multi_kernel(const uint16_t *__restr
         Ininf[8] = SigmaX1;
         Ininf[9] = SigmaY1;
         Ininf[10] = 0.8f * Bkg * rBScalFactor;
-        mle_fit<R, kAS3D2E>(roi, Ininf, D, kTPB);
+        mle_fit<R, kAS3D2E, DIST, SUM2>(roi, Ininf, D, kTPB);
     }
 
     // emitter selection (2Emitter_core.h:245-271, 3Emitter_core.h:247-280)

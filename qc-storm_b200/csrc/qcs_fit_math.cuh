@@ -1,14 +1,16 @@
 // Device arithmetic of the MLEbfgs fit: losses, numerical gradient, BFGS
 // update and the fixed iteration schedule, one CUDA thread per ROI.
 //
-// Bit-level contract: every floating-point expression here has the operand
-// order and shape of the reference CUDA code (QC-STORM bfgsMLE_dll), and the
-// same __expf/__logf intrinsics, so that nvcc emits the same rounding and the
-// same fused multiply-adds and the results equal the reference kernels' bit
-// for bit on the same GPU.  The fixed-schedule optimiser with a numerical
-// gradient amplifies any rounding difference (a single fused multiply-add
-// more or less moves most fits by more than 1e-3 px), so this is the only way
-// to reproduce the reference's results rather than its statistics.
+// Bit-level contract: the results equal the reference CUDA kernels' (QC-STORM
+// bfgsMLE_dll, compiled by nvcc for sm_100a) bit for bit on the same records.
+// The fixed-schedule optimiser with a numerical gradient amplifies any
+// rounding difference (one fused multiply-add more or less moves most fits by
+// more than 1e-3 px), so matching the reference's results rather than its
+// statistics needs the same rounding sequence: every expression keeps the
+// reference's operand order and its __expf/__logf intrinsics, and the sums of
+// two products, whose fusion nvcc decides from the surrounding code, are
+// spelled with explicit round-to-nearest intrinsics chosen per kind and ROI
+// size (ArithSpec below).
 // References (MLEbfgs/bfgs_MLE_dll x64/bfgsMLE_dll/bfgsMLE_dll/):
 //   loss        bfgsMLE_Loc_LD/bfgsMLE_GS2D_core.h:459-518, bfgsMLE_AS3D_core.h:485-544,
 //               bfgsMLE_Loc_HD/bfgsMLE_GS2D_2Emitter_core.h:519-592,
@@ -47,7 +49,50 @@ struct RoiRef {
     int ld;
 };
 
-template <int R, int KIND>
+// Contraction of a sum of two products a*b + c*d, the only operand shape
+// whose fused multiply-add nvcc chooses from the surrounding code (use
+// counts after unrolling) rather than from the expression itself:
+//   kFuseFirst   fma(a, b, c*d)     kFuseSecond  fma(c, d, a*b)
+//   kNoFuse      a*b + c*d          kCompiler    written as a*b + c*d and
+//                                                left to the compiler
+enum SumMode { kFuseFirst = 0, kFuseSecond = 1, kNoFuse = 2, kCompiler = 3 };
+
+template <int MODE>
+__device__ __forceinline__ float sum_of_products(float a, float b, float c, float d) {
+    if (MODE == kFuseFirst) return __fmaf_rn(a, b, __fmul_rn(c, d));
+    if (MODE == kFuseSecond) return __fmaf_rn(c, d, __fmul_rn(a, b));
+    if (MODE == kNoFuse) return __fadd_rn(__fmul_rn(a, b), __fmul_rn(c, d));
+    return a * b + c * d;
+}
+
+// Per-kind, per-ROI-size contraction choices of the loss (the squared
+// distance of each emitter) and of the weighted-MLE mask exponent.
+// SUM2 is the sum of the first two emitters' model terms (multi-emitter kinds).
+// The choices below are the ones the reference kernels get from nvcc 12.9 for
+// sm_100a, found by running the reference's own kernels on a B200 next to
+// each explicit variant of these kernels on the same records and keeping the
+// variant whose every output bit matches (tests/test_gpu_reference_parity.py
+// re-checks them).  They differ between ROI sizes because nvcc's unrolling,
+// and with it the use count that decides each fusion, differs.  Sizes not
+// listed keep the plain expression (kCompiler).
+template <int KIND, int R>
+struct ArithSpec {
+    enum { DIST = kCompiler, MASK = kCompiler, SUM2 = kCompiler };
+};
+template <> struct ArithSpec<kGS2D, 7> { enum { DIST = kFuseFirst, MASK = kNoFuse, SUM2 = kCompiler }; };
+template <> struct ArithSpec<kGS2D, 9> { enum { DIST = kFuseSecond, MASK = kCompiler, SUM2 = kCompiler }; };
+template <> struct ArithSpec<kGS2D, 11> { enum { DIST = kFuseSecond, MASK = kNoFuse, SUM2 = kCompiler }; };
+template <> struct ArithSpec<kGS2D, 13> { enum { DIST = kFuseSecond, MASK = kCompiler, SUM2 = kCompiler }; };
+template <> struct ArithSpec<kAS3D, 7> { enum { DIST = kFuseFirst, MASK = kFuseFirst, SUM2 = kCompiler }; };
+template <> struct ArithSpec<kAS3D, 9> { enum { DIST = kFuseFirst, MASK = kFuseFirst, SUM2 = kCompiler }; };
+template <> struct ArithSpec<kAS3D, 11> { enum { DIST = kFuseFirst, MASK = kFuseFirst, SUM2 = kCompiler }; };
+template <> struct ArithSpec<k2E, 7> { enum { DIST = kFuseFirst, MASK = kCompiler, SUM2 = kFuseFirst }; };
+template <> struct ArithSpec<k2E, 11> { enum { DIST = kFuseSecond, MASK = kCompiler, SUM2 = kFuseFirst }; };
+template <> struct ArithSpec<k3E, 7> { enum { DIST = kFuseSecond, MASK = kCompiler, SUM2 = kFuseFirst }; };
+template <> struct ArithSpec<k3E, 11> { enum { DIST = kFuseSecond, MASK = kCompiler, SUM2 = kFuseFirst }; };
+template <> struct ArithSpec<kAS3D2E, 7> { enum { DIST = kFuseFirst, MASK = kCompiler, SUM2 = kFuseFirst }; };
+
+template <int R, int KIND, int DIST = ArithSpec<KIND, R>::DIST, int SUM2 = ArithSpec<KIND, R>::SUM2>
 __device__ __forceinline__ float loss(const RoiRef &roi, float *Ininf) {
     typedef KindTraits<KIND> T;
 #pragma unroll
@@ -66,44 +111,42 @@ __device__ __forceinline__ float loss(const RoiRef &roi, float *Ininf) {
             const float colpos = col + 0.5f;
             float Loss_t;
             if (KIND == kGS2D) {
-                float tdat = -((colpos - Ininf[1]) * (colpos - Ininf[1]) + (rowpos - Ininf[2]) * (rowpos - Ininf[2])) *
-                             Ininf[3] * QCS_SSCALE;
+                const float dx = colpos - Ininf[1], dy = rowpos - Ininf[2];
+                float tdat = -(sum_of_products<DIST>(dx, dx, dy, dy)) * Ininf[3] * QCS_SSCALE;
                 float IVal = Ininf[0] * QCS_ASCALE * __expf(tdat) + Ininf[4] * QCS_BSCALE;
                 Loss_t = IVal - pixval - pixval * (__logf(IVal) - __logf(pixval));
             } else if (KIND == kAS3D) {
-                float tdat = -((colpos - Ininf[1]) * (colpos - Ininf[1]) * Ininf[3] * QCS_SSCALE +
-                               (rowpos - Ininf[2]) * (rowpos - Ininf[2]) * Ininf[4] * QCS_SSCALE);
+                const float dx = colpos - Ininf[1], dy = rowpos - Ininf[2];
+                float tdat = -(sum_of_products<DIST>(dx * dx * Ininf[3], QCS_SSCALE, dy * dy * Ininf[4], QCS_SSCALE));
                 float IVal = Ininf[0] * QCS_ASCALE * __expf(tdat) + Ininf[5] * QCS_BSCALE;
                 Loss_t = IVal - pixval - pixval * (__logf(IVal) - __logf(pixval));
             } else if (KIND == k2E) {
-                float IVal0 = Ininf[0] * QCS_ASCALE *
-                              __expf(-((colpos - Ininf[1]) * (colpos - Ininf[1]) + (rowpos - Ininf[2]) * (rowpos - Ininf[2])) *
-                                     Ininf[6] * QCS_SSCALE);
-                float IVal1 = Ininf[3] * QCS_ASCALE *
-                              __expf(-((colpos - Ininf[4]) * (colpos - Ininf[4]) + (rowpos - Ininf[5]) * (rowpos - Ininf[5])) *
-                                     Ininf[6] * QCS_SSCALE);
-                float IVal_all = IVal0 + IVal1 + Ininf[7] * QCS_BSCALE;
+                const float dx0 = colpos - Ininf[1], dy0 = rowpos - Ininf[2];
+                const float dx1 = colpos - Ininf[4], dy1 = rowpos - Ininf[5];
+                const float A0 = Ininf[0] * QCS_ASCALE, A1 = Ininf[3] * QCS_ASCALE;
+                const float e0 = __expf(-(sum_of_products<DIST>(dx0, dx0, dy0, dy0)) * Ininf[6] * QCS_SSCALE);
+                const float e1 = __expf(-(sum_of_products<DIST>(dx1, dx1, dy1, dy1)) * Ininf[6] * QCS_SSCALE);
+                float IVal_all = sum_of_products<SUM2>(A0, e0, A1, e1) + Ininf[7] * QCS_BSCALE;
                 Loss_t = IVal_all - pixval - pixval * (__logf(IVal_all) - __logf(pixval));
             } else if (KIND == k3E) {
-                float IVal0 = Ininf[0] * QCS_ASCALE *
-                              __expf(-((colpos - Ininf[1]) * (colpos - Ininf[1]) + (rowpos - Ininf[2]) * (rowpos - Ininf[2])) *
-                                     Ininf[9] * QCS_SSCALE);
-                float IVal1 = Ininf[3] * QCS_ASCALE *
-                              __expf(-((colpos - Ininf[4]) * (colpos - Ininf[4]) + (rowpos - Ininf[5]) * (rowpos - Ininf[5])) *
-                                     Ininf[9] * QCS_SSCALE);
-                float IVal2 = Ininf[6] * QCS_ASCALE *
-                              __expf(-((colpos - Ininf[7]) * (colpos - Ininf[7]) + (rowpos - Ininf[8]) * (rowpos - Ininf[8])) *
-                                     Ininf[9] * QCS_SSCALE);
-                float IVal_all = IVal0 + IVal1 + IVal2 + Ininf[10] * QCS_BSCALE;
+                const float dx0 = colpos - Ininf[1], dy0 = rowpos - Ininf[2];
+                const float dx1 = colpos - Ininf[4], dy1 = rowpos - Ininf[5];
+                const float dx2 = colpos - Ininf[7], dy2 = rowpos - Ininf[8];
+                const float A0 = Ininf[0] * QCS_ASCALE, A1 = Ininf[3] * QCS_ASCALE, A2 = Ininf[6] * QCS_ASCALE;
+                const float e0 = __expf(-(sum_of_products<DIST>(dx0, dx0, dy0, dy0)) * Ininf[9] * QCS_SSCALE);
+                const float e1 = __expf(-(sum_of_products<DIST>(dx1, dx1, dy1, dy1)) * Ininf[9] * QCS_SSCALE);
+                const float e2 = __expf(-(sum_of_products<DIST>(dx2, dx2, dy2, dy2)) * Ininf[9] * QCS_SSCALE);
+                float IVal_all = sum_of_products<SUM2>(A0, e0, A1, e1) + A2 * e2 + Ininf[10] * QCS_BSCALE;
                 Loss_t = IVal_all - pixval - pixval * (__logf(IVal_all) - __logf(pixval));
             } else {  // kAS3D2E
-                float IVal0 = Ininf[0] * QCS_ASCALE *
-                              __expf(-((colpos - Ininf[1]) * (colpos - Ininf[1]) * Ininf[3] * QCS_SSCALE +
-                                       (rowpos - Ininf[2]) * (rowpos - Ininf[2]) * Ininf[4] * QCS_SSCALE));
-                float IVal1 = Ininf[5] * QCS_ASCALE *
-                              __expf(-((colpos - Ininf[6]) * (colpos - Ininf[6]) * Ininf[8] * QCS_SSCALE +
-                                       (rowpos - Ininf[7]) * (rowpos - Ininf[7]) * Ininf[9] * QCS_SSCALE));
-                float IVal_all = IVal0 + IVal1 + Ininf[10] * QCS_BSCALE;
+                const float dx0 = colpos - Ininf[1], dy0 = rowpos - Ininf[2];
+                const float dx1 = colpos - Ininf[6], dy1 = rowpos - Ininf[7];
+                const float A0 = Ininf[0] * QCS_ASCALE, A1 = Ininf[5] * QCS_ASCALE;
+                const float e0 = __expf(-(sum_of_products<DIST>(dx0 * dx0 * Ininf[3], QCS_SSCALE, dy0 * dy0 * Ininf[4],
+                                                                QCS_SSCALE)));
+                const float e1 = __expf(-(sum_of_products<DIST>(dx1 * dx1 * Ininf[8], QCS_SSCALE, dy1 * dy1 * Ininf[9],
+                                                                QCS_SSCALE)));
+                float IVal_all = sum_of_products<SUM2>(A0, e0, A1, e1) + Ininf[10] * QCS_BSCALE;
                 Loss_t = IVal_all - pixval - pixval * (__logf(IVal_all) - __logf(pixval));
             }
             if (T::WEIGHTED)
@@ -117,7 +160,7 @@ __device__ __forceinline__ float loss(const RoiRef &roi, float *Ininf) {
 
 // Central difference on a working copy; each loss call clamps the copy in
 // place and later parameters see the clamped values, as in the reference.
-template <int R, int KIND>
+template <int R, int KIND, int DIST = ArithSpec<KIND, R>::DIST, int SUM2 = ArithSpec<KIND, R>::SUM2>
 __device__ __forceinline__ void numerical_gradient(const RoiRef &roi, const float *Ininf, float *grad) {
     enum { P = KindTraits<KIND>::P };
     float tIninf[P];
@@ -125,9 +168,9 @@ __device__ __forceinline__ void numerical_gradient(const RoiRef &roi, const floa
     for (int cnt = 0; cnt < P; cnt++) tIninf[cnt] = Ininf[cnt];
     for (int cnt = 0; cnt < P; cnt++) {
         tIninf[cnt] = tIninf[cnt] - 0.002f;
-        float tgradn = loss<R, KIND>(roi, tIninf);
+        float tgradn = loss<R, KIND, DIST, SUM2>(roi, tIninf);
         tIninf[cnt] = tIninf[cnt] + 0.004f;
-        float tgradp = loss<R, KIND>(roi, tIninf);
+        float tgradp = loss<R, KIND, DIST, SUM2>(roi, tIninf);
         grad[cnt] = (tgradp - tgradn) * 250.0f;
         tIninf[cnt] = tIninf[cnt] - 0.002f;
     }
@@ -187,7 +230,7 @@ __device__ __forceinline__ void bfgs_update(float *D, int ld, const float *sk, c
 
 // Fixed schedule: IT quasi-Newton iterations, each with an 11-step bisection
 // of the step length in [1e-5, 1]; no convergence test.  D: P x P scratch.
-template <int R, int KIND>
+template <int R, int KIND, int DIST = ArithSpec<KIND, R>::DIST, int SUM2 = ArithSpec<KIND, R>::SUM2>
 __device__ __forceinline__ void mle_fit(const RoiRef &roi, float *Ininf, float *D, int ld) {
     enum { P = KindTraits<KIND>::P, IT = KindTraits<KIND>::IT };
     float grad[P], d0[P], td0[P], sk[P], yk[P], tgrad[P];
@@ -198,7 +241,7 @@ __device__ __forceinline__ void mle_fit(const RoiRef &roi, float *Ininf, float *
 #pragma unroll
         for (int c = 0; c < P; c++) D[(r * P + c) * ld] = (r == c) ? 1.0f : 0.0f;
     }
-    numerical_gradient<R, KIND>(roi, Ininf, grad);
+    numerical_gradient<R, KIND, DIST, SUM2>(roi, Ininf, grad);
 #pragma unroll
     for (int rcnt = 0; rcnt < P; rcnt++) d0[rcnt] = -grad[rcnt];
 
@@ -219,8 +262,8 @@ __device__ __forceinline__ void mle_fit(const RoiRef &roi, float *Ininf, float *
         for (int cnt = 0; cnt < P; cnt++) xd[cnt] = d0[cnt] * 0.0001f + Ininf[cnt];
 #pragma unroll
         for (int cnt = 0; cnt < P; cnt++) xd[P + cnt] = d0[cnt] * 1.0f + Ininf[cnt];
-        ddat[0] = loss<R, KIND>(roi, &xd[0]);
-        ddat[1] = loss<R, KIND>(roi, &xd[P]);
+        ddat[0] = loss<R, KIND, DIST, SUM2>(roi, &xd[0]);
+        ddat[1] = loss<R, KIND, DIST, SUM2>(roi, &xd[P]);
 
         for (int cnt = 0; cnt < kBisections; cnt++) {
             const int xdsel = (ddat[0] < ddat[1]);
@@ -231,11 +274,11 @@ __device__ __forceinline__ void mle_fit(const RoiRef &roi, float *Ininf, float *
                 if (xdsel) {
 #pragma unroll
                     for (int k = 0; k < P; k++) xd[P + k] = d0[k] * dpos[1] + Ininf[k];
-                    ddat[1] = loss<R, KIND>(roi, &xd[P]);
+                    ddat[1] = loss<R, KIND, DIST, SUM2>(roi, &xd[P]);
                 } else {
 #pragma unroll
                     for (int k = 0; k < P; k++) xd[k] = d0[k] * dpos[0] + Ininf[k];
-                    ddat[0] = loss<R, KIND>(roi, &xd[0]);
+                    ddat[0] = loss<R, KIND, DIST, SUM2>(roi, &xd[0]);
                 }
             }
         }
@@ -252,7 +295,7 @@ __device__ __forceinline__ void mle_fit(const RoiRef &roi, float *Ininf, float *
         if (itcnt < IT - 1) {
 #pragma unroll
             for (int rcnt = 0; rcnt < P; rcnt++) tgrad[rcnt] = grad[rcnt];
-            numerical_gradient<R, KIND>(roi, Ininf, grad);
+            numerical_gradient<R, KIND, DIST, SUM2>(roi, Ininf, grad);
 #pragma unroll
             for (int rcnt = 0; rcnt < P; rcnt++) yk[rcnt] = grad[rcnt] - tgrad[rcnt];
             bfgs_update<P>(D, ld, sk, yk);
@@ -267,7 +310,7 @@ __device__ __forceinline__ void mle_fit(const RoiRef &roi, float *Ininf, float *
 }
 
 // Weighted-MLE mask (bfgsMLE_core.h:206-238).
-template <int R>
+template <int R, int MASK = kCompiler>
 __device__ __forceinline__ void wle_weights(float *w, int ld, float WLE_SigmaX, float WLE_SigmaY, int MoleculeType) {
     const float ROICenter = R / 2.0f;
     const float WLE_SigmaX1 = 1.0f / (2.0f * WLE_SigmaX * WLE_SigmaX);
@@ -279,8 +322,9 @@ __device__ __forceinline__ void wle_weights(float *w, int ld, float WLE_SigmaX, 
             if (MoleculeType == 0)
                 w[(row * R + col) * ld] = 1.0f;
             else
-                w[(row * R + col) * ld] = __expf(-((colpos - ROICenter) * (colpos - ROICenter) * WLE_SigmaX1 +
-                                                   (rowpos - ROICenter) * (rowpos - ROICenter) * WLE_SigmaY1));
+                w[(row * R + col) * ld] =
+                    __expf(-sum_of_products<MASK>((colpos - ROICenter) * (colpos - ROICenter), WLE_SigmaX1,
+                                                  (rowpos - ROICenter) * (rowpos - ROICenter), WLE_SigmaY1));
         }
     }
 }

@@ -38,6 +38,7 @@ _SIGS = {
     "qcs_fit_single_device": (C.c_int, [C.c_int, C.POINTER(LocPara), C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
                                         C.c_void_p]),
     "qcs_crlb_device": (C.c_int, [C.POINTER(LocPara), C.c_void_p, C.c_int, C.c_void_p]),
+    "qcs_measure_mufu_rate": (C.c_int, [C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_double)]),
 }
 
 
@@ -94,7 +95,7 @@ class LocContext:
         except Exception:
             pass
 
-    def localize(self, rois, wle=None, para=None):
+    def localize(self, rois, wle=None, para=None, stream=0):
         """BFGS_MLELocalization on host arrays; returns (rows[n_valid, 12], ratios[7])."""
         para = para or self.para
         rois, pr = _host(rois, np.uint16)
@@ -102,7 +103,8 @@ class LocContext:
         pw = None
         if wle is not None:
             wle, pw = _host(wle, np.float32)
-        check(self.lib.qcs_loc_bfgs_mle_localization(self.h, pr, pw, C.byref(para), n, None))
+        check(self.lib.qcs_loc_bfgs_mle_localization(self.h, pr, pw, C.byref(para), n,
+                                                     C.c_void_p(stream) if stream else None))
         nv = self.lib.qcs_loc_valid_num(self.h)
         ptr = self.lib.qcs_loc_h_loc_arry(self.h)
         rows = np.ctypeslib.as_array((C.c_float * (12 * nv)).from_address(ptr)).reshape(nv, 12).copy() if nv else \
@@ -139,3 +141,11 @@ def fit_single_device(loc_type, para, d_rois, d_wle, n, d_loc, stream=0):
 
 def crlb_device(para, d_loc, n, stream=0):
     check(load().qcs_crlb_device(C.byref(para), C.c_void_p(d_loc), int(n), C.c_void_p(stream) if stream else None))
+
+
+def mufu_rate(iters=4000):
+    """Measured MUFU operations per second of the current device."""
+    ms = C.c_float(0)
+    ops = C.c_double(0)
+    check(load().qcs_measure_mufu_rate(int(iters), C.byref(ms), C.byref(ops)))
+    return ops.value / (ms.value * 1e-3)
