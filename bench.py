@@ -57,7 +57,7 @@ def env_int(k, d):
 
 def start_clock_sampler(gpu_index):
     f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
-    q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+    q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
     try:
@@ -68,7 +68,10 @@ def start_clock_sampler(gpu_index):
     return p, f.name
 
 
-def stop_clock_sampler(p, path):
+def stop_clock_sampler(p, path, t_start, t_end):
+    """Median SM clock and active throttle reasons of the samples taken
+    between host times t_start and t_end."""
+    import datetime
     out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
     if p is None:
         return out
@@ -82,14 +85,17 @@ def stop_clock_sampler(p, path):
     with open(path) as fh:
         for line in fh:
             parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 10:
                 continue
             try:
-                sm.append(float(parts[1]))
-                mx.append(float(parts[2]))
+                ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                if ts < t_start or ts > t_end:
+                    continue
+                sm.append(float(parts[2]))
+                mx.append(float(parts[3]))
             except ValueError:
                 continue
-            for name, v in zip(names, parts[5:9]):
+            for name, v in zip(names, parts[6:10]):
                 if v.lower().startswith("active"):
                     reasons.add(name)
     os.unlink(path)
@@ -193,8 +199,8 @@ def profile_fit(n):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-fit", type=int, default=0, metavar="N",
@@ -212,6 +218,10 @@ def main():
     from qcstorm_b200 import lib, synth
 
     torch.cuda.set_device(local)
+    # a created stream: the default stream's handle is 0, which the C ABI reads
+    # as "the context's own stream"
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     if args.profile_fit:
         return profile_fit(args.profile_fit)
     dist = None
@@ -229,7 +239,6 @@ def main():
         h_batches.append(h)
         d_batches.append(h.cuda())
     ctx = lib.LocContext(para, capacity=N_PER_STEP)
-    stream = torch.cuda.current_stream()
     sh = stream.cuda_stream
 
     def step(k):
@@ -245,14 +254,17 @@ def main():
         dist.barrier()
     torch.cuda.synchronize()
     sampler, spath = start_clock_sampler(local)
+    time.sleep(0.5)  # first nvidia-smi sample lands before the timed region
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    t_start = time.time()
     e0.record(stream)
     for k in range(args.steps):
         step(k)
     e1.record(stream)
     torch.cuda.synchronize()
-    clocks = stop_clock_sampler(sampler, spath)
+    t_end = time.time()
+    clocks = stop_clock_sampler(sampler, spath, t_start, t_end)
     if dist:
         dist.barrier()
     ms = e0.elapsed_time(e1)
@@ -272,7 +284,7 @@ def main():
         lib.fit_single_device(0, para, d_batches[k].data_ptr(), wle_b[k].data_ptr(), N_PER_STEP, d_loc.data_ptr(), sh)
     torch.cuda.synchronize()
     kt = []
-    for k in range(args.steps):
+    for k in range(min(args.steps, 50)):
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)
         a.record(stream)

@@ -37,23 +37,28 @@ struct SmemLayout {
         P = KindTraits<KIND>::P,
         PIX = R * R,
         IMG = 0,
-        W = PIX * kTPB,
+        LP = PIX * kTPB,
+        W = LP + PIX * kTPB,
         D = W + (KindTraits<KIND>::WEIGHTED ? PIX * kTPB : 0),
         TOTAL = D + P * P * kTPB,  // floats
     };
 };
 
 // Stage the block's ROIs: element k of slot s at smem[k * kTPB + s].
+// Its natural log (the data term of the Poisson deviance) is stored beside
+// it at s_lp, computed once instead of once per loss evaluation.
 template <int R>
-__device__ __forceinline__ void stage_rois(float *s_img, const uint16_t *rois, const Queue &q, int base, int cnt,
-                                           float Offset, float KAdc) {
+__device__ __forceinline__ void stage_rois(float *s_img, float *s_lp, const uint16_t *rois, const Queue &q, int base,
+                                           int cnt, float Offset, float KAdc) {
     enum { PIX = R * R, WHOLE = R * (R + 1) };
     for (int idx = threadIdx.x; idx < cnt * PIX; idx += kTPB) {
         const int slot = idx / PIX;
         const int k = idx - slot * PIX;
         const int id = queue_at(q, base + slot);
         const uint16_t u = __ldg(rois + (size_t)id * WHOLE + k);
-        s_img[k * kTPB + slot] = fmaxf((u - Offset) * KAdc, 1.0f);
+        const float pixval = fmaxf((u - Offset) * KAdc, 1.0f);
+        s_img[k * kTPB + slot] = pixval;
+        s_lp[k * kTPB + slot] = __logf(pixval);
     }
 }
 
@@ -148,7 +153,7 @@ __global__ void __launch_bounds__(kTPB) fit_single_kernel(const uint16_t *__rest
     if (base >= n) return;
     const int cnt = min(kTPB, n - base);
     float *s_img = smem + L::IMG;
-    stage_rois<R>(s_img, rois, q, base, cnt, c.Offset, c.KAdc);
+    stage_rois<R>(s_img, smem + L::LP, rois, q, base, cnt, c.Offset, c.KAdc);
     __syncthreads();
     const int tid = threadIdx.x;
     if (tid >= cnt) return;
@@ -164,7 +169,7 @@ __global__ void __launch_bounds__(kTPB) fit_single_kernel(const uint16_t *__rest
     const float *pw = wle + (size_t)CurFluoID * QCS_WLE_PARA_NUM;
 
     float Ininf[P];
-    const RoiRef roi{img, w, kTPB};
+    const RoiRef roi{img, smem + L::LP + tid, w, kTPB};
     float row[12];
     bool accepted;
     float CurSNR;
@@ -334,7 +339,7 @@ __global__ void __launch_bounds__(kTPB) fit_multi_kernel(const uint16_t *__restr
     if (base >= n) return;
     const int cnt = min(kTPB, n - base);
     float *s_img = smem + L::IMG;
-    stage_rois<R>(s_img, rois, q, base, cnt, c.Offset, c.KAdc);
+    stage_rois<R>(s_img, smem + L::LP, rois, q, base, cnt, c.Offset, c.KAdc);
     __syncthreads();
     const int tid = threadIdx.x;
     if (tid >= cnt) return;
@@ -352,7 +357,7 @@ __global__ void __launch_bounds__(kTPB) fit_multi_kernel(const uint16_t *__restr
     const float QE = c.QE;
 
     float Ininf[P];
-    const RoiRef roi{img, w, kTPB};
+    const RoiRef roi{img, smem + L::LP + tid, w, kTPB};
     float NearNeighborDistance = 1000;
 
     if (KIND == k2E) {

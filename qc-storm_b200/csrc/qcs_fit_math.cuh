@@ -45,6 +45,7 @@ constexpr int kBisections = 11;
 // One ROI's pixels as seen by its thread: element k at img[k * ld].
 struct RoiRef {
     const float *img;  // photoelectrons, max((adu - offset) * gain, 1)
+    const float *lp;   // __logf of img, computed once at staging
     const float *w;    // weighted-MLE mask (read by the weighted kinds only)
     int ld;
 };
@@ -107,6 +108,7 @@ __device__ __forceinline__ float loss(const RoiRef &roi, float *Ininf) {
     for (int row = 0; row < R; row++) {
         for (int col = 0; col < R; col++) {
             const float pixval = roi.img[(row * R + col) * roi.ld];
+            const float logpix = roi.lp[(row * R + col) * roi.ld];
             const float rowpos = row + 0.5f;
             const float colpos = col + 0.5f;
             float Loss_t;
@@ -114,12 +116,12 @@ __device__ __forceinline__ float loss(const RoiRef &roi, float *Ininf) {
                 const float dx = colpos - Ininf[1], dy = rowpos - Ininf[2];
                 float tdat = -(sum_of_products<DIST>(dx, dx, dy, dy)) * Ininf[3] * QCS_SSCALE;
                 float IVal = Ininf[0] * QCS_ASCALE * __expf(tdat) + Ininf[4] * QCS_BSCALE;
-                Loss_t = IVal - pixval - pixval * (__logf(IVal) - __logf(pixval));
+                Loss_t = IVal - pixval - pixval * (__logf(IVal) - logpix);
             } else if (KIND == kAS3D) {
                 const float dx = colpos - Ininf[1], dy = rowpos - Ininf[2];
                 float tdat = -(sum_of_products<DIST>(dx * dx * Ininf[3], QCS_SSCALE, dy * dy * Ininf[4], QCS_SSCALE));
                 float IVal = Ininf[0] * QCS_ASCALE * __expf(tdat) + Ininf[5] * QCS_BSCALE;
-                Loss_t = IVal - pixval - pixval * (__logf(IVal) - __logf(pixval));
+                Loss_t = IVal - pixval - pixval * (__logf(IVal) - logpix);
             } else if (KIND == k2E) {
                 const float dx0 = colpos - Ininf[1], dy0 = rowpos - Ininf[2];
                 const float dx1 = colpos - Ininf[4], dy1 = rowpos - Ininf[5];
@@ -127,7 +129,7 @@ __device__ __forceinline__ float loss(const RoiRef &roi, float *Ininf) {
                 const float e0 = __expf(-(sum_of_products<DIST>(dx0, dx0, dy0, dy0)) * Ininf[6] * QCS_SSCALE);
                 const float e1 = __expf(-(sum_of_products<DIST>(dx1, dx1, dy1, dy1)) * Ininf[6] * QCS_SSCALE);
                 float IVal_all = sum_of_products<SUM2>(A0, e0, A1, e1) + Ininf[7] * QCS_BSCALE;
-                Loss_t = IVal_all - pixval - pixval * (__logf(IVal_all) - __logf(pixval));
+                Loss_t = IVal_all - pixval - pixval * (__logf(IVal_all) - logpix);
             } else if (KIND == k3E) {
                 const float dx0 = colpos - Ininf[1], dy0 = rowpos - Ininf[2];
                 const float dx1 = colpos - Ininf[4], dy1 = rowpos - Ininf[5];
@@ -137,7 +139,7 @@ __device__ __forceinline__ float loss(const RoiRef &roi, float *Ininf) {
                 const float e1 = __expf(-(sum_of_products<DIST>(dx1, dx1, dy1, dy1)) * Ininf[9] * QCS_SSCALE);
                 const float e2 = __expf(-(sum_of_products<DIST>(dx2, dx2, dy2, dy2)) * Ininf[9] * QCS_SSCALE);
                 float IVal_all = sum_of_products<SUM2>(A0, e0, A1, e1) + A2 * e2 + Ininf[10] * QCS_BSCALE;
-                Loss_t = IVal_all - pixval - pixval * (__logf(IVal_all) - __logf(pixval));
+                Loss_t = IVal_all - pixval - pixval * (__logf(IVal_all) - logpix);
             } else {  // kAS3D2E
                 const float dx0 = colpos - Ininf[1], dy0 = rowpos - Ininf[2];
                 const float dx1 = colpos - Ininf[6], dy1 = rowpos - Ininf[7];
@@ -147,7 +149,7 @@ __device__ __forceinline__ float loss(const RoiRef &roi, float *Ininf) {
                 const float e1 = __expf(-(sum_of_products<DIST>(dx1 * dx1 * Ininf[8], QCS_SSCALE, dy1 * dy1 * Ininf[9],
                                                                 QCS_SSCALE)));
                 float IVal_all = sum_of_products<SUM2>(A0, e0, A1, e1) + Ininf[10] * QCS_BSCALE;
-                Loss_t = IVal_all - pixval - pixval * (__logf(IVal_all) - __logf(pixval));
+                Loss_t = IVal_all - pixval - pixval * (__logf(IVal_all) - logpix);
             }
             if (T::WEIGHTED)
                 TotalLoss = TotalLoss + roi.w[(row * R + col) * roi.ld] * Loss_t;
@@ -234,8 +236,7 @@ template <int R, int KIND, int DIST = ArithSpec<KIND, R>::DIST, int SUM2 = Arith
 __device__ __forceinline__ void mle_fit(const RoiRef &roi, float *Ininf, float *D, int ld) {
     enum { P = KindTraits<KIND>::P, IT = KindTraits<KIND>::IT };
     float grad[P], d0[P], td0[P], sk[P], yk[P], tgrad[P];
-    float xd[P * 2];
-    float ddat[2], dpos[2];
+    float ddat[2], dpos[2];  // two-element arrays indexed by constants only
 #pragma unroll
     for (int r = 0; r < P; r++) {
 #pragma unroll
@@ -258,28 +259,32 @@ __device__ __forceinline__ void mle_fit(const RoiRef &roi, float *Ininf, float *
 
         dpos[0] = 0.00001f;
         dpos[1] = 1.0f;
+        {
+            float xlo[P], xhi[P];
 #pragma unroll
-        for (int cnt = 0; cnt < P; cnt++) xd[cnt] = d0[cnt] * 0.0001f + Ininf[cnt];
+            for (int cnt = 0; cnt < P; cnt++) xlo[cnt] = d0[cnt] * 0.0001f + Ininf[cnt];
 #pragma unroll
-        for (int cnt = 0; cnt < P; cnt++) xd[P + cnt] = d0[cnt] * 1.0f + Ininf[cnt];
-        ddat[0] = loss<R, KIND, DIST, SUM2>(roi, &xd[0]);
-        ddat[1] = loss<R, KIND, DIST, SUM2>(roi, &xd[P]);
+            for (int cnt = 0; cnt < P; cnt++) xhi[cnt] = d0[cnt] * 1.0f + Ininf[cnt];
+            ddat[0] = loss<R, KIND, DIST, SUM2>(roi, xlo);
+            ddat[1] = loss<R, KIND, DIST, SUM2>(roi, xhi);
+        }
 
+        // Bisection: the half that moves is chosen per ROI; the moved point
+        // is built with a select so that every thread of a warp runs the same
+        // single loss evaluation (no divergent branches around the loss).
         for (int cnt = 0; cnt < kBisections; cnt++) {
             const int xdsel = (ddat[0] < ddat[1]);
-            dpos[xdsel] = (dpos[0] + dpos[1]) * 0.5f;
+            const float mid = (dpos[0] + dpos[1]) * 0.5f;
+            dpos[0] = xdsel ? dpos[0] : mid;
+            dpos[1] = xdsel ? mid : dpos[1];
             if (cnt < kBisections - 1) {
-                // the selected half is rebuilt in place; written per slot so the
-                // array stays in registers
-                if (xdsel) {
+                const float dsel = xdsel ? dpos[1] : dpos[0];
+                float xn[P];
 #pragma unroll
-                    for (int k = 0; k < P; k++) xd[P + k] = d0[k] * dpos[1] + Ininf[k];
-                    ddat[1] = loss<R, KIND, DIST, SUM2>(roi, &xd[P]);
-                } else {
-#pragma unroll
-                    for (int k = 0; k < P; k++) xd[k] = d0[k] * dpos[0] + Ininf[k];
-                    ddat[0] = loss<R, KIND, DIST, SUM2>(roi, &xd[0]);
-                }
+                for (int k = 0; k < P; k++) xn[k] = d0[k] * dsel + Ininf[k];
+                const float f = loss<R, KIND, DIST, SUM2>(roi, xn);
+                ddat[0] = xdsel ? ddat[0] : f;
+                ddat[1] = xdsel ? f : ddat[1];
             }
         }
         const float scale = (dpos[0] + dpos[1]) * 0.5f;
