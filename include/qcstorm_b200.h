@@ -216,6 +216,27 @@ int qcs_fit_single_device(int loc_type, const qcs_loc_para *p, const uint16_t *d
  * LocPrecCalc_GaussianCRLB.cu:23-40): CRLB columns of n device rows. */
 int qcs_crlb_device(const qcs_loc_para *p, float *d_loc, int n, void *stream);
 
+/* ---- allocation-free localization --------------------------------------- */
+/*
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory: code recording the localization into a CUDA graph while its stream
+ * is captured (cudaMalloc is not allowed during capture), hosts that own all
+ * device memory through their own pool, and camera-rate loops that cannot
+ * take the device-wide synchronisation of cudaMalloc/cudaFree mid-stream.
+ * Same result as qcs_loc_localize_device (classify, single-emitter fit,
+ * 2E/3E cascade, CRLB) on caller-owned device buffers: n records d_rois, WLE
+ * rows d_wle (required), rows into d_rows (room for 2 x n rows), row count
+ * into *d_nvalid (device int, may be NULL).  Allocates nothing: its queues
+ * and counters live in one fixed library array, so n is limited to
+ * QCS_NOALLOC_MAX_ROIS (else QCS_ERR_CAPACITY).  The first call on a device
+ * looks up that array's address; make it before any stream capture.  All
+ * calls on a device share the array: calls that overlap on the GPU race and
+ * must not be issued.  Asynchronous on `stream`.
+ */
+#define QCS_NOALLOC_MAX_ROIS 8192
+int qcs_localize_noalloc(const qcs_loc_para *p, const uint16_t *d_rois, const float *d_wle, int n, float *d_rows,
+                         int *d_nvalid, void *stream);
+
 /* ---- diagnostics --------------------------------------------------------- */
 /* Sustained special-function-unit rate of the loss's __expf/__logf pair on
  * the current device: *ops MUFU operations in *ms milliseconds.  Used as the

@@ -39,6 +39,8 @@ _SIGS = {
                                         C.c_void_p]),
     "qcs_crlb_device": (C.c_int, [C.POINTER(LocPara), C.c_void_p, C.c_int, C.c_void_p]),
     "qcs_measure_mufu_rate": (C.c_int, [C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_double)]),
+    "qcs_localize_noalloc": (C.c_int, [C.POINTER(LocPara), C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                       C.c_void_p]),
 }
 
 
