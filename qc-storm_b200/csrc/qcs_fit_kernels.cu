@@ -31,25 +31,31 @@ namespace {
 
 constexpr int kTPB = 64;  // ROIs (threads) per block
 
+// One thread's view of the staged photoelectron values (element k at p[k * kTPB]).
+struct PixView {
+    const float2 *p;
+    __device__ __forceinline__ float operator[](int i) const { return p[i].x; }
+};
+
 template <int R, int KIND>
 struct SmemLayout {
     enum {
         P = KindTraits<KIND>::P,
         PIX = R * R,
-        IMG = 0,
-        LP = PIX * kTPB,
-        W = LP + PIX * kTPB,
+        IMG = 0,                 // float2 (value, log) pairs: 2 floats per element
+        W = 2 * PIX * kTPB,
         D = W + (KindTraits<KIND>::WEIGHTED ? PIX * kTPB : 0),
         TOTAL = D + P * P * kTPB,  // floats
     };
 };
 
 // Stage the block's ROIs: element k of slot s at smem[k * kTPB + s].
-// Its natural log (the data term of the Poisson deviance) is stored beside
-// it at s_lp, computed once instead of once per loss evaluation.
+// Each value is stored with its natural log (the data term of the Poisson
+// deviance), computed once instead of once per loss evaluation, as one
+// float2 so that the loss reads both with a single 64-bit load.
 template <int R>
-__device__ __forceinline__ void stage_rois(float *s_img, float *s_lp, const uint16_t *rois, const Queue &q, int base,
-                                           int cnt, float Offset, float KAdc) {
+__device__ __forceinline__ void stage_rois(float2 *s_img, const uint16_t *rois, const Queue &q, int base, int cnt,
+                                           float Offset, float KAdc) {
     enum { PIX = R * R, WHOLE = R * (R + 1) };
     for (int idx = threadIdx.x; idx < cnt * PIX; idx += kTPB) {
         const int slot = idx / PIX;
@@ -57,8 +63,7 @@ __device__ __forceinline__ void stage_rois(float *s_img, float *s_lp, const uint
         const int id = queue_at(q, base + slot);
         const uint16_t u = __ldg(rois + (size_t)id * WHOLE + k);
         const float pixval = fmaxf((u - Offset) * KAdc, 1.0f);
-        s_img[k * kTPB + slot] = pixval;
-        s_lp[k * kTPB + slot] = __logf(pixval);
+        s_img[k * kTPB + slot] = make_float2(pixval, __logf(pixval));
     }
 }
 
@@ -78,7 +83,7 @@ __device__ __forceinline__ void zero_row(float *loc, int id) {
 }
 
 template <int R>
-__device__ __forceinline__ void edge_means(const float *img, float &Mean1, float &Mean2, float &Mean3, float &Mean4) {
+__device__ __forceinline__ void edge_means(const PixView &img, float &Mean1, float &Mean2, float &Mean3, float &Mean4) {
     Mean1 = 0;
     Mean2 = 0;
     Mean3 = 0;
@@ -95,7 +100,7 @@ __device__ __forceinline__ void edge_means(const float *img, float &Mean1, float
 // Start positions of the extra emitters: the brightest (and for three
 // emitters also the second brightest) non-central block of a 3 x 3 tiling.
 template <int R>
-__device__ __forceinline__ void block_starts(const float *img, int nstart, float *xs, float *ys) {
+__device__ __forceinline__ void block_starts(const PixView &img, int nstart, float *xs, float *ys) {
     const int ROISize_Half = R / 2;
     const float ROICenter = R / 2.0f;
     const int SumROILen = R / 3 + 1;
@@ -152,14 +157,14 @@ __global__ void __launch_bounds__(kTPB) fit_single_kernel(const uint16_t *__rest
     const int base = blockIdx.x * kTPB;
     if (base >= n) return;
     const int cnt = min(kTPB, n - base);
-    float *s_img = smem + L::IMG;
-    stage_rois<R>(s_img, smem + L::LP, rois, q, base, cnt, c.Offset, c.KAdc);
+    float2 *s_img = reinterpret_cast<float2 *>(smem + L::IMG);
+    stage_rois<R>(s_img, rois, q, base, cnt, c.Offset, c.KAdc);
     __syncthreads();
     const int tid = threadIdx.x;
     if (tid >= cnt) return;
 
     const int CurFluoID = queue_at(q, base + tid);
-    const float *img = s_img + tid;
+    const PixView img{s_img + tid};
     float *w = smem + L::W + tid;
     float *D = smem + L::D + tid;
     const uint16_t *hdr = rois + (size_t)CurFluoID * WHOLE + PIX;
@@ -169,7 +174,7 @@ __global__ void __launch_bounds__(kTPB) fit_single_kernel(const uint16_t *__rest
     const float *pw = wle + (size_t)CurFluoID * QCS_WLE_PARA_NUM;
 
     float Ininf[P];
-    const RoiRef roi{img, smem + L::LP + tid, w, kTPB};
+    const RoiRef roi{s_img + tid, w, kTPB};
     float row[12];
     bool accepted;
     float CurSNR;
@@ -338,15 +343,15 @@ __global__ void __launch_bounds__(kTPB) fit_multi_kernel(const uint16_t *__restr
     const int base = blockIdx.x * kTPB;
     if (base >= n) return;
     const int cnt = min(kTPB, n - base);
-    float *s_img = smem + L::IMG;
-    stage_rois<R>(s_img, smem + L::LP, rois, q, base, cnt, c.Offset, c.KAdc);
+    float2 *s_img = reinterpret_cast<float2 *>(smem + L::IMG);
+    stage_rois<R>(s_img, rois, q, base, cnt, c.Offset, c.KAdc);
     __syncthreads();
     const int tid = threadIdx.x;
     if (tid >= cnt) return;
 
     const int slot = base + tid;
     const int CurFluoID = queue_at(q, slot);
-    const float *img = s_img + tid;
+    const PixView img{s_img + tid};
     float *w = smem + L::W + tid;
     float *D = smem + L::D + tid;
     const uint16_t *hdr = rois + (size_t)CurFluoID * WHOLE + PIX;
@@ -357,7 +362,7 @@ __global__ void __launch_bounds__(kTPB) fit_multi_kernel(const uint16_t *__restr
     const float QE = c.QE;
 
     float Ininf[P];
-    const RoiRef roi{img, smem + L::LP + tid, w, kTPB};
+    const RoiRef roi{s_img + tid, w, kTPB};
     float NearNeighborDistance = 1000;
 
     if (KIND == k2E) {

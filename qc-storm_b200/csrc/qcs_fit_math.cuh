@@ -43,12 +43,17 @@ constexpr int kBisections = 11;
 #define QCS_SSCALE (0.1f)
 
 // One ROI's pixels as seen by its thread: element k at img[k * ld].
+// img holds pairs (photoelectrons max((adu - offset) * gain, 1), its __logf),
+// element k at img[k * ld]; w the weighted-MLE mask, element k at w[k * ld].
 struct RoiRef {
-    const float *img;  // photoelectrons, max((adu - offset) * gain, 1)
-    const float *lp;   // __logf of img, computed once at staging
-    const float *w;    // weighted-MLE mask (read by the weighted kinds only)
+    const float2 *img;
+    const float *w;    // read by the weighted kinds only
     int ld;
 };
+
+// Pixel rows are unrolled up to this ROI size (7x7 and 9x9 cover the
+// high-throughput single-emitter cases); the row loop stays rolled.
+constexpr int kUnrollMaxR = 9;
 
 // Contraction of a sum of two products a*b + c*d, the only operand shape
 // whose fused multiply-add nvcc chooses from the surrounding code (use
@@ -76,10 +81,13 @@ __device__ __forceinline__ float sum_of_products(float a, float b, float c, floa
 // re-checks them).  They differ between ROI sizes because nvcc's unrolling,
 // and with it the use count that decides each fusion, differs.  Sizes not
 // listed keep the plain expression (kCompiler).
+// MODEL is amplitude * exp + background of the single-emitter kinds: the
+// amplitude product is fused (its only use), the background product is not.
 template <int KIND, int R>
 struct ArithSpec {
     enum { DIST = kCompiler, MASK = kCompiler, SUM2 = kCompiler };
 };
+constexpr int kModelSum = kFuseFirst;
 template <> struct ArithSpec<kGS2D, 7> { enum { DIST = kFuseFirst, MASK = kNoFuse, SUM2 = kCompiler }; };
 template <> struct ArithSpec<kGS2D, 9> { enum { DIST = kFuseSecond, MASK = kCompiler, SUM2 = kCompiler }; };
 template <> struct ArithSpec<kGS2D, 11> { enum { DIST = kFuseSecond, MASK = kNoFuse, SUM2 = kCompiler }; };
@@ -93,6 +101,22 @@ template <> struct ArithSpec<k3E, 7> { enum { DIST = kFuseSecond, MASK = kCompil
 template <> struct ArithSpec<k3E, 11> { enum { DIST = kFuseSecond, MASK = kCompiler, SUM2 = kFuseFirst }; };
 template <> struct ArithSpec<kAS3D2E, 7> { enum { DIST = kFuseFirst, MASK = kCompiler, SUM2 = kFuseFirst }; };
 
+// Model exponential of one single-emitter parameter vector v at the pixel
+// centred on (cp, rp) (GS2D: v = A, x, y, S, B; AS3D: A, x, y, Sx, Sy, B).
+template <int KIND, int DIST>
+__device__ __forceinline__ float single_expo(float cp, float rp, const float *v) {
+    const float dx = cp - v[1], dy = rp - v[2];
+    if (KIND == kGS2D) return __expf(-(sum_of_products<DIST>(dx, dx, dy, dy)) * v[3] * QCS_SSCALE);
+    return __expf(-(sum_of_products<DIST>(dx * dx * v[3], QCS_SSCALE, dy * dy * v[4], QCS_SSCALE)));
+}
+
+// Poisson deviance term of one pixel given the model exponential e.
+template <int KIND>
+__device__ __forceinline__ float single_term(float e, const float *v, float pixval, float logpix) {
+    const float IVal = sum_of_products<kModelSum>(v[0] * QCS_ASCALE, e, v[KindTraits<KIND>::P - 1], QCS_BSCALE);
+    return __fmaf_rn(-pixval, __logf(IVal) - logpix, __fsub_rn(IVal, pixval));
+}
+
 template <int R, int KIND, int DIST = ArithSpec<KIND, R>::DIST, int SUM2 = ArithSpec<KIND, R>::SUM2>
 __device__ __forceinline__ float loss(const RoiRef &roi, float *Ininf) {
     typedef KindTraits<KIND> T;
@@ -105,23 +129,17 @@ __device__ __forceinline__ float loss(const RoiRef &roi, float *Ininf) {
         }
     }
     float TotalLoss = 0;
+#pragma unroll 1
     for (int row = 0; row < R; row++) {
+#pragma unroll(R <= kUnrollMaxR ? R : 1)
         for (int col = 0; col < R; col++) {
-            const float pixval = roi.img[(row * R + col) * roi.ld];
-            const float logpix = roi.lp[(row * R + col) * roi.ld];
+            const float2 pl = roi.img[(row * R + col) * roi.ld];
+            const float pixval = pl.x, logpix = pl.y;
             const float rowpos = row + 0.5f;
             const float colpos = col + 0.5f;
             float Loss_t;
-            if (KIND == kGS2D) {
-                const float dx = colpos - Ininf[1], dy = rowpos - Ininf[2];
-                float tdat = -(sum_of_products<DIST>(dx, dx, dy, dy)) * Ininf[3] * QCS_SSCALE;
-                float IVal = Ininf[0] * QCS_ASCALE * __expf(tdat) + Ininf[4] * QCS_BSCALE;
-                Loss_t = IVal - pixval - pixval * (__logf(IVal) - logpix);
-            } else if (KIND == kAS3D) {
-                const float dx = colpos - Ininf[1], dy = rowpos - Ininf[2];
-                float tdat = -(sum_of_products<DIST>(dx * dx * Ininf[3], QCS_SSCALE, dy * dy * Ininf[4], QCS_SSCALE));
-                float IVal = Ininf[0] * QCS_ASCALE * __expf(tdat) + Ininf[5] * QCS_BSCALE;
-                Loss_t = IVal - pixval - pixval * (__logf(IVal) - logpix);
+            if (KIND == kGS2D || KIND == kAS3D) {
+                Loss_t = single_term<KIND>(single_expo<KIND, DIST>(colpos, rowpos, Ininf), Ininf, pixval, logpix);
             } else if (KIND == k2E) {
                 const float dx0 = colpos - Ininf[1], dy0 = rowpos - Ininf[2];
                 const float dx1 = colpos - Ininf[4], dy1 = rowpos - Ininf[5];
@@ -152,9 +170,9 @@ __device__ __forceinline__ float loss(const RoiRef &roi, float *Ininf) {
                 Loss_t = IVal_all - pixval - pixval * (__logf(IVal_all) - logpix);
             }
             if (T::WEIGHTED)
-                TotalLoss = TotalLoss + roi.w[(row * R + col) * roi.ld] * Loss_t;
+                TotalLoss = __fmaf_rn(roi.w[(row * R + col) * roi.ld], Loss_t, TotalLoss);
             else
-                TotalLoss = TotalLoss + Loss_t;
+                TotalLoss = __fadd_rn(TotalLoss, Loss_t);
         }
     }
     return TotalLoss;
@@ -176,6 +194,78 @@ __device__ __forceinline__ void numerical_gradient(const RoiRef &roi, const floa
         grad[cnt] = (tgradp - tgradn) * 250.0f;
         tIninf[cnt] = tIninf[cnt] - 0.002f;
     }
+}
+
+// The central-difference gradient of the single-emitter kinds in one sweep
+// over the pixels: the 2P evaluation points are first replayed exactly as
+// numerical_gradient produces them (with its in-place clamping), then every
+// pixel is loaded once and each point's deviance accumulated in its own sum,
+// in pixel order.  The amplitude and background points leave the exponent's
+// inputs (x, y, widths) unchanged, so their exponential is the base point's;
+// this is checked bit for bit per ROI, and a warp with any ROI where it does
+// not hold falls back to the point-by-point gradient.  Each sum therefore
+// equals the separate loss evaluation bit for bit.
+template <int R, int KIND, int DIST = ArithSpec<KIND, R>::DIST>
+__device__ __forceinline__ void numerical_gradient_shared(const RoiRef &roi, const float *Ininf, float *grad) {
+    typedef KindTraits<KIND> T;
+    enum { P = T::P, NE = 2 * P };
+    float v[NE][P];
+    {
+        float t[P];
+#pragma unroll
+        for (int k = 0; k < P; k++) t[k] = Ininf[k];
+#pragma unroll
+        for (int k = 0; k < P; k++) {
+            t[k] = t[k] - 0.002f;
+#pragma unroll
+            for (int c = 0; c < P; c++) {
+                if (T::CLAMP001) { if (t[c] < 0.01f) t[c] = 0.01f; } else { if (t[c] < 0.0f) t[c] = 0.0f; }
+                v[2 * k][c] = t[c];
+            }
+            t[k] = t[k] + 0.004f;
+#pragma unroll
+            for (int c = 0; c < P; c++) {
+                if (T::CLAMP001) { if (t[c] < 0.01f) t[c] = 0.01f; } else { if (t[c] < 0.0f) t[c] = 0.0f; }
+                v[2 * k + 1][c] = t[c];
+            }
+            t[k] = t[k] - 0.002f;
+        }
+    }
+    bool share = true;
+#pragma unroll
+    for (int c = 1; c < P - 1; c++) {
+        const unsigned b = __float_as_uint(v[0][c]);
+        share = share && (__float_as_uint(v[1][c]) == b) && (__float_as_uint(v[NE - 2][c]) == b) &&
+                (__float_as_uint(v[NE - 1][c]) == b);
+    }
+    if (!__all_sync(__activemask(), share)) {
+        numerical_gradient<R, KIND, DIST>(roi, Ininf, grad);
+        return;
+    }
+    float tot[NE];
+#pragma unroll
+    for (int j = 0; j < NE; j++) tot[j] = 0;
+#pragma unroll 1
+    for (int row = 0; row < R; row++) {
+#pragma unroll(R <= kUnrollMaxR ? R : 1)
+        for (int col = 0; col < R; col++) {
+            const float2 pl = roi.img[(row * R + col) * roi.ld];
+            const float pixval = pl.x, logpix = pl.y;
+            const float w = T::WEIGHTED ? roi.w[(row * R + col) * roi.ld] : 1.0f;
+            const float rowpos = row + 0.5f;
+            const float colpos = col + 0.5f;
+            const float e_base = single_expo<KIND, DIST>(colpos, rowpos, v[0]);
+#pragma unroll
+            for (int j = 0; j < NE; j++) {
+                const bool base = (j < 2) || (j >= NE - 2);
+                const float e = base ? e_base : single_expo<KIND, DIST>(colpos, rowpos, v[j]);
+                const float Lt = single_term<KIND>(e, v[j], pixval, logpix);
+                tot[j] = T::WEIGHTED ? __fmaf_rn(w, Lt, tot[j]) : __fadd_rn(tot[j], Lt);
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < P; k++) grad[k] = (tot[2 * k + 1] - tot[2 * k]) * 250.0f;
 }
 
 // D <- (I - s y'/(y's)) D (I - y s'/(y's)) + s s'/(y's); D is row-major P x P
@@ -230,6 +320,14 @@ __device__ __forceinline__ void bfgs_update(float *D, int ld, const float *sk, c
     }
 }
 
+template <int R, int KIND, int DIST, int SUM2>
+__device__ __forceinline__ void gradient(const RoiRef &roi, const float *Ininf, float *grad) {
+    if (KIND == kGS2D || KIND == kAS3D)
+        numerical_gradient_shared<R, KIND, DIST>(roi, Ininf, grad);
+    else
+        numerical_gradient<R, KIND, DIST, SUM2>(roi, Ininf, grad);
+}
+
 // Fixed schedule: IT quasi-Newton iterations, each with an 11-step bisection
 // of the step length in [1e-5, 1]; no convergence test.  D: P x P scratch.
 template <int R, int KIND, int DIST = ArithSpec<KIND, R>::DIST, int SUM2 = ArithSpec<KIND, R>::SUM2>
@@ -242,7 +340,7 @@ __device__ __forceinline__ void mle_fit(const RoiRef &roi, float *Ininf, float *
 #pragma unroll
         for (int c = 0; c < P; c++) D[(r * P + c) * ld] = (r == c) ? 1.0f : 0.0f;
     }
-    numerical_gradient<R, KIND, DIST, SUM2>(roi, Ininf, grad);
+    gradient<R, KIND, DIST, SUM2>(roi, Ininf, grad);
 #pragma unroll
     for (int rcnt = 0; rcnt < P; rcnt++) d0[rcnt] = -grad[rcnt];
 
@@ -300,7 +398,7 @@ __device__ __forceinline__ void mle_fit(const RoiRef &roi, float *Ininf, float *
         if (itcnt < IT - 1) {
 #pragma unroll
             for (int rcnt = 0; rcnt < P; rcnt++) tgrad[rcnt] = grad[rcnt];
-            numerical_gradient<R, KIND, DIST, SUM2>(roi, Ininf, grad);
+            gradient<R, KIND, DIST, SUM2>(roi, Ininf, grad);
 #pragma unroll
             for (int rcnt = 0; rcnt < P; rcnt++) yk[rcnt] = grad[rcnt] - tgrad[rcnt];
             bfgs_update<P>(D, ld, sk, yk);
