@@ -139,6 +139,68 @@ const char *qcs_last_error(void);
 /* 1 if the library found a usable CUDA device, else 0. */
 int qcs_device_available(void);
 
+/* ---- ROI extraction: LDROIExtractData_TypeDef --------------------------- */
+/*
+ * Molecule detection and ROI cutting on batches of raw frames
+ * (SubregionExtraction/LDROIExtraction.h:35-93): background removal, image
+ * variance, 5-tap Gaussian smoothing, 3x3 local-maximum detection,
+ * single/multi classification, ROI records with header, and the WLE pre-pass
+ * of the new records.  Records and WLE rows accumulate in device memory
+ * across calls until qcs_extract_reset_roi_num, like TotalROINumber.
+ * Differences a caller can see: a batch's records come in pixel order
+ * (y * width + x over the stacked batch) instead of GPU arrival order; the
+ * variance comes from exact integer sums (the reference's float atomics
+ * vary run to run); detections beyond QCS_MAX_POINT_NUM per batch or beyond
+ * the context capacity are dropped and counted (qcs_extract_dropped_num)
+ * instead of overrunning buffers; frames already in device memory
+ * (QCS_IMAGE_SOURCE_GPU) are read in place, which the reference rejects.
+ */
+typedef struct qcs_extract_data qcs_extract_data;
+
+/* LDROIExtractData_TypeDef::GetMaxBatchedNumForCurrentImageSize
+ * (LDROIExtraction.h:86, LDROIExtraction.cu:207-216). */
+int qcs_extract_max_batched_num(int image_width, int image_high);
+/* LDROIExtractData_TypeDef::Init(LocalizationPara&) (LDROIExtraction.cu:219-286):
+ * frame buffers for qcs_extract_max_batched_num frames of ImageWidth x
+ * ImageHigh, QCS_MAX_POINT_NUM accumulated records of ROISize, smoothing taps
+ * from ROISize / LocType / MultiEmitterFitEn (FilterInit). */
+int qcs_extract_init(const qcs_loc_para *p, qcs_extract_data **out);
+/* Same with explicit frames per batch and record capacity (<= 0: defaults). */
+int qcs_extract_init_ex(const qcs_loc_para *p, int max_batched_num, int capacity, qcs_extract_data **out);
+/* LDROIExtractData_TypeDef::Deinit (LDROIExtraction.cu:289). */
+int qcs_extract_deinit(qcs_extract_data *c);
+/*
+ * LDROIExtractData_TypeDef::ExtractMolecules(unsigned short *pImgData,
+ * int ImageSource, LocalizationPara&, int StartFrame_CurBatch,
+ * int BatchedImageNum, cudaStream_t) (LDROIExtraction.cu:30-80).
+ * img: batched_num stacked frames, host memory (QCS_IMAGE_SOURCE_CPU_PINNED /
+ * _CPU_NORMAL) or device memory (QCS_IMAGE_SOURCE_GPU, read in place, must
+ * stay valid until the stream reaches this work).  Asynchronous on `stream`
+ * (NULL: the context's own stream); the reference synchronises twice per call.
+ */
+int qcs_extract_molecules(qcs_extract_data *c, const uint16_t *img, int image_source, const qcs_loc_para *p,
+                          int start_frame, int batched_num, void *stream);
+/* GetAccumulatedROINum (LDROIExtraction.cu:181): waits for the last call. */
+int qcs_extract_accumulated_roi_num(qcs_extract_data *c, int *n);
+/* ResetROINum (LDROIExtraction.cu:187-194): count 0, frame range (-1, -1). */
+int qcs_extract_reset_roi_num(qcs_extract_data *c);
+/* h_ImageROI and Get_h_WLEPara() (LDROIExtraction.h:43, .cu:196): host copies
+ * of the accumulated records / WLE rows, brought up to date on each call
+ * (waits for the last extraction); NULL on error. */
+const uint16_t *qcs_extract_h_image_roi(qcs_extract_data *c);
+const float *qcs_extract_h_wle_para(qcs_extract_data *c);
+/* d_ImageROI-equivalent accumulation buffer and Get_d_WLEPara()
+ * (LDROIExtraction.cu:201), device memory, to feed qcs_loc_localize_device
+ * without a host round trip; qcs_extract_device_roi_num: device int holding
+ * the accumulated count. */
+const uint16_t *qcs_extract_d_image_roi(const qcs_extract_data *c);
+const float *qcs_extract_d_wle_para(const qcs_extract_data *c);
+const int *qcs_extract_device_roi_num(const qcs_extract_data *c);
+/* FirstFrame / EndFrame (LDROIExtraction.h:46-47). */
+int qcs_extract_frame_range(const qcs_extract_data *c, int *first_frame, int *end_frame);
+/* Detections dropped for capacity since the last reset (no counterpart). */
+int qcs_extract_dropped_num(qcs_extract_data *c, int *n);
+
 /* ---- localization context: LDLocData_TypeDef --------------------------- */
 /*
  * One context owns every buffer of the localization path for records of one

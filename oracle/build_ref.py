@@ -16,7 +16,15 @@ reference source text is kept in the repository):
   2. SplineInterpolation.h names a function-pointer parameter after an
      enclosing template parameter (InputDataLen), which MSVC accepts and GCC
      rejects; the parameter name is dropped (names in a function-pointer
-     parameter list have no meaning).
+     parameter list have no meaning);
+  3. gpuRemoveBackgroundIntensity (LDROIExtraction_ImageFiltering.cu:240-250)
+     has its 32 threads (one warp) read their neighbours' BkgVal entries
+     after one barrier and overwrite their own entry in the next loop
+     iteration before the next barrier.  A warp executing in lock step reads
+     before any lane writes; the emulator runs one thread at a time between
+     barriers, so lane 0 would overwrite its entry before lane 1 reads it.
+     A __syncthreads() is inserted after the read, which restores the
+     lock-step order on the host and changes nothing the GPU computes.
 Nothing else is changed.  Only the built .so lands in oracle/_ref/.
 
 With --gpu the same sources are compiled unmodified by nvcc for sm_100a
@@ -66,12 +74,16 @@ FNPTR_PARAM = re.compile(
     r"(\(\s*\*\s*FindPositionID\s*\)\s*\([^()]*?)int\s+InputDataLen\s*,")
 
 
+BKG_MEAN = re.compile(r"(float\s+MeanBkg\s*=\s*\(BkgVal\[Sel0\][^;]*;)")
+
+
 def rewrite(text, launches=True):
     def launch(m):
         kernel, cfg, empty = m.group(1), m.group(2).strip(), m.group(3)
         return "qcs_emu_cfg(%s).run((%s)%s" % (cfg, kernel, ")" if empty else ", ")
     if launches:
         text, _ = LAUNCH.subn(launch, text)
+        text = BKG_MEAN.sub(r"\1 __syncthreads();", text)
     text = FNPTR_PARAM.sub(r"\1int,", text)
     return text
 

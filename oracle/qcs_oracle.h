@@ -46,10 +46,22 @@ int qcso_fit_single_f64(int kind, const qcs_loc_para *p, const uint16_t *rois, c
 int qcso_crlb(const qcs_loc_para *p, float *loc, int n);
 
 /* ROI extraction over n_frames frames fed in batches of `batch` frames, as
- * consecutive ExtractMolecules calls; rois_out cap x R(R+1), wle_out cap x 6. */
+ * consecutive ExtractMolecules calls; rois_out cap x R(R+1), wle_out cap x 6.
+ * flags selects the arithmetic of the two steps whose rounding depends on how
+ * the reference is built and run:
+ *   QCSO_EXTRACT_FMA_CONV        smoothing taps accumulated with fused
+ *                                multiply-add, as nvcc compiles the
+ *                                reference's convolution kernels (without
+ *                                it: separately rounded, the host build);
+ *   QCSO_EXTRACT_EXACT_VARIANCE  variance from exact integer sums (the
+ *                                product's deterministic definition; without
+ *                                it: float sums in pixel order, the order the
+ *                                host build's one-block-at-a-time run adds in). */
+#define QCSO_EXTRACT_FMA_CONV 1
+#define QCSO_EXTRACT_EXACT_VARIANCE 2
 int qcso_extract(const qcs_loc_para *p, const uint16_t *frames, int n_frames, int batch,
-                 int start_frame, uint16_t *rois_out, float *wle_out, int cap, int *n_roi,
-                 int *first_frame, int *end_frame);
+                 int start_frame, int flags, uint16_t *rois_out, float *wle_out, int cap,
+                 int *n_roi, int *first_frame, int *end_frame);
 
 #ifdef __cplusplus
 }

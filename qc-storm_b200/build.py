@@ -20,9 +20,10 @@ LIB = os.path.join(HERE, "lib", "libqcstorm_b200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2", "-I" + INCLUDE]
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2,-ffp-contract=off", "-I" + INCLUDE]
 
-UNITS = ["qcs_fit_kernels.cu", "qcs_crlb.cu", "qcs_wle.cu", "qcs_cascade.cu", "qcs_api.cu", "qcs_diag.cu", "qcs_noalloc.cu"]
+UNITS = ["qcs_fit_kernels.cu", "qcs_crlb.cu", "qcs_wle.cu", "qcs_cascade.cu", "qcs_api.cu", "qcs_diag.cu", "qcs_noalloc.cu",
+         "qcs_extract.cu"]
 
 
 def deps():

@@ -9,6 +9,7 @@
 
 #include "../../include/qcstorm_b200.h"
 #include "qcs_cascade.h"
+#include "qcs_error.h"
 #include "qcs_fit_math.cuh"
 #include "qcs_kernels.h"
 
@@ -16,7 +17,9 @@ namespace {
 
 thread_local std::string g_err;
 
-int fail(int code, const char *what, cudaError_t e = cudaSuccess) {
+}  // namespace
+
+int qcs::fail(int code, const char *what, cudaError_t e) {
     g_err = what;
     if (e != cudaSuccess) {
         g_err += ": ";
@@ -25,11 +28,9 @@ int fail(int code, const char *what, cudaError_t e = cudaSuccess) {
     return code;
 }
 
-#define QCS_CUDA(call, what)                                  \
-    do {                                                      \
-        cudaError_t e_ = (call);                              \
-        if (e_ != cudaSuccess) return fail(QCS_ERR_CUDA, what, e_); \
-    } while (0)
+namespace {
+
+using qcs::fail;
 
 int check_para(const qcs_loc_para *p, bool multi_ok_sizes = true) {
     if (!p) return fail(QCS_ERR_ARG, "null parameter struct");

@@ -35,4 +35,11 @@ cudaError_t launch_crlb(float *loc, const int *n_dev, int n, int max_rows, int l
 size_t wle_scratch_bytes(int n);
 cudaError_t launch_wle(const uint16_t *rois, int n, int R, int loc_type, float *wle, void *scratch, cudaStream_t s);
 
+// The same pass over records [d_span[0], d_span[0] + d_span[1]) (read on the
+// device; d_span[1] <= max_n) that are already in ascending (frame, y, x)
+// order, as ROI extraction writes them, with keys[i] = frame << 32 | y << 16 | x
+// of record i: no sort, no scratch, no host sync.
+cudaError_t launch_wle_presorted(const uint16_t *rois, const unsigned long long *keys, const int *d_span, int max_n,
+                                 int R, int loc_type, float *wle, cudaStream_t s);
+
 }  // namespace qcs

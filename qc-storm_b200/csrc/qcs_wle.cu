@@ -11,6 +11,10 @@
 // results).  The nearest-neighbour search replaces the reference's O(N^2)
 // all-pairs loop with a (frame, y, x) radix sort and a y-bounded scan of the
 // sorted neighbours; the integer squared distance it minimises is the same.
+// Records produced by ROI extraction are already in (frame, y, x) order;
+// launch_wle_presorted takes their range from device memory and scans their
+// compact key array without the sort, so the pass needs no host
+// synchronisation.
 #include <cstdint>
 #include <cub/device/device_radix_sort.cuh>
 #include <cuda_runtime.h>
@@ -126,11 +130,25 @@ __device__ __forceinline__ void two_sided_width(float *SigmaL, float *SigmaR, co
     *SigmaR = SDat_R * QCS_INTERP_GAP / MaxValue / 1.2533f;
 }
 
+// Records [begin, begin + n): from the arguments, or from span[0], span[1]
+// in device memory when span is set (grid-stride loops cover any n).
+struct Span {
+    int begin, n;
+    const int *span;
+    __device__ __forceinline__ void get(int &b, int &m) const {
+        if (span) {
+            b = span[0];
+            m = span[1];
+        } else {
+            b = begin;
+            m = n;
+        }
+    }
+};
+
 template <int R>
-__global__ void psf_width_kernel(const uint16_t *__restrict__ rois, float *__restrict__ wle, int n) {
+__device__ __forceinline__ void psf_width_one(const uint16_t *__restrict__ rois, float *__restrict__ wle, int gid) {
     enum { Len = R, ILen = (R - 1) * kInterp + 1, WHOLE = R * (R + 1) };
-    const int gid = threadIdx.x + blockDim.x * blockIdx.x;
-    if (gid >= n) return;
     const uint16_t *pROI = rois + (size_t)gid * WHOLE;
     float MeanX[Len], MeanY[Len], x0[Len], xn[ILen], yn_MeanX[ILen], yn_MeanY[ILen];
     for (int cnt = 0; cnt < Len; cnt++) {
@@ -171,6 +189,14 @@ __global__ void psf_width_kernel(const uint16_t *__restrict__ rois, float *__res
     o[4] = SigmaD;
 }
 
+template <int R>
+__global__ void psf_width_kernel(const uint16_t *__restrict__ rois, float *__restrict__ wle, Span sp) {
+    int b, n;
+    sp.get(b, n);
+    for (int k = threadIdx.x + blockDim.x * blockIdx.x; k < n; k += gridDim.x * blockDim.x)
+        psf_width_one<R>(rois, wle, b + k);
+}
+
 // Sort key: frame (32 bits) | y (16) | x (16) of the ROI centre.
 __global__ void nn_keys_kernel(const uint16_t *__restrict__ rois, int n, int whole, int pix,
                                unsigned long long *keys, int *vals) {
@@ -182,37 +208,69 @@ __global__ void nn_keys_kernel(const uint16_t *__restrict__ rois, int n, int who
     vals[i] = i;
 }
 
-// Minimum squared distance to another ROI of the same frame, scanning the
-// sorted order both ways until the row distance alone exceeds the best.
+// Distance to the nearest other ROI centre of the same frame: scans the
+// (frame, y, x)-sorted keys k[0..n) outwards from a, in each direction until
+// the frame changes or the row distance alone exceeds the best so far.  Keys
+// are fetched 8 at a time so that their loads overlap; they are examined in
+// the same order as a one-by-one scan, which stops at the same key.
+__device__ __forceinline__ float nn_sorted(const unsigned long long *__restrict__ k, int a, int n) {
+    const unsigned long long ka = k[a];
+    const unsigned long long frame = ka >> 32;
+    const int ya = (int)((ka >> 16) & 0xFFFF), xa = (int)(ka & 0xFFFF);
+    float best = 100000000.0f;
+    bool go = true;
+    for (int b = a + 1; go && b < n; b += 8) {
+        unsigned long long kb[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) kb[j] = (b + j < n) ? __ldg(k + b + j) : ~0ull;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            if (!go) break;
+            if ((kb[j] >> 32) != frame) {
+                go = false;
+                break;
+            }
+            const int dy = (int)((kb[j] >> 16) & 0xFFFF) - ya, dx = (int)(kb[j] & 0xFFFF) - xa;
+            if ((float)(dy * dy) > best) {
+                go = false;
+                break;
+            }
+            best = fminf(best, (float)(dx * dx + dy * dy));
+        }
+    }
+    go = true;
+    for (int b = a - 1; go && b >= 0; b -= 8) {
+        unsigned long long kb[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) kb[j] = (b - j >= 0) ? __ldg(k + b - j) : ~0ull;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            if (!go) break;
+            if ((kb[j] >> 32) != frame) {
+                go = false;
+                break;
+            }
+            const int dy = (int)((kb[j] >> 16) & 0xFFFF) - ya, dx = (int)(kb[j] & 0xFFFF) - xa;
+            if ((float)(dy * dy) > best) {
+                go = false;
+                break;
+            }
+            best = fminf(best, (float)(dx * dx + dy * dy));
+        }
+    }
+    return sqrtf(best);
+}
+
+// Minimum distance for each record, over the radix-sorted keys.
 __global__ void nn_scan_kernel(const unsigned long long *__restrict__ keys, const int *__restrict__ vals, int n,
                                float *__restrict__ wle) {
     const int a = threadIdx.x + blockDim.x * blockIdx.x;
     if (a >= n) return;
-    const unsigned long long ka = keys[a];
-    const unsigned long long frame = ka >> 32;
-    const int ya = (int)((ka >> 16) & 0xFFFF), xa = (int)(ka & 0xFFFF);
-    float best = 100000000.0f;
-    for (int b = a + 1; b < n; b++) {
-        const unsigned long long kb = keys[b];
-        if ((kb >> 32) != frame) break;
-        const int dy = (int)((kb >> 16) & 0xFFFF) - ya, dx = (int)(kb & 0xFFFF) - xa;
-        if ((float)(dy * dy) > best) break;
-        best = fminf(best, (float)(dx * dx + dy * dy));
-    }
-    for (int b = a - 1; b >= 0; b--) {
-        const unsigned long long kb = keys[b];
-        if ((kb >> 32) != frame) break;
-        const int dy = (int)((kb >> 16) & 0xFFFF) - ya, dx = (int)(kb & 0xFFFF) - xa;
-        if ((float)(dy * dy) > best) break;
-        best = fminf(best, (float)(dx * dx + dy * dy));
-    }
-    wle[(size_t)vals[a] * QCS_WLE_PARA_NUM + 0] = sqrtf(best);
+    wle[(size_t)vals[a] * QCS_WLE_PARA_NUM + 0] = nn_sorted(keys, a, n);
 }
 
-__global__ void classify_kernel(const uint16_t *__restrict__ rois, float *__restrict__ wle, int n, int R, int whole,
-                                int LocType) {
-    const int gid = threadIdx.x + blockDim.x * blockIdx.x;
-    if (gid >= n) return;
+__device__ __forceinline__ void classify_one(const uint16_t *__restrict__ rois, float *__restrict__ wle, int gid, int R,
+                                             int whole, int LocType) {
     float MaxMeanSigmaTh;
     if (LocType == QCS_LOCTYPE_GS2D)
         MaxMeanSigmaTh = R / 2.1f / 2.35f;
@@ -238,6 +296,48 @@ __global__ void classify_kernel(const uint16_t *__restrict__ rois, float *__rest
     w[5] = MoleculeType;
 }
 
+__global__ void classify_kernel(const uint16_t *__restrict__ rois, float *__restrict__ wle, Span sp, int R, int whole,
+                                int LocType) {
+    int b, n;
+    sp.get(b, n);
+    for (int k = threadIdx.x + blockDim.x * blockIdx.x; k < n; k += gridDim.x * blockDim.x)
+        classify_one(rois, wle, b + k, R, whole, LocType);
+}
+
+// Records already in ascending (frame, y, x) order with their keys in a
+// compact array: PSF widths, nearest neighbour and molecule type of each
+// record in one pass (one thread per record).
+template <int R>
+__global__ void wle_sorted_kernel(const uint16_t *__restrict__ rois, const unsigned long long *__restrict__ keys,
+                                  Span sp, float *__restrict__ wle, int LocType) {
+    int b0, n;
+    sp.get(b0, n);
+    for (int a = threadIdx.x + blockDim.x * blockIdx.x; a < n; a += gridDim.x * blockDim.x) {
+        psf_width_one<R>(rois, wle, b0 + a);
+        wle[(size_t)(b0 + a) * QCS_WLE_PARA_NUM + 0] = nn_sorted(keys + b0, a, n);
+        classify_one(rois, wle, b0 + a, R, R * (R + 1), LocType);
+    }
+}
+
+template <int R>
+void psf_width_launch(const uint16_t *rois, float *wle, Span sp, int grid, int tpb, cudaStream_t s) {
+    psf_width_kernel<R><<<grid, tpb, 0, s>>>(rois, wle, sp);
+}
+
+cudaError_t launch_psf_width(int R, const uint16_t *rois, float *wle, Span sp, int grid, int tpb, cudaStream_t s) {
+    switch (R) {
+    case 5: psf_width_launch<5>(rois, wle, sp, grid, tpb, s); break;
+    case 7: psf_width_launch<7>(rois, wle, sp, grid, tpb, s); break;
+    case 9: psf_width_launch<9>(rois, wle, sp, grid, tpb, s); break;
+    case 11: psf_width_launch<11>(rois, wle, sp, grid, tpb, s); break;
+    case 13: psf_width_launch<13>(rois, wle, sp, grid, tpb, s); break;
+    case 15: psf_width_launch<15>(rois, wle, sp, grid, tpb, s); break;
+    case 17: psf_width_launch<17>(rois, wle, sp, grid, tpb, s); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaSuccess;
+}
+
 size_t sort_temp_bytes(int n) {
     size_t bytes = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const unsigned long long *)nullptr, (unsigned long long *)nullptr,
@@ -258,16 +358,9 @@ cudaError_t launch_wle(const uint16_t *rois, int n, int R, int loc_type, float *
     if (n <= 0) return cudaSuccess;
     const int tpb = 64;
     const int grid = (n + tpb - 1) / tpb;
-    switch (R) {
-    case 5: psf_width_kernel<5><<<grid, tpb, 0, s>>>(rois, wle, n); break;
-    case 7: psf_width_kernel<7><<<grid, tpb, 0, s>>>(rois, wle, n); break;
-    case 9: psf_width_kernel<9><<<grid, tpb, 0, s>>>(rois, wle, n); break;
-    case 11: psf_width_kernel<11><<<grid, tpb, 0, s>>>(rois, wle, n); break;
-    case 13: psf_width_kernel<13><<<grid, tpb, 0, s>>>(rois, wle, n); break;
-    case 15: psf_width_kernel<15><<<grid, tpb, 0, s>>>(rois, wle, n); break;
-    case 17: psf_width_kernel<17><<<grid, tpb, 0, s>>>(rois, wle, n); break;
-    default: return cudaErrorInvalidValue;
-    }
+    const Span sp{0, n, nullptr};
+    cudaError_t e = launch_psf_width(R, rois, wle, sp, grid, tpb, s);
+    if (e != cudaSuccess) return e;
     const size_t nn = (size_t)n;
     char *p = static_cast<char *>(scratch);
     unsigned long long *k_in = reinterpret_cast<unsigned long long *>(p);
@@ -281,10 +374,30 @@ cudaError_t launch_wle(const uint16_t *rois, int n, int R, int loc_type, float *
     size_t temp = sort_temp_bytes(n);
     const int whole = R * (R + 1);
     nn_keys_kernel<<<grid, tpb, 0, s>>>(rois, n, whole, R * R, k_in, v_in);
-    cudaError_t e = cub::DeviceRadixSort::SortPairs(p, temp, k_in, k_out, v_in, v_out, n, 0, 64, s);
+    e = cub::DeviceRadixSort::SortPairs(p, temp, k_in, k_out, v_in, v_out, n, 0, 64, s);
     if (e != cudaSuccess) return e;
     nn_scan_kernel<<<grid, tpb, 0, s>>>(k_out, v_out, n, wle);
-    classify_kernel<<<grid, tpb, 0, s>>>(rois, wle, n, R, whole, loc_type);
+    classify_kernel<<<grid, tpb, 0, s>>>(rois, wle, sp, R, whole, loc_type);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wle_presorted(const uint16_t *rois, const unsigned long long *keys, const int *d_span, int max_n,
+                                 int R, int loc_type, float *wle, cudaStream_t s) {
+    if (max_n <= 0) return cudaSuccess;
+    const int tpb = 64;
+    int grid = (max_n + tpb - 1) / tpb;
+    if (grid > 148 * 8) grid = 148 * 8;
+    const Span sp{0, 0, d_span};
+    switch (R) {
+    case 5: wle_sorted_kernel<5><<<grid, tpb, 0, s>>>(rois, keys, sp, wle, loc_type); break;
+    case 7: wle_sorted_kernel<7><<<grid, tpb, 0, s>>>(rois, keys, sp, wle, loc_type); break;
+    case 9: wle_sorted_kernel<9><<<grid, tpb, 0, s>>>(rois, keys, sp, wle, loc_type); break;
+    case 11: wle_sorted_kernel<11><<<grid, tpb, 0, s>>>(rois, keys, sp, wle, loc_type); break;
+    case 13: wle_sorted_kernel<13><<<grid, tpb, 0, s>>>(rois, keys, sp, wle, loc_type); break;
+    case 15: wle_sorted_kernel<15><<<grid, tpb, 0, s>>>(rois, keys, sp, wle, loc_type); break;
+    case 17: wle_sorted_kernel<17><<<grid, tpb, 0, s>>>(rois, keys, sp, wle, loc_type); break;
+    default: return cudaErrorInvalidValue;
+    }
     return cudaGetLastError();
 }
 

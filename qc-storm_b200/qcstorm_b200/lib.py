@@ -41,6 +41,21 @@ _SIGS = {
     "qcs_measure_mufu_rate": (C.c_int, [C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_double)]),
     "qcs_localize_noalloc": (C.c_int, [C.POINTER(LocPara), C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
                                        C.c_void_p]),
+    "qcs_extract_max_batched_num": (C.c_int, [C.c_int, C.c_int]),
+    "qcs_extract_init": (C.c_int, [C.POINTER(LocPara), C.POINTER(C.c_void_p)]),
+    "qcs_extract_init_ex": (C.c_int, [C.POINTER(LocPara), C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "qcs_extract_deinit": (C.c_int, [C.c_void_p]),
+    "qcs_extract_molecules": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(LocPara), C.c_int, C.c_int,
+                                        C.c_void_p]),
+    "qcs_extract_accumulated_roi_num": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "qcs_extract_reset_roi_num": (C.c_int, [C.c_void_p]),
+    "qcs_extract_h_image_roi": (C.c_void_p, [C.c_void_p]),
+    "qcs_extract_h_wle_para": (C.c_void_p, [C.c_void_p]),
+    "qcs_extract_d_image_roi": (C.c_void_p, [C.c_void_p]),
+    "qcs_extract_d_wle_para": (C.c_void_p, [C.c_void_p]),
+    "qcs_extract_device_roi_num": (C.c_void_p, [C.c_void_p]),
+    "qcs_extract_frame_range": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "qcs_extract_dropped_num": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
 }
 
 
@@ -151,3 +166,83 @@ def mufu_rate(iters=4000):
     ops = C.c_double(0)
     check(load().qcs_measure_mufu_rate(int(iters), C.byref(ms), C.byref(ops)))
     return ops.value / (ms.value * 1e-3)
+
+
+IMAGE_SOURCE = {"gpu": 0, "pinned": 1, "normal": 2}
+
+
+class ExtractContext:
+    """LDROIExtractData_TypeDef: detection and ROI cutting on batches of frames.
+
+    Records and WLE rows accumulate on the device across extract() calls until
+    reset(), like the reference's TotalROINumber."""
+
+    def __init__(self, para, max_batched_num=0, capacity=0):
+        self.lib = load()
+        self.para = para
+        h = C.c_void_p()
+        check(self.lib.qcs_extract_init_ex(C.byref(para), int(max_batched_num), int(capacity), C.byref(h)))
+        self.h = h
+        self.whole = para.ROISize * (para.ROISize + 1)
+
+    def close(self):
+        if self.h:
+            self.lib.qcs_extract_deinit(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def extract(self, frames, start_frame=0, para=None, stream=0):
+        """ExtractMolecules on a host array of stacked frames (n, H, W) uint16."""
+        para = para or self.para
+        frames, pf = _host(frames, np.uint16)
+        nb = frames.shape[0] if frames.ndim == 3 else 1
+        check(self.lib.qcs_extract_molecules(self.h, pf, IMAGE_SOURCE["normal"], C.byref(para), int(start_frame), nb,
+                                             C.c_void_p(stream) if stream else None))
+
+    def extract_device(self, d_frames, batched_num, start_frame=0, para=None, stream=0, source="gpu"):
+        """ExtractMolecules on frames at a device (or pinned host) address."""
+        para = para or self.para
+        check(self.lib.qcs_extract_molecules(self.h, C.c_void_p(d_frames), IMAGE_SOURCE[source], C.byref(para),
+                                             int(start_frame), int(batched_num),
+                                             C.c_void_p(stream) if stream else None))
+
+    def accumulated(self):
+        n = C.c_int(0)
+        check(self.lib.qcs_extract_accumulated_roi_num(self.h, C.byref(n)))
+        return n.value
+
+    def reset(self):
+        check(self.lib.qcs_extract_reset_roi_num(self.h))
+
+    def records(self):
+        """Host copies of the accumulated (records[n, R(R+1)] uint16, wle[n, 6] float32)."""
+        n = self.accumulated()
+        pr = self.lib.qcs_extract_h_image_roi(self.h)
+        pw = self.lib.qcs_extract_h_wle_para(self.h)
+        if not pr or not pw:
+            raise QcsError(4, self.lib.qcs_last_error().decode())
+        if n == 0:
+            return np.zeros((0, self.whole), np.uint16), np.zeros((0, 6), np.float32)
+        rois = np.ctypeslib.as_array((C.c_uint16 * (self.whole * n)).from_address(pr)).reshape(n, self.whole).copy()
+        wle = np.ctypeslib.as_array((C.c_float * (6 * n)).from_address(pw)).reshape(n, 6).copy()
+        return rois, wle
+
+    def frame_range(self):
+        a, b = C.c_int(0), C.c_int(0)
+        check(self.lib.qcs_extract_frame_range(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def dropped(self):
+        n = C.c_int(0)
+        check(self.lib.qcs_extract_dropped_num(self.h, C.byref(n)))
+        return n.value
+
+    def device_records(self):
+        """(device address of the records, of the WLE rows, of the int count)."""
+        return (self.lib.qcs_extract_d_image_roi(self.h), self.lib.qcs_extract_d_wle_para(self.h),
+                self.lib.qcs_extract_device_roi_num(self.h))

@@ -78,6 +78,36 @@ def crlb(para, loc, lib="oracle"):
     return out
 
 
+EXTRACT_FMA_CONV = 1
+EXTRACT_EXACT_VARIANCE = 2
+
+
+def extract(para, frames, batch, start_frame=0, flags=0, lib="oracle", cap=None):
+    """ROI extraction over a stack of frames fed `batch` frames per call.
+
+    Returns (records n x R(R+1) uint16, wle n x 6, first_frame, end_frame).
+    lib: "oracle" (flags select its arithmetic), "ref" (host build of the
+    reference) or "ref_gpu" (the reference's CUDA build)."""
+    frames = np.ascontiguousarray(frames, np.uint16)
+    nf = frames.shape[0]
+    R = para.ROISize
+    cap = cap or 200000
+    rois = np.zeros((cap, R * (R + 1)), np.uint16)
+    wl = np.zeros((cap, 6), np.float32)
+    n, f0, f1 = C.c_int(0), C.c_int(0), C.c_int(0)
+    if lib == "oracle":
+        st = oracle().qcso_extract(C.byref(para), _p(frames), nf, batch, start_frame, flags, _p(rois), _p(wl), cap,
+                                   C.byref(n), C.byref(f0), C.byref(f1))
+    else:
+        L = ref_host() if lib == "ref" else ref_gpu()
+        f = L.qcsref_extract if lib == "ref" else L.qcsrefg_extract
+        st = f(C.byref(para), _p(frames), nf, batch, start_frame, _p(rois), _p(wl), cap, C.byref(n), C.byref(f0),
+               C.byref(f1))
+    assert st == 0, st
+    k = min(n.value, cap)
+    return rois[:k].copy(), wl[:k].copy(), f0.value, f1.value
+
+
 def set_threads(n):
     oracle().qcso_set_threads(int(n))
 
