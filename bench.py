@@ -5,10 +5,11 @@ One step = one localization call over N = 100,000 synthetic 7x7 ROI records
 (the reference's per-call batch size, MaxPointNum = 102,400): WLE pre-pass
 (PSF width, nearest neighbour, molecule type) -> single-emitter fit with the
 reference's fixed schedule -> CRLB, all on the device through the C ABI
-(qcs_loc_localize_device).  Records: seeded synthetic config-0 ROIs (sigma
+(qcs_loc_localize_device).  Records: seeded synthetic 7x7 ROIs (sigma
 U(1.0,1.6) px, photons log-U[500,5000], background U(20,100) e-/px, Poisson),
 16 distinct batches rotated across steps (179 MB of records, more than the
-126 MB L2).
+126 MB L2).  The `frames` object adds the whole-frame pipeline (2048 x 2048
+frames -> extraction -> multi-emitter localization -> CRLB) in frames/s.
 
 Printed JSON line (rank 0): `value` is device-timed fits/s with records
 resident in HBM; `e2e` is the same metric through the host-buffer call
@@ -166,13 +167,92 @@ def run_reference_arm(args, rank):
 
 def config_dict(args):
     return {
-        "workload": "GS2D 7x7 single-emitter MLEbfgs, %d ROI records per call: WLE pre-pass + fit + CRLB "
-                    "(config-0 generator)" % N_PER_STEP,
+        "workload": "GS2D 7x7 single-emitter MLEbfgs, %d ROI records per call: WLE pre-pass + fit + CRLB; "
+                    "sigma U(1.0,1.6) px, photons log-U[500,5000], background U(20,100) e-/px" % N_PER_STEP,
         "roi_size": R, "rois_per_step": N_PER_STEP, "mode": "plain MLEbfgs, reference schedule, bit-exact with "
                                                           "the reference CUDA kernel",
         "input_batches": BATCHES, "l2": "records rotate over %d batches (%.0f MB > 126 MB L2)" % (
             BATCHES, BATCHES * N_PER_STEP * R * (R + 1) * 2 / 1e6),
         "parallelism": "dp%d (independent frame batches per GPU)" % args.gpus,
+    }
+
+
+FRAME_W = FRAME_H = 2048
+FRAMES = 8             # distinct frames rotated across steps (2048 x 2048 uint16 = 8.4 MB each)
+FRAMES_PER_CALL = 32   # frames whose ROIs accumulate before one localization call
+MAX_POINT_NUM = 102400
+
+
+def frame_pipeline(stream, steps, warmup):
+    """Whole-frame pipeline: 2048 x 2048 uint16 frames -> ROI extraction
+    (background, smoothing, detection, 7x7 cut, WLE; one frame per extraction
+    batch, records accumulating on the device) -> after FRAMES_PER_CALL frames
+    one multi-emitter MLEbfgs call (1E -> 2E -> 3E cascade) -> CRLB, as the
+    reference's plug-ins accumulate ROIs across extraction batches before
+    localizing.  Everything runs on one stream with no host synchronisation
+    (the record count stays on the device).  value: frames/s with frames
+    resident in HBM; e2e: the same with every frame copied from pinned host
+    memory and the rows read back to the host (qcs_loc_read_rows) inside the
+    timed region."""
+    import torch
+    from qcstorm_b200 import lib, synth
+    fr, para, _ = synth.frames(FRAMES, width=FRAME_W, height=FRAME_H, density=3000, seed=77)
+    para.MultiEmitterFitEn = 1
+    ex = lib.ExtractContext(para, max_batched_num=1, capacity=MAX_POINT_NUM)
+    loc = lib.LocContext(para, capacity=MAX_POINT_NUM)
+    d_fr = torch.from_numpy(fr.view(np.int16)).cuda()
+    h_fr = torch.from_numpy(fr.view(np.int16)).pin_memory()
+    sh = stream.cuda_stream
+    d_rois, d_wle, d_n = ex.device_records()
+    frame_bytes = FRAME_W * FRAME_H * 2
+
+    def step(k, host=False):
+        ex.reset(sh)
+        for j in range(FRAMES_PER_CALL):
+            f = k * FRAMES_PER_CALL + j
+            if host:
+                ex.extract_device(h_fr.data_ptr() + (f % FRAMES) * frame_bytes, 1, f, stream=sh, source="pinned")
+            else:
+                ex.extract_device(d_fr.data_ptr() + (f % FRAMES) * frame_bytes, 1, f, stream=sh)
+        loc.localize_device_n(d_rois, d_wle, d_n, MAX_POINT_NUM, sh)
+
+    step(0)
+    rows0, _ = loc.read_rows(sh)
+    recs0 = ex.accumulated()
+    assert ex.dropped() == 0
+    for k in range(warmup):
+        step(k)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(steps):
+        step(k)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    e2e_steps = max(3, steps // 4)
+    t0 = time.perf_counter()
+    out_rows = 0
+    for k in range(e2e_steps):
+        step(k, host=True)
+        r, _ = loc.read_rows(sh)
+        out_rows += r.shape[0]
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
+    ex.close()
+    loc.close()
+    return {
+        "workload": "2048x2048 uint16 frames, ~3000 emitters/frame (20%% in pairs < 3 px), GS2D 7x7, multi-emitter "
+                    "fitting on; %d frames per localization call, %d distinct frames rotated" % (
+                        FRAMES_PER_CALL, FRAMES),
+        "frames_per_s": FRAMES_PER_CALL * 1e3 / ms, "ms_per_call": ms, "frames_per_call": FRAMES_PER_CALL,
+        "records_per_call": recs0, "rows_per_call": int(rows0.shape[0]),
+        "localizations_per_s": rows0.shape[0] * 1e3 / ms, "steps": steps,
+        "e2e": {"frames_per_s": FRAMES_PER_CALL * 1e3 / e2e_ms, "ms_per_call": e2e_ms,
+                "h2d_bytes_per_call": FRAMES_PER_CALL * frame_bytes,
+                "d2h_bytes_per_call": int(out_rows / e2e_steps) * 48 + 32,
+                "calls": "%d x qcs_extract_molecules (pinned frame) -> qcs_loc_localize_device_n -> "
+                         "qcs_loc_read_rows" % FRAMES_PER_CALL},
     }
 
 
@@ -203,6 +283,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-frames", action="store_true", help="skip the whole-frame pipeline measurement")
     ap.add_argument("--profile-fit", type=int, default=0, metavar="N",
                     help="only run the single-emitter fit kernel 3 times on N records (for ncu captures)")
     args = ap.parse_args()
@@ -314,6 +395,10 @@ def main():
            "d2h_bytes_per_step": int(rows / e2e_steps) * 48 + 32,
            "call": "qcs_loc_bfgs_mle_localization (pinned host records, WLE on device, synchronous)"}
 
+    frames = None
+    if not args.no_frames:
+        frames = frame_pipeline(stream, steps=min(max(args.steps // 40, 5), 40), warmup=3)
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         cpu, _ = cpu_reference_rate(steps=1)
@@ -329,7 +414,7 @@ def main():
                          "kernel_ms": fit_ms,
                          "algorithmic": "%d px-evals x %d MUFU per fit; peak = measured __expf/__logf rate" % (
                              PX_EVALS_PER_FIT, MUFU_PER_PX_EVAL)},
-            "cpu_baseline": cpu, "clocks": clocks,
+            "cpu_baseline": cpu, "clocks": clocks, "frames": frames,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -182,8 +182,10 @@ int qcs_extract_molecules(qcs_extract_data *c, const uint16_t *img, int image_so
                           int start_frame, int batched_num, void *stream);
 /* GetAccumulatedROINum (LDROIExtraction.cu:181): waits for the last call. */
 int qcs_extract_accumulated_roi_num(qcs_extract_data *c, int *n);
-/* ResetROINum (LDROIExtraction.cu:187-194): count 0, frame range (-1, -1). */
-int qcs_extract_reset_roi_num(qcs_extract_data *c);
+/* ResetROINum (LDROIExtraction.cu:187-194): count 0, frame range (-1, -1).
+ * The device count is cleared in stream order on `stream` (NULL: the stream
+ * of the last call), with no host synchronisation. */
+int qcs_extract_reset_roi_num(qcs_extract_data *c, void *stream);
 /* h_ImageROI and Get_h_WLEPara() (LDROIExtraction.h:43, .cu:196): host copies
  * of the accumulated records / WLE rows, brought up to date on each call
  * (waits for the last extraction); NULL on error. */
@@ -233,6 +235,10 @@ int qcs_loc_capacity(const qcs_loc_data *c);
  */
 int qcs_loc_bfgs_mle_localization(qcs_loc_data *c, const uint16_t *h_rois, const float *h_wle,
                                   const qcs_loc_para *p, int n, void *stream);
+/* After qcs_loc_localize_device / _device_n: wait for `stream` (NULL: the
+ * context's stream) and bring the rows, their count and the fit ratios to
+ * the host, as qcs_loc_bfgs_mle_localization leaves them. */
+int qcs_loc_read_rows(qcs_loc_data *c, const qcs_loc_para *p, void *stream);
 /* h_LocArry: valid until the next call on the context (bfgs_top.h:38). */
 const float *qcs_loc_h_loc_arry(const qcs_loc_data *c);
 /* oValidFluoNum (bfgs_top.h:42). */
@@ -251,6 +257,12 @@ int qcs_loc_fit_ratios(const qcs_loc_data *c, float *out7);
  */
 int qcs_loc_localize_device(qcs_loc_data *c, const uint16_t *d_rois, const float *d_wle,
                             const qcs_loc_para *p, int n, void *stream);
+/* The same with the record count read on the device: *d_n (clamped to
+ * [0, max_n], max_n <= capacity), e.g. qcs_extract_device_roi_num, so that
+ * frames -> extraction -> localization runs with no host round trip.  d_wle is
+ * required (the extraction writes it).  No counterpart in the reference. */
+int qcs_loc_localize_device_n(qcs_loc_data *c, const uint16_t *d_rois, const float *d_wle, const qcs_loc_para *p,
+                              const int *d_n, int max_n, void *stream);
 const float *qcs_loc_device_rows(const qcs_loc_data *c);
 const int *qcs_loc_device_valid_num(const qcs_loc_data *c);
 /* The context's own device record / WLE buffers (capacity records). */

@@ -45,19 +45,6 @@ int check() {
     return (int)e;
 }
 
-// gpu_CalculatePSFWidth<ROISize> (WLEParaEstimation_core.h:44-156) calls
-// FindPositionID through a function pointer (SplineInterpolation.h:88) from a
-// frame of 1120 bytes at ROISize 9 up to 2480 at 19 (ptxas, sm_100a).  Above
-// the default 1 KB per-thread stack the driver raises the limit to the
-// kernel's static frame only, so the indirect callee's frame overflows it and
-// the widths depend on what ran before in the process.  A 4 KB stack (a
-// per-process context limit) lets the reference run as its source intends.
-void provision_stack() {
-    size_t cur = 0;
-    if (cudaDeviceGetLimit(&cur, cudaLimitStackSize) == cudaSuccess && cur < 4096)
-        cudaDeviceSetLimit(cudaLimitStackSize, 4096);
-}
-
 }  // namespace
 
 extern "C" {
@@ -67,7 +54,6 @@ extern "C" {
 // buffers (and so make the reference read or write past them) are refused here.
 int qcsrefg_localize(const qcs_loc_para *p, const unsigned short *rois, const float *wle, int n,
                      float *out, int out_cap, int *n_valid, float *ratios) {
-    provision_stack();
     LocalizationPara r;
     to_ref(p, r);
     if (n < 0 || n > MaxPointNum / 2) return -1;
@@ -106,7 +92,6 @@ int qcsrefg_localize(const qcs_loc_para *p, const unsigned short *rois, const fl
 // out: n rows of 12 floats, zero-initialised before the launch.
 int qcsrefg_fit_kernel(int kind, const qcs_loc_para *p, const unsigned short *rois, const float *wle,
                        int n, float *out, float *ms) {
-    provision_stack();
     LocalizationPara r;
     to_ref(p, r);
     CoreFittingPara c;
@@ -180,7 +165,6 @@ int qcsrefg_fit_kernel(int kind, const qcs_loc_para *p, const unsigned short *ro
 // order of the reference's atomic counter; *n_rows = n + appended.
 int qcsrefg_fit_multi_kernel(int kind, const qcs_loc_para *p, const unsigned short *rois, const float *wle, int n,
                              float *out, int out_cap, int *n_rows) {
-    provision_stack();
     LocalizationPara r;
     to_ref(p, r);
     if (n <= 0 || n > MaxPointNum / 2 || out_cap < 2 * n) return -1;
@@ -275,7 +259,6 @@ __global__ void probe_psf_kernel(float *out, const float *para) {
 extern "C" {
 
 int qcsrefg_probe_weights(int R, float sx, float sy, int type, float *out) {
-    provision_stack();
     float *d;
     cudaMalloc((void **)&d, sizeof(float) * 17 * 17);
     switch (R) {
@@ -293,7 +276,6 @@ int qcsrefg_probe_weights(int R, float sx, float sy, int type, float *out) {
 }
 
 int qcsrefg_probe_psf(int G, const float *para6, float *out) {
-    provision_stack();
     float *d, *dp;
     cudaMalloc((void **)&d, sizeof(float) * 15 * 15);
     cudaMalloc((void **)&dp, sizeof(float) * 6);
@@ -310,7 +292,6 @@ int qcsrefg_probe_psf(int G, const float *para6, float *out) {
 // CRLB over n rows in place; rows padded to a multiple of 32 (no bounds guard
 // in the reference kernel).
 int qcsrefg_crlb(const qcs_loc_para *p, float *loc, int n) {
-    provision_stack();
     LocalizationPara r;
     to_ref(p, r);
     const int padded = (n + ThreadsPerBlock - 1) / ThreadsPerBlock * ThreadsPerBlock;
@@ -326,7 +307,6 @@ int qcsrefg_crlb(const qcs_loc_para *p, float *loc, int n) {
 }
 
 int qcsrefg_wle(const qcs_loc_para *p, const unsigned short *rois, int n, float *wle_out) {
-    provision_stack();
     LocalizationPara r;
     to_ref(p, r);
     WLEParameterEstimation_TypeDef w;
@@ -350,7 +330,6 @@ int qcsrefg_wle(const qcs_loc_para *p, const unsigned short *rois, int n, float 
 int qcsrefg_extract(const qcs_loc_para *p, const unsigned short *frames, int n_frames, int batch,
                     int start_frame, unsigned short *rois_out, float *wle_out, int cap, int *n_roi,
                     int *first_frame, int *end_frame) {
-    provision_stack();
     LocalizationPara r;
     to_ref(p, r);
     if ((size_t)r.ImageWidth * r.ImageHigh * batch > (size_t)512 * 512 * 4) return -1;

@@ -207,6 +207,25 @@ int qcs_loc_localize_device(qcs_loc_data *c, const uint16_t *d_rois, const float
     return QCS_OK;
 }
 
+int qcs_loc_localize_device_n(qcs_loc_data *c, const uint16_t *d_rois, const float *d_wle, const qcs_loc_para *p,
+                              const int *d_n, int max_n, void *stream) {
+    int st = check_call(c, p, max_n);
+    if (st) return st;
+    if (!d_rois || !d_wle || !d_n) return fail(QCS_ERR_ARG, "null pointer");
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+    qcs::CascadeArgs a;
+    a.para = *p;
+    a.rois = d_rois;
+    a.wle = d_wle;
+    a.n = max_n;
+    a.n_dev = d_n;
+    a.loc = c->d_loc;
+    a.max_rows = c->max_rows;
+    a.stream = s;
+    QCS_CUDA(qcs::run_cascade(a, c->st), "localization cascade");
+    return QCS_OK;
+}
+
 const float *qcs_loc_device_rows(const qcs_loc_data *c) { return c ? c->d_loc : nullptr; }
 const int *qcs_loc_device_valid_num(const qcs_loc_data *c) { return c ? c->st.counters + qcs::kCntValid : nullptr; }
 uint16_t *qcs_loc_device_roi_buffer(qcs_loc_data *c) { return c ? c->d_rois : nullptr; }
@@ -262,6 +281,25 @@ int qcs_loc_bfgs_mle_localization(qcs_loc_data *c, const uint16_t *h_rois, const
                  "read localizations");
     QCS_CUDA(cudaStreamSynchronize(s), "read localizations");
     c->valid = rows;
+    compute_ratios(c, p, n);
+    return QCS_OK;
+}
+
+int qcs_loc_read_rows(qcs_loc_data *c, const qcs_loc_para *p, void *stream) {
+    if (!c || !p) return fail(QCS_ERR_ARG, "null argument");
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+    QCS_CUDA(cudaMemcpyAsync(c->h_counters, c->st.counters, qcs::kCntNum * sizeof(int), cudaMemcpyDeviceToHost, s),
+             "read counters");
+    QCS_CUDA(cudaStreamSynchronize(s), "localization");
+    const int rows = c->h_counters[qcs::kCntValid];
+    if (rows > 0)
+        QCS_CUDA(cudaMemcpyAsync(c->h_loc, c->d_loc, (size_t)rows * QCS_OUT_PARA_NUM * sizeof(float),
+                                 cudaMemcpyDeviceToHost, s),
+                 "read localizations");
+    QCS_CUDA(cudaStreamSynchronize(s), "read localizations");
+    c->valid = rows;
+    // records of the call: single-emitter queue plus the classifier's 2E entries
+    const int n = c->h_counters[qcs::kCntSingle] + (p->MultiEmitterFitEn ? c->h_counters[qcs::kCnt2EClassify] : 0);
     compute_ratios(c, p, n);
     return QCS_OK;
 }

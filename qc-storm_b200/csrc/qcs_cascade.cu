@@ -48,8 +48,10 @@ __device__ __forceinline__ int block_scan(int pred, int *total) {
 // (MLEFit, WLEFit) and the two-emitter queue (MultiFit), both ascending
 // (bfgs_top_MoleculeClasify.cu:26-92).
 __global__ void __launch_bounds__(kScanThreads) classify_queues_kernel(const float *__restrict__ wle, int n,
-                                                                       int multi, CascadeState st) {
+                                                                       const int *__restrict__ n_dev, int multi,
+                                                                       CascadeState st) {
     __shared__ int tot;
+    if (n_dev) n = min(max(*n_dev, 0), n);
     int n1 = 0, n2 = 0;
     for (int base = 0; base < n; base += kScanThreads) {
         const int i = base + threadIdx.x;
@@ -145,7 +147,8 @@ __global__ void __launch_bounds__(kScanThreads) compact_multi_kernel(CascadeStat
     }
 }
 
-__global__ void init_counters_kernel(CascadeState st, int n) {
+__global__ void init_counters_kernel(CascadeState st, int n, const int *__restrict__ n_dev) {
+    if (n_dev) n = min(max(*n_dev, 0), n);
     st.counters[kCntSingle] = n;
     st.counters[kCnt2E] = 0;
     st.counters[kCnt2EClassify] = 0;
@@ -171,9 +174,9 @@ cudaError_t run_cascade(const CascadeArgs &a, const CascadeState &st) {
     cudaError_t e;
 
     if (multi)
-        classify_queues_kernel<<<1, kScanThreads, 0, a.stream>>>(a.wle, n, multi, st);
+        classify_queues_kernel<<<1, kScanThreads, 0, a.stream>>>(a.wle, n, a.n_dev, multi, st);
     else
-        init_counters_kernel<<<1, 1, 0, a.stream>>>(st, n);
+        init_counters_kernel<<<1, 1, 0, a.stream>>>(st, n, a.n_dev);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
 
     FitLaunch f;
@@ -184,8 +187,8 @@ cudaError_t run_cascade(const CascadeArgs &a, const CascadeState &st) {
     f.stream = a.stream;
     f.mo = MultiOut{nullptr, nullptr};
     // Single emitter over the classify queue (identity when multi-emitter
-    // fitting is off, as in the reference).
-    f.q = multi ? Queue{st.q_single, st.counters + kCntSingle, 0} : Queue{nullptr, nullptr, n};
+    // fitting is off, as in the reference); its length is on the device.
+    f.q = Queue{multi ? st.q_single : nullptr, st.counters + kCntSingle, 0};
     f.max_count = n;
     f.to2e = multi ? st.to2e : nullptr;
     if ((e = launch_fit(as3d ? kAS3D : kGS2D, R, f)) != cudaSuccess) return e;

@@ -37,7 +37,8 @@ struct CascadeArgs {
     qcs_loc_para para;
     const uint16_t *rois;  // device, n records
     const float *wle;      // device, n x 6
-    int n;
+    int n;                 // record count, or its upper bound when n_dev is set
+    const int *n_dev = nullptr;  // device record count (read on the device), or null
     float *loc;            // device, max_rows x 12
     int max_rows;
     cudaStream_t stream;

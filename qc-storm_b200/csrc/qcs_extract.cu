@@ -77,16 +77,25 @@ struct EmitPara {
 
 __device__ __forceinline__ int clampi(int v, int lo, int hi) { return min(max(v, lo), hi); }
 
-// float -> uint16 as the reference's implicit conversion of non-negative
-// values: truncation, saturating at 65535.
-__device__ __forceinline__ uint16_t to_u16(float v) { return (uint16_t)min(__float2uint_rz(v), 65535u); }
+// Exact int <-> float conversions on the FMA pipe (the conversion pipe runs
+// at a quarter of its rate).  For 0 <= u < 2^23 the float with bits
+// 0x4B000000 | u is 2^23 + u, so subtracting 2^23 gives (float)u exactly.
+// For 0 <= v < 2^23, v + 2^23 rounded toward zero is 2^23 + floor(v): its low
+// 23 bits are floor(v), the truncating conversion of the reference's
+// float -> unsigned short stores (saturated at 65535 first).
+__device__ __forceinline__ float u2f(uint32_t u) { return __fsub_rn(__uint_as_float(0x4B000000u | u), 8388608.0f); }
+__device__ __forceinline__ uint32_t trunc_u16(float v) {
+    return __float_as_uint(__fadd_rz(fminf(v, 65535.0f), 8388608.0f)) - 0x4B000000u;
+}
+// trunc_u16 as a float (the value a uint16 intermediate image would hold)
+__device__ __forceinline__ float trunc_u16f(float v) { return __fsub_rn(__fadd_rz(fminf(v, 65535.0f), 8388608.0f), 8388608.0f); }
 
-// dst[r][c] = src pixel (clamp(gx0 + c), clamp(gy0 + r)) for a ROWS x COLS
-// tile.  Every load of a thread is issued before the first store, so the
-// loads of a thread overlap instead of each waiting out the memory latency.
+// dst[r * COLS + c] = (float) src pixel (clamp(gx0 + c), clamp(gy0 + r)) for a
+// ROWS x COLS tile.  Every load of a thread is issued before the first store,
+// so the loads of a thread overlap instead of each waiting out the latency.
 template <int ROWS, int COLS, int THREADS>
-__device__ __forceinline__ void load_tile_clamped(uint16_t (*dst)[COLS], const uint16_t *__restrict__ src, int W,
-                                                  int H, int gx0, int gy0) {
+__device__ __forceinline__ void load_tile_clamped_f(float *dst, const uint16_t *__restrict__ src, int W, int H, int gx0,
+                                                    int gy0) {
     constexpr int N = ROWS * COLS, PER = (N + THREADS - 1) / THREADS;
     uint16_t v[PER];
 #pragma unroll
@@ -100,10 +109,7 @@ __device__ __forceinline__ void load_tile_clamped(uint16_t (*dst)[COLS], const u
 #pragma unroll
     for (int j = 0; j < PER; ++j) {
         const int i = threadIdx.x + j * THREADS;
-        if (i < N) {
-            const int r = i / COLS, c = i - r * COLS;
-            dst[r][c] = v[j];
-        }
+        if (i < N) dst[i] = u2f(v[j]);
     }
 }
 
@@ -196,19 +202,19 @@ __global__ void __launch_bounds__(kBgThreads) background_kernel(const uint16_t *
         const int se_next = __shfl_down_sync(0xffffffffu, se, 1);
         const int sum_e = (g == 0 ? se : so_prev) + se + so;
         const int sum_o = se + so + (g == 15 ? so : se_next);
-        const float mean_e = __fdiv_rn(__fmul_rn(__int2float_rn(sum_e), 0.125f), 3.0f);
-        const float mean_o = __fdiv_rn(__fmul_rn(__int2float_rn(sum_o), 0.125f), 3.0f);
+        const float mean_e = __fdiv_rn(__fmul_rn(u2f((uint32_t)sum_e), 0.125f), 3.0f);
+        const float mean_o = __fdiv_rn(__fmul_rn(u2f((uint32_t)sum_o), 0.125f), 3.0f);
         const uint32_t cw = t[r + 4][q + 2];
-        const uint16_t ve = to_u16(fmaxf(__fsub_rn(__uint2float_rn(cw & 0xFFFFu), mean_e), 0.0f));
-        const uint16_t vo = to_u16(fmaxf(__fsub_rn(__uint2float_rn(cw >> 16), mean_o), 0.0f));
+        const uint32_t ve = trunc_u16(fmaxf(__fsub_rn(u2f(cw & 0xFFFFu), mean_e), 0.0f));
+        const uint32_t vo = trunc_u16(fmaxf(__fsub_rn(u2f(cw >> 16), mean_o), 0.0f));
         const int y = y0 + r;
         if (y < H) {
             uint16_t *out = bg + (size_t)y * W;
             if (store_wide && x + 1 < W) {
-                *reinterpret_cast<uint32_t *>(out + x) = (uint32_t)ve | ((uint32_t)vo << 16);
+                *reinterpret_cast<uint32_t *>(out + x) = ve | (vo << 16);
             } else {
-                if (x < W) out[x] = ve;
-                if (x + 1 < W) out[x + 1] = vo;
+                if (x < W) out[x] = (uint16_t)ve;
+                if (x + 1 < W) out[x + 1] = (uint16_t)vo;
             }
         }
         if (r + 1 < r1) {
@@ -277,39 +283,44 @@ __global__ void __launch_bounds__(kVarThreads) variance_kernel(const uint16_t *_
     }
 }
 
+// Smoothing and detection on float tiles holding integer values (every
+// intermediate image of the reference is uint16, so each pass ends with the
+// truncation to uint16, kept in float).
 template <bool SMOOTH>
 __global__ void __launch_bounds__(kDetThreads) detect_kernel(const uint16_t *__restrict__ bg, uint8_t *__restrict__ pos,
                                                              int *__restrict__ chunk_count, const float *__restrict__ var,
                                                              Taps taps, DetectPara dp) {
-    __shared__ uint16_t bgt[SMOOTH ? kDetTY + 6 : 1][kDetTX + 6];
-    __shared__ uint16_t ht[SMOOTH ? kDetTY + 6 : 1][kDetTX + 2];
-    __shared__ uint16_t sm[kDetTY + 2][kDetTX + 2];
+    constexpr int kIn = SMOOTH ? (kDetTY + 6) * (kDetTX + 6) : (kDetTY + 2) * (kDetTX + 2);
+    // background-removed tile, then (same storage) the smoothed tile
+    __shared__ float buf[kIn];
+    __shared__ float ht[SMOOTH ? (kDetTY + 6) * (kDetTX + 2) : 1];
     const int W = dp.W, Hb = dp.Hb;
     const int x0 = blockIdx.x * kDetTX, y0 = blockIdx.y * kDetTY;
+    float *sm = buf;  // sm[r * (kDetTX + 2) + c] is pixel (x0 - 1 + c, y0 - 1 + r)
     if (SMOOTH) {
-        // background-removed tile, halo 3, coordinates clamped like every
-        // read of the reference's filters
-        load_tile_clamped<kDetTY + 6, kDetTX + 6, kDetThreads>(bgt, bg, W, Hb, x0 - 3, y0 - 3);
+        // halo 3, coordinates clamped like every read of the reference's filters
+        load_tile_clamped_f<kDetTY + 6, kDetTX + 6, kDetThreads>(buf, bg, W, Hb, x0 - 3, y0 - 3);
         __syncthreads();
         // horizontal pass: ht[r][c] is column x0 - 1 + c of row clamp(y0 - 3 + r)
         for (int i = threadIdx.x; i < (kDetTY + 6) * (kDetTX + 2); i += kDetThreads) {
             const int r = i / (kDetTX + 2), c = i - r * (kDetTX + 2);
+            const float *row = buf + r * (kDetTX + 6) + c;
             float acc = 0.0f;
 #pragma unroll
-            for (int k = 0; k < 5; ++k) acc = __fmaf_rn(__uint2float_rn(bgt[r][c + k]), taps.t[k], acc);
-            ht[r][c] = to_u16(acc);
+            for (int k = 0; k < 5; ++k) acc = __fmaf_rn(row[k], taps.t[k], acc);
+            ht[i] = trunc_u16f(acc);
         }
         __syncthreads();
-        // vertical pass: sm[r][c] is pixel (x0 - 1 + c, y0 - 1 + r)
+        // vertical pass into buf
         for (int i = threadIdx.x; i < (kDetTY + 2) * (kDetTX + 2); i += kDetThreads) {
-            const int r = i / (kDetTX + 2), c = i - r * (kDetTX + 2);
+            const float *col = ht + i;
             float acc = 0.0f;
 #pragma unroll
-            for (int k = 0; k < 5; ++k) acc = __fmaf_rn(__uint2float_rn(ht[r + k][c]), taps.t[k], acc);
-            sm[r][c] = to_u16(acc);
+            for (int k = 0; k < 5; ++k) acc = __fmaf_rn(col[k * (kDetTX + 2)], taps.t[k], acc);
+            sm[i] = trunc_u16f(acc);
         }
     } else {
-        load_tile_clamped<kDetTY + 2, kDetTX + 2, kDetThreads>(sm, bg, W, Hb, x0 - 1, y0 - 1);
+        load_tile_clamped_f<kDetTY + 2, kDetTX + 2, kDetThreads>(buf, bg, W, Hb, x0 - 1, y0 - 1);
     }
     __syncthreads();
     const float sd = __fsqrt_rn(var[0]);
@@ -317,7 +328,7 @@ __global__ void __launch_bounds__(kDetThreads) detect_kernel(const uint16_t *__r
     const float th1 = __fmul_rn(dp.low_th ? 3.5f : 3.8f, sd);
     // one column per thread, rows r0, r0 + kRowStep, ...: the row inside the
     // frame advances without a division per pixel
-    constexpr int kRowStep = kDetThreads / kDetTX;
+    constexpr int kRowStep = kDetThreads / kDetTX, L = kDetTX + 2;
     const int c = threadIdx.x % kDetTX, r0 = threadIdx.x / kDetTX;
     const int x = x0 + c;
     const bool col_in = x >= dp.half && x < W - dp.half;
@@ -328,13 +339,14 @@ __global__ void __launch_bounds__(kDetThreads) detect_kernel(const uint16_t *__r
         if (x < W) {
             uint8_t flag = 0;
             if (col_in && ry >= dp.half && ry < dp.H0 - dp.half) {
-                const int C = sm[r + 1][c + 1];
-                if ((float)C >= th) {
-                    const int v00 = sm[r][c], v01 = sm[r][c + 1], v02 = sm[r][c + 2];
-                    const int v10 = sm[r + 1][c], v12 = sm[r + 1][c + 2];
-                    const int v20 = sm[r + 2][c], v21 = sm[r + 2][c + 1], v22 = sm[r + 2][c + 2];
-                    const int j1 = ((float)v00 > th1) + ((float)v01 > th1) + ((float)v02 > th1) + ((float)v10 > th1) +
-                                   ((float)v12 > th1) + ((float)v20 > th1) + ((float)v21 > th1) + ((float)v22 > th1);
+                const float *p = sm + r * L + c;
+                const float C = p[L + 1];
+                if (C >= th) {
+                    const float v00 = p[0], v01 = p[1], v02 = p[2];
+                    const float v10 = p[L], v12 = p[L + 2];
+                    const float v20 = p[2 * L], v21 = p[2 * L + 1], v22 = p[2 * L + 2];
+                    const int j1 = (v00 > th1) + (v01 > th1) + (v02 > th1) + (v10 > th1) + (v12 > th1) + (v20 > th1) +
+                                   (v21 > th1) + (v22 > th1);
                     const int ji = (C > v01) + (C >= v12) + (C >= v21) + (C > v10);
                     const int jo = (C > v00) + (C > v02) + (C > v20) + (C > v22);
                     if (j1 >= 7 && ji == 4 && jo >= 3) {
@@ -533,8 +545,33 @@ struct qcs_extract_data {
     int *h_state = nullptr;
     int h_copied = 0;
     cudaStream_t stream = nullptr, last = nullptr;
+    cudaEvent_t done = nullptr;  // recorded after the work of each call
     int first_frame = -1, end_frame = -1;
 };
+
+namespace {
+
+// Orders a call on stream s after the context's previous work (which may
+// have been issued on another stream).
+cudaError_t order_after_last(qcs_extract_data *c, cudaStream_t s) {
+    if (s == c->last) return cudaSuccess;
+    return cudaStreamWaitEvent(s, c->done, 0);
+}
+
+cudaError_t mark_done(qcs_extract_data *c, cudaStream_t s) {
+    c->last = s;
+    return cudaEventRecord(c->done, s);
+}
+
+// Brings the device state words into h_state (waits for the last call).
+int read_state(qcs_extract_data *c) {
+    QCS_CUDA(cudaMemcpyAsync(c->h_state, c->d_state, qcs::kStNum * sizeof(int), cudaMemcpyDeviceToHost, c->last),
+             "read extraction counters");
+    QCS_CUDA(cudaStreamSynchronize(c->last), "extraction");
+    return QCS_OK;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -562,6 +599,7 @@ int qcs_extract_deinit(qcs_extract_data *c) {
     cudaFreeHost(c->h_rois);
     cudaFreeHost(c->h_wle);
     cudaFreeHost(c->h_state);
+    if (c->done) cudaEventDestroy(c->done);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return QCS_OK;
@@ -610,6 +648,7 @@ int qcs_extract_init_ex(const qcs_loc_para *p, int max_batched_num, int capacity
     if (e == cudaSuccess) e = cudaMallocHost((void **)&c->h_wle, (size_t)capacity * QCS_WLE_PARA_NUM * sizeof(float));
     if (e == cudaSuccess) e = cudaMallocHost((void **)&c->h_state, qcs::kStNum * sizeof(int));
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaMemsetAsync(c->d_state, 0, qcs::kStNum * sizeof(int), c->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(c->d_var_acc, 0, 4 * sizeof(unsigned long long), c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
@@ -637,6 +676,7 @@ int qcs_extract_molecules(qcs_extract_data *c, const uint16_t *img, int image_so
     if (start_frame < 0) return fail(QCS_ERR_ARG, "negative start frame");
     if (p->LocType < QCS_LOCTYPE_GS2D || p->LocType > QCS_LOCTYPE_DH3D) return fail(QCS_ERR_ARG, "LocType out of range");
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+    QCS_CUDA(order_after_last(c, s), "order after the previous call");
     const uint16_t *raw = nullptr;
     if (image_source == QCS_IMAGE_SOURCE_CPU_PINNED || image_source == QCS_IMAGE_SOURCE_CPU_NORMAL) {
         QCS_CUDA(cudaMemcpyAsync(c->d_raw, img, (size_t)npx * sizeof(uint16_t), cudaMemcpyHostToDevice, s),
@@ -689,25 +729,24 @@ int qcs_extract_molecules(qcs_extract_data *c, const uint16_t *img, int image_so
     QCS_CUDA(qcs::launch_wle_presorted(c->d_rois, c->d_keys, c->d_state + qcs::kStBase, batch_max, c->R, p->LocType,
                                        c->d_wle, s),
              "WLE pre-pass");
-    QCS_CUDA(cudaMemcpyAsync(c->h_state, c->d_state, qcs::kStNum * sizeof(int), cudaMemcpyDeviceToHost, s),
-             "read extraction counters");
-    c->last = s;
+    QCS_CUDA(mark_done(c, s), "record completion");
     return QCS_OK;
 }
 
 int qcs_extract_accumulated_roi_num(qcs_extract_data *c, int *n) {
     if (!c || !n) return fail(QCS_ERR_ARG, "null argument");
-    QCS_CUDA(cudaStreamSynchronize(c->last), "extraction");
+    const int st = read_state(c);
+    if (st) return st;
     *n = c->h_state[qcs::kStAccum];
     return QCS_OK;
 }
 
-int qcs_extract_reset_roi_num(qcs_extract_data *c) {
+int qcs_extract_reset_roi_num(qcs_extract_data *c, void *stream) {
     if (!c) return fail(QCS_ERR_ARG, "null context");
-    QCS_CUDA(cudaStreamSynchronize(c->last), "extraction");
-    QCS_CUDA(cudaMemsetAsync(c->d_state, 0, qcs::kStNum * sizeof(int), c->last), "reset counters");
-    QCS_CUDA(cudaStreamSynchronize(c->last), "reset counters");
-    memset(c->h_state, 0, qcs::kStNum * sizeof(int));
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->last;
+    QCS_CUDA(order_after_last(c, s), "order after the previous call");
+    QCS_CUDA(cudaMemsetAsync(c->d_state, 0, qcs::kStNum * sizeof(int), s), "reset counters");
+    QCS_CUDA(mark_done(c, s), "record completion");
     c->h_copied = 0;
     c->first_frame = -1;
     c->end_frame = -1;
@@ -715,7 +754,8 @@ int qcs_extract_reset_roi_num(qcs_extract_data *c) {
 }
 
 static int copy_to_host(qcs_extract_data *c) {
-    QCS_CUDA(cudaStreamSynchronize(c->last), "extraction");
+    const int st = read_state(c);
+    if (st) return st;
     const int n = c->h_state[qcs::kStAccum];
     if (n > c->h_copied) {
         const size_t a = (size_t)c->h_copied, m = (size_t)(n - c->h_copied);
@@ -754,7 +794,8 @@ int qcs_extract_frame_range(const qcs_extract_data *c, int *first_frame, int *en
 
 int qcs_extract_dropped_num(qcs_extract_data *c, int *n) {
     if (!c || !n) return fail(QCS_ERR_ARG, "null argument");
-    QCS_CUDA(cudaStreamSynchronize(c->last), "extraction");
+    const int st = read_state(c);
+    if (st) return st;
     *n = c->h_state[qcs::kStDropped];
     return QCS_OK;
 }

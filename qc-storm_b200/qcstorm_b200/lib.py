@@ -23,11 +23,14 @@ _SIGS = {
     "qcs_loc_capacity": (C.c_int, [C.c_void_p]),
     "qcs_loc_bfgs_mle_localization": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(LocPara), C.c_int,
                                                 C.c_void_p]),
+    "qcs_loc_read_rows": (C.c_int, [C.c_void_p, C.POINTER(LocPara), C.c_void_p]),
     "qcs_loc_h_loc_arry": (C.c_void_p, [C.c_void_p]),
     "qcs_loc_valid_num": (C.c_int, [C.c_void_p]),
     "qcs_loc_fit_ratios": (C.c_int, [C.c_void_p, C.c_void_p]),
     "qcs_loc_localize_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(LocPara), C.c_int,
                                           C.c_void_p]),
+    "qcs_loc_localize_device_n": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(LocPara), C.c_void_p,
+                                            C.c_int, C.c_void_p]),
     "qcs_loc_device_rows": (C.c_void_p, [C.c_void_p]),
     "qcs_loc_device_valid_num": (C.c_void_p, [C.c_void_p]),
     "qcs_loc_device_roi_buffer": (C.c_void_p, [C.c_void_p]),
@@ -48,7 +51,7 @@ _SIGS = {
     "qcs_extract_molecules": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(LocPara), C.c_int, C.c_int,
                                         C.c_void_p]),
     "qcs_extract_accumulated_roi_num": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
-    "qcs_extract_reset_roi_num": (C.c_int, [C.c_void_p]),
+    "qcs_extract_reset_roi_num": (C.c_int, [C.c_void_p, C.c_void_p]),
     "qcs_extract_h_image_roi": (C.c_void_p, [C.c_void_p]),
     "qcs_extract_h_wle_para": (C.c_void_p, [C.c_void_p]),
     "qcs_extract_d_image_roi": (C.c_void_p, [C.c_void_p]),
@@ -144,6 +147,24 @@ class LocContext:
         check(self.lib.qcs_loc_localize_device(self.h, C.c_void_p(d_rois), C.c_void_p(d_wle) if d_wle else None,
                                                C.byref(para), int(n), C.c_void_p(stream) if stream else None))
 
+    def localize_device_n(self, d_rois, d_wle, d_n, max_n, stream=0, para=None):
+        """Localization of *d_n device records (count read on the device)."""
+        para = para or self.para
+        check(self.lib.qcs_loc_localize_device_n(self.h, C.c_void_p(d_rois), C.c_void_p(d_wle), C.byref(para),
+                                                 C.c_void_p(d_n), int(max_n), C.c_void_p(stream) if stream else None))
+
+    def read_rows(self, stream=0, para=None):
+        """Rows of the last device call, on the host: (rows[n_valid, 12], ratios[7])."""
+        para = para or self.para
+        check(self.lib.qcs_loc_read_rows(self.h, C.byref(para), C.c_void_p(stream) if stream else None))
+        nv = self.lib.qcs_loc_valid_num(self.h)
+        ptr = self.lib.qcs_loc_h_loc_arry(self.h)
+        rows = np.ctypeslib.as_array((C.c_float * (12 * nv)).from_address(ptr)).reshape(nv, 12).copy() if nv else \
+            np.zeros((0, 12), np.float32)
+        ratios = np.zeros(7, np.float32)
+        check(self.lib.qcs_loc_fit_ratios(self.h, C.c_void_p(ratios.ctypes.data)))
+        return rows, ratios
+
     def device_rows(self):
         return self.lib.qcs_loc_device_rows(self.h)
 
@@ -216,8 +237,8 @@ class ExtractContext:
         check(self.lib.qcs_extract_accumulated_roi_num(self.h, C.byref(n)))
         return n.value
 
-    def reset(self):
-        check(self.lib.qcs_extract_reset_roi_num(self.h))
+    def reset(self, stream=0):
+        check(self.lib.qcs_extract_reset_roi_num(self.h, C.c_void_p(stream) if stream else None))
 
     def records(self):
         """Host copies of the accumulated (records[n, R(R+1)] uint16, wle[n, 6] float32)."""

@@ -221,3 +221,30 @@ class _DeviceView:
     def __init__(self, ptr, shape, typestr):
         self.__cuda_array_interface__ = {"shape": shape, "typestr": typestr, "data": (int(ptr), False),
                                          "version": 2}
+
+
+def test_pipeline_device_count_no_host_sync(cuda_ok):
+    """Frames -> extraction -> localization with the record count read on the
+    device (qcs_loc_localize_device_n), several frames in a row on one stream
+    with asynchronous resets: each frame's rows (qcs_loc_read_rows) equal the
+    host-record entry point's rows on that frame's records."""
+    import torch
+    fr, para, _ = make(CASES[0])
+    ex = qlib.ExtractContext(para, max_batched_num=1)
+    loc = qlib.LocContext(para)
+    ref = qlib.LocContext(para)
+    s = torch.cuda.Stream()
+    d_rois, d_wle, d_n = ex.device_records()
+    for k in range(fr.shape[0]):
+        ex.reset(s.cuda_stream)
+        ex.extract(fr[k:k + 1], 40 + k, stream=s.cuda_stream)
+        loc.localize_device_n(d_rois, d_wle, d_n, loc.capacity, s.cuda_stream)
+        rows, ratios = loc.read_rows(s.cuda_stream)
+        rois, wle = ex.records()
+        assert rois.shape[0] > 0 and (rois[:, para.ROISize ** 2 + 2] == 40 + k).all()
+        rows_h, ratios_h = ref.localize(rois, wle)
+        assert np.array_equal(rows.view(np.uint32), rows_h.view(np.uint32))
+        assert np.array_equal(ratios, ratios_h)
+    loc.close()
+    ref.close()
+    ex.close()

@@ -52,7 +52,7 @@ def test_gpu_against_cpu_oracle(cuda_ok, gen, R):
 
 
 def test_full_size_subset_invariance_and_determinism(cuda_ok):
-    """Config-0 batch size (1e5) and a 1e6-record call: per-ROI results do not
+    """The 1e5-record batch of the 7x7 workload and a 1e6-record call: per-ROI results do not
     depend on what else is in the batch, and repeated calls are bit-equal."""
     n = 1_000_000
     rec, para, truth = synth.gs2d_rois(n, R=7, seed=62)
