@@ -3,9 +3,10 @@
 // 9x9 (2D) or 15x15 (astigmatic 3D) grid with the emitter at the centre, the
 // fitted total photons, background (+ read noise^2) and sigma x/y;
 // CRLB = PixelSize / sqrt(FI) in nm, 100 when the row is not fittable.
-// Re-expressed from LocPrecCalc_GaussianCRLB.h:65-243 with the same
-// expression shapes (bit-identical results); adds the bounds guard that the
-// reference kernel lacks (:65-128) and reads the row count from the device.
+// Re-expressed from LocPrecCalc_GaussianCRLB.h:65-243 with every rounding
+// step explicit (bit-identical results at 9 x 9); adds the bounds guard that
+// the reference kernel lacks (:65-128) and reads the row count from the
+// device.
 #include <cuda_runtime.h>
 
 #include "qcs_fit_math.cuh"
@@ -14,133 +15,141 @@
 namespace qcs {
 namespace {
 
-enum { kParaTPhn = 0, kParaBkgn = 1, kParaXPos = 2, kParaYPos = 3, kParaSigX = 4, kParaSigY = 5 };
-
-// Contraction of the PSF exponent x^2/(2 sx^2) + y^2/(2 sy^2) per grid size
-// (see SumMode in qcs_fit_math.cuh).
-// PEAK: peak * exp(.) + background; D2: f(+h) - 2 f(0) + f(-h);
-// FI: FI + (d2 - model * d2log).  0 = fused multiply-add, 1 = separately
-// rounded multiply and add, kCompiler = left to the compiler.
+// Contraction of the PSF exponent dx^2/(2 sx^2) + dy^2/(2 sy^2) at each of
+// the reference's evaluation sites, as nvcc compiles GaussianPSF_generate2D
+// inlined into them (found by comparing every combination against the
+// reference's CUDA build; see SumMode in qcs_fit_math.cuh): CENTRE = the
+// model and the base point of both derivatives (x0 = y0 = 0), SHIFT_X = the
+// +-dh points of the x derivative, SHIFT_Y = those of the y derivative.
+// PeakPn * exp(.) + background and d2 - model * d2log are fused
+// multiply-adds at every site.
 template <int G>
-struct CrlbSpec {
-    enum { MODE = kCompiler, PEAK = kCompiler, D2 = kCompiler, FI = kCompiler };
+struct CrlbSites;
+template <>
+struct CrlbSites<9> {
+    enum { CENTRE = kFuseSecond, SHIFT_X = kFuseFirst, SHIFT_Y = kFuseSecond };
+};
+template <>
+struct CrlbSites<15> {
+    enum { CENTRE = kFuseFirst, SHIFT_X = kFuseFirst, SHIFT_Y = kFuseSecond };
 };
 
-template <int S>
-__device__ __forceinline__ float mul_add(float a, float b, float c) {
-    if (S == 0) return __fmaf_rn(a, b, c);
-    if (S == 1) return __fadd_rn(__fmul_rn(a, b), c);
-    return a * b + c;
+struct PsfPara {
+    float peak, six, siy, bkg;
+};
+
+// Gaussian PSF value of the reference's model at offsets dx = CurX - x0,
+// dy = CurY - y0 (LocPrecCalc_GaussianCRLB.h:131-173).
+template <int MODE>
+__device__ __forceinline__ float psf_value(const PsfPara &p, float dx, float dy) {
+    const float e = __expf(-sum_of_products<MODE>(__fmul_rn(dx, dx), p.six, __fmul_rn(dy, dy), p.siy));
+    return __fmaf_rn(p.peak, e, p.bkg);
 }
 
-template <int G, int MODE = CrlbSpec<G>::MODE, int PEAK = CrlbSpec<G>::PEAK>
-__device__ __forceinline__ void psf_generate(float *pPSFDat, const float *ParaArry) {
-    enum { Half = G / 2 };
-    const float TotalPhoton_e = ParaArry[kParaTPhn];
-    const float Background_e = ParaArry[kParaBkgn];
-    const float x0 = ParaArry[kParaXPos];
-    const float y0 = ParaArry[kParaYPos];
-    const float PSFSigmaX = ParaArry[kParaSigX];
-    const float PSFSigmaY = ParaArry[kParaSigY];
-    const float pi = 3.141592654f;
-    const float PeakPn = 1 / (2 * pi * PSFSigmaX * PSFSigmaY) * TotalPhoton_e;
-    const float PSFSigma_ix = 1 / (2 * PSFSigmaX * PSFSigmaX);
-    const float PSFSigma_iy = 1 / (2 * PSFSigmaY * PSFSigmaY);
-    float CurX, CurY;
-    for (int ycnt = 0; ycnt < G; ycnt++) {
-        CurY = ycnt - Half;
-        for (int xcnt = 0; xcnt < G; xcnt++) {
-            CurX = xcnt - Half;
-            pPSFDat[ycnt * G + xcnt] =
-                mul_add<PEAK>(PeakPn,
-                              __expf(-sum_of_products<MODE>((CurX - x0) * (CurX - x0), PSFSigma_ix,
-                                                            (CurY - y0) * (CurY - y0), PSFSigma_iy)),
-                              Background_e);
-        }
-    }
-}
-
-template <int N>
-__device__ __forceinline__ void log_calc(const float *d, float *l) {
-#pragma unroll
-    for (int cnt = 0; cnt < N; cnt++) l[cnt] = logf(d[cnt]);
-}
-
-template <int N, int D2>
-__device__ __forceinline__ void deriv2(float *Deriv2, const float *dat_0, const float *dat_p, const float *dat_n,
-                                       float dh) {
-#pragma unroll
-    for (int cnt = 0; cnt < N; cnt++) {
-        if (D2 == kCompiler)
-            Deriv2[cnt] = (dat_p[cnt] - 2 * dat_0[cnt] + dat_n[cnt]) / dh / dh;
-        else
-            Deriv2[cnt] = __fadd_rn(mul_add<D2>(-2.0f, dat_0[cnt], dat_p[cnt]), dat_n[cnt]) / dh / dh;
-    }
-}
-
-template <int G, int N, int MODE, int PEAK, int D2>
-__device__ __forceinline__ void derivative2(float *d2, float *d2log, float *ParaArry, int ParaID) {
-    float t0[N], tl0[N], tp[N], tlp[N], tn[N], tln[N];
+// (f(+h) - 2 f(0) + f(-h)) / h / h with the reference's rounding
+// (LocPrecCalc_GaussianCRLB.h:188-196; 2 f(0) is exact, so fusing it changes nothing).
+__device__ __forceinline__ float second_diff(float fp, float f0, float fn) {
     const float dh = 0.02f;
-    psf_generate<G, MODE, PEAK>(t0, ParaArry);
-    log_calc<N>(t0, tl0);
-    ParaArry[ParaID] += dh;
-    psf_generate<G, MODE, PEAK>(tp, ParaArry);
-    log_calc<N>(tp, tlp);
-    ParaArry[ParaID] -= 2 * dh;
-    psf_generate<G, MODE, PEAK>(tn, ParaArry);
-    log_calc<N>(tn, tln);
-    ParaArry[ParaID] += dh;
-    deriv2<N, D2>(d2, t0, tp, tn, dh);
-    deriv2<N, D2>(d2log, tl0, tlp, tln, dh);
+    return __fdiv_rn(__fdiv_rn(__fadd_rn(__fmaf_rn(-2.0f, f0, fp), fn), dh), dh);
 }
 
-template <int N, int FI>
-__device__ __forceinline__ float crlb_std(const float *model, const float *d2, const float *d2log) {
-    float FishirInf = 0;
-    for (int cnt = 0; cnt < N; cnt++) {
-        if (FI == kCompiler)
-            FishirInf += (d2[cnt] - model[cnt] * d2log[cnt]);
-        else
-            FishirInf = __fadd_rn(FishirInf, mul_add<FI>(-model[cnt], d2log[cnt], d2[cnt]));
-    }
-    if (FishirInf == 0.0f) FishirInf = 1;
-    return sqrtf(1 / FishirInf);
-}
-
-template <int G, int MODE = CrlbSpec<G>::MODE, int PEAK = CrlbSpec<G>::PEAK, int D2 = CrlbSpec<G>::D2,
-          int FI = CrlbSpec<G>::FI>
-__global__ void crlb_kernel(float *__restrict__ loc, const int *__restrict__ n_dev, int n, float ReadNoise_e, float QE,
-                            float PixelSize) {
-    enum { N = G * G };
+// One thread per row.  The reference evaluates the PSF on the full grid
+// seven times per row (model, then base, +dh, -dh for each derivative) and
+// sums d2 - model * d2log over every pixel.  The same values come from far
+// fewer evaluations, exactly: the base points equal the model (same
+// parameters, same rounding), the model is symmetric in x and y, the -dh
+// evaluation is the +dh one mirrored (x - (-h) = -((-x) - h) exactly), and
+// each derivative's terms are symmetric across the other axis.  So the
+// model is evaluated on one quadrant, each +dh grid on half the rows
+// (columns), each term on half the grid, and the Fisher sums still add every
+// pixel's term in the reference's pixel order.  Per-thread tables live in
+// shared memory, [entry][thread].
+template <int G, int TPB>
+__global__ void __launch_bounds__(TPB) crlb_kernel(float *__restrict__ loc, const int *__restrict__ n_dev, int n,
+                                                   float ReadNoise_e, float QE, float PixelSize) {
+    enum { H = G / 2, Q = H + 1 };
+    using S = CrlbSites<G>;
+    __shared__ float sM[Q * Q][TPB], sLM[Q * Q][TPB], sTX[Q * G][TPB], sTY[G * Q][TPB];
     const int rows = n_dev ? *n_dev : n;
     const int gid = threadIdx.x + blockDim.x * blockIdx.x;
     if (gid >= rows) return;
+    const int t = threadIdx.x;
     float *r = loc + (size_t)gid * 12;
-    const float TotalPhoton_e = r[QCS_POS_TPHO] * QE;
-    float Background_e = r[QCS_POS_BAKG] * QE;
-    const float PSFSigmaX = r[QCS_POS_SIGX];
-    const float PSFSigmaY = r[QCS_POS_SIGY];
-    float ParaStdX = 100.0f;
-    float ParaStdY = 100.0f;
-    if ((TotalPhoton_e > 1) && (Background_e > 1) && (PSFSigmaX > 0.1) && (PSFSigmaY > 0.1) && (PSFSigmaX < 10) &&
-        (PSFSigmaY < 10)) {
-        float model[N], d2[N], d2log[N];
-        float ParaArry[6];
-        Background_e = (Background_e * QE + ReadNoise_e * ReadNoise_e) / QE;
-        ParaArry[kParaTPhn] = TotalPhoton_e;
-        ParaArry[kParaBkgn] = Background_e;
-        ParaArry[kParaXPos] = 0;
-        ParaArry[kParaYPos] = 0;
-        ParaArry[kParaSigX] = PSFSigmaX;
-        ParaArry[kParaSigY] = PSFSigmaY;
-        psf_generate<G, MODE, PEAK>(model, ParaArry);
-        derivative2<G, N, MODE, PEAK, D2>(d2, d2log, ParaArry, kParaXPos);
-        ParaStdX = crlb_std<N, FI>(model, d2, d2log);
-        derivative2<G, N, MODE, PEAK, D2>(d2, d2log, ParaArry, kParaYPos);
-        ParaStdY = crlb_std<N, FI>(model, d2, d2log);
-        ParaStdX = ParaStdX * PixelSize;
-        ParaStdY = ParaStdY * PixelSize;
+    const float TotalPhoton_e = __fmul_rn(r[QCS_POS_TPHO], QE);
+    float Background_e = __fmul_rn(r[QCS_POS_BAKG], QE);
+    const float sx = r[QCS_POS_SIGX], sy = r[QCS_POS_SIGY];
+    float ParaStdX = 100.0f, ParaStdY = 100.0f;
+    if ((TotalPhoton_e > 1) && (Background_e > 1) && (sx > 0.1) && (sy > 0.1) && (sx < 10) && (sy < 10)) {
+        // read noise counted into the background (LocPrecCalc_GaussianCRLB.h:89-92)
+        Background_e = __fdiv_rn(__fmaf_rn(ReadNoise_e, ReadNoise_e, __fmul_rn(Background_e, QE)), QE);
+        const float pi = 3.141592654f;
+        PsfPara p;
+        p.peak = __fmul_rn(__fdiv_rn(1.0f, __fmul_rn(__fmul_rn(__fmul_rn(2.0f, pi), sx), sy)), TotalPhoton_e);
+        p.six = __fdiv_rn(1.0f, __fmul_rn(__fmul_rn(2.0f, sx), sx));
+        p.siy = __fdiv_rn(1.0f, __fmul_rn(__fmul_rn(2.0f, sy), sy));
+        p.bkg = Background_e;
+        const float h = 0.02f;
+        // model on one quadrant: sM[a][b] at |CurY| = a, |CurX| = b
+#pragma unroll 1
+        for (int a = 0; a < Q; ++a)
+#pragma unroll
+            for (int b = 0; b < Q; ++b) {
+                const float v = psf_value<S::CENTRE>(p, (float)b, (float)a);
+                sM[a * Q + b][t] = v;
+                sLM[a * Q + b][t] = logf(v);
+            }
+        // x derivative: +dh row at |CurY| = a, terms for every column
+#pragma unroll 1
+        for (int a = 0; a < Q; ++a) {
+            float tp[G], lp[G];
+#pragma unroll
+            for (int x = 0; x < G; ++x) {
+                tp[x] = psf_value<S::SHIFT_X>(p, __fsub_rn((float)(x - H), h), (float)a);
+                lp[x] = logf(tp[x]);
+            }
+#pragma unroll
+            for (int x = 0; x < G; ++x) {
+                const int b = x < H ? H - x : x - H;
+                const float m = sM[a * Q + b][t];
+                const float d2 = second_diff(tp[x], m, tp[G - 1 - x]);
+                const float dl = second_diff(lp[x], sLM[a * Q + b][t], lp[G - 1 - x]);
+                sTX[a * G + x][t] = __fmaf_rn(-m, dl, d2);
+            }
+        }
+        // y derivative: +dh column at |CurX| = b, terms for every row
+#pragma unroll 1
+        for (int b = 0; b < Q; ++b) {
+            float tp[G], lp[G];
+#pragma unroll
+            for (int y = 0; y < G; ++y) {
+                tp[y] = psf_value<S::SHIFT_Y>(p, (float)b, __fsub_rn((float)(y - H), h));
+                lp[y] = logf(tp[y]);
+            }
+#pragma unroll
+            for (int y = 0; y < G; ++y) {
+                const int a = y < H ? H - y : y - H;
+                const float m = sM[a * Q + b][t];
+                const float d2 = second_diff(tp[y], m, tp[G - 1 - y]);
+                const float dl = second_diff(lp[y], sLM[a * Q + b][t], lp[G - 1 - y]);
+                sTY[y * Q + b][t] = __fmaf_rn(-m, dl, d2);
+            }
+        }
+        // Fisher information, pixel order (LocPrecCalc_GaussianCRLB.h:226-243)
+        float FX = 0, FY = 0;
+#pragma unroll 1
+        for (int y = 0; y < G; ++y) {
+            const int a = y < H ? H - y : y - H;
+#pragma unroll
+            for (int x = 0; x < G; ++x) {
+                const int b = x < H ? H - x : x - H;
+                FX = __fadd_rn(FX, sTX[a * G + x][t]);
+                FY = __fadd_rn(FY, sTY[y * Q + b][t]);
+            }
+        }
+        if (FX == 0.0f) FX = 1;
+        if (FY == 0.0f) FY = 1;
+        ParaStdX = __fmul_rn(__fsqrt_rn(__fdiv_rn(1.0f, FX)), PixelSize);
+        ParaStdY = __fmul_rn(__fsqrt_rn(__fdiv_rn(1.0f, FY)), PixelSize);
     }
     r[QCS_POS_CRBX] = ParaStdX;
     r[QCS_POS_CRBY] = ParaStdY;
@@ -150,13 +159,14 @@ __global__ void crlb_kernel(float *__restrict__ loc, const int *__restrict__ n_d
 
 cudaError_t launch_crlb(float *loc, const int *n_dev, int n, int max_rows, int loc_type, float ReadNoise_e, float QE,
                         float PixelSize, cudaStream_t s) {
-    const int tpb = 64;
-    const int grid = (max_rows + tpb - 1) / tpb;
-    if (grid == 0) return cudaSuccess;
-    if (loc_type != QCS_LOCTYPE_AS3D)
-        crlb_kernel<9><<<grid, tpb, 0, s>>>(loc, n_dev, n, ReadNoise_e, QE, PixelSize);
-    else
-        crlb_kernel<15><<<grid, tpb, 0, s>>>(loc, n_dev, n, ReadNoise_e, QE, PixelSize);
+    if (max_rows <= 0) return cudaSuccess;
+    if (loc_type != QCS_LOCTYPE_AS3D) {
+        constexpr int tpb = 64;
+        crlb_kernel<9, tpb><<<(max_rows + tpb - 1) / tpb, tpb, 0, s>>>(loc, n_dev, n, ReadNoise_e, QE, PixelSize);
+    } else {
+        constexpr int tpb = 32;
+        crlb_kernel<15, tpb><<<(max_rows + tpb - 1) / tpb, tpb, 0, s>>>(loc, n_dev, n, ReadNoise_e, QE, PixelSize);
+    }
     return cudaGetLastError();
 }
 
