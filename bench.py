@@ -47,6 +47,12 @@ BATCHES = 16
 R = 7
 PX_EVALS_PER_FIT = 176 * R * R  # reference schedule: 176 loss evaluations of R*R pixels
 MUFU_PER_PX_EVAL = 2            # exp of the model, log of the model (log of the data is invariant)
+# DRAM bytes (read + write) per fit of fit_single_kernel<7, GS2D>, from one ncu capture of
+# `bench.py --profile-fit 1200000` (profiles/fit_single_gs2d7_crlb9_1.2M_records.md:
+# 164.27 MB read + 39.28 MB written for 1.2 M fits); algorithmic: 112 B record + 24 B WLE row
+# read, 48 B row written.
+DRAM_BYTES_PER_FIT = (164.267776e6 + 39.283456e6) / 1.2e6
+ALGO_BYTES_PER_FIT = 112 + 24 + 48
 
 
 def env_int(k, d):
@@ -183,7 +189,7 @@ FRAMES_PER_CALL = 32   # frames whose ROIs accumulate before one localization ca
 MAX_POINT_NUM = 102400
 
 
-def frame_pipeline(stream, steps, warmup):
+def frame_pipeline(stream, steps, warmup, e2e=True):
     """Whole-frame pipeline: 2048 x 2048 uint16 frames -> ROI extraction
     (background, smoothing, detection, 7x7 cut, WLE; one frame per extraction
     batch, records accumulating on the device) -> after FRAMES_PER_CALL frames
@@ -231,7 +237,7 @@ def frame_pipeline(stream, steps, warmup):
     e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / steps
-    e2e_steps = max(3, steps // 4)
+    e2e_steps = max(3, steps // 4) if e2e else 1
     t0 = time.perf_counter()
     out_rows = 0
     for k in range(e2e_steps):
@@ -270,9 +276,18 @@ def profile_fit(n):
     out = torch.empty((n, 12), dtype=torch.float32, device="cuda")
     for _ in range(3):
         lib.fit_single_device(0, para, d.data_ptr(), w.data_ptr(), n, out.data_ptr(), sh)
+        lib.crlb_device(para, out.data_ptr(), n, sh)
     torch.cuda.synchronize()
     print(json.dumps({"profile_fit": n, "accepted": float((out[:, 0] > 0).float().mean())}))
     ctx.close()
+    return 0
+
+
+def profile_frames(calls, stream):
+    """`calls` localization calls of the whole-frame pipeline (for ncu captures)."""
+    r = frame_pipeline(stream, steps=calls, warmup=0, e2e=False)
+    print(json.dumps({"profile_frames": calls, "frames_per_call": FRAMES_PER_CALL,
+                      "records_per_call": r["records_per_call"]}))
     return 0
 
 
@@ -285,7 +300,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-frames", action="store_true", help="skip the whole-frame pipeline measurement")
     ap.add_argument("--profile-fit", type=int, default=0, metavar="N",
-                    help="only run the single-emitter fit kernel 3 times on N records (for ncu captures)")
+                    help="only run the single-emitter fit and CRLB kernels 3 times on N records (for ncu captures)")
+    ap.add_argument("--profile-frames", type=int, default=0, metavar="K",
+                    help="only run K calls of the whole-frame pipeline (for ncu captures)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -305,6 +322,8 @@ def main():
     torch.cuda.set_stream(stream)
     if args.profile_fit:
         return profile_fit(args.profile_fit)
+    if args.profile_frames:
+        return profile_frames(args.profile_frames, stream)
     dist = None
     if world > 1:
         import datetime
@@ -410,7 +429,10 @@ def main():
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config_dict(args),
             "e2e": e2e, "gpu_launches": launches_per_step * args.steps,
             "roofline": {"bound": "sfu", "kernel": "fit_single_kernel<7,GS2D>", "achieved": achieved,
-                         "peak": mufu_peak, "unit": "MUFU op/s", "frac": achieved / mufu_peak, "traffic": None,
+                         "peak": mufu_peak, "unit": "MUFU op/s", "frac": achieved / mufu_peak,
+                         "traffic": DRAM_BYTES_PER_FIT * N_PER_STEP,
+                         "traffic_algorithmic": ALGO_BYTES_PER_FIT * N_PER_STEP,
+                         "traffic_note": "DRAM bytes per launch from ncu on 1.2 M records, scaled to %d" % N_PER_STEP,
                          "kernel_ms": fit_ms,
                          "algorithmic": "%d px-evals x %d MUFU per fit; peak = measured __expf/__logf rate" % (
                              PX_EVALS_PER_FIT, MUFU_PER_PX_EVAL)},
