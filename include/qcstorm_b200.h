@@ -269,6 +269,29 @@ const int *qcs_loc_device_valid_num(const qcs_loc_data *c);
 uint16_t *qcs_loc_device_roi_buffer(qcs_loc_data *c);
 float *qcs_loc_device_wle_buffer(qcs_loc_data *c);
 
+/* ---- zero-row removal: ZeroLocalizationsRemovel_TypeDef ------------------ */
+/*
+ * Drops rejected rows (peak photons <= 1) and optionally orders the rest by
+ * frame (bfgsMLE_Loc_top/ZeroLocalizationsRemove.cu:21-186).  The reference
+ * launches one kernel per frame and appends through an atomic counter; here
+ * one stable sort orders rows by frame, row order within a frame.
+ */
+typedef struct qcs_zero_data qcs_zero_data;
+/* ZeroLocalizationsRemovel_TypeDef::Init (:104-122); capacity in rows (<= 0: 2 x QCS_MAX_POINT_NUM). */
+int qcs_zero_init(int capacity, qcs_zero_data **out);
+int qcs_zero_deinit(qcs_zero_data *c);
+/* RemoveZeroLocalizations(ih_LocArry, iFluoNum, SortFrameEn, FirstFrame, EndFrame, cstream) (:21-39):
+ * host rows in; kept rows in qcs_zero_h_loc_arry (h_LocArry), count in qcs_zero_valid_num (ValidFluoNum). */
+int qcs_zero_remove(qcs_zero_data *c, const float *h_rows, int n, int sort_frame_en, int first_frame, int end_frame,
+                    void *stream);
+const float *qcs_zero_h_loc_arry(const qcs_zero_data *c);
+int qcs_zero_valid_num(const qcs_zero_data *c);
+/* Device form, asynchronous: d_rows (n rows, or *d_n of them when d_n is set,
+ * e.g. qcs_loc_device_valid_num) -> d_out, kept count -> *d_nvalid (may be
+ * NULL).  Both row arrays 16-byte aligned.  No counterpart in the reference. */
+int qcs_zero_remove_device(qcs_zero_data *c, const float *d_rows, int n, const int *d_n, int sort_frame_en,
+                           int first_frame, int end_frame, float *d_out, int *d_nvalid, void *stream);
+
 /* ---- WLE pre-pass: WLEParameterEstimation_TypeDef ---------------------- */
 /* WLEParameterEstimation_TypeDef::WLEParameterEstimate (WLEParaEstimation.h:41,
  * WLEParaEstimation.cpp:20-40): PSF width, same-frame nearest neighbour and

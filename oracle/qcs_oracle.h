@@ -63,6 +63,10 @@ int qcso_extract(const qcs_loc_para *p, const uint16_t *frames, int n_frames, in
                  int start_frame, int flags, uint16_t *rois_out, float *wle_out, int cap,
                  int *n_roi, int *first_frame, int *end_frame);
 
+/* RemoveZeroLocalizations: rows n x 12 in, kept rows into out (n x 12), count in *n_out. */
+int qcso_zero_remove(const float *rows, int n, int sort_frame, int first_frame, int end_frame, float *out,
+                     int *n_out);
+
 #ifdef __cplusplus
 }
 #endif

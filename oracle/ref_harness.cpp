@@ -9,6 +9,7 @@
 //                      bfgsMLE_Single_Emitter_Fit.cu:96)
 //   qcsref_crlb        GaussianCRLB_Calc_top (LocPrecCalc_GaussianCRLB.h:65-128)
 //   qcsref_wle         WLEParameterEstimation_TypeDef::WLEParameterEstimate
+//   qcsref_zero_remove ZeroLocalizationsRemovel_TypeDef::RemoveZeroLocalizations
 //                      (WLEParaEstimation.cpp:20-40)
 //   qcsref_extract     LDROIExtractData_TypeDef::ExtractMolecules (LDROIExtraction.cu:30-80)
 #include <cstdio>
@@ -21,6 +22,7 @@
 #include "bfgsMLE_GS2D_core.h"
 #include "bfgsMLE_AS3D_core.h"
 #include "LocPrecCalc_GaussianCRLB.h"
+#include "ZeroLocalizationsRemove.h"
 
 #include "../include/qcstorm_b200.h"
 
@@ -224,6 +226,21 @@ int qcsref_extract(const qcs_loc_para *p, const unsigned short *frames, int n_fr
     *first_frame = ex.FirstFrame;
     *end_frame = ex.EndFrame;
     ex.Deinit();
+    return 0;
+}
+
+// RemoveZeroLocalizations over n rows (ZeroLocalizationsRemove.cu:21-39);
+// n must fit its MaxPointNum buffers.
+int qcsref_zero_remove(const float *rows, int n, int sort_frame, int first_frame, int end_frame, float *out,
+                       int *n_out) {
+    if (n < 0 || n > MaxPointNum) return -1;
+    ZeroLocalizationsRemovel_TypeDef z;
+    z.Init();
+    std::vector<float> in(rows, rows + (size_t)n * 12);
+    z.RemoveZeroLocalizations(in.data(), n, sort_frame, first_frame, end_frame, nullptr);
+    *n_out = z.ValidFluoNum;
+    memcpy(out, z.h_LocArry, sizeof(float) * 12 * (size_t)z.ValidFluoNum);
+    z.Deinit();
     return 0;
 }
 

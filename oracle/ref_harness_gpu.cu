@@ -11,6 +11,7 @@
 //   qcsrefg_crlb        LocPrecCalc_GaussianCRLB (LocPrecCalc_GaussianCRLB.cu:23-40)
 //   qcsrefg_wle         WLEParameterEstimation_TypeDef::WLEParameterEstimate
 //   qcsrefg_extract     LDROIExtractData_TypeDef::ExtractMolecules
+//   qcsrefg_zero_remove ZeroLocalizationsRemovel_TypeDef::RemoveZeroLocalizations
 // Every entry point returns 0, or the CUDA error code of the first failure.
 #include <cstdio>
 #include <cstring>
@@ -25,6 +26,7 @@
 #include "bfgsMLE_GS2D_3Emitter_core.h"
 #include "bfgsMLE_AS3D_2Emitter_core.h"
 #include "LocPrecCalc_GaussianCRLB.h"
+#include "ZeroLocalizationsRemove.h"
 
 #include "../include/qcstorm_b200.h"
 
@@ -357,6 +359,27 @@ int qcsrefg_extract(const qcs_loc_para *p, const unsigned short *frames, int n_f
     *end_frame = ex.EndFrame;
     cudaStreamDestroy(s);
     ex.Deinit();
+    return st;
+}
+
+int qcsrefg_zero_remove(const float *rows, int n, int sort_frame, int first_frame, int end_frame, float *out,
+                        int *n_out) {
+    if (n < 0 || n > MaxPointNum) return -1;
+    ZeroLocalizationsRemovel_TypeDef z;
+    z.Init();
+    float *pinned = nullptr;
+    cudaMallocHost((void **)&pinned, sizeof(float) * 12 * (size_t)(n > 0 ? n : 1));
+    memcpy(pinned, rows, sizeof(float) * 12 * (size_t)n);
+    cudaStream_t s;
+    cudaStreamCreate(&s);
+    z.RemoveZeroLocalizations(pinned, n, sort_frame, first_frame, end_frame, s);
+    cudaStreamSynchronize(s);
+    int st = check();
+    *n_out = z.ValidFluoNum;
+    memcpy(out, z.h_LocArry, sizeof(float) * 12 * (size_t)z.ValidFluoNum);
+    cudaStreamDestroy(s);
+    cudaFreeHost(pinned);
+    z.Deinit();
     return st;
 }
 

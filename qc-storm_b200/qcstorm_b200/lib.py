@@ -44,6 +44,13 @@ _SIGS = {
     "qcs_measure_mufu_rate": (C.c_int, [C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_double)]),
     "qcs_localize_noalloc": (C.c_int, [C.POINTER(LocPara), C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
                                        C.c_void_p]),
+    "qcs_zero_init": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
+    "qcs_zero_deinit": (C.c_int, [C.c_void_p]),
+    "qcs_zero_remove": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]),
+    "qcs_zero_h_loc_arry": (C.c_void_p, [C.c_void_p]),
+    "qcs_zero_valid_num": (C.c_int, [C.c_void_p]),
+    "qcs_zero_remove_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                         C.c_void_p, C.c_void_p, C.c_void_p]),
     "qcs_extract_max_batched_num": (C.c_int, [C.c_int, C.c_int]),
     "qcs_extract_init": (C.c_int, [C.POINTER(LocPara), C.POINTER(C.c_void_p)]),
     "qcs_extract_init_ex": (C.c_int, [C.POINTER(LocPara), C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
@@ -267,3 +274,42 @@ class ExtractContext:
         """(device address of the records, of the WLE rows, of the int count)."""
         return (self.lib.qcs_extract_d_image_roi(self.h), self.lib.qcs_extract_d_wle_para(self.h),
                 self.lib.qcs_extract_device_roi_num(self.h))
+
+
+class ZeroRemover:
+    """ZeroLocalizationsRemovel_TypeDef: drop rejected rows, optionally order by frame."""
+
+    def __init__(self, capacity=0):
+        self.lib = load()
+        h = C.c_void_p()
+        check(self.lib.qcs_zero_init(int(capacity), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.lib.qcs_zero_deinit(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def remove(self, rows, sort_frame=False, first_frame=0, end_frame=0, stream=0):
+        rows, pr = _host(rows, np.float32)
+        n = rows.shape[0]
+        check(self.lib.qcs_zero_remove(self.h, pr, n, int(bool(sort_frame)), int(first_frame), int(end_frame),
+                                       C.c_void_p(stream) if stream else None))
+        k = self.lib.qcs_zero_valid_num(self.h)
+        ptr = self.lib.qcs_zero_h_loc_arry(self.h)
+        if k == 0:
+            return np.zeros((0, 12), np.float32)
+        return np.ctypeslib.as_array((C.c_float * (12 * k)).from_address(ptr)).reshape(k, 12).copy()
+
+    def remove_device(self, d_rows, n, d_out, d_n=0, d_nvalid=0, sort_frame=False, first_frame=0, end_frame=0,
+                      stream=0):
+        check(self.lib.qcs_zero_remove_device(self.h, C.c_void_p(d_rows), int(n), C.c_void_p(d_n) if d_n else None,
+                                              int(bool(sort_frame)), int(first_frame), int(end_frame),
+                                              C.c_void_p(d_out), C.c_void_p(d_nvalid) if d_nvalid else None,
+                                              C.c_void_p(stream) if stream else None))

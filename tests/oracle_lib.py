@@ -152,3 +152,20 @@ def ref_gpu_crlb(para, loc):
     st = ref_gpu().qcsrefg_crlb(C.byref(para), _p(out), out.shape[0])
     assert st == 0, st
     return out
+
+
+def zero_remove(rows, sort_frame=0, first_frame=0, end_frame=0, lib="oracle"):
+    """RemoveZeroLocalizations through the oracle ("oracle"), the host build
+    ("ref") or the reference's CUDA build ("ref_gpu")."""
+    rows = np.ascontiguousarray(rows, np.float32)
+    out = np.zeros_like(rows)
+    n = C.c_int(0)
+    if lib == "oracle":
+        f = oracle().qcso_zero_remove
+    elif lib == "ref":
+        f = ref_host().qcsref_zero_remove
+    else:
+        f = ref_gpu().qcsrefg_zero_remove
+    st = f(_p(rows), rows.shape[0], int(sort_frame), int(first_frame), int(end_frame), _p(out), C.byref(n))
+    assert st == 0, st
+    return out[:n.value].copy()
