@@ -313,6 +313,58 @@ int qcs_fit_single_device(int loc_type, const qcs_loc_para *p, const uint16_t *d
  * LocPrecCalc_GaussianCRLB.cu:23-40): CRLB columns of n device rows. */
 int qcs_crlb_device(const qcs_loc_para *p, float *d_loc, int n, void *stream);
 
+/* ---- learned start points (no counterpart in the reference) ------------- */
+/*
+ * A small network (64 features -> 128 -> 128 -> 8, ReLU, BF16 tensor-core
+ * GEMMs with FP32 accumulation) predicts each GS2D 7x7 ROI's start point
+ * (x, y, sigma, peak photons, background) for the BFGS fit, trained on the
+ * GPU by these entry points on ROIs labelled by converged plain fits.
+ * Parameters: qcs_learned_param_count() floats (W1 64x128, b1, W2 128x128,
+ * b2, W3 128x8, b3, row-major [in][out]).
+ */
+typedef struct qcs_learned_net qcs_learned_net;
+int qcs_learned_param_count(void);
+/* batch: training batch size and inference chunk (<= 0: 4096); seed of the initial weights. */
+int qcs_learned_create(int batch, unsigned long long seed, qcs_learned_net **out);
+int qcs_learned_destroy(qcs_learned_net *net);
+int qcs_learned_get_params(qcs_learned_net *net, float *h_params);
+int qcs_learned_set_params(qcs_learned_net *net, const float *h_params);
+/* Features (n x 64) and per-record (min, range) of n GS2D 7x7 device records. */
+int qcs_learned_features_device(const qcs_loc_para *p, const uint16_t *d_rois, int n, float *d_feat, float *d_scale,
+                                void *stream);
+/* Training targets (n x 5) and validity (n) from plain-fit rows of the same records. */
+int qcs_learned_targets_device(const qcs_loc_para *p, const uint16_t *d_rois, const float *d_rows,
+                               const float *d_scale, int n, float *d_targets, float *d_valid, void *stream);
+/* Network outputs (n x 8) of n feature rows. */
+int qcs_learned_forward_device(qcs_learned_net *net, const float *d_feat, int n, float *d_out, void *stream);
+/* Loss and parameter gradient of one batch (n <= batch); gradients via qcs_learned_get_grads. */
+int qcs_learned_gradient_device(qcs_learned_net *net, const float *d_feat, const float *d_targets,
+                                const float *d_valid, int n, float *h_loss, void *stream);
+int qcs_learned_get_grads(qcs_learned_net *net, float *h_grads);
+/* Adam training over n rows for `epochs` epochs; h_epoch_loss (epochs floats, may be NULL). */
+int qcs_learned_train_device(qcs_learned_net *net, const float *d_feat, const float *d_targets, const float *d_valid,
+                             int n, int epochs, float lr, unsigned long long seed, float *h_epoch_loss, void *stream);
+/* Start points (n x 5: peak e-, x, y, sigma, background e-) of n device records;
+ * d_work holds qcs_learned_work_bytes(n) bytes. */
+int qcs_learned_start_device(qcs_learned_net *net, const qcs_loc_para *p, const uint16_t *d_rois, int n,
+                             float *d_start, float *d_work, void *stream);
+size_t qcs_learned_work_bytes(int n);
+/* GS2D 7x7 single-emitter fits from given start points d_start (n x 5: peak
+ * e-, x, y in ROI pixels, sigma, background e-) with `iters` BFGS iterations
+ * (2..5 or 8) and the plain fit's loss, line search and accept rules; fits
+ * that are not accepted or whose Poisson deviance exceeds dev_th (<= 0: 100)
+ * are refitted by the plain kernel; then CRLB.  Rows in the context (n). */
+int qcs_fit_from_start_device(qcs_loc_data *c, const uint16_t *d_rois, const float *d_wle, const qcs_loc_para *p,
+                              int n, const float *d_start, int iters, float dev_th, void *stream);
+/* GS2D 7x7 single-emitter localization from learned start points: `iters`
+ * BFGS iterations (2..5 or 8) instead of 8; fits that are not accepted or
+ * whose Poisson deviance exceeds dev_th (<= 0: 100) are refitted by the plain
+ * kernel; then CRLB.  Rows in the context like qcs_loc_localize_device (n rows). */
+int qcs_learned_localize_device(qcs_loc_data *c, qcs_learned_net *net, const uint16_t *d_rois, const float *d_wle,
+                                const qcs_loc_para *p, int n, int iters, float dev_th, void *stream);
+/* Number of plain refits of the last qcs_learned_localize_device call (waits for it). */
+int qcs_learned_refit_num(qcs_loc_data *c, int *n);
+
 /* ---- allocation-free localization --------------------------------------- */
 /*
  * No counterpart in the reference.  For callers that cannot allocate device

@@ -12,6 +12,7 @@
 #include "qcs_error.h"
 #include "qcs_fit_math.cuh"
 #include "qcs_kernels.h"
+#include "qcs_learned.h"
 
 namespace {
 
@@ -223,6 +224,85 @@ int qcs_loc_localize_device_n(qcs_loc_data *c, const uint16_t *d_rois, const flo
     a.max_rows = c->max_rows;
     a.stream = s;
     QCS_CUDA(qcs::run_cascade(a, c->st), "localization cascade");
+    return QCS_OK;
+}
+
+}  // extern "C"
+
+namespace {
+// rows for n records after a learned-start call; refits stay counted at
+// st.counters[kCntSingle]
+__global__ void learned_counters_kernel(qcs::CascadeState st, int n) {
+    st.counters[qcs::kCnt2E] = 0;
+    st.counters[qcs::kCnt2EClassify] = 0;
+    st.counters[qcs::kCnt3E] = 0;
+    st.counters[qcs::kCntRejected] = 0;
+    st.counters[qcs::kCntRows] = n;
+    st.counters[qcs::kCntValid] = n;
+}
+}  // namespace
+
+extern "C" {
+
+int qcs_fit_from_start_device(qcs_loc_data *c, const uint16_t *d_rois, const float *d_wle, const qcs_loc_para *p,
+                              int n, const float *d_start, int iters, float dev_th, void *stream) {
+    int st = check_call(c, p, n);
+    if (st) return st;
+    if (p->LocType != QCS_LOCTYPE_GS2D || p->ROISize != 7 || p->MultiEmitterFitEn)
+        return fail(QCS_ERR_ARG, "start-point fits: GS2D 7x7 single-emitter fitting only");
+    if (!(iters >= 2 && iters <= 5) && iters != 8) return fail(QCS_ERR_ARG, "iters must be 2..5 or 8");
+    if (n == 0) return QCS_OK;
+    if (!d_rois || !d_start) return fail(QCS_ERR_ARG, "null pointer");
+    if (!(dev_th > 0.0f)) dev_th = 100.0f;
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+    const float *wle = d_wle;
+    if (!wle) {
+        QCS_CUDA(qcs::launch_wle(d_rois, n, c->R, p->LocType, c->d_wle, c->d_wle_scratch, s), "WLE pre-pass");
+        wle = c->d_wle;
+    }
+    qcs::FitLaunch f;
+    f.rois = d_rois;
+    f.wle = wle;
+    f.q = qcs::Queue{nullptr, nullptr, n};
+    f.max_count = n;
+    f.loc = c->d_loc;
+    f.to2e = nullptr;
+    f.mo = qcs::MultiOut{nullptr, nullptr};
+    f.para = qcs::core_para(*p);
+    f.stream = s;
+    QCS_CUDA(qcs::launch_fit_learned(7, iters, f, d_start, dev_th, c->st.to2e, n), "start-point fit");
+    // plain refit of the flagged records
+    QCS_CUDA(qcs::launch_flag_queue(c->st.to2e, n, c->st.q_single, c->st.counters + qcs::kCntSingle, s),
+             "refit queue");
+    f.q = qcs::Queue{c->st.q_single, c->st.counters + qcs::kCntSingle, 0};
+    QCS_CUDA(qcs::launch_fit(qcs::kGS2D, 7, f), "plain refit");
+    learned_counters_kernel<<<1, 1, 0, s>>>(c->st, n);
+    QCS_CUDA(cudaGetLastError(), "counters");
+    QCS_CUDA(qcs::launch_crlb(c->d_loc, nullptr, n, n, p->LocType, p->ReadNoise_e, p->QE, p->PixelSize, s), "CRLB");
+    return QCS_OK;
+}
+
+int qcs_learned_localize_device(qcs_loc_data *c, qcs_learned_net *net, const uint16_t *d_rois, const float *d_wle,
+                                const qcs_loc_para *p, int n, int iters, float dev_th, void *stream) {
+    int st = check_call(c, p, n);
+    if (st) return st;
+    if (!net) return fail(QCS_ERR_ARG, "null network");
+    if (p->LocType != QCS_LOCTYPE_GS2D || p->ROISize != 7 || p->MultiEmitterFitEn)
+        return fail(QCS_ERR_ARG, "learned start points: GS2D 7x7 single-emitter fitting only");
+    if (n == 0) return QCS_OK;
+    if (!d_rois) return fail(QCS_ERR_ARG, "null ROI pointer");
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+    const float *start = nullptr;
+    QCS_CUDA(qcs::learned::start_points(net, p, d_rois, n, &start, s), "learned start points");
+    return qcs_fit_from_start_device(c, d_rois, d_wle, p, n, start, iters, dev_th, s);
+}
+
+int qcs_learned_refit_num(qcs_loc_data *c, int *n) {
+    if (!c || !n) return fail(QCS_ERR_ARG, "null argument");
+    QCS_CUDA(cudaDeviceSynchronize(), "localization");
+    QCS_CUDA(cudaMemcpy(c->h_counters, c->st.counters, qcs::kCntNum * sizeof(int), cudaMemcpyDeviceToHost),
+             "read counters");
+    *n = c->h_counters[qcs::kCntSingle];
     return QCS_OK;
 }
 

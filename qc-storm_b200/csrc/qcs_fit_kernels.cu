@@ -330,6 +330,132 @@ __global__ void __launch_bounds__(kTPB) fit_single_kernel(const uint16_t *__rest
     if (to2e) to2e[CurFluoID] = (!accepted && c.MultiEmitterFitEn && IsFittingValid && (CurSNR > 6.0f)) ? 1 : 0;
 }
 
+// ---------------------------------------------- learned-start GS2D fit ---
+// The GS2D fit of fit_single_kernel started from a given point (peak e-,
+// x, y in ROI pixels, sigma, background e-) instead of the centre / edge-mean
+// pre-estimate, with ITERS BFGS iterations instead of 8.  The same weighted
+// loss, line search, accept rules and output row.  refit[id] = 1 when the fit
+// is not accepted or when its unweighted Poisson deviance
+// 2 sum(mu - n - n ln(mu / n)) exceeds dev_th: those ROIs are refitted by the
+// plain kernel.
+template <int R, int ITERS, int DIST = ArithSpec<kGS2D, R>::DIST, int MASK = ArithSpec<kGS2D, R>::MASK>
+__global__ void __launch_bounds__(kTPB) fit_learned_kernel(const uint16_t *__restrict__ rois,
+                                                           const float *__restrict__ wle,
+                                                           const float *__restrict__ start, int n,
+                                                           float *__restrict__ loc, uint8_t *__restrict__ refit,
+                                                           CorePara c, float dev_th) {
+    typedef SmemLayout<R, kGS2D> L;
+    enum { P = 5, PIX = R * R, WHOLE = R * (R + 1), ROISize_Half = R / 2 };
+    extern __shared__ float smem[];
+    const Queue q{nullptr, nullptr, n};
+    const int base = blockIdx.x * kTPB;
+    if (base >= n) return;
+    const int cnt = min(kTPB, n - base);
+    float2 *s_img = reinterpret_cast<float2 *>(smem + L::IMG);
+    stage_rois<R>(s_img, rois, q, base, cnt, c.Offset, c.KAdc);
+    __syncthreads();
+    const int tid = threadIdx.x;
+    if (tid >= cnt) return;
+    const int id = base + tid;
+    float *w = smem + L::W + tid;
+    float *D = smem + L::D + tid;
+    const uint16_t *hdr = rois + (size_t)id * WHOLE + PIX;
+    const int XOffset = hdr[0], YOffset = hdr[1];
+    const int CurFrame = hdr[2] + 65536 * hdr[3];
+    const float *pw = wle + (size_t)id * QCS_WLE_PARA_NUM;
+    const RoiRef roi{s_img + tid, w, kTPB};
+
+    const float XYLBound = R / 2.0f - 1.5f;
+    const float XYUBound = R / 2.0f + 1.5f;
+    const float Simga_Max_Th = R / 1.5f / 2.35f;
+    float SigmaL = pw[1], SigmaR = pw[2], SigmaU = pw[3], SigmaD = pw[4];
+    const int MoleculeType = pw[5];
+    SigmaL = fminf(SigmaL, SigmaR);
+    SigmaU = fminf(SigmaU, SigmaD);
+    float WLE_SigmaX = fminf(fminf(SigmaL, SigmaU), R / 2.0f / 2.35f);
+    if (MoleculeType != QCS_MOLECULE_MLEFIT) WLE_SigmaX = fminf(WLE_SigmaX / 1.2f, R / 2.0f / 2.35f);
+    if (c.WLEEn == 0 && MoleculeType != QCS_MOLECULE_MULTIFIT) WLE_SigmaX = R;
+    wle_weights<R, MASK>(w, kTPB, WLE_SigmaX, WLE_SigmaX, MoleculeType);
+
+    const float *st = start + (size_t)id * 5;
+    float Ininf[P];
+    Ininf[0] = st[0] * rAScalFactor;
+    Ininf[1] = st[1];
+    Ininf[2] = st[2];
+    Ininf[3] = (0.5f / (st[3] * st[3])) * rSScalFactor;
+    Ininf[4] = st[4] * rBScalFactor;
+    mle_fit<R, kGS2D, DIST, ArithSpec<kGS2D, R>::SUM2, ITERS>(roi, Ininf, D, kTPB);
+
+    const float PeakPhoton = Ininf[0] * QCS_ASCALE / c.QE;
+    const float Background = Ininf[4] * QCS_BSCALE / c.QE;
+    float FittedXPos = Ininf[1], FittedYPos = Ininf[2];
+    float SimgaX = sqrtf(0.5f / (Ininf[3] * QCS_SSCALE));
+    FittedXPos = isnan(FittedXPos) ? -1 : FittedXPos;
+    FittedYPos = isnan(FittedYPos) ? -1 : FittedYPos;
+    SimgaX = isnan(SimgaX) ? -1 : SimgaX;
+    const float CurSNR = sqrtf(c.QE) * PeakPhoton / sqrtf(PeakPhoton + Background);
+    const bool valid = !isnan(Background);
+    const bool accepted = valid && (CurSNR > 4.0f) && (SimgaX <= Simga_Max_Th) && (SimgaX >= 0.6f) &&
+                          (FittedXPos > XYLBound) && (FittedXPos < XYUBound) && (FittedYPos > XYLBound) &&
+                          (FittedYPos < XYUBound);
+    // goodness of fit at the final point (unweighted Poisson deviance)
+    float dev = 0.0f;
+#pragma unroll 1
+    for (int r = 0; r < R; r++)
+        for (int col = 0; col < R; col++) {
+            const float2 pl = roi.img[(r * R + col) * roi.ld];
+            const float e = single_expo<kGS2D, DIST>(col + 0.5f, r + 0.5f, Ininf);
+            dev += single_term<kGS2D>(e, Ininf, pl.x, pl.y);
+        }
+    dev *= 2.0f;
+    refit[id] = (!accepted || !(dev <= dev_th)) ? 1 : 0;
+    if (accepted) {
+        float row[12];
+        row[0] = PeakPhoton;
+        row[1] = FittedXPos - ROISize_Half + XOffset;
+        row[2] = FittedYPos - ROISize_Half + YOffset;
+        row[3] = 0.0f;
+        row[4] = SimgaX;
+        row[5] = SimgaX;
+        row[6] = PeakPhoton * 2 * 3.141593f * SimgaX * SimgaX;
+        row[7] = Background;
+        row[8] = CurSNR;
+        row[9] = 0.0f;
+        row[10] = 0.0f;
+        row[11] = CurFrame;
+        store_row(loc, id, row);
+    } else {
+        zero_row(loc, id);
+    }
+}
+
+// Ids of the records with a nonzero flag (in no particular order: every
+// record is fitted on its own, so the order changes no result) and their
+// count; *count must be zero on entry.
+__global__ void flag_queue_kernel(const uint8_t *__restrict__ flags, int n, int *__restrict__ ids,
+                                  int *__restrict__ count) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int f = (i < n) ? (flags[i] != 0) : 0;
+    const unsigned ballot = __ballot_sync(0xffffffffu, f);
+    int base = 0;
+    if (lane == 0 && ballot) base = atomicAdd(count, __popc(ballot));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (f) ids[base + __popc(ballot & ((1u << lane) - 1u))] = i;
+}
+
+template <int R, int ITERS>
+cudaError_t launch_learned(const FitLaunch &a, const float *start, float dev_th, uint8_t *refit, int n) {
+    const size_t smem = SmemLayout<R, kGS2D>::TOTAL * sizeof(float);
+    auto k = fit_learned_kernel<R, ITERS>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const int grid = (n + kTPB - 1) / kTPB;
+    if (grid == 0) return cudaSuccess;
+    k<<<grid, kTPB, smem, a.stream>>>(a.rois, a.wle, start, n, a.loc, refit, a.para, dev_th);
+    return cudaGetLastError();
+}
+
 // -------------------------------------------------------- multi emitter ---
 template <int R, int KIND, int DIST = ArithSpec<KIND, R>::DIST, int MASK = ArithSpec<KIND, R>::MASK,
           int SUM2 = ArithSpec<KIND, R>::SUM2>
@@ -589,6 +715,26 @@ cudaError_t launch_multi(const FitLaunch &a) {
 }
 
 }  // namespace
+
+cudaError_t launch_fit_learned(int R, int iters, const FitLaunch &a, const float *start, float dev_th,
+                               uint8_t *refit, int n) {
+    if (R != 7) return cudaErrorInvalidValue;
+    switch (iters) {
+    case 2: return launch_learned<7, 2>(a, start, dev_th, refit, n);
+    case 3: return launch_learned<7, 3>(a, start, dev_th, refit, n);
+    case 4: return launch_learned<7, 4>(a, start, dev_th, refit, n);
+    case 5: return launch_learned<7, 5>(a, start, dev_th, refit, n);
+    case 8: return launch_learned<7, 8>(a, start, dev_th, refit, n);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_flag_queue(const uint8_t *flags, int n, int *ids, int *count, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(count, 0, sizeof(int), s);
+    if (e != cudaSuccess || n <= 0) return e;
+    flag_queue_kernel<<<(n + 255) / 256, 256, 0, s>>>(flags, n, ids, count);
+    return cudaGetLastError();
+}
 
 // ROI sizes: odd 5..17 for single emitter, 5..13 for multi emitter (the
 // reference's shared-memory limit, bfgsMLE_Multi_Emitter_Fit.cu:62-70).

@@ -330,9 +330,10 @@ __device__ __forceinline__ void gradient(const RoiRef &roi, const float *Ininf, 
 
 // Fixed schedule: IT quasi-Newton iterations, each with an 11-step bisection
 // of the step length in [1e-5, 1]; no convergence test.  D: P x P scratch.
-template <int R, int KIND, int DIST = ArithSpec<KIND, R>::DIST, int SUM2 = ArithSpec<KIND, R>::SUM2>
+template <int R, int KIND, int DIST = ArithSpec<KIND, R>::DIST, int SUM2 = ArithSpec<KIND, R>::SUM2,
+          int ITERS = KindTraits<KIND>::IT>
 __device__ __forceinline__ void mle_fit(const RoiRef &roi, float *Ininf, float *D, int ld) {
-    enum { P = KindTraits<KIND>::P, IT = KindTraits<KIND>::IT };
+    enum { P = KindTraits<KIND>::P, IT = ITERS };
     float grad[P], d0[P], td0[P], sk[P], yk[P], tgrad[P];
     float ddat[2], dpos[2];  // two-element arrays indexed by constants only
 #pragma unroll

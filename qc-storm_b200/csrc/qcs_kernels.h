@@ -24,6 +24,14 @@ struct FitLaunch {
 // kind: FitKind (qcs_fit_math.cuh); R: ROI size.
 cudaError_t launch_fit(int kind, int R, const FitLaunch &a);
 
+// GS2D fit of a.rois[0, n) started from start[5 * i] (peak e-, x, y, sigma,
+// background e-) with `iters` BFGS iterations (2..5 or 8, R = 7); rows into
+// a.loc, refit[i] = 1 for fits to redo with the plain kernel.
+cudaError_t launch_fit_learned(int R, int iters, const FitLaunch &a, const float *start, float dev_th,
+                               uint8_t *refit, int n);
+// ids[] = the indices i < n with flags[i] != 0 (any order), *count = their number.
+cudaError_t launch_flag_queue(const uint8_t *flags, int n, int *ids, int *count, cudaStream_t s);
+
 // CRLB columns 9/10 of rows [0, *n_dev) (or [0, n) when n_dev is null);
 // grid sized for max_rows.  LocPrecCalc_GaussianCRLB.h:65-243.
 cudaError_t launch_crlb(float *loc, const int *n_dev, int n, int max_rows, int loc_type, float ReadNoise_e, float QE,

@@ -1,0 +1,615 @@
+// Learned start points for the GS2D 7x7 fit: a small network predicts each
+// ROI's (x, y, sigma, peak photons, background) from its pixels, so that the
+// BFGS fit can start near the optimum and run fewer iterations.  No
+// counterpart in the reference (it starts from the centre / edge-mean
+// pre-estimate, bfgsMLE_GS2D_core.h:522-575).
+//
+// Network (per ROI): 64 features -> 128 (ReLU) -> 128 (ReLU) -> 8 outputs
+// (5 used: dx, dy, sigma - 1.3, log(peak / range), (background - min) / range).
+// Features: the 49 photoelectron pixels max((adu - offset) * gain, 1) scaled
+// to [0, 1] by the ROI's min and range, log(range) / 8, log(min) / 8, zeros.
+// Training and inference GEMMs run on the tensor cores in BF16 with FP32
+// accumulation (mma.sync m16n8k16); master weights and Adam moments are FP32.
+// Labels are the converged plain MLEbfgs fits of the same ROIs.
+#include <cstdint>
+#include <cstring>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "../../include/qcstorm_b200.h"
+#include "qcs_error.h"
+#include "qcs_learned.h"
+
+namespace qcs {
+namespace learned {
+
+constexpr int kGemmThreads = 128;  // 4 warps, 64 x 64 block tile, k step 16
+constexpr int kTile = 64;
+
+// ---------------------------------------------------------------- features
+__global__ void features_kernel(const uint16_t *__restrict__ rois, int n, float offset, float kadc,
+                                float *__restrict__ feat, float *__restrict__ scale) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint16_t *r = rois + (size_t)i * kWhole;
+    float e[kPix];
+    float lo = 1e30f, hi = -1e30f;
+#pragma unroll
+    for (int k = 0; k < kPix; ++k) {
+        e[k] = fmaxf(((float)r[k] - offset) * kadc, 1.0f);
+        lo = fminf(lo, e[k]);
+        hi = fmaxf(hi, e[k]);
+    }
+    const float rng = fmaxf(hi - lo, 1.0f);
+    const float inv = 1.0f / rng;
+    float *f = feat + (size_t)i * kIn;
+#pragma unroll
+    for (int k = 0; k < kPix; ++k) f[k] = (e[k] - lo) * inv;
+    f[kPix] = logf(rng) * 0.125f;
+    f[kPix + 1] = logf(lo) * 0.125f;
+#pragma unroll
+    for (int k = kPix + 2; k < kIn; ++k) f[k] = 0.0f;
+    scale[2 * i] = lo;
+    scale[2 * i + 1] = rng;
+}
+
+// Targets from the plain fit rows (12 floats per record, record order);
+// valid[i] = 1 for accepted fits.
+__global__ void targets_kernel(const uint16_t *__restrict__ rois, const float *__restrict__ rows,
+                               const float *__restrict__ scale, int n, float qe, float *__restrict__ tgt,
+                               float *__restrict__ valid) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float *row = rows + (size_t)i * 12;
+    const uint16_t *h = rois + (size_t)i * kWhole + kPix;
+    const float lo = scale[2 * i], rng = scale[2 * i + 1];
+    const bool ok = row[QCS_POS_PPHO] > 0.0f && row[QCS_POS_SIGX] > 0.0f;
+    float *t = tgt + (size_t)i * kOutUsed;
+    if (ok) {
+        // ROI coordinates of the fitted centre (inverse of the row's x = fit - R/2 + header x)
+        t[0] = row[QCS_POS_XPOS] + (float)kHalf - (float)h[0] - kCentre;
+        t[1] = row[QCS_POS_YPOS] + (float)kHalf - (float)h[1] - kCentre;
+        t[2] = row[QCS_POS_SIGX] - kSigma0;
+        t[3] = logf(fmaxf(row[QCS_POS_PPHO] * qe, 1e-3f) / rng);
+        t[4] = (row[QCS_POS_BAKG] * qe - lo) / rng;
+    } else {
+#pragma unroll
+        for (int j = 0; j < kOutUsed; ++j) t[j] = 0.0f;
+    }
+    valid[i] = ok ? 1.0f : 0.0f;
+}
+
+// ------------------------------------------------------------------- GEMM
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t *>(&v);
+}
+
+// C(m, n) = beta * C(m, n) + sum_k A(m, k) B(k, n), M x N x K, with
+// A(m, k) = A[m * sam + k * sak], B(k, n) = B[k * sbk + n * sbn] (FP32 in
+// memory, rounded to BF16 for the tensor cores), C row-major with ldc.
+// mma.sync.m16n8k16 fragment layouts (PTX ISA, bf16): lane = 4 g + t;
+// A: {(g, 2t..2t+1), (g+8, 2t..), (g, 2t+8..), (g+8, 2t+8..)};
+// B: {(k = 2t..2t+1, n = g), (k = 2t+8..2t+9, n = g)};
+// C: {(g, 2t..2t+1), (g+8, 2t..2t+1)}.
+__global__ void __launch_bounds__(kGemmThreads) gemm_bf16_kernel(int M, int N, int K, const float *__restrict__ A,
+                                                                 int sam, int sak, const float *__restrict__ B,
+                                                                 int sbk, int sbn, float *__restrict__ Cm, int ldc,
+                                                                 float beta) {
+    __shared__ __nv_bfloat16 As[kTile][16 + 8];
+    __shared__ __nv_bfloat16 Bs[16][kTile + 8];
+    const int m0 = blockIdx.y * kTile, n0 = blockIdx.x * kTile;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, t = lane & 3;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    float acc[2][4][4];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.0f;
+    for (int k0 = 0; k0 < K; k0 += 16) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int idx = threadIdx.x + j * kGemmThreads;  // 0..1023
+            const int r = idx >> 4, c = idx & 15;             // A tile 64 x 16
+            const int gm = m0 + r, gk = k0 + c;
+            As[r][c] = __float2bfloat16_rn((gm < M && gk < K) ? A[(size_t)gm * sam + (size_t)gk * sak] : 0.0f);
+            const int kr = idx >> 6, nc = idx & 63;           // B tile 16 x 64
+            const int bk = k0 + kr, bn = n0 + nc;
+            Bs[kr][nc] = __float2bfloat16_rn((bk < K && bn < N) ? B[(size_t)bk * sbk + (size_t)bn * sbn] : 0.0f);
+        }
+        __syncthreads();
+        uint32_t af[2][4], bfr[4][2];
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi) {
+            const int r = wm + mi * 16 + g;
+            af[mi][0] = *reinterpret_cast<const uint32_t *>(&As[r][2 * t]);
+            af[mi][1] = *reinterpret_cast<const uint32_t *>(&As[r + 8][2 * t]);
+            af[mi][2] = *reinterpret_cast<const uint32_t *>(&As[r][2 * t + 8]);
+            af[mi][3] = *reinterpret_cast<const uint32_t *>(&As[r + 8][2 * t + 8]);
+        }
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) {
+            const int c = wn + ni * 8 + g;
+            const __nv_bfloat162 b01 = __halves2bfloat162(Bs[2 * t][c], Bs[2 * t + 1][c]);
+            const __nv_bfloat162 b23 = __halves2bfloat162(Bs[2 * t + 8][c], Bs[2 * t + 9][c]);
+            bfr[ni][0] = *reinterpret_cast<const uint32_t *>(&b01);
+            bfr[ni][1] = *reinterpret_cast<const uint32_t *>(&b23);
+        }
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+                asm volatile(
+                    "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
+                    "{%8, %9}, {%0, %1, %2, %3};\n"
+                    : "+f"(acc[mi][ni][0]), "+f"(acc[mi][ni][1]), "+f"(acc[mi][ni][2]), "+f"(acc[mi][ni][3])
+                    : "r"(af[mi][0]), "r"(af[mi][1]), "r"(af[mi][2]), "r"(af[mi][3]), "r"(bfr[ni][0]),
+                      "r"(bfr[ni][1]));
+        __syncthreads();
+    }
+#pragma unroll
+    for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int r = m0 + wm + mi * 16 + g + h * 8;
+                const int c = n0 + wn + ni * 8 + 2 * t;
+                if (r >= M) continue;
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    if (c + q >= N) continue;
+                    float *dst = Cm + (size_t)r * ldc + c + q;
+                    const float v = acc[mi][ni][2 * h + q];
+                    *dst = (beta == 0.0f) ? v : beta * (*dst) + v;
+                }
+            }
+}
+
+cudaError_t gemm(int M, int N, int K, const float *A, int sam, int sak, const float *B, int sbk, int sbn, float *C,
+                 int ldc, float beta, cudaStream_t s) {
+    dim3 grid((N + kTile - 1) / kTile, (M + kTile - 1) / kTile);
+    gemm_bf16_kernel<<<grid, kGemmThreads, 0, s>>>(M, N, K, A, sam, sak, B, sbk, sbn, C, ldc, beta);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------ elementwise layers
+// Z (rows x cols) += bias; A = relu(Z) (A may alias Z when the caller does not need Z).
+__global__ void bias_relu_kernel(float *__restrict__ Z, const float *__restrict__ bias, int rows, int cols,
+                                 float *__restrict__ A, int relu) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)rows * cols) return;
+    const float z = Z[i] + bias[i % cols];
+    Z[i] = z;
+    A[i] = relu ? fmaxf(z, 0.0f) : z;
+}
+
+// dZ = dA * (Z > 0)
+__global__ void relu_back_kernel(float *__restrict__ dA, const float *__restrict__ Z, long long total) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    if (!(Z[i] > 0.0f)) dA[i] = 0.0f;
+}
+
+// Column sums of dZ (rows x cols) into g (bias gradient), one block per column group.
+__global__ void colsum_kernel(const float *__restrict__ dZ, int rows, int cols, float *__restrict__ g) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= cols) return;
+    float s = 0.0f;
+    for (int r = 0; r < rows; ++r) s += dZ[(size_t)r * cols + c];
+    g[c] = s;
+}
+
+// Masked weighted MSE on the first kOutUsed outputs: loss and dY.
+__global__ void mse_kernel(const float *__restrict__ Y, const float *__restrict__ T, const float *__restrict__ valid,
+                           int rows, float inv_count, float *__restrict__ dY, float *__restrict__ loss) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= rows) return;
+    const float v = valid[i];
+    float l = 0.0f;
+#pragma unroll
+    for (int j = 0; j < kOut; ++j) {
+        float d = 0.0f;
+        if (j < kOutUsed) {
+            const float e = Y[(size_t)i * kOut + j] - T[(size_t)i * kOutUsed + j];
+            d = 2.0f * kTargetWeight[j] * e * v * inv_count;
+            l += kTargetWeight[j] * e * e * v;
+        }
+        dY[(size_t)i * kOut + j] = d;
+    }
+    atomicAdd(loss, l * inv_count);
+}
+
+__global__ void adam_kernel(float *__restrict__ w, const float *__restrict__ g, float *__restrict__ m,
+                            float *__restrict__ v, int n, float lr, float b1, float b2, float c1, float c2, float eps) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.0f - b1) * gi;
+    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    w[i] -= lr * (mi * c1) / (sqrtf(vi * c2) + eps);
+}
+
+__global__ void gather_rows_kernel(const float *__restrict__ src, const int *__restrict__ idx, int rows, int cols,
+                                   float *__restrict__ dst) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)rows * cols) return;
+    const int r = (int)(i / cols), c = (int)(i - (long long)r * cols);
+    dst[i] = src[(size_t)idx[r] * cols + c];
+}
+
+// Predictions -> fit start (photoelectron peak, ROI x, y, sigma, background).
+__global__ void start_kernel(const float *__restrict__ Y, const float *__restrict__ scale, int n,
+                             float *__restrict__ start) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float *y = Y + (size_t)i * kOut;
+    const float lo = scale[2 * i], rng = scale[2 * i + 1];
+    float *s = start + (size_t)i * kStart;
+    s[0] = rng * expf(fminf(fmaxf(y[3], -6.0f), 3.0f));
+    s[1] = kCentre + fminf(fmaxf(y[0], -1.5f), 1.5f);
+    s[2] = kCentre + fminf(fmaxf(y[1], -1.5f), 1.5f);
+    s[3] = fminf(fmaxf(kSigma0 + y[2], 0.6f), 3.0f);
+    s[4] = fmaxf(lo + rng * y[4], 1.0f);
+}
+
+}  // namespace learned
+}  // namespace qcs
+
+using qcs::fail;
+namespace L = qcs::learned;
+
+struct qcs_learned_net {
+    // parameters (FP32 master copies), their gradients and Adam moments, in one block
+    float *d_par = nullptr, *d_grad = nullptr, *d_m = nullptr, *d_v = nullptr;
+    // activations of one batch
+    float *d_x = nullptr, *d_z1 = nullptr, *d_a1 = nullptr, *d_z2 = nullptr, *d_a2 = nullptr, *d_y = nullptr;
+    float *d_t = nullptr, *d_valid = nullptr, *d_dy = nullptr, *d_d2 = nullptr, *d_d1 = nullptr, *d_loss = nullptr;
+    int *d_idx = nullptr;
+    float *d_start = nullptr;  // start points and feature work of the last localization call
+    size_t start_cap = 0;
+    int batch = 0;
+    long long step = 0;
+    cudaStream_t stream = nullptr;
+};
+
+namespace {
+
+struct Views {
+    float *W1, *b1, *W2, *b2, *W3, *b3;
+};
+Views views(float *p) {
+    Views v;
+    v.W1 = p;
+    v.b1 = v.W1 + L::kIn * L::kHidden;
+    v.W2 = v.b1 + L::kHidden;
+    v.b2 = v.W2 + L::kHidden * L::kHidden;
+    v.W3 = v.b2 + L::kHidden;
+    v.b3 = v.W3 + L::kHidden * L::kOut;
+    return v;
+}
+
+inline int blocks(long long n, int t = 256) { return (int)((n + t - 1) / t); }
+
+// Forward over `rows` feature rows into net->d_y (and the hidden activations).
+cudaError_t forward(qcs_learned_net *net, const float *x, int rows, float *z1, float *a1, float *z2, float *a2,
+                    float *y, cudaStream_t s) {
+    const Views w = views(net->d_par);
+    cudaError_t e;
+    if ((e = L::gemm(rows, L::kHidden, L::kIn, x, L::kIn, 1, w.W1, L::kHidden, 1, z1, L::kHidden, 0.0f, s))) return e;
+    L::bias_relu_kernel<<<blocks((long long)rows * L::kHidden), 256, 0, s>>>(z1, w.b1, rows, L::kHidden, a1, 1);
+    if ((e = L::gemm(rows, L::kHidden, L::kHidden, a1, L::kHidden, 1, w.W2, L::kHidden, 1, z2, L::kHidden, 0.0f, s)))
+        return e;
+    L::bias_relu_kernel<<<blocks((long long)rows * L::kHidden), 256, 0, s>>>(z2, w.b2, rows, L::kHidden, a2, 1);
+    if ((e = L::gemm(rows, L::kOut, L::kHidden, a2, L::kHidden, 1, w.W3, L::kOut, 1, y, L::kOut, 0.0f, s))) return e;
+    L::bias_relu_kernel<<<blocks((long long)rows * L::kOut), 256, 0, s>>>(y, w.b3, rows, L::kOut, y, 0);
+    return cudaGetLastError();
+}
+
+// Backward of the masked MSE for one batch already forwarded; fills d_grad.
+cudaError_t backward(qcs_learned_net *net, int rows, cudaStream_t s) {
+    const Views w = views(net->d_par);
+    const Views g = views(net->d_grad);
+    cudaError_t e;
+    // layer 3: dW3 = a2^T dy, db3 = colsum(dy), d2 = dy W3^T
+    if ((e = L::gemm(L::kHidden, L::kOut, rows, net->d_a2, 1, L::kHidden, net->d_dy, L::kOut, 1, g.W3, L::kOut, 0.0f,
+                     s)))
+        return e;
+    L::colsum_kernel<<<1, L::kOut, 0, s>>>(net->d_dy, rows, L::kOut, g.b3);
+    if ((e = L::gemm(rows, L::kHidden, L::kOut, net->d_dy, L::kOut, 1, w.W3, 1, L::kOut, net->d_d2, L::kHidden, 0.0f,
+                     s)))
+        return e;
+    L::relu_back_kernel<<<blocks((long long)rows * L::kHidden), 256, 0, s>>>(net->d_d2, net->d_z2,
+                                                                           (long long)rows * L::kHidden);
+    // layer 2
+    if ((e = L::gemm(L::kHidden, L::kHidden, rows, net->d_a1, 1, L::kHidden, net->d_d2, L::kHidden, 1, g.W2,
+                     L::kHidden, 0.0f, s)))
+        return e;
+    L::colsum_kernel<<<1, L::kHidden, 0, s>>>(net->d_d2, rows, L::kHidden, g.b2);
+    if ((e = L::gemm(rows, L::kHidden, L::kHidden, net->d_d2, L::kHidden, 1, w.W2, 1, L::kHidden, net->d_d1,
+                     L::kHidden, 0.0f, s)))
+        return e;
+    L::relu_back_kernel<<<blocks((long long)rows * L::kHidden), 256, 0, s>>>(net->d_d1, net->d_z1,
+                                                                           (long long)rows * L::kHidden);
+    // layer 1
+    if ((e = L::gemm(L::kIn, L::kHidden, rows, net->d_x, 1, L::kIn, net->d_d1, L::kHidden, 1, g.W1, L::kHidden, 0.0f,
+                     s)))
+        return e;
+    L::colsum_kernel<<<1, L::kHidden, 0, s>>>(net->d_d1, rows, L::kHidden, g.b1);
+    return cudaGetLastError();
+}
+
+// xorshift-based permutation of [0, n) on the host, copied to the device
+void shuffle(int *h, int n, unsigned long long &state) {
+    for (int i = 0; i < n; ++i) h[i] = i;
+    for (int i = n - 1; i > 0; --i) {
+        state ^= state << 13;
+        state ^= state >> 7;
+        state ^= state << 17;
+        const int j = (int)(state % (unsigned long long)(i + 1));
+        const int t = h[i];
+        h[i] = h[j];
+        h[j] = t;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int qcs_learned_param_count(void) { return L::kParams; }
+
+int qcs_learned_destroy(qcs_learned_net *net) {
+    if (!net) return QCS_OK;
+    if (net->stream) cudaStreamSynchronize(net->stream);
+    cudaFree(net->d_par);
+    cudaFree(net->d_x);
+    cudaFree(net->d_idx);
+    cudaFree(net->d_start);
+    if (net->stream) cudaStreamDestroy(net->stream);
+    delete net;
+    return QCS_OK;
+}
+
+int qcs_learned_create(int batch, unsigned long long seed, qcs_learned_net **out) {
+    if (!out) return fail(QCS_ERR_ARG, "null output handle");
+    *out = nullptr;
+    if (batch <= 0) batch = 4096;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(QCS_ERR_CUDA, "no CUDA device: qcstorm_b200 has no CPU fallback");
+    qcs_learned_net *net = new qcs_learned_net();
+    net->batch = batch;
+    const size_t P = L::kParams;
+    const size_t B = (size_t)batch;
+    const size_t acts = B * (L::kIn + 4 * L::kHidden + L::kOut + L::kOutUsed + 1 + L::kOut + 2 * L::kHidden) + 4;
+    cudaError_t e = cudaMalloc((void **)&net->d_par, 4 * P * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&net->d_x, acts * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&net->d_idx, B * sizeof(int));
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&net->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        qcs_learned_destroy(net);
+        return fail(e == cudaErrorMemoryAllocation ? QCS_ERR_NOMEM : QCS_ERR_CUDA, "qcs_learned_create", e);
+    }
+    net->d_grad = net->d_par + P;
+    net->d_m = net->d_grad + P;
+    net->d_v = net->d_m + P;
+    float *a = net->d_x + B * L::kIn;
+    net->d_z1 = a;
+    a += B * L::kHidden;
+    net->d_a1 = a;
+    a += B * L::kHidden;
+    net->d_z2 = a;
+    a += B * L::kHidden;
+    net->d_a2 = a;
+    a += B * L::kHidden;
+    net->d_y = a;
+    a += B * L::kOut;
+    net->d_t = a;
+    a += B * L::kOutUsed;
+    net->d_valid = a;
+    a += B;
+    net->d_dy = a;
+    a += B * L::kOut;
+    net->d_d2 = a;
+    a += B * L::kHidden;
+    net->d_d1 = a;
+    a += B * L::kHidden;
+    net->d_loss = a;
+    // He-style initialisation from a host xorshift generator (uniform, variance 2 / fan_in)
+    float *h = new float[P];
+    unsigned long long st = seed ? seed : 0x9E3779B97F4A7C15ull;
+    auto uni = [&]() {
+        st ^= st << 13;
+        st ^= st >> 7;
+        st ^= st << 17;
+        return (float)((st >> 11) * (1.0 / 9007199254740992.0)) * 2.0f - 1.0f;
+    };
+    const Views hv = views(h);
+    for (int i = 0; i < L::kIn * L::kHidden; ++i) hv.W1[i] = uni() * sqrtf(6.0f / L::kIn);
+    for (int i = 0; i < L::kHidden; ++i) hv.b1[i] = 0.0f;
+    for (int i = 0; i < L::kHidden * L::kHidden; ++i) hv.W2[i] = uni() * sqrtf(6.0f / L::kHidden);
+    for (int i = 0; i < L::kHidden; ++i) hv.b2[i] = 0.0f;
+    for (int i = 0; i < L::kHidden * L::kOut; ++i) hv.W3[i] = uni() * sqrtf(3.0f / L::kHidden);
+    for (int i = 0; i < L::kOut; ++i) hv.b3[i] = 0.0f;
+    e = cudaMemcpy(net->d_par, h, P * sizeof(float), cudaMemcpyHostToDevice);
+    delete[] h;
+    if (e == cudaSuccess) e = cudaMemset(net->d_m, 0, 2 * P * sizeof(float));
+    if (e != cudaSuccess) {
+        qcs_learned_destroy(net);
+        return fail(QCS_ERR_CUDA, "initialise parameters", e);
+    }
+    *out = net;
+    return QCS_OK;
+}
+
+int qcs_learned_get_params(qcs_learned_net *net, float *h_params) {
+    if (!net || !h_params) return fail(QCS_ERR_ARG, "null argument");
+    QCS_CUDA(cudaMemcpy(h_params, net->d_par, L::kParams * sizeof(float), cudaMemcpyDeviceToHost), "read parameters");
+    return QCS_OK;
+}
+
+int qcs_learned_set_params(qcs_learned_net *net, const float *h_params) {
+    if (!net || !h_params) return fail(QCS_ERR_ARG, "null argument");
+    QCS_CUDA(cudaMemcpy(net->d_par, h_params, L::kParams * sizeof(float), cudaMemcpyHostToDevice), "set parameters");
+    return QCS_OK;
+}
+
+int qcs_learned_features_device(const qcs_loc_para *p, const uint16_t *d_rois, int n, float *d_feat, float *d_scale,
+                                void *stream) {
+    if (!p || (!d_rois && n > 0) || !d_feat || !d_scale) return fail(QCS_ERR_ARG, "null argument");
+    if (p->ROISize != L::kR || p->LocType != QCS_LOCTYPE_GS2D)
+        return fail(QCS_ERR_ROISIZE, "learned start points are built for GS2D 7x7 ROIs");
+    if (n <= 0) return QCS_OK;
+    L::features_kernel<<<blocks(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(d_rois, n, p->Offset, p->KAdc, d_feat,
+                                                                                 d_scale);
+    QCS_CUDA(cudaGetLastError(), "features");
+    return QCS_OK;
+}
+
+int qcs_learned_targets_device(const qcs_loc_para *p, const uint16_t *d_rois, const float *d_rows,
+                               const float *d_scale, int n, float *d_targets, float *d_valid, void *stream) {
+    if (!p || !d_rois || !d_rows || !d_scale || !d_targets || !d_valid) return fail(QCS_ERR_ARG, "null argument");
+    if (n <= 0) return QCS_OK;
+    L::targets_kernel<<<blocks(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(d_rois, d_rows, d_scale, n, p->QE,
+                                                                                d_targets, d_valid);
+    QCS_CUDA(cudaGetLastError(), "targets");
+    return QCS_OK;
+}
+
+int qcs_learned_forward_device(qcs_learned_net *net, const float *d_feat, int n, float *d_out, void *stream) {
+    if (!net || !d_feat || !d_out) return fail(QCS_ERR_ARG, "null argument");
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : net->stream;
+    for (int r0 = 0; r0 < n; r0 += net->batch) {
+        const int rows = (n - r0) < net->batch ? (n - r0) : net->batch;
+        QCS_CUDA(forward(net, d_feat + (size_t)r0 * L::kIn, rows, net->d_z1, net->d_a1, net->d_z2, net->d_a2,
+                         d_out + (size_t)r0 * L::kOut, s),
+                 "forward");
+    }
+    return QCS_OK;
+}
+
+int qcs_learned_gradient_device(qcs_learned_net *net, const float *d_feat, const float *d_targets,
+                                const float *d_valid, int n, float *h_loss, void *stream) {
+    if (!net || !d_feat || !d_targets || !d_valid) return fail(QCS_ERR_ARG, "null argument");
+    if (n <= 0 || n > net->batch) return fail(QCS_ERR_CAPACITY, "gradient batch must be 1..batch rows");
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : net->stream;
+    QCS_CUDA(cudaMemcpyAsync(net->d_x, d_feat, (size_t)n * L::kIn * sizeof(float), cudaMemcpyDeviceToDevice, s),
+             "copy features");
+    QCS_CUDA(forward(net, net->d_x, n, net->d_z1, net->d_a1, net->d_z2, net->d_a2, net->d_y, s), "forward");
+    QCS_CUDA(cudaMemsetAsync(net->d_loss, 0, sizeof(float), s), "clear loss");
+    L::mse_kernel<<<blocks(n), 256, 0, s>>>(net->d_y, d_targets, d_valid, n, 1.0f / (float)n, net->d_dy, net->d_loss);
+    QCS_CUDA(backward(net, n, s), "backward");
+    if (h_loss) {
+        QCS_CUDA(cudaMemcpyAsync(h_loss, net->d_loss, sizeof(float), cudaMemcpyDeviceToHost, s), "read loss");
+        QCS_CUDA(cudaStreamSynchronize(s), "gradient");
+    }
+    return QCS_OK;
+}
+
+int qcs_learned_get_grads(qcs_learned_net *net, float *h_grads) {
+    if (!net || !h_grads) return fail(QCS_ERR_ARG, "null argument");
+    QCS_CUDA(cudaMemcpy(h_grads, net->d_grad, L::kParams * sizeof(float), cudaMemcpyDeviceToHost), "read gradients");
+    return QCS_OK;
+}
+
+int qcs_learned_train_device(qcs_learned_net *net, const float *d_feat, const float *d_targets, const float *d_valid,
+                             int n, int epochs, float lr, unsigned long long seed, float *h_epoch_loss, void *stream) {
+    if (!net || !d_feat || !d_targets || !d_valid) return fail(QCS_ERR_ARG, "null argument");
+    if (n < net->batch) return fail(QCS_ERR_ARG, "fewer training rows than one batch");
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : net->stream;
+    const int B = net->batch;
+    const int steps = n / B;
+    int *h_perm = new int[n];
+    int *d_perm = nullptr;
+    float *d_vb = nullptr, *d_tb = nullptr;
+    cudaError_t e = cudaMalloc((void **)&d_perm, (size_t)n * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&d_vb, (size_t)B * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&d_tb, (size_t)B * L::kOutUsed * sizeof(float));
+    unsigned long long state = seed ? seed : 0x2545F4914F6CDD1Dull;
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    for (int ep = 0; ep < epochs && e == cudaSuccess; ++ep) {
+        shuffle(h_perm, n, state);
+        e = cudaMemcpyAsync(d_perm, h_perm, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(net->d_loss, 0, sizeof(float), s);
+        for (int st = 0; st < steps && e == cudaSuccess; ++st) {
+            const int *idx = d_perm + (size_t)st * B;
+            L::gather_rows_kernel<<<blocks((long long)B * L::kIn), 256, 0, s>>>(d_feat, idx, B, L::kIn, net->d_x);
+            L::gather_rows_kernel<<<blocks((long long)B * L::kOutUsed), 256, 0, s>>>(d_targets, idx, B, L::kOutUsed,
+                                                                                   d_tb);
+            L::gather_rows_kernel<<<blocks(B), 256, 0, s>>>(d_valid, idx, B, 1, d_vb);
+            e = forward(net, net->d_x, B, net->d_z1, net->d_a1, net->d_z2, net->d_a2, net->d_y, s);
+            if (e != cudaSuccess) break;
+            // per-batch mean loss and its gradient; the loss accumulates over the epoch
+            L::mse_kernel<<<blocks(B), 256, 0, s>>>(net->d_y, d_tb, d_vb, B, 1.0f / (float)B, net->d_dy, net->d_loss);
+            e = backward(net, B, s);
+            if (e != cudaSuccess) break;
+            net->step++;
+            const float c1 = 1.0f / (1.0f - powf(b1, (float)net->step));
+            const float c2 = 1.0f / (1.0f - powf(b2, (float)net->step));
+            L::adam_kernel<<<blocks(L::kParams), 256, 0, s>>>(net->d_par, net->d_grad, net->d_m, net->d_v, L::kParams,
+                                                             lr, b1, b2, c1, c2, eps);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess && h_epoch_loss) {
+            e = cudaMemcpyAsync(h_epoch_loss + ep, net->d_loss, sizeof(float), cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            h_epoch_loss[ep] /= (float)steps;
+        }
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(d_perm);
+    cudaFree(d_vb);
+    cudaFree(d_tb);
+    delete[] h_perm;
+    if (e != cudaSuccess) return fail(QCS_ERR_CUDA, "training", e);
+    return QCS_OK;
+}
+
+int qcs_learned_start_device(qcs_learned_net *net, const qcs_loc_para *p, const uint16_t *d_rois, int n,
+                             float *d_start, float *d_work, void *stream) {
+    if (!net || !p || !d_start || !d_work) return fail(QCS_ERR_ARG, "null argument");
+    if (n <= 0) return QCS_OK;
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : net->stream;
+    float *feat = d_work, *scale = feat + (size_t)n * L::kIn, *y = scale + 2 * (size_t)n;
+    int st = qcs_learned_features_device(p, d_rois, n, feat, scale, s);
+    if (st) return st;
+    st = qcs_learned_forward_device(net, feat, n, y, s);
+    if (st) return st;
+    L::start_kernel<<<blocks(n), 256, 0, s>>>(y, scale, n, d_start);
+    QCS_CUDA(cudaGetLastError(), "start points");
+    return QCS_OK;
+}
+
+size_t qcs_learned_work_bytes(int n) { return (size_t)(n > 0 ? n : 0) * (L::kIn + 2 + L::kOut) * sizeof(float); }
+
+}  // extern "C"
+
+// Start points of n records into net-owned memory (grown, outside any
+// capture, when n exceeds what the last call needed): features, one GEMM per
+// layer over all n rows (activations rectified in place), start points.
+cudaError_t qcs::learned::start_points(qcs_learned_net *net, const qcs_loc_para *p, const uint16_t *d_rois, int n,
+                                       const float **d_start, cudaStream_t s) {
+    const size_t need = (size_t)n * (L::kStart + L::kIn + 2 + 2 * L::kHidden + L::kOut);
+    if (need > net->start_cap) {
+        cudaFree(net->d_start);
+        net->d_start = nullptr;
+        net->start_cap = 0;
+        cudaError_t e = cudaMalloc((void **)&net->d_start, need * sizeof(float));
+        if (e != cudaSuccess) return e;
+        net->start_cap = need;
+    }
+    float *start = net->d_start, *feat = start + (size_t)n * L::kStart, *scale = feat + (size_t)n * L::kIn;
+    float *h1 = scale + 2 * (size_t)n, *h2 = h1 + (size_t)n * L::kHidden, *y = h2 + (size_t)n * L::kHidden;
+    L::features_kernel<<<blocks(n), 256, 0, s>>>(d_rois, n, p->Offset, p->KAdc, feat, scale);
+    cudaError_t e = forward(net, feat, n, h1, h1, h2, h2, y, s);
+    if (e != cudaSuccess) return e;
+    L::start_kernel<<<blocks(n), 256, 0, s>>>(y, scale, n, start);
+    *d_start = start;
+    return cudaGetLastError();
+}

@@ -51,6 +51,29 @@ _SIGS = {
     "qcs_zero_valid_num": (C.c_int, [C.c_void_p]),
     "qcs_zero_remove_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int,
                                          C.c_void_p, C.c_void_p, C.c_void_p]),
+    "qcs_learned_param_count": (C.c_int, []),
+    "qcs_learned_create": (C.c_int, [C.c_int, C.c_ulonglong, C.POINTER(C.c_void_p)]),
+    "qcs_learned_destroy": (C.c_int, [C.c_void_p]),
+    "qcs_learned_get_params": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "qcs_learned_set_params": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "qcs_learned_features_device": (C.c_int, [C.POINTER(LocPara), C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                              C.c_void_p]),
+    "qcs_learned_targets_device": (C.c_int, [C.POINTER(LocPara), C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                             C.c_void_p, C.c_void_p, C.c_void_p]),
+    "qcs_learned_forward_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "qcs_learned_gradient_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                              C.POINTER(C.c_float), C.c_void_p]),
+    "qcs_learned_get_grads": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "qcs_learned_train_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                                           C.c_float, C.c_ulonglong, C.c_void_p, C.c_void_p]),
+    "qcs_learned_start_device": (C.c_int, [C.c_void_p, C.POINTER(LocPara), C.c_void_p, C.c_int, C.c_void_p,
+                                           C.c_void_p, C.c_void_p]),
+    "qcs_learned_work_bytes": (C.c_size_t, [C.c_int]),
+    "qcs_learned_localize_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(LocPara),
+                                              C.c_int, C.c_int, C.c_float, C.c_void_p]),
+    "qcs_learned_refit_num": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "qcs_fit_from_start_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(LocPara), C.c_int,
+                                            C.c_void_p, C.c_int, C.c_float, C.c_void_p]),
     "qcs_extract_max_batched_num": (C.c_int, [C.c_int, C.c_int]),
     "qcs_extract_init": (C.c_int, [C.POINTER(LocPara), C.POINTER(C.c_void_p)]),
     "qcs_extract_init_ex": (C.c_int, [C.POINTER(LocPara), C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
@@ -313,3 +336,112 @@ class ZeroRemover:
                                               int(bool(sort_frame)), int(first_frame), int(end_frame),
                                               C.c_void_p(d_out), C.c_void_p(d_nvalid) if d_nvalid else None,
                                               C.c_void_p(stream) if stream else None))
+
+
+class LearnedNet:
+    """Learned start points for GS2D 7x7 fits (qcs_learned_*): device tensors are torch CUDA tensors."""
+
+    def __init__(self, batch=4096, seed=1):
+        self.lib = load()
+        h = C.c_void_p()
+        check(self.lib.qcs_learned_create(int(batch), int(seed), C.byref(h)))
+        self.h = h
+        self.n_params = self.lib.qcs_learned_param_count()
+
+    def close(self):
+        if self.h:
+            self.lib.qcs_learned_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def params(self):
+        out = np.zeros(self.n_params, np.float32)
+        check(self.lib.qcs_learned_get_params(self.h, C.c_void_p(out.ctypes.data)))
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == self.n_params
+        check(self.lib.qcs_learned_set_params(self.h, C.c_void_p(p.ctypes.data)))
+
+    def grads(self):
+        out = np.zeros(self.n_params, np.float32)
+        check(self.lib.qcs_learned_get_grads(self.h, C.c_void_p(out.ctypes.data)))
+        return out
+
+    @staticmethod
+    def features(para, d_rois, n, stream=0):
+        import torch
+        feat = torch.empty((n, 64), dtype=torch.float32, device="cuda")
+        scale = torch.empty((n, 2), dtype=torch.float32, device="cuda")
+        check(load().qcs_learned_features_device(C.byref(para), C.c_void_p(d_rois), int(n), C.c_void_p(feat.data_ptr()),
+                                                 C.c_void_p(scale.data_ptr()), C.c_void_p(stream) if stream else None))
+        return feat, scale
+
+    @staticmethod
+    def targets(para, d_rois, d_rows, scale, n, stream=0):
+        import torch
+        t = torch.empty((n, 5), dtype=torch.float32, device="cuda")
+        v = torch.empty((n,), dtype=torch.float32, device="cuda")
+        check(load().qcs_learned_targets_device(C.byref(para), C.c_void_p(d_rois), C.c_void_p(d_rows),
+                                                C.c_void_p(scale.data_ptr()), int(n), C.c_void_p(t.data_ptr()),
+                                                C.c_void_p(v.data_ptr()), C.c_void_p(stream) if stream else None))
+        return t, v
+
+    def forward(self, feat, stream=0):
+        import torch
+        n = feat.shape[0]
+        out = torch.empty((n, 8), dtype=torch.float32, device="cuda")
+        check(self.lib.qcs_learned_forward_device(self.h, C.c_void_p(feat.data_ptr()), int(n),
+                                                  C.c_void_p(out.data_ptr()), C.c_void_p(stream) if stream else None))
+        return out
+
+    def gradient(self, feat, tgt, valid, stream=0):
+        loss = C.c_float(0)
+        check(self.lib.qcs_learned_gradient_device(self.h, C.c_void_p(feat.data_ptr()), C.c_void_p(tgt.data_ptr()),
+                                                   C.c_void_p(valid.data_ptr()), int(feat.shape[0]), C.byref(loss),
+                                                   C.c_void_p(stream) if stream else None))
+        return loss.value
+
+    def train(self, feat, tgt, valid, epochs, lr=1e-3, seed=7, stream=0):
+        losses = np.zeros(epochs, np.float32)
+        check(self.lib.qcs_learned_train_device(self.h, C.c_void_p(feat.data_ptr()), C.c_void_p(tgt.data_ptr()),
+                                                C.c_void_p(valid.data_ptr()), int(feat.shape[0]), int(epochs),
+                                                C.c_float(lr), int(seed), C.c_void_p(losses.ctypes.data),
+                                                C.c_void_p(stream) if stream else None))
+        return losses
+
+    def start(self, para, d_rois, n, stream=0):
+        import torch
+        st = torch.empty((n, 5), dtype=torch.float32, device="cuda")
+        work = torch.empty((int(self.lib.qcs_learned_work_bytes(int(n))) // 4 + 1,), dtype=torch.float32,
+                           device="cuda")
+        check(self.lib.qcs_learned_start_device(self.h, C.byref(para), C.c_void_p(d_rois), int(n),
+                                                C.c_void_p(st.data_ptr()), C.c_void_p(work.data_ptr()),
+                                                C.c_void_p(stream) if stream else None))
+        return st
+
+    def localize(self, ctx, d_rois, n, d_wle=0, iters=3, dev_th=0.0, para=None, stream=0):
+        """qcs_learned_localize_device on a LocContext; rows stay in the context."""
+        para = para or ctx.para
+        check(self.lib.qcs_learned_localize_device(ctx.h, self.h, C.c_void_p(d_rois), C.c_void_p(d_wle) if d_wle else None,
+                                                   C.byref(para), int(n), int(iters), C.c_float(dev_th),
+                                                   C.c_void_p(stream) if stream else None))
+
+    def refits(self, ctx):
+        k = C.c_int(0)
+        check(self.lib.qcs_learned_refit_num(ctx.h, C.byref(k)))
+        return k.value
+
+
+def fit_from_start(ctx, d_rois, n, d_start, d_wle=0, iters=3, dev_th=0.0, para=None, stream=0):
+    """qcs_fit_from_start_device: GS2D 7x7 fits from given start points; rows stay in the context."""
+    para = para or ctx.para
+    check(load().qcs_fit_from_start_device(ctx.h, C.c_void_p(d_rois), C.c_void_p(d_wle) if d_wle else None,
+                                           C.byref(para), int(n), C.c_void_p(d_start), int(iters), C.c_float(dev_th),
+                                           C.c_void_p(stream) if stream else None))
