@@ -345,7 +345,7 @@ int qcs_learned_get_grads(qcs_learned_net *net, float *h_grads);
 int qcs_learned_train_device(qcs_learned_net *net, const float *d_feat, const float *d_targets, const float *d_valid,
                              int n, int epochs, float lr, unsigned long long seed, float *h_epoch_loss, void *stream);
 /* Start points (n x 5: peak e-, x, y, sigma, background e-) of n device records;
- * d_work holds qcs_learned_work_bytes(n) bytes. */
+ * d_work holds qcs_learned_work_bytes(n) bytes (unused by the fused path). */
 int qcs_learned_start_device(qcs_learned_net *net, const qcs_loc_para *p, const uint16_t *d_rois, int n,
                              float *d_start, float *d_work, void *stream);
 size_t qcs_learned_work_bytes(int n);
@@ -362,6 +362,13 @@ int qcs_fit_from_start_device(qcs_loc_data *c, const uint16_t *d_rois, const flo
  * kernel; then CRLB.  Rows in the context like qcs_loc_localize_device (n rows). */
 int qcs_learned_localize_device(qcs_loc_data *c, qcs_learned_net *net, const uint16_t *d_rois, const float *d_wle,
                                 const qcs_loc_para *p, int n, int iters, float dev_th, void *stream);
+/* Inference path of qcs_learned_localize_device: fused = 1 (default) runs the
+ * whole network per 128-ROI tile in one tcgen05 kernel; 0 runs it layer by
+ * layer through the training GEMMs. */
+int qcs_learned_set_inference(qcs_learned_net *net, int fused);
+/* QCS_OK, or QCS_ERR_CUDA if a fused-inference launch gave up waiting for its
+ * tensor-core work (waits for the device). */
+int qcs_learned_fused_status(qcs_learned_net *net);
 /* Number of plain refits of the last qcs_learned_localize_device call (waits for it). */
 int qcs_learned_refit_num(qcs_loc_data *c, int *n);
 

@@ -258,6 +258,265 @@ __global__ void start_kernel(const float *__restrict__ Y, const float *__restric
     s[4] = fmaxf(lo + rng * y[4], 1.0f);
 }
 
+// ------------------------------------------- fused tcgen05 inference ---
+// One persistent CTA of 128 threads per 128-ROI tile: features -> layer 1 ->
+// ReLU -> layer 2 -> ReLU -> layer 3 -> start point, with every activation
+// kept on chip.  The three GEMMs are tcgen05.mma (M = 128, kind::f16, BF16
+// operands in shared memory, FP32 accumulators in tensor memory), issued by
+// one thread and completed through an mbarrier; each warp reads its 32
+// accumulator rows back with tcgen05.ld.  Operands use the K-major,
+// no-swizzle UMMA layout: 8-row x 16-byte core matrices, 8-row groups 128 B
+// apart (SBO), 8-element K groups rows x 16 B apart (LBO).
+namespace tc {
+
+constexpr int kM = 128;        // ROIs per tile (the MMA's M)
+constexpr int kN3 = 16;        // layer-3 N padded to the M = 128 minimum
+constexpr int kW1 = kHidden * kIn, kW2 = kHidden * kHidden, kW3 = kN3 * kHidden;  // bf16 elements
+constexpr int kOffW1 = 0;
+constexpr int kOffW2 = kOffW1 + kW1 * 2;
+constexpr int kOffW3 = kOffW2 + kW2 * 2;
+constexpr int kOffA1 = kOffW3 + kW3 * 2;
+constexpr int kOffA2 = kOffA1 + kM * kIn * 2;
+constexpr int kOffBar = kOffA2 + kM * kHidden * 2;
+constexpr int kSmemBytes = kOffBar + 16 + 1024;  // + alignment slack
+constexpr int kTmemCols = 256;                  // layer 1 / 3 at column 0, layer 2 at column 128
+constexpr int kWeightVec = (kW1 + kW2 + kW3) * 2 / 16;
+
+// element (n, k) of an N x K K-major operand image, in bf16 elements
+__host__ __device__ constexpr int img_index(int n, int k, int N) { return ((k >> 3) * N + n) * 8 + (k & 7); }
+
+// UMMA shared-memory descriptor: start address, leading (K-group) and stride
+// (8-row group) byte offsets, version 1, no swizzle.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
+}
+
+// instruction descriptor: FP32 accumulate, BF16 A and B, both K-major, N, M
+__host__ __device__ constexpr uint32_t instr_desc(int M, int N) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+        :
+        : "r"(tmem_d), "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+// Bounded wait for the barrier phase; false when it did not complete.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
+    for (int it = 0; it < (1 << 22); ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.b32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(phase)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ uint4 pack8(const float *v) {
+    uint4 u;
+    u.x = pack_bf16(v[0], v[1]);
+    u.y = pack_bf16(v[2], v[3]);
+    u.z = pack_bf16(v[4], v[5]);
+    u.w = pack_bf16(v[6], v[7]);
+    return u;
+}
+
+// Relu(D + bias) of this thread's accumulator row (ncols columns from tmem
+// column col0) into the next layer's A operand (row tid).
+__device__ __forceinline__ void epilogue_hidden(uint32_t taddr_row, const float *__restrict__ bias, uint8_t *a_next,
+                                                int tid) {
+#pragma unroll 1
+    for (int c0 = 0; c0 < kHidden; c0 += 16) {
+        float v[16];
+        tmem_ld16(taddr_row + c0, v);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) v[j] = fmaxf(v[j] + __ldg(bias + c0 + j), 0.0f);
+        *reinterpret_cast<uint4 *>(a_next + (size_t)((c0 >> 3) * kM + tid) * 16) = pack8(v);
+        *reinterpret_cast<uint4 *>(a_next + (size_t)(((c0 >> 3) + 1) * kM + tid) * 16) = pack8(v + 8);
+    }
+}
+
+__global__ void __launch_bounds__(128, 1) mlp_tc_kernel(const uint16_t *__restrict__ rois, int n, float offset,
+                                                        float kadc, const uint4 *__restrict__ wimg,
+                                                        const float *__restrict__ b1, const float *__restrict__ b2,
+                                                        const float *__restrict__ b3, float *__restrict__ start,
+                                                        int *__restrict__ err) {
+    extern __shared__ uint8_t smem_raw[];
+    const uint32_t raw = (uint32_t)__cvta_generic_to_shared(smem_raw);
+    const uint32_t sbase = (raw + 1023u) & ~1023u;
+    uint8_t *base = smem_raw + (sbase - raw);
+    const uint32_t sW1 = sbase + kOffW1, sW2 = sbase + kOffW2, sW3 = sbase + kOffW3;
+    const uint32_t sA1 = sbase + kOffA1, sA2 = sbase + kOffA2, sBar = sbase + kOffBar, sTmem = sBar + 8;
+    const int tid = threadIdx.x, warp = tid >> 5;
+
+    uint4 *wdst = reinterpret_cast<uint4 *>(base + kOffW1);
+    for (int i = tid; i < kWeightVec; i += blockDim.x) wdst[i] = wimg[i];
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(sBar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sTmem), "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_async_smem();
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = *reinterpret_cast<volatile uint32_t *>(base + kOffBar + 8);
+    const uint32_t row_lane = (uint32_t)(warp * 32) << 16;
+    uint32_t phase = 0;
+    bool ok = true;
+    const int ntiles = (n + kM - 1) / kM;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int i = tile * kM + tid;
+        // features of this thread's ROI into A1 (row tid)
+        float lo = 1.0f, rng = 1.0f;
+        {
+            float f[kIn];
+#pragma unroll
+            for (int k = 0; k < kIn; ++k) f[k] = 0.0f;
+            if (i < n) {
+                const uint16_t *r = rois + (size_t)i * kWhole;
+                float hi = -1e30f;
+                lo = 1e30f;
+#pragma unroll
+                for (int k = 0; k < kPix; ++k) {
+                    f[k] = fmaxf(((float)r[k] - offset) * kadc, 1.0f);
+                    lo = fminf(lo, f[k]);
+                    hi = fmaxf(hi, f[k]);
+                }
+                rng = fmaxf(hi - lo, 1.0f);
+                const float inv = 1.0f / rng;
+#pragma unroll
+                for (int k = 0; k < kPix; ++k) f[k] = (f[k] - lo) * inv;
+                f[kPix] = logf(rng) * 0.125f;
+                f[kPix + 1] = logf(lo) * 0.125f;
+            }
+#pragma unroll
+            for (int kg = 0; kg < kIn / 8; ++kg)
+                *reinterpret_cast<uint4 *>(base + kOffA1 + (size_t)(kg * kM + tid) * 16) = pack8(f + 8 * kg);
+        }
+        fence_async_smem();
+        fence_before();
+        __syncthreads();
+        fence_after();
+        // layer 1: D[128 x 128] at column 0
+        if (tid == 0) {
+#pragma unroll
+            for (int ks = 0; ks < kIn / 16; ++ks)
+                mma_bf16(tmem, smem_desc(sA1 + ks * 2 * kM * 16, kM * 16, 128),
+                         smem_desc(sW1 + ks * 2 * kHidden * 16, kHidden * 16, 128), instr_desc(kM, kHidden),
+                         ks > 0);
+            mma_commit(sBar);
+        }
+        ok = __syncthreads_and(mbar_wait(sBar, phase));
+        phase ^= 1u;
+        if (!ok) break;
+        fence_after();
+        epilogue_hidden(tmem + row_lane, b1, base + kOffA2, tid);
+        fence_async_smem();
+        fence_before();
+        __syncthreads();
+        fence_after();
+        // layer 2: D[128 x 128] at column 128
+        if (tid == 0) {
+#pragma unroll
+            for (int ks = 0; ks < kHidden / 16; ++ks)
+                mma_bf16(tmem + kHidden, smem_desc(sA2 + ks * 2 * kM * 16, kM * 16, 128),
+                         smem_desc(sW2 + ks * 2 * kHidden * 16, kHidden * 16, 128), instr_desc(kM, kHidden),
+                         ks > 0);
+            mma_commit(sBar);
+        }
+        ok = __syncthreads_and(mbar_wait(sBar, phase));
+        phase ^= 1u;
+        if (!ok) break;
+        fence_after();
+        epilogue_hidden(tmem + row_lane + kHidden, b2, base + kOffA2, tid);  // layer 2 has read A2
+        fence_async_smem();
+        fence_before();
+        __syncthreads();
+        fence_after();
+        // layer 3: D[128 x 16] at column 0
+        if (tid == 0) {
+#pragma unroll
+            for (int ks = 0; ks < kHidden / 16; ++ks)
+                mma_bf16(tmem, smem_desc(sA2 + ks * 2 * kM * 16, kM * 16, 128),
+                         smem_desc(sW3 + ks * 2 * kN3 * 16, kN3 * 16, 128), instr_desc(kM, kN3), ks > 0);
+            mma_commit(sBar);
+        }
+        ok = __syncthreads_and(mbar_wait(sBar, phase));
+        phase ^= 1u;
+        if (!ok) break;
+        fence_after();
+        float y[16];
+        tmem_ld16(tmem + row_lane, y);
+        if (i < n) {
+            float *st = start + (size_t)i * kStart;
+            st[0] = rng * expf(fminf(fmaxf(y[3] + __ldg(b3 + 3), -6.0f), 3.0f));
+            st[1] = kCentre + fminf(fmaxf(y[0] + __ldg(b3 + 0), -1.5f), 1.5f);
+            st[2] = kCentre + fminf(fmaxf(y[1] + __ldg(b3 + 1), -1.5f), 1.5f);
+            st[3] = fminf(fmaxf(kSigma0 + y[2] + __ldg(b3 + 2), 0.6f), 3.0f);
+            st[4] = fmaxf(lo + rng * (y[4] + __ldg(b3 + 4)), 1.0f);
+        }
+        fence_before();
+        __syncthreads();  // accumulator columns are free for the next tile
+        fence_after();
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+    if (!ok && tid == 0) atomicExch(err, 1);
+}
+
+// FP32 master weights -> BF16 operand images (W1 | W2 | W3, N x K K-major).
+__global__ void weight_image_kernel(const float *__restrict__ par, __nv_bfloat16 *__restrict__ img) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const float *W1 = par, *W2 = W1 + kIn * kHidden + kHidden, *W3 = W2 + kHidden * kHidden + kHidden;
+    if (i < kW1) {
+        const int k = i / kHidden, nn = i % kHidden;
+        img[img_index(nn, k, kHidden)] = __float2bfloat16_rn(W1[i]);
+    } else if (i < kW1 + kW2) {
+        const int j = i - kW1, k = j / kHidden, nn = j % kHidden;
+        img[kW1 + img_index(nn, k, kHidden)] = __float2bfloat16_rn(W2[j]);
+    } else if (i < kW1 + kW2 + kW3) {
+        const int j = i - kW1 - kW2, k = j / kN3, nn = j % kN3;
+        img[kW1 + kW2 + img_index(nn, k, kN3)] = __float2bfloat16_rn(nn < kOut ? W3[k * kOut + nn] : 0.0f);
+    }
+}
+
+}  // namespace tc
 }  // namespace learned
 }  // namespace qcs
 
@@ -273,6 +532,9 @@ struct qcs_learned_net {
     int *d_idx = nullptr;
     float *d_start = nullptr;  // start points and feature work of the last localization call
     size_t start_cap = 0;
+    __nv_bfloat16 *d_wimg = nullptr;  // BF16 operand images of the weights (fused inference)
+    int *d_err = nullptr;             // set by the fused kernel when an MMA wait gives up
+    bool use_tc = true;
     int batch = 0;
     long long step = 0;
     cudaStream_t stream = nullptr;
@@ -358,6 +620,28 @@ void shuffle(int *h, int n, unsigned long long &state) {
     }
 }
 
+// Start points of n ROIs through the fused tcgen05 kernel: BF16 operand
+// images of the current weights, then one persistent launch (two CTAs of
+// 101 KB shared memory and 256 tensor-memory columns per SM).
+cudaError_t fused_start_points(qcs_learned_net *net, const qcs_loc_para *p, const uint16_t *d_rois, int n,
+                               float *start, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    const int tiles = (n + L::tc::kM - 1) / L::tc::kM;
+    int dev = 0, sms = 148;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(L::tc::mlp_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, L::tc::kSmemBytes);
+    if (e != cudaSuccess) return e;
+    const int grid = tiles < 2 * sms ? tiles : 2 * sms;
+    const Views w = views(net->d_par);
+    L::tc::weight_image_kernel<<<blocks(L::tc::kW1 + L::tc::kW2 + L::tc::kW3), 256, 0, s>>>(net->d_par, net->d_wimg);
+    L::tc::mlp_tc_kernel<<<grid, 128, L::tc::kSmemBytes, s>>>(d_rois, n, p->Offset, p->KAdc,
+                                                              reinterpret_cast<const uint4 *>(net->d_wimg), w.b1, w.b2,
+                                                              w.b3, start, net->d_err);
+    return cudaGetLastError();
+}
+
 }  // namespace
 
 extern "C" {
@@ -371,6 +655,8 @@ int qcs_learned_destroy(qcs_learned_net *net) {
     cudaFree(net->d_x);
     cudaFree(net->d_idx);
     cudaFree(net->d_start);
+    cudaFree(net->d_wimg);
+    cudaFree(net->d_err);
     if (net->stream) cudaStreamDestroy(net->stream);
     delete net;
     return QCS_OK;
@@ -391,6 +677,9 @@ int qcs_learned_create(int batch, unsigned long long seed, qcs_learned_net **out
     cudaError_t e = cudaMalloc((void **)&net->d_par, 4 * P * sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc((void **)&net->d_x, acts * sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc((void **)&net->d_idx, B * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&net->d_wimg, L::tc::kWeightVec * 16);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&net->d_err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(net->d_err, 0, sizeof(int));
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&net->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         qcs_learned_destroy(net);
@@ -576,6 +865,10 @@ int qcs_learned_start_device(qcs_learned_net *net, const qcs_loc_para *p, const 
     if (!net || !p || !d_start || !d_work) return fail(QCS_ERR_ARG, "null argument");
     if (n <= 0) return QCS_OK;
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : net->stream;
+    if (net->use_tc) {
+        QCS_CUDA(fused_start_points(net, p, d_rois, n, d_start, s), "fused start points");
+        return QCS_OK;
+    }
     float *feat = d_work, *scale = feat + (size_t)n * L::kIn, *y = scale + 2 * (size_t)n;
     int st = qcs_learned_features_device(p, d_rois, n, feat, scale, s);
     if (st) return st;
@@ -587,6 +880,20 @@ int qcs_learned_start_device(qcs_learned_net *net, const qcs_loc_para *p, const 
 }
 
 size_t qcs_learned_work_bytes(int n) { return (size_t)(n > 0 ? n : 0) * (L::kIn + 2 + L::kOut) * sizeof(float); }
+
+int qcs_learned_set_inference(qcs_learned_net *net, int fused) {
+    if (!net) return fail(QCS_ERR_ARG, "null network");
+    net->use_tc = fused != 0;
+    return QCS_OK;
+}
+
+int qcs_learned_fused_status(qcs_learned_net *net) {
+    if (!net) return fail(QCS_ERR_ARG, "null network");
+    int h = 0;
+    QCS_CUDA(cudaDeviceSynchronize(), "fused inference");
+    QCS_CUDA(cudaMemcpy(&h, net->d_err, sizeof(int), cudaMemcpyDeviceToHost), "read status");
+    return h ? fail(QCS_ERR_CUDA, "fused inference: a tensor-core wait gave up") : QCS_OK;
+}
 
 }  // extern "C"
 
@@ -606,10 +913,11 @@ cudaError_t qcs::learned::start_points(qcs_learned_net *net, const qcs_loc_para 
     }
     float *start = net->d_start, *feat = start + (size_t)n * L::kStart, *scale = feat + (size_t)n * L::kIn;
     float *h1 = scale + 2 * (size_t)n, *h2 = h1 + (size_t)n * L::kHidden, *y = h2 + (size_t)n * L::kHidden;
+    *d_start = start;
+    if (net->use_tc) return fused_start_points(net, p, d_rois, n, start, s);
     L::features_kernel<<<blocks(n), 256, 0, s>>>(d_rois, n, p->Offset, p->KAdc, feat, scale);
     cudaError_t e = forward(net, feat, n, h1, h1, h2, h2, y, s);
     if (e != cudaSuccess) return e;
     L::start_kernel<<<blocks(n), 256, 0, s>>>(y, scale, n, start);
-    *d_start = start;
     return cudaGetLastError();
 }

@@ -72,6 +72,8 @@ _SIGS = {
     "qcs_learned_localize_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(LocPara),
                                               C.c_int, C.c_int, C.c_float, C.c_void_p]),
     "qcs_learned_refit_num": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "qcs_learned_set_inference": (C.c_int, [C.c_void_p, C.c_int]),
+    "qcs_learned_fused_status": (C.c_int, [C.c_void_p]),
     "qcs_fit_from_start_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(LocPara), C.c_int,
                                             C.c_void_p, C.c_int, C.c_float, C.c_void_p]),
     "qcs_extract_max_batched_num": (C.c_int, [C.c_int, C.c_int]),
@@ -432,6 +434,12 @@ class LearnedNet:
         check(self.lib.qcs_learned_localize_device(ctx.h, self.h, C.c_void_p(d_rois), C.c_void_p(d_wle) if d_wle else None,
                                                    C.byref(para), int(n), int(iters), C.c_float(dev_th),
                                                    C.c_void_p(stream) if stream else None))
+
+    def set_fused(self, fused=True):
+        check(self.lib.qcs_learned_set_inference(self.h, int(bool(fused))))
+
+    def fused_status(self):
+        check(self.lib.qcs_learned_fused_status(self.h))
 
     def refits(self, ctx):
         k = C.c_int(0)

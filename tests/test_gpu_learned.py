@@ -80,6 +80,55 @@ def test_forward_and_gradient_match_oracle(cuda_ok):
     net.close()
 
 
+def start_from_y(y, scale):
+    """The start-point transform of the network outputs (clamps as in qcs_learned.cu start_kernel)."""
+    lo, rng = scale[:, 0].astype(np.float64), scale[:, 1].astype(np.float64)
+    return np.stack([rng * np.exp(np.clip(y[:, 3], -6, 3)), NO.CENTRE + np.clip(y[:, 0], -1.5, 1.5),
+                     NO.CENTRE + np.clip(y[:, 1], -1.5, 1.5), np.clip(NO.SIGMA0 + y[:, 2], 0.6, 3.0),
+                     np.maximum(lo + rng * y[:, 4], 1.0)], 1)
+
+
+def assert_start_close(a, b, scale, tol):
+    """Start points agree to `tol` in network-output units: relative for the
+    peak (exp of an output), absolute for x, y, sigma, background / range."""
+    rng = scale[:, 1].astype(np.float64)
+    assert np.max(np.abs(np.log(a[:, 0] / b[:, 0]))) <= tol
+    assert np.max(np.abs(a[:, 1:4] - b[:, 1:4])) <= tol
+    assert np.max(np.abs(a[:, 4] - b[:, 4]) / rng) <= tol
+
+
+@pytest.mark.parametrize("n", [1, 1000, 100_000])
+def test_fused_tensor_core_start_points(cuda_ok, n):
+    """The fused tcgen05 inference kernel (features, three BF16 GEMMs with
+    FP32 accumulation in tensor memory, start transform, one launch) against
+    the layer-by-layer path and against the numpy forward pass: the ragged
+    last 128-ROI tile, a single ROI, and more tiles than resident CTAs.  The
+    network is trained briefly so that its outputs are not near zero."""
+    import torch
+    rec, para, _ = synth.gs2d_rois(max(n, 4096), seed=13)
+    d = to_dev(rec)
+    feat, scale = qlib.LearnedNet.features(para, d.data_ptr(), rec.shape[0])
+    rows = plain_rows(rec, para)
+    d_rows = to_dev(rows.astype(np.float32))
+    t, v = qlib.LearnedNet.targets(para, d.data_ptr(), d_rows.data_ptr(), scale, rec.shape[0])
+    net = qlib.LearnedNet(batch=1024, seed=4)
+    net.train(feat, t, v, epochs=2, lr=2e-3)
+    net.set_fused(True)
+    fused = net.start(para, d.data_ptr(), n).cpu().numpy().astype(np.float64)
+    net.fused_status()
+    net.set_fused(False)
+    layered = net.start(para, d.data_ptr(), n).cpu().numpy().astype(np.float64)
+    torch.cuda.synchronize()
+    sc = scale.cpu().numpy()[:n]
+    assert np.all(np.isfinite(fused))
+    y_scale = max(1.0, float(np.max(np.abs(NO.forward(net.params(), feat[:min(n, 2048)].cpu().numpy())[0]))))
+    assert_start_close(fused, layered, sc, 2e-3 * y_scale)
+    k = min(n, 2048)
+    y_o, _ = NO.forward(net.params(), feat[:k].cpu().numpy())
+    assert_start_close(fused[:k], start_from_y(y_o, sc[:k]), sc[:k], 2e-3 * y_scale)
+    net.close()
+
+
 def rmse_xy(rows, rec, truth, sel):
     """RMSE per axis (px) of the fitted centres in ROI coordinates: the row's
     x is fit - R/2 + header x (header word 0 / 1 of the record)."""
