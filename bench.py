@@ -262,6 +262,147 @@ def frame_pipeline(stream, steps, warmup, e2e=True):
     }
 
 
+LEARNED_ITERS = 2          # BFGS iterations from the network's start points (plain: 8)
+TRAIN_RECORDS = 200_000    # training records, same generator, seeds disjoint from the timed batches
+TRAIN_EPOCHS = 8
+
+
+def train_learned_net(para, stream, seed=4242):
+    """Train the start-point network on the GPU: TRAIN_RECORDS fresh records
+    labelled by plain fits, features and targets on the device, Adam over
+    TRAIN_EPOCHS epochs (qcs_learned_train_device).  Returns (net, info)."""
+    import torch
+    from qcstorm_b200 import lib, synth
+    sh = stream.cuda_stream
+    t0 = time.perf_counter()
+    tr, _, _ = synth.gs2d_rois(TRAIN_RECORDS, R=R, seed=seed)
+    d_tr = torch.from_numpy(tr.view(np.int16)).cuda()
+    ctx = lib.LocContext(para, capacity=TRAIN_RECORDS)
+    ctx.localize_device(d_tr.data_ptr(), TRAIN_RECORDS, 0, sh)
+    stream.synchronize()
+    feat, scale = lib.LearnedNet.features(para, d_tr.data_ptr(), TRAIN_RECORDS, stream=sh)
+    tgt, valid = lib.LearnedNet.targets(para, d_tr.data_ptr(), ctx.device_rows(), scale, TRAIN_RECORDS, stream=sh)
+    net = lib.LearnedNet(batch=4096, seed=5)
+    losses = net.train(feat, tgt, valid, epochs=TRAIN_EPOCHS, lr=2e-3, stream=sh)
+    stream.synchronize()
+    info = {"records": TRAIN_RECORDS, "epochs": TRAIN_EPOCHS, "seconds": time.perf_counter() - t0,
+            "loss_first_epoch": float(losses[0]), "loss_last_epoch": float(losses[-1]),
+            "labels": "plain MLEbfgs fits of the training records on this GPU"}
+    ctx.close()
+    return net, info
+
+
+def fit_accuracy(rows, rec, truth, sel, para):
+    """Position RMSE (px, per axis), relative photon RMSE and CRLB (px) over sel."""
+    fx = rows[sel, 1] + R // 2 - rec[sel, R * R].astype(np.float64)
+    fy = rows[sel, 2] + R // 2 - rec[sel, R * R + 1].astype(np.float64)
+    rmse = float(np.sqrt(np.mean((fx - truth["x"][sel]) ** 2 + (fy - truth["y"][sel]) ** 2) / 2))
+    ph = float(np.sqrt(np.mean((rows[sel, 6] / truth["photons"][sel] - 1) ** 2)))
+    crlb = float(np.sqrt(np.mean((rows[sel, 9] ** 2 + rows[sel, 10] ** 2) / 2)) / para.PixelSize)
+    return rmse, ph, crlb
+
+
+def learned_measure(args, stream, ctx, para, d_batches, h_batches, rec0, truth0, plain_value, world, dist):
+    """Learned start points + LEARNED_ITERS BFGS iterations + plain refits of
+    the fits the deviance judge rejects + CRLB (qcs_learned_localize_device),
+    on the same device-resident batches as the plain step, WLE pre-pass
+    included; accuracy of plain vs learned on batch 0 against ground truth."""
+    import torch
+    sh = stream.cuda_stream
+    net, train = train_learned_net(para, stream)
+
+    def step(k):
+        net.localize(ctx, d_batches[k % BATCHES].data_ptr(), N_PER_STEP, 0, iters=LEARNED_ITERS, stream=sh)
+
+    for k in range(args.warmup):
+        step(k)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(args.steps):
+        step(k)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = args.steps * N_PER_STEP * world / (ms * 1e-3)
+
+    # accuracy on batch 0: plain and learned rows of the same records
+    ctx.localize_device(d_batches[0].data_ptr(), N_PER_STEP, 0, sh)
+    plain, _ = ctx.read_rows(sh)
+    step(0)
+    learned, _ = ctx.read_rows(sh)
+    refits = net.refits(ctx)
+    both = (plain[:, 0] > 0) & (learned[:, 0] > 0)
+    rp, pp, crlb = fit_accuracy(plain, rec0, truth0, both, para)
+    rl, pl, _ = fit_accuracy(learned, rec0, truth0, both, para)
+
+    # end to end: pinned host records -> device -> learned localization -> rows on the host
+    d_in = torch.empty_like(d_batches[0])
+    e2e_steps = max(3, min(args.steps, 10))
+    for k in range(2):
+        d_in.copy_(h_batches[k], non_blocking=True)
+        net.localize(ctx, d_in.data_ptr(), N_PER_STEP, 0, iters=LEARNED_ITERS, stream=sh)
+        ctx.read_rows(sh)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(e2e_steps):
+        d_in.copy_(h_batches[k % BATCHES], non_blocking=True)
+        net.localize(ctx, d_in.data_ptr(), N_PER_STEP, 0, iters=LEARNED_ITERS, stream=sh)
+        ctx.read_rows(sh)
+    e2e_s = time.perf_counter() - t0
+    net.close()
+    return {
+        "value": value, "unit": UNIT, "ms_per_step": ms / args.steps, "vs_plain": value / plain_value,
+        "iters": LEARNED_ITERS, "refits_per_step": refits,
+        "gpu_launches_per_step": 12,
+        "e2e": {"value": e2e_steps * N_PER_STEP * world / e2e_s, "unit": UNIT,
+                "h2d_bytes_per_step": N_PER_STEP * R * (R + 1) * 2,
+                "d2h_bytes_per_step": N_PER_STEP * 48 + 32,
+                "call": "pinned records -> qcs_learned_localize_device -> qcs_loc_read_rows"},
+        "accuracy": {"records": N_PER_STEP, "compared": int(both.sum()),
+                     "rmse_px": {"plain": rp, "learned": rl}, "photon_rel_rmse": {"plain": pp, "learned": pl},
+                     "crlb_px": crlb, "accepted": {"plain": float((plain[:, 0] > 0).mean()),
+                                                   "learned": float((learned[:, 0] > 0).mean())},
+                     "equal_rmse": bool(rl <= 1.02 * rp),
+                     "basis": "records accepted by both; ground truth of the generator"},
+        "train": train,
+        "network": "64-128-128-8 MLP on the 7x7 pixels (+2 scale features), BF16 operands, FP32 accumulation; "
+                   "inference fused with the features in one tcgen05 kernel",
+    }
+
+
+def profile_learned(n, stream):
+    """Three learned-start localization calls over n records inside the NVTX
+    range "learned" (for ncu --nvtx-include learned/), after training."""
+    import torch
+    from qcstorm_b200 import lib, synth
+    rec, para, _ = synth.gs2d_rois(n, R=R, seed=5)
+    net, _ = train_learned_net(para, stream)
+    d = torch.from_numpy(rec.view(np.int16)).cuda()
+    ctx = lib.LocContext(para, capacity=n)
+    sh = stream.cuda_stream
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("learned")
+    for _ in range(3):
+        net.localize(ctx, d.data_ptr(), n, 0, iters=LEARNED_ITERS, stream=sh)
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    print(json.dumps({"profile_learned": n, "refits": net.refits(ctx)}))
+    ctx.close()
+    net.close()
+    return 0
+
+
 def profile_fit(n):
     """Three launches of the single-emitter fit kernel over n records."""
     import torch
@@ -303,6 +444,9 @@ def main():
                     help="only run the single-emitter fit and CRLB kernels 3 times on N records (for ncu captures)")
     ap.add_argument("--profile-frames", type=int, default=0, metavar="K",
                     help="only run K calls of the whole-frame pipeline (for ncu captures)")
+    ap.add_argument("--profile-learned", type=int, default=0, metavar="N",
+                    help="only train the start-point network and run 3 learned-start calls on N records")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-start measurement")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -324,6 +468,8 @@ def main():
         return profile_fit(args.profile_fit)
     if args.profile_frames:
         return profile_frames(args.profile_frames, stream)
+    if args.profile_learned:
+        return profile_learned(args.profile_learned, stream)
     dist = None
     if world > 1:
         import datetime
@@ -333,8 +479,11 @@ def main():
     # ---- inputs: BATCHES distinct batches resident in HBM, pinned host copies
     d_batches, h_batches = [], []
     para = None
+    rec0 = truth0 = None
     for b in range(BATCHES):
-        rec, para, _ = synth.gs2d_rois(N_PER_STEP, R=R, seed=1000 * rank + b)
+        rec, para, truth = synth.gs2d_rois(N_PER_STEP, R=R, seed=1000 * rank + b)
+        if b == 0:
+            rec0, truth0 = rec, truth
         h = torch.from_numpy(rec.view(np.int16)).pin_memory()
         h_batches.append(h)
         d_batches.append(h.cuda())
@@ -414,6 +563,10 @@ def main():
            "d2h_bytes_per_step": int(rows / e2e_steps) * 48 + 32,
            "call": "qcs_loc_bfgs_mle_localization (pinned host records, WLE on device, synchronous)"}
 
+    learned = None
+    if not args.no_learned:
+        learned = learned_measure(args, stream, ctx, para, d_batches, h_batches, rec0, truth0, value, world, dist)
+
     frames = None
     if not args.no_frames:
         frames = frame_pipeline(stream, steps=min(max(args.steps // 40, 5), 40), warmup=3)
@@ -436,7 +589,7 @@ def main():
                          "kernel_ms": fit_ms,
                          "algorithmic": "%d px-evals x %d MUFU per fit; peak = measured __expf/__logf rate" % (
                              PX_EVALS_PER_FIT, MUFU_PER_PX_EVAL)},
-            "cpu_baseline": cpu, "clocks": clocks, "frames": frames,
+            "cpu_baseline": cpu, "clocks": clocks, "learned": learned, "frames": frames,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -309,6 +309,13 @@ int qcs_wle_estimate_device(qcs_loc_data *c, const uint16_t *d_rois, int n, cons
  * loc_type: QCS_LOCTYPE_*; rows: n x 12 in d_loc, CRLB columns left 0. */
 int qcs_fit_single_device(int loc_type, const qcs_loc_para *p, const uint16_t *d_rois, const float *d_wle, int n,
                           float *d_loc, void *stream);
+/* The fit of qcs_fit_single_device with `lanes` lanes per ROI (8; also 4 or
+ * 16 for GS2D 7x7): the same rows bit for bit, with about half the latency
+ * per ROI, for short batches.  ROI sizes: GS2D 7, 9, 11, 13 and AS3D 7, 9, 11
+ * (the sizes whose pixel-distance rounding is fixed in the source);
+ * QCS_ERR_ARG otherwise. */
+int qcs_fit_single_group_device(int loc_type, const qcs_loc_para *p, const uint16_t *d_rois, const float *d_wle,
+                                int n, float *d_loc, int lanes, void *stream);
 /* LDLocData_TypeDef::LocPrecCalc_GaussianCRLB (bfgs_top.h:90,
  * LocPrecCalc_GaussianCRLB.cu:23-40): CRLB columns of n device rows. */
 int qcs_crlb_device(const qcs_loc_para *p, float *d_loc, int n, void *stream);

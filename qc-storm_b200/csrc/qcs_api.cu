@@ -59,6 +59,8 @@ struct qcs_loc_data {
     float *h_loc = nullptr;
     int *h_counters = nullptr;
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;  // high-priority stream for work overlapped with the main stream
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int valid = 0;
     float ratios[7] = {0, 0, 0, 0, 0, 0, 0};
 };
@@ -119,6 +121,9 @@ int qcs_loc_deinit(qcs_loc_data *c) {
     cudaFreeHost(c->h_loc);
     cudaFreeHost(c->h_counters);
     if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->side) cudaStreamDestroy(c->side);
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
     delete c;
     return QCS_OK;
 }
@@ -153,6 +158,11 @@ int qcs_loc_init_capacity(const qcs_loc_para *p, int capacity, qcs_loc_data **ou
     if (e == cudaSuccess) e = cudaMallocHost((void **)&c->h_loc, (size_t)c->max_rows * QCS_OUT_PARA_NUM * sizeof(float));
     if (e == cudaSuccess) e = cudaMallocHost((void **)&c->h_counters, qcs::kCntNum * sizeof(int));
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    int prio_least = 0, prio_greatest = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest);
+    if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&c->side, cudaStreamNonBlocking, prio_greatest);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         qcs_loc_deinit(c);
         return fail(e == cudaErrorMemoryAllocation ? QCS_ERR_NOMEM : QCS_ERR_CUDA, "qcs_loc_init", e);
@@ -274,11 +284,24 @@ int qcs_fit_from_start_device(qcs_loc_data *c, const uint16_t *d_rois, const flo
     // plain refit of the flagged records
     QCS_CUDA(qcs::launch_flag_queue(c->st.to2e, n, c->st.q_single, c->st.counters + qcs::kCntSingle, s),
              "refit queue");
+    // The plain refits (a short, latency-bound queue) and their CRLB run on
+    // the high-priority side stream while the main stream computes the CRLB
+    // of every other row; the two touch disjoint rows.
+    QCS_CUDA(cudaEventRecord(c->ev_fork, s), "fork");
+    QCS_CUDA(cudaStreamWaitEvent(c->side, c->ev_fork, 0), "fork");
     f.q = qcs::Queue{c->st.q_single, c->st.counters + qcs::kCntSingle, 0};
-    QCS_CUDA(qcs::launch_fit(qcs::kGS2D, 7, f), "plain refit");
+    f.stream = c->side;
+    QCS_CUDA(qcs::launch_fit_group(qcs::kGS2D, 7, 8, f), "plain refit");
+    QCS_CUDA(qcs::launch_crlb(c->d_loc, c->st.counters + qcs::kCntSingle, 0, n, p->LocType, p->ReadNoise_e, p->QE,
+                              p->PixelSize, c->side, c->st.q_single, nullptr),
+             "refit CRLB");
+    QCS_CUDA(cudaEventRecord(c->ev_join, c->side), "join");
     learned_counters_kernel<<<1, 1, 0, s>>>(c->st, n);
     QCS_CUDA(cudaGetLastError(), "counters");
-    QCS_CUDA(qcs::launch_crlb(c->d_loc, nullptr, n, n, p->LocType, p->ReadNoise_e, p->QE, p->PixelSize, s), "CRLB");
+    QCS_CUDA(qcs::launch_crlb(c->d_loc, nullptr, n, n, p->LocType, p->ReadNoise_e, p->QE, p->PixelSize, s, nullptr,
+                              c->st.to2e),
+             "CRLB");
+    QCS_CUDA(cudaStreamWaitEvent(s, c->ev_join, 0), "join");
     return QCS_OK;
 }
 
@@ -439,6 +462,34 @@ int qcs_fit_single_device(int loc_type, const qcs_loc_para *p, const uint16_t *d
     f.para = qcs::core_para(q);
     f.stream = static_cast<cudaStream_t>(stream);
     QCS_CUDA(qcs::launch_fit(loc_type == QCS_LOCTYPE_AS3D ? qcs::kAS3D : qcs::kGS2D, p->ROISize, f), "fit launch");
+    return QCS_OK;
+}
+
+int qcs_fit_single_group_device(int loc_type, const qcs_loc_para *p, const uint16_t *d_rois, const float *d_wle,
+                                int n, float *d_loc, int lanes, void *stream) {
+    int st = check_para(p, false);
+    if (st) return st;
+    if (n < 0) return fail(QCS_ERR_ARG, "negative ROI count");
+    const int kind = loc_type == QCS_LOCTYPE_AS3D ? qcs::kAS3D : qcs::kGS2D;
+    if (!qcs::group_fit_supported(kind, p->ROISize))
+        return fail(QCS_ERR_ARG, "group fit: GS2D 7/9/11/13 or AS3D 7/9/11 ROIs");
+    if (lanes != 8 && !((lanes == 4 || lanes == 16) && kind == qcs::kGS2D && p->ROISize == 7))
+        return fail(QCS_ERR_ARG, "lanes per ROI: 8, or 4 / 16 for GS2D 7x7");
+    if (n == 0) return QCS_OK;
+    if (!d_rois || !d_wle || !d_loc) return fail(QCS_ERR_ARG, "null pointer");
+    qcs::FitLaunch f;
+    f.rois = d_rois;
+    f.wle = d_wle;
+    f.q = qcs::Queue{nullptr, nullptr, n};
+    f.max_count = n;
+    f.loc = d_loc;
+    f.to2e = nullptr;
+    f.mo = qcs::MultiOut{nullptr, nullptr};
+    qcs_loc_para q = *p;
+    q.MultiEmitterFitEn = 0;
+    f.para = qcs::core_para(q);
+    f.stream = static_cast<cudaStream_t>(stream);
+    QCS_CUDA(qcs::launch_fit_group(kind, p->ROISize, lanes, f), "group fit launch");
     return QCS_OK;
 }
 

@@ -66,13 +66,16 @@ __device__ __forceinline__ float second_diff(float fp, float f0, float fn) {
 // shared memory, [entry][thread].
 template <int G, int TPB>
 __global__ void __launch_bounds__(TPB) crlb_kernel(float *__restrict__ loc, const int *__restrict__ n_dev, int n,
+                                                   const int *__restrict__ ids, const uint8_t *__restrict__ skip,
                                                    float ReadNoise_e, float QE, float PixelSize) {
     enum { H = G / 2, Q = H + 1 };
     using S = CrlbSites<G>;
     __shared__ float sM[Q * Q][TPB], sLM[Q * Q][TPB], sTX[Q * G][TPB], sTY[G * Q][TPB];
     const int rows = n_dev ? *n_dev : n;
-    const int gid = threadIdx.x + blockDim.x * blockIdx.x;
-    if (gid >= rows) return;
+    const int slot = threadIdx.x + blockDim.x * blockIdx.x;
+    if (slot >= rows) return;
+    const int gid = ids ? ids[slot] : slot;
+    if (skip && skip[gid]) return;
     const int t = threadIdx.x;
     float *r = loc + (size_t)gid * 12;
     const float TotalPhoton_e = __fmul_rn(r[QCS_POS_TPHO], QE);
@@ -158,14 +161,16 @@ __global__ void __launch_bounds__(TPB) crlb_kernel(float *__restrict__ loc, cons
 }  // namespace
 
 cudaError_t launch_crlb(float *loc, const int *n_dev, int n, int max_rows, int loc_type, float ReadNoise_e, float QE,
-                        float PixelSize, cudaStream_t s) {
+                        float PixelSize, cudaStream_t s, const int *ids, const uint8_t *skip) {
     if (max_rows <= 0) return cudaSuccess;
     if (loc_type != QCS_LOCTYPE_AS3D) {
         constexpr int tpb = 64;
-        crlb_kernel<9, tpb><<<(max_rows + tpb - 1) / tpb, tpb, 0, s>>>(loc, n_dev, n, ReadNoise_e, QE, PixelSize);
+        crlb_kernel<9, tpb><<<(max_rows + tpb - 1) / tpb, tpb, 0, s>>>(loc, n_dev, n, ids, skip, ReadNoise_e, QE,
+                                                                       PixelSize);
     } else {
         constexpr int tpb = 32;
-        crlb_kernel<15, tpb><<<(max_rows + tpb - 1) / tpb, tpb, 0, s>>>(loc, n_dev, n, ReadNoise_e, QE, PixelSize);
+        crlb_kernel<15, tpb><<<(max_rows + tpb - 1) / tpb, tpb, 0, s>>>(loc, n_dev, n, ids, skip, ReadNoise_e, QE,
+                                                                        PixelSize);
     }
     return cudaGetLastError();
 }

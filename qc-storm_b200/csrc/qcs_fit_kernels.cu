@@ -31,10 +31,11 @@ namespace {
 
 constexpr int kTPB = 64;  // ROIs (threads) per block
 
-// One thread's view of the staged photoelectron values (element k at p[k * kTPB]).
+// One ROI's staged photoelectron values: pixel k at p[k * ld].x.
 struct PixView {
     const float2 *p;
-    __device__ __forceinline__ float operator[](int i) const { return p[i].x; }
+    int ld;
+    __device__ __forceinline__ float operator[](int k) const { return p[k * ld].x; }
 };
 
 template <int R, int KIND>
@@ -90,10 +91,10 @@ __device__ __forceinline__ void edge_means(const PixView &img, float &Mean1, flo
     Mean4 = 0;
 #pragma unroll
     for (int cnt = 0; cnt < R; cnt++) {
-        Mean1 += img[(cnt * R + 0) * kTPB];
-        Mean2 += img[(cnt * R + R - 1) * kTPB];
-        Mean3 += img[(0 * R + cnt) * kTPB];
-        Mean4 += img[((R - 1) * R + cnt) * kTPB];
+        Mean1 += img[cnt * R + 0];
+        Mean2 += img[cnt * R + R - 1];
+        Mean3 += img[0 * R + cnt];
+        Mean4 += img[(R - 1) * R + cnt];
     }
 }
 
@@ -119,7 +120,7 @@ __device__ __forceinline__ void block_starts(const PixView &img, int nstart, flo
         const int XBias = StartPos[cnt % 3];
         const int YBias = StartPos[cnt / 3];
         for (int r = 0; r < SumROILen; r++)
-            for (int c = 0; c < SumROILen; c++) SumDat_t += img[((r + YBias) * R + c + XBias) * kTPB];
+            for (int c = 0; c < SumROILen; c++) SumDat_t += img[(r + YBias) * R + c + XBias];
         SumData[cnt] = SumDat_t;
     }
     SumData[9 / 2] = 0;
@@ -145,46 +146,22 @@ __device__ __forceinline__ float zpoly(const CorePara &c, float SigmaDif) {
 }
 
 // ------------------------------------------------------- single emitter ---
-template <int R, int KIND, int DIST = ArithSpec<KIND, R>::DIST, int MASK = ArithSpec<KIND, R>::MASK>
-__global__ void __launch_bounds__(kTPB) fit_single_kernel(const uint16_t *__restrict__ rois,
-                                                          const float *__restrict__ wle, Queue q,
-                                                          float *__restrict__ loc, uint8_t *__restrict__ to2e,
-                                                          CorePara c) {
-    typedef SmemLayout<R, KIND> L;
-    enum { P = KindTraits<KIND>::P, PIX = R * R, WHOLE = R * (R + 1), ROISize_Half = R / 2 };
-    extern __shared__ float smem[];
-    const int n = queue_len(q);
-    const int base = blockIdx.x * kTPB;
-    if (base >= n) return;
-    const int cnt = min(kTPB, n - base);
-    float2 *s_img = reinterpret_cast<float2 *>(smem + L::IMG);
-    stage_rois<R>(s_img, rois, q, base, cnt, c.Offset, c.KAdc);
-    __syncthreads();
-    const int tid = threadIdx.x;
-    if (tid >= cnt) return;
+// Weighted-MLE mask widths and accept bound of one single-emitter ROI.
+struct SinglePrep {
+    float WLE_SigmaX, WLE_SigmaY;
+    int MoleculeType;
+    float Simga_Max_Th;
+};
 
-    const int CurFluoID = queue_at(q, base + tid);
-    const PixView img{s_img + tid};
-    float *w = smem + L::W + tid;
-    float *D = smem + L::D + tid;
-    const uint16_t *hdr = rois + (size_t)CurFluoID * WHOLE + PIX;
-    const int XOffset = hdr[0];
-    const int YOffset = hdr[1];
-    const int CurFrame = hdr[2] + 65536 * hdr[3];
-    const float *pw = wle + (size_t)CurFluoID * QCS_WLE_PARA_NUM;
-
-    float Ininf[P];
-    const RoiRef roi{s_img + tid, w, kTPB};
-    float row[12];
-    bool accepted;
-    float CurSNR;
-    int IsFittingValid;
-
+// PreEstimation_GS2D / PreEstimation_AS3D and the WLE mask widths: the start
+// point Ininf of the fit from the ROI's edge means and centre pixel.
+template <int R, int KIND>
+__device__ __forceinline__ SinglePrep single_prefit(const PixView &img, const float *pw, const CorePara &c,
+                                                    float *Ininf) {
+    SinglePrep sp;
+    sp.Simga_Max_Th = R / 1.5f / 2.35f;
+    if (c.MultiEmitterFitEn) sp.Simga_Max_Th = R / 2.0f / 2.35f;
     if (KIND == kGS2D) {
-        const float XYLBound = R / 2.0f - 1.5f;
-        const float XYUBound = R / 2.0f + 1.5f;
-        float Simga_Max_Th = R / 1.5f / 2.35f;
-        if (c.MultiEmitterFitEn) Simga_Max_Th = R / 2.0f / 2.35f;
         float SigmaL = pw[1], SigmaR = pw[2], SigmaU = pw[3], SigmaD = pw[4];
         const int MoleculeType = pw[5];
         SigmaL = fminf(SigmaL, SigmaR);
@@ -199,7 +176,7 @@ __global__ void __launch_bounds__(kTPB) fit_single_kernel(const uint16_t *__rest
             Mean1 = fminf(Mean1, Mean2);
             Mean3 = fminf(Mean3, Mean4);
             const float Bkg = (Mean1 + Mean3) / 2 / R;
-            const float Amp = img[(CenterPos * R + CenterPos) * kTPB] - Bkg;
+            const float Amp = img[CenterPos * R + CenterPos] - Bkg;
             const float SigmaX = WLE_SigmaX;
             const float ParaSigma1 = (1.0f / (2.0f * SigmaX * SigmaX));
             Ininf[0] = Amp * rAScalFactor;
@@ -213,9 +190,58 @@ __global__ void __launch_bounds__(kTPB) fit_single_kernel(const uint16_t *__rest
             WLE_SigmaX = fminf(WLE_SigmaX, R / 2.0f / 2.35f);
         }
         if (c.WLEEn == 0 && MoleculeType != QCS_MOLECULE_MULTIFIT) WLE_SigmaX = R;
-        wle_weights<R, MASK>(w, kTPB, WLE_SigmaX, WLE_SigmaX, MoleculeType);
-        mle_fit<R, kGS2D, DIST>(roi, Ininf, D, kTPB);
+        sp.WLE_SigmaX = WLE_SigmaX;
+        sp.WLE_SigmaY = WLE_SigmaX;
+        sp.MoleculeType = MoleculeType;
+    } else {  // kAS3D
+        const float SigmaL = pw[1], SigmaR = pw[2], SigmaU = pw[3], SigmaD = pw[4];
+        const int MoleculeType = pw[5];
+        float WLE_SigmaX = fminf(SigmaL, SigmaR);
+        float WLE_SigmaY = fminf(SigmaU, SigmaD);
+        // PreEstimation_AS3D
+        {
+            const int CenterPos = R / 2;
+            float Mean1, Mean2, Mean3, Mean4;
+            edge_means<R>(img, Mean1, Mean2, Mean3, Mean4);
+            Mean1 = fminf(Mean1, Mean2);
+            Mean3 = fminf(Mean3, Mean4);
+            const float Bkg = (Mean1 + Mean3) / 2 / R;
+            const float Amp = img[CenterPos * R + CenterPos] - Bkg;
+            const float SigmaX = WLE_SigmaX;
+            const float SigmaY = WLE_SigmaY;
+            const float SigmaX1 = rSScalFactor * (0.5f / (SigmaX * SigmaX));
+            const float SigmaY1 = rSScalFactor * (0.5f / (SigmaY * SigmaY));
+            Ininf[0] = Amp * rAScalFactor;
+            Ininf[1] = (float)CenterPos + 0.5f;
+            Ininf[2] = (float)CenterPos + 0.5f;
+            Ininf[3] = SigmaX1;
+            Ininf[4] = SigmaY1;
+            Ininf[5] = Bkg * rBScalFactor;
+        }
+        if (MoleculeType != QCS_MOLECULE_MLEFIT) {
+            WLE_SigmaX = fminf(WLE_SigmaX, R / 1.6f / 2.35f);
+            WLE_SigmaY = fminf(WLE_SigmaY, R / 1.6f / 2.35f);
+        }
+        if (c.WLEEn == 0 && MoleculeType != QCS_MOLECULE_MULTIFIT) {
+            WLE_SigmaX = R;
+            WLE_SigmaY = R;
+        }
+        sp.WLE_SigmaX = WLE_SigmaX;
+        sp.WLE_SigmaY = WLE_SigmaY;
+        sp.MoleculeType = MoleculeType;
+    }
+    return sp;
+}
 
+// Output row and accept decision of a finished single-emitter fit.
+template <int R, int KIND>
+__device__ __forceinline__ void single_finish(const float *Ininf, const CorePara &c, float Simga_Max_Th, int XOffset,
+                                              int YOffset, int CurFrame, float (&row)[12], bool &accepted,
+                                              float &CurSNR, int &IsFittingValid) {
+    enum { ROISize_Half = R / 2 };
+    if (KIND == kGS2D) {
+        const float XYLBound = R / 2.0f - 1.5f;
+        const float XYUBound = R / 2.0f + 1.5f;
         const float PeakPhoton = Ininf[0] * QCS_ASCALE / c.QE;
         const float Background = Ininf[4] * QCS_BSCALE / c.QE;
         float FittedXPos = Ininf[1];
@@ -246,44 +272,7 @@ __global__ void __launch_bounds__(kTPB) fit_single_kernel(const uint16_t *__rest
     } else {  // kAS3D
         const float XYLBound = R / 2.0f - 2.5f;
         const float XYUBound = R / 2.0f + 2.5f;
-        float Simga_Max_Th = R / 1.5f / 2.35f;
-        if (c.MultiEmitterFitEn) Simga_Max_Th = R / 2.0f / 2.35f;
         const float Simga_Min_Th = 0.8f;
-        const float SigmaL = pw[1], SigmaR = pw[2], SigmaU = pw[3], SigmaD = pw[4];
-        const int MoleculeType = pw[5];
-        float WLE_SigmaX = fminf(SigmaL, SigmaR);
-        float WLE_SigmaY = fminf(SigmaU, SigmaD);
-        // PreEstimation_AS3D
-        {
-            const int CenterPos = R / 2;
-            float Mean1, Mean2, Mean3, Mean4;
-            edge_means<R>(img, Mean1, Mean2, Mean3, Mean4);
-            Mean1 = fminf(Mean1, Mean2);
-            Mean3 = fminf(Mean3, Mean4);
-            const float Bkg = (Mean1 + Mean3) / 2 / R;
-            const float Amp = img[(CenterPos * R + CenterPos) * kTPB] - Bkg;
-            const float SigmaX = WLE_SigmaX;
-            const float SigmaY = WLE_SigmaY;
-            const float SigmaX1 = rSScalFactor * (0.5f / (SigmaX * SigmaX));
-            const float SigmaY1 = rSScalFactor * (0.5f / (SigmaY * SigmaY));
-            Ininf[0] = Amp * rAScalFactor;
-            Ininf[1] = (float)CenterPos + 0.5f;
-            Ininf[2] = (float)CenterPos + 0.5f;
-            Ininf[3] = SigmaX1;
-            Ininf[4] = SigmaY1;
-            Ininf[5] = Bkg * rBScalFactor;
-        }
-        if (MoleculeType != QCS_MOLECULE_MLEFIT) {
-            WLE_SigmaX = fminf(WLE_SigmaX, R / 1.6f / 2.35f);
-            WLE_SigmaY = fminf(WLE_SigmaY, R / 1.6f / 2.35f);
-        }
-        if (c.WLEEn == 0 && MoleculeType != QCS_MOLECULE_MULTIFIT) {
-            WLE_SigmaX = R;
-            WLE_SigmaY = R;
-        }
-        wle_weights<R, MASK>(w, kTPB, WLE_SigmaX, WLE_SigmaY, MoleculeType);
-        mle_fit<R, kAS3D, DIST>(roi, Ininf, D, kTPB);
-
         float PeakPhoton = Ininf[0] * QCS_ASCALE;
         float Background = Ininf[5] * QCS_BSCALE;
         float FittedXPos = Ininf[1];
@@ -320,21 +309,149 @@ __global__ void __launch_bounds__(kTPB) fit_single_kernel(const uint16_t *__rest
         row[8] = CurSNR;
         row[11] = CurFrame;
     }
-    if (accepted) {
-        row[9] = 0.0f;
-        row[10] = 0.0f;
+    row[9] = 0.0f;
+    row[10] = 0.0f;
+}
+
+template <int R, int KIND, int DIST = ArithSpec<KIND, R>::DIST, int MASK = ArithSpec<KIND, R>::MASK>
+__global__ void __launch_bounds__(kTPB) fit_single_kernel(const uint16_t *__restrict__ rois,
+                                                          const float *__restrict__ wle, Queue q,
+                                                          float *__restrict__ loc, uint8_t *__restrict__ to2e,
+                                                          CorePara c) {
+    typedef SmemLayout<R, KIND> L;
+    enum { P = KindTraits<KIND>::P, PIX = R * R, WHOLE = R * (R + 1) };
+    extern __shared__ float smem[];
+    const int n = queue_len(q);
+    const int base = blockIdx.x * kTPB;
+    if (base >= n) return;
+    const int cnt = min(kTPB, n - base);
+    float2 *s_img = reinterpret_cast<float2 *>(smem + L::IMG);
+    stage_rois<R>(s_img, rois, q, base, cnt, c.Offset, c.KAdc);
+    __syncthreads();
+    const int tid = threadIdx.x;
+    if (tid >= cnt) return;
+
+    const int CurFluoID = queue_at(q, base + tid);
+    const PixView img{s_img + tid, kTPB};
+    float *w = smem + L::W + tid;
+    float *D = smem + L::D + tid;
+    const uint16_t *hdr = rois + (size_t)CurFluoID * WHOLE + PIX;
+    const int XOffset = hdr[0];
+    const int YOffset = hdr[1];
+    const int CurFrame = hdr[2] + 65536 * hdr[3];
+    const float *pw = wle + (size_t)CurFluoID * QCS_WLE_PARA_NUM;
+
+    float Ininf[P];
+    const SinglePrep sp = single_prefit<R, KIND>(img, pw, c, Ininf);
+    wle_weights<R, MASK>(w, kTPB, sp.WLE_SigmaX, sp.WLE_SigmaY, sp.MoleculeType);
+    mle_fit<R, KIND, DIST>(RoiRef{s_img + tid, w, kTPB}, Ininf, D, kTPB);
+    float row[12];
+    bool accepted;
+    float CurSNR;
+    int IsFittingValid;
+    single_finish<R, KIND>(Ininf, c, sp.Simga_Max_Th, XOffset, YOffset, CurFrame, row, accepted, CurSNR,
+                           IsFittingValid);
+    if (accepted)
         store_row(loc, CurFluoID, row);
-    } else {
+    else
         zero_row(loc, CurFluoID);
+    if (to2e) to2e[CurFluoID] = (!accepted && c.MultiEmitterFitEn && IsFittingValid && (CurSNR > 6.0f)) ? 1 : 0;
+}
+
+// The same fit with G lanes per ROI (GroupEval): bit for bit the rows of
+// fit_single_kernel, with about half the latency per ROI and about twice the
+// instructions.  For short queues (refits, small calls), where one thread
+// per ROI leaves the GPU mostly idle and the launch lasts as long as one
+// thread's serial fit.  Each ROI's pixels, weights and loss terms are
+// contiguous in shared memory (rows padded to 4 floats); D per lane.
+constexpr int kGroupTPB = 128;
+
+template <int R, int KIND>
+struct GroupLayout {
+    enum {
+        P = KindTraits<KIND>::P,
+        PIX = R * R,
+        PIXP = (PIX + 3) / 4 * 4,
+    };
+    template <int G>
+    struct At {
+        enum {
+            SLOTS = kGroupTPB / G,
+            IMG = 0,                       // float2 per pixel
+            W = IMG + 2 * PIXP * SLOTS,    // floats
+            PART = W + PIXP * SLOTS,
+            D = PART + PIXP * SLOTS,
+            TOTAL = D + P * P * kGroupTPB,
+        };
+    };
+};
+
+template <int R, int KIND, int G, int DIST = ArithSpec<KIND, R>::DIST, int MASK = ArithSpec<KIND, R>::MASK>
+__global__ void __launch_bounds__(kGroupTPB) fit_single_group_kernel(const uint16_t *__restrict__ rois,
+                                                                     const float *__restrict__ wle, Queue q,
+                                                                     float *__restrict__ loc,
+                                                                     uint8_t *__restrict__ to2e, CorePara c) {
+    typedef GroupLayout<R, KIND> GL;
+    typedef typename GL::template At<G> L;
+    enum { P = KindTraits<KIND>::P, PIX = R * R, PIXP = GL::PIXP, WHOLE = R * (R + 1), SLOTS = L::SLOTS };
+    static_assert(G == 4 || G == 8 || G == 16, "lanes per ROI");
+    static_assert(DIST != kCompiler, "the group sums equal the thread kernel's only for a fixed distance rounding");
+    extern __shared__ __align__(16) float smem[];
+    const int n = queue_len(q);
+    const int base = blockIdx.x * SLOTS;
+    if (base >= n) return;
+    const int cnt = min(SLOTS, n - base);
+    float2 *s_img = reinterpret_cast<float2 *>(smem + L::IMG);
+    for (int idx = threadIdx.x; idx < cnt * PIX; idx += kGroupTPB) {
+        const int slot = idx / PIX;
+        const int k = idx - slot * PIX;
+        const int id = queue_at(q, base + slot);
+        const uint16_t u = __ldg(rois + (size_t)id * WHOLE + k);
+        const float pixval = fmaxf((u - c.Offset) * c.KAdc, 1.0f);
+        s_img[slot * PIXP + k] = make_float2(pixval, __logf(pixval));
     }
+    __syncthreads();
+    const int slot = threadIdx.x / G;
+    const int lane = threadIdx.x % G;
+    if (slot >= cnt) return;
+    const unsigned mask = ((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1));
+
+    const int CurFluoID = queue_at(q, base + slot);
+    const float2 *img2 = s_img + slot * PIXP;
+    float *w = smem + L::W + slot * PIXP;
+    float *part = smem + L::PART + slot * PIXP;
+    float *D = smem + L::D + threadIdx.x;
+    const uint16_t *hdr = rois + (size_t)CurFluoID * WHOLE + PIX;
+    const int XOffset = hdr[0];
+    const int YOffset = hdr[1];
+    const int CurFrame = hdr[2] + 65536 * hdr[3];
+    const float *pw = wle + (size_t)CurFluoID * QCS_WLE_PARA_NUM;
+
+    float Ininf[P];
+    const SinglePrep sp = single_prefit<R, KIND>(PixView{img2, 1}, pw, c, Ininf);
+    if (lane == 0) wle_weights<R, MASK>(w, 1, sp.WLE_SigmaX, sp.WLE_SigmaY, sp.MoleculeType);
+    __syncwarp(mask);
+    bfgs_fit<P, KindTraits<KIND>::IT>(GroupEval<R, KIND, DIST, G>{img2, w, part, lane, mask}, Ininf, D, kGroupTPB);
+    float row[12];
+    bool accepted;
+    float CurSNR;
+    int IsFittingValid;
+    single_finish<R, KIND>(Ininf, c, sp.Simga_Max_Th, XOffset, YOffset, CurFrame, row, accepted, CurSNR,
+                           IsFittingValid);
+    if (lane != 0) return;
+    if (accepted)
+        store_row(loc, CurFluoID, row);
+    else
+        zero_row(loc, CurFluoID);
     if (to2e) to2e[CurFluoID] = (!accepted && c.MultiEmitterFitEn && IsFittingValid && (CurSNR > 6.0f)) ? 1 : 0;
 }
 
 // ---------------------------------------------- learned-start GS2D fit ---
 // The GS2D fit of fit_single_kernel started from a given point (peak e-,
 // x, y in ROI pixels, sigma, background e-) instead of the centre / edge-mean
-// pre-estimate, with ITERS BFGS iterations instead of 8.  The same weighted
-// loss, line search, accept rules and output row.  refit[id] = 1 when the fit
+// pre-estimate, with ITERS BFGS iterations instead of 8 and the analytic
+// gradient (AnalyticEvalGS2D) instead of the central difference.  The same
+// weighted loss, line search, accept rules and output row.  refit[id] = 1 when the fit
 // is not accepted or when its unweighted Poisson deviance
 // 2 sum(mu - n - n ln(mu / n)) exceeds dev_th: those ROIs are refitted by the
 // plain kernel.
@@ -384,7 +501,7 @@ __global__ void __launch_bounds__(kTPB) fit_learned_kernel(const uint16_t *__res
     Ininf[2] = st[2];
     Ininf[3] = (0.5f / (st[3] * st[3])) * rSScalFactor;
     Ininf[4] = st[4] * rBScalFactor;
-    mle_fit<R, kGS2D, DIST, ArithSpec<kGS2D, R>::SUM2, ITERS>(roi, Ininf, D, kTPB);
+    bfgs_fit<P, ITERS>(AnalyticEvalGS2D<R, DIST>{roi}, Ininf, D, kTPB);
 
     const float PeakPhoton = Ininf[0] * QCS_ASCALE / c.QE;
     const float Background = Ininf[4] * QCS_BSCALE / c.QE;
@@ -477,7 +594,7 @@ __global__ void __launch_bounds__(kTPB) fit_multi_kernel(const uint16_t *__restr
 
     const int slot = base + tid;
     const int CurFluoID = queue_at(q, slot);
-    const PixView img{s_img + tid};
+    const PixView img{s_img + tid, kTPB};
     float *w = smem + L::W + tid;
     float *D = smem + L::D + tid;
     const uint16_t *hdr = rois + (size_t)CurFluoID * WHOLE + PIX;
@@ -502,7 +619,7 @@ __global__ void __launch_bounds__(kTPB) fit_multi_kernel(const uint16_t *__restr
             Mean3 = fminf(Mean3, Mean4);
             Mean1 = fminf(Mean1, Mean3);
             const float Bkg = Mean1 / R;
-            const float Amp = img[(ROISize_Half * R + ROISize_Half) * kTPB] - Bkg;
+            const float Amp = img[ROISize_Half * R + ROISize_Half] - Bkg;
             const float SigmaX = R / 2.2f / 2.35f;
             const float SigmaX1 = (1.0f / (2.0f * SigmaX * SigmaX));
             float xs[1], ys[1];
@@ -526,7 +643,7 @@ __global__ void __launch_bounds__(kTPB) fit_multi_kernel(const uint16_t *__restr
         Mean1 = fminf(Mean1, Mean2);
         Mean3 = fminf(Mean3, Mean4);
         const float Bkg = (Mean1 + Mean3) / 2 / R;
-        const float Amp = img[(ROISize_Half * R + ROISize_Half) * kTPB] - Bkg;
+        const float Amp = img[ROISize_Half * R + ROISize_Half] - Bkg;
         const float SigmaX = R / 2.2f / 2.35f;
         const float SigmaX1 = (1.0f / (2.0f * SigmaX * SigmaX));
         float xs[2], ys[2];
@@ -549,7 +666,7 @@ __global__ void __launch_bounds__(kTPB) fit_multi_kernel(const uint16_t *__restr
         Mean1 = fminf(Mean1, Mean2);
         Mean3 = fminf(Mean3, Mean4);
         const float Bkg = (Mean1 + Mean3) / 2 / R;
-        const float Amp = img[(ROISize_Half * R + ROISize_Half) * kTPB] - Bkg;
+        const float Amp = img[ROISize_Half * R + ROISize_Half] - Bkg;
         const float SigmaX = R / 2.2f / 2.35f;
         const float SigmaY = R / 2.2f / 2.35f;
         const float SigmaX1 = rSScalFactor * (0.5f / (SigmaX * SigmaX));
@@ -702,6 +819,19 @@ cudaError_t launch_single(const FitLaunch &a) {
     return cudaGetLastError();
 }
 
+template <int R, int KIND, int G>
+cudaError_t launch_single_group(const FitLaunch &a) {
+    typedef typename GroupLayout<R, KIND>::template At<G> L;
+    const size_t smem = L::TOTAL * sizeof(float);
+    auto k = fit_single_group_kernel<R, KIND, G>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const int grid = (a.max_count + L::SLOTS - 1) / L::SLOTS;
+    if (grid == 0) return cudaSuccess;
+    k<<<grid, kGroupTPB, smem, a.stream>>>(a.rois, a.wle, a.q, a.loc, a.to2e, a.para);
+    return cudaGetLastError();
+}
+
 template <int R, int KIND>
 cudaError_t launch_multi(const FitLaunch &a) {
     const size_t smem = SmemLayout<R, KIND>::TOTAL * sizeof(float);
@@ -734,6 +864,34 @@ cudaError_t launch_flag_queue(const uint8_t *flags, int n, int *ids, int *count,
     if (e != cudaSuccess || n <= 0) return e;
     flag_queue_kernel<<<(n + 255) / 256, 256, 0, s>>>(flags, n, ids, count);
     return cudaGetLastError();
+}
+
+// Sizes whose pixel distance is written with an explicit contraction
+// (ArithSpec DIST != kCompiler): there the group kernel's per-pixel terms are
+// the thread kernel's bit for bit.  Where nvcc chooses the contraction from
+// the surrounding code (GS2D / AS3D 5x5, 15x15, 17x17, AS3D 13x13) the two
+// kernels' choices differ, so those sizes are not offered.
+bool group_fit_supported(int kind, int R) {
+    if (kind == kGS2D) return R == 7 || R == 9 || R == 11 || R == 13;
+    if (kind == kAS3D) return R == 7 || R == 9 || R == 11;
+    return false;
+}
+
+cudaError_t launch_fit_group(int kind, int R, int lanes, const FitLaunch &a) {
+    if (!group_fit_supported(kind, R)) return cudaErrorInvalidValue;
+    const bool gs = kind == kGS2D;
+    if (lanes == 4 || lanes == 16) {
+        if (!gs || R != 7) return cudaErrorInvalidValue;
+        return lanes == 4 ? launch_single_group<7, kGS2D, 4>(a) : launch_single_group<7, kGS2D, 16>(a);
+    }
+    if (lanes != 8) return cudaErrorInvalidValue;
+    switch (R) {
+    case 7: return gs ? launch_single_group<7, kGS2D, 8>(a) : launch_single_group<7, kAS3D, 8>(a);
+    case 9: return gs ? launch_single_group<9, kGS2D, 8>(a) : launch_single_group<9, kAS3D, 8>(a);
+    case 11: return gs ? launch_single_group<11, kGS2D, 8>(a) : launch_single_group<11, kAS3D, 8>(a);
+    case 13: return launch_single_group<13, kGS2D, 8>(a);
+    }
+    return cudaErrorInvalidValue;
 }
 
 // ROI sizes: odd 5..17 for single emitter, 5..13 for multi emitter (the

@@ -328,12 +328,192 @@ __device__ __forceinline__ void gradient(const RoiRef &roi, const float *Ininf, 
         numerical_gradient<R, KIND, DIST, SUM2>(roi, Ininf, grad);
 }
 
+// Loss and gradient of one ROI evaluated by its own thread.
+template <int R, int KIND, int DIST, int SUM2>
+struct ThreadEval {
+    RoiRef roi;
+    __device__ __forceinline__ float loss(float *x) const { return qcs::loss<R, KIND, DIST, SUM2>(roi, x); }
+    __device__ __forceinline__ void gradient(const float *x, float *g) const {
+        qcs::gradient<R, KIND, DIST, SUM2>(roi, x, g);
+    }
+};
+
+// GS2D loss of ThreadEval with the analytic gradient in one pass over the
+// pixels (learned-start fits; the reference's fits use the central
+// difference).  With mu = 128 A e + 64 B, e = exp(-0.1 S r^2), r^2 = dx^2 +
+// dy^2, dx = col + 0.5 - X, and the weighted deviance sum w (mu - n - n ln
+// mu/n), each parameter's derivative is sum w (1 - n / mu) dmu/dtheta:
+//   dmu/dA = 128 e, dmu/dX = 128 A e 0.2 S dx, dmu/dY = 128 A e 0.2 S dy,
+//   dmu/dS = -128 A e 0.1 r^2, dmu/dB = 64,
+// at the point clamped as the loss clamps it.  One exponential and one
+// division per pixel instead of the central difference's ten losses.
+template <int R, int DIST>
+struct AnalyticEvalGS2D {
+    RoiRef roi;
+    __device__ __forceinline__ float loss(float *x) const {
+        return qcs::loss<R, kGS2D, DIST, ArithSpec<kGS2D, R>::SUM2>(roi, x);
+    }
+    __device__ __forceinline__ void gradient(const float *v, float *g) const {
+        float c[5];
+#pragma unroll
+        for (int k = 0; k < 5; k++) c[k] = v[k] < 0.0f ? 0.0f : v[k];
+        const float A128 = c[0] * QCS_ASCALE, B64 = c[4] * QCS_BSCALE, S01 = c[3] * QCS_SSCALE;
+        float gA = 0, gX = 0, gY = 0, gS = 0, gB = 0;
+#pragma unroll 1
+        for (int row = 0; row < R; row++) {
+            const float dy = (row + 0.5f) - c[2];
+#pragma unroll(R <= kUnrollMaxR ? R : 1)
+            for (int col = 0; col < R; col++) {
+                const float2 pl = roi.img[(row * R + col) * roi.ld];
+                const float w = roi.w[(row * R + col) * roi.ld];
+                const float dx = (col + 0.5f) - c[1];
+                const float r2 = __fmaf_rn(dx, dx, dy * dy);
+                const float e = __expf(-r2 * S01);
+                const float mu = __fmaf_rn(A128, e, B64);
+                const float q = w * (1.0f - __fdividef(pl.x, mu));
+                const float qe = q * e;
+                gA += qe;
+                gX = __fmaf_rn(qe, dx, gX);
+                gY = __fmaf_rn(qe, dy, gY);
+                gS = __fmaf_rn(qe, r2, gS);
+                gB += q;
+            }
+        }
+        g[0] = QCS_ASCALE * gA;
+        g[1] = A128 * 2.0f * S01 * gX;
+        g[2] = A128 * 2.0f * S01 * gY;
+        g[3] = -A128 * QCS_SSCALE * gS;
+        g[4] = QCS_BSCALE * gB;
+    }
+};
+
+// Loss and gradient of one single-emitter ROI (GS2D / AS3D) evaluated by a
+// group of G consecutive lanes of a warp, bit for bit equal to ThreadEval:
+//  - loss: the lanes compute the pixel terms k = lane, lane + G, ... (the
+//    same expressions as loss()) into the ROI's scratch row; then every lane
+//    accumulates the row in pixel order with the same fused multiply-adds,
+//    so all lanes hold the serial sum;
+//  - gradient: the 2P central-difference points are replayed as
+//    numerical_gradient does (in-place clamping); lane l accumulates the
+//    sums of points l, l + G, ... over all pixels in pixel order.  Each
+//    point evaluates its own exponential, which equals the shared one of
+//    numerical_gradient_shared whenever that one applies.
+// img / w / part: the ROI's PIX (value, log) pairs, weights and scratch,
+// contiguous and 16-byte aligned; mask: the group's lanes.  The sums equal
+// the serial kernel's only where the pixel distance's contraction is fixed in
+// the source (DIST != kCompiler).
+template <int R, int KIND, int DIST, int G>
+struct GroupEval {
+    const float2 *img;
+    const float *w;
+    float *part;
+    int lane;
+    unsigned mask;
+
+    __device__ __forceinline__ float loss(float *Ininf) const {
+        typedef KindTraits<KIND> T;
+        enum { PIX = R * R };
+#pragma unroll
+        for (int k = 0; k < T::P; k++) {
+            if (T::CLAMP001) {
+                if (Ininf[k] < 0.01f) Ininf[k] = 0.01f;
+            } else {
+                if (Ininf[k] < 0.0f) Ininf[k] = 0.0f;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < (PIX + G - 1) / G; i++) {
+            const int k = lane + i * G;
+            if (k < PIX) {
+                const int row = k / R, col = k - (k / R) * R;
+                const float2 pl = img[k];
+                part[k] = single_term<KIND>(single_expo<KIND, DIST>(col + 0.5f, row + 0.5f, Ininf), Ininf, pl.x,
+                                            pl.y);
+            }
+        }
+        __syncwarp(mask);
+        float TotalLoss = 0;
+        const float4 *w4 = reinterpret_cast<const float4 *>(w);
+        const float4 *p4 = reinterpret_cast<const float4 *>(part);
+#pragma unroll
+        for (int q = 0; q < PIX / 4; q++) {
+            const float4 a = w4[q], t = p4[q];
+            TotalLoss = __fmaf_rn(a.x, t.x, TotalLoss);
+            TotalLoss = __fmaf_rn(a.y, t.y, TotalLoss);
+            TotalLoss = __fmaf_rn(a.z, t.z, TotalLoss);
+            TotalLoss = __fmaf_rn(a.w, t.w, TotalLoss);
+        }
+#pragma unroll
+        for (int k = PIX / 4 * 4; k < PIX; k++) TotalLoss = __fmaf_rn(w[k], part[k], TotalLoss);
+        __syncwarp(mask);
+        return TotalLoss;
+    }
+
+    __device__ __forceinline__ void gradient(const float *Ininf, float *grad) const {
+        typedef KindTraits<KIND> T;
+        enum { P = T::P, NE = 2 * P, NC = (NE + G - 1) / G, PIX = R * R };
+        float v[NC][P] = {};
+        {
+            float t[P];
+#pragma unroll
+            for (int k = 0; k < P; k++) t[k] = Ininf[k];
+#pragma unroll
+            for (int k = 0; k < P; k++) {
+                t[k] = t[k] - 0.002f;
+#pragma unroll
+                for (int c = 0; c < P; c++) {
+                    if (T::CLAMP001) { if (t[c] < 0.01f) t[c] = 0.01f; } else { if (t[c] < 0.0f) t[c] = 0.0f; }
+                }
+#pragma unroll
+                for (int j = 0; j < NC; j++)
+                    if (lane + j * G == 2 * k)
+#pragma unroll
+                        for (int c = 0; c < P; c++) v[j][c] = t[c];
+                t[k] = t[k] + 0.004f;
+#pragma unroll
+                for (int c = 0; c < P; c++) {
+                    if (T::CLAMP001) { if (t[c] < 0.01f) t[c] = 0.01f; } else { if (t[c] < 0.0f) t[c] = 0.0f; }
+                }
+#pragma unroll
+                for (int j = 0; j < NC; j++)
+                    if (lane + j * G == 2 * k + 1)
+#pragma unroll
+                        for (int c = 0; c < P; c++) v[j][c] = t[c];
+                t[k] = t[k] - 0.002f;
+            }
+        }
+        float tot[NC];
+#pragma unroll
+        for (int j = 0; j < NC; j++) tot[j] = 0;
+#pragma unroll 1
+        for (int row = 0; row < R; row++) {
+#pragma unroll(R <= kUnrollMaxR ? R : 1)
+            for (int col = 0; col < R; col++) {
+                const float2 pl = img[row * R + col];
+                const float wk = w[row * R + col];
+#pragma unroll
+                for (int j = 0; j < NC; j++) {
+                    if (lane + j * G < NE) {
+                        const float e = single_expo<KIND, DIST>(col + 0.5f, row + 0.5f, v[j]);
+                        tot[j] = __fmaf_rn(wk, single_term<KIND>(e, v[j], pl.x, pl.y), tot[j]);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < P; k++) {
+            const float tn = __shfl_sync(mask, tot[(2 * k) / G], (2 * k) % G, G);
+            const float tp = __shfl_sync(mask, tot[(2 * k + 1) / G], (2 * k + 1) % G, G);
+            grad[k] = (tp - tn) * 250.0f;
+        }
+    }
+};
+
 // Fixed schedule: IT quasi-Newton iterations, each with an 11-step bisection
-// of the step length in [1e-5, 1]; no convergence test.  D: P x P scratch.
-template <int R, int KIND, int DIST = ArithSpec<KIND, R>::DIST, int SUM2 = ArithSpec<KIND, R>::SUM2,
-          int ITERS = KindTraits<KIND>::IT>
-__device__ __forceinline__ void mle_fit(const RoiRef &roi, float *Ininf, float *D, int ld) {
-    enum { P = KindTraits<KIND>::P, IT = ITERS };
+// of the step length in [1e-5, 1]; no convergence test.  D: P x P scratch at
+// D[(r * P + c) * ld]; ev evaluates the loss and the gradient.
+template <int P, int IT, class Eval>
+__device__ __forceinline__ void bfgs_fit(const Eval &ev, float *Ininf, float *D, int ld) {
     float grad[P], d0[P], td0[P], sk[P], yk[P], tgrad[P];
     float ddat[2], dpos[2];  // two-element arrays indexed by constants only
 #pragma unroll
@@ -341,7 +521,7 @@ __device__ __forceinline__ void mle_fit(const RoiRef &roi, float *Ininf, float *
 #pragma unroll
         for (int c = 0; c < P; c++) D[(r * P + c) * ld] = (r == c) ? 1.0f : 0.0f;
     }
-    gradient<R, KIND, DIST, SUM2>(roi, Ininf, grad);
+    ev.gradient(Ininf, grad);
 #pragma unroll
     for (int rcnt = 0; rcnt < P; rcnt++) d0[rcnt] = -grad[rcnt];
 
@@ -364,8 +544,8 @@ __device__ __forceinline__ void mle_fit(const RoiRef &roi, float *Ininf, float *
             for (int cnt = 0; cnt < P; cnt++) xlo[cnt] = d0[cnt] * 0.0001f + Ininf[cnt];
 #pragma unroll
             for (int cnt = 0; cnt < P; cnt++) xhi[cnt] = d0[cnt] * 1.0f + Ininf[cnt];
-            ddat[0] = loss<R, KIND, DIST, SUM2>(roi, xlo);
-            ddat[1] = loss<R, KIND, DIST, SUM2>(roi, xhi);
+            ddat[0] = ev.loss(xlo);
+            ddat[1] = ev.loss(xhi);
         }
 
         // Bisection: the half that moves is chosen per ROI; the moved point
@@ -381,7 +561,7 @@ __device__ __forceinline__ void mle_fit(const RoiRef &roi, float *Ininf, float *
                 float xn[P];
 #pragma unroll
                 for (int k = 0; k < P; k++) xn[k] = d0[k] * dsel + Ininf[k];
-                const float f = loss<R, KIND, DIST, SUM2>(roi, xn);
+                const float f = ev.loss(xn);
                 ddat[0] = xdsel ? ddat[0] : f;
                 ddat[1] = xdsel ? f : ddat[1];
             }
@@ -399,7 +579,7 @@ __device__ __forceinline__ void mle_fit(const RoiRef &roi, float *Ininf, float *
         if (itcnt < IT - 1) {
 #pragma unroll
             for (int rcnt = 0; rcnt < P; rcnt++) tgrad[rcnt] = grad[rcnt];
-            gradient<R, KIND, DIST, SUM2>(roi, Ininf, grad);
+            ev.gradient(Ininf, grad);
 #pragma unroll
             for (int rcnt = 0; rcnt < P; rcnt++) yk[rcnt] = grad[rcnt] - tgrad[rcnt];
             bfgs_update<P>(D, ld, sk, yk);
@@ -411,6 +591,12 @@ __device__ __forceinline__ void mle_fit(const RoiRef &roi, float *Ininf, float *
             }
         }
     }
+}
+
+template <int R, int KIND, int DIST = ArithSpec<KIND, R>::DIST, int SUM2 = ArithSpec<KIND, R>::SUM2,
+          int ITERS = KindTraits<KIND>::IT>
+__device__ __forceinline__ void mle_fit(const RoiRef &roi, float *Ininf, float *D, int ld) {
+    bfgs_fit<KindTraits<KIND>::P, ITERS>(ThreadEval<R, KIND, DIST, SUM2>{roi}, Ininf, D, ld);
 }
 
 // Weighted-MLE mask (bfgsMLE_core.h:206-238).

@@ -24,6 +24,12 @@ struct FitLaunch {
 // kind: FitKind (qcs_fit_math.cuh); R: ROI size.
 cudaError_t launch_fit(int kind, int R, const FitLaunch &a);
 
+// Single-emitter kinds with `lanes` lanes per ROI (8; also 4 and 16 for GS2D
+// 7x7): the rows of launch_fit bit for bit, lower latency.  Sizes: GS2D 7, 9,
+// 11, 13 and AS3D 7, 9, 11 (group_fit_supported).
+bool group_fit_supported(int kind, int R);
+cudaError_t launch_fit_group(int kind, int R, int lanes, const FitLaunch &a);
+
 // GS2D fit of a.rois[0, n) started from start[5 * i] (peak e-, x, y, sigma,
 // background e-) with `iters` BFGS iterations (2..5 or 8, R = 7); rows into
 // a.loc, refit[i] = 1 for fits to redo with the plain kernel.
@@ -34,8 +40,10 @@ cudaError_t launch_flag_queue(const uint8_t *flags, int n, int *ids, int *count,
 
 // CRLB columns 9/10 of rows [0, *n_dev) (or [0, n) when n_dev is null);
 // grid sized for max_rows.  LocPrecCalc_GaussianCRLB.h:65-243.
+// ids (optional): the rows are loc[ids[i]] for i < count; skip (optional,
+// indexed by row): rows with skip[row] != 0 are left unchanged.
 cudaError_t launch_crlb(float *loc, const int *n_dev, int n, int max_rows, int loc_type, float ReadNoise_e, float QE,
-                        float PixelSize, cudaStream_t s);
+                        float PixelSize, cudaStream_t s, const int *ids = nullptr, const uint8_t *skip = nullptr);
 
 // WLE pre-pass over n records: PSF width, same-frame nearest neighbour and
 // molecule type into wle (6 floats per record).  scratch must hold

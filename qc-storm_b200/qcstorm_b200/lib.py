@@ -41,6 +41,8 @@ _SIGS = {
     "qcs_fit_single_device": (C.c_int, [C.c_int, C.POINTER(LocPara), C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
                                         C.c_void_p]),
     "qcs_crlb_device": (C.c_int, [C.POINTER(LocPara), C.c_void_p, C.c_int, C.c_void_p]),
+    "qcs_fit_single_group_device": (C.c_int, [C.c_int, C.POINTER(LocPara), C.c_void_p, C.c_void_p, C.c_int,
+                                              C.c_void_p, C.c_int, C.c_void_p]),
     "qcs_measure_mufu_rate": (C.c_int, [C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_double)]),
     "qcs_localize_noalloc": (C.c_int, [C.POINTER(LocPara), C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
                                        C.c_void_p]),
@@ -207,6 +209,13 @@ class LocContext:
 def fit_single_device(loc_type, para, d_rois, d_wle, n, d_loc, stream=0):
     check(load().qcs_fit_single_device(int(loc_type), C.byref(para), C.c_void_p(d_rois), C.c_void_p(d_wle), int(n),
                                        C.c_void_p(d_loc), C.c_void_p(stream) if stream else None))
+
+
+def fit_single_group_device(loc_type, para, d_rois, d_wle, n, d_loc, lanes=8, stream=0):
+    """qcs_fit_single_group_device: the single-emitter fit with `lanes` lanes per ROI."""
+    check(load().qcs_fit_single_group_device(int(loc_type), C.byref(para), C.c_void_p(d_rois), C.c_void_p(d_wle),
+                                             int(n), C.c_void_p(d_loc), int(lanes),
+                                             C.c_void_p(stream) if stream else None))
 
 
 def crlb_device(para, d_loc, n, stream=0):

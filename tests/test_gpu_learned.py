@@ -149,6 +149,30 @@ def naive_start(rec, para):
     return np.ascontiguousarray(st, np.float32)
 
 
+def test_refits_reproduce_plain_rows(cuda_ok):
+    """With a deviance bound no fit meets, every record is refitted plainly
+    (group kernel on the side stream, CRLB of the refit queue there, the
+    main-stream CRLB skipping those rows): the rows, CRLB columns included,
+    equal the plain localization's bit for bit."""
+    import ctypes as C
+    import torch
+    rec, para, _ = synth.gs2d_rois(20_000, seed=31)
+    n = rec.shape[0]
+    d = to_dev(rec)
+    ctx = qlib.LocContext(para, capacity=n)
+    s = torch.cuda.Stream()
+    ctx.localize_device(d.data_ptr(), n, 0, s.cuda_stream)
+    plain, _ = ctx.read_rows(s.cuda_stream)
+    st = to_dev(naive_start(rec, para))
+    qlib.fit_from_start(ctx, d.data_ptr(), n, st.data_ptr(), iters=2, dev_th=1e-6, stream=s.cuda_stream)
+    refit, _ = ctx.read_rows(s.cuda_stream)
+    k = C.c_int(0)
+    qlib.check(qlib.load().qcs_learned_refit_num(ctx.h, C.byref(k)))
+    assert k.value == n
+    np.testing.assert_array_equal(refit.view(np.uint32), plain.view(np.uint32))
+    ctx.close()
+
+
 def rmse_photons(rows, truth, sel):
     return float(np.sqrt(np.mean((rows[sel, 6] / truth["photons"][sel] - 1) ** 2)))
 
