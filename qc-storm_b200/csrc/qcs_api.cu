@@ -54,6 +54,7 @@ struct qcs_loc_data {
     float *d_loc = nullptr;
     void *d_wle_scratch = nullptr;
     size_t wle_scratch = 0;
+    qcs::WleSorter *wle_sorter = nullptr;  // WLE pre-pass, sort only for out-of-order records
     qcs::CascadeState st{};
     void *d_state = nullptr;
     float *h_loc = nullptr;
@@ -120,6 +121,7 @@ int qcs_loc_deinit(qcs_loc_data *c) {
     cudaFree(c->d_state);
     cudaFreeHost(c->h_loc);
     cudaFreeHost(c->h_counters);
+    qcs::wle_sorter_destroy(c->wle_sorter);
     if (c->stream) cudaStreamDestroy(c->stream);
     if (c->side) cudaStreamDestroy(c->side);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
@@ -163,6 +165,7 @@ int qcs_loc_init_capacity(const qcs_loc_para *p, int capacity, qcs_loc_data **ou
     if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&c->side, cudaStreamNonBlocking, prio_greatest);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = qcs::wle_sorter_create(capacity, c->d_wle_scratch, &c->wle_sorter);
     if (e != cudaSuccess) {
         qcs_loc_deinit(c);
         return fail(e == cudaErrorMemoryAllocation ? QCS_ERR_NOMEM : QCS_ERR_CUDA, "qcs_loc_init", e);
@@ -203,7 +206,7 @@ int qcs_loc_localize_device(qcs_loc_data *c, const uint16_t *d_rois, const float
     if (!d_rois && n > 0) return fail(QCS_ERR_ARG, "null ROI pointer");
     const float *wle = d_wle;
     if (!wle && n > 0) {
-        QCS_CUDA(qcs::launch_wle(d_rois, n, c->R, p->LocType, c->d_wle, c->d_wle_scratch, s), "WLE pre-pass");
+        QCS_CUDA(qcs::launch_wle_ctx(c->wle_sorter, d_rois, n, c->R, p->LocType, c->d_wle, s), "WLE pre-pass");
         wle = c->d_wle;
     }
     qcs::CascadeArgs a;
@@ -267,7 +270,7 @@ int qcs_fit_from_start_device(qcs_loc_data *c, const uint16_t *d_rois, const flo
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
     const float *wle = d_wle;
     if (!wle) {
-        QCS_CUDA(qcs::launch_wle(d_rois, n, c->R, p->LocType, c->d_wle, c->d_wle_scratch, s), "WLE pre-pass");
+        QCS_CUDA(qcs::launch_wle_ctx(c->wle_sorter, d_rois, n, c->R, p->LocType, c->d_wle, s), "WLE pre-pass");
         wle = c->d_wle;
     }
     qcs::FitLaunch f;
@@ -424,7 +427,7 @@ int qcs_wle_estimate(qcs_loc_data *c, const uint16_t *h_rois, int n, const qcs_l
     cudaStream_t s = c->stream;
     QCS_CUDA(cudaMemcpyAsync(c->d_rois, h_rois, (size_t)n * c->whole * sizeof(uint16_t), cudaMemcpyHostToDevice, s),
              "copy ROI records");
-    QCS_CUDA(qcs::launch_wle(c->d_rois, n, c->R, p->LocType, c->d_wle, c->d_wle_scratch, s), "WLE pre-pass");
+    QCS_CUDA(qcs::launch_wle_ctx(c->wle_sorter, c->d_rois, n, c->R, p->LocType, c->d_wle, s), "WLE pre-pass");
     QCS_CUDA(cudaMemcpyAsync(h_wle, c->d_wle, (size_t)n * QCS_WLE_PARA_NUM * sizeof(float), cudaMemcpyDeviceToHost, s),
              "read WLE records");
     QCS_CUDA(cudaStreamSynchronize(s), "WLE pre-pass");
@@ -438,7 +441,7 @@ int qcs_wle_estimate_device(qcs_loc_data *c, const uint16_t *d_rois, int n, cons
     if (n == 0) return QCS_OK;
     if (!d_rois || !d_wle) return fail(QCS_ERR_ARG, "null pointer");
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
-    QCS_CUDA(qcs::launch_wle(d_rois, n, c->R, p->LocType, d_wle, c->d_wle_scratch, s), "WLE pre-pass");
+    QCS_CUDA(qcs::launch_wle_ctx(c->wle_sorter, d_rois, n, c->R, p->LocType, d_wle, s), "WLE pre-pass");
     return QCS_OK;
 }
 

@@ -49,6 +49,17 @@ cudaError_t launch_crlb(float *loc, const int *n_dev, int n, int max_rows, int l
 // molecule type into wle (6 floats per record).  scratch must hold
 // wle_scratch_bytes(n) bytes.
 size_t wle_scratch_bytes(int n);
+
+// WLE pre-pass of a localization context: the nearest-neighbour key sort
+// runs (inside a CUDA graph's IF node) only when the records are not already
+// in (frame, y, x) order.  scratch: wle_scratch_bytes(capacity) bytes, owned
+// by the caller.  Calls above capacity, or on a stream being captured, take
+// launch_wle.
+struct WleSorter;
+cudaError_t wle_sorter_create(int capacity, void *scratch, WleSorter **out);
+void wle_sorter_destroy(WleSorter *w);
+cudaError_t launch_wle_ctx(WleSorter *w, const uint16_t *rois, int n, int R, int loc_type, float *wle,
+                           cudaStream_t s);
 cudaError_t launch_wle(const uint16_t *rois, int n, int R, int loc_type, float *wle, void *scratch, cudaStream_t s);
 
 // The same pass over records [d_span[0], d_span[0] + d_span[1]) (read on the

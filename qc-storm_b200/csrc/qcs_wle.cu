@@ -351,7 +351,7 @@ inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
 size_t wle_scratch_bytes(int n) {
     const size_t nn = (size_t)(n > 0 ? n : 1);
-    return 2 * align256(nn * 8) + 2 * align256(nn * 4) + align256(sort_temp_bytes((int)nn));
+    return 2 * align256(nn * 8) + 2 * align256(nn * 4) + align256(sort_temp_bytes((int)nn)) + align256(sizeof(int));
 }
 
 cudaError_t launch_wle(const uint16_t *rois, int n, int R, int loc_type, float *wle, void *scratch, cudaStream_t s) {
@@ -377,6 +377,168 @@ cudaError_t launch_wle(const uint16_t *rois, int n, int R, int loc_type, float *
     e = cub::DeviceRadixSort::SortPairs(p, temp, k_in, k_out, v_in, v_out, n, 0, 64, s);
     if (e != cudaSuccess) return e;
     nn_scan_kernel<<<grid, tpb, 0, s>>>(k_out, v_out, n, wle);
+    classify_kernel<<<grid, tpb, 0, s>>>(rois, wle, sp, R, whole, loc_type);
+    return cudaGetLastError();
+}
+
+namespace {
+
+// Keys of records [0, n) and padding (all ones, after every real key) up to
+// cap; *unsorted = 1 when some record's key is below its predecessor's.
+__global__ void nn_keys_flag_kernel(const uint16_t *__restrict__ rois, int n, int cap, int whole, int pix,
+                                    unsigned long long *__restrict__ keys, int *__restrict__ vals,
+                                    int *__restrict__ unsorted) {
+    const int i = threadIdx.x + blockDim.x * blockIdx.x;
+    bool bad = false;
+    if (i < cap) {
+        unsigned long long k = ~0ull;
+        if (i < n) {
+            const uint16_t *h = rois + (size_t)i * whole + pix;
+            k = (((unsigned long long)h[2] + 65536ull * h[3]) << 32) | ((unsigned long long)h[1] << 16) | h[0];
+            if (i > 0) {
+                const uint16_t *g = h - whole;
+                const unsigned long long kp =
+                    (((unsigned long long)g[2] + 65536ull * g[3]) << 32) | ((unsigned long long)g[1] << 16) | g[0];
+                bad = kp > k;
+            }
+        }
+        keys[i] = k;
+        vals[i] = i;
+    }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(unsorted, 1);
+}
+
+// Sets the sort's IF condition from the flag of nn_keys_flag_kernel.
+__global__ void wle_sort_cond_kernel(cudaGraphConditionalHandle h, const int *__restrict__ unsorted) {
+    cudaGraphSetConditional(h, *unsorted ? 1u : 0u);
+}
+
+// nn_scan_kernel over the sorted keys when the records were out of order,
+// else over the records' own keys (already sorted, identity order).
+__global__ void nn_scan_select_kernel(const unsigned long long *__restrict__ k_in, const unsigned long long *__restrict__ k_out,
+                                      const int *__restrict__ v_out, const int *__restrict__ unsorted, int n,
+                                      float *__restrict__ wle) {
+    const int a = threadIdx.x + blockDim.x * blockIdx.x;
+    if (a >= n) return;
+    if (*unsorted)
+        wle[(size_t)v_out[a] * QCS_WLE_PARA_NUM + 0] = nn_sorted(k_out, a, n);
+    else
+        wle[(size_t)a * QCS_WLE_PARA_NUM + 0] = nn_sorted(k_in, a, n);
+}
+
+}  // namespace
+
+// The WLE pre-pass of a localization context.  Records produced by ROI
+// extraction (and most callers' batches) are already in (frame, y, x)
+// order; then the radix sort of the nearest-neighbour keys is the identity
+// and only costs time.  Here the keys kernel flags out-of-order records and
+// a CUDA graph holds the sort inside an IF node whose condition a one-thread
+// kernel sets from that flag, so the sort runs only when needed and the host
+// never waits.  The sort covers `capacity` keys (padding sorts last).
+struct WleSorter {
+    int capacity = 0;
+    void *scratch = nullptr;  // wle_scratch_bytes(capacity), owned by the caller
+    unsigned long long *k_in = nullptr, *k_out = nullptr;
+    int *v_in = nullptr, *v_out = nullptr, *flag = nullptr;
+    cudaStream_t cap = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+void wle_sorter_destroy(WleSorter *w) {
+    if (!w) return;
+    if (w->exec) cudaGraphExecDestroy(w->exec);
+    if (w->graph) cudaGraphDestroy(w->graph);
+    if (w->cap) cudaStreamDestroy(w->cap);
+    delete w;
+}
+
+cudaError_t wle_sorter_create(int capacity, void *scratch, WleSorter **out) {
+    *out = nullptr;
+    WleSorter *w = new WleSorter();
+    w->capacity = capacity;
+    w->scratch = scratch;
+    const size_t nn = (size_t)capacity;
+    char *p = static_cast<char *>(scratch);
+    w->k_in = reinterpret_cast<unsigned long long *>(p);
+    p += align256(nn * 8);
+    w->k_out = reinterpret_cast<unsigned long long *>(p);
+    p += align256(nn * 8);
+    w->v_in = reinterpret_cast<int *>(p);
+    p += align256(nn * 4);
+    w->v_out = reinterpret_cast<int *>(p);
+    p += align256(nn * 4);
+    void *temp = p;
+    size_t temp_bytes = sort_temp_bytes(capacity);
+    p += align256(temp_bytes);
+    w->flag = reinterpret_cast<int *>(p);
+
+    cudaGraphConditionalHandle h = 0;
+    cudaGraphNode_t kn = nullptr, cn = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&w->cap, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaGraphCreate(&w->graph, 0);
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h, w->graph, 0, cudaGraphCondAssignDefault);
+    if (e == cudaSuccess) {
+        cudaKernelNodeParams kp = {};
+        const int *flag = w->flag;
+        void *args[] = {&h, &flag};
+        kp.func = reinterpret_cast<void *>(wle_sort_cond_kernel);
+        kp.gridDim = dim3(1);
+        kp.blockDim = dim3(1);
+        kp.sharedMemBytes = 0;
+        kp.kernelParams = args;
+        e = cudaGraphAddKernelNode(&kn, w->graph, nullptr, 0, &kp);
+    }
+    cudaGraph_t body = nullptr;
+    if (e == cudaSuccess) {
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeIf;
+        cp.conditional.size = 1;
+        e = cudaGraphAddNode(&cn, w->graph, &kn, 1, &cp);
+        if (e == cudaSuccess) body = cp.conditional.phGraph_out[0];
+    }
+    if (e == cudaSuccess)
+        e = cudaStreamBeginCaptureToGraph(w->cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
+    if (e == cudaSuccess) {
+        cudaError_t es = cub::DeviceRadixSort::SortPairs(temp, temp_bytes, w->k_in, w->k_out, w->v_in, w->v_out,
+                                                         capacity, 0, 64, w->cap);
+        cudaGraph_t captured = nullptr;
+        e = cudaStreamEndCapture(w->cap, &captured);
+        if (e == cudaSuccess) e = es;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&w->exec, w->graph, 0);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        wle_sorter_destroy(w);
+        return e;
+    }
+    *out = w;
+    return cudaSuccess;
+}
+
+cudaError_t launch_wle_ctx(WleSorter *w, const uint16_t *rois, int n, int R, int loc_type, float *wle,
+                           cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(s, &cs);
+    if (e != cudaSuccess) return e;
+    if (n > w->capacity || cs != cudaStreamCaptureStatusNone)
+        return launch_wle(rois, n, R, loc_type, wle, w->scratch, s);
+    const int tpb = 64;
+    const int grid = (n + tpb - 1) / tpb;
+    const Span sp{0, n, nullptr};
+    e = launch_psf_width(R, rois, wle, sp, grid, tpb, s);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(w->flag, 0, sizeof(int), s);
+    if (e != cudaSuccess) return e;
+    const int whole = R * (R + 1);
+    nn_keys_flag_kernel<<<(w->capacity + tpb - 1) / tpb, tpb, 0, s>>>(rois, n, w->capacity, whole, R * R, w->k_in,
+                                                                      w->v_in, w->flag);
+    e = cudaGraphLaunch(w->exec, s);
+    if (e != cudaSuccess) return e;
+    nn_scan_select_kernel<<<grid, tpb, 0, s>>>(w->k_in, w->k_out, w->v_out, w->flag, n, wle);
     classify_kernel<<<grid, tpb, 0, s>>>(rois, wle, sp, R, whole, loc_type);
     return cudaGetLastError();
 }
