@@ -292,6 +292,31 @@ def train_learned_net(para, stream, seed=4242):
     return net, info
 
 
+E2E_STEPS = 40  # end-to-end steps (each ~1 ms)
+
+
+def e2e_pipelined(ctxs, streams, h_batches, steps, net=None):
+    """`steps` calls of the asynchronous host-buffer localization
+    (qcs_loc_localize_async, or qcs_learned_localize_async with net) over two
+    contexts used in turn on their own streams: call k's record copy and row
+    copy overlap call k-1's kernels.  Every call copies its pinned records in
+    and its rows and counters out; qcs_loc_finish waits for it.  Returns
+    (seconds, rows read)."""
+    import torch
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    rows = 0
+    for k in range(steps):
+        c = ctxs[k % 2]
+        if k >= 2:
+            rows += c.finish(copy=False)[0].shape[0]
+        c.localize_async(h_batches[k % len(h_batches)].data_ptr(), N_PER_STEP, stream=streams[k % 2].cuda_stream,
+                         net=net, iters=LEARNED_ITERS)
+    for k in range(max(0, steps - 2), steps):
+        rows += ctxs[k % 2].finish(copy=False)[0].shape[0]
+    return time.perf_counter() - t0, rows
+
+
 def fit_accuracy(rows, rec, truth, sel, para):
     """Position RMSE (px, per axis), relative photon RMSE and CRLB (px) over sel."""
     fx = rows[sel, 1] + R // 2 - rec[sel, R * R].astype(np.float64)
@@ -346,20 +371,14 @@ def learned_measure(args, stream, ctx, para, d_batches, h_batches, rec0, truth0,
     rp, pp, crlb = fit_accuracy(plain, rec0, truth0, both, para)
     rl, pl, _ = fit_accuracy(learned, rec0, truth0, both, para)
 
-    # end to end: pinned host records -> device -> learned localization -> rows on the host
-    d_in = torch.empty_like(d_batches[0])
-    e2e_steps = max(3, min(args.steps, 10))
-    for k in range(2):
-        d_in.copy_(h_batches[k], non_blocking=True)
-        net.localize(ctx, d_in.data_ptr(), N_PER_STEP, 0, iters=LEARNED_ITERS, stream=sh)
-        ctx.read_rows(sh)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for k in range(e2e_steps):
-        d_in.copy_(h_batches[k % BATCHES], non_blocking=True)
-        net.localize(ctx, d_in.data_ptr(), N_PER_STEP, 0, iters=LEARNED_ITERS, stream=sh)
-        ctx.read_rows(sh)
-    e2e_s = time.perf_counter() - t0
+    # end to end: pinned host records in, rows out, through qcs_learned_localize_async
+    from qcstorm_b200 import lib
+    ctxs = [ctx, lib.LocContext(para, capacity=N_PER_STEP)]
+    streams = [stream, torch.cuda.Stream()]
+    e2e_pipelined(ctxs, streams, h_batches, 4, net=net)
+    e2e_steps = E2E_STEPS
+    e2e_s, _ = e2e_pipelined(ctxs, streams, h_batches, e2e_steps, net=net)
+    ctxs[1].close()
     net.close()
     return {
         "value": value, "unit": UNIT, "ms_per_step": ms / args.steps, "vs_plain": value / plain_value,
@@ -368,7 +387,8 @@ def learned_measure(args, stream, ctx, para, d_batches, h_batches, rec0, truth0,
         "e2e": {"value": e2e_steps * N_PER_STEP * world / e2e_s, "unit": UNIT,
                 "h2d_bytes_per_step": N_PER_STEP * R * (R + 1) * 2,
                 "d2h_bytes_per_step": N_PER_STEP * 48 + 32,
-                "call": "pinned records -> qcs_learned_localize_device -> qcs_loc_read_rows"},
+                "call": "qcs_learned_localize_async + qcs_loc_finish on two contexts in turn (pinned records in, "
+                        "rows and counters out every step)"},
         "accuracy": {"records": N_PER_STEP, "compared": int(both.sum()),
                      "rmse_px": {"plain": rp, "learned": rl}, "photon_rel_rmse": {"plain": pp, "learned": pl},
                      "crlb_px": crlb, "accepted": {"plain": float((plain[:, 0] > 0).mean()),
@@ -546,22 +566,29 @@ def main():
     mufu_peak = lib.mufu_rate()
     achieved = N_PER_STEP * PX_EVALS_PER_FIT * MUFU_PER_PX_EVAL / (fit_ms * 1e-3)
 
-    # ---- end to end through the host-buffer call (pinned records in, rows out)
-    e2e_steps = max(3, min(args.steps, 10))
+    # ---- end to end through the host-buffer calls (pinned records in, rows out every step)
+    ctxs = [ctx, lib.LocContext(para, capacity=N_PER_STEP)]
+    streams = [stream, torch.cuda.Stream()]
+    e2e_pipelined(ctxs, streams, h_batches, 4)
+    e2e_steps = E2E_STEPS
+    e2e_s, rows = e2e_pipelined(ctxs, streams, h_batches, e2e_steps)
+    ctxs[1].close()
+    # the synchronous reference-shaped call, one at a time
+    sync_steps = 10
     for k in range(2):
         ctx.localize(h_batches[k].numpy().view(np.uint16), None, stream=sh)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    rows = 0
-    for k in range(e2e_steps):
-        out, _ = ctx.localize(h_batches[k % BATCHES].numpy().view(np.uint16), None, stream=sh)
-        rows += out.shape[0]
-    torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
+    for k in range(sync_steps):
+        ctx.localize(h_batches[k % BATCHES].numpy().view(np.uint16), None, stream=sh)
+    sync_s = time.perf_counter() - t0
     e2e = {"value": e2e_steps * N_PER_STEP * world / e2e_s, "unit": UNIT,
            "h2d_bytes_per_step": N_PER_STEP * R * (R + 1) * 2,
            "d2h_bytes_per_step": int(rows / e2e_steps) * 48 + 32,
-           "call": "qcs_loc_bfgs_mle_localization (pinned host records, WLE on device, synchronous)"}
+           "call": "qcs_loc_localize_async + qcs_loc_finish on two contexts in turn (pinned host records in, rows "
+                   "and counters out every step, WLE on device)",
+           "sync_value": sync_steps * N_PER_STEP * world / sync_s,
+           "sync_call": "qcs_loc_bfgs_mle_localization, one call at a time"}
 
     learned = None
     if not args.no_learned:

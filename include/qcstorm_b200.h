@@ -239,6 +239,21 @@ int qcs_loc_bfgs_mle_localization(qcs_loc_data *c, const uint16_t *h_rois, const
  * context's stream) and bring the rows, their count and the fit ratios to
  * the host, as qcs_loc_bfgs_mle_localization leaves them. */
 int qcs_loc_read_rows(qcs_loc_data *c, const qcs_loc_para *p, void *stream);
+/* Asynchronous form of qcs_loc_bfgs_mle_localization (bfgs_top.cu:26): enqueues
+ * the copy of n host records (and WLE rows, or NULL) to the device, the
+ * localization, and the copy of the counters and of every row slot the call
+ * can fill (n, or 3n with multi-emitter fitting) into the context's host
+ * buffers on `stream` (NULL: the context's stream), and returns without
+ * waiting.  With records in pinned memory the copies overlap kernels of other
+ * streams: two contexts used in turn keep the copy engines and the SMs busy
+ * at once.  qcs_loc_finish waits for the call and sets h_LocArry,
+ * oValidFluoNum and the fit ratios; until then the context refuses other
+ * calls and the host buffers must not be read. */
+int qcs_loc_localize_async(qcs_loc_data *c, const uint16_t *h_rois, const float *h_wle, const qcs_loc_para *p, int n,
+                           void *stream);
+/* Waits for the context's pending asynchronous call (qcs_loc_localize_async,
+ * qcs_learned_localize_async) and publishes its rows, count and ratios. */
+int qcs_loc_finish(qcs_loc_data *c, const qcs_loc_para *p);
 /* h_LocArry: valid until the next call on the context (bfgs_top.h:38). */
 const float *qcs_loc_h_loc_arry(const qcs_loc_data *c);
 /* oValidFluoNum (bfgs_top.h:42). */
@@ -376,6 +391,13 @@ int qcs_learned_set_inference(qcs_learned_net *net, int fused);
 /* QCS_OK, or QCS_ERR_CUDA if a fused-inference launch gave up waiting for its
  * tensor-core work (waits for the device). */
 int qcs_learned_fused_status(qcs_learned_net *net);
+/* qcs_learned_localize_device on host records, asynchronously like
+ * qcs_loc_localize_async (finish with qcs_loc_finish).  One network may serve
+ * several contexts at once: its start points go to each context's own
+ * buffer, and its weight image is rebuilt only after a parameter change
+ * (change parameters only while no call using the network is in flight). */
+int qcs_learned_localize_async(qcs_loc_data *c, qcs_learned_net *net, const uint16_t *h_rois, const float *h_wle,
+                               const qcs_loc_para *p, int n, int iters, float dev_th, void *stream);
 /* Number of plain refits of the last qcs_learned_localize_device call (waits for it). */
 int qcs_learned_refit_num(qcs_loc_data *c, int *n);
 

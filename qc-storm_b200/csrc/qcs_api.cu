@@ -62,6 +62,10 @@ struct qcs_loc_data {
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;  // high-priority stream for work overlapped with the main stream
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaEvent_t ev_done = nullptr;  // end of the last asynchronous host call
+    float *d_start = nullptr;       // learned start points, capacity x 5
+    int pending = 0;                // an asynchronous host call awaits qcs_loc_finish
+    int pending_n = 0;
     int valid = 0;
     float ratios[7] = {0, 0, 0, 0, 0, 0, 0};
 };
@@ -121,7 +125,10 @@ int qcs_loc_deinit(qcs_loc_data *c) {
     cudaFree(c->d_state);
     cudaFreeHost(c->h_loc);
     cudaFreeHost(c->h_counters);
+    if (c->pending && c->ev_done) cudaEventSynchronize(c->ev_done);
     qcs::wle_sorter_destroy(c->wle_sorter);
+    cudaFree(c->d_start);
+    if (c->ev_done) cudaEventDestroy(c->ev_done);
     if (c->stream) cudaStreamDestroy(c->stream);
     if (c->side) cudaStreamDestroy(c->side);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
@@ -166,6 +173,8 @@ int qcs_loc_init_capacity(const qcs_loc_para *p, int capacity, qcs_loc_data **ou
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
     if (e == cudaSuccess) e = qcs::wle_sorter_create(capacity, c->d_wle_scratch, &c->wle_sorter);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_done, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = A((void **)&c->d_start, cap * 5 * sizeof(float));
     if (e != cudaSuccess) {
         qcs_loc_deinit(c);
         return fail(e == cudaErrorMemoryAllocation ? QCS_ERR_NOMEM : QCS_ERR_CUDA, "qcs_loc_init", e);
@@ -195,6 +204,7 @@ static int check_call(qcs_loc_data *c, const qcs_loc_para *p, int n) {
     if (p->ROISize != c->R) return fail(QCS_ERR_ROISIZE, "ROISize differs from the one the context was created with");
     if (n < 0) return fail(QCS_ERR_ARG, "negative ROI count");
     if (n > c->capacity) return fail(QCS_ERR_CAPACITY, "ROI count above the context capacity");
+    if (c->pending) return fail(QCS_ERR_ARG, "an asynchronous call on this context awaits qcs_loc_finish");
     return QCS_OK;
 }
 
@@ -318,9 +328,8 @@ int qcs_learned_localize_device(qcs_loc_data *c, qcs_learned_net *net, const uin
     if (n == 0) return QCS_OK;
     if (!d_rois) return fail(QCS_ERR_ARG, "null ROI pointer");
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
-    const float *start = nullptr;
-    QCS_CUDA(qcs::learned::start_points(net, p, d_rois, n, &start, s), "learned start points");
-    return qcs_fit_from_start_device(c, d_rois, d_wle, p, n, start, iters, dev_th, s);
+    QCS_CUDA(qcs::learned::start_points(net, p, d_rois, n, c->d_start, s), "learned start points");
+    return qcs_fit_from_start_device(c, d_rois, d_wle, p, n, c->d_start, iters, dev_th, s);
 }
 
 int qcs_learned_refit_num(qcs_loc_data *c, int *n) {
@@ -388,6 +397,77 @@ int qcs_loc_bfgs_mle_localization(qcs_loc_data *c, const uint16_t *h_rois, const
     QCS_CUDA(cudaStreamSynchronize(s), "read localizations");
     c->valid = rows;
     compute_ratios(c, p, n);
+    return QCS_OK;
+}
+
+}  // extern "C"
+
+// Host records in, rows and counters out, on stream s, without waiting:
+// device_call runs the localization of the records copied to c->d_rois.
+template <class F>
+static int enqueue_host_call(qcs_loc_data *c, const uint16_t *h_rois, const float *h_wle, const qcs_loc_para *p,
+                             int n, cudaStream_t s, F device_call) {
+    if (c->pending) return fail(QCS_ERR_ARG, "the previous asynchronous call awaits qcs_loc_finish");
+    c->valid = 0;
+    for (int i = 0; i < 7; ++i) c->ratios[i] = 0;
+    c->pending_n = n;
+    if (n > 0) {
+        if (!h_rois) return fail(QCS_ERR_ARG, "null ROI pointer");
+        QCS_CUDA(cudaMemcpyAsync(c->d_rois, h_rois, (size_t)n * c->whole * sizeof(uint16_t), cudaMemcpyHostToDevice,
+                                 s),
+                 "copy ROI records");
+        if (h_wle)
+            QCS_CUDA(cudaMemcpyAsync(c->d_wle, h_wle, (size_t)n * QCS_WLE_PARA_NUM * sizeof(float),
+                                     cudaMemcpyHostToDevice, s),
+                     "copy WLE records");
+        int st = device_call(h_wle ? c->d_wle : nullptr);
+        if (st) return st;
+        // rows: one per record, then at most two appended emitters per record
+        const long long most = p->MultiEmitterFitEn ? 3ll * n : (long long)n;
+        const int rows = (int)(most < c->max_rows ? most : c->max_rows);
+        QCS_CUDA(cudaMemcpyAsync(c->h_counters, c->st.counters, qcs::kCntNum * sizeof(int), cudaMemcpyDeviceToHost,
+                                 s),
+                 "read counters");
+        QCS_CUDA(cudaMemcpyAsync(c->h_loc, c->d_loc, (size_t)rows * QCS_OUT_PARA_NUM * sizeof(float),
+                                 cudaMemcpyDeviceToHost, s),
+                 "read localizations");
+    }
+    QCS_CUDA(cudaEventRecord(c->ev_done, s), "record completion");
+    c->pending = 1;
+    return QCS_OK;
+}
+
+extern "C" {
+
+int qcs_loc_localize_async(qcs_loc_data *c, const uint16_t *h_rois, const float *h_wle, const qcs_loc_para *p, int n,
+                           void *stream) {
+    int st = check_call(c, p, n);
+    if (st) return st;
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+    return enqueue_host_call(c, h_rois, h_wle, p, n, s, [&](const float *d_wle) {
+        return qcs_loc_localize_device(c, c->d_rois, d_wle, p, n, s);
+    });
+}
+
+int qcs_learned_localize_async(qcs_loc_data *c, qcs_learned_net *net, const uint16_t *h_rois, const float *h_wle,
+                               const qcs_loc_para *p, int n, int iters, float dev_th, void *stream) {
+    int st = check_call(c, p, n);
+    if (st) return st;
+    if (!net) return fail(QCS_ERR_ARG, "null network");
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+    return enqueue_host_call(c, h_rois, h_wle, p, n, s, [&](const float *d_wle) {
+        return qcs_learned_localize_device(c, net, c->d_rois, d_wle, p, n, iters, dev_th, s);
+    });
+}
+
+int qcs_loc_finish(qcs_loc_data *c, const qcs_loc_para *p) {
+    if (!c || !p) return fail(QCS_ERR_ARG, "null argument");
+    if (!c->pending) return fail(QCS_ERR_ARG, "no asynchronous call to finish");
+    c->pending = 0;
+    QCS_CUDA(cudaEventSynchronize(c->ev_done), "localization");
+    if (c->pending_n == 0) return QCS_OK;
+    c->valid = c->h_counters[qcs::kCntValid];
+    compute_ratios(c, p, c->pending_n);
     return QCS_OK;
 }
 

@@ -534,6 +534,9 @@ struct qcs_learned_net {
     size_t start_cap = 0;
     __nv_bfloat16 *d_wimg = nullptr;  // BF16 operand images of the weights (fused inference)
     int *d_err = nullptr;             // set by the fused kernel when an MMA wait gives up
+    unsigned version = 1;             // bumped whenever the parameters change
+    unsigned wimg_version = 0;        // parameter version d_wimg was built from
+    cudaEvent_t wimg_ready = nullptr; // recorded after d_wimg was built
     bool use_tc = true;
     int batch = 0;
     long long step = 0;
@@ -635,7 +638,18 @@ cudaError_t fused_start_points(qcs_learned_net *net, const qcs_loc_para *p, cons
     if (e != cudaSuccess) return e;
     const int grid = tiles < 2 * sms ? tiles : 2 * sms;
     const Views w = views(net->d_par);
-    L::tc::weight_image_kernel<<<blocks(L::tc::kW1 + L::tc::kW2 + L::tc::kW3), 256, 0, s>>>(net->d_par, net->d_wimg);
+    // the weight image is rebuilt only after a parameter change; calls on
+    // other streams wait for the build that made the current one
+    if (net->wimg_version != net->version) {
+        L::tc::weight_image_kernel<<<blocks(L::tc::kW1 + L::tc::kW2 + L::tc::kW3), 256, 0, s>>>(net->d_par,
+                                                                                             net->d_wimg);
+        e = cudaEventRecord(net->wimg_ready, s);
+        if (e != cudaSuccess) return e;
+        net->wimg_version = net->version;
+    } else {
+        e = cudaStreamWaitEvent(s, net->wimg_ready, 0);
+        if (e != cudaSuccess) return e;
+    }
     L::tc::mlp_tc_kernel<<<grid, 128, L::tc::kSmemBytes, s>>>(d_rois, n, p->Offset, p->KAdc,
                                                               reinterpret_cast<const uint4 *>(net->d_wimg), w.b1, w.b2,
                                                               w.b3, start, net->d_err);
@@ -657,6 +671,7 @@ int qcs_learned_destroy(qcs_learned_net *net) {
     cudaFree(net->d_start);
     cudaFree(net->d_wimg);
     cudaFree(net->d_err);
+    if (net->wimg_ready) cudaEventDestroy(net->wimg_ready);
     if (net->stream) cudaStreamDestroy(net->stream);
     delete net;
     return QCS_OK;
@@ -681,6 +696,7 @@ int qcs_learned_create(int batch, unsigned long long seed, qcs_learned_net **out
     if (e == cudaSuccess) e = cudaMalloc((void **)&net->d_err, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(net->d_err, 0, sizeof(int));
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&net->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&net->wimg_ready, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         qcs_learned_destroy(net);
         return fail(e == cudaErrorMemoryAllocation ? QCS_ERR_NOMEM : QCS_ERR_CUDA, "qcs_learned_create", e);
@@ -746,6 +762,7 @@ int qcs_learned_get_params(qcs_learned_net *net, float *h_params) {
 int qcs_learned_set_params(qcs_learned_net *net, const float *h_params) {
     if (!net || !h_params) return fail(QCS_ERR_ARG, "null argument");
     QCS_CUDA(cudaMemcpy(net->d_par, h_params, L::kParams * sizeof(float), cudaMemcpyHostToDevice), "set parameters");
+    net->version++;
     return QCS_OK;
 }
 
@@ -852,6 +869,7 @@ int qcs_learned_train_device(qcs_learned_net *net, const float *d_feat, const fl
         }
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    net->version++;
     cudaFree(d_perm);
     cudaFree(d_vb);
     cudaFree(d_tb);
@@ -897,11 +915,13 @@ int qcs_learned_fused_status(qcs_learned_net *net) {
 
 }  // extern "C"
 
-// Start points of n records into net-owned memory (grown, outside any
-// capture, when n exceeds what the last call needed): features, one GEMM per
-// layer over all n rows (activations rectified in place), start points.
+// Start points of n records into out (n x 5): the fused kernel, or, with
+// fused inference off, features and one GEMM per layer over all n rows in
+// net-owned memory (grown, outside any capture, when n exceeds what the last
+// call needed; not for concurrent calls).
 cudaError_t qcs::learned::start_points(qcs_learned_net *net, const qcs_loc_para *p, const uint16_t *d_rois, int n,
-                                       const float **d_start, cudaStream_t s) {
+                                       float *out, cudaStream_t s) {
+    if (net->use_tc) return fused_start_points(net, p, d_rois, n, out, s);
     const size_t need = (size_t)n * (L::kStart + L::kIn + 2 + 2 * L::kHidden + L::kOut);
     if (need > net->start_cap) {
         cudaFree(net->d_start);
@@ -913,11 +933,10 @@ cudaError_t qcs::learned::start_points(qcs_learned_net *net, const qcs_loc_para 
     }
     float *start = net->d_start, *feat = start + (size_t)n * L::kStart, *scale = feat + (size_t)n * L::kIn;
     float *h1 = scale + 2 * (size_t)n, *h2 = h1 + (size_t)n * L::kHidden, *y = h2 + (size_t)n * L::kHidden;
-    *d_start = start;
-    if (net->use_tc) return fused_start_points(net, p, d_rois, n, start, s);
+    (void)start;
     L::features_kernel<<<blocks(n), 256, 0, s>>>(d_rois, n, p->Offset, p->KAdc, feat, scale);
     cudaError_t e = forward(net, feat, n, h1, h1, h2, h2, y, s);
     if (e != cudaSuccess) return e;
-    L::start_kernel<<<blocks(n), 256, 0, s>>>(y, scale, n, start);
+    L::start_kernel<<<blocks(n), 256, 0, s>>>(y, scale, n, out);
     return cudaGetLastError();
 }

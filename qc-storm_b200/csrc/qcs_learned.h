@@ -26,9 +26,9 @@ constexpr int kParams = kIn * kHidden + kHidden + kHidden * kHidden + kHidden + 
 __constant__ const float kTargetWeight[kOutUsed] = {4.0f, 4.0f, 1.0f, 1.0f, 1.0f};
 
 // Start points (peak e-, x, y, sigma, background e- per record) of n device
-// records, computed by `net` into memory it owns; *d_start points there.
-cudaError_t start_points(qcs_learned_net *net, const qcs_loc_para *p, const uint16_t *d_rois, int n,
-                         const float **d_start, cudaStream_t s);
+// records into out (n x 5 floats).
+cudaError_t start_points(qcs_learned_net *net, const qcs_loc_para *p, const uint16_t *d_rois, int n, float *out,
+                         cudaStream_t s);
 
 }  // namespace learned
 }  // namespace qcs

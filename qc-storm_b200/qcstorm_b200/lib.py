@@ -75,6 +75,10 @@ _SIGS = {
                                               C.c_int, C.c_int, C.c_float, C.c_void_p]),
     "qcs_learned_refit_num": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "qcs_learned_set_inference": (C.c_int, [C.c_void_p, C.c_int]),
+    "qcs_loc_localize_async": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(LocPara), C.c_int, C.c_void_p]),
+    "qcs_learned_localize_async": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(LocPara),
+                                             C.c_int, C.c_int, C.c_float, C.c_void_p]),
+    "qcs_loc_finish": (C.c_int, [C.c_void_p, C.POINTER(LocPara)]),
     "qcs_learned_fused_status": (C.c_int, [C.c_void_p]),
     "qcs_fit_from_start_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(LocPara), C.c_int,
                                             C.c_void_p, C.c_int, C.c_float, C.c_void_p]),
@@ -174,6 +178,31 @@ class LocContext:
         out = np.zeros((rois.shape[0], 6), np.float32)
         check(self.lib.qcs_wle_estimate(self.h, pr, rois.shape[0], C.byref(para), C.c_void_p(out.ctypes.data)))
         return out
+
+    def localize_async(self, h_rois_ptr, n, h_wle_ptr=0, stream=0, para=None, net=None, iters=2, dev_th=0.0):
+        """qcs_loc_localize_async (or, with net, qcs_learned_localize_async) on host
+        memory given by address (pinned for overlap); finish() publishes the rows."""
+        para = para or self.para
+        self._async_para = para
+        wle = C.c_void_p(h_wle_ptr) if h_wle_ptr else None
+        st = C.c_void_p(stream) if stream else None
+        if net is None:
+            check(self.lib.qcs_loc_localize_async(self.h, C.c_void_p(h_rois_ptr), wle, C.byref(para), int(n), st))
+        else:
+            check(self.lib.qcs_learned_localize_async(self.h, net.h, C.c_void_p(h_rois_ptr), wle, C.byref(para),
+                                                      int(n), int(iters), C.c_float(dev_th), st))
+
+    def finish(self, copy=True):
+        """qcs_loc_finish: (rows[n_valid, 12], ratios[7]); copy=False returns a view of
+        the context's pinned row buffer, valid until the next call."""
+        check(self.lib.qcs_loc_finish(self.h, C.byref(getattr(self, "_async_para", None) or self.para)))
+        nv = self.lib.qcs_loc_valid_num(self.h)
+        ptr = self.lib.qcs_loc_h_loc_arry(self.h)
+        rows = np.ctypeslib.as_array((C.c_float * (12 * nv)).from_address(ptr)).reshape(nv, 12) if nv else \
+            np.zeros((0, 12), np.float32)
+        ratios = np.zeros(7, np.float32)
+        check(self.lib.qcs_loc_fit_ratios(self.h, C.c_void_p(ratios.ctypes.data)))
+        return (rows.copy() if copy else rows), ratios
 
     # device-pointer forms (integers from torch.Tensor.data_ptr(), stream handles)
     def localize_device(self, d_rois, n, d_wle=0, stream=0, para=None):
