@@ -73,6 +73,14 @@ extern "C" {
 #define QCS_POS_CRBX 9
 #define QCS_POS_CRBY 10
 #define QCS_POS_FRME 11
+
+/* Super-resolution rendering modes (ImgRender/ImageRender_base.h:36-39) and
+ * the length of the display-intensity histogram (:27). */
+#define QCS_RENDER_FITTED_PHOTON_CRLB 0   /* weight peak photons, width from the CRLB */
+#define QCS_RENDER_1PHOTON_CRLB 1         /* weight 1, width from the CRLB */
+#define QCS_RENDER_1PHOTON_FIXED 2        /* weight 1, fixed width */
+#define QCS_RENDER_FITTED_PHOTON_1PIXEL 3 /* weight peak photons, one pixel (2D) */
+#define QCS_RENDER_HIST_LEN 400
 /* molecule type in WLE record column 5 (WLEParaEstimation_Parameters.h:32-34) */
 #define QCS_MOLECULE_MLEFIT 0
 #define QCS_MOLECULE_WLEFIT 1
@@ -400,6 +408,41 @@ int qcs_learned_localize_async(qcs_loc_data *c, qcs_learned_net *net, const uint
                                const qcs_loc_para *p, int n, int iters, float dev_th, void *stream);
 /* Number of plain refits of the last qcs_learned_localize_device call (waits for it). */
 int qcs_learned_refit_num(qcs_loc_data *c, int *n);
+
+/* ---- super-resolution render (ImageRenderData_TypeDef) ------------------ */
+typedef struct qcs_render_data qcs_render_data;
+/* ImageRenderData_TypeDef::Init (ImgRender/ImageRender_top.cu:223): a float SR
+ * image of p->SRImageWidth x p->SRImageHigh, zeroed; for 3D localization types
+ * (LocType != GS2D) also the z-weighted colour map; the display maximum and
+ * QCS_RENDER_HIST_LEN-bin histogram; room for `capacity` host rows per call
+ * (<= 0: QCS_MAX_POINT_NUM). */
+int qcs_render_init(const qcs_loc_para *p, int capacity, qcs_render_data **out);
+int qcs_render_deinit(qcs_render_data *r);
+/* ResetFillImgTop (ImageRender_top.cu:168-183): the images back to zero. */
+int qcs_render_reset(qcs_render_data *r, void *stream);
+/* ResetFillMaxVal(0) (ImageRender_top.cu:68-79): display maximum, histogram
+ * and the row count behind the periodic histogram rescale back to zero. */
+int qcs_render_reset_max(qcs_render_data *r, void *stream);
+/* FluoRenderTop(h_LocArry, LocPara, RenderingMode, FixedlocPrec, FluoNum,
+ * stream) (ImageRender_top.cu:29): adds n host rows (12 floats each) to the
+ * image with mode QCS_RENDER_*; fixed_prec (nm) for QCS_RENDER_1PHOTON_FIXED.
+ * Rows are selected and widened as in FluoRenderWithPrec_2D / _3D
+ * (ImageRender_2d.cu:55-155, ImageRender_3d.cu:60-148); the histogram step is
+ * skipped while the running maximum is 0 (the reference divides by it). */
+int qcs_render_rows(qcs_render_data *r, const float *h_rows, const qcs_loc_para *p, int mode, float fixed_prec, int n,
+                    void *stream);
+/* The same for rows already on the device, the count read at d_n (NULL: max_n)
+ * when the kernels run: the hand-off from a localization call, e.g.
+ * qcs_loc_device_rows(ctx) with qcs_loc_device_valid_num(ctx), no host round
+ * trip (no counterpart in the reference, which copies rows from the host). */
+int qcs_render_rows_device(qcs_render_data *r, const float *d_rows, const int *d_n, int max_n, const qcs_loc_para *p,
+                           int mode, float fixed_prec, void *stream);
+/* d_SRIntensityImg, d_SRColorMapImg (NULL for 2D) (ImageRender_top.h). */
+float *qcs_render_d_image(qcs_render_data *r);
+float *qcs_render_d_colormap(qcs_render_data *r);
+/* Copies the image, colour map, maximum and histogram (any may be NULL) to the
+ * host and waits. */
+int qcs_render_read(qcs_render_data *r, float *h_img, float *h_colormap, int *h_max, int *h_hist, void *stream);
 
 /* ---- allocation-free localization --------------------------------------- */
 /*

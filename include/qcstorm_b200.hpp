@@ -56,6 +56,13 @@
 #define Pos_CrbX QCS_POS_CRBX
 #define Pos_CrbY QCS_POS_CRBY
 #define Pos_Frme QCS_POS_FRME
+
+// ImgRender/ImageRender_base.h:27, 36-39
+#define ImgRend_MaxDatHistLen QCS_RENDER_HIST_LEN
+#define RenderingMode_FittedPhoton_CalculatedLocPrec QCS_RENDER_FITTED_PHOTON_CRLB
+#define RenderingMode_1Photon_CalculatedLocPrec QCS_RENDER_1PHOTON_CRLB
+#define RenderingMode_1Photon_FixedLocPrec QCS_RENDER_1PHOTON_FIXED
+#define RenderingMode_FittedPhoton_1Pixel QCS_RENDER_FITTED_PHOTON_1PIXEL
 #endif
 #ifndef WLE_ParaNumber
 #define WLE_ParaNumber QCS_WLE_PARA_NUM
@@ -296,6 +303,43 @@ public:
 
 private:
     qcs_zero_data *z_ = nullptr;
+};
+
+// ImgRender/ImageRender_top.h: the super-resolution render of localization
+// rows.  d_SRIntensityImg / d_SRColorMapImg point at the device images; the
+// display-image helpers (GetDispImgTop, GetSaveImgTop) are not provided.
+class ImageRenderData_TypeDef {
+public:
+    float *d_SRIntensityImg = nullptr;
+    float *d_SRColorMapImg = nullptr;
+
+    void Init(LocalizationPara &LocPara, int /*MaxDispImgWidth*/ = 0, int /*MaxDispImgHigh*/ = 0) {
+        qcs_facade::report(qcs_render_init(&LocPara, 0, &r_), "ImageRenderData_TypeDef::Init");
+        d_SRIntensityImg = r_ ? qcs_render_d_image(r_) : nullptr;
+        d_SRColorMapImg = r_ ? qcs_render_d_colormap(r_) : nullptr;
+    }
+    void Deinit(LocalizationPara & /*LocPara*/) {
+        qcs_render_deinit(r_);
+        r_ = nullptr;
+        d_SRIntensityImg = d_SRColorMapImg = nullptr;
+    }
+    void FluoRenderTop(float *h_LocArry, LocalizationPara &LocPara, int RenderingMode, float FixedlocPrec, int FluoNum,
+                       cudaStream_t cstream) {
+        qcs_facade::report(qcs_render_rows(r_, h_LocArry, &LocPara, RenderingMode, FixedlocPrec, FluoNum, cstream),
+                           "FluoRenderTop");
+    }
+    void ResetFillImgTop(LocalizationPara & /*LocPara*/) {
+        qcs_facade::report(qcs_render_reset(r_, nullptr), "ResetFillImgTop");
+    }
+    // Mode 0: maximum and histogram to zero (the rescale, mode 1, runs on the
+    // device inside FluoRenderTop)
+    void ResetFillMaxVal(int Mode) {
+        if (Mode == 0) qcs_facade::report(qcs_render_reset_max(r_, nullptr), "ResetFillMaxVal");
+    }
+    qcs_render_data *handle() { return r_; }
+
+private:
+    qcs_render_data *r_ = nullptr;
 };
 
 #endif /* QCSTORM_B200_HPP */

@@ -52,7 +52,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 # Reference sub-directories and translation units of the localization path.
 DIRS = ["bfgsMLE_Loc_LD", "bfgsMLE_Loc_HD", "bfgsMLE_Loc_top", "WLEParaEstimation",
-        "SubregionExtraction", "cudaWrapper"]
+        "SubregionExtraction", "cudaWrapper", "ImgRender"]
 UNITS = [
     "bfgsMLE_Loc_LD/bfgs_base.cu",
     "bfgsMLE_Loc_LD/bfgsMLE_Single_Emitter_Fit.cu",
@@ -66,6 +66,10 @@ UNITS = [
     "SubregionExtraction/LDROIExtraction.cu",
     "SubregionExtraction/LDROIExtraction_ImageFiltering.cu",
     "SubregionExtraction/LDROIExtraction_ROIExtraction.cu",
+    "ImgRender/ImageRender_2d.cu",
+    "ImgRender/ImageRender_3d.cu",
+    "ImgRender/ImageRender_top.cu",
+    "ImgRender/ImageRerender_rc.cu",
 ]
 
 LAUNCH = re.compile(

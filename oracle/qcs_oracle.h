@@ -64,6 +64,12 @@ int qcso_extract(const qcs_loc_para *p, const uint16_t *frames, int n_frames, in
                  int *n_roi, int *first_frame, int *end_frame);
 
 /* RemoveZeroLocalizations: rows n x 12 in, kept rows into out (n x 12), count in *n_out. */
+/* Super-resolution render of n rows into img (SRImageWidth x SRImageHigh) and,
+ * for 3D types, the z-weighted colormap; max_val and hist (400 ints) are the
+ * running display maximum and histogram.  All four are read and updated. */
+int qcso_render(const qcs_loc_para *p, const float *rows, int n, int mode, float fixed_prec, float *img,
+                float *colormap, int *max_val, int *hist);
+
 int qcso_zero_remove(const float *rows, int n, int sort_frame, int first_frame, int end_frame, float *out,
                      int *n_out);
 

@@ -27,6 +27,8 @@
 #include "bfgsMLE_AS3D_2Emitter_core.h"
 #include "LocPrecCalc_GaussianCRLB.h"
 #include "ZeroLocalizationsRemove.h"
+#include "ImageRender_2d.h"
+#include "ImageRender_3d.h"
 
 #include "../include/qcstorm_b200.h"
 
@@ -380,6 +382,52 @@ int qcsrefg_zero_remove(const float *rows, int n, int sort_frame, int first_fram
     cudaStreamDestroy(s);
     cudaFreeHost(pinned);
     z.Deinit();
+    return st;
+}
+
+// ImageRenderData_TypeDef::FluoRenderTop's device part (ImageRender_top.cu:29-60):
+// the reference's FluoRenderWithPrec_2D / _3D launchers (ImageRender_2d.cu:372,
+// ImageRender_3d.cu:333) on a render object holding only the buffers they
+// touch.  img, colormap (3D only; may be NULL for 2D), max_val and hist (400
+// ints) are read as the starting state and written back.
+int qcsrefg_render(const qcs_loc_para *p, const float *rows, int n, int mode, float fixed_prec, float *img, float *colormap,
+            int *max_val, int *hist) {
+    LocalizationPara r;
+    to_ref(p, r);
+    ImageRenderData_TypeDef d;
+    memset(&d, 0, sizeof(d));
+    const size_t px = (size_t)r.SRImageWidth * (size_t)r.SRImageHigh;
+    const bool is2d = RendType_Is2D(r.LocType);
+    const int padded = (n + 31) / 32 * 32 + 32;
+    cudaMalloc((void **)&d.d_LocArry, sizeof(float) * OutParaNumGS2D * (size_t)padded);
+    cudaMemset(d.d_LocArry, 0, sizeof(float) * OutParaNumGS2D * (size_t)padded);
+    if (n > 0) cudaMemcpy(d.d_LocArry, rows, sizeof(float) * OutParaNumGS2D * (size_t)n, cudaMemcpyHostToDevice);
+    cudaMalloc((void **)&d.d_SRIntensityImg, sizeof(float) * px);
+    cudaMemcpy(d.d_SRIntensityImg, img, sizeof(float) * px, cudaMemcpyHostToDevice);
+    if (!is2d) {
+        cudaMalloc((void **)&d.d_SRColorMapImg, sizeof(float) * px);
+        cudaMemcpy(d.d_SRColorMapImg, colormap, sizeof(float) * px, cudaMemcpyHostToDevice);
+    }
+    cudaMalloc((void **)&d.d_MaxImageVal, sizeof(int));
+    cudaMemcpy(d.d_MaxImageVal, max_val, sizeof(int), cudaMemcpyHostToDevice);
+    cudaMalloc((void **)&d.d_HistMaxDat, sizeof(int) * ImgRend_MaxDatHistLen);
+    cudaMemcpy(d.d_HistMaxDat, hist, sizeof(int) * ImgRend_MaxDatHistLen, cudaMemcpyHostToDevice);
+    if (n > 0) {
+        if (is2d)
+            ImgRender_FluoRenderWithPrec_2D(nullptr, &d, r, mode, fixed_prec, n, 0);
+        else
+            ImgRender_FluoRender_3D(nullptr, &d, r, mode, fixed_prec, n, 0);
+    }
+    int st = check();
+    cudaMemcpy(img, d.d_SRIntensityImg, sizeof(float) * px, cudaMemcpyDeviceToHost);
+    if (!is2d) cudaMemcpy(colormap, d.d_SRColorMapImg, sizeof(float) * px, cudaMemcpyDeviceToHost);
+    cudaMemcpy(max_val, d.d_MaxImageVal, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaMemcpy(hist, d.d_HistMaxDat, sizeof(int) * ImgRend_MaxDatHistLen, cudaMemcpyDeviceToHost);
+    cudaFree(d.d_LocArry);
+    cudaFree(d.d_SRIntensityImg);
+    if (!is2d) cudaFree(d.d_SRColorMapImg);
+    cudaFree(d.d_MaxImageVal);
+    cudaFree(d.d_HistMaxDat);
     return st;
 }
 

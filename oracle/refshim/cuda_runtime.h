@@ -73,6 +73,7 @@ using std::isnan;
 inline int atomicAdd(int *p, int v) { return __atomic_fetch_add(p, v, __ATOMIC_RELAXED); }
 inline unsigned int atomicAdd(unsigned int *p, unsigned int v) { return __atomic_fetch_add(p, v, __ATOMIC_RELAXED); }
 inline float atomicAdd(float *p, float v) { float o = *p; *p = o + v; return o; }
+inline int atomicMax(int *p, int v) { int o = *p; if (v > o) *p = v; return o; }
 
 // ---- runtime API subset ----------------------------------------------------
 typedef int cudaError_t;

@@ -79,6 +79,17 @@ _SIGS = {
     "qcs_learned_localize_async": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(LocPara),
                                              C.c_int, C.c_int, C.c_float, C.c_void_p]),
     "qcs_loc_finish": (C.c_int, [C.c_void_p, C.POINTER(LocPara)]),
+    "qcs_render_init": (C.c_int, [C.POINTER(LocPara), C.c_int, C.POINTER(C.c_void_p)]),
+    "qcs_render_deinit": (C.c_int, [C.c_void_p]),
+    "qcs_render_reset": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "qcs_render_reset_max": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "qcs_render_rows": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(LocPara), C.c_int, C.c_float, C.c_int,
+                                  C.c_void_p]),
+    "qcs_render_rows_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(LocPara), C.c_int,
+                                         C.c_float, C.c_void_p]),
+    "qcs_render_d_image": (C.c_void_p, [C.c_void_p]),
+    "qcs_render_d_colormap": (C.c_void_p, [C.c_void_p]),
+    "qcs_render_read": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "qcs_learned_fused_status": (C.c_int, [C.c_void_p]),
     "qcs_fit_from_start_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(LocPara), C.c_int,
                                             C.c_void_p, C.c_int, C.c_float, C.c_void_p]),
@@ -491,3 +502,59 @@ def fit_from_start(ctx, d_rois, n, d_start, d_wle=0, iters=3, dev_th=0.0, para=N
     check(load().qcs_fit_from_start_device(ctx.h, C.c_void_p(d_rois), C.c_void_p(d_wle) if d_wle else None,
                                            C.byref(para), int(n), C.c_void_p(d_start), int(iters), C.c_float(dev_th),
                                            C.c_void_p(stream) if stream else None))
+
+
+class RenderContext:
+    """Super-resolution render (qcs_render_*): SR image, colour map (3D), display maximum and histogram."""
+
+    def __init__(self, para, capacity=0):
+        self.lib = load()
+        self.para = para
+        h = C.c_void_p()
+        check(self.lib.qcs_render_init(C.byref(para), int(capacity), C.byref(h)))
+        self.h = h.value
+
+    def close(self):
+        if self.h:
+            self.lib.qcs_render_deinit(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def reset(self, stream=0, display=True):
+        """Images to zero (and, with display, the maximum and histogram)."""
+        st = C.c_void_p(stream) if stream else None
+        check(self.lib.qcs_render_reset(self.h, st))
+        if display:
+            check(self.lib.qcs_render_reset_max(self.h, st))
+
+    def render(self, rows, mode=0, fixed_prec=0.0, para=None, stream=0):
+        """qcs_render_rows on host rows (n x 12)."""
+        para = para or self.para
+        rows, pr = _host(rows, np.float32)
+        check(self.lib.qcs_render_rows(self.h, pr, C.byref(para), int(mode), C.c_float(fixed_prec), rows.shape[0],
+                                       C.c_void_p(stream) if stream else None))
+
+    def render_device(self, d_rows, d_n, max_n, mode=0, fixed_prec=0.0, para=None, stream=0):
+        """qcs_render_rows_device: rows and (optionally) their count in device memory."""
+        para = para or self.para
+        check(self.lib.qcs_render_rows_device(self.h, C.c_void_p(d_rows), C.c_void_p(d_n) if d_n else None,
+                                              int(max_n), C.byref(para), int(mode), C.c_float(fixed_prec),
+                                              C.c_void_p(stream) if stream else None))
+
+    def read(self, stream=0):
+        """(image, colormap or None, max, hist) on the host."""
+        shape = (self.para.SRImageHigh, self.para.SRImageWidth)
+        img = np.zeros(shape, np.float32)
+        is3d = self.para.LocType != 0
+        cmap = np.zeros(shape, np.float32) if is3d else None
+        mx = C.c_int(0)
+        hist = np.zeros(400, np.int32)
+        check(self.lib.qcs_render_read(self.h, C.c_void_p(img.ctypes.data),
+                                       C.c_void_p(cmap.ctypes.data) if is3d else None, C.byref(mx),
+                                       C.c_void_p(hist.ctypes.data), C.c_void_p(stream) if stream else None))
+        return img, cmap, mx.value, hist

@@ -69,6 +69,16 @@ int main(int argc, char **argv) {
     zero.RemoveZeroLocalizations(loc.h_LocArry, loc.oValidFluoNum, 1, extract.FirstFrame, extract.EndFrame, stream);
     spill(dir + "/kept.bin", zero.h_LocArry, sizeof(float) * OutParaNumGS2D * zero.ValidFluoNum);
 
+    para.UpdateSRImageSize();
+    ImageRenderData_TypeDef render;
+    render.Init(para, 0, 0);
+    render.FluoRenderTop(zero.h_LocArry, para, RenderingMode_FittedPhoton_CalculatedLocPrec, 0, zero.ValidFluoNum,
+                         stream);
+    std::vector<float> img((size_t)para.SRImageWidth * para.SRImageHigh);
+    cudaMemcpy(img.data(), render.d_SRIntensityImg, img.size() * sizeof(float), cudaMemcpyDeviceToHost);
+    spill(dir + "/render.bin", img.data(), img.size() * sizeof(float));
+    render.Deinit(para);
+
     FILE *c = fopen((dir + "/counts.txt").c_str(), "w");
     fprintf(c, "%d %d %d %d %d %d %d\n", n, loc.oValidFluoNum, zero.ValidFluoNum, extract.FirstFrame, extract.EndFrame,
             LDLocData_TypeDef::GetFirstFrame(zero.h_LocArry, zero.ValidFluoNum),

@@ -169,3 +169,25 @@ def zero_remove(rows, sort_frame=0, first_frame=0, end_frame=0, lib="oracle"):
     st = f(_p(rows), rows.shape[0], int(sort_frame), int(first_frame), int(end_frame), _p(out), C.byref(n))
     assert st == 0, st
     return out[:n.value].copy()
+
+
+def render(para, rows, mode, fixed_prec=0.0, state=None, lib="oracle"):
+    """Super-resolution render of rows through the oracle ("oracle"), the host
+    build of the reference ("ref") or its CUDA build ("ref_gpu").  state:
+    (image, colormap, max, hist) to start from (zeros when None).  Returns the
+    updated (image, colormap, max, hist)."""
+    rows = np.ascontiguousarray(rows, np.float32)
+    shape = (para.SRImageHigh, para.SRImageWidth)
+    if state is None:
+        img, cmap = np.zeros(shape, np.float32), np.zeros(shape, np.float32)
+        mx, hist = 0, np.zeros(400, np.int32)
+    else:
+        img, cmap, mx, hist = (np.array(state[0], np.float32), np.array(state[1], np.float32), int(state[2]),
+                               np.array(state[3], np.int32))
+    m = C.c_int(mx)
+    f = {"oracle": lambda: oracle().qcso_render, "ref": lambda: ref_host().qcsref_render,
+         "ref_gpu": lambda: ref_gpu().qcsrefg_render}[lib]()
+    st = f(C.byref(para), _p(rows), rows.shape[0], int(mode), C.c_float(fixed_prec), _p(img), _p(cmap),
+           C.byref(m), _p(hist))
+    assert st == 0, st
+    return img, cmap, m.value, hist
