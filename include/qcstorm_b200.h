@@ -444,6 +444,32 @@ float *qcs_render_d_colormap(qcs_render_data *r);
  * host and waits. */
 int qcs_render_read(qcs_render_data *r, float *h_img, float *h_colormap, int *h_max, int *h_hist, void *stream);
 
+/* ---- localization file (12 float32 per row) ------------------------------ */
+/* The worker's LocFile.Write(WriteLocArry, WriteLocNum * OutParaNumGS2D *
+ * sizeof(float)) (Plugin for ImageJ/QC-STORM_ CPPDLL/QC-STORM_ CPPDLL/
+ * OnlineLocalizationLD.cpp:284): rows appended as 12 native float32 each, no
+ * header, the file utility/Output file load and postprocessing/
+ * py_LoadBinaryLocData.py reads with np.fromfile(...).reshape(-1, 12). */
+typedef struct qcs_locfile qcs_locfile;
+/* append = 0 truncates; capacity: most rows per qcs_locfile_write_device call
+ * (<= 0: 2 x QCS_MAX_POINT_NUM), for its two pinned staging buffers. */
+int qcs_locfile_open(const char *path, int append, int capacity, qcs_locfile **out);
+/* Appends n host rows (after any device rows queued before). */
+int qcs_locfile_write(qcs_locfile *f, const float *h_rows, int n);
+/* Appends rows on the device, their count read at d_n (NULL: max_n) -- e.g.
+ * the output of qcs_zero_remove_device -- without waiting: the copy and the
+ * append run in order on `stream` (a host function appends after the copy).
+ * Reuses a staging buffer only after its previous append; rows[0, max_n) must
+ * stay valid until the copy has run.  Appends happen in the order of their
+ * stream: give every call on one file the same stream. */
+int qcs_locfile_write_device(qcs_locfile *f, const float *d_rows, const int *d_n, int max_n, void *stream);
+/* Waits for queued appends and flushes the file. */
+int qcs_locfile_flush(qcs_locfile *f);
+/* Rows in the file (after qcs_locfile_flush for device rows). */
+long long qcs_locfile_rows(const qcs_locfile *f);
+/* Waits for queued appends and closes; reports a failed write. */
+int qcs_locfile_close(qcs_locfile *f);
+
 /* ---- allocation-free localization --------------------------------------- */
 /*
  * No counterpart in the reference.  For callers that cannot allocate device

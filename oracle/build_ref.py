@@ -4,8 +4,9 @@
 Compiles the reference's own CUDA sources (MLEbfgs/bfgs_MLE_dll x64/bfgsMLE_dll/
 bfgsMLE_dll/) with g++ against the host shim in oracle/refshim/, links them with
 oracle/ref_harness.cpp and writes oracle/_ref/libqcs_ref_host.so.  The result
-runs the reference's fit kernels, WLE pre-pass, CRLB, cascade orchestration and
-ROI extraction on the CPU, one emulated CUDA block at a time; it is the checker
+runs the reference's fit kernels, WLE pre-pass, CRLB, cascade orchestration,
+ROI extraction and super-resolution render on the CPU, one emulated CUDA block
+at a time; it is the checker
 the CPU oracle (oracle/qcs_oracle.c) is pinned against.
 
 Two mechanical rewrites are applied while the sources are read, into a

@@ -23,7 +23,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2,-ffp-contract=off", "-I" + INCLUDE]
 
 UNITS = ["qcs_fit_kernels.cu", "qcs_crlb.cu", "qcs_wle.cu", "qcs_cascade.cu", "qcs_api.cu", "qcs_diag.cu", "qcs_noalloc.cu",
-         "qcs_extract.cu", "qcs_post.cu", "qcs_learned.cu", "qcs_render.cu"]
+         "qcs_extract.cu", "qcs_post.cu", "qcs_learned.cu", "qcs_render.cu",
+         "qcs_locfile.cu"]
 
 
 def deps():

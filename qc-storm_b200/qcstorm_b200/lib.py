@@ -79,6 +79,12 @@ _SIGS = {
     "qcs_learned_localize_async": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(LocPara),
                                              C.c_int, C.c_int, C.c_float, C.c_void_p]),
     "qcs_loc_finish": (C.c_int, [C.c_void_p, C.POINTER(LocPara)]),
+    "qcs_locfile_open": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
+    "qcs_locfile_write": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
+    "qcs_locfile_write_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    "qcs_locfile_flush": (C.c_int, [C.c_void_p]),
+    "qcs_locfile_rows": (C.c_longlong, [C.c_void_p]),
+    "qcs_locfile_close": (C.c_int, [C.c_void_p]),
     "qcs_render_init": (C.c_int, [C.POINTER(LocPara), C.c_int, C.POINTER(C.c_void_p)]),
     "qcs_render_deinit": (C.c_int, [C.c_void_p]),
     "qcs_render_reset": (C.c_int, [C.c_void_p, C.c_void_p]),
@@ -558,3 +564,32 @@ class RenderContext:
                                        C.c_void_p(cmap.ctypes.data) if is3d else None, C.byref(mx),
                                        C.c_void_p(hist.ctypes.data), C.c_void_p(stream) if stream else None))
         return img, cmap, mx.value, hist
+
+
+class LocFile:
+    """Localization file: 12 float32 per row (qcs_locfile_*)."""
+
+    def __init__(self, path, append=False, capacity=0):
+        self.lib = load()
+        h = C.c_void_p()
+        check(self.lib.qcs_locfile_open(os.fsencode(path), int(bool(append)), int(capacity), C.byref(h)))
+        self.h = h.value
+
+    def write(self, rows):
+        rows, pr = _host(rows, np.float32)
+        check(self.lib.qcs_locfile_write(self.h, pr, int(rows.shape[0])))
+
+    def write_device(self, d_rows, d_n, max_n, stream=0):
+        check(self.lib.qcs_locfile_write_device(self.h, C.c_void_p(d_rows), C.c_void_p(d_n) if d_n else None,
+                                                int(max_n), C.c_void_p(stream) if stream else None))
+
+    def flush(self):
+        check(self.lib.qcs_locfile_flush(self.h))
+
+    def rows(self):
+        return int(self.lib.qcs_locfile_rows(self.h))
+
+    def close(self):
+        if self.h:
+            h, self.h = self.h, None
+            check(self.lib.qcs_locfile_close(h))
