@@ -263,6 +263,7 @@ def frame_pipeline(stream, steps, warmup, e2e=True):
 
 
 LEARNED_ITERS = 2          # BFGS iterations from the network's start points (plain: 8)
+LEARNED_BISECTIONS = 6     # line-search steps per iteration (plain: 11)
 TRAIN_RECORDS = 200_000    # training records, same generator, seeds disjoint from the timed batches
 TRAIN_EPOCHS = 8
 
@@ -311,7 +312,7 @@ def e2e_pipelined(ctxs, streams, h_batches, steps, net=None):
         if k >= 2:
             rows += c.finish(copy=False)[0].shape[0]
         c.localize_async(h_batches[k % len(h_batches)].data_ptr(), N_PER_STEP, stream=streams[k % 2].cuda_stream,
-                         net=net, iters=LEARNED_ITERS)
+                         net=net, iters=LEARNED_ITERS, bisections=LEARNED_BISECTIONS)
     for k in range(max(0, steps - 2), steps):
         rows += ctxs[k % 2].finish(copy=False)[0].shape[0]
     return time.perf_counter() - t0, rows
@@ -328,7 +329,8 @@ def fit_accuracy(rows, rec, truth, sel, para):
 
 
 def learned_measure(args, stream, ctx, para, d_batches, h_batches, rec0, truth0, plain_value, world, dist):
-    """Learned start points + LEARNED_ITERS BFGS iterations + plain refits of
+    """Learned start points + LEARNED_ITERS BFGS iterations (LEARNED_BISECTIONS
+    line-search steps each, analytic gradient) + plain refits of
     the fits the deviance judge rejects + CRLB (qcs_learned_localize_device),
     on the same device-resident batches as the plain step, WLE pre-pass
     included; accuracy of plain vs learned on batch 0 against ground truth."""
@@ -337,7 +339,8 @@ def learned_measure(args, stream, ctx, para, d_batches, h_batches, rec0, truth0,
     net, train = train_learned_net(para, stream)
 
     def step(k):
-        net.localize(ctx, d_batches[k % BATCHES].data_ptr(), N_PER_STEP, 0, iters=LEARNED_ITERS, stream=sh)
+        net.localize(ctx, d_batches[k % BATCHES].data_ptr(), N_PER_STEP, 0, iters=LEARNED_ITERS,
+                     bisections=LEARNED_BISECTIONS, stream=sh)
 
     for k in range(args.warmup):
         step(k)
@@ -382,7 +385,8 @@ def learned_measure(args, stream, ctx, para, d_batches, h_batches, rec0, truth0,
     net.close()
     return {
         "value": value, "unit": UNIT, "ms_per_step": ms / args.steps, "vs_plain": value / plain_value,
-        "iters": LEARNED_ITERS, "refits_per_step": refits,
+        "iters": LEARNED_ITERS, "bisections": LEARNED_BISECTIONS, "refits_per_step": refits,
+        # mlp_tc (features + network), WLE (5), fit_learned, flag_queue, group refit, refit CRLB, counters, CRLB
         "gpu_launches_per_step": 12,
         "e2e": {"value": e2e_steps * N_PER_STEP * world / e2e_s, "unit": UNIT,
                 "h2d_bytes_per_step": N_PER_STEP * R * (R + 1) * 2,
@@ -414,7 +418,7 @@ def profile_learned(n, stream):
     torch.cuda.synchronize()
     torch.cuda.nvtx.range_push("learned")
     for _ in range(3):
-        net.localize(ctx, d.data_ptr(), n, 0, iters=LEARNED_ITERS, stream=sh)
+        net.localize(ctx, d.data_ptr(), n, 0, iters=LEARNED_ITERS, bisections=LEARNED_BISECTIONS, stream=sh)
     torch.cuda.synchronize()
     torch.cuda.nvtx.range_pop()
     print(json.dumps({"profile_learned": n, "refits": net.refits(ctx)}))
@@ -513,7 +517,9 @@ def main():
     def step(k):
         ctx.localize_device(d_batches[k % BATCHES].data_ptr(), N_PER_STEP, 0, sh)
 
-    launches_per_step = 8  # psf_width, nn_keys, nn_scan, classify, init_counters, fit, finish, crlb
+    # psf_width, nn_keys_flag, the sort's condition kernel (the sort itself only for out-of-order records),
+    # nn_scan_select, classify, init_counters, fit, finish, crlb
+    launches_per_step = 9
 
     # ---- device-timed steps
     for k in range(args.warmup):

@@ -380,18 +380,20 @@ int qcs_learned_start_device(qcs_learned_net *net, const qcs_loc_para *p, const 
                              float *d_start, float *d_work, void *stream);
 size_t qcs_learned_work_bytes(int n);
 /* GS2D 7x7 single-emitter fits from given start points d_start (n x 5: peak
- * e-, x, y in ROI pixels, sigma, background e-) with `iters` BFGS iterations
- * (2..5 or 8) and the plain fit's loss, line search and accept rules; fits
- * that are not accepted or whose Poisson deviance exceeds dev_th (<= 0: 100)
- * are refitted by the plain kernel; then CRLB.  Rows in the context (n). */
+ * e-, x, y in ROI pixels, sigma, background e-) with the plain fit's weighted
+ * loss and accept rules, `iters` BFGS iterations of `bisections` line-search
+ * steps each (<= 0: the reference's 11; schedules: 2..5 or 8 iterations with
+ * 11 steps, 2 or 3 with 4, 6 or 8) and the loss's analytic gradient; fits that
+ * are not accepted or whose Poisson deviance exceeds dev_th (<= 0: 100) are
+ * refitted by the plain kernel; then CRLB.  Rows in the context (n). */
 int qcs_fit_from_start_device(qcs_loc_data *c, const uint16_t *d_rois, const float *d_wle, const qcs_loc_para *p,
-                              int n, const float *d_start, int iters, float dev_th, void *stream);
-/* GS2D 7x7 single-emitter localization from learned start points: `iters`
- * BFGS iterations (2..5 or 8) instead of 8; fits that are not accepted or
- * whose Poisson deviance exceeds dev_th (<= 0: 100) are refitted by the plain
- * kernel; then CRLB.  Rows in the context like qcs_loc_localize_device (n rows). */
+                              int n, const float *d_start, int iters, int bisections, float dev_th, void *stream);
+/* GS2D 7x7 single-emitter localization from learned start points with the
+ * schedule of qcs_fit_from_start_device.  Rows in the context like
+ * qcs_loc_localize_device (n rows). */
 int qcs_learned_localize_device(qcs_loc_data *c, qcs_learned_net *net, const uint16_t *d_rois, const float *d_wle,
-                                const qcs_loc_para *p, int n, int iters, float dev_th, void *stream);
+                                const qcs_loc_para *p, int n, int iters, int bisections, float dev_th,
+                                void *stream);
 /* Inference path of qcs_learned_localize_device: fused = 1 (default) runs the
  * whole network per 128-ROI tile in one tcgen05 kernel; 0 runs it layer by
  * layer through the training GEMMs. */
@@ -405,7 +407,8 @@ int qcs_learned_fused_status(qcs_learned_net *net);
  * buffer, and its weight image is rebuilt only after a parameter change
  * (change parameters only while no call using the network is in flight). */
 int qcs_learned_localize_async(qcs_loc_data *c, qcs_learned_net *net, const uint16_t *h_rois, const float *h_wle,
-                               const qcs_loc_para *p, int n, int iters, float dev_th, void *stream);
+                               const qcs_loc_para *p, int n, int iters, int bisections, float dev_th,
+                               void *stream);
 /* Number of plain refits of the last qcs_learned_localize_device call (waits for it). */
 int qcs_learned_refit_num(qcs_loc_data *c, int *n);
 

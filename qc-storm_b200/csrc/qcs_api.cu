@@ -268,12 +268,15 @@ __global__ void learned_counters_kernel(qcs::CascadeState st, int n) {
 extern "C" {
 
 int qcs_fit_from_start_device(qcs_loc_data *c, const uint16_t *d_rois, const float *d_wle, const qcs_loc_para *p,
-                              int n, const float *d_start, int iters, float dev_th, void *stream) {
+                              int n, const float *d_start, int iters, int bisections, float dev_th, void *stream) {
     int st = check_call(c, p, n);
     if (st) return st;
     if (p->LocType != QCS_LOCTYPE_GS2D || p->ROISize != 7 || p->MultiEmitterFitEn)
         return fail(QCS_ERR_ARG, "start-point fits: GS2D 7x7 single-emitter fitting only");
-    if (!(iters >= 2 && iters <= 5) && iters != 8) return fail(QCS_ERR_ARG, "iters must be 2..5 or 8");
+    if (bisections <= 0) bisections = 11;
+    const bool schedule = (bisections == 11 && ((iters >= 2 && iters <= 5) || iters == 8)) ||
+                          ((iters == 2 || iters == 3) && (bisections == 4 || bisections == 6 || bisections == 8));
+    if (!schedule) return fail(QCS_ERR_ARG, "schedule: iters 2..5 or 8 with 11 bisections, or 2..3 with 4, 6 or 8");
     if (n == 0) return QCS_OK;
     if (!d_rois || !d_start) return fail(QCS_ERR_ARG, "null pointer");
     if (!(dev_th > 0.0f)) dev_th = 100.0f;
@@ -293,7 +296,7 @@ int qcs_fit_from_start_device(qcs_loc_data *c, const uint16_t *d_rois, const flo
     f.mo = qcs::MultiOut{nullptr, nullptr};
     f.para = qcs::core_para(*p);
     f.stream = s;
-    QCS_CUDA(qcs::launch_fit_learned(7, iters, f, d_start, dev_th, c->st.to2e, n), "start-point fit");
+    QCS_CUDA(qcs::launch_fit_learned(7, iters, bisections, f, d_start, dev_th, c->st.to2e, n), "start-point fit");
     // plain refit of the flagged records
     QCS_CUDA(qcs::launch_flag_queue(c->st.to2e, n, c->st.q_single, c->st.counters + qcs::kCntSingle, s),
              "refit queue");
@@ -319,7 +322,7 @@ int qcs_fit_from_start_device(qcs_loc_data *c, const uint16_t *d_rois, const flo
 }
 
 int qcs_learned_localize_device(qcs_loc_data *c, qcs_learned_net *net, const uint16_t *d_rois, const float *d_wle,
-                                const qcs_loc_para *p, int n, int iters, float dev_th, void *stream) {
+                                const qcs_loc_para *p, int n, int iters, int bisections, float dev_th, void *stream) {
     int st = check_call(c, p, n);
     if (st) return st;
     if (!net) return fail(QCS_ERR_ARG, "null network");
@@ -329,7 +332,7 @@ int qcs_learned_localize_device(qcs_loc_data *c, qcs_learned_net *net, const uin
     if (!d_rois) return fail(QCS_ERR_ARG, "null ROI pointer");
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
     QCS_CUDA(qcs::learned::start_points(net, p, d_rois, n, c->d_start, s), "learned start points");
-    return qcs_fit_from_start_device(c, d_rois, d_wle, p, n, c->d_start, iters, dev_th, s);
+    return qcs_fit_from_start_device(c, d_rois, d_wle, p, n, c->d_start, iters, bisections, dev_th, s);
 }
 
 int qcs_learned_refit_num(qcs_loc_data *c, int *n) {
@@ -450,13 +453,14 @@ int qcs_loc_localize_async(qcs_loc_data *c, const uint16_t *h_rois, const float 
 }
 
 int qcs_learned_localize_async(qcs_loc_data *c, qcs_learned_net *net, const uint16_t *h_rois, const float *h_wle,
-                               const qcs_loc_para *p, int n, int iters, float dev_th, void *stream) {
+                               const qcs_loc_para *p, int n, int iters, int bisections, float dev_th,
+                               void *stream) {
     int st = check_call(c, p, n);
     if (st) return st;
     if (!net) return fail(QCS_ERR_ARG, "null network");
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
     return enqueue_host_call(c, h_rois, h_wle, p, n, s, [&](const float *d_wle) {
-        return qcs_learned_localize_device(c, net, c->d_rois, d_wle, p, n, iters, dev_th, s);
+        return qcs_learned_localize_device(c, net, c->d_rois, d_wle, p, n, iters, bisections, dev_th, s);
     });
 }
 

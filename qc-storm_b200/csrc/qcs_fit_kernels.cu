@@ -455,7 +455,7 @@ __global__ void __launch_bounds__(kGroupTPB) fit_single_group_kernel(const uint1
 // is not accepted or when its unweighted Poisson deviance
 // 2 sum(mu - n - n ln(mu / n)) exceeds dev_th: those ROIs are refitted by the
 // plain kernel.
-template <int R, int ITERS, int DIST = ArithSpec<kGS2D, R>::DIST, int MASK = ArithSpec<kGS2D, R>::MASK>
+template <int R, int ITERS, int NB, int DIST = ArithSpec<kGS2D, R>::DIST, int MASK = ArithSpec<kGS2D, R>::MASK>
 __global__ void __launch_bounds__(kTPB) fit_learned_kernel(const uint16_t *__restrict__ rois,
                                                            const float *__restrict__ wle,
                                                            const float *__restrict__ start, int n,
@@ -501,7 +501,7 @@ __global__ void __launch_bounds__(kTPB) fit_learned_kernel(const uint16_t *__res
     Ininf[2] = st[2];
     Ininf[3] = (0.5f / (st[3] * st[3])) * rSScalFactor;
     Ininf[4] = st[4] * rBScalFactor;
-    bfgs_fit<P, ITERS>(AnalyticEvalGS2D<R, DIST>{roi}, Ininf, D, kTPB);
+    bfgs_fit<P, ITERS, AnalyticEvalGS2D<R, DIST>, NB>(AnalyticEvalGS2D<R, DIST>{roi}, Ininf, D, kTPB);
 
     const float PeakPhoton = Ininf[0] * QCS_ASCALE / c.QE;
     const float Background = Ininf[4] * QCS_BSCALE / c.QE;
@@ -561,10 +561,10 @@ __global__ void flag_queue_kernel(const uint8_t *__restrict__ flags, int n, int 
     if (f) ids[base + __popc(ballot & ((1u << lane) - 1u))] = i;
 }
 
-template <int R, int ITERS>
+template <int R, int ITERS, int NB>
 cudaError_t launch_learned(const FitLaunch &a, const float *start, float dev_th, uint8_t *refit, int n) {
     const size_t smem = SmemLayout<R, kGS2D>::TOTAL * sizeof(float);
-    auto k = fit_learned_kernel<R, ITERS>;
+    auto k = fit_learned_kernel<R, ITERS, NB>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const int grid = (n + kTPB - 1) / kTPB;
@@ -846,17 +846,29 @@ cudaError_t launch_multi(const FitLaunch &a) {
 
 }  // namespace
 
-cudaError_t launch_fit_learned(int R, int iters, const FitLaunch &a, const float *start, float dev_th,
-                               uint8_t *refit, int n) {
+cudaError_t launch_fit_learned(int R, int iters, int bisections, const FitLaunch &a, const float *start,
+                               float dev_th, uint8_t *refit, int n) {
     if (R != 7) return cudaErrorInvalidValue;
-    switch (iters) {
-    case 2: return launch_learned<7, 2>(a, start, dev_th, refit, n);
-    case 3: return launch_learned<7, 3>(a, start, dev_th, refit, n);
-    case 4: return launch_learned<7, 4>(a, start, dev_th, refit, n);
-    case 5: return launch_learned<7, 5>(a, start, dev_th, refit, n);
-    case 8: return launch_learned<7, 8>(a, start, dev_th, refit, n);
-    default: return cudaErrorInvalidValue;
+    if (bisections == kBisections) {
+        switch (iters) {
+        case 2: return launch_learned<7, 2, kBisections>(a, start, dev_th, refit, n);
+        case 3: return launch_learned<7, 3, kBisections>(a, start, dev_th, refit, n);
+        case 4: return launch_learned<7, 4, kBisections>(a, start, dev_th, refit, n);
+        case 5: return launch_learned<7, 5, kBisections>(a, start, dev_th, refit, n);
+        case 8: return launch_learned<7, 8, kBisections>(a, start, dev_th, refit, n);
+        }
+        return cudaErrorInvalidValue;
     }
+#define QCS_LEARNED(IT, NB) \
+    if (iters == IT && bisections == NB) return launch_learned<7, IT, NB>(a, start, dev_th, refit, n);
+    QCS_LEARNED(2, 4)
+    QCS_LEARNED(2, 6)
+    QCS_LEARNED(2, 8)
+    QCS_LEARNED(3, 4)
+    QCS_LEARNED(3, 6)
+    QCS_LEARNED(3, 8)
+#undef QCS_LEARNED
+    return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_flag_queue(const uint8_t *flags, int n, int *ids, int *count, cudaStream_t s) {

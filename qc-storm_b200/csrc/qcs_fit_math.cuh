@@ -509,10 +509,11 @@ struct GroupEval {
     }
 };
 
-// Fixed schedule: IT quasi-Newton iterations, each with an 11-step bisection
-// of the step length in [1e-5, 1]; no convergence test.  D: P x P scratch at
-// D[(r * P + c) * ld]; ev evaluates the loss and the gradient.
-template <int P, int IT, class Eval>
+// Fixed schedule: IT quasi-Newton iterations, each with an NB-step bisection
+// of the step length in [1e-5, 1] (the reference: 11); no convergence test.
+// D: P x P scratch at D[(r * P + c) * ld]; ev evaluates the loss and the
+// gradient.
+template <int P, int IT, class Eval, int NB = kBisections>
 __device__ __forceinline__ void bfgs_fit(const Eval &ev, float *Ininf, float *D, int ld) {
     float grad[P], d0[P], td0[P], sk[P], yk[P], tgrad[P];
     float ddat[2], dpos[2];  // two-element arrays indexed by constants only
@@ -551,12 +552,12 @@ __device__ __forceinline__ void bfgs_fit(const Eval &ev, float *Ininf, float *D,
         // Bisection: the half that moves is chosen per ROI; the moved point
         // is built with a select so that every thread of a warp runs the same
         // single loss evaluation (no divergent branches around the loss).
-        for (int cnt = 0; cnt < kBisections; cnt++) {
+        for (int cnt = 0; cnt < NB; cnt++) {
             const int xdsel = (ddat[0] < ddat[1]);
             const float mid = (dpos[0] + dpos[1]) * 0.5f;
             dpos[0] = xdsel ? dpos[0] : mid;
             dpos[1] = xdsel ? mid : dpos[1];
-            if (cnt < kBisections - 1) {
+            if (cnt < NB - 1) {
                 const float dsel = xdsel ? dpos[1] : dpos[0];
                 float xn[P];
 #pragma unroll

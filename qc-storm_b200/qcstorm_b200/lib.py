@@ -72,12 +72,12 @@ _SIGS = {
                                            C.c_void_p, C.c_void_p]),
     "qcs_learned_work_bytes": (C.c_size_t, [C.c_int]),
     "qcs_learned_localize_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(LocPara),
-                                              C.c_int, C.c_int, C.c_float, C.c_void_p]),
+                                              C.c_int, C.c_int, C.c_int, C.c_float, C.c_void_p]),
     "qcs_learned_refit_num": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "qcs_learned_set_inference": (C.c_int, [C.c_void_p, C.c_int]),
     "qcs_loc_localize_async": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(LocPara), C.c_int, C.c_void_p]),
     "qcs_learned_localize_async": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(LocPara),
-                                             C.c_int, C.c_int, C.c_float, C.c_void_p]),
+                                             C.c_int, C.c_int, C.c_int, C.c_float, C.c_void_p]),
     "qcs_loc_finish": (C.c_int, [C.c_void_p, C.POINTER(LocPara)]),
     "qcs_locfile_open": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
     "qcs_locfile_write": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),
@@ -98,7 +98,7 @@ _SIGS = {
     "qcs_render_read": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "qcs_learned_fused_status": (C.c_int, [C.c_void_p]),
     "qcs_fit_from_start_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(LocPara), C.c_int,
-                                            C.c_void_p, C.c_int, C.c_float, C.c_void_p]),
+                                            C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_void_p]),
     "qcs_extract_max_batched_num": (C.c_int, [C.c_int, C.c_int]),
     "qcs_extract_init": (C.c_int, [C.POINTER(LocPara), C.POINTER(C.c_void_p)]),
     "qcs_extract_init_ex": (C.c_int, [C.POINTER(LocPara), C.c_int, C.c_int, C.POINTER(C.c_void_p)]),
@@ -196,7 +196,8 @@ class LocContext:
         check(self.lib.qcs_wle_estimate(self.h, pr, rois.shape[0], C.byref(para), C.c_void_p(out.ctypes.data)))
         return out
 
-    def localize_async(self, h_rois_ptr, n, h_wle_ptr=0, stream=0, para=None, net=None, iters=2, dev_th=0.0):
+    def localize_async(self, h_rois_ptr, n, h_wle_ptr=0, stream=0, para=None, net=None, iters=2, dev_th=0.0,
+                       bisections=0):
         """qcs_loc_localize_async (or, with net, qcs_learned_localize_async) on host
         memory given by address (pinned for overlap); finish() publishes the rows."""
         para = para or self.para
@@ -207,7 +208,7 @@ class LocContext:
             check(self.lib.qcs_loc_localize_async(self.h, C.c_void_p(h_rois_ptr), wle, C.byref(para), int(n), st))
         else:
             check(self.lib.qcs_learned_localize_async(self.h, net.h, C.c_void_p(h_rois_ptr), wle, C.byref(para),
-                                                      int(n), int(iters), C.c_float(dev_th), st))
+                                                      int(n), int(iters), int(bisections), C.c_float(dev_th), st))
 
     def finish(self, copy=True):
         """qcs_loc_finish: (rows[n_valid, 12], ratios[7]); copy=False returns a view of
@@ -483,11 +484,12 @@ class LearnedNet:
                                                 C.c_void_p(stream) if stream else None))
         return st
 
-    def localize(self, ctx, d_rois, n, d_wle=0, iters=3, dev_th=0.0, para=None, stream=0):
+    def localize(self, ctx, d_rois, n, d_wle=0, iters=3, dev_th=0.0, para=None, stream=0, bisections=0):
         """qcs_learned_localize_device on a LocContext; rows stay in the context."""
         para = para or ctx.para
         check(self.lib.qcs_learned_localize_device(ctx.h, self.h, C.c_void_p(d_rois), C.c_void_p(d_wle) if d_wle else None,
-                                                   C.byref(para), int(n), int(iters), C.c_float(dev_th),
+                                                   C.byref(para), int(n), int(iters), int(bisections),
+                                                   C.c_float(dev_th),
                                                    C.c_void_p(stream) if stream else None))
 
     def set_fused(self, fused=True):
@@ -502,11 +504,12 @@ class LearnedNet:
         return k.value
 
 
-def fit_from_start(ctx, d_rois, n, d_start, d_wle=0, iters=3, dev_th=0.0, para=None, stream=0):
+def fit_from_start(ctx, d_rois, n, d_start, d_wle=0, iters=3, dev_th=0.0, para=None, stream=0, bisections=0):
     """qcs_fit_from_start_device: GS2D 7x7 fits from given start points; rows stay in the context."""
     para = para or ctx.para
     check(load().qcs_fit_from_start_device(ctx.h, C.c_void_p(d_rois), C.c_void_p(d_wle) if d_wle else None,
-                                           C.byref(para), int(n), C.c_void_p(d_start), int(iters), C.c_float(dev_th),
+                                           C.byref(para), int(n), C.c_void_p(d_start), int(iters), int(bisections),
+                                           C.c_float(dev_th),
                                            C.c_void_p(stream) if stream else None))
 
 

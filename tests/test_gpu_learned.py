@@ -177,9 +177,10 @@ def rmse_photons(rows, truth, sel):
     return float(np.sqrt(np.mean((rows[sel, 6] / truth["photons"][sel] - 1) ** 2)))
 
 
-def test_trained_start_points_reach_plain_rmse_with_fewer_iterations(cuda_ok):
+@pytest.mark.parametrize("bisections", [11, 6])
+def test_trained_start_points_reach_plain_rmse_with_fewer_iterations(cuda_ok, bisections):
     """Train on 200k ROIs labelled by plain fits; on 50k fresh ROIs, 2 BFGS
-    iterations from the network's start points (plus plain refits of the
+    iterations (11 or 6 line-search steps) from the network's start points (plus plain refits of the
     fits the deviance judge rejects) match plain 8-iteration fits in position
     RMSE and beat them in photon RMSE, while 2 iterations from the plain
     centre / edge-mean start do not reach the plain RMSE."""
@@ -202,11 +203,12 @@ def test_trained_start_points_reach_plain_rmse_with_fewer_iterations(cuda_ok):
     s = torch.cuda.Stream()
     ctx.localize_device(d_ev.data_ptr(), m, 0, s.cuda_stream)
     plain, _ = ctx.read_rows(s.cuda_stream)
-    net.localize(ctx, d_ev.data_ptr(), m, iters=2, stream=s.cuda_stream)
+    net.localize(ctx, d_ev.data_ptr(), m, iters=2, bisections=bisections, stream=s.cuda_stream)
     learned, _ = ctx.read_rows(s.cuda_stream)
     refits = net.refits(ctx)
     d_start = to_dev(naive_start(ev, para))
-    qlib.fit_from_start(ctx, d_ev.data_ptr(), m, d_start.data_ptr(), iters=2, stream=s.cuda_stream)
+    qlib.fit_from_start(ctx, d_ev.data_ptr(), m, d_start.data_ptr(), iters=2, bisections=bisections,
+                        stream=s.cuda_stream)
     naive, _ = ctx.read_rows(s.cuda_stream)
     both = (plain[:, 0] > 0) & (learned[:, 0] > 0) & (naive[:, 0] > 0)
     r_plain, r_learn, r_naive = (rmse_xy(plain, ev, truth, both), rmse_xy(learned, ev, truth, both),
