@@ -272,15 +272,24 @@ namespace tc {
 constexpr int kM = 128;        // ROIs per tile (the MMA's M)
 constexpr int kN3 = 16;        // layer-3 N padded to the M = 128 minimum
 constexpr int kW1 = kHidden * kIn, kW2 = kHidden * kHidden, kW3 = kN3 * kHidden;  // bf16 elements
+constexpr int kRecBytes = kM * kWhole * 2;  // one tile of records, 14,336 B
+// Shared memory: the weight images, the layer-2 operand (the layer-1 operand
+// lives in its first half: layer 1's MMA has finished reading it before the
+// layer-1 epilogue writes layer 2's operand), one tile of records, barriers.
 constexpr int kOffW1 = 0;
 constexpr int kOffW2 = kOffW1 + kW1 * 2;
 constexpr int kOffW3 = kOffW2 + kW2 * 2;
-constexpr int kOffA1 = kOffW3 + kW3 * 2;
-constexpr int kOffA2 = kOffA1 + kM * kIn * 2;
-constexpr int kOffBar = kOffA2 + kM * kHidden * 2;
-constexpr int kSmemBytes = kOffBar + 16 + 1024;  // + alignment slack
-constexpr int kTmemCols = 256;                  // layer 1 / 3 at column 0, layer 2 at column 128
+constexpr int kOffA2 = kOffW3 + kW3 * 2;
+constexpr int kOffA1 = kOffA2;
+constexpr int kOffRec = kOffA2 + kM * kHidden * 2;
+constexpr int kOffBar = kOffRec + kRecBytes;  // MMA barrier, record barrier, TMEM address
+constexpr int kAlign = 128;
+constexpr int kSmemBytes = kOffBar + 32 + kAlign;  // + alignment slack
+constexpr int kTmemCols = 256;                     // layer 1 / 3 at column 0, layer 2 at column 128
 constexpr int kWeightVec = (kW1 + kW2 + kW3) * 2 / 16;
+constexpr int kWaitPolls = 1 << 22;                // bound of every barrier wait
+static_assert(kOffA1 + kM * kIn * 2 <= kOffRec, "layer-1 operand inside the layer-2 buffer");
+static_assert(kRecBytes % 16 == 0 && kOffRec % 16 == 0, "bulk copies move 16-byte multiples");
 
 // element (n, k) of an N x K K-major operand image, in bf16 elements
 __host__ __device__ constexpr int img_index(int n, int k, int N) { return ((k >> 3) * N + n) * 8 + (k & 7); }
@@ -311,7 +320,7 @@ __device__ __forceinline__ void mma_commit(uint32_t bar) {
 
 // Bounded wait for the barrier phase; false when it did not complete.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
-    for (int it = 0; it < (1 << 22); ++it) {
+    for (int it = 0; it < kWaitPolls; ++it) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.b32 %0, 1, 0, p;\n\t}\n"
@@ -321,6 +330,15 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
         if (done) return true;
     }
     return false;
+}
+
+// Bulk copy (TMA, no multicast) of `bytes` contiguous global bytes into this
+// CTA's shared memory, completing on `bar` (which expects the bytes).
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
 }
 
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
@@ -364,6 +382,12 @@ __device__ __forceinline__ void epilogue_hidden(uint32_t taddr_row, const float 
     }
 }
 
+__device__ __forceinline__ int tile_rows(int tile, int n) { return min(kM, n - tile * kM); }
+
+// BULK: records reach shared memory by one bulk copy per tile, issued one
+// tile ahead (d_rois 16-byte aligned); otherwise each thread loads its own
+// record from global memory.
+template <bool BULK>
 __global__ void __launch_bounds__(128, 1) mlp_tc_kernel(const uint16_t *__restrict__ rois, int n, float offset,
                                                         float kadc, const uint4 *__restrict__ wimg,
                                                         const float *__restrict__ b1, const float *__restrict__ b2,
@@ -371,18 +395,24 @@ __global__ void __launch_bounds__(128, 1) mlp_tc_kernel(const uint16_t *__restri
                                                         int *__restrict__ err) {
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = (uint32_t)__cvta_generic_to_shared(smem_raw);
-    const uint32_t sbase = (raw + 1023u) & ~1023u;
+    const uint32_t sbase = (raw + (kAlign - 1)) & ~(uint32_t)(kAlign - 1);
     uint8_t *base = smem_raw + (sbase - raw);
     const uint32_t sW1 = sbase + kOffW1, sW2 = sbase + kOffW2, sW3 = sbase + kOffW3;
-    const uint32_t sA1 = sbase + kOffA1, sA2 = sbase + kOffA2, sBar = sbase + kOffBar, sTmem = sBar + 8;
+    const uint32_t sA1 = sbase + kOffA1, sA2 = sbase + kOffA2, sRec = sbase + kOffRec;
+    const uint32_t sBar = sbase + kOffBar, sRecBar = sBar + 8, sTmem = sBar + 16;
     const int tid = threadIdx.x, warp = tid >> 5;
+    const int ntiles = (n + kM - 1) / kM;
 
-    uint4 *wdst = reinterpret_cast<uint4 *>(base + kOffW1);
-    for (int i = tid; i < kWeightVec; i += blockDim.x) wdst[i] = wimg[i];
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(sBar) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(sRecBar) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        if (BULK && (int)blockIdx.x < ntiles)
+            bulk_load(sRec, rois + (size_t)blockIdx.x * kM * kWhole, (uint32_t)(tile_rows(blockIdx.x, n) * kWhole * 2),
+                      sRecBar);
     }
+    uint4 *wdst = reinterpret_cast<uint4 *>(base + kOffW1);
+    for (int i = tid; i < kWeightVec; i += blockDim.x) wdst[i] = wimg[i];
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sTmem), "r"(kTmemCols)
                      : "memory");
@@ -392,26 +422,49 @@ __global__ void __launch_bounds__(128, 1) mlp_tc_kernel(const uint16_t *__restri
     fence_before();
     __syncthreads();
     fence_after();
-    const uint32_t tmem = *reinterpret_cast<volatile uint32_t *>(base + kOffBar + 8);
+    const uint32_t tmem = *reinterpret_cast<volatile uint32_t *>(base + kOffBar + 16);
     const uint32_t row_lane = (uint32_t)(warp * 32) << 16;
-    uint32_t phase = 0;
-    bool ok = true;
-    const int ntiles = (n + kM - 1) / kM;
+    uint32_t phase = 0, rec_phase = 0;
+    bool ok = true, copy_pending = BULK && (int)blockIdx.x < ntiles;
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int i = tile * kM + tid;
+        const int rows = tile_rows(tile, n);
+        if (BULK) {
+            ok = __syncthreads_and(mbar_wait(sRecBar, rec_phase));
+            if (!ok) break;  // rec_phase still names the copy in flight
+            rec_phase ^= 1u;
+            copy_pending = false;
+        }
         // features of this thread's ROI into A1 (row tid)
         float lo = 1.0f, rng = 1.0f;
         {
             float f[kIn];
 #pragma unroll
             for (int k = 0; k < kIn; ++k) f[k] = 0.0f;
-            if (i < n) {
-                const uint16_t *r = rois + (size_t)i * kWhole;
+            if (tid < rows) {
+                uint16_t px[kWhole];
+                if (BULK) {
+                    const uint4 *r4 = reinterpret_cast<const uint4 *>(base + kOffRec + (size_t)tid * kWhole * 2);
+#pragma unroll
+                    for (int q = 0; q < kWhole / 8; ++q) {
+                        const uint4 u = r4[q];
+                        const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+                        for (int h = 0; h < 4; ++h) {
+                            px[q * 8 + 2 * h] = (uint16_t)(w[h] & 0xFFFFu);
+                            px[q * 8 + 2 * h + 1] = (uint16_t)(w[h] >> 16);
+                        }
+                    }
+                } else {
+                    const uint16_t *r = rois + (size_t)i * kWhole;
+#pragma unroll
+                    for (int k = 0; k < kPix; ++k) px[k] = r[k];
+                }
                 float hi = -1e30f;
                 lo = 1e30f;
 #pragma unroll
                 for (int k = 0; k < kPix; ++k) {
-                    f[k] = fmaxf(((float)r[k] - offset) * kadc, 1.0f);
+                    f[k] = fmaxf(((float)px[k] - offset) * kadc, 1.0f);
                     lo = fminf(lo, f[k]);
                     hi = fmaxf(hi, f[k]);
                 }
@@ -430,6 +483,15 @@ __global__ void __launch_bounds__(128, 1) mlp_tc_kernel(const uint16_t *__restri
         fence_before();
         __syncthreads();
         fence_after();
+        // the records are consumed: fetch the next tile of this CTA while the MMAs run
+        if (BULK && tid == 0) {
+            const int next = tile + gridDim.x;
+            if (next < ntiles) {
+                bulk_load(sRec, rois + (size_t)next * kM * kWhole, (uint32_t)(tile_rows(next, n) * kWhole * 2),
+                          sRecBar);
+                copy_pending = true;
+            }
+        }
         // layer 1: D[128 x 128] at column 0
         if (tid == 0) {
 #pragma unroll
@@ -443,7 +505,7 @@ __global__ void __launch_bounds__(128, 1) mlp_tc_kernel(const uint16_t *__restri
         phase ^= 1u;
         if (!ok) break;
         fence_after();
-        epilogue_hidden(tmem + row_lane, b1, base + kOffA2, tid);
+        epilogue_hidden(tmem + row_lane, b1, base + kOffA2, tid);  // layer 1 has read A1 (aliased here)
         fence_async_smem();
         fence_before();
         __syncthreads();
@@ -480,7 +542,7 @@ __global__ void __launch_bounds__(128, 1) mlp_tc_kernel(const uint16_t *__restri
         fence_after();
         float y[16];
         tmem_ld16(tmem + row_lane, y);
-        if (i < n) {
+        if (tid < rows) {
             float *st = start + (size_t)i * kStart;
             st[0] = rng * expf(fminf(fmaxf(y[3] + __ldg(b3 + 3), -6.0f), 3.0f));
             st[1] = kCentre + fminf(fmaxf(y[0] + __ldg(b3 + 0), -1.5f), 1.5f);
@@ -492,6 +554,9 @@ __global__ void __launch_bounds__(128, 1) mlp_tc_kernel(const uint16_t *__restri
         __syncthreads();  // accumulator columns are free for the next tile
         fence_after();
     }
+    // error path: a copy issued for the next tile may still be landing in this
+    // CTA's shared memory; wait for it (bounded) before the CTA ends
+    if (BULK && __syncthreads_or(copy_pending)) mbar_wait(sRecBar, rec_phase);
     fence_before();
     __syncthreads();
     fence_after();
@@ -633,8 +698,9 @@ cudaError_t fused_start_points(qcs_learned_net *net, const qcs_loc_para *p, cons
     int dev = 0, sms = 148;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(L::tc::mlp_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, L::tc::kSmemBytes);
+    const bool bulk = (reinterpret_cast<uintptr_t>(d_rois) & 15) == 0;
+    auto kern = bulk ? L::tc::mlp_tc_kernel<true> : L::tc::mlp_tc_kernel<false>;
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::tc::kSmemBytes);
     if (e != cudaSuccess) return e;
     const int grid = tiles < 2 * sms ? tiles : 2 * sms;
     const Views w = views(net->d_par);
@@ -650,9 +716,8 @@ cudaError_t fused_start_points(qcs_learned_net *net, const qcs_loc_para *p, cons
         e = cudaStreamWaitEvent(s, net->wimg_ready, 0);
         if (e != cudaSuccess) return e;
     }
-    L::tc::mlp_tc_kernel<<<grid, 128, L::tc::kSmemBytes, s>>>(d_rois, n, p->Offset, p->KAdc,
-                                                              reinterpret_cast<const uint4 *>(net->d_wimg), w.b1, w.b2,
-                                                              w.b3, start, net->d_err);
+    kern<<<grid, 128, L::tc::kSmemBytes, s>>>(d_rois, n, p->Offset, p->KAdc, reinterpret_cast<const uint4 *>(net->d_wimg),
+                                              w.b1, w.b2, w.b3, start, net->d_err);
     return cudaGetLastError();
 }
 

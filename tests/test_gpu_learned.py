@@ -80,6 +80,23 @@ def test_forward_and_gradient_match_oracle(cuda_ok):
     net.close()
 
 
+def test_fused_start_points_misaligned_records(cuda_ok):
+    """Records not on a 16-byte boundary cannot be bulk-copied: the fused kernel
+    then loads each record directly and gives the same start points."""
+    import torch
+    rec, para, _ = synth.gs2d_rois(3000, seed=14)
+    n = rec.shape[0]
+    d = to_dev(rec)
+    buf = torch.zeros(n * rec.shape[1] + 4, dtype=torch.int16, device="cuda")
+    buf[4:] = d.reshape(-1)
+    net = qlib.LearnedNet(batch=512, seed=8)
+    a = net.start(para, d.data_ptr(), n).cpu().numpy()
+    b = net.start(para, buf.data_ptr() + 8, n).cpu().numpy()
+    net.fused_status()
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    net.close()
+
+
 def start_from_y(y, scale):
     """The start-point transform of the network outputs (clamps as in qcs_learned.cu start_kernel)."""
     lo, rng = scale[:, 0].astype(np.float64), scale[:, 1].astype(np.float64)
