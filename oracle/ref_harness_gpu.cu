@@ -311,6 +311,8 @@ int qcsrefg_crlb(const qcs_loc_para *p, float *loc, int n) {
 }
 
 int qcsrefg_wle(const qcs_loc_para *p, const unsigned short *rois, int n, float *wle_out) {
+    // WLEParameterEstimation_TypeDef sizes its buffers for MaxPointNum records
+    if (n < 0 || n > MaxPointNum) return -1;
     LocalizationPara r;
     to_ref(p, r);
     WLEParameterEstimation_TypeDef w;

@@ -140,6 +140,20 @@ def test_wle_bit_exact(cuda_ok, gen, R, changes):
         np.testing.assert_allclose(ours[:, 3:5], host[:, 3:5], rtol=1e-5)
 
 
+@pytest.mark.parametrize("gen,R,kind", [(synth.gs2d_rois, 7, 0), (synth.as3d_rois, 9, 1)])
+def test_fit_kernel_large_batch(cuda_ok, gen, R, kind):
+    """300,000 fits per kind: every row equals the reference kernel's bit for
+    bit (the WLE rows from the product's pre-pass, fed to both)."""
+    n = 300_000
+    rec, para, _ = gen(n, R=R, seed=123)
+    ctx = qlib.LocContext(para, capacity=n)
+    wl = ctx.wle(rec)
+    ctx.close()
+    ref, _ = O.ref_gpu_fit_kernel(kind, para, rec, wl)
+    ours = product_fit_kernel(kind, para, rec, wl)
+    assert np.array_equal(bits(ref), bits(ours)), mismatch_report(ref, ours)
+
+
 def test_crlb(cuda_ok):
     import torch
     for gen, R in ((synth.gs2d_rois, 7), (synth.as3d_rois, 9)):
