@@ -49,9 +49,9 @@ PX_EVALS_PER_FIT = 176 * R * R  # reference schedule: 176 loss evaluations of R*
 MUFU_PER_PX_EVAL = 2            # exp of the model, log of the model (log of the data is invariant)
 # DRAM bytes (read + write) per fit of fit_single_kernel<7, GS2D>, from one ncu capture of
 # `bench.py --profile-fit 1200000` (profiles/fit_single_gs2d7_crlb9_1.2M_records.md:
-# 164.27 MB read + 39.28 MB written for 1.2 M fits); algorithmic: 112 B record + 24 B WLE row
+# 163.41 MB read + 37.19 MB written for 1.2 M fits); algorithmic: 112 B record + 24 B WLE row
 # read, 48 B row written.
-DRAM_BYTES_PER_FIT = (164.267776e6 + 39.283456e6) / 1.2e6
+DRAM_BYTES_PER_FIT = (163.412480e6 + 37.192192e6) / 1.2e6
 ALGO_BYTES_PER_FIT = 112 + 24 + 48
 
 
