@@ -112,6 +112,29 @@ def stop_clock_sampler(p, path, t_start, t_end):
     return out
 
 
+def batch_seed(rank, b):
+    """Seed of record batch b on `rank`: every rank localizes records of its own
+    (weak scaling; the path has no data-path collective)."""
+    return 1000 * rank + b
+
+
+def max_over_ranks(ms, dist):
+    """The slowest rank's time (ms) when several ranks run: all-reduce MAX, on
+    the GPU under NCCL, on the CPU under gloo."""
+    if dist is None:
+        return ms
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(steps, per_step, world, ms):
+    """Whole-job rate: every rank's records over the slowest rank's time."""
+    return steps * per_step * world / (ms * 1e-3)
+
+
 def cpu_reference_rate(steps=1, per_thread=6000, threads=None):
     """fits/s of the reference's own code compiled for the host (oracle/_ref),
     WLE + localization + CRLB, one chunk of records per host thread; falls back
@@ -189,7 +212,7 @@ FRAMES_PER_CALL = 32   # frames whose ROIs accumulate before one localization ca
 MAX_POINT_NUM = 102400
 
 
-def frame_pipeline(stream, steps, warmup, e2e=True):
+def frame_pipeline(stream, steps, warmup, e2e=True, dist=None, world=1):
     """Whole-frame pipeline: 2048 x 2048 uint16 frames -> ROI extraction
     (background, smoothing, detection, 7x7 cut, WLE; one frame per extraction
     batch, records accumulating on the device) -> after FRAMES_PER_CALL frames
@@ -236,7 +259,7 @@ def frame_pipeline(stream, steps, warmup, e2e=True):
         step(k)
     e1.record(stream)
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / steps
+    ms = max_over_ranks(e0.elapsed_time(e1), dist) / steps
     e2e_steps = max(3, steps // 4) if e2e else 1
     t0 = time.perf_counter()
     out_rows = 0
@@ -244,17 +267,17 @@ def frame_pipeline(stream, steps, warmup, e2e=True):
         step(k, host=True)
         r, _ = loc.read_rows(sh)
         out_rows += r.shape[0]
-    e2e_ms = (time.perf_counter() - t0) * 1e3 / e2e_steps
+    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3, dist) / e2e_steps
     ex.close()
     loc.close()
     return {
         "workload": "2048x2048 uint16 frames, ~3000 emitters/frame (20%% in pairs < 3 px), GS2D 7x7, multi-emitter "
                     "fitting on; %d frames per localization call, %d distinct frames rotated" % (
                         FRAMES_PER_CALL, FRAMES),
-        "frames_per_s": FRAMES_PER_CALL * 1e3 / ms, "ms_per_call": ms, "frames_per_call": FRAMES_PER_CALL,
+        "frames_per_s": world * FRAMES_PER_CALL * 1e3 / ms, "ms_per_call": ms, "frames_per_call": FRAMES_PER_CALL,
         "records_per_call": recs0, "rows_per_call": int(rows0.shape[0]),
-        "localizations_per_s": rows0.shape[0] * 1e3 / ms, "steps": steps,
-        "e2e": {"frames_per_s": FRAMES_PER_CALL * 1e3 / e2e_ms, "ms_per_call": e2e_ms,
+        "localizations_per_s": world * rows0.shape[0] * 1e3 / ms, "steps": steps,
+        "e2e": {"frames_per_s": world * FRAMES_PER_CALL * 1e3 / e2e_ms, "ms_per_call": e2e_ms,
                 "h2d_bytes_per_call": FRAMES_PER_CALL * frame_bytes,
                 "d2h_bytes_per_call": int(out_rows / e2e_steps) * 48 + 32,
                 "calls": "%d x qcs_extract_molecules (pinned frame) -> qcs_loc_localize_device_n -> "
@@ -357,12 +380,8 @@ def learned_measure(args, stream, ctx, para, d_batches, h_batches, rec0, truth0,
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
-    ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = args.steps * N_PER_STEP * world / (ms * 1e-3)
+    ms = max_over_ranks(e0.elapsed_time(e1), dist)
+    value = job_rate(args.steps, N_PER_STEP, world, ms)
 
     # accuracy on batch 0: plain and learned rows of the same records
     ctx.localize_device(d_batches[0].data_ptr(), N_PER_STEP, 0, sh)
@@ -381,6 +400,7 @@ def learned_measure(args, stream, ctx, para, d_batches, h_batches, rec0, truth0,
     e2e_pipelined(ctxs, streams, h_batches, 4, net=net)
     e2e_steps = E2E_STEPS
     e2e_s, _ = e2e_pipelined(ctxs, streams, h_batches, e2e_steps, net=net)
+    e2e_s = max_over_ranks(e2e_s * 1e3, dist) * 1e-3
     ctxs[1].close()
     net.close()
     return {
@@ -505,7 +525,7 @@ def main():
     para = None
     rec0 = truth0 = None
     for b in range(BATCHES):
-        rec, para, truth = synth.gs2d_rois(N_PER_STEP, R=R, seed=1000 * rank + b)
+        rec, para, truth = synth.gs2d_rois(N_PER_STEP, R=R, seed=batch_seed(rank, b))
         if b == 0:
             rec0, truth0 = rec, truth
         h = torch.from_numpy(rec.view(np.int16)).pin_memory()
@@ -542,12 +562,8 @@ def main():
     clocks = stop_clock_sampler(sampler, spath, t_start, t_end)
     if dist:
         dist.barrier()
-    ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = args.steps * N_PER_STEP * world / (ms * 1e-3)
+    ms = max_over_ranks(e0.elapsed_time(e1), dist)
+    value = job_rate(args.steps, N_PER_STEP, world, ms)
 
     # ---- dominant kernel alone: the single-emitter fit (for the roofline)
     wle_b = [torch.empty((N_PER_STEP, 6), dtype=torch.float32, device="cuda") for _ in range(BATCHES)]
@@ -578,6 +594,7 @@ def main():
     e2e_pipelined(ctxs, streams, h_batches, 4)
     e2e_steps = E2E_STEPS
     e2e_s, rows = e2e_pipelined(ctxs, streams, h_batches, e2e_steps)
+    e2e_s = max_over_ranks(e2e_s * 1e3, dist) * 1e-3
     ctxs[1].close()
     # the synchronous reference-shaped call, one at a time
     sync_steps = 10
@@ -587,7 +604,7 @@ def main():
     t0 = time.perf_counter()
     for k in range(sync_steps):
         ctx.localize(h_batches[k % BATCHES].numpy().view(np.uint16), None, stream=sh)
-    sync_s = time.perf_counter() - t0
+    sync_s = max_over_ranks((time.perf_counter() - t0) * 1e3, dist) * 1e-3
     e2e = {"value": e2e_steps * N_PER_STEP * world / e2e_s, "unit": UNIT,
            "h2d_bytes_per_step": N_PER_STEP * R * (R + 1) * 2,
            "d2h_bytes_per_step": int(rows / e2e_steps) * 48 + 32,
@@ -602,7 +619,7 @@ def main():
 
     frames = None
     if not args.no_frames:
-        frames = frame_pipeline(stream, steps=min(max(args.steps // 40, 5), 40), warmup=3)
+        frames = frame_pipeline(stream, steps=min(max(args.steps // 40, 5), 40), warmup=3, dist=dist, world=world)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:

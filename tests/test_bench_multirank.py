@@ -1,0 +1,69 @@
+"""bench.py with several ranks, on the CPU (gloo), as the GPU run launches it
+under torch.distributed.run with NCCL: each rank localizes records of its own
+(no data-path collective), the timed region is the slowest rank's (all-reduce
+MAX), the rate counts every rank's records, and the reference arm runs on rank
+0 alone while the other ranks exit without work."""
+import json
+import os
+import socket
+import subprocess
+import sys
+from datetime import timedelta
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    sys.path.insert(0, ROOT)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    import bench
+    ms = bench.max_over_ranks(10.0 + 5.0 * rank, dist)
+    seeds = [bench.batch_seed(rank, b) for b in range(bench.BATCHES)]
+    every = [None] * world
+    dist.all_gather_object(every, seeds)
+    q.put((rank, ms, every, bench.job_rate(100, bench.N_PER_STEP, world, ms)))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_ranks_gloo():
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = free_port()
+    procs = [ctx.Process(target=_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = [q.get(timeout=120) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, ms, every, rate in out:
+        assert ms == 15.0  # the slower rank's time on both
+        assert not set(every[0]) & set(every[1])  # records of their own
+        assert rate == pytest.approx(100 * 100_000 * 2 / 15e-3)
+
+
+def test_reference_arm_under_torchrun_two_ranks():
+    port = free_port()
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2", "--master-addr",
+           "127.0.0.1", "--master-port", str(port), os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus",
+           "2", "--steps", "1", "--warmup", "0"]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1  # rank 0 only
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
+    assert d["cpu_baseline"]["cores"] >= 1 and d["e2e"]["h2d_bytes_per_step"] == 0
