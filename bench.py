@@ -12,9 +12,13 @@ U(1.0,1.6) px, photons log-U[500,5000], background U(20,100) e-/px, Poisson),
 frames -> extraction -> multi-emitter localization -> CRLB) in frames/s.
 
 Printed JSON line (rank 0): `value` is device-timed fits/s with records
-resident in HBM; `e2e` is the same metric through the host-buffer call
-qcs_loc_bfgs_mle_localization (pinned host records in, rows out, copies
-inside the timed region); `roofline` is the fit kernel against the measured
+resident in HBM, two localization contexts used in turn on two streams (one
+call's latency-bound tail overlaps the next call's kernels; `value_one_stream`
+is one context on one stream); `e2e` is the same metric through the
+asynchronous host-buffer calls (qcs_loc_localize_async + qcs_loc_finish on two
+contexts in turn: pinned host records in, rows and counters out, every copy
+inside the timed region; `e2e.sync_value`: the synchronous
+qcs_loc_bfgs_mle_localization, one call at a time); `roofline` is the fit kernel against the measured
 special-function-unit rate (the loss is exp/log bound, not HBM or tensor
 bound); `cpu_baseline` is the reference's own code compiled for the host
 (oracle/_ref) on all host cores.
@@ -128,6 +132,37 @@ def max_over_ranks(ms, dist):
     t = torch.tensor([ms], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def device_timed(steps, warmup, enqueue, streams, dist):
+    """Device time (ms, the slowest rank's) of `steps` calls enqueue(k, stream)
+    after `warmup` untimed ones.  With two streams the calls alternate between
+    them (two contexts in turn), so one call's latency-bound tail overlaps the
+    next call's kernels; the CUDA events bracket every stream."""
+    import torch
+    for k in range(warmup):
+        enqueue(k, streams[k % len(streams)])
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    a = streams[0]
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(a)
+    for s in streams[1:]:
+        s.wait_event(e0)
+    for k in range(steps):
+        enqueue(k, streams[k % len(streams)])
+    for s in streams[1:]:
+        ev = torch.cuda.Event()
+        ev.record(s)
+        a.wait_event(ev)
+    e1.record(a)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    return max_over_ranks(e0.elapsed_time(e1), dist)
 
 
 def job_rate(steps, per_step, world, ms):
@@ -351,42 +386,30 @@ def fit_accuracy(rows, rec, truth, sel, para):
     return rmse, ph, crlb
 
 
-def learned_measure(args, stream, ctx, para, d_batches, h_batches, rec0, truth0, plain_value, world, dist):
+def learned_measure(args, streams, ctxs, para, d_batches, h_batches, rec0, truth0, plain_value, world, dist):
     """Learned start points + LEARNED_ITERS BFGS iterations (LEARNED_BISECTIONS
     line-search steps each, analytic gradient) + plain refits of
     the fits the deviance judge rejects + CRLB (qcs_learned_localize_device),
     on the same device-resident batches as the plain step, WLE pre-pass
     included; accuracy of plain vs learned on batch 0 against ground truth."""
-    import torch
+    stream, ctx = streams[0], ctxs[0]
     sh = stream.cuda_stream
     net, train = train_learned_net(para, stream)
 
-    def step(k):
-        net.localize(ctx, d_batches[k % BATCHES].data_ptr(), N_PER_STEP, 0, iters=LEARNED_ITERS,
-                     bisections=LEARNED_BISECTIONS, stream=sh)
+    def step(k, s, c=None):
+        net.localize(c or ctxs[k % 2], d_batches[k % BATCHES].data_ptr(), N_PER_STEP, 0, iters=LEARNED_ITERS,
+                     bisections=LEARNED_BISECTIONS, stream=s.cuda_stream)
 
-    for k in range(args.warmup):
-        step(k)
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for k in range(args.steps):
-        step(k)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    ms = max_over_ranks(e0.elapsed_time(e1), dist)
+    ms = device_timed(args.steps, args.warmup, step, streams, dist)
     value = job_rate(args.steps, N_PER_STEP, world, ms)
+    one_steps = min(args.steps, 200)
+    ms1 = device_timed(one_steps, 3, lambda k, s: step(k, s, ctx), [stream], dist)
+    value1 = job_rate(one_steps, N_PER_STEP, world, ms1)
 
     # accuracy on batch 0: plain and learned rows of the same records
     ctx.localize_device(d_batches[0].data_ptr(), N_PER_STEP, 0, sh)
     plain, _ = ctx.read_rows(sh)
-    step(0)
+    step(0, stream, ctx)
     learned, _ = ctx.read_rows(sh)
     refits = net.refits(ctx)
     both = (plain[:, 0] > 0) & (learned[:, 0] > 0)
@@ -394,17 +417,14 @@ def learned_measure(args, stream, ctx, para, d_batches, h_batches, rec0, truth0,
     rl, pl, _ = fit_accuracy(learned, rec0, truth0, both, para)
 
     # end to end: pinned host records in, rows out, through qcs_learned_localize_async
-    from qcstorm_b200 import lib
-    ctxs = [ctx, lib.LocContext(para, capacity=N_PER_STEP)]
-    streams = [stream, torch.cuda.Stream()]
     e2e_pipelined(ctxs, streams, h_batches, 4, net=net)
     e2e_steps = E2E_STEPS
     e2e_s, _ = e2e_pipelined(ctxs, streams, h_batches, e2e_steps, net=net)
     e2e_s = max_over_ranks(e2e_s * 1e3, dist) * 1e-3
-    ctxs[1].close()
     net.close()
     return {
         "value": value, "unit": UNIT, "ms_per_step": ms / args.steps, "vs_plain": value / plain_value,
+        "value_one_stream": value1, "timing": "two contexts in turn on two streams (value_one_stream: one)",
         "iters": LEARNED_ITERS, "bisections": LEARNED_BISECTIONS, "refits_per_step": refits,
         # mlp_tc (features + network), WLE (5), fit_learned, flag_queue, group refit, refit CRLB, counters, CRLB
         "gpu_launches_per_step": 12,
@@ -532,38 +552,28 @@ def main():
         h_batches.append(h)
         d_batches.append(h.cuda())
     ctx = lib.LocContext(para, capacity=N_PER_STEP)
+    ctxs = [ctx, lib.LocContext(para, capacity=N_PER_STEP)]
+    streams = [stream, torch.cuda.Stream()]
     sh = stream.cuda_stream
 
-    def step(k):
-        ctx.localize_device(d_batches[k % BATCHES].data_ptr(), N_PER_STEP, 0, sh)
+    def step(k, s, c=None):
+        (c or ctxs[k % 2]).localize_device(d_batches[k % BATCHES].data_ptr(), N_PER_STEP, 0, s.cuda_stream)
 
     # psf_width, nn_keys_flag, the sort's condition kernel (the sort itself only for out-of-order records),
     # nn_scan_select, classify, init_counters, fit, finish, crlb
     launches_per_step = 9
 
-    # ---- device-timed steps
-    for k in range(args.warmup):
-        step(k)
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
+    # ---- device-timed steps: two contexts in turn on two streams
     sampler, spath = start_clock_sampler(local)
     time.sleep(0.5)  # first nvidia-smi sample lands before the timed region
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
     t_start = time.time()
-    e0.record(stream)
-    for k in range(args.steps):
-        step(k)
-    e1.record(stream)
-    torch.cuda.synchronize()
+    ms = device_timed(args.steps, args.warmup, step, streams, dist)
     t_end = time.time()
     clocks = stop_clock_sampler(sampler, spath, t_start, t_end)
-    if dist:
-        dist.barrier()
-    ms = max_over_ranks(e0.elapsed_time(e1), dist)
     value = job_rate(args.steps, N_PER_STEP, world, ms)
+    one_steps = min(args.steps, 200)
+    ms1 = device_timed(one_steps, 3, lambda k, s: step(k, s, ctx), [stream], dist)
+    value1 = job_rate(one_steps, N_PER_STEP, world, ms1)
 
     # ---- dominant kernel alone: the single-emitter fit (for the roofline)
     wle_b = [torch.empty((N_PER_STEP, 6), dtype=torch.float32, device="cuda") for _ in range(BATCHES)]
@@ -589,13 +599,10 @@ def main():
     achieved = N_PER_STEP * PX_EVALS_PER_FIT * MUFU_PER_PX_EVAL / (fit_ms * 1e-3)
 
     # ---- end to end through the host-buffer calls (pinned records in, rows out every step)
-    ctxs = [ctx, lib.LocContext(para, capacity=N_PER_STEP)]
-    streams = [stream, torch.cuda.Stream()]
     e2e_pipelined(ctxs, streams, h_batches, 4)
     e2e_steps = E2E_STEPS
     e2e_s, rows = e2e_pipelined(ctxs, streams, h_batches, e2e_steps)
     e2e_s = max_over_ranks(e2e_s * 1e3, dist) * 1e-3
-    ctxs[1].close()
     # the synchronous reference-shaped call, one at a time
     sync_steps = 10
     for k in range(2):
@@ -615,7 +622,7 @@ def main():
 
     learned = None
     if not args.no_learned:
-        learned = learned_measure(args, stream, ctx, para, d_batches, h_batches, rec0, truth0, value, world, dist)
+        learned = learned_measure(args, streams, ctxs, para, d_batches, h_batches, rec0, truth0, value, world, dist)
 
     frames = None
     if not args.no_frames:
@@ -630,6 +637,8 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config_dict(args),
+            "value_one_stream": value1, "timing": "two contexts in turn on two streams, CUDA events around both "
+                                                  "(value_one_stream: one context, one stream)",
             "e2e": e2e, "gpu_launches": launches_per_step * args.steps,
             "roofline": {"bound": "sfu", "kernel": "fit_single_kernel<7,GS2D>", "achieved": achieved,
                          "peak": mufu_peak, "unit": "MUFU op/s", "frac": achieved / mufu_peak,
@@ -642,7 +651,8 @@ def main():
             "cpu_baseline": cpu, "clocks": clocks, "learned": learned, "frames": frames,
         }
         print(json.dumps(line), flush=True)
-    ctx.close()
+    for c in ctxs:
+        c.close()
     if dist:
         dist.destroy_process_group()
     return 0
