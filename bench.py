@@ -247,7 +247,70 @@ FRAMES_PER_CALL = 32   # frames whose ROIs accumulate before one localization ca
 MAX_POINT_NUM = 102400
 
 
-def frame_pipeline(stream, steps, warmup, e2e=True, dist=None, world=1):
+TRAIN_FRAMES = 32      # frames (seeds disjoint from the timed ones) whose records train the frame network
+COUNT_TH = 0.5         # emitter-count routing threshold of the learned frame pipeline
+
+
+def frame_truth_match(rows, truth, radius=1.0):
+    """Distance (px) of each localization to the nearest true emitter of its
+    frame (frame f holds the emitters of distinct frame f % FRAMES); rows with
+    no emitter within `radius` count as unmatched."""
+    from scipy.spatial import cKDTree
+    rows = rows[rows[:, 0] > 0]
+    frame = rows[:, 11].astype(np.int64)
+    dist = np.full(rows.shape[0], np.inf)
+    for f in np.unique(frame):
+        t = truth[int(f) % len(truth)]
+        sel = frame == f
+        d, _ = cKDTree(np.stack([t["x"], t["y"]], 1)).query(np.stack([rows[sel, 1], rows[sel, 2]], 1))
+        dist[sel] = d
+    ok = dist < radius
+    return {"localizations": int(rows.shape[0]), "matched": int(ok.sum()),
+            "rmse_px": float(np.sqrt(np.mean(dist[ok] ** 2))) if ok.any() else None}
+
+
+def train_frame_net(para, stream, seed=9001):
+    """The network of the learned frame pipeline, trained on the GPU on the
+    records that extraction cuts from TRAIN_FRAMES fresh frames (same
+    generator, other seeds): start-point targets from the records the plain
+    multi-emitter cascade kept single, emitter-count classes from its outcome
+    (qcs_loc_count_labels_device).  Returns (net, info)."""
+    import torch
+    from qcstorm_b200 import lib, synth
+    sh = stream.cuda_stream
+    t0 = time.perf_counter()
+    fr, _, _ = synth.frames(TRAIN_FRAMES, width=FRAME_W, height=FRAME_H, density=3000, seed=seed)
+    ex = lib.ExtractContext(para, max_batched_num=1, capacity=MAX_POINT_NUM)
+    loc = lib.LocContext(para, capacity=MAX_POINT_NUM)
+    d_fr = torch.from_numpy(fr.view(np.int16)).cuda()
+    fb = FRAME_W * FRAME_H * 2
+    torch.cuda.synchronize()
+    for f in range(TRAIN_FRAMES):
+        ex.extract_device(d_fr.data_ptr() + f * fb, 1, f, stream=sh)
+    n = ex.accumulated()
+    d_rois, d_wle, _ = ex.device_records()
+    loc.localize_device(d_rois, n, d_wle, sh)
+    labels = lib.count_labels(loc, n, sh)
+    feat, scale = lib.LearnedNet.features(para, d_rois, n, stream=sh)
+    tgt, valid = lib.LearnedNet.targets(para, d_rois, loc.device_rows(), scale, n, stream=sh)
+    stream.synchronize()
+    valid = valid * (labels == 0).float()
+    counts = [int(c) for c in torch.bincount(labels.long(), minlength=3).cpu()]
+    torch.cuda.synchronize()
+    net = lib.LearnedNet(batch=4096, seed=5)
+    losses = net.train(feat, tgt, valid, epochs=TRAIN_EPOCHS, lr=2e-3, stream=sh, classes=labels)
+    stream.synchronize()
+    info = {"frames": TRAIN_FRAMES, "records": n, "epochs": TRAIN_EPOCHS, "seconds": time.perf_counter() - t0,
+            "loss_first_epoch": float(losses[0]), "loss_last_epoch": float(losses[-1]),
+            "class_counts": counts,
+            "labels": "plain multi-emitter cascade on this GPU: fits of the records it kept single, and its "
+                      "outcome per record (0: kept single, 1: kept by the 2E fit, 2: passed on to the 3E fit)"}
+    ex.close()
+    loc.close()
+    return net, info
+
+
+def frame_pipeline(stream, steps, warmup, e2e=True, dist=None, world=1, net=None):
     """Whole-frame pipeline: 2048 x 2048 uint16 frames -> ROI extraction
     (background, smoothing, detection, 7x7 cut, WLE; one frame per extraction
     batch, records accumulating on the device) -> after FRAMES_PER_CALL frames
@@ -257,10 +320,14 @@ def frame_pipeline(stream, steps, warmup, e2e=True, dist=None, world=1):
     (the record count stays on the device).  value: frames/s with frames
     resident in HBM; e2e: the same with every frame copied from pinned host
     memory and the rows read back to the host (qcs_loc_read_rows) inside the
-    timed region."""
+    timed region.  With net, the localization call is the learned one
+    (qcs_learned_localize_device_n: start points and emitter-count classes
+    from the network, LEARNED_ITERS x LEARNED_BISECTIONS single-emitter fits,
+    plain refits, the 2E / 3E stages); `accuracy` compares the first call's
+    localizations with the generator's emitters."""
     import torch
     from qcstorm_b200 import lib, synth
-    fr, para, _ = synth.frames(FRAMES, width=FRAME_W, height=FRAME_H, density=3000, seed=77)
+    fr, para, truth = synth.frames(FRAMES, width=FRAME_W, height=FRAME_H, density=3000, seed=77)
     para.MultiEmitterFitEn = 1
     ex = lib.ExtractContext(para, max_batched_num=1, capacity=MAX_POINT_NUM)
     loc = lib.LocContext(para, capacity=MAX_POINT_NUM)
@@ -278,12 +345,17 @@ def frame_pipeline(stream, steps, warmup, e2e=True, dist=None, world=1):
                 ex.extract_device(h_fr.data_ptr() + (f % FRAMES) * frame_bytes, 1, f, stream=sh, source="pinned")
             else:
                 ex.extract_device(d_fr.data_ptr() + (f % FRAMES) * frame_bytes, 1, f, stream=sh)
-        loc.localize_device_n(d_rois, d_wle, d_n, MAX_POINT_NUM, sh)
+        if net is None:
+            loc.localize_device_n(d_rois, d_wle, d_n, MAX_POINT_NUM, sh)
+        else:
+            net.localize_n(loc, d_rois, d_wle, d_n, MAX_POINT_NUM, iters=LEARNED_ITERS, bisections=LEARNED_BISECTIONS,
+                           stream=sh)
 
     step(0)
-    rows0, _ = loc.read_rows(sh)
+    rows0, ratios0 = loc.read_rows(sh)
     recs0 = ex.accumulated()
     assert ex.dropped() == 0
+    accuracy = frame_truth_match(rows0, truth)
     for k in range(warmup):
         step(k)
     torch.cuda.synchronize()
@@ -305,19 +377,41 @@ def frame_pipeline(stream, steps, warmup, e2e=True, dist=None, world=1):
     e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3, dist) / e2e_steps
     ex.close()
     loc.close()
+    call = "qcs_loc_localize_device_n" if net is None else "qcs_learned_localize_device_n"
     return {
         "workload": "2048x2048 uint16 frames, ~3000 emitters/frame (20%% in pairs < 3 px), GS2D 7x7, multi-emitter "
                     "fitting on; %d frames per localization call, %d distinct frames rotated" % (
                         FRAMES_PER_CALL, FRAMES),
         "frames_per_s": world * FRAMES_PER_CALL * 1e3 / ms, "ms_per_call": ms, "frames_per_call": FRAMES_PER_CALL,
         "records_per_call": recs0, "rows_per_call": int(rows0.shape[0]),
+        "single_emitter_fits_per_call": int(round(float(ratios0[0]) * recs0)),
         "localizations_per_s": world * rows0.shape[0] * 1e3 / ms, "steps": steps,
+        "accuracy": dict(accuracy, basis="first call's localizations against the generator's emitters of their "
+                                         "frames (nearest within 1 px)"),
         "e2e": {"frames_per_s": world * FRAMES_PER_CALL * 1e3 / e2e_ms, "ms_per_call": e2e_ms,
                 "h2d_bytes_per_call": FRAMES_PER_CALL * frame_bytes,
                 "d2h_bytes_per_call": int(out_rows / e2e_steps) * 48 + 32,
-                "calls": "%d x qcs_extract_molecules (pinned frame) -> qcs_loc_localize_device_n -> "
-                         "qcs_loc_read_rows" % FRAMES_PER_CALL},
+                "calls": "%d x qcs_extract_molecules (pinned frame) -> %s -> qcs_loc_read_rows" % (
+                    FRAMES_PER_CALL, call)},
     }
+
+
+def frame_pipeline_learned(stream, steps, warmup, dist=None, world=1):
+    """The frame pipeline with the learned localization call, after training
+    its network on records of other frames."""
+    from qcstorm_b200.abi import default_para
+    # the camera of synth.frames, multi-emitter fitting on (as in frame_pipeline)
+    para = default_para(Offset=100.0, KAdc=0.45, QE=1.0, ImageWidth=FRAME_W, ImageHigh=FRAME_H, MultiEmitterFitEn=1)
+    net, info = train_frame_net(para, stream)
+    net.set_count_threshold(COUNT_TH)
+    r = frame_pipeline(stream, steps, warmup, e2e=True, dist=dist, world=world, net=net)
+    net.fused_status()
+    net.close()
+    r["train"] = info
+    r["count_threshold"] = COUNT_TH
+    r["schedule"] = "%d BFGS iterations x %d line-search steps from the network's start points" % (
+        LEARNED_ITERS, LEARNED_BISECTIONS)
+    return r
 
 
 LEARNED_ITERS = 2          # BFGS iterations from the network's start points (plain: 8)
@@ -626,7 +720,11 @@ def main():
 
     frames = None
     if not args.no_frames:
-        frames = frame_pipeline(stream, steps=min(max(args.steps // 40, 5), 40), warmup=3, dist=dist, world=world)
+        fsteps = min(max(args.steps // 40, 5), 40)
+        frames = frame_pipeline(stream, steps=fsteps, warmup=3, dist=dist, world=world)
+        if not args.no_learned:
+            frames["learned"] = frame_pipeline_learned(stream, fsteps, 3, dist=dist, world=world)
+            frames["learned"]["vs_plain"] = frames["learned"]["frames_per_s"] / frames["frames_per_s"]
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:

@@ -347,8 +347,11 @@ int qcs_crlb_device(const qcs_loc_para *p, float *d_loc, int n, void *stream);
 /*
  * A small network (64 features -> 128 -> 128 -> 8, ReLU, BF16 tensor-core
  * GEMMs with FP32 accumulation) predicts each GS2D 7x7 ROI's start point
- * (x, y, sigma, peak photons, background) for the BFGS fit, trained on the
- * GPU by these entry points on ROIs labelled by converged plain fits.
+ * (x, y, sigma, peak photons, background) for the BFGS fit and, from three
+ * logits, its emitter-count class (0: one emitter; 1: the stage of the
+ * two-emitter fit; 2: the stage of the three-emitter fit), trained on the
+ * GPU by these entry points on ROIs labelled by converged plain fits and by
+ * the plain multi-emitter cascade's outcome.
  * Parameters: qcs_learned_param_count() floats (W1 64x128, b1, W2 128x128,
  * b2, W3 128x8, b3, row-major [in][out]).
  */
@@ -370,10 +373,37 @@ int qcs_learned_forward_device(qcs_learned_net *net, const float *d_feat, int n,
 /* Loss and parameter gradient of one batch (n <= batch); gradients via qcs_learned_get_grads. */
 int qcs_learned_gradient_device(qcs_learned_net *net, const float *d_feat, const float *d_targets,
                                 const float *d_valid, int n, float *h_loss, void *stream);
+/* The same with emitter-count labels d_classes (n floats: 0, 1, 2, or -1 for
+ * none; NULL: none): the loss adds 0.5 x the softmax cross-entropy of the
+ * count logits (outputs 5..7) per labelled row, over the batch. */
+int qcs_learned_gradient_counts_device(qcs_learned_net *net, const float *d_feat, const float *d_targets,
+                                       const float *d_valid, const float *d_classes, int n, float *h_loss,
+                                       void *stream);
 int qcs_learned_get_grads(qcs_learned_net *net, float *h_grads);
 /* Adam training over n rows for `epochs` epochs; h_epoch_loss (epochs floats, may be NULL). */
 int qcs_learned_train_device(qcs_learned_net *net, const float *d_feat, const float *d_targets, const float *d_valid,
                              int n, int epochs, float lr, unsigned long long seed, float *h_epoch_loss, void *stream);
+/* The same with emitter-count labels (as qcs_learned_gradient_counts_device). */
+int qcs_learned_train_counts_device(qcs_learned_net *net, const float *d_feat, const float *d_targets,
+                                    const float *d_valid, const float *d_classes, int n, int epochs, float lr,
+                                    unsigned long long seed, float *h_epoch_loss, void *stream);
+/* Emitter-count labels of the n records of the last multi-emitter call on c
+ * (d_labels: n floats): 0 where the plain cascade did not send the record to
+ * the two-emitter fit, 1 where that fit kept it, 2 where it passed it on to
+ * the three-emitter fit. */
+int qcs_loc_count_labels_device(qcs_loc_data *c, int n, float *d_labels, void *stream);
+/* Routing threshold th of the count classes: with multi-emitter fitting on,
+ * qcs_learned_localize_device sends a record straight to the three-emitter
+ * fit when p(class 2) >= th, else to the two-emitter fit when p(class 1) +
+ * p(class 2) >= th (softmax probabilities); th = 0 (the default) routes by
+ * the WLE classes alone, as the reference does.  QCS_ERR_ARG outside [0, 1]. */
+int qcs_learned_set_count_threshold(qcs_learned_net *net, float th);
+float qcs_learned_count_threshold(const qcs_learned_net *net);
+/* Start points (as qcs_learned_start_device) and emitter-count classes
+ * (uint8 per record, at the routing threshold, or 0.5 when routing is off)
+ * of n device records. */
+int qcs_learned_classes_device(qcs_learned_net *net, const qcs_loc_para *p, const uint16_t *d_rois, int n,
+                               float *d_start, uint8_t *d_classes, void *stream);
 /* Start points (n x 5: peak e-, x, y, sigma, background e-) of n device records;
  * d_work holds qcs_learned_work_bytes(n) bytes (unused by the fused path). */
 int qcs_learned_start_device(qcs_learned_net *net, const qcs_loc_para *p, const uint16_t *d_rois, int n,
@@ -385,15 +415,35 @@ size_t qcs_learned_work_bytes(int n);
  * steps each (<= 0: the reference's 11; schedules: 2..5 or 8 iterations with
  * 11 steps, 2 or 3 with 4, 6 or 8) and the loss's analytic gradient; fits that
  * are not accepted or whose Poisson deviance exceeds dev_th (<= 0: 100) are
- * refitted by the plain kernel; then CRLB.  Rows in the context (n). */
+ * refitted by the plain kernel; then CRLB.  Rows in the context (n).  With
+ * p->MultiEmitterFitEn the single-emitter fit is the first stage of the
+ * reference's cascade (bfgs_top.cu:26-204): it runs over the single-emitter
+ * queue, a plain refit decides which rejects go on to the two-emitter fit,
+ * and the 2E / 3E stages, appended rows and CRLB follow as in
+ * qcs_loc_localize_device. */
 int qcs_fit_from_start_device(qcs_loc_data *c, const uint16_t *d_rois, const float *d_wle, const qcs_loc_para *p,
                               int n, const float *d_start, int iters, int bisections, float dev_th, void *stream);
-/* GS2D 7x7 single-emitter localization from learned start points with the
- * schedule of qcs_fit_from_start_device.  Rows in the context like
- * qcs_loc_localize_device (n rows). */
+/* The same with emitter-count classes d_classes (uint8 per record, or NULL;
+ * multi-emitter fitting only): class 1 joins the two-emitter queue and class
+ * 2 the three-emitter queue without the stages before. */
+int qcs_fit_from_start_classes_device(qcs_loc_data *c, const uint16_t *d_rois, const float *d_wle,
+                                      const qcs_loc_para *p, int n, const float *d_start, const uint8_t *d_classes,
+                                      int iters, int bisections, float dev_th, void *stream);
+/* GS2D 7x7 localization from learned start points with the schedule of
+ * qcs_fit_from_start_device, and, with multi-emitter fitting on and a count
+ * threshold set, the network's emitter-count classes.  Rows in the context
+ * like qcs_loc_localize_device. */
 int qcs_learned_localize_device(qcs_loc_data *c, qcs_learned_net *net, const uint16_t *d_rois, const float *d_wle,
                                 const qcs_loc_para *p, int n, int iters, int bisections, float dev_th,
                                 void *stream);
+/* qcs_learned_localize_device with the record count in device memory (*d_n,
+ * at most max_n; e.g. qcs_extract_device_roi_num after extraction), like
+ * qcs_loc_localize_device_n; GS2D 7x7 with multi-emitter fitting on, d_wle
+ * required.  The fused inference reads the count on the device; the
+ * layer-by-layer inference computes all max_n records. */
+int qcs_learned_localize_device_n(qcs_loc_data *c, qcs_learned_net *net, const uint16_t *d_rois, const float *d_wle,
+                                  const qcs_loc_para *p, const int *d_n, int max_n, int iters, int bisections,
+                                  float dev_th, void *stream);
 /* Inference path of qcs_learned_localize_device: fused = 1 (default) runs the
  * whole network per 128-ROI tile in one tcgen05 kernel; 0 runs it layer by
  * layer through the training GEMMs. */
@@ -409,7 +459,7 @@ int qcs_learned_fused_status(qcs_learned_net *net);
 int qcs_learned_localize_async(qcs_loc_data *c, qcs_learned_net *net, const uint16_t *h_rois, const float *h_wle,
                                const qcs_loc_para *p, int n, int iters, int bisections, float dev_th,
                                void *stream);
-/* Number of plain refits of the last qcs_learned_localize_device call (waits for it). */
+/* Number of plain single-emitter refits of the last qcs_learned_localize_device call (waits for it). */
 int qcs_learned_refit_num(qcs_loc_data *c, int *n);
 
 /* ---- super-resolution render (ImageRenderData_TypeDef) ------------------ */

@@ -1,7 +1,8 @@
 """TEST INFRASTRUCTURE ONLY -- numpy restatement of the learned start-point
 network of qc-storm_b200/csrc/qcs_learned.cu (features, targets, forward pass,
-masked weighted MSE and its gradient), used by the tests to check the GPU
-kernels' forward outputs and gradients.  The network has no counterpart in
+masked weighted MSE plus the emitter-count cross-entropy and its gradient,
+the class rule), used by the tests to check the GPU kernels' forward outputs,
+gradients and classes.  The network has no counterpart in
 the reference; its definition is the one in qcs_learned.cu / qcs_learned.h.
 
 GEMM operands are rounded to bfloat16 as the tensor-core kernels round them;
@@ -18,6 +19,7 @@ CENTRE = R / 2.0
 SIGMA0 = 1.3
 N_IN, N_HID, N_OUT, N_USED = 64, 128, 8, 5
 TARGET_WEIGHT = np.array([4.0, 4.0, 1.0, 1.0, 1.0])
+COUNT0, CLASSES, COUNT_WEIGHT = 5, 3, 0.5  # outputs 5..7: emitter-count logits
 N_PARAMS = N_IN * N_HID + N_HID + N_HID * N_HID + N_HID + N_HID * N_OUT + N_OUT
 
 
@@ -76,8 +78,20 @@ def forward(params, x):
     return y, (x, z1, a1, z2, a2)
 
 
-def loss_and_grad(params, x, t, valid):
-    """Mean over the batch of sum_j w_j (y_j - t_j)^2 * valid, and its gradient."""
+def count_class(logits, th):
+    """Emitter-count class per row of the three logits: 2 when p2 >= th, else
+    1 when p1 + p2 >= th, else 0 (float32 softmax numerators, as the kernels)."""
+    lg = np.asarray(logits, np.float32)
+    e = np.exp(lg - lg.max(axis=1, keepdims=True))
+    s = e.sum(axis=1)
+    th = np.float32(th)
+    return np.where(e[:, 2] >= th * s, 2, np.where(e[:, 1] + e[:, 2] >= th * s, 1, 0)).astype(np.uint8)
+
+
+def loss_and_grad(params, x, t, valid, classes=None):
+    """Mean over the batch of sum_j w_j (y_j - t_j)^2 * valid plus, for rows
+    with a class label c >= 0, COUNT_WEIGHT * (-log softmax(logits)[c]); and
+    its gradient."""
     W1, b1, W2, b2, W3, b3 = split_params(params)
     y, (x, z1, a1, z2, a2) = forward(params, x)
     n = x.shape[0]
@@ -85,6 +99,18 @@ def loss_and_grad(params, x, t, valid):
     loss = float(np.sum(TARGET_WEIGHT * e * e * valid[:, None]) / n)
     dy = np.zeros_like(y)
     dy[:, :N_USED] = 2.0 * TARGET_WEIGHT * e * valid[:, None] / n
+    if classes is not None:
+        c = np.asarray(classes).astype(np.int64)
+        lab = c >= 0
+        lg = y[:, COUNT0:COUNT0 + CLASSES]
+        m = lg.max(axis=1, keepdims=True)
+        p = np.exp(lg - m)
+        p /= p.sum(axis=1, keepdims=True)
+        rows = np.nonzero(lab)[0]
+        loss += float(COUNT_WEIGHT * np.sum(-np.log(p[rows, c[rows]])) / n)
+        onehot = np.zeros_like(p)
+        onehot[rows, c[rows]] = 1.0
+        dy[:, COUNT0:COUNT0 + CLASSES] = COUNT_WEIGHT * (p - onehot) * lab[:, None] / n
     gW3 = bf16(a2).T @ bf16(dy)
     gb3 = dy.sum(axis=0)
     d2 = bf16(dy) @ bf16(W3).T

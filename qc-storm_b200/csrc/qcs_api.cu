@@ -63,7 +63,10 @@ struct qcs_loc_data {
     cudaStream_t side = nullptr;  // high-priority stream for work overlapped with the main stream
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaEvent_t ev_done = nullptr;  // end of the last asynchronous host call
-    float *d_start = nullptr;       // learned start points, capacity x 5
+    float *d_start = nullptr;       // learned start points, capacity x 5 (one block with the three below)
+    int *q_refit = nullptr;         // learned multi-emitter path: records to refit plainly
+    uint8_t *d_refit = nullptr;     //   their per-record flags
+    uint8_t *d_cls = nullptr;       //   emitter-count class per record
     int pending = 0;                // an asynchronous host call awaits qcs_loc_finish
     int pending_n = 0;
     int valid = 0;
@@ -174,7 +177,7 @@ int qcs_loc_init_capacity(const qcs_loc_para *p, int capacity, qcs_loc_data **ou
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
     if (e == cudaSuccess) e = qcs::wle_sorter_create(capacity, c->d_wle_scratch, &c->wle_sorter);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_done, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = A((void **)&c->d_start, cap * 5 * sizeof(float));
+    if (e == cudaSuccess) e = A((void **)&c->d_start, cap * (5 * sizeof(float) + sizeof(int) + 2));
     if (e != cudaSuccess) {
         qcs_loc_deinit(c);
         return fail(e == cudaErrorMemoryAllocation ? QCS_ERR_NOMEM : QCS_ERR_CUDA, "qcs_loc_init", e);
@@ -189,6 +192,9 @@ int qcs_loc_init_capacity(const qcs_loc_para *p, int capacity, qcs_loc_data **ou
     c->st.extra2 = reinterpret_cast<float *>(s); s += a_row;
     c->st.extra3 = reinterpret_cast<float *>(s); s += a_row;
     c->st.counters = reinterpret_cast<int *>(s);
+    c->q_refit = reinterpret_cast<int *>(c->d_start + cap * 5);
+    c->d_refit = reinterpret_cast<uint8_t *>(c->q_refit + cap);
+    c->d_cls = c->d_refit + cap;
     *out = c;
     return QCS_OK;
 }
@@ -256,6 +262,7 @@ namespace {
 // rows for n records after a learned-start call; refits stay counted at
 // st.counters[kCntSingle]
 __global__ void learned_counters_kernel(qcs::CascadeState st, int n) {
+    st.counters[qcs::kCntRefit] = st.counters[qcs::kCntSingle];
     st.counters[qcs::kCnt2E] = 0;
     st.counters[qcs::kCnt2EClassify] = 0;
     st.counters[qcs::kCnt3E] = 0;
@@ -263,20 +270,79 @@ __global__ void learned_counters_kernel(qcs::CascadeState st, int n) {
     st.counters[qcs::kCntRows] = n;
     st.counters[qcs::kCntValid] = n;
 }
+
+// BFGS schedules the learned-start fit is compiled for
+bool learned_schedule(int iters, int bisections) {
+    return (bisections == 11 && ((iters >= 2 && iters <= 5) || iters == 8)) ||
+           ((iters == 2 || iters == 3) && (bisections == 4 || bisections == 6 || bisections == 8));
+}
+
+// Emitter-count class of each of n records from the cascade state of a plain
+// multi-emitter call: 0 for records the call did not send to the two-emitter
+// fit, then, over the 2E queue, 1 where that fit kept the ROI and 2 where it
+// passed it on to the three-emitter fit.
+__global__ void labels_zero_kernel(float *__restrict__ cls, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) cls[i] = 0.0f;
+}
+__global__ void labels_2e_kernel(qcs::CascadeState st, int n, float *__restrict__ cls) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= st.counters[qcs::kCnt2E]) return;
+    const int id = st.q2[k];
+    if (id >= 0 && id < n) cls[id] = st.res2[k] == 0 ? 2.0f : 1.0f;
+}
+
+// The learned multi-emitter call: the cascade's queues (with the predicted
+// classes when cls is set), the learned-start single-emitter fit over the
+// single queue, a plain refit of the fits it flags (which also flags the
+// rejects that go on to the 2E fit), then the reference's 2E / 3E stages and
+// the CRLB.
+cudaError_t learned_multi(qcs_loc_data *c, const uint16_t *d_rois, const float *wle, const qcs_loc_para *p, int n,
+                          const int *n_dev, const float *d_start, const uint8_t *cls, int iters, int bisections,
+                          float dev_th, cudaStream_t s) {
+    qcs::CascadeArgs a;
+    a.para = *p;
+    a.rois = d_rois;
+    a.wle = wle;
+    a.n = n;
+    a.n_dev = n_dev;
+    a.loc = c->d_loc;
+    a.max_rows = c->max_rows;
+    a.stream = s;
+    a.pred = cls;
+    cudaError_t e;
+    if ((e = qcs::cascade_classify(a, c->st)) != cudaSuccess) return e;
+    qcs::FitLaunch f = qcs::cascade_single_launch(a, c->st);
+    if ((e = cudaMemsetAsync(c->d_refit, 0, (size_t)n, s)) != cudaSuccess) return e;
+    if ((e = qcs::launch_fit_learned(7, iters, bisections, f, d_start, dev_th, c->d_refit)) != cudaSuccess) return e;
+    if ((e = qcs::launch_flag_queue(c->d_refit, n, c->q_refit, c->st.counters + qcs::kCntRefit, s)) != cudaSuccess)
+        return e;
+    f.q = qcs::Queue{c->q_refit, c->st.counters + qcs::kCntRefit, 0};
+    if ((e = qcs::launch_fit_group(qcs::kGS2D, 7, 8, f)) != cudaSuccess) return e;
+    return qcs::cascade_tail(a, c->st);
+}
 }  // namespace
 
 extern "C" {
 
 int qcs_fit_from_start_device(qcs_loc_data *c, const uint16_t *d_rois, const float *d_wle, const qcs_loc_para *p,
                               int n, const float *d_start, int iters, int bisections, float dev_th, void *stream) {
+    return qcs_fit_from_start_classes_device(c, d_rois, d_wle, p, n, d_start, nullptr, iters, bisections, dev_th,
+                                             stream);
+}
+
+int qcs_fit_from_start_classes_device(qcs_loc_data *c, const uint16_t *d_rois, const float *d_wle,
+                                      const qcs_loc_para *p, int n, const float *d_start, const uint8_t *d_classes,
+                                      int iters, int bisections, float dev_th, void *stream) {
     int st = check_call(c, p, n);
     if (st) return st;
-    if (p->LocType != QCS_LOCTYPE_GS2D || p->ROISize != 7 || p->MultiEmitterFitEn)
-        return fail(QCS_ERR_ARG, "start-point fits: GS2D 7x7 single-emitter fitting only");
+    if (p->LocType != QCS_LOCTYPE_GS2D || p->ROISize != 7)
+        return fail(QCS_ERR_ARG, "start-point fits: GS2D 7x7 only");
+    if (d_classes && !p->MultiEmitterFitEn)
+        return fail(QCS_ERR_ARG, "emitter-count classes need multi-emitter fitting");
     if (bisections <= 0) bisections = 11;
-    const bool schedule = (bisections == 11 && ((iters >= 2 && iters <= 5) || iters == 8)) ||
-                          ((iters == 2 || iters == 3) && (bisections == 4 || bisections == 6 || bisections == 8));
-    if (!schedule) return fail(QCS_ERR_ARG, "schedule: iters 2..5 or 8 with 11 bisections, or 2..3 with 4, 6 or 8");
+    if (!learned_schedule(iters, bisections))
+        return fail(QCS_ERR_ARG, "schedule: iters 2..5 or 8 with 11 bisections, or 2..3 with 4, 6 or 8");
     if (n == 0) return QCS_OK;
     if (!d_rois || !d_start) return fail(QCS_ERR_ARG, "null pointer");
     if (!(dev_th > 0.0f)) dev_th = 100.0f;
@@ -285,6 +351,11 @@ int qcs_fit_from_start_device(qcs_loc_data *c, const uint16_t *d_rois, const flo
     if (!wle) {
         QCS_CUDA(qcs::launch_wle_ctx(c->wle_sorter, d_rois, n, c->R, p->LocType, c->d_wle, s), "WLE pre-pass");
         wle = c->d_wle;
+    }
+    if (p->MultiEmitterFitEn) {
+        QCS_CUDA(learned_multi(c, d_rois, wle, p, n, nullptr, d_start, d_classes, iters, bisections, dev_th, s),
+                 "learned multi-emitter localization");
+        return QCS_OK;
     }
     qcs::FitLaunch f;
     f.rois = d_rois;
@@ -296,7 +367,7 @@ int qcs_fit_from_start_device(qcs_loc_data *c, const uint16_t *d_rois, const flo
     f.mo = qcs::MultiOut{nullptr, nullptr};
     f.para = qcs::core_para(*p);
     f.stream = s;
-    QCS_CUDA(qcs::launch_fit_learned(7, iters, bisections, f, d_start, dev_th, c->st.to2e, n), "start-point fit");
+    QCS_CUDA(qcs::launch_fit_learned(7, iters, bisections, f, d_start, dev_th, c->st.to2e), "start-point fit");
     // plain refit of the flagged records
     QCS_CUDA(qcs::launch_flag_queue(c->st.to2e, n, c->st.q_single, c->st.counters + qcs::kCntSingle, s),
              "refit queue");
@@ -326,13 +397,37 @@ int qcs_learned_localize_device(qcs_loc_data *c, qcs_learned_net *net, const uin
     int st = check_call(c, p, n);
     if (st) return st;
     if (!net) return fail(QCS_ERR_ARG, "null network");
-    if (p->LocType != QCS_LOCTYPE_GS2D || p->ROISize != 7 || p->MultiEmitterFitEn)
-        return fail(QCS_ERR_ARG, "learned start points: GS2D 7x7 single-emitter fitting only");
+    if (p->LocType != QCS_LOCTYPE_GS2D || p->ROISize != 7)
+        return fail(QCS_ERR_ARG, "learned start points: GS2D 7x7 only");
     if (n == 0) return QCS_OK;
     if (!d_rois) return fail(QCS_ERR_ARG, "null ROI pointer");
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
-    QCS_CUDA(qcs::learned::start_points(net, p, d_rois, n, c->d_start, s), "learned start points");
-    return qcs_fit_from_start_device(c, d_rois, d_wle, p, n, c->d_start, iters, bisections, dev_th, s);
+    // emitter-count routing: multi-emitter fitting on and a threshold set
+    uint8_t *cls = (p->MultiEmitterFitEn && qcs_learned_count_threshold(net) > 0.0f) ? c->d_cls : nullptr;
+    QCS_CUDA(qcs::learned::start_points(net, p, d_rois, n, c->d_start, s, cls), "learned start points");
+    return qcs_fit_from_start_classes_device(c, d_rois, d_wle, p, n, c->d_start, cls, iters, bisections, dev_th, s);
+}
+
+int qcs_learned_localize_device_n(qcs_loc_data *c, qcs_learned_net *net, const uint16_t *d_rois, const float *d_wle,
+                                  const qcs_loc_para *p, const int *d_n, int max_n, int iters, int bisections,
+                                  float dev_th, void *stream) {
+    int st = check_call(c, p, max_n);
+    if (st) return st;
+    if (!net) return fail(QCS_ERR_ARG, "null network");
+    if (p->LocType != QCS_LOCTYPE_GS2D || p->ROISize != 7 || !p->MultiEmitterFitEn)
+        return fail(QCS_ERR_ARG, "device-count learned localization: GS2D 7x7 with multi-emitter fitting");
+    if (!d_rois || !d_wle || !d_n) return fail(QCS_ERR_ARG, "null pointer");
+    if (bisections <= 0) bisections = 11;
+    if (!learned_schedule(iters, bisections))
+        return fail(QCS_ERR_ARG, "schedule: iters 2..5 or 8 with 11 bisections, or 2..3 with 4, 6 or 8");
+    if (!(dev_th > 0.0f)) dev_th = 100.0f;
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+    uint8_t *cls = qcs_learned_count_threshold(net) > 0.0f ? c->d_cls : nullptr;
+    if (max_n == 0) return QCS_OK;
+    QCS_CUDA(qcs::learned::start_points(net, p, d_rois, max_n, c->d_start, s, cls, d_n), "learned start points");
+    QCS_CUDA(learned_multi(c, d_rois, d_wle, p, max_n, d_n, c->d_start, cls, iters, bisections, dev_th, s),
+             "learned multi-emitter localization");
+    return QCS_OK;
 }
 
 int qcs_learned_refit_num(qcs_loc_data *c, int *n) {
@@ -340,7 +435,18 @@ int qcs_learned_refit_num(qcs_loc_data *c, int *n) {
     QCS_CUDA(cudaDeviceSynchronize(), "localization");
     QCS_CUDA(cudaMemcpy(c->h_counters, c->st.counters, qcs::kCntNum * sizeof(int), cudaMemcpyDeviceToHost),
              "read counters");
-    *n = c->h_counters[qcs::kCntSingle];
+    *n = c->h_counters[qcs::kCntRefit];
+    return QCS_OK;
+}
+
+int qcs_loc_count_labels_device(qcs_loc_data *c, int n, float *d_labels, void *stream) {
+    if (!c || !d_labels) return fail(QCS_ERR_ARG, "null argument");
+    if (n < 0 || n > c->capacity) return fail(QCS_ERR_CAPACITY, "record count outside the context capacity");
+    if (n == 0) return QCS_OK;
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+    labels_zero_kernel<<<(n + 255) / 256, 256, 0, s>>>(d_labels, n);
+    labels_2e_kernel<<<(n + 255) / 256, 256, 0, s>>>(c->st, n, d_labels);
+    QCS_CUDA(cudaGetLastError(), "count labels");
     return QCS_OK;
 }
 
@@ -359,11 +465,12 @@ static void compute_ratios(qcs_loc_data *c, const qcs_loc_para *p, int n) {
     c->ratios[3] = (float)single / div;
     if (p->MultiEmitterFitEn) {
         const int n2 = k[qcs::kCnt2E], n2c = k[qcs::kCnt2EClassify], n3 = k[qcs::kCnt3E], rej = k[qcs::kCntRejected];
+        const int n3c = k[qcs::kCnt3EClassify];  // learned classes only: records sent straight to 3E
         c->ratios[1] = (float)n2 / div;
         c->ratios[2] = (float)n3 / div;
         c->ratios[3] = (float)(single - (n2 - n2c)) / div;
         if (p->LocType == QCS_LOCTYPE_GS2D) {
-            c->ratios[4] = (float)(n2 - n3) / div;
+            c->ratios[4] = (float)(n2 - (n3 - n3c)) / div;
             c->ratios[5] = (float)(n3 - rej) / div;
         } else {
             c->ratios[4] = (float)(n2 - rej) / div;
@@ -488,8 +595,9 @@ int qcs_loc_read_rows(qcs_loc_data *c, const qcs_loc_para *p, void *stream) {
                  "read localizations");
     QCS_CUDA(cudaStreamSynchronize(s), "read localizations");
     c->valid = rows;
-    // records of the call: single-emitter queue plus the classifier's 2E entries
-    const int n = c->h_counters[qcs::kCntSingle] + (p->MultiEmitterFitEn ? c->h_counters[qcs::kCnt2EClassify] : 0);
+    // records of the call: single-emitter queue plus the classifier's 2E and 3E entries
+    const int n = c->h_counters[qcs::kCntSingle] +
+                  (p->MultiEmitterFitEn ? c->h_counters[qcs::kCnt2EClassify] + c->h_counters[qcs::kCnt3EClassify] : 0);
     compute_ratios(c, p, n);
     return QCS_OK;
 }

@@ -46,33 +46,45 @@ __device__ __forceinline__ int block_scan(int pred, int *total) {
 
 // Split records by WLE molecule type into the single-emitter queue
 // (MLEFit, WLEFit) and the two-emitter queue (MultiFit), both ascending
-// (bfgs_top_MoleculeClasify.cu:26-92).
+// (bfgs_top_MoleculeClasify.cu:26-92).  With a predicted emitter-count class
+// per record (pred, learned path only: 0 one emitter, 1 the two-emitter
+// stage, 2 the three-emitter stage), class 2 goes straight to the 3E queue
+// and class 1 to the 2E queue, so neither pays for the fits that would have
+// rejected it; pred == null is the reference's split.
 __global__ void __launch_bounds__(kScanThreads) classify_queues_kernel(const float *__restrict__ wle, int n,
                                                                        const int *__restrict__ n_dev, int multi,
+                                                                       const uint8_t *__restrict__ pred,
                                                                        CascadeState st) {
     __shared__ int tot;
     if (n_dev) n = min(max(*n_dev, 0), n);
-    int n1 = 0, n2 = 0;
+    int n1 = 0, n2 = 0, n3 = 0;
     for (int base = 0; base < n; base += kScanThreads) {
         const int i = base + threadIdx.x;
         const int valid = i < n;
         const int type = valid ? (int)wle[(size_t)i * QCS_WLE_PARA_NUM + 5] : 0;
-        const int to_multi = valid && multi && (type > QCS_MOLECULE_WLEFIT);
-        const int to_single = valid && !to_multi;
+        const int cls = (valid && pred) ? pred[i] : 0;
+        const int to_3e = valid && multi && cls == 2;
+        const int to_multi = valid && multi && !to_3e && (type > QCS_MOLECULE_WLEFIT || cls == 1);
+        const int to_single = valid && !to_multi && !to_3e;
         int p1 = block_scan(to_single, &tot);
         const int t1 = tot;
         if (to_single) st.q_single[n1 + p1] = i;
         int p2 = block_scan(to_multi, &tot);
         const int t2 = tot;
         if (to_multi) st.q2[n2 + p2] = i;
+        int p3 = block_scan(to_3e, &tot);
+        const int t3 = tot;
+        if (to_3e) st.q3[n3 + p3] = i;
         n1 += t1;
         n2 += t2;
+        n3 += t3;
     }
     if (threadIdx.x == 0) {
         st.counters[kCntSingle] = n1;
         st.counters[kCnt2E] = n2;
         st.counters[kCnt2EClassify] = n2;
-        st.counters[kCnt3E] = 0;
+        st.counters[kCnt3E] = n3;
+        st.counters[kCnt3EClassify] = n3;
         st.counters[kCntRejected] = 0;
         st.counters[kCntRows] = n;
     }
@@ -110,7 +122,8 @@ __global__ void __launch_bounds__(kScanThreads) compact_multi_kernel(CascadeStat
     const float *extra = (stage == 2) ? st.extra2 : st.extra3;
     const int *queue = (stage == 2) ? st.q2 : st.q3;
     int rows = st.counters[kCntRows];
-    int n3 = 0, rejected = st.counters[kCntRejected];
+    // after the 2E stage, rejects follow the records classified straight to 3E
+    int n3 = (stage == 2) ? st.counters[kCnt3E] : 0, rejected = st.counters[kCntRejected];
     for (int base = 0; base < nslots; base += kScanThreads) {
         const int k = base + threadIdx.x;
         const int r = (k < nslots) ? res[k] : -1;
@@ -153,6 +166,7 @@ __global__ void init_counters_kernel(CascadeState st, int n, const int *__restri
     st.counters[kCnt2E] = 0;
     st.counters[kCnt2EClassify] = 0;
     st.counters[kCnt3E] = 0;
+    st.counters[kCnt3EClassify] = 0;
     st.counters[kCntRejected] = 0;
     st.counters[kCntRows] = n;
 }
@@ -164,35 +178,39 @@ __global__ void finish_kernel(CascadeState st, int max_rows) {
 
 }  // namespace
 
-cudaError_t run_cascade(const CascadeArgs &a, const CascadeState &st) {
-    const qcs_loc_para &p = a.para;
-    const int n = a.n;
-    const int R = p.ROISize;
-    const int multi = p.MultiEmitterFitEn;
-    const bool as3d = (p.LocType == QCS_LOCTYPE_AS3D);
-    const CorePara c = core_para(p);
-    cudaError_t e;
-
-    if (multi)
-        classify_queues_kernel<<<1, kScanThreads, 0, a.stream>>>(a.wle, n, a.n_dev, multi, st);
+cudaError_t cascade_classify(const CascadeArgs &a, const CascadeState &st) {
+    if (a.para.MultiEmitterFitEn)
+        classify_queues_kernel<<<1, kScanThreads, 0, a.stream>>>(a.wle, a.n, a.n_dev, 1, a.pred, st);
     else
-        init_counters_kernel<<<1, 1, 0, a.stream>>>(st, n, a.n_dev);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        init_counters_kernel<<<1, 1, 0, a.stream>>>(st, a.n, a.n_dev);
+    return cudaGetLastError();
+}
 
+FitLaunch cascade_single_launch(const CascadeArgs &a, const CascadeState &st) {
+    const int multi = a.para.MultiEmitterFitEn;
     FitLaunch f;
     f.rois = a.rois;
     f.wle = a.wle;
     f.loc = a.loc;
-    f.para = c;
+    f.para = core_para(a.para);
     f.stream = a.stream;
     f.mo = MultiOut{nullptr, nullptr};
     // Single emitter over the classify queue (identity when multi-emitter
     // fitting is off, as in the reference); its length is on the device.
     f.q = Queue{multi ? st.q_single : nullptr, st.counters + kCntSingle, 0};
-    f.max_count = n;
+    f.max_count = a.n;
     f.to2e = multi ? st.to2e : nullptr;
-    if ((e = launch_fit(as3d ? kAS3D : kGS2D, R, f)) != cudaSuccess) return e;
+    return f;
+}
 
+cudaError_t cascade_tail(const CascadeArgs &a, const CascadeState &st) {
+    const qcs_loc_para &p = a.para;
+    const int n = a.n;
+    const int R = p.ROISize;
+    const int multi = p.MultiEmitterFitEn;
+    const bool as3d = (p.LocType == QCS_LOCTYPE_AS3D);
+    cudaError_t e;
+    FitLaunch f = cascade_single_launch(a, st);
     if (multi) {
         append_2e_kernel<<<1, kScanThreads, 0, a.stream>>>(st);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -218,6 +236,14 @@ cudaError_t run_cascade(const CascadeArgs &a, const CascadeState &st) {
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     return launch_crlb(a.loc, st.counters + kCntValid, 0, multi ? a.max_rows : n, p.LocType, p.ReadNoise_e, p.QE,
                        p.PixelSize, a.stream);
+}
+
+cudaError_t run_cascade(const CascadeArgs &a, const CascadeState &st) {
+    cudaError_t e = cascade_classify(a, st);
+    if (e != cudaSuccess) return e;
+    const bool as3d = (a.para.LocType == QCS_LOCTYPE_AS3D);
+    if ((e = launch_fit(as3d ? kAS3D : kGS2D, a.para.ROISize, cascade_single_launch(a, st))) != cudaSuccess) return e;
+    return cascade_tail(a, st);
 }
 
 }  // namespace qcs

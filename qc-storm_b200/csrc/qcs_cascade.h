@@ -17,7 +17,9 @@ enum {
     kCntRejected = 4,    // ROIs rejected by the last multi-emitter stage
     kCntRows = 5,        // rows produced (records + appended second emitters)
     kCntValid = 6,       // rows produced, capped at the row capacity
-    kCntNum = 8
+    kCnt3EClassify = 7,  // three-emitter queue entries that came from the classifier (learned classes)
+    kCntRefit = 8,       // learned path: records refitted by the plain single-emitter fit
+    kCntNum = 16
 };
 
 // Scratch of one context, sized for `capacity` records.
@@ -42,8 +44,19 @@ struct CascadeArgs {
     float *loc;            // device, max_rows x 12
     int max_rows;
     cudaStream_t stream;
+    const uint8_t *pred = nullptr;  // learned emitter-count class per record, or null (the reference's split)
 };
 
+// The whole localization call: queues, single-emitter fit, 2E / 3E fits,
+// CRLB.
 cudaError_t run_cascade(const CascadeArgs &a, const CascadeState &st);
+
+// Its phases, for callers that replace the single-emitter fit (the learned
+// path): the queues; the single-emitter launch run_cascade makes over them;
+// everything after the single-emitter fit (which must have set to2e for
+// every record of the single queue when multi-emitter fitting is on).
+cudaError_t cascade_classify(const CascadeArgs &a, const CascadeState &st);
+struct FitLaunch cascade_single_launch(const CascadeArgs &a, const CascadeState &st);
+cudaError_t cascade_tail(const CascadeArgs &a, const CascadeState &st);
 
 }  // namespace qcs

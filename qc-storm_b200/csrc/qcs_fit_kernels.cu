@@ -451,20 +451,22 @@ __global__ void __launch_bounds__(kGroupTPB) fit_single_group_kernel(const uint1
 // x, y in ROI pixels, sigma, background e-) instead of the centre / edge-mean
 // pre-estimate, with ITERS BFGS iterations instead of 8 and the analytic
 // gradient (AnalyticEvalGS2D) instead of the central difference.  The same
-// weighted loss, line search, accept rules and output row.  refit[id] = 1 when the fit
-// is not accepted or when its unweighted Poisson deviance
-// 2 sum(mu - n - n ln(mu / n)) exceeds dev_th: those ROIs are refitted by the
-// plain kernel.
+// weighted loss, line search, accept rules (the narrower sigma bound with
+// multi-emitter fitting on) and output row, over the records of a queue.
+// refit[id] = 1 when the fit is not accepted or when its unweighted Poisson
+// deviance 2 sum(mu - n - n ln(mu / n)) exceeds dev_th: those ROIs are
+// refitted by the plain kernel, which also decides whether a rejected one
+// goes on to the two-emitter fit (to2e).
 template <int R, int ITERS, int NB, int DIST = ArithSpec<kGS2D, R>::DIST, int MASK = ArithSpec<kGS2D, R>::MASK>
 __global__ void __launch_bounds__(kTPB) fit_learned_kernel(const uint16_t *__restrict__ rois,
                                                            const float *__restrict__ wle,
-                                                           const float *__restrict__ start, int n,
+                                                           const float *__restrict__ start, Queue q,
                                                            float *__restrict__ loc, uint8_t *__restrict__ refit,
-                                                           CorePara c, float dev_th) {
+                                                           uint8_t *__restrict__ to2e, CorePara c, float dev_th) {
     typedef SmemLayout<R, kGS2D> L;
     enum { P = 5, PIX = R * R, WHOLE = R * (R + 1), ROISize_Half = R / 2 };
     extern __shared__ float smem[];
-    const Queue q{nullptr, nullptr, n};
+    const int n = queue_len(q);
     const int base = blockIdx.x * kTPB;
     if (base >= n) return;
     const int cnt = min(kTPB, n - base);
@@ -473,7 +475,7 @@ __global__ void __launch_bounds__(kTPB) fit_learned_kernel(const uint16_t *__res
     __syncthreads();
     const int tid = threadIdx.x;
     if (tid >= cnt) return;
-    const int id = base + tid;
+    const int id = queue_at(q, base + tid);
     float *w = smem + L::W + tid;
     float *D = smem + L::D + tid;
     const uint16_t *hdr = rois + (size_t)id * WHOLE + PIX;
@@ -484,7 +486,7 @@ __global__ void __launch_bounds__(kTPB) fit_learned_kernel(const uint16_t *__res
 
     const float XYLBound = R / 2.0f - 1.5f;
     const float XYUBound = R / 2.0f + 1.5f;
-    const float Simga_Max_Th = R / 1.5f / 2.35f;
+    const float Simga_Max_Th = c.MultiEmitterFitEn ? R / 2.0f / 2.35f : R / 1.5f / 2.35f;
     float SigmaL = pw[1], SigmaR = pw[2], SigmaU = pw[3], SigmaD = pw[4];
     const int MoleculeType = pw[5];
     SigmaL = fminf(SigmaL, SigmaR);
@@ -526,6 +528,7 @@ __global__ void __launch_bounds__(kTPB) fit_learned_kernel(const uint16_t *__res
         }
     dev *= 2.0f;
     refit[id] = (!accepted || !(dev <= dev_th)) ? 1 : 0;
+    if (to2e) to2e[id] = 0;  // a kept fit is final; a refit sets the flag again
     if (accepted) {
         float row[12];
         row[0] = PeakPhoton;
@@ -562,14 +565,14 @@ __global__ void flag_queue_kernel(const uint8_t *__restrict__ flags, int n, int 
 }
 
 template <int R, int ITERS, int NB>
-cudaError_t launch_learned(const FitLaunch &a, const float *start, float dev_th, uint8_t *refit, int n) {
+cudaError_t launch_learned(const FitLaunch &a, const float *start, float dev_th, uint8_t *refit) {
     const size_t smem = SmemLayout<R, kGS2D>::TOTAL * sizeof(float);
     auto k = fit_learned_kernel<R, ITERS, NB>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    const int grid = (n + kTPB - 1) / kTPB;
+    const int grid = (a.max_count + kTPB - 1) / kTPB;
     if (grid == 0) return cudaSuccess;
-    k<<<grid, kTPB, smem, a.stream>>>(a.rois, a.wle, start, n, a.loc, refit, a.para, dev_th);
+    k<<<grid, kTPB, smem, a.stream>>>(a.rois, a.wle, start, a.q, a.loc, refit, a.to2e, a.para, dev_th);
     return cudaGetLastError();
 }
 
@@ -847,20 +850,20 @@ cudaError_t launch_multi(const FitLaunch &a) {
 }  // namespace
 
 cudaError_t launch_fit_learned(int R, int iters, int bisections, const FitLaunch &a, const float *start,
-                               float dev_th, uint8_t *refit, int n) {
+                               float dev_th, uint8_t *refit) {
     if (R != 7) return cudaErrorInvalidValue;
     if (bisections == kBisections) {
         switch (iters) {
-        case 2: return launch_learned<7, 2, kBisections>(a, start, dev_th, refit, n);
-        case 3: return launch_learned<7, 3, kBisections>(a, start, dev_th, refit, n);
-        case 4: return launch_learned<7, 4, kBisections>(a, start, dev_th, refit, n);
-        case 5: return launch_learned<7, 5, kBisections>(a, start, dev_th, refit, n);
-        case 8: return launch_learned<7, 8, kBisections>(a, start, dev_th, refit, n);
+        case 2: return launch_learned<7, 2, kBisections>(a, start, dev_th, refit);
+        case 3: return launch_learned<7, 3, kBisections>(a, start, dev_th, refit);
+        case 4: return launch_learned<7, 4, kBisections>(a, start, dev_th, refit);
+        case 5: return launch_learned<7, 5, kBisections>(a, start, dev_th, refit);
+        case 8: return launch_learned<7, 8, kBisections>(a, start, dev_th, refit);
         }
         return cudaErrorInvalidValue;
     }
 #define QCS_LEARNED(IT, NB) \
-    if (iters == IT && bisections == NB) return launch_learned<7, IT, NB>(a, start, dev_th, refit, n);
+    if (iters == IT && bisections == NB) return launch_learned<7, IT, NB>(a, start, dev_th, refit);
     QCS_LEARNED(2, 4)
     QCS_LEARNED(2, 6)
     QCS_LEARNED(2, 8)

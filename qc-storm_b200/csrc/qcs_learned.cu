@@ -4,8 +4,11 @@
 // counterpart in the reference (it starts from the centre / edge-mean
 // pre-estimate, bfgsMLE_GS2D_core.h:522-575).
 //
-// Network (per ROI): 64 features -> 128 (ReLU) -> 128 (ReLU) -> 8 outputs
-// (5 used: dx, dy, sigma - 1.3, log(peak / range), (background - min) / range).
+// Network (per ROI): 64 features -> 128 (ReLU) -> 128 (ReLU) -> 8 outputs:
+// dx, dy, sigma - 1.3, log(peak / range), (background - min) / range, and
+// three logits of the ROI's emitter-count class (0: one emitter; 1: the
+// two-emitter fit's stage; 2: the three-emitter fit's stage), with which the
+// multi-emitter cascade sends a ROI straight to the stage it would reach.
 // Features: the 49 photoelectron pixels max((adu - offset) * gain, 1) scaled
 // to [0, 1] by the ROI's min and range, log(range) / 8, log(min) / 8, zeros.
 // Training and inference GEMMs run on the tensor cores in BF16 with FP32
@@ -203,22 +206,37 @@ __global__ void colsum_kernel(const float *__restrict__ dZ, int rows, int cols, 
     g[c] = s;
 }
 
-// Masked weighted MSE on the first kOutUsed outputs: loss and dY.
+// Masked weighted MSE on the first kOutUsed outputs plus, where cls is set
+// and cls[i] >= 0, kCountWeight x the softmax cross-entropy of the count
+// logits against class cls[i]: loss and dY.
 __global__ void mse_kernel(const float *__restrict__ Y, const float *__restrict__ T, const float *__restrict__ valid,
-                           int rows, float inv_count, float *__restrict__ dY, float *__restrict__ loss) {
+                           const float *__restrict__ cls, int rows, float inv_count, float *__restrict__ dY,
+                           float *__restrict__ loss) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= rows) return;
     const float v = valid[i];
+    const float *y = Y + (size_t)i * kOut;
     float l = 0.0f;
 #pragma unroll
     for (int j = 0; j < kOut; ++j) {
         float d = 0.0f;
         if (j < kOutUsed) {
-            const float e = Y[(size_t)i * kOut + j] - T[(size_t)i * kOutUsed + j];
+            const float e = y[j] - T[(size_t)i * kOutUsed + j];
             d = 2.0f * kTargetWeight[j] * e * v * inv_count;
             l += kTargetWeight[j] * e * e * v;
         }
         dY[(size_t)i * kOut + j] = d;
+    }
+    const int label = cls ? (int)cls[i] : -1;
+    if (label >= 0 && label < kClasses) {
+        const float l0 = y[kCount0], l1 = y[kCount0 + 1], l2 = y[kCount0 + 2];
+        const float m = fmaxf(l0, fmaxf(l1, l2));
+        const float e[kClasses] = {expf(l0 - m), expf(l1 - m), expf(l2 - m)};
+        const float sum = e[0] + e[1] + e[2];
+        l += kCountWeight * (logf(sum) - (y[kCount0 + label] - m));
+#pragma unroll
+        for (int j = 0; j < kClasses; ++j)
+            dY[(size_t)i * kOut + kCount0 + j] = kCountWeight * (e[j] / sum - (j == label ? 1.0f : 0.0f)) * inv_count;
     }
     atomicAdd(loss, l * inv_count);
 }
@@ -243,12 +261,14 @@ __global__ void gather_rows_kernel(const float *__restrict__ src, const int *__r
     dst[i] = src[(size_t)idx[r] * cols + c];
 }
 
-// Predictions -> fit start (photoelectron peak, ROI x, y, sigma, background).
+// Predictions -> fit start (photoelectron peak, ROI x, y, sigma, background)
+// and, with cls set, the emitter-count class at threshold th.
 __global__ void start_kernel(const float *__restrict__ Y, const float *__restrict__ scale, int n,
-                             float *__restrict__ start) {
+                             float *__restrict__ start, uint8_t *__restrict__ cls, float th) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float *y = Y + (size_t)i * kOut;
+    if (cls) cls[i] = (uint8_t)count_class(y[kCount0], y[kCount0 + 1], y[kCount0 + 2], th);
     const float lo = scale[2 * i], rng = scale[2 * i + 1];
     float *s = start + (size_t)i * kStart;
     s[0] = rng * expf(fminf(fmaxf(y[3], -6.0f), 3.0f));
@@ -392,8 +412,10 @@ __global__ void __launch_bounds__(128, 1) mlp_tc_kernel(const uint16_t *__restri
                                                         float kadc, const uint4 *__restrict__ wimg,
                                                         const float *__restrict__ b1, const float *__restrict__ b2,
                                                         const float *__restrict__ b3, float *__restrict__ start,
-                                                        int *__restrict__ err) {
+                                                        uint8_t *__restrict__ cls, float count_th,
+                                                        const int *__restrict__ n_dev, int *__restrict__ err) {
     extern __shared__ uint8_t smem_raw[];
+    if (n_dev) n = min(max(*n_dev, 0), n);  // record count on the device, at most n
     const uint32_t raw = (uint32_t)__cvta_generic_to_shared(smem_raw);
     const uint32_t sbase = (raw + (kAlign - 1)) & ~(uint32_t)(kAlign - 1);
     uint8_t *base = smem_raw + (sbase - raw);
@@ -549,6 +571,9 @@ __global__ void __launch_bounds__(128, 1) mlp_tc_kernel(const uint16_t *__restri
             st[2] = kCentre + fminf(fmaxf(y[1] + __ldg(b3 + 1), -1.5f), 1.5f);
             st[3] = fminf(fmaxf(kSigma0 + y[2] + __ldg(b3 + 2), 0.6f), 3.0f);
             st[4] = fmaxf(lo + rng * (y[4] + __ldg(b3 + 4)), 1.0f);
+            if (cls)
+                cls[i] = (uint8_t)count_class(y[kCount0] + __ldg(b3 + kCount0), y[kCount0 + 1] + __ldg(b3 + kCount0 + 1),
+                                              y[kCount0 + 2] + __ldg(b3 + kCount0 + 2), count_th);
         }
         fence_before();
         __syncthreads();  // accumulator columns are free for the next tile
@@ -603,6 +628,7 @@ struct qcs_learned_net {
     unsigned wimg_version = 0;        // parameter version d_wimg was built from
     cudaEvent_t wimg_ready = nullptr; // recorded after d_wimg was built
     bool use_tc = true;
+    float count_th = 0.0f;            // emitter-count routing threshold; 0 = no routing
     int batch = 0;
     long long step = 0;
     cudaStream_t stream = nullptr;
@@ -625,6 +651,9 @@ Views views(float *p) {
 }
 
 inline int blocks(long long n, int t = 256) { return (int)((n + t - 1) / t); }
+
+// threshold of the class outputs: the routing threshold, or 0.5 when routing is off
+inline float class_threshold(const qcs_learned_net *net) { return net->count_th > 0.0f ? net->count_th : 0.5f; }
 
 // Forward over `rows` feature rows into net->d_y (and the hidden activations).
 cudaError_t forward(qcs_learned_net *net, const float *x, int rows, float *z1, float *a1, float *z2, float *a2,
@@ -692,7 +721,7 @@ void shuffle(int *h, int n, unsigned long long &state) {
 // images of the current weights, then one persistent launch (two CTAs of
 // 101 KB shared memory and 256 tensor-memory columns per SM).
 cudaError_t fused_start_points(qcs_learned_net *net, const qcs_loc_para *p, const uint16_t *d_rois, int n,
-                               float *start, cudaStream_t s) {
+                               const int *n_dev, float *start, uint8_t *cls, cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
     const int tiles = (n + L::tc::kM - 1) / L::tc::kM;
     int dev = 0, sms = 148;
@@ -717,7 +746,8 @@ cudaError_t fused_start_points(qcs_learned_net *net, const qcs_loc_para *p, cons
         if (e != cudaSuccess) return e;
     }
     kern<<<grid, 128, L::tc::kSmemBytes, s>>>(d_rois, n, p->Offset, p->KAdc, reinterpret_cast<const uint4 *>(net->d_wimg),
-                                              w.b1, w.b2, w.b3, start, net->d_err);
+                                              w.b1, w.b2, w.b3, start, cls, class_threshold(net), n_dev,
+                                              net->d_err);
     return cudaGetLastError();
 }
 
@@ -867,6 +897,12 @@ int qcs_learned_forward_device(qcs_learned_net *net, const float *d_feat, int n,
 
 int qcs_learned_gradient_device(qcs_learned_net *net, const float *d_feat, const float *d_targets,
                                 const float *d_valid, int n, float *h_loss, void *stream) {
+    return qcs_learned_gradient_counts_device(net, d_feat, d_targets, d_valid, nullptr, n, h_loss, stream);
+}
+
+int qcs_learned_gradient_counts_device(qcs_learned_net *net, const float *d_feat, const float *d_targets,
+                                       const float *d_valid, const float *d_classes, int n, float *h_loss,
+                                       void *stream) {
     if (!net || !d_feat || !d_targets || !d_valid) return fail(QCS_ERR_ARG, "null argument");
     if (n <= 0 || n > net->batch) return fail(QCS_ERR_CAPACITY, "gradient batch must be 1..batch rows");
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : net->stream;
@@ -874,7 +910,8 @@ int qcs_learned_gradient_device(qcs_learned_net *net, const float *d_feat, const
              "copy features");
     QCS_CUDA(forward(net, net->d_x, n, net->d_z1, net->d_a1, net->d_z2, net->d_a2, net->d_y, s), "forward");
     QCS_CUDA(cudaMemsetAsync(net->d_loss, 0, sizeof(float), s), "clear loss");
-    L::mse_kernel<<<blocks(n), 256, 0, s>>>(net->d_y, d_targets, d_valid, n, 1.0f / (float)n, net->d_dy, net->d_loss);
+    L::mse_kernel<<<blocks(n), 256, 0, s>>>(net->d_y, d_targets, d_valid, d_classes, n, 1.0f / (float)n, net->d_dy,
+                                            net->d_loss);
     QCS_CUDA(backward(net, n, s), "backward");
     if (h_loss) {
         QCS_CUDA(cudaMemcpyAsync(h_loss, net->d_loss, sizeof(float), cudaMemcpyDeviceToHost, s), "read loss");
@@ -891,6 +928,13 @@ int qcs_learned_get_grads(qcs_learned_net *net, float *h_grads) {
 
 int qcs_learned_train_device(qcs_learned_net *net, const float *d_feat, const float *d_targets, const float *d_valid,
                              int n, int epochs, float lr, unsigned long long seed, float *h_epoch_loss, void *stream) {
+    return qcs_learned_train_counts_device(net, d_feat, d_targets, d_valid, nullptr, n, epochs, lr, seed, h_epoch_loss,
+                                           stream);
+}
+
+int qcs_learned_train_counts_device(qcs_learned_net *net, const float *d_feat, const float *d_targets,
+                                    const float *d_valid, const float *d_classes, int n, int epochs, float lr,
+                                    unsigned long long seed, float *h_epoch_loss, void *stream) {
     if (!net || !d_feat || !d_targets || !d_valid) return fail(QCS_ERR_ARG, "null argument");
     if (n < net->batch) return fail(QCS_ERR_ARG, "fewer training rows than one batch");
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : net->stream;
@@ -900,7 +944,8 @@ int qcs_learned_train_device(qcs_learned_net *net, const float *d_feat, const fl
     int *d_perm = nullptr;
     float *d_vb = nullptr, *d_tb = nullptr;
     cudaError_t e = cudaMalloc((void **)&d_perm, (size_t)n * sizeof(int));
-    if (e == cudaSuccess) e = cudaMalloc((void **)&d_vb, (size_t)B * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&d_vb, (size_t)B * 2 * sizeof(float));  // valid | classes
+    float *d_cb = d_classes ? d_vb + B : nullptr;
     if (e == cudaSuccess) e = cudaMalloc((void **)&d_tb, (size_t)B * L::kOutUsed * sizeof(float));
     unsigned long long state = seed ? seed : 0x2545F4914F6CDD1Dull;
     const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
@@ -914,10 +959,12 @@ int qcs_learned_train_device(qcs_learned_net *net, const float *d_feat, const fl
             L::gather_rows_kernel<<<blocks((long long)B * L::kOutUsed), 256, 0, s>>>(d_targets, idx, B, L::kOutUsed,
                                                                                    d_tb);
             L::gather_rows_kernel<<<blocks(B), 256, 0, s>>>(d_valid, idx, B, 1, d_vb);
+            if (d_cb) L::gather_rows_kernel<<<blocks(B), 256, 0, s>>>(d_classes, idx, B, 1, d_cb);
             e = forward(net, net->d_x, B, net->d_z1, net->d_a1, net->d_z2, net->d_a2, net->d_y, s);
             if (e != cudaSuccess) break;
             // per-batch mean loss and its gradient; the loss accumulates over the epoch
-            L::mse_kernel<<<blocks(B), 256, 0, s>>>(net->d_y, d_tb, d_vb, B, 1.0f / (float)B, net->d_dy, net->d_loss);
+            L::mse_kernel<<<blocks(B), 256, 0, s>>>(net->d_y, d_tb, d_vb, d_cb, B, 1.0f / (float)B, net->d_dy,
+                                                    net->d_loss);
             e = backward(net, B, s);
             if (e != cudaSuccess) break;
             net->step++;
@@ -949,7 +996,7 @@ int qcs_learned_start_device(qcs_learned_net *net, const qcs_loc_para *p, const 
     if (n <= 0) return QCS_OK;
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : net->stream;
     if (net->use_tc) {
-        QCS_CUDA(fused_start_points(net, p, d_rois, n, d_start, s), "fused start points");
+        QCS_CUDA(fused_start_points(net, p, d_rois, n, nullptr, d_start, nullptr, s), "fused start points");
         return QCS_OK;
     }
     float *feat = d_work, *scale = feat + (size_t)n * L::kIn, *y = scale + 2 * (size_t)n;
@@ -957,10 +1004,31 @@ int qcs_learned_start_device(qcs_learned_net *net, const qcs_loc_para *p, const 
     if (st) return st;
     st = qcs_learned_forward_device(net, feat, n, y, s);
     if (st) return st;
-    L::start_kernel<<<blocks(n), 256, 0, s>>>(y, scale, n, d_start);
+    L::start_kernel<<<blocks(n), 256, 0, s>>>(y, scale, n, d_start, nullptr, 0.0f);
     QCS_CUDA(cudaGetLastError(), "start points");
     return QCS_OK;
 }
+
+int qcs_learned_classes_device(qcs_learned_net *net, const qcs_loc_para *p, const uint16_t *d_rois, int n,
+                               float *d_start, uint8_t *d_classes, void *stream) {
+    if (!net || !p || !d_start || !d_classes) return fail(QCS_ERR_ARG, "null argument");
+    if (p->ROISize != L::kR || p->LocType != QCS_LOCTYPE_GS2D)
+        return fail(QCS_ERR_ROISIZE, "learned start points are built for GS2D 7x7 ROIs");
+    if (n <= 0) return QCS_OK;
+    if (!d_rois) return fail(QCS_ERR_ARG, "null ROI pointer");
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : net->stream;
+    QCS_CUDA(L::start_points(net, p, d_rois, n, d_start, s, d_classes), "start points and classes");
+    return QCS_OK;
+}
+
+int qcs_learned_set_count_threshold(qcs_learned_net *net, float th) {
+    if (!net) return fail(QCS_ERR_ARG, "null network");
+    if (!(th >= 0.0f && th <= 1.0f)) return fail(QCS_ERR_ARG, "count threshold must be in [0, 1] (0: no routing)");
+    net->count_th = th;
+    return QCS_OK;
+}
+
+float qcs_learned_count_threshold(const qcs_learned_net *net) { return net ? net->count_th : 0.0f; }
 
 size_t qcs_learned_work_bytes(int n) { return (size_t)(n > 0 ? n : 0) * (L::kIn + 2 + L::kOut) * sizeof(float); }
 
@@ -985,8 +1053,8 @@ int qcs_learned_fused_status(qcs_learned_net *net) {
 // net-owned memory (grown, outside any capture, when n exceeds what the last
 // call needed; not for concurrent calls).
 cudaError_t qcs::learned::start_points(qcs_learned_net *net, const qcs_loc_para *p, const uint16_t *d_rois, int n,
-                                       float *out, cudaStream_t s) {
-    if (net->use_tc) return fused_start_points(net, p, d_rois, n, out, s);
+                                       float *out, cudaStream_t s, uint8_t *cls, const int *n_dev) {
+    if (net->use_tc) return fused_start_points(net, p, d_rois, n, n_dev, out, cls, s);
     const size_t need = (size_t)n * (L::kStart + L::kIn + 2 + 2 * L::kHidden + L::kOut);
     if (need > net->start_cap) {
         cudaFree(net->d_start);
@@ -1002,6 +1070,6 @@ cudaError_t qcs::learned::start_points(qcs_learned_net *net, const qcs_loc_para 
     L::features_kernel<<<blocks(n), 256, 0, s>>>(d_rois, n, p->Offset, p->KAdc, feat, scale);
     cudaError_t e = forward(net, feat, n, h1, h1, h2, h2, y, s);
     if (e != cudaSuccess) return e;
-    L::start_kernel<<<blocks(n), 256, 0, s>>>(y, scale, n, out);
+    L::start_kernel<<<blocks(n), 256, 0, s>>>(y, scale, n, out, cls, class_threshold(net));
     return cudaGetLastError();
 }

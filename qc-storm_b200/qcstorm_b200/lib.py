@@ -114,6 +114,21 @@ _SIGS = {
     "qcs_extract_device_roi_num": (C.c_void_p, [C.c_void_p]),
     "qcs_extract_frame_range": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "qcs_extract_dropped_num": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "qcs_learned_gradient_counts_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                     C.c_int, C.POINTER(C.c_float), C.c_void_p]),
+    "qcs_learned_train_counts_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                  C.c_int, C.c_int, C.c_float, C.c_ulonglong, C.c_void_p,
+                                                  C.c_void_p]),
+    "qcs_loc_count_labels_device": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "qcs_learned_set_count_threshold": (C.c_int, [C.c_void_p, C.c_float]),
+    "qcs_learned_localize_device_n": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(LocPara),
+                                                C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_void_p]),
+    "qcs_learned_count_threshold": (C.c_float, [C.c_void_p]),
+    "qcs_learned_classes_device": (C.c_int, [C.c_void_p, C.POINTER(LocPara), C.c_void_p, C.c_int, C.c_void_p,
+                                             C.c_void_p, C.c_void_p]),
+    "qcs_fit_from_start_classes_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(LocPara), C.c_int,
+                                                    C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_float,
+                                                    C.c_void_p]),
 }
 
 
@@ -459,20 +474,39 @@ class LearnedNet:
                                                   C.c_void_p(out.data_ptr()), C.c_void_p(stream) if stream else None))
         return out
 
-    def gradient(self, feat, tgt, valid, stream=0):
+    def gradient(self, feat, tgt, valid, stream=0, classes=None):
+        """Loss and gradient of one batch; classes: emitter-count labels (float, -1 = none) or None."""
         loss = C.c_float(0)
-        check(self.lib.qcs_learned_gradient_device(self.h, C.c_void_p(feat.data_ptr()), C.c_void_p(tgt.data_ptr()),
-                                                   C.c_void_p(valid.data_ptr()), int(feat.shape[0]), C.byref(loss),
-                                                   C.c_void_p(stream) if stream else None))
+        check(self.lib.qcs_learned_gradient_counts_device(
+            self.h, C.c_void_p(feat.data_ptr()), C.c_void_p(tgt.data_ptr()), C.c_void_p(valid.data_ptr()),
+            C.c_void_p(classes.data_ptr()) if classes is not None else None, int(feat.shape[0]), C.byref(loss),
+            C.c_void_p(stream) if stream else None))
         return loss.value
 
-    def train(self, feat, tgt, valid, epochs, lr=1e-3, seed=7, stream=0):
+    def train(self, feat, tgt, valid, epochs, lr=1e-3, seed=7, stream=0, classes=None):
         losses = np.zeros(epochs, np.float32)
-        check(self.lib.qcs_learned_train_device(self.h, C.c_void_p(feat.data_ptr()), C.c_void_p(tgt.data_ptr()),
-                                                C.c_void_p(valid.data_ptr()), int(feat.shape[0]), int(epochs),
-                                                C.c_float(lr), int(seed), C.c_void_p(losses.ctypes.data),
-                                                C.c_void_p(stream) if stream else None))
+        check(self.lib.qcs_learned_train_counts_device(
+            self.h, C.c_void_p(feat.data_ptr()), C.c_void_p(tgt.data_ptr()), C.c_void_p(valid.data_ptr()),
+            C.c_void_p(classes.data_ptr()) if classes is not None else None, int(feat.shape[0]), int(epochs),
+            C.c_float(lr), int(seed), C.c_void_p(losses.ctypes.data), C.c_void_p(stream) if stream else None))
         return losses
+
+    def set_count_threshold(self, th):
+        """Emitter-count routing threshold (0: route by the WLE classes alone)."""
+        check(self.lib.qcs_learned_set_count_threshold(self.h, C.c_float(th)))
+
+    def count_threshold(self):
+        return float(self.lib.qcs_learned_count_threshold(self.h))
+
+    def classes(self, para, d_rois, n, stream=0):
+        """Start points (n x 5) and emitter-count classes (n, uint8) of n device records."""
+        import torch
+        st = torch.empty((n, 5), dtype=torch.float32, device="cuda")
+        cls = torch.empty((n,), dtype=torch.uint8, device="cuda")
+        check(self.lib.qcs_learned_classes_device(self.h, C.byref(para), C.c_void_p(d_rois), int(n),
+                                                  C.c_void_p(st.data_ptr()), C.c_void_p(cls.data_ptr()),
+                                                  C.c_void_p(stream) if stream else None))
+        return st, cls
 
     def start(self, para, d_rois, n, stream=0):
         import torch
@@ -492,6 +526,14 @@ class LearnedNet:
                                                    C.c_float(dev_th),
                                                    C.c_void_p(stream) if stream else None))
 
+    def localize_n(self, ctx, d_rois, d_wle, d_n, max_n, iters=2, dev_th=0.0, para=None, stream=0, bisections=0):
+        """qcs_learned_localize_device_n: record count on the device (multi-emitter fitting)."""
+        para = para or ctx.para
+        check(self.lib.qcs_learned_localize_device_n(ctx.h, self.h, C.c_void_p(d_rois), C.c_void_p(d_wle),
+                                                     C.byref(para), C.c_void_p(d_n), int(max_n), int(iters),
+                                                     int(bisections), C.c_float(dev_th),
+                                                     C.c_void_p(stream) if stream else None))
+
     def set_fused(self, fused=True):
         check(self.lib.qcs_learned_set_inference(self.h, int(bool(fused))))
 
@@ -504,13 +546,25 @@ class LearnedNet:
         return k.value
 
 
-def fit_from_start(ctx, d_rois, n, d_start, d_wle=0, iters=3, dev_th=0.0, para=None, stream=0, bisections=0):
-    """qcs_fit_from_start_device: GS2D 7x7 fits from given start points; rows stay in the context."""
+def fit_from_start(ctx, d_rois, n, d_start, d_wle=0, iters=3, dev_th=0.0, para=None, stream=0, bisections=0,
+                   d_classes=0):
+    """qcs_fit_from_start_classes_device: GS2D 7x7 fits from given start points (and, with
+    multi-emitter fitting on, optional emitter-count classes); rows stay in the context."""
     para = para or ctx.para
-    check(load().qcs_fit_from_start_device(ctx.h, C.c_void_p(d_rois), C.c_void_p(d_wle) if d_wle else None,
-                                           C.byref(para), int(n), C.c_void_p(d_start), int(iters), int(bisections),
-                                           C.c_float(dev_th),
-                                           C.c_void_p(stream) if stream else None))
+    check(load().qcs_fit_from_start_classes_device(ctx.h, C.c_void_p(d_rois), C.c_void_p(d_wle) if d_wle else None,
+                                                   C.byref(para), int(n), C.c_void_p(d_start),
+                                                   C.c_void_p(d_classes) if d_classes else None, int(iters),
+                                                   int(bisections), C.c_float(dev_th),
+                                                   C.c_void_p(stream) if stream else None))
+
+
+def count_labels(ctx, n, stream=0):
+    """Emitter-count labels (float, n) of the last multi-emitter call's records on ctx."""
+    import torch
+    out = torch.empty((n,), dtype=torch.float32, device="cuda")
+    check(load().qcs_loc_count_labels_device(ctx.h, int(n), C.c_void_p(out.data_ptr()),
+                                             C.c_void_p(stream) if stream else None))
+    return out
 
 
 class RenderContext:
