@@ -345,27 +345,38 @@ int qcs_crlb_device(const qcs_loc_para *p, float *d_loc, int n, void *stream);
 
 /* ---- learned start points (no counterpart in the reference) ------------- */
 /*
- * A small network (64 features -> 128 -> 128 -> 8, ReLU, BF16 tensor-core
- * GEMMs with FP32 accumulation) predicts each GS2D 7x7 ROI's start point
- * (x, y, sigma, peak photons, background) for the BFGS fit and, from three
- * logits, its emitter-count class (0: one emitter; 1: the stage of the
- * two-emitter fit; 2: the stage of the three-emitter fit), trained on the
- * GPU by these entry points on ROIs labelled by converged plain fits and by
- * the plain multi-emitter cascade's outcome.
- * Parameters: qcs_learned_param_count() floats (W1 64x128, b1, W2 128x128,
- * b2, W3 128x8, b3, row-major [in][out]).
+ * A small network (K features -> 128 -> 128 -> 8, ReLU, BF16 tensor-core
+ * GEMMs with FP32 accumulation; K = 64 for 7x7 ROIs, 128 for 9x9 and 11x11)
+ * predicts each ROI's start point for the BFGS fit (GS2D: x, y, sigma, peak
+ * photons, background; AS3D: x, y, sigma_x, sigma_y, peak photons,
+ * background) and, for GS2D, from three logits its emitter-count class (0:
+ * one emitter; 1: the stage of the two-emitter fit; 2: the stage of the
+ * three-emitter fit), trained on the GPU by these entry points on ROIs
+ * labelled by converged plain fits and by the plain multi-emitter cascade's
+ * outcome.  One network per localization type and ROI size.
+ * Parameters: W1 Kx128, b1, W2 128x128, b2, W3 128x8, b3, row-major [in][out]
+ * (qcs_learned_shape gives the count).
  */
 typedef struct qcs_learned_net qcs_learned_net;
+/* Parameter count of the GS2D 7x7 network (K = 64). */
 int qcs_learned_param_count(void);
-/* batch: training batch size and inference chunk (<= 0: 4096); seed of the initial weights. */
+/* A network for loc_type (QCS_LOCTYPE_GS2D or QCS_LOCTYPE_AS3D) and ROISize 7,
+ * 9 or 11 (else QCS_ERR_ROISIZE); batch: training batch size and inference
+ * chunk (<= 0: 4096); seed of the initial weights. */
+int qcs_learned_create_for(int loc_type, int roi_size, int batch, unsigned long long seed, qcs_learned_net **out);
+/* qcs_learned_create_for(QCS_LOCTYPE_GS2D, 7, batch, seed, out). */
 int qcs_learned_create(int batch, unsigned long long seed, qcs_learned_net **out);
+/* The network's localization type, ROI size and parameter count (any may be NULL). */
+int qcs_learned_shape(const qcs_learned_net *net, int *loc_type, int *roi_size, int *params);
 int qcs_learned_destroy(qcs_learned_net *net);
 int qcs_learned_get_params(qcs_learned_net *net, float *h_params);
 int qcs_learned_set_params(qcs_learned_net *net, const float *h_params);
-/* Features (n x 64) and per-record (min, range) of n GS2D 7x7 device records. */
+/* Features (n x K: 64 for 7x7, 128 for 9x9 and 11x11) and per-record (min,
+ * range) of n device records of p->ROISize (GS2D or AS3D). */
 int qcs_learned_features_device(const qcs_loc_para *p, const uint16_t *d_rois, int n, float *d_feat, float *d_scale,
                                 void *stream);
-/* Training targets (n x 5) and validity (n) from plain-fit rows of the same records. */
+/* Training targets (n x 5 for GS2D, n x 6 for AS3D) and validity (n) from
+ * plain-fit rows of the same records. */
 int qcs_learned_targets_device(const qcs_loc_para *p, const uint16_t *d_rois, const float *d_rows,
                                const float *d_scale, int n, float *d_targets, float *d_valid, void *stream);
 /* Network outputs (n x 8) of n feature rows. */
@@ -404,18 +415,22 @@ float qcs_learned_count_threshold(const qcs_learned_net *net);
  * of n device records. */
 int qcs_learned_classes_device(qcs_learned_net *net, const qcs_loc_para *p, const uint16_t *d_rois, int n,
                                float *d_start, uint8_t *d_classes, void *stream);
-/* Start points (n x 5: peak e-, x, y, sigma, background e-) of n device records;
- * d_work holds qcs_learned_work_bytes(n) bytes (unused by the fused path). */
+/* Start points of n device records (GS2D n x 5: peak e-, x, y, sigma,
+ * background e-; AS3D n x 6: peak e-, x, y, sigma_x, sigma_y, background
+ * e-); d_work holds qcs_learned_work_bytes(n) bytes (unused by the fused
+ * path). */
 int qcs_learned_start_device(qcs_learned_net *net, const qcs_loc_para *p, const uint16_t *d_rois, int n,
                              float *d_start, float *d_work, void *stream);
 size_t qcs_learned_work_bytes(int n);
-/* GS2D 7x7 single-emitter fits from given start points d_start (n x 5: peak
- * e-, x, y in ROI pixels, sigma, background e-) with the plain fit's weighted
- * loss and accept rules, `iters` BFGS iterations of `bisections` line-search
- * steps each (<= 0: the reference's 11; schedules: 2..5 or 8 iterations with
- * 11 steps, 2 or 3 with 4, 6 or 8) and the loss's analytic gradient; fits that
- * are not accepted or whose Poisson deviance exceeds dev_th (<= 0: 100) are
- * refitted by the plain kernel; then CRLB.  Rows in the context (n).  With
+/* Single-emitter fits (GS2D or AS3D, ROISize 7, 9 or 11) from given start
+ * points d_start (GS2D n x 5: peak e-, x, y in ROI pixels, sigma, background
+ * e-; AS3D n x 6: peak e-, x, y, sigma_x, sigma_y, background e-) with the
+ * plain fit's weighted loss and accept rules, `iters` BFGS iterations of
+ * `bisections` line-search steps each (<= 0: the reference's 11; schedules:
+ * 2..4 iterations of 6 steps or 3 of 11; GS2D 7x7 also 2..5 or 8 of 11 and 2
+ * or 3 of 4 or 8) and the loss's analytic gradient; fits that are not
+ * accepted or whose Poisson deviance exceeds dev_th (<= 0: 100) are refitted
+ * by the plain kernel; then CRLB.  Rows in the context (n).  With
  * p->MultiEmitterFitEn the single-emitter fit is the first stage of the
  * reference's cascade (bfgs_top.cu:26-204): it runs over the single-emitter
  * queue, a plain refit decides which rejects go on to the two-emitter fit,
@@ -429,16 +444,17 @@ int qcs_fit_from_start_device(qcs_loc_data *c, const uint16_t *d_rois, const flo
 int qcs_fit_from_start_classes_device(qcs_loc_data *c, const uint16_t *d_rois, const float *d_wle,
                                       const qcs_loc_para *p, int n, const float *d_start, const uint8_t *d_classes,
                                       int iters, int bisections, float dev_th, void *stream);
-/* GS2D 7x7 localization from learned start points with the schedule of
- * qcs_fit_from_start_device, and, with multi-emitter fitting on and a count
- * threshold set, the network's emitter-count classes.  Rows in the context
- * like qcs_loc_localize_device. */
+/* Localization from learned start points with the schedule of
+ * qcs_fit_from_start_device (the network's shape must be the call's:
+ * QCS_ERR_ROISIZE otherwise), and, with multi-emitter fitting on (GS2D) and a
+ * count threshold set, the network's emitter-count classes.  Rows in the
+ * context like qcs_loc_localize_device. */
 int qcs_learned_localize_device(qcs_loc_data *c, qcs_learned_net *net, const uint16_t *d_rois, const float *d_wle,
                                 const qcs_loc_para *p, int n, int iters, int bisections, float dev_th,
                                 void *stream);
 /* qcs_learned_localize_device with the record count in device memory (*d_n,
  * at most max_n; e.g. qcs_extract_device_roi_num after extraction), like
- * qcs_loc_localize_device_n; GS2D 7x7 with multi-emitter fitting on, d_wle
+ * qcs_loc_localize_device_n; GS2D with multi-emitter fitting on, d_wle
  * required.  The fused inference reads the count on the device; the
  * layer-by-layer inference computes all max_n records. */
 int qcs_learned_localize_device_n(qcs_loc_data *c, qcs_learned_net *net, const uint16_t *d_rois, const float *d_wle,

@@ -17,8 +17,21 @@ WHOLE = R * (R + 1)
 HALF = R // 2
 CENTRE = R / 2.0
 SIGMA0 = 1.3
-N_IN, N_HID, N_OUT, N_USED = 64, 128, 8, 5
-TARGET_WEIGHT = np.array([4.0, 4.0, 1.0, 1.0, 1.0])
+N_IN, N_HID, N_OUT, N_USED = 64, 128, 8, 5   # the GS2D 7x7 network
+TARGET_WEIGHT = np.array([4.0, 4.0, 1.0, 1.0, 1.0, 1.0])  # GS2D uses the first 5, AS3D all 6
+
+
+def in_width(r):
+    """Input width of the network for r x r ROIs (r*r pixels + 2 scale features, padded)."""
+    return 64 if r * r + 2 <= 64 else 128
+
+
+def used_outputs(loc_type):
+    return 6 if loc_type == 1 else 5
+
+
+def param_count(n_in):
+    return n_in * N_HID + N_HID + N_HID * N_HID + N_HID + N_HID * N_OUT + N_OUT
 COUNT0, CLASSES, COUNT_WEIGHT = 5, 3, 0.5  # outputs 5..7: emitter-count logits
 N_PARAMS = N_IN * N_HID + N_HID + N_HID * N_HID + N_HID + N_HID * N_OUT + N_OUT
 
@@ -33,37 +46,44 @@ def bf16(a):
 
 def split_params(p):
     p = np.asarray(p, np.float64)
+    n_in = (p.size - param_count(0)) // N_HID
     o = 0
     out = []
-    for shape in ((N_IN, N_HID), (N_HID,), (N_HID, N_HID), (N_HID,), (N_HID, N_OUT), (N_OUT,)):
+    for shape in ((n_in, N_HID), (N_HID,), (N_HID, N_HID), (N_HID,), (N_HID, N_OUT), (N_OUT,)):
         size = int(np.prod(shape))
         out.append(p[o:o + size].reshape(shape))
         o += size
     return out
 
 
-def features(rois, offset, kadc):
-    e = np.maximum((rois[:, :PIX].astype(np.float32) - np.float32(offset)) * np.float32(kadc), np.float32(1.0))
+def features(rois, offset, kadc, r=R):
+    pix = r * r
+    e = np.maximum((rois[:, :pix].astype(np.float32) - np.float32(offset)) * np.float32(kadc), np.float32(1.0))
     lo = e.min(axis=1)
     rng = np.maximum(e.max(axis=1) - lo, np.float32(1.0))
-    f = np.zeros((rois.shape[0], N_IN), np.float32)
-    f[:, :PIX] = (e - lo[:, None]) * (np.float32(1.0) / rng)[:, None]
-    f[:, PIX] = np.log(rng) * np.float32(0.125)
-    f[:, PIX + 1] = np.log(lo) * np.float32(0.125)
+    f = np.zeros((rois.shape[0], in_width(r)), np.float32)
+    f[:, :pix] = (e - lo[:, None]) * (np.float32(1.0) / rng)[:, None]
+    f[:, pix] = np.log(rng) * np.float32(0.125)
+    f[:, pix + 1] = np.log(lo) * np.float32(0.125)
     return f, np.stack([lo, rng], axis=1)
 
 
-def targets(rois, rows, scale, qe):
+def targets(rois, rows, scale, qe, r=R, loc_type=0):
+    """GS2D: dx, dy, sigma - 1.3, log(peak / range), (bkg - min) / range; AS3D
+    adds sigma_y - 1.3 (the row's sigma_x, sigma_y in columns 4, 5)."""
+    pix = r * r
     lo, rng = scale[:, 0], scale[:, 1]
     ok = (rows[:, 0] > 0) & (rows[:, 4] > 0)
-    t = np.zeros((rows.shape[0], N_USED), np.float32)
-    hx = rois[:, PIX].astype(np.float32)
-    hy = rois[:, PIX + 1].astype(np.float32)
-    t[:, 0] = rows[:, 1] + HALF - hx - CENTRE
-    t[:, 1] = rows[:, 2] + HALF - hy - CENTRE
+    t = np.zeros((rows.shape[0], used_outputs(loc_type)), np.float32)
+    hx = rois[:, pix].astype(np.float32)
+    hy = rois[:, pix + 1].astype(np.float32)
+    t[:, 0] = rows[:, 1] + r // 2 - hx - r / 2.0
+    t[:, 1] = rows[:, 2] + r // 2 - hy - r / 2.0
     t[:, 2] = rows[:, 4] - SIGMA0
     t[:, 3] = np.log(np.maximum(rows[:, 0] * qe, 1e-3) / rng)
     t[:, 4] = (rows[:, 7] * qe - lo) / rng
+    if loc_type == 1:
+        t[:, 5] = rows[:, 5] - SIGMA0
     t[~ok] = 0
     return t, ok.astype(np.float32)
 
@@ -95,10 +115,12 @@ def loss_and_grad(params, x, t, valid, classes=None):
     W1, b1, W2, b2, W3, b3 = split_params(params)
     y, (x, z1, a1, z2, a2) = forward(params, x)
     n = x.shape[0]
-    e = y[:, :N_USED] - t
-    loss = float(np.sum(TARGET_WEIGHT * e * e * valid[:, None]) / n)
+    nu = t.shape[1]
+    e = y[:, :nu] - t
+    tw = TARGET_WEIGHT[:nu]
+    loss = float(np.sum(tw * e * e * valid[:, None]) / n)
     dy = np.zeros_like(y)
-    dy[:, :N_USED] = 2.0 * TARGET_WEIGHT * e * valid[:, None] / n
+    dy[:, :nu] = 2.0 * tw * e * valid[:, None] / n
     if classes is not None:
         c = np.asarray(classes).astype(np.int64)
         lab = c >= 0

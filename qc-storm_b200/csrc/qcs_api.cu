@@ -63,7 +63,7 @@ struct qcs_loc_data {
     cudaStream_t side = nullptr;  // high-priority stream for work overlapped with the main stream
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaEvent_t ev_done = nullptr;  // end of the last asynchronous host call
-    float *d_start = nullptr;       // learned start points, capacity x 5 (one block with the three below)
+    float *d_start = nullptr;       // learned start points, capacity x 6 (one block with the three below)
     int *q_refit = nullptr;         // learned multi-emitter path: records to refit plainly
     uint8_t *d_refit = nullptr;     //   their per-record flags
     uint8_t *d_cls = nullptr;       //   emitter-count class per record
@@ -177,7 +177,7 @@ int qcs_loc_init_capacity(const qcs_loc_para *p, int capacity, qcs_loc_data **ou
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
     if (e == cudaSuccess) e = qcs::wle_sorter_create(capacity, c->d_wle_scratch, &c->wle_sorter);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_done, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = A((void **)&c->d_start, cap * (5 * sizeof(float) + sizeof(int) + 2));
+    if (e == cudaSuccess) e = A((void **)&c->d_start, cap * (6 * sizeof(float) + sizeof(int) + 2));
     if (e != cudaSuccess) {
         qcs_loc_deinit(c);
         return fail(e == cudaErrorMemoryAllocation ? QCS_ERR_NOMEM : QCS_ERR_CUDA, "qcs_loc_init", e);
@@ -192,7 +192,7 @@ int qcs_loc_init_capacity(const qcs_loc_para *p, int capacity, qcs_loc_data **ou
     c->st.extra2 = reinterpret_cast<float *>(s); s += a_row;
     c->st.extra3 = reinterpret_cast<float *>(s); s += a_row;
     c->st.counters = reinterpret_cast<int *>(s);
-    c->q_refit = reinterpret_cast<int *>(c->d_start + cap * 5);
+    c->q_refit = reinterpret_cast<int *>(c->d_start + cap * 6);
     c->d_refit = reinterpret_cast<uint8_t *>(c->q_refit + cap);
     c->d_cls = c->d_refit + cap;
     *out = c;
@@ -271,11 +271,16 @@ __global__ void learned_counters_kernel(qcs::CascadeState st, int n) {
     st.counters[qcs::kCntValid] = n;
 }
 
-// BFGS schedules the learned-start fit is compiled for
-bool learned_schedule(int iters, int bisections) {
-    return (bisections == 11 && ((iters >= 2 && iters <= 5) || iters == 8)) ||
-           ((iters == 2 || iters == 3) && (bisections == 4 || bisections == 6 || bisections == 8));
+// fit kind of a learned-start call; -1 when the shape has no learned path
+int learned_kind(const qcs_loc_para *p) {
+    if (p->ROISize != 7 && p->ROISize != 9 && p->ROISize != 11) return -1;
+    if (p->LocType == QCS_LOCTYPE_GS2D) return qcs::kGS2D;
+    if (p->LocType == QCS_LOCTYPE_AS3D && !p->MultiEmitterFitEn) return qcs::kAS3D;
+    return -1;
 }
+const char *kLearnedShapes = "start-point fits: GS2D or AS3D, ROISize 7, 9 or 11 (multi-emitter fitting: GS2D)";
+const char *kLearnedSchedules =
+    "schedule: 2..4 iterations of 6 bisections or 3 of 11 (GS2D 7x7 also 2..5 or 8 of 11, 2 or 3 of 4 or 8)";
 
 // Emitter-count class of each of n records from the cascade state of a plain
 // multi-emitter call: 0 for records the call did not send to the two-emitter
@@ -314,11 +319,13 @@ cudaError_t learned_multi(qcs_loc_data *c, const uint16_t *d_rois, const float *
     if ((e = qcs::cascade_classify(a, c->st)) != cudaSuccess) return e;
     qcs::FitLaunch f = qcs::cascade_single_launch(a, c->st);
     if ((e = cudaMemsetAsync(c->d_refit, 0, (size_t)n, s)) != cudaSuccess) return e;
-    if ((e = qcs::launch_fit_learned(7, iters, bisections, f, d_start, dev_th, c->d_refit)) != cudaSuccess) return e;
+    const int R = p->ROISize;
+    if ((e = qcs::launch_fit_learned(qcs::kGS2D, R, iters, bisections, f, d_start, dev_th, c->d_refit)) != cudaSuccess)
+        return e;
     if ((e = qcs::launch_flag_queue(c->d_refit, n, c->q_refit, c->st.counters + qcs::kCntRefit, s)) != cudaSuccess)
         return e;
     f.q = qcs::Queue{c->q_refit, c->st.counters + qcs::kCntRefit, 0};
-    if ((e = qcs::launch_fit_group(qcs::kGS2D, 7, 8, f)) != cudaSuccess) return e;
+    if ((e = qcs::launch_fit_group(qcs::kGS2D, R, 8, f)) != cudaSuccess) return e;
     return qcs::cascade_tail(a, c->st);
 }
 }  // namespace
@@ -336,13 +343,12 @@ int qcs_fit_from_start_classes_device(qcs_loc_data *c, const uint16_t *d_rois, c
                                       int iters, int bisections, float dev_th, void *stream) {
     int st = check_call(c, p, n);
     if (st) return st;
-    if (p->LocType != QCS_LOCTYPE_GS2D || p->ROISize != 7)
-        return fail(QCS_ERR_ARG, "start-point fits: GS2D 7x7 only");
+    const int kind = learned_kind(p);
+    if (kind < 0) return fail(QCS_ERR_ARG, kLearnedShapes);
     if (d_classes && !p->MultiEmitterFitEn)
         return fail(QCS_ERR_ARG, "emitter-count classes need multi-emitter fitting");
     if (bisections <= 0) bisections = 11;
-    if (!learned_schedule(iters, bisections))
-        return fail(QCS_ERR_ARG, "schedule: iters 2..5 or 8 with 11 bisections, or 2..3 with 4, 6 or 8");
+    if (!qcs::learned_schedule_supported(kind, p->ROISize, iters, bisections)) return fail(QCS_ERR_ARG, kLearnedSchedules);
     if (n == 0) return QCS_OK;
     if (!d_rois || !d_start) return fail(QCS_ERR_ARG, "null pointer");
     if (!(dev_th > 0.0f)) dev_th = 100.0f;
@@ -367,7 +373,8 @@ int qcs_fit_from_start_classes_device(qcs_loc_data *c, const uint16_t *d_rois, c
     f.mo = qcs::MultiOut{nullptr, nullptr};
     f.para = qcs::core_para(*p);
     f.stream = s;
-    QCS_CUDA(qcs::launch_fit_learned(7, iters, bisections, f, d_start, dev_th, c->st.to2e), "start-point fit");
+    QCS_CUDA(qcs::launch_fit_learned(kind, p->ROISize, iters, bisections, f, d_start, dev_th, c->st.to2e),
+             "start-point fit");
     // plain refit of the flagged records
     QCS_CUDA(qcs::launch_flag_queue(c->st.to2e, n, c->st.q_single, c->st.counters + qcs::kCntSingle, s),
              "refit queue");
@@ -378,7 +385,7 @@ int qcs_fit_from_start_classes_device(qcs_loc_data *c, const uint16_t *d_rois, c
     QCS_CUDA(cudaStreamWaitEvent(c->side, c->ev_fork, 0), "fork");
     f.q = qcs::Queue{c->st.q_single, c->st.counters + qcs::kCntSingle, 0};
     f.stream = c->side;
-    QCS_CUDA(qcs::launch_fit_group(qcs::kGS2D, 7, 8, f), "plain refit");
+    QCS_CUDA(qcs::launch_fit_group(kind, p->ROISize, 8, f), "plain refit");
     QCS_CUDA(qcs::launch_crlb(c->d_loc, c->st.counters + qcs::kCntSingle, 0, n, p->LocType, p->ReadNoise_e, p->QE,
                               p->PixelSize, c->side, c->st.q_single, nullptr),
              "refit CRLB");
@@ -397,8 +404,11 @@ int qcs_learned_localize_device(qcs_loc_data *c, qcs_learned_net *net, const uin
     int st = check_call(c, p, n);
     if (st) return st;
     if (!net) return fail(QCS_ERR_ARG, "null network");
-    if (p->LocType != QCS_LOCTYPE_GS2D || p->ROISize != 7)
-        return fail(QCS_ERR_ARG, "learned start points: GS2D 7x7 only");
+    if (learned_kind(p) < 0) return fail(QCS_ERR_ARG, kLearnedShapes);
+    int lt = -1, rs = 0;
+    qcs_learned_shape(net, &lt, &rs, nullptr);
+    if (lt != p->LocType || rs != p->ROISize)
+        return fail(QCS_ERR_ROISIZE, "the network was built for another localization type or ROI size");
     if (n == 0) return QCS_OK;
     if (!d_rois) return fail(QCS_ERR_ARG, "null ROI pointer");
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
@@ -414,12 +424,16 @@ int qcs_learned_localize_device_n(qcs_loc_data *c, qcs_learned_net *net, const u
     int st = check_call(c, p, max_n);
     if (st) return st;
     if (!net) return fail(QCS_ERR_ARG, "null network");
-    if (p->LocType != QCS_LOCTYPE_GS2D || p->ROISize != 7 || !p->MultiEmitterFitEn)
-        return fail(QCS_ERR_ARG, "device-count learned localization: GS2D 7x7 with multi-emitter fitting");
+    if (learned_kind(p) != qcs::kGS2D || !p->MultiEmitterFitEn)
+        return fail(QCS_ERR_ARG, "device-count learned localization: GS2D 7/9/11 with multi-emitter fitting");
+    int lt = -1, rs = 0;
+    qcs_learned_shape(net, &lt, &rs, nullptr);
+    if (lt != p->LocType || rs != p->ROISize)
+        return fail(QCS_ERR_ROISIZE, "the network was built for another localization type or ROI size");
     if (!d_rois || !d_wle || !d_n) return fail(QCS_ERR_ARG, "null pointer");
     if (bisections <= 0) bisections = 11;
-    if (!learned_schedule(iters, bisections))
-        return fail(QCS_ERR_ARG, "schedule: iters 2..5 or 8 with 11 bisections, or 2..3 with 4, 6 or 8");
+    if (!qcs::learned_schedule_supported(qcs::kGS2D, p->ROISize, iters, bisections))
+        return fail(QCS_ERR_ARG, kLearnedSchedules);
     if (!(dev_th > 0.0f)) dev_th = 100.0f;
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
     uint8_t *cls = qcs_learned_count_threshold(net) > 0.0f ? c->d_cls : nullptr;

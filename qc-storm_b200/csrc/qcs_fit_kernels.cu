@@ -17,6 +17,7 @@
 // appends rows in queue order (qcs_cascade.cu), which is deterministic.
 #include <cstdint>
 #include <cuda_runtime.h>
+#include <type_traits>
 
 #include "qcs_device.cuh"
 #include "qcs_fit_math.cuh"
@@ -446,25 +447,29 @@ __global__ void __launch_bounds__(kGroupTPB) fit_single_group_kernel(const uint1
     if (to2e) to2e[CurFluoID] = (!accepted && c.MultiEmitterFitEn && IsFittingValid && (CurSNR > 6.0f)) ? 1 : 0;
 }
 
-// ---------------------------------------------- learned-start GS2D fit ---
-// The GS2D fit of fit_single_kernel started from a given point (peak e-,
-// x, y in ROI pixels, sigma, background e-) instead of the centre / edge-mean
-// pre-estimate, with ITERS BFGS iterations instead of 8 and the analytic
-// gradient (AnalyticEvalGS2D) instead of the central difference.  The same
-// weighted loss, line search, accept rules (the narrower sigma bound with
-// multi-emitter fitting on) and output row, over the records of a queue.
+// ------------------------------------------- learned-start single fits ---
+// The single-emitter fit of fit_single_kernel (GS2D or AS3D) started from a
+// given point (GS2D: peak e-, x, y in ROI pixels, sigma, background e-; AS3D:
+// peak e-, x, y, sigma_x, sigma_y, background e-) instead of the centre /
+// edge-mean pre-estimate, with ITERS BFGS iterations of NB line-search steps
+// instead of the reference's schedule, and the analytic gradient
+// (AnalyticEvalGS2D / AnalyticEvalAS3D) instead of the central difference.
+// The same weighted loss, WLE mask, accept rules (the narrower sigma bound
+// with multi-emitter fitting on) and output row, over the records of a queue.
 // refit[id] = 1 when the fit is not accepted or when its unweighted Poisson
 // deviance 2 sum(mu - n - n ln(mu / n)) exceeds dev_th: those ROIs are
 // refitted by the plain kernel, which also decides whether a rejected one
 // goes on to the two-emitter fit (to2e).
-template <int R, int ITERS, int NB, int DIST = ArithSpec<kGS2D, R>::DIST, int MASK = ArithSpec<kGS2D, R>::MASK>
+template <int KIND, int R, int ITERS, int NB, int DIST = ArithSpec<KIND, R>::DIST,
+          int MASK = ArithSpec<KIND, R>::MASK>
 __global__ void __launch_bounds__(kTPB) fit_learned_kernel(const uint16_t *__restrict__ rois,
                                                            const float *__restrict__ wle,
                                                            const float *__restrict__ start, Queue q,
                                                            float *__restrict__ loc, uint8_t *__restrict__ refit,
                                                            uint8_t *__restrict__ to2e, CorePara c, float dev_th) {
-    typedef SmemLayout<R, kGS2D> L;
-    enum { P = 5, PIX = R * R, WHOLE = R * (R + 1), ROISize_Half = R / 2 };
+    typedef SmemLayout<R, KIND> L;
+    enum { P = KindTraits<KIND>::P, PIX = R * R, WHOLE = R * (R + 1) };
+    typedef typename std::conditional<KIND == kGS2D, AnalyticEvalGS2D<R, DIST>, AnalyticEvalAS3D<R, DIST>>::type Eval;
     extern __shared__ float smem[];
     const int n = queue_len(q);
     const int base = blockIdx.x * kTPB;
@@ -482,71 +487,59 @@ __global__ void __launch_bounds__(kTPB) fit_learned_kernel(const uint16_t *__res
     const int XOffset = hdr[0], YOffset = hdr[1];
     const int CurFrame = hdr[2] + 65536 * hdr[3];
     const float *pw = wle + (size_t)id * QCS_WLE_PARA_NUM;
+    const PixView img{s_img + tid, kTPB};
     const RoiRef roi{s_img + tid, w, kTPB};
 
-    const float XYLBound = R / 2.0f - 1.5f;
-    const float XYUBound = R / 2.0f + 1.5f;
-    const float Simga_Max_Th = c.MultiEmitterFitEn ? R / 2.0f / 2.35f : R / 1.5f / 2.35f;
-    float SigmaL = pw[1], SigmaR = pw[2], SigmaU = pw[3], SigmaD = pw[4];
-    const int MoleculeType = pw[5];
-    SigmaL = fminf(SigmaL, SigmaR);
-    SigmaU = fminf(SigmaU, SigmaD);
-    float WLE_SigmaX = fminf(fminf(SigmaL, SigmaU), R / 2.0f / 2.35f);
-    if (MoleculeType != QCS_MOLECULE_MLEFIT) WLE_SigmaX = fminf(WLE_SigmaX / 1.2f, R / 2.0f / 2.35f);
-    if (c.WLEEn == 0 && MoleculeType != QCS_MOLECULE_MULTIFIT) WLE_SigmaX = R;
-    wle_weights<R, MASK>(w, kTPB, WLE_SigmaX, WLE_SigmaX, MoleculeType);
-
-    const float *st = start + (size_t)id * 5;
     float Ininf[P];
+    const SinglePrep sp = single_prefit<R, KIND>(img, pw, c, Ininf);  // mask widths (start replaced below)
+    wle_weights<R, MASK>(w, kTPB, sp.WLE_SigmaX, sp.WLE_SigmaY, sp.MoleculeType);
+    const float *st = start + (size_t)id * P;
     Ininf[0] = st[0] * rAScalFactor;
     Ininf[1] = st[1];
     Ininf[2] = st[2];
     Ininf[3] = (0.5f / (st[3] * st[3])) * rSScalFactor;
-    Ininf[4] = st[4] * rBScalFactor;
-    bfgs_fit<P, ITERS, AnalyticEvalGS2D<R, DIST>, NB>(AnalyticEvalGS2D<R, DIST>{roi}, Ininf, D, kTPB);
+    if (KIND == kGS2D) {
+        Ininf[4] = st[4] * rBScalFactor;
+    } else {
+        Ininf[4] = (0.5f / (st[4] * st[4])) * rSScalFactor;
+        Ininf[P - 1] = st[5] * rBScalFactor;
+    }
+    bfgs_fit<P, ITERS, Eval, NB>(Eval{roi}, Ininf, D, kTPB);
 
-    const float PeakPhoton = Ininf[0] * QCS_ASCALE / c.QE;
-    const float Background = Ininf[4] * QCS_BSCALE / c.QE;
-    float FittedXPos = Ininf[1], FittedYPos = Ininf[2];
-    float SimgaX = sqrtf(0.5f / (Ininf[3] * QCS_SSCALE));
-    FittedXPos = isnan(FittedXPos) ? -1 : FittedXPos;
-    FittedYPos = isnan(FittedYPos) ? -1 : FittedYPos;
-    SimgaX = isnan(SimgaX) ? -1 : SimgaX;
-    const float CurSNR = sqrtf(c.QE) * PeakPhoton / sqrtf(PeakPhoton + Background);
-    const bool valid = !isnan(Background);
-    const bool accepted = valid && (CurSNR > 4.0f) && (SimgaX <= Simga_Max_Th) && (SimgaX >= 0.6f) &&
-                          (FittedXPos > XYLBound) && (FittedXPos < XYUBound) && (FittedYPos > XYLBound) &&
-                          (FittedYPos < XYUBound);
+    float row[12];
+    bool accepted;
+    float CurSNR;
+    int IsFittingValid;
+    single_finish<R, KIND>(Ininf, c, sp.Simga_Max_Th, XOffset, YOffset, CurFrame, row, accepted, CurSNR,
+                           IsFittingValid);
     // goodness of fit at the final point (unweighted Poisson deviance)
     float dev = 0.0f;
 #pragma unroll 1
     for (int r = 0; r < R; r++)
         for (int col = 0; col < R; col++) {
             const float2 pl = roi.img[(r * R + col) * roi.ld];
-            const float e = single_expo<kGS2D, DIST>(col + 0.5f, r + 0.5f, Ininf);
-            dev += single_term<kGS2D>(e, Ininf, pl.x, pl.y);
+            const float e = single_expo<KIND, DIST>(col + 0.5f, r + 0.5f, Ininf);
+            dev += single_term<KIND>(e, Ininf, pl.x, pl.y);
         }
     dev *= 2.0f;
     refit[id] = (!accepted || !(dev <= dev_th)) ? 1 : 0;
     if (to2e) to2e[id] = 0;  // a kept fit is final; a refit sets the flag again
-    if (accepted) {
-        float row[12];
-        row[0] = PeakPhoton;
-        row[1] = FittedXPos - ROISize_Half + XOffset;
-        row[2] = FittedYPos - ROISize_Half + YOffset;
-        row[3] = 0.0f;
-        row[4] = SimgaX;
-        row[5] = SimgaX;
-        row[6] = PeakPhoton * 2 * 3.141593f * SimgaX * SimgaX;
-        row[7] = Background;
-        row[8] = CurSNR;
-        row[9] = 0.0f;
-        row[10] = 0.0f;
-        row[11] = CurFrame;
+    if (accepted)
         store_row(loc, id, row);
-    } else {
+    else
         zero_row(loc, id);
-    }
+}
+
+template <int KIND, int R, int ITERS, int NB>
+cudaError_t launch_learned(const FitLaunch &a, const float *start, float dev_th, uint8_t *refit) {
+    const size_t smem = SmemLayout<R, KIND>::TOTAL * sizeof(float);
+    auto k = fit_learned_kernel<KIND, R, ITERS, NB>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const int grid = (a.max_count + kTPB - 1) / kTPB;
+    if (grid == 0) return cudaSuccess;
+    k<<<grid, kTPB, smem, a.stream>>>(a.rois, a.wle, start, a.q, a.loc, refit, a.to2e, a.para, dev_th);
+    return cudaGetLastError();
 }
 
 // Ids of the records with a nonzero flag (in no particular order: every
@@ -849,28 +842,58 @@ cudaError_t launch_multi(const FitLaunch &a) {
 
 }  // namespace
 
-cudaError_t launch_fit_learned(int R, int iters, int bisections, const FitLaunch &a, const float *start,
-                               float dev_th, uint8_t *refit) {
-    if (R != 7) return cudaErrorInvalidValue;
-    if (bisections == kBisections) {
-        switch (iters) {
-        case 2: return launch_learned<7, 2, kBisections>(a, start, dev_th, refit);
-        case 3: return launch_learned<7, 3, kBisections>(a, start, dev_th, refit);
-        case 4: return launch_learned<7, 4, kBisections>(a, start, dev_th, refit);
-        case 5: return launch_learned<7, 5, kBisections>(a, start, dev_th, refit);
-        case 8: return launch_learned<7, 8, kBisections>(a, start, dev_th, refit);
-        }
-        return cudaErrorInvalidValue;
-    }
+// Schedules compiled per shape: every shape 2..4 iterations of 6 steps and
+// 3 of 11; GS2D 7x7 (the bench's shape) also 2..5 or 8 iterations of 11
+// steps and 2 or 3 of 4 or 8.
+bool learned_schedule_supported(int kind, int R, int iters, int bisections) {
+    if (kind == kGS2D && R == 7)
+        return (bisections == kBisections && ((iters >= 2 && iters <= 5) || iters == 8)) ||
+               ((iters == 2 || iters == 3) && (bisections == 4 || bisections == 8)) ||
+               (bisections == 6 && iters >= 2 && iters <= 4);
+    if ((kind == kGS2D || kind == kAS3D) && (R == 7 || R == 9 || R == 11))
+        return (bisections == 6 && iters >= 2 && iters <= 4) || (bisections == kBisections && iters == 3);
+    return false;
+}
+
+template <int KIND, int R>
+cudaError_t launch_learned_shape(int iters, int bisections, const FitLaunch &a, const float *start, float dev_th,
+                                 uint8_t *refit) {
 #define QCS_LEARNED(IT, NB) \
-    if (iters == IT && bisections == NB) return launch_learned<7, IT, NB>(a, start, dev_th, refit);
-    QCS_LEARNED(2, 4)
+    if (iters == IT && bisections == NB) return launch_learned<KIND, R, IT, NB>(a, start, dev_th, refit);
     QCS_LEARNED(2, 6)
-    QCS_LEARNED(2, 8)
-    QCS_LEARNED(3, 4)
     QCS_LEARNED(3, 6)
-    QCS_LEARNED(3, 8)
+    QCS_LEARNED(4, 6)
+    QCS_LEARNED(3, kBisections)
+    if constexpr (KIND == kGS2D && R == 7) {
+        QCS_LEARNED(2, kBisections)
+        QCS_LEARNED(4, kBisections)
+        QCS_LEARNED(5, kBisections)
+        QCS_LEARNED(8, kBisections)
+        QCS_LEARNED(2, 4)
+        QCS_LEARNED(2, 8)
+        QCS_LEARNED(3, 4)
+        QCS_LEARNED(3, 8)
+    }
 #undef QCS_LEARNED
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_fit_learned(int kind, int R, int iters, int bisections, const FitLaunch &a, const float *start,
+                               float dev_th, uint8_t *refit) {
+    if (!learned_schedule_supported(kind, R, iters, bisections)) return cudaErrorInvalidValue;
+    if (kind == kGS2D) {
+        switch (R) {
+        case 7: return launch_learned_shape<kGS2D, 7>(iters, bisections, a, start, dev_th, refit);
+        case 9: return launch_learned_shape<kGS2D, 9>(iters, bisections, a, start, dev_th, refit);
+        case 11: return launch_learned_shape<kGS2D, 11>(iters, bisections, a, start, dev_th, refit);
+        }
+    } else if (kind == kAS3D) {
+        switch (R) {
+        case 7: return launch_learned_shape<kAS3D, 7>(iters, bisections, a, start, dev_th, refit);
+        case 9: return launch_learned_shape<kAS3D, 9>(iters, bisections, a, start, dev_th, refit);
+        case 11: return launch_learned_shape<kAS3D, 11>(iters, bisections, a, start, dev_th, refit);
+        }
+    }
     return cudaErrorInvalidValue;
 }
 

@@ -387,6 +387,55 @@ struct AnalyticEvalGS2D {
     }
 };
 
+// The same for AS3D (separate widths): with mu = 128 A e + 64 B,
+// e = exp(-0.1 (Sx dx^2 + Sy dy^2)),
+//   dmu/dA = 128 e, dmu/dX = 128 A e 0.2 Sx dx, dmu/dY = 128 A e 0.2 Sy dy,
+//   dmu/dSx = -128 A e 0.1 dx^2, dmu/dSy = -128 A e 0.1 dy^2, dmu/dB = 64,
+// at the point clamped as the AS3D loss clamps it (every parameter >= 0.01).
+template <int R, int DIST>
+struct AnalyticEvalAS3D {
+    RoiRef roi;
+    __device__ __forceinline__ float loss(float *x) const {
+        return qcs::loss<R, kAS3D, DIST, ArithSpec<kAS3D, R>::SUM2>(roi, x);
+    }
+    __device__ __forceinline__ void gradient(const float *v, float *g) const {
+        float c[6];
+#pragma unroll
+        for (int k = 0; k < 6; k++) c[k] = v[k] < 0.01f ? 0.01f : v[k];
+        const float A128 = c[0] * QCS_ASCALE, B64 = c[5] * QCS_BSCALE;
+        const float Sx = c[3] * QCS_SSCALE, Sy = c[4] * QCS_SSCALE;
+        float gA = 0, gX = 0, gY = 0, gSx = 0, gSy = 0, gB = 0;
+#pragma unroll 1
+        for (int row = 0; row < R; row++) {
+            const float dy = (row + 0.5f) - c[2];
+            const float qy = dy * dy;
+#pragma unroll(R <= kUnrollMaxR ? R : 1)
+            for (int col = 0; col < R; col++) {
+                const float2 pl = roi.img[(row * R + col) * roi.ld];
+                const float w = roi.w[(row * R + col) * roi.ld];
+                const float dx = (col + 0.5f) - c[1];
+                const float qx = dx * dx;
+                const float e = __expf(-__fmaf_rn(qx, Sx, qy * Sy));
+                const float mu = __fmaf_rn(A128, e, B64);
+                const float q = w * (1.0f - __fdividef(pl.x, mu));
+                const float qe = q * e;
+                gA += qe;
+                gX = __fmaf_rn(qe, dx, gX);
+                gY = __fmaf_rn(qe, dy, gY);
+                gSx = __fmaf_rn(qe, qx, gSx);
+                gSy = __fmaf_rn(qe, qy, gSy);
+                gB += q;
+            }
+        }
+        g[0] = QCS_ASCALE * gA;
+        g[1] = A128 * 2.0f * Sx * gX;
+        g[2] = A128 * 2.0f * Sy * gY;
+        g[3] = -A128 * QCS_SSCALE * gSx;
+        g[4] = -A128 * QCS_SSCALE * gSy;
+        g[5] = QCS_BSCALE * gB;
+    }
+};
+
 // Loss and gradient of one single-emitter ROI (GS2D / AS3D) evaluated by a
 // group of G consecutive lanes of a warp, bit for bit equal to ThreadEval:
 //  - loss: the lanes compute the pixel terms k = lane, lane + G, ... (the

@@ -30,12 +30,15 @@ cudaError_t launch_fit(int kind, int R, const FitLaunch &a);
 bool group_fit_supported(int kind, int R);
 cudaError_t launch_fit_group(int kind, int R, int lanes, const FitLaunch &a);
 
-// GS2D fit of the records of a.q (grid from a.max_count) started from
-// start[5 * id] (peak e-, x, y, sigma, background e-) with `iters` BFGS
-// iterations of `bisections` line-search steps (iters 2..5 or 8 with 11
-// steps; iters 2 or 3 with 4, 6 or 8; R = 7); rows into a.loc, refit[id] = 1
-// for fits to redo with the plain kernel, a.to2e[id] = 0 when a.to2e is set.
-cudaError_t launch_fit_learned(int R, int iters, int bisections, const FitLaunch &a, const float *start,
+// Single-emitter fit (kind kGS2D or kAS3D; R = 7, 9, 11) of the records of
+// a.q (grid from a.max_count) started from start[P * id] (GS2D P = 5: peak
+// e-, x, y, sigma, background e-; AS3D P = 6: peak e-, x, y, sigma_x,
+// sigma_y, background e-) with `iters` BFGS iterations of `bisections`
+// line-search steps (learned_schedule_supported); rows into a.loc,
+// refit[id] = 1 for fits to redo with the plain kernel, a.to2e[id] = 0 when
+// a.to2e is set.
+bool learned_schedule_supported(int kind, int R, int iters, int bisections);
+cudaError_t launch_fit_learned(int kind, int R, int iters, int bisections, const FitLaunch &a, const float *start,
                                float dev_th, uint8_t *refit);
 // ids[] = the indices i < n with flags[i] != 0 (any order), *count = their number.
 cudaError_t launch_flag_queue(const uint8_t *flags, int n, int *ids, int *count, cudaStream_t s);

@@ -1,15 +1,17 @@
-// Learned start points for the GS2D 7x7 fit: a small network predicts each
-// ROI's (x, y, sigma, peak photons, background) from its pixels, so that the
-// BFGS fit can start near the optimum and run fewer iterations.  No
-// counterpart in the reference (it starts from the centre / edge-mean
-// pre-estimate, bfgsMLE_GS2D_core.h:522-575).
+// Learned start points for the single-emitter fits (GS2D and AS3D, 7x7, 9x9
+// and 11x11 ROIs): a small network predicts each ROI's optimum from its
+// pixels, so that the BFGS fit can start near it and run fewer iterations.
+// No counterpart in the reference (it starts from the centre / edge-mean
+// pre-estimates, bfgsMLE_GS2D_core.h:522-575, bfgsMLE_AS3D_core.h:548-607).
 //
-// Network (per ROI): 64 features -> 128 (ReLU) -> 128 (ReLU) -> 8 outputs:
-// dx, dy, sigma - 1.3, log(peak / range), (background - min) / range, and
-// three logits of the ROI's emitter-count class (0: one emitter; 1: the
-// two-emitter fit's stage; 2: the three-emitter fit's stage), with which the
-// multi-emitter cascade sends a ROI straight to the stage it would reach.
-// Features: the 49 photoelectron pixels max((adu - offset) * gain, 1) scaled
+// Network (per ROI): 64 (7x7) or 128 (9x9, 11x11) features -> 128 (ReLU) ->
+// 128 (ReLU) -> 8 outputs: GS2D dx, dy, sigma - 1.3, log(peak / range),
+// (background - min) / range, and three logits of the ROI's emitter-count
+// class (0: one emitter; 1: the two-emitter fit's stage; 2: the three-emitter
+// fit's stage), with which the multi-emitter cascade sends a ROI straight to
+// the stage it would reach; AS3D dx, dy, sigma_x - 1.3, log(peak / range),
+// (background - min) / range, sigma_y - 1.3.
+// Features: the R*R photoelectron pixels max((adu - offset) * gain, 1) scaled
 // to [0, 1] by the ROI's min and range, log(range) / 8, log(min) / 8, zeros.
 // Training and inference GEMMs run on the tensor cores in BF16 with FP32
 // accumulation (mma.sync m16n8k16); master weights and Adam moments are FP32.
@@ -29,55 +31,77 @@ namespace learned {
 constexpr int kGemmThreads = 128;  // 4 warps, 64 x 64 block tile, k step 16
 constexpr int kTile = 64;
 
+// One feature of record r (R x R pixels then header words): feature k of
+// in_width(R), given the record's photoelectron min lo, 1 / range inv and the
+// two scale features.  The fused inference kernel builds the same values.
+template <int R>
+__device__ __forceinline__ float feature(const uint16_t *r, int k, float offset, float kadc, float lo, float inv,
+                                         float f_rng, float f_lo) {
+    enum { PIX = R * R };
+    if (k < PIX) return (fmaxf(((float)r[k] - offset) * kadc, 1.0f) - lo) * inv;
+    if (k == PIX) return f_rng;
+    if (k == PIX + 1) return f_lo;
+    return 0.0f;
+}
+
+// photoelectron min and range of a record's R x R pixels
+template <int R>
+__device__ __forceinline__ void record_range(const uint16_t *r, float offset, float kadc, float &lo, float &rng) {
+    float hi = -1e30f;
+    lo = 1e30f;
+#pragma unroll 7
+    for (int k = 0; k < R * R; ++k) {
+        const float e = fmaxf(((float)r[k] - offset) * kadc, 1.0f);
+        lo = fminf(lo, e);
+        hi = fmaxf(hi, e);
+    }
+    rng = fmaxf(hi - lo, 1.0f);
+}
+
 // ---------------------------------------------------------------- features
+template <int R>
 __global__ void features_kernel(const uint16_t *__restrict__ rois, int n, float offset, float kadc,
                                 float *__restrict__ feat, float *__restrict__ scale) {
+    enum { KIN = in_width(R), WHOLE = R * (R + 1) };
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const uint16_t *r = rois + (size_t)i * kWhole;
-    float e[kPix];
-    float lo = 1e30f, hi = -1e30f;
-#pragma unroll
-    for (int k = 0; k < kPix; ++k) {
-        e[k] = fmaxf(((float)r[k] - offset) * kadc, 1.0f);
-        lo = fminf(lo, e[k]);
-        hi = fmaxf(hi, e[k]);
-    }
-    const float rng = fmaxf(hi - lo, 1.0f);
+    const uint16_t *r = rois + (size_t)i * WHOLE;
+    float lo, rng;
+    record_range<R>(r, offset, kadc, lo, rng);
     const float inv = 1.0f / rng;
-    float *f = feat + (size_t)i * kIn;
-#pragma unroll
-    for (int k = 0; k < kPix; ++k) f[k] = (e[k] - lo) * inv;
-    f[kPix] = logf(rng) * 0.125f;
-    f[kPix + 1] = logf(lo) * 0.125f;
-#pragma unroll
-    for (int k = kPix + 2; k < kIn; ++k) f[k] = 0.0f;
+    const float f_rng = logf(rng) * 0.125f, f_lo = logf(lo) * 0.125f;
+    float *f = feat + (size_t)i * KIN;
+    for (int k = 0; k < KIN; ++k) f[k] = feature<R>(r, k, offset, kadc, lo, inv, f_rng, f_lo);
     scale[2 * i] = lo;
     scale[2 * i + 1] = rng;
 }
 
-// Targets from the plain fit rows (12 floats per record, record order);
-// valid[i] = 1 for accepted fits.
+// Targets (used_outputs(LT) per record) from the plain fit rows (12 floats
+// per record, record order); valid[i] = 1 for accepted fits.
+template <int R, int LT>
 __global__ void targets_kernel(const uint16_t *__restrict__ rois, const float *__restrict__ rows,
                                const float *__restrict__ scale, int n, float qe, float *__restrict__ tgt,
                                float *__restrict__ valid) {
+    enum { PIX = R * R, WHOLE = R * (R + 1), HALF = R / 2, NU = used_outputs(LT) };
+    const float centre = R / 2.0f;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float *row = rows + (size_t)i * 12;
-    const uint16_t *h = rois + (size_t)i * kWhole + kPix;
+    const uint16_t *h = rois + (size_t)i * WHOLE + PIX;
     const float lo = scale[2 * i], rng = scale[2 * i + 1];
     const bool ok = row[QCS_POS_PPHO] > 0.0f && row[QCS_POS_SIGX] > 0.0f;
-    float *t = tgt + (size_t)i * kOutUsed;
+    float *t = tgt + (size_t)i * NU;
     if (ok) {
         // ROI coordinates of the fitted centre (inverse of the row's x = fit - R/2 + header x)
-        t[0] = row[QCS_POS_XPOS] + (float)kHalf - (float)h[0] - kCentre;
-        t[1] = row[QCS_POS_YPOS] + (float)kHalf - (float)h[1] - kCentre;
+        t[0] = row[QCS_POS_XPOS] + (float)HALF - (float)h[0] - centre;
+        t[1] = row[QCS_POS_YPOS] + (float)HALF - (float)h[1] - centre;
         t[2] = row[QCS_POS_SIGX] - kSigma0;
         t[3] = logf(fmaxf(row[QCS_POS_PPHO] * qe, 1e-3f) / rng);
         t[4] = (row[QCS_POS_BAKG] * qe - lo) / rng;
+        if (NU > 5) t[5] = row[QCS_POS_SIGY] - kSigma0;
     } else {
 #pragma unroll
-        for (int j = 0; j < kOutUsed; ++j) t[j] = 0.0f;
+        for (int j = 0; j < NU; ++j) t[j] = 0.0f;
     }
     valid[i] = ok ? 1.0f : 0.0f;
 }
@@ -206,11 +230,11 @@ __global__ void colsum_kernel(const float *__restrict__ dZ, int rows, int cols, 
     g[c] = s;
 }
 
-// Masked weighted MSE on the first kOutUsed outputs plus, where cls is set
-// and cls[i] >= 0, kCountWeight x the softmax cross-entropy of the count
-// logits against class cls[i]: loss and dY.
+// Masked weighted MSE on the first nused outputs plus, where cls is set and
+// cls[i] >= 0 (GS2D networks), kCountWeight x the softmax cross-entropy of
+// the count logits against class cls[i]: loss and dY.
 __global__ void mse_kernel(const float *__restrict__ Y, const float *__restrict__ T, const float *__restrict__ valid,
-                           const float *__restrict__ cls, int rows, float inv_count, float *__restrict__ dY,
+                           const float *__restrict__ cls, int rows, int nused, float inv_count, float *__restrict__ dY,
                            float *__restrict__ loss) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= rows) return;
@@ -220,8 +244,8 @@ __global__ void mse_kernel(const float *__restrict__ Y, const float *__restrict_
 #pragma unroll
     for (int j = 0; j < kOut; ++j) {
         float d = 0.0f;
-        if (j < kOutUsed) {
-            const float e = y[j] - T[(size_t)i * kOutUsed + j];
+        if (j < nused) {
+            const float e = y[j] - T[(size_t)i * nused + j];
             d = 2.0f * kTargetWeight[j] * e * v * inv_count;
             l += kTargetWeight[j] * e * e * v;
         }
@@ -261,21 +285,36 @@ __global__ void gather_rows_kernel(const float *__restrict__ src, const int *__r
     dst[i] = src[(size_t)idx[r] * cols + c];
 }
 
-// Predictions -> fit start (photoelectron peak, ROI x, y, sigma, background)
-// and, with cls set, the emitter-count class at threshold th.
+// Network outputs y (bias included) -> the fit's start point st
+// (start_width(LT) floats: peak e-, x, y, sigma(s), background e-), with
+// positions held inside the kind's accept window and widths in range.
+template <int R, int LT>
+__device__ __forceinline__ void start_from_outputs(const float *y, float lo, float rng, float *st) {
+    const float centre = R / 2.0f;
+    const float win = LT == QCS_LOCTYPE_AS3D ? 2.5f : 1.5f;
+    const float smax = LT == QCS_LOCTYPE_AS3D ? 4.0f : 3.0f;
+    st[0] = rng * expf(fminf(fmaxf(y[3], -6.0f), 3.0f));
+    st[1] = centre + fminf(fmaxf(y[0], -win), win);
+    st[2] = centre + fminf(fmaxf(y[1], -win), win);
+    st[3] = fminf(fmaxf(kSigma0 + y[2], 0.6f), smax);
+    if (LT == QCS_LOCTYPE_AS3D) {
+        st[4] = fminf(fmaxf(kSigma0 + y[5], 0.6f), smax);
+        st[5] = fmaxf(lo + rng * y[4], 1.0f);
+    } else {
+        st[4] = fmaxf(lo + rng * y[4], 1.0f);
+    }
+}
+
+// Predictions -> fit start and, with cls set (GS2D), the emitter-count class
+// at threshold th.
+template <int R, int LT>
 __global__ void start_kernel(const float *__restrict__ Y, const float *__restrict__ scale, int n,
                              float *__restrict__ start, uint8_t *__restrict__ cls, float th) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float *y = Y + (size_t)i * kOut;
     if (cls) cls[i] = (uint8_t)count_class(y[kCount0], y[kCount0 + 1], y[kCount0 + 2], th);
-    const float lo = scale[2 * i], rng = scale[2 * i + 1];
-    float *s = start + (size_t)i * kStart;
-    s[0] = rng * expf(fminf(fmaxf(y[3], -6.0f), 3.0f));
-    s[1] = kCentre + fminf(fmaxf(y[0], -1.5f), 1.5f);
-    s[2] = kCentre + fminf(fmaxf(y[1], -1.5f), 1.5f);
-    s[3] = fminf(fmaxf(kSigma0 + y[2], 0.6f), 3.0f);
-    s[4] = fmaxf(lo + rng * y[4], 1.0f);
+    start_from_outputs<R, LT>(y, scale[2 * i], scale[2 * i + 1], start + (size_t)i * start_width(LT));
 }
 
 // ------------------------------------------- fused tcgen05 inference ---
@@ -291,25 +330,34 @@ namespace tc {
 
 constexpr int kM = 128;        // ROIs per tile (the MMA's M)
 constexpr int kN3 = 16;        // layer-3 N padded to the M = 128 minimum
-constexpr int kW1 = kHidden * kIn, kW2 = kHidden * kHidden, kW3 = kN3 * kHidden;  // bf16 elements
-constexpr int kRecBytes = kM * kWhole * 2;  // one tile of records, 14,336 B
-// Shared memory: the weight images, the layer-2 operand (the layer-1 operand
-// lives in its first half: layer 1's MMA has finished reading it before the
-// layer-1 epilogue writes layer 2's operand), one tile of records, barriers.
-constexpr int kOffW1 = 0;
-constexpr int kOffW2 = kOffW1 + kW1 * 2;
-constexpr int kOffW3 = kOffW2 + kW2 * 2;
-constexpr int kOffA2 = kOffW3 + kW3 * 2;
-constexpr int kOffA1 = kOffA2;
-constexpr int kOffRec = kOffA2 + kM * kHidden * 2;
-constexpr int kOffBar = kOffRec + kRecBytes;  // MMA barrier, record barrier, TMEM address
 constexpr int kAlign = 128;
-constexpr int kSmemBytes = kOffBar + 32 + kAlign;  // + alignment slack
 constexpr int kTmemCols = 256;                     // layer 1 / 3 at column 0, layer 2 at column 128
-constexpr int kWeightVec = (kW1 + kW2 + kW3) * 2 / 16;
 constexpr int kWaitPolls = 1 << 22;                // bound of every barrier wait
-static_assert(kOffA1 + kM * kIn * 2 <= kOffRec, "layer-1 operand inside the layer-2 buffer");
-static_assert(kRecBytes % 16 == 0 && kOffRec % 16 == 0, "bulk copies move 16-byte multiples");
+
+// Shared memory of one CTA for R x R records and KIN features: the weight
+// images, the layer-2 operand (the layer-1 operand lives in its first part:
+// layer 1's MMA has finished reading it before the layer-1 epilogue writes
+// layer 2's operand), one tile of records, barriers.
+template <int R>
+struct Layout {
+    enum : int {
+        KIN = in_width(R),
+        WHOLE = R * (R + 1),
+        W1 = kHidden * KIN, W2 = kHidden * kHidden, W3 = kN3 * kHidden,  // bf16 elements
+        REC_BYTES = kM * WHOLE * 2,                                         // one tile of records
+        OFF_W1 = 0,
+        OFF_W2 = OFF_W1 + W1 * 2,
+        OFF_W3 = OFF_W2 + W2 * 2,
+        OFF_A2 = OFF_W3 + W3 * 2,
+        OFF_A1 = OFF_A2,
+        OFF_REC = OFF_A2 + kM * kHidden * 2,
+        OFF_BAR = OFF_REC + REC_BYTES,  // MMA barrier, record barrier, TMEM address
+        SMEM = OFF_BAR + 32 + kAlign,   // + alignment slack
+        WEIGHT_VEC = (W1 + W2 + W3) * 2 / 16,
+    };
+    static_assert(OFF_A1 + kM * KIN * 2 <= OFF_REC, "layer-1 operand inside the layer-2 buffer");
+    static_assert(REC_BYTES % 16 == 0 && OFF_REC % 16 == 0, "a full tile is a whole number of 16-byte blocks");
+};
 
 // element (n, k) of an N x K K-major operand image, in bf16 elements
 __host__ __device__ constexpr int img_index(int n, int k, int N) { return ((k >> 3) * N + n) * 8 + (k & 7); }
@@ -404,24 +452,33 @@ __device__ __forceinline__ void epilogue_hidden(uint32_t taddr_row, const float 
 
 __device__ __forceinline__ int tile_rows(int tile, int n) { return min(kM, n - tile * kM); }
 
+// bytes of a tile's records moved by the bulk copy (a multiple of 16; the
+// rest, under 16 bytes of a ragged last tile, is copied by plain loads)
+template <int R>
+__device__ __forceinline__ uint32_t bulk_bytes(int rows) {
+    return (uint32_t)(rows * R * (R + 1) * 2) & ~15u;
+}
+
 // BULK: records reach shared memory by one bulk copy per tile, issued one
-// tile ahead (d_rois 16-byte aligned); otherwise each thread loads its own
-// record from global memory.
-template <bool BULK>
+// tile ahead (d_rois 16-byte aligned); otherwise each thread reads its own
+// record from global memory.  LT: the start point's kind (GS2D / AS3D).
+template <bool BULK, int R, int LT>
 __global__ void __launch_bounds__(128, 1) mlp_tc_kernel(const uint16_t *__restrict__ rois, int n, float offset,
                                                         float kadc, const uint4 *__restrict__ wimg,
                                                         const float *__restrict__ b1, const float *__restrict__ b2,
                                                         const float *__restrict__ b3, float *__restrict__ start,
                                                         uint8_t *__restrict__ cls, float count_th,
                                                         const int *__restrict__ n_dev, int *__restrict__ err) {
+    typedef Layout<R> L;
+    enum { KIN = L::KIN, WHOLE = L::WHOLE, NST = start_width(LT) };
     extern __shared__ uint8_t smem_raw[];
     if (n_dev) n = min(max(*n_dev, 0), n);  // record count on the device, at most n
     const uint32_t raw = (uint32_t)__cvta_generic_to_shared(smem_raw);
     const uint32_t sbase = (raw + (kAlign - 1)) & ~(uint32_t)(kAlign - 1);
     uint8_t *base = smem_raw + (sbase - raw);
-    const uint32_t sW1 = sbase + kOffW1, sW2 = sbase + kOffW2, sW3 = sbase + kOffW3;
-    const uint32_t sA1 = sbase + kOffA1, sA2 = sbase + kOffA2, sRec = sbase + kOffRec;
-    const uint32_t sBar = sbase + kOffBar, sRecBar = sBar + 8, sTmem = sBar + 16;
+    const uint32_t sW1 = sbase + L::OFF_W1, sW2 = sbase + L::OFF_W2, sW3 = sbase + L::OFF_W3;
+    const uint32_t sA1 = sbase + L::OFF_A1, sA2 = sbase + L::OFF_A2, sRec = sbase + L::OFF_REC;
+    const uint32_t sBar = sbase + L::OFF_BAR, sRecBar = sBar + 8, sTmem = sBar + 16;
     const int tid = threadIdx.x, warp = tid >> 5;
     const int ntiles = (n + kM - 1) / kM;
 
@@ -430,11 +487,10 @@ __global__ void __launch_bounds__(128, 1) mlp_tc_kernel(const uint16_t *__restri
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(sRecBar) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         if (BULK && (int)blockIdx.x < ntiles)
-            bulk_load(sRec, rois + (size_t)blockIdx.x * kM * kWhole, (uint32_t)(tile_rows(blockIdx.x, n) * kWhole * 2),
-                      sRecBar);
+            bulk_load(sRec, rois + (size_t)blockIdx.x * kM * WHOLE, bulk_bytes<R>(tile_rows(blockIdx.x, n)), sRecBar);
     }
-    uint4 *wdst = reinterpret_cast<uint4 *>(base + kOffW1);
-    for (int i = tid; i < kWeightVec; i += blockDim.x) wdst[i] = wimg[i];
+    uint4 *wdst = reinterpret_cast<uint4 *>(base + L::OFF_W1);
+    for (int i = tid; i < L::WEIGHT_VEC; i += blockDim.x) wdst[i] = wimg[i];
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sTmem), "r"(kTmemCols)
                      : "memory");
@@ -444,10 +500,11 @@ __global__ void __launch_bounds__(128, 1) mlp_tc_kernel(const uint16_t *__restri
     fence_before();
     __syncthreads();
     fence_after();
-    const uint32_t tmem = *reinterpret_cast<volatile uint32_t *>(base + kOffBar + 16);
+    const uint32_t tmem = *reinterpret_cast<volatile uint32_t *>(base + L::OFF_BAR + 16);
     const uint32_t row_lane = (uint32_t)(warp * 32) << 16;
     uint32_t phase = 0, rec_phase = 0;
     bool ok = true, copy_pending = BULK && (int)blockIdx.x < ntiles;
+    uint16_t *srec = reinterpret_cast<uint16_t *>(base + L::OFF_REC);
     for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         const int i = tile * kM + tid;
         const int rows = tile_rows(tile, n);
@@ -456,50 +513,31 @@ __global__ void __launch_bounds__(128, 1) mlp_tc_kernel(const uint16_t *__restri
             if (!ok) break;  // rec_phase still names the copy in flight
             rec_phase ^= 1u;
             copy_pending = false;
+            const int copied = (int)bulk_bytes<R>(rows) / 2, total = rows * WHOLE;
+            if (copied < total) {  // the ragged last tile's last few words (same for every thread)
+                if (tid < total - copied) srec[copied + tid] = rois[(size_t)tile * kM * WHOLE + copied + tid];
+                __syncthreads();
+            }
         }
         // features of this thread's ROI into A1 (row tid)
         float lo = 1.0f, rng = 1.0f;
         {
-            float f[kIn];
-#pragma unroll
-            for (int k = 0; k < kIn; ++k) f[k] = 0.0f;
-            if (tid < rows) {
-                uint16_t px[kWhole];
-                if (BULK) {
-                    const uint4 *r4 = reinterpret_cast<const uint4 *>(base + kOffRec + (size_t)tid * kWhole * 2);
-#pragma unroll
-                    for (int q = 0; q < kWhole / 8; ++q) {
-                        const uint4 u = r4[q];
-                        const uint32_t w[4] = {u.x, u.y, u.z, u.w};
-#pragma unroll
-                        for (int h = 0; h < 4; ++h) {
-                            px[q * 8 + 2 * h] = (uint16_t)(w[h] & 0xFFFFu);
-                            px[q * 8 + 2 * h + 1] = (uint16_t)(w[h] >> 16);
-                        }
-                    }
-                } else {
-                    const uint16_t *r = rois + (size_t)i * kWhole;
-#pragma unroll
-                    for (int k = 0; k < kPix; ++k) px[k] = r[k];
-                }
-                float hi = -1e30f;
-                lo = 1e30f;
-#pragma unroll
-                for (int k = 0; k < kPix; ++k) {
-                    f[k] = fmaxf(((float)px[k] - offset) * kadc, 1.0f);
-                    lo = fminf(lo, f[k]);
-                    hi = fmaxf(hi, f[k]);
-                }
-                rng = fmaxf(hi - lo, 1.0f);
-                const float inv = 1.0f / rng;
-#pragma unroll
-                for (int k = 0; k < kPix; ++k) f[k] = (f[k] - lo) * inv;
-                f[kPix] = logf(rng) * 0.125f;
-                f[kPix + 1] = logf(lo) * 0.125f;
+            const uint16_t *r = BULK ? srec + (size_t)tid * WHOLE : rois + (size_t)i * WHOLE;
+            float inv = 0.0f, f_rng = 0.0f, f_lo = 0.0f;
+            const bool live = tid < rows;
+            if (live) {
+                record_range<R>(r, offset, kadc, lo, rng);
+                inv = 1.0f / rng;
+                f_rng = logf(rng) * 0.125f;
+                f_lo = logf(lo) * 0.125f;
             }
+#pragma unroll 1
+            for (int kg = 0; kg < KIN / 8; ++kg) {
+                float f[8];
 #pragma unroll
-            for (int kg = 0; kg < kIn / 8; ++kg)
-                *reinterpret_cast<uint4 *>(base + kOffA1 + (size_t)(kg * kM + tid) * 16) = pack8(f + 8 * kg);
+                for (int j = 0; j < 8; ++j) f[j] = live ? feature<R>(r, kg * 8 + j, offset, kadc, lo, inv, f_rng, f_lo) : 0.0f;
+                *reinterpret_cast<uint4 *>(base + L::OFF_A1 + (size_t)(kg * kM + tid) * 16) = pack8(f);
+            }
         }
         fence_async_smem();
         fence_before();
@@ -509,15 +547,14 @@ __global__ void __launch_bounds__(128, 1) mlp_tc_kernel(const uint16_t *__restri
         if (BULK && tid == 0) {
             const int next = tile + gridDim.x;
             if (next < ntiles) {
-                bulk_load(sRec, rois + (size_t)next * kM * kWhole, (uint32_t)(tile_rows(next, n) * kWhole * 2),
-                          sRecBar);
+                bulk_load(sRec, rois + (size_t)next * kM * WHOLE, bulk_bytes<R>(tile_rows(next, n)), sRecBar);
                 copy_pending = true;
             }
         }
         // layer 1: D[128 x 128] at column 0
         if (tid == 0) {
 #pragma unroll
-            for (int ks = 0; ks < kIn / 16; ++ks)
+            for (int ks = 0; ks < KIN / 16; ++ks)
                 mma_bf16(tmem, smem_desc(sA1 + ks * 2 * kM * 16, kM * 16, 128),
                          smem_desc(sW1 + ks * 2 * kHidden * 16, kHidden * 16, 128), instr_desc(kM, kHidden),
                          ks > 0);
@@ -527,7 +564,7 @@ __global__ void __launch_bounds__(128, 1) mlp_tc_kernel(const uint16_t *__restri
         phase ^= 1u;
         if (!ok) break;
         fence_after();
-        epilogue_hidden(tmem + row_lane, b1, base + kOffA2, tid);  // layer 1 has read A1 (aliased here)
+        epilogue_hidden(tmem + row_lane, b1, base + L::OFF_A2, tid);  // layer 1 has read A1 (aliased here)
         fence_async_smem();
         fence_before();
         __syncthreads();
@@ -545,7 +582,7 @@ __global__ void __launch_bounds__(128, 1) mlp_tc_kernel(const uint16_t *__restri
         phase ^= 1u;
         if (!ok) break;
         fence_after();
-        epilogue_hidden(tmem + row_lane + kHidden, b2, base + kOffA2, tid);  // layer 2 has read A2
+        epilogue_hidden(tmem + row_lane + kHidden, b2, base + L::OFF_A2, tid);  // layer 2 has read A2
         fence_async_smem();
         fence_before();
         __syncthreads();
@@ -565,15 +602,11 @@ __global__ void __launch_bounds__(128, 1) mlp_tc_kernel(const uint16_t *__restri
         float y[16];
         tmem_ld16(tmem + row_lane, y);
         if (tid < rows) {
-            float *st = start + (size_t)i * kStart;
-            st[0] = rng * expf(fminf(fmaxf(y[3] + __ldg(b3 + 3), -6.0f), 3.0f));
-            st[1] = kCentre + fminf(fmaxf(y[0] + __ldg(b3 + 0), -1.5f), 1.5f);
-            st[2] = kCentre + fminf(fmaxf(y[1] + __ldg(b3 + 1), -1.5f), 1.5f);
-            st[3] = fminf(fmaxf(kSigma0 + y[2] + __ldg(b3 + 2), 0.6f), 3.0f);
-            st[4] = fmaxf(lo + rng * (y[4] + __ldg(b3 + 4)), 1.0f);
-            if (cls)
-                cls[i] = (uint8_t)count_class(y[kCount0] + __ldg(b3 + kCount0), y[kCount0 + 1] + __ldg(b3 + kCount0 + 1),
-                                              y[kCount0 + 2] + __ldg(b3 + kCount0 + 2), count_th);
+#pragma unroll
+            for (int j = 0; j < kOut; ++j) y[j] += __ldg(b3 + j);
+            start_from_outputs<R, LT>(y, lo, rng, start + (size_t)i * NST);
+            if (LT == QCS_LOCTYPE_GS2D && cls)
+                cls[i] = (uint8_t)count_class(y[kCount0], y[kCount0 + 1], y[kCount0 + 2], count_th);
         }
         fence_before();
         __syncthreads();  // accumulator columns are free for the next tile
@@ -591,18 +624,20 @@ __global__ void __launch_bounds__(128, 1) mlp_tc_kernel(const uint16_t *__restri
 }
 
 // FP32 master weights -> BF16 operand images (W1 | W2 | W3, N x K K-major).
+template <int KIN>
 __global__ void weight_image_kernel(const float *__restrict__ par, __nv_bfloat16 *__restrict__ img) {
+    constexpr int W1 = kHidden * KIN, W2 = kHidden * kHidden, W3 = kN3 * kHidden;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const float *W1 = par, *W2 = W1 + kIn * kHidden + kHidden, *W3 = W2 + kHidden * kHidden + kHidden;
-    if (i < kW1) {
+    const float *pW1 = par, *pW2 = pW1 + KIN * kHidden + kHidden, *pW3 = pW2 + kHidden * kHidden + kHidden;
+    if (i < W1) {
         const int k = i / kHidden, nn = i % kHidden;
-        img[img_index(nn, k, kHidden)] = __float2bfloat16_rn(W1[i]);
-    } else if (i < kW1 + kW2) {
-        const int j = i - kW1, k = j / kHidden, nn = j % kHidden;
-        img[kW1 + img_index(nn, k, kHidden)] = __float2bfloat16_rn(W2[j]);
-    } else if (i < kW1 + kW2 + kW3) {
-        const int j = i - kW1 - kW2, k = j / kN3, nn = j % kN3;
-        img[kW1 + kW2 + img_index(nn, k, kN3)] = __float2bfloat16_rn(nn < kOut ? W3[k * kOut + nn] : 0.0f);
+        img[img_index(nn, k, kHidden)] = __float2bfloat16_rn(pW1[i]);
+    } else if (i < W1 + W2) {
+        const int j = i - W1, k = j / kHidden, nn = j % kHidden;
+        img[W1 + img_index(nn, k, kHidden)] = __float2bfloat16_rn(pW2[j]);
+    } else if (i < W1 + W2 + W3) {
+        const int j = i - W1 - W2, k = j / kN3, nn = j % kN3;
+        img[W1 + W2 + img_index(nn, k, kN3)] = __float2bfloat16_rn(nn < kOut ? pW3[k * kOut + nn] : 0.0f);
     }
 }
 
@@ -614,6 +649,10 @@ using qcs::fail;
 namespace L = qcs::learned;
 
 struct qcs_learned_net {
+    int loc_type = QCS_LOCTYPE_GS2D;  // the shape the network is built for
+    int R = 7;
+    int kin = 64;                     // input width: in_width(R)
+    int params = 0;                   // param_count(kin)
     // parameters (FP32 master copies), their gradients and Adam moments, in one block
     float *d_par = nullptr, *d_grad = nullptr, *d_m = nullptr, *d_v = nullptr;
     // activations of one batch
@@ -639,10 +678,10 @@ namespace {
 struct Views {
     float *W1, *b1, *W2, *b2, *W3, *b3;
 };
-Views views(float *p) {
+Views views(float *p, int kin) {
     Views v;
     v.W1 = p;
-    v.b1 = v.W1 + L::kIn * L::kHidden;
+    v.b1 = v.W1 + kin * L::kHidden;
     v.W2 = v.b1 + L::kHidden;
     v.b2 = v.W2 + L::kHidden * L::kHidden;
     v.W3 = v.b2 + L::kHidden;
@@ -658,9 +697,10 @@ inline float class_threshold(const qcs_learned_net *net) { return net->count_th 
 // Forward over `rows` feature rows into net->d_y (and the hidden activations).
 cudaError_t forward(qcs_learned_net *net, const float *x, int rows, float *z1, float *a1, float *z2, float *a2,
                     float *y, cudaStream_t s) {
-    const Views w = views(net->d_par);
+    const Views w = views(net->d_par, net->kin);
     cudaError_t e;
-    if ((e = L::gemm(rows, L::kHidden, L::kIn, x, L::kIn, 1, w.W1, L::kHidden, 1, z1, L::kHidden, 0.0f, s))) return e;
+    if ((e = L::gemm(rows, L::kHidden, net->kin, x, net->kin, 1, w.W1, L::kHidden, 1, z1, L::kHidden, 0.0f, s)))
+        return e;
     L::bias_relu_kernel<<<blocks((long long)rows * L::kHidden), 256, 0, s>>>(z1, w.b1, rows, L::kHidden, a1, 1);
     if ((e = L::gemm(rows, L::kHidden, L::kHidden, a1, L::kHidden, 1, w.W2, L::kHidden, 1, z2, L::kHidden, 0.0f, s)))
         return e;
@@ -672,8 +712,8 @@ cudaError_t forward(qcs_learned_net *net, const float *x, int rows, float *z1, f
 
 // Backward of the masked MSE for one batch already forwarded; fills d_grad.
 cudaError_t backward(qcs_learned_net *net, int rows, cudaStream_t s) {
-    const Views w = views(net->d_par);
-    const Views g = views(net->d_grad);
+    const Views w = views(net->d_par, net->kin);
+    const Views g = views(net->d_grad, net->kin);
     cudaError_t e;
     // layer 3: dW3 = a2^T dy, db3 = colsum(dy), d2 = dy W3^T
     if ((e = L::gemm(L::kHidden, L::kOut, rows, net->d_a2, 1, L::kHidden, net->d_dy, L::kOut, 1, g.W3, L::kOut, 0.0f,
@@ -696,8 +736,8 @@ cudaError_t backward(qcs_learned_net *net, int rows, cudaStream_t s) {
     L::relu_back_kernel<<<blocks((long long)rows * L::kHidden), 256, 0, s>>>(net->d_d1, net->d_z1,
                                                                            (long long)rows * L::kHidden);
     // layer 1
-    if ((e = L::gemm(L::kIn, L::kHidden, rows, net->d_x, 1, L::kIn, net->d_d1, L::kHidden, 1, g.W1, L::kHidden, 0.0f,
-                     s)))
+    if ((e = L::gemm(net->kin, L::kHidden, rows, net->d_x, 1, net->kin, net->d_d1, L::kHidden, 1, g.W1, L::kHidden,
+                     0.0f, s)))
         return e;
     L::colsum_kernel<<<1, L::kHidden, 0, s>>>(net->d_d1, rows, L::kHidden, g.b1);
     return cudaGetLastError();
@@ -717,9 +757,35 @@ void shuffle(int *h, int n, unsigned long long &state) {
     }
 }
 
+// Compile-time shape for the dispatch below.
+template <int R_, int LT_>
+struct Shape {
+    static constexpr int R = R_, LT = LT_;
+};
+
+// f(Shape<R, LT>{}) for the network shape (loc_type, R).
+template <class F>
+cudaError_t by_shape(int loc_type, int R, F &&f) {
+    if (loc_type == QCS_LOCTYPE_AS3D) {
+        switch (R) {
+        case 7: return f(Shape<7, QCS_LOCTYPE_AS3D>{});
+        case 9: return f(Shape<9, QCS_LOCTYPE_AS3D>{});
+        case 11: return f(Shape<11, QCS_LOCTYPE_AS3D>{});
+        }
+    } else if (loc_type == QCS_LOCTYPE_GS2D) {
+        switch (R) {
+        case 7: return f(Shape<7, QCS_LOCTYPE_GS2D>{});
+        case 9: return f(Shape<9, QCS_LOCTYPE_GS2D>{});
+        case 11: return f(Shape<11, QCS_LOCTYPE_GS2D>{});
+        }
+    }
+    return cudaErrorInvalidValue;
+}
+
 // Start points of n ROIs through the fused tcgen05 kernel: BF16 operand
-// images of the current weights, then one persistent launch (two CTAs of
-// 101 KB shared memory and 256 tensor-memory columns per SM).
+// images of the current weights, then one persistent launch (7x7: two CTAs
+// of 101 KB shared memory and 256 tensor-memory columns per SM; 9x9, 11x11:
+// one CTA of 123 or 133 KB).
 cudaError_t fused_start_points(qcs_learned_net *net, const qcs_loc_para *p, const uint16_t *d_rois, int n,
                                const int *n_dev, float *start, uint8_t *cls, cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
@@ -727,35 +793,48 @@ cudaError_t fused_start_points(qcs_learned_net *net, const qcs_loc_para *p, cons
     int dev = 0, sms = 148;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const bool bulk = (reinterpret_cast<uintptr_t>(d_rois) & 15) == 0;
-    auto kern = bulk ? L::tc::mlp_tc_kernel<true> : L::tc::mlp_tc_kernel<false>;
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L::tc::kSmemBytes);
     if (e != cudaSuccess) return e;
-    const int grid = tiles < 2 * sms ? tiles : 2 * sms;
-    const Views w = views(net->d_par);
-    // the weight image is rebuilt only after a parameter change; calls on
-    // other streams wait for the build that made the current one
-    if (net->wimg_version != net->version) {
-        L::tc::weight_image_kernel<<<blocks(L::tc::kW1 + L::tc::kW2 + L::tc::kW3), 256, 0, s>>>(net->d_par,
-                                                                                             net->d_wimg);
-        e = cudaEventRecord(net->wimg_ready, s);
-        if (e != cudaSuccess) return e;
-        net->wimg_version = net->version;
-    } else {
-        e = cudaStreamWaitEvent(s, net->wimg_ready, 0);
-        if (e != cudaSuccess) return e;
-    }
-    kern<<<grid, 128, L::tc::kSmemBytes, s>>>(d_rois, n, p->Offset, p->KAdc, reinterpret_cast<const uint4 *>(net->d_wimg),
-                                              w.b1, w.b2, w.b3, start, cls, class_threshold(net), n_dev,
-                                              net->d_err);
-    return cudaGetLastError();
+    const bool bulk = (reinterpret_cast<uintptr_t>(d_rois) & 15) == 0;
+    const Views w = views(net->d_par, net->kin);
+    const float th = class_threshold(net);
+    return by_shape(net->loc_type, net->R, [&](auto sh) -> cudaError_t {
+        constexpr int R = decltype(sh)::R, LT = decltype(sh)::LT;
+        typedef L::tc::Layout<R> Lay;
+        auto kern = bulk ? L::tc::mlp_tc_kernel<true, R, LT> : L::tc::mlp_tc_kernel<false, R, LT>;
+        cudaError_t e2 = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Lay::SMEM);
+        if (e2 != cudaSuccess) return e2;
+        const int per_sm = Lay::SMEM <= 113 * 1024 ? 2 : 1;
+        const int grid = tiles < per_sm * sms ? tiles : per_sm * sms;
+        // the weight image is rebuilt only after a parameter change; calls on
+        // other streams wait for the build that made the current one
+        if (net->wimg_version != net->version) {
+            L::tc::weight_image_kernel<Lay::KIN><<<blocks(Lay::W1 + Lay::W2 + Lay::W3), 256, 0, s>>>(net->d_par,
+                                                                                                  net->d_wimg);
+            e2 = cudaEventRecord(net->wimg_ready, s);
+            if (e2 != cudaSuccess) return e2;
+            net->wimg_version = net->version;
+        } else {
+            e2 = cudaStreamWaitEvent(s, net->wimg_ready, 0);
+            if (e2 != cudaSuccess) return e2;
+        }
+        kern<<<grid, 128, Lay::SMEM, s>>>(d_rois, n, p->Offset, p->KAdc, reinterpret_cast<const uint4 *>(net->d_wimg),
+                                          w.b1, w.b2, w.b3, start, cls, th, n_dev, net->d_err);
+        return cudaGetLastError();
+    });
+}
+
+// net's shape against the call's parameters
+int check_shape(const qcs_learned_net *net, const qcs_loc_para *p) {
+    if (p->ROISize != net->R || p->LocType != net->loc_type)
+        return fail(QCS_ERR_ROISIZE, "the network was built for another localization type or ROI size");
+    return QCS_OK;
 }
 
 }  // namespace
 
 extern "C" {
 
-int qcs_learned_param_count(void) { return L::kParams; }
+int qcs_learned_param_count(void) { return L::param_count(L::in_width(7)); }
 
 int qcs_learned_destroy(qcs_learned_net *net) {
     if (!net) return QCS_OK;
@@ -772,22 +851,30 @@ int qcs_learned_destroy(qcs_learned_net *net) {
     return QCS_OK;
 }
 
-int qcs_learned_create(int batch, unsigned long long seed, qcs_learned_net **out) {
+int qcs_learned_create_for(int loc_type, int roi_size, int batch, unsigned long long seed, qcs_learned_net **out) {
     if (!out) return fail(QCS_ERR_ARG, "null output handle");
     *out = nullptr;
+    if (!L::shape_supported(loc_type, roi_size))
+        return fail(QCS_ERR_ROISIZE, "learned start points: GS2D or AS3D, ROISize 7, 9 or 11");
     if (batch <= 0) batch = 4096;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
         return fail(QCS_ERR_CUDA, "no CUDA device: qcstorm_b200 has no CPU fallback");
     qcs_learned_net *net = new qcs_learned_net();
+    net->loc_type = loc_type;
+    net->R = roi_size;
+    net->kin = L::in_width(roi_size);
+    net->params = L::param_count(net->kin);
     net->batch = batch;
-    const size_t P = L::kParams;
+    const int kin = net->kin;
+    const size_t P = net->params;
     const size_t B = (size_t)batch;
-    const size_t acts = B * (L::kIn + 4 * L::kHidden + L::kOut + L::kOutUsed + 1 + L::kOut + 2 * L::kHidden) + 4;
+    const size_t acts = B * (kin + 4 * L::kHidden + L::kOut + L::kUsedMax + 1 + L::kOut + 2 * L::kHidden) + 4;
+    const size_t wimg_bytes = (size_t)(L::kHidden * kin + L::kHidden * L::kHidden + L::tc::kN3 * L::kHidden) * 2;
     cudaError_t e = cudaMalloc((void **)&net->d_par, 4 * P * sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc((void **)&net->d_x, acts * sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc((void **)&net->d_idx, B * sizeof(int));
-    if (e == cudaSuccess) e = cudaMalloc((void **)&net->d_wimg, L::tc::kWeightVec * 16);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&net->d_wimg, wimg_bytes);
     if (e == cudaSuccess) e = cudaMalloc((void **)&net->d_err, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(net->d_err, 0, sizeof(int));
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&net->stream, cudaStreamNonBlocking);
@@ -799,7 +886,7 @@ int qcs_learned_create(int batch, unsigned long long seed, qcs_learned_net **out
     net->d_grad = net->d_par + P;
     net->d_m = net->d_grad + P;
     net->d_v = net->d_m + P;
-    float *a = net->d_x + B * L::kIn;
+    float *a = net->d_x + B * kin;
     net->d_z1 = a;
     a += B * L::kHidden;
     net->d_a1 = a;
@@ -811,7 +898,7 @@ int qcs_learned_create(int batch, unsigned long long seed, qcs_learned_net **out
     net->d_y = a;
     a += B * L::kOut;
     net->d_t = a;
-    a += B * L::kOutUsed;
+    a += B * L::kUsedMax;
     net->d_valid = a;
     a += B;
     net->d_dy = a;
@@ -830,8 +917,8 @@ int qcs_learned_create(int batch, unsigned long long seed, qcs_learned_net **out
         st ^= st << 17;
         return (float)((st >> 11) * (1.0 / 9007199254740992.0)) * 2.0f - 1.0f;
     };
-    const Views hv = views(h);
-    for (int i = 0; i < L::kIn * L::kHidden; ++i) hv.W1[i] = uni() * sqrtf(6.0f / L::kIn);
+    const Views hv = views(h, kin);
+    for (int i = 0; i < kin * L::kHidden; ++i) hv.W1[i] = uni() * sqrtf(6.0f / kin);
     for (int i = 0; i < L::kHidden; ++i) hv.b1[i] = 0.0f;
     for (int i = 0; i < L::kHidden * L::kHidden; ++i) hv.W2[i] = uni() * sqrtf(6.0f / L::kHidden);
     for (int i = 0; i < L::kHidden; ++i) hv.b2[i] = 0.0f;
@@ -848,15 +935,29 @@ int qcs_learned_create(int batch, unsigned long long seed, qcs_learned_net **out
     return QCS_OK;
 }
 
+int qcs_learned_create(int batch, unsigned long long seed, qcs_learned_net **out) {
+    return qcs_learned_create_for(QCS_LOCTYPE_GS2D, 7, batch, seed, out);
+}
+
+int qcs_learned_shape(const qcs_learned_net *net, int *loc_type, int *roi_size, int *params) {
+    if (!net) return fail(QCS_ERR_ARG, "null network");
+    if (loc_type) *loc_type = net->loc_type;
+    if (roi_size) *roi_size = net->R;
+    if (params) *params = net->params;
+    return QCS_OK;
+}
+
 int qcs_learned_get_params(qcs_learned_net *net, float *h_params) {
     if (!net || !h_params) return fail(QCS_ERR_ARG, "null argument");
-    QCS_CUDA(cudaMemcpy(h_params, net->d_par, L::kParams * sizeof(float), cudaMemcpyDeviceToHost), "read parameters");
+    QCS_CUDA(cudaMemcpy(h_params, net->d_par, (size_t)net->params * sizeof(float), cudaMemcpyDeviceToHost),
+             "read parameters");
     return QCS_OK;
 }
 
 int qcs_learned_set_params(qcs_learned_net *net, const float *h_params) {
     if (!net || !h_params) return fail(QCS_ERR_ARG, "null argument");
-    QCS_CUDA(cudaMemcpy(net->d_par, h_params, L::kParams * sizeof(float), cudaMemcpyHostToDevice), "set parameters");
+    QCS_CUDA(cudaMemcpy(net->d_par, h_params, (size_t)net->params * sizeof(float), cudaMemcpyHostToDevice),
+             "set parameters");
     net->version++;
     return QCS_OK;
 }
@@ -864,22 +965,32 @@ int qcs_learned_set_params(qcs_learned_net *net, const float *h_params) {
 int qcs_learned_features_device(const qcs_loc_para *p, const uint16_t *d_rois, int n, float *d_feat, float *d_scale,
                                 void *stream) {
     if (!p || (!d_rois && n > 0) || !d_feat || !d_scale) return fail(QCS_ERR_ARG, "null argument");
-    if (p->ROISize != L::kR || p->LocType != QCS_LOCTYPE_GS2D)
-        return fail(QCS_ERR_ROISIZE, "learned start points are built for GS2D 7x7 ROIs");
+    if (!L::shape_supported(p->LocType, p->ROISize))
+        return fail(QCS_ERR_ROISIZE, "learned start points: GS2D or AS3D, ROISize 7, 9 or 11");
     if (n <= 0) return QCS_OK;
-    L::features_kernel<<<blocks(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(d_rois, n, p->Offset, p->KAdc, d_feat,
-                                                                                 d_scale);
-    QCS_CUDA(cudaGetLastError(), "features");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    QCS_CUDA(by_shape(QCS_LOCTYPE_GS2D, p->ROISize, [&](auto sh) -> cudaError_t {
+                 L::features_kernel<decltype(sh)::R><<<blocks(n), 256, 0, s>>>(d_rois, n, p->Offset, p->KAdc, d_feat,
+                                                                                d_scale);
+                 return cudaGetLastError();
+             }),
+             "features");
     return QCS_OK;
 }
 
 int qcs_learned_targets_device(const qcs_loc_para *p, const uint16_t *d_rois, const float *d_rows,
                                const float *d_scale, int n, float *d_targets, float *d_valid, void *stream) {
     if (!p || !d_rois || !d_rows || !d_scale || !d_targets || !d_valid) return fail(QCS_ERR_ARG, "null argument");
+    if (!L::shape_supported(p->LocType, p->ROISize))
+        return fail(QCS_ERR_ROISIZE, "learned start points: GS2D or AS3D, ROISize 7, 9 or 11");
     if (n <= 0) return QCS_OK;
-    L::targets_kernel<<<blocks(n), 256, 0, static_cast<cudaStream_t>(stream)>>>(d_rois, d_rows, d_scale, n, p->QE,
-                                                                                d_targets, d_valid);
-    QCS_CUDA(cudaGetLastError(), "targets");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    QCS_CUDA(by_shape(p->LocType, p->ROISize, [&](auto sh) -> cudaError_t {
+                 L::targets_kernel<decltype(sh)::R, decltype(sh)::LT>
+                     <<<blocks(n), 256, 0, s>>>(d_rois, d_rows, d_scale, n, p->QE, d_targets, d_valid);
+                 return cudaGetLastError();
+             }),
+             "targets");
     return QCS_OK;
 }
 
@@ -888,7 +999,7 @@ int qcs_learned_forward_device(qcs_learned_net *net, const float *d_feat, int n,
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : net->stream;
     for (int r0 = 0; r0 < n; r0 += net->batch) {
         const int rows = (n - r0) < net->batch ? (n - r0) : net->batch;
-        QCS_CUDA(forward(net, d_feat + (size_t)r0 * L::kIn, rows, net->d_z1, net->d_a1, net->d_z2, net->d_a2,
+        QCS_CUDA(forward(net, d_feat + (size_t)r0 * net->kin, rows, net->d_z1, net->d_a1, net->d_z2, net->d_a2,
                          d_out + (size_t)r0 * L::kOut, s),
                  "forward");
     }
@@ -905,13 +1016,14 @@ int qcs_learned_gradient_counts_device(qcs_learned_net *net, const float *d_feat
                                        void *stream) {
     if (!net || !d_feat || !d_targets || !d_valid) return fail(QCS_ERR_ARG, "null argument");
     if (n <= 0 || n > net->batch) return fail(QCS_ERR_CAPACITY, "gradient batch must be 1..batch rows");
+    if (d_classes && net->loc_type != QCS_LOCTYPE_GS2D) return fail(QCS_ERR_ARG, "count classes: GS2D networks only");
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : net->stream;
-    QCS_CUDA(cudaMemcpyAsync(net->d_x, d_feat, (size_t)n * L::kIn * sizeof(float), cudaMemcpyDeviceToDevice, s),
+    QCS_CUDA(cudaMemcpyAsync(net->d_x, d_feat, (size_t)n * net->kin * sizeof(float), cudaMemcpyDeviceToDevice, s),
              "copy features");
     QCS_CUDA(forward(net, net->d_x, n, net->d_z1, net->d_a1, net->d_z2, net->d_a2, net->d_y, s), "forward");
     QCS_CUDA(cudaMemsetAsync(net->d_loss, 0, sizeof(float), s), "clear loss");
-    L::mse_kernel<<<blocks(n), 256, 0, s>>>(net->d_y, d_targets, d_valid, d_classes, n, 1.0f / (float)n, net->d_dy,
-                                            net->d_loss);
+    L::mse_kernel<<<blocks(n), 256, 0, s>>>(net->d_y, d_targets, d_valid, d_classes, n, L::used_outputs(net->loc_type),
+                                            1.0f / (float)n, net->d_dy, net->d_loss);
     QCS_CUDA(backward(net, n, s), "backward");
     if (h_loss) {
         QCS_CUDA(cudaMemcpyAsync(h_loss, net->d_loss, sizeof(float), cudaMemcpyDeviceToHost, s), "read loss");
@@ -922,7 +1034,8 @@ int qcs_learned_gradient_counts_device(qcs_learned_net *net, const float *d_feat
 
 int qcs_learned_get_grads(qcs_learned_net *net, float *h_grads) {
     if (!net || !h_grads) return fail(QCS_ERR_ARG, "null argument");
-    QCS_CUDA(cudaMemcpy(h_grads, net->d_grad, L::kParams * sizeof(float), cudaMemcpyDeviceToHost), "read gradients");
+    QCS_CUDA(cudaMemcpy(h_grads, net->d_grad, (size_t)net->params * sizeof(float), cudaMemcpyDeviceToHost),
+             "read gradients");
     return QCS_OK;
 }
 
@@ -937,16 +1050,18 @@ int qcs_learned_train_counts_device(qcs_learned_net *net, const float *d_feat, c
                                     unsigned long long seed, float *h_epoch_loss, void *stream) {
     if (!net || !d_feat || !d_targets || !d_valid) return fail(QCS_ERR_ARG, "null argument");
     if (n < net->batch) return fail(QCS_ERR_ARG, "fewer training rows than one batch");
+    if (d_classes && net->loc_type != QCS_LOCTYPE_GS2D) return fail(QCS_ERR_ARG, "count classes: GS2D networks only");
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : net->stream;
     const int B = net->batch;
     const int steps = n / B;
+    const int kin = net->kin, nu = L::used_outputs(net->loc_type);
     int *h_perm = new int[n];
     int *d_perm = nullptr;
     float *d_vb = nullptr, *d_tb = nullptr;
     cudaError_t e = cudaMalloc((void **)&d_perm, (size_t)n * sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc((void **)&d_vb, (size_t)B * 2 * sizeof(float));  // valid | classes
     float *d_cb = d_classes ? d_vb + B : nullptr;
-    if (e == cudaSuccess) e = cudaMalloc((void **)&d_tb, (size_t)B * L::kOutUsed * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&d_tb, (size_t)B * nu * sizeof(float));
     unsigned long long state = seed ? seed : 0x2545F4914F6CDD1Dull;
     const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
     for (int ep = 0; ep < epochs && e == cudaSuccess; ++ep) {
@@ -955,23 +1070,22 @@ int qcs_learned_train_counts_device(qcs_learned_net *net, const float *d_feat, c
         if (e == cudaSuccess) e = cudaMemsetAsync(net->d_loss, 0, sizeof(float), s);
         for (int st = 0; st < steps && e == cudaSuccess; ++st) {
             const int *idx = d_perm + (size_t)st * B;
-            L::gather_rows_kernel<<<blocks((long long)B * L::kIn), 256, 0, s>>>(d_feat, idx, B, L::kIn, net->d_x);
-            L::gather_rows_kernel<<<blocks((long long)B * L::kOutUsed), 256, 0, s>>>(d_targets, idx, B, L::kOutUsed,
-                                                                                   d_tb);
+            L::gather_rows_kernel<<<blocks((long long)B * kin), 256, 0, s>>>(d_feat, idx, B, kin, net->d_x);
+            L::gather_rows_kernel<<<blocks((long long)B * nu), 256, 0, s>>>(d_targets, idx, B, nu, d_tb);
             L::gather_rows_kernel<<<blocks(B), 256, 0, s>>>(d_valid, idx, B, 1, d_vb);
             if (d_cb) L::gather_rows_kernel<<<blocks(B), 256, 0, s>>>(d_classes, idx, B, 1, d_cb);
             e = forward(net, net->d_x, B, net->d_z1, net->d_a1, net->d_z2, net->d_a2, net->d_y, s);
             if (e != cudaSuccess) break;
             // per-batch mean loss and its gradient; the loss accumulates over the epoch
-            L::mse_kernel<<<blocks(B), 256, 0, s>>>(net->d_y, d_tb, d_vb, d_cb, B, 1.0f / (float)B, net->d_dy,
+            L::mse_kernel<<<blocks(B), 256, 0, s>>>(net->d_y, d_tb, d_vb, d_cb, B, nu, 1.0f / (float)B, net->d_dy,
                                                     net->d_loss);
             e = backward(net, B, s);
             if (e != cudaSuccess) break;
             net->step++;
             const float c1 = 1.0f / (1.0f - powf(b1, (float)net->step));
             const float c2 = 1.0f / (1.0f - powf(b2, (float)net->step));
-            L::adam_kernel<<<blocks(L::kParams), 256, 0, s>>>(net->d_par, net->d_grad, net->d_m, net->d_v, L::kParams,
-                                                             lr, b1, b2, c1, c2, eps);
+            L::adam_kernel<<<blocks(net->params), 256, 0, s>>>(net->d_par, net->d_grad, net->d_m, net->d_v,
+                                                               net->params, lr, b1, b2, c1, c2, eps);
             e = cudaGetLastError();
         }
         if (e == cudaSuccess && h_epoch_loss) {
@@ -993,27 +1107,34 @@ int qcs_learned_train_counts_device(qcs_learned_net *net, const float *d_feat, c
 int qcs_learned_start_device(qcs_learned_net *net, const qcs_loc_para *p, const uint16_t *d_rois, int n,
                              float *d_start, float *d_work, void *stream) {
     if (!net || !p || !d_start || !d_work) return fail(QCS_ERR_ARG, "null argument");
+    int st = check_shape(net, p);
+    if (st) return st;
     if (n <= 0) return QCS_OK;
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : net->stream;
     if (net->use_tc) {
         QCS_CUDA(fused_start_points(net, p, d_rois, n, nullptr, d_start, nullptr, s), "fused start points");
         return QCS_OK;
     }
-    float *feat = d_work, *scale = feat + (size_t)n * L::kIn, *y = scale + 2 * (size_t)n;
-    int st = qcs_learned_features_device(p, d_rois, n, feat, scale, s);
+    float *feat = d_work, *scale = feat + (size_t)n * net->kin, *y = scale + 2 * (size_t)n;
+    st = qcs_learned_features_device(p, d_rois, n, feat, scale, s);
     if (st) return st;
     st = qcs_learned_forward_device(net, feat, n, y, s);
     if (st) return st;
-    L::start_kernel<<<blocks(n), 256, 0, s>>>(y, scale, n, d_start, nullptr, 0.0f);
-    QCS_CUDA(cudaGetLastError(), "start points");
+    QCS_CUDA(by_shape(net->loc_type, net->R, [&](auto sh) -> cudaError_t {
+                 L::start_kernel<decltype(sh)::R, decltype(sh)::LT>
+                     <<<blocks(n), 256, 0, s>>>(y, scale, n, d_start, nullptr, 0.0f);
+                 return cudaGetLastError();
+             }),
+             "start points");
     return QCS_OK;
 }
 
 int qcs_learned_classes_device(qcs_learned_net *net, const qcs_loc_para *p, const uint16_t *d_rois, int n,
                                float *d_start, uint8_t *d_classes, void *stream) {
     if (!net || !p || !d_start || !d_classes) return fail(QCS_ERR_ARG, "null argument");
-    if (p->ROISize != L::kR || p->LocType != QCS_LOCTYPE_GS2D)
-        return fail(QCS_ERR_ROISIZE, "learned start points are built for GS2D 7x7 ROIs");
+    int st = check_shape(net, p);
+    if (st) return st;
+    if (net->loc_type != QCS_LOCTYPE_GS2D) return fail(QCS_ERR_ARG, "count classes: GS2D networks only");
     if (n <= 0) return QCS_OK;
     if (!d_rois) return fail(QCS_ERR_ARG, "null ROI pointer");
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : net->stream;
@@ -1024,13 +1145,16 @@ int qcs_learned_classes_device(qcs_learned_net *net, const qcs_loc_para *p, cons
 int qcs_learned_set_count_threshold(qcs_learned_net *net, float th) {
     if (!net) return fail(QCS_ERR_ARG, "null network");
     if (!(th >= 0.0f && th <= 1.0f)) return fail(QCS_ERR_ARG, "count threshold must be in [0, 1] (0: no routing)");
+    if (th > 0.0f && net->loc_type != QCS_LOCTYPE_GS2D) return fail(QCS_ERR_ARG, "count classes: GS2D networks only");
     net->count_th = th;
     return QCS_OK;
 }
 
 float qcs_learned_count_threshold(const qcs_learned_net *net) { return net ? net->count_th : 0.0f; }
 
-size_t qcs_learned_work_bytes(int n) { return (size_t)(n > 0 ? n : 0) * (L::kIn + 2 + L::kOut) * sizeof(float); }
+size_t qcs_learned_work_bytes(int n) {
+    return (size_t)(n > 0 ? n : 0) * (L::in_width(11) + 2 + L::kOut) * sizeof(float);
+}
 
 int qcs_learned_set_inference(qcs_learned_net *net, int fused) {
     if (!net) return fail(QCS_ERR_ARG, "null network");
@@ -1048,14 +1172,15 @@ int qcs_learned_fused_status(qcs_learned_net *net) {
 
 }  // extern "C"
 
-// Start points of n records into out (n x 5): the fused kernel, or, with
-// fused inference off, features and one GEMM per layer over all n rows in
+// Start points of n records into out: the fused kernel, or, with fused
+// inference off, features and one GEMM per layer over all n rows in
 // net-owned memory (grown, outside any capture, when n exceeds what the last
 // call needed; not for concurrent calls).
 cudaError_t qcs::learned::start_points(qcs_learned_net *net, const qcs_loc_para *p, const uint16_t *d_rois, int n,
                                        float *out, cudaStream_t s, uint8_t *cls, const int *n_dev) {
     if (net->use_tc) return fused_start_points(net, p, d_rois, n, n_dev, out, cls, s);
-    const size_t need = (size_t)n * (L::kStart + L::kIn + 2 + 2 * L::kHidden + L::kOut);
+    const int kin = net->kin;
+    const size_t need = (size_t)n * (kin + 2 + 2 * L::kHidden + L::kOut);
     if (need > net->start_cap) {
         cudaFree(net->d_start);
         net->d_start = nullptr;
@@ -1064,12 +1189,15 @@ cudaError_t qcs::learned::start_points(qcs_learned_net *net, const qcs_loc_para 
         if (e != cudaSuccess) return e;
         net->start_cap = need;
     }
-    float *start = net->d_start, *feat = start + (size_t)n * L::kStart, *scale = feat + (size_t)n * L::kIn;
+    float *feat = net->d_start, *scale = feat + (size_t)n * kin;
     float *h1 = scale + 2 * (size_t)n, *h2 = h1 + (size_t)n * L::kHidden, *y = h2 + (size_t)n * L::kHidden;
-    (void)start;
-    L::features_kernel<<<blocks(n), 256, 0, s>>>(d_rois, n, p->Offset, p->KAdc, feat, scale);
-    cudaError_t e = forward(net, feat, n, h1, h1, h2, h2, y, s);
-    if (e != cudaSuccess) return e;
-    L::start_kernel<<<blocks(n), 256, 0, s>>>(y, scale, n, out, cls, class_threshold(net));
-    return cudaGetLastError();
+    const float th = class_threshold(net);
+    return by_shape(net->loc_type, net->R, [&](auto sh) -> cudaError_t {
+        constexpr int R = decltype(sh)::R, LT = decltype(sh)::LT;
+        L::features_kernel<R><<<blocks(n), 256, 0, s>>>(d_rois, n, p->Offset, p->KAdc, feat, scale);
+        cudaError_t e = forward(net, feat, n, h1, h1, h2, h2, y, s);
+        if (e != cudaSuccess) return e;
+        L::start_kernel<R, LT><<<blocks(n), 256, 0, s>>>(y, scale, n, out, LT == QCS_LOCTYPE_GS2D ? cls : nullptr, th);
+        return cudaGetLastError();
+    });
 }

@@ -9,24 +9,33 @@
 namespace qcs {
 namespace learned {
 
-constexpr int kR = 7;                   // ROI size the network is built for
-constexpr int kPix = kR * kR;           // 49 pixels
-constexpr int kWhole = kR * (kR + 1);   // record length in uint16
-constexpr int kHalf = kR / 2;
-constexpr float kCentre = kR / 2.0f;    // ROI centre in the fit's pixel coordinates
-constexpr float kSigma0 = 1.3f;         // sigma offset of the sigma output
-constexpr int kIn = 64;                 // 49 pixels + 2 scale features + zero padding
+constexpr float kSigma0 = 1.3f;         // sigma offset of the sigma outputs
 constexpr int kHidden = 128;
-constexpr int kOut = 8;                 // 5 start-point outputs, 3 emitter-count logits
-constexpr int kOutUsed = 5;             // dx, dy, sigma - 1.3, log(peak / range), (bkg - min) / range
-constexpr int kCount0 = 5;              // logits of the emitter-count classes 0, 1, 2 (outputs 5..7)
+constexpr int kOut = 8;                 // start-point outputs, then (GS2D) three emitter-count logits
+constexpr int kUsedMax = 6;             // start-point outputs of the widest kind (AS3D)
+constexpr int kCount0 = 5;              // GS2D: logits of the emitter-count classes 0, 1, 2 (outputs 5..7)
 constexpr int kClasses = 3;             // one emitter / two-emitter stage / three-emitter stage
-constexpr int kStart = 5;               // start point: peak e-, x, y, sigma, background e-
-constexpr int kParams = kIn * kHidden + kHidden + kHidden * kHidden + kHidden + kHidden * kOut + kOut;
 
-// loss weight of each output (positions matter most) and of the emitter-count
-// cross-entropy
-__constant__ const float kTargetWeight[kOutUsed] = {4.0f, 4.0f, 1.0f, 1.0f, 1.0f};
+// Network shapes: one per localization type (GS2D, AS3D) and ROI size (7, 9, 11).
+// Input: the R*R photoelectron pixels scaled to [0, 1] by the ROI's range,
+// log(range) / 8, log(min) / 8, zero padding to 64 (7x7) or 128 (9x9, 11x11).
+__host__ __device__ constexpr int in_width(int R) { return R * R + 2 <= 64 ? 64 : 128; }
+// Outputs fitted to the targets: GS2D dx, dy, sigma - 1.3, log(peak / range),
+// (background - min) / range; AS3D the same with sigma_x and then sigma_y - 1.3.
+__host__ __device__ constexpr int used_outputs(int loc_type) { return loc_type == QCS_LOCTYPE_AS3D ? 6 : 5; }
+// Start point per record: GS2D peak e-, x, y, sigma, background e-; AS3D
+// peak e-, x, y, sigma_x, sigma_y, background e- (the fit's parameter order).
+__host__ __device__ constexpr int start_width(int loc_type) { return loc_type == QCS_LOCTYPE_AS3D ? 6 : 5; }
+constexpr int param_count(int kin) {
+    return kin * kHidden + kHidden + kHidden * kHidden + kHidden + kHidden * kOut + kOut;
+}
+inline bool shape_supported(int loc_type, int R) {
+    return (loc_type == QCS_LOCTYPE_GS2D || loc_type == QCS_LOCTYPE_AS3D) && (R == 7 || R == 9 || R == 11);
+}
+
+// loss weight of each start-point output (positions matter most) and of the
+// emitter-count cross-entropy
+__constant__ const float kTargetWeight[kUsedMax] = {4.0f, 4.0f, 1.0f, 1.0f, 1.0f, 1.0f};
 constexpr float kCountWeight = 0.5f;
 
 // Emitter-count class from the three logits: 2 when p(class 2) >= th, else 1
@@ -40,11 +49,10 @@ __host__ __device__ inline int count_class(float l0, float l1, float l2, float t
     return 0;
 }
 
-// Start points (peak e-, x, y, sigma, background e- per record) of n device
-// records into out (n x 5 floats); with cls set, also each record's
-// emitter-count class at the network's count threshold.  With n_dev set the
-// fused kernel reads the record count there (at most n); the layer-by-layer
-// path computes all n.
+// Start points (start_width floats per record) of n device records into out;
+// with cls set (GS2D networks), also each record's emitter-count class at the
+// network's count threshold.  With n_dev set the fused kernel reads the
+// record count there (at most n); the layer-by-layer path computes all n.
 cudaError_t start_points(qcs_learned_net *net, const qcs_loc_para *p, const uint16_t *d_rois, int n, float *out,
                          cudaStream_t s, uint8_t *cls = nullptr, const int *n_dev = nullptr);
 

@@ -121,6 +121,8 @@ _SIGS = {
                                                   C.c_void_p]),
     "qcs_loc_count_labels_device": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "qcs_learned_set_count_threshold": (C.c_int, [C.c_void_p, C.c_float]),
+    "qcs_learned_create_for": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_ulonglong, C.POINTER(C.c_void_p)]),
+    "qcs_learned_shape": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "qcs_learned_localize_device_n": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(LocPara),
                                                 C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_void_p]),
     "qcs_learned_count_threshold": (C.c_float, [C.c_void_p]),
@@ -411,15 +413,28 @@ class ZeroRemover:
                                               C.c_void_p(stream) if stream else None))
 
 
-class LearnedNet:
-    """Learned start points for GS2D 7x7 fits (qcs_learned_*): device tensors are torch CUDA tensors."""
+def learned_in_width(roi_size):
+    """Network input width for an R x R ROI (R*R pixels + 2 scale features, padded)."""
+    return 64 if roi_size * roi_size + 2 <= 64 else 128
 
-    def __init__(self, batch=4096, seed=1):
+
+def learned_start_width(loc_type):
+    """Start-point floats per record: GS2D 5, AS3D 6."""
+    return 6 if loc_type == 1 else 5
+
+
+class LearnedNet:
+    """Learned start points (qcs_learned_*) for one localization type and ROI
+    size (GS2D or AS3D; 7, 9 or 11): device tensors are torch CUDA tensors."""
+
+    def __init__(self, batch=4096, seed=1, loc_type=0, roi_size=7):
         self.lib = load()
         h = C.c_void_p()
-        check(self.lib.qcs_learned_create(int(batch), int(seed), C.byref(h)))
+        check(self.lib.qcs_learned_create_for(int(loc_type), int(roi_size), int(batch), int(seed), C.byref(h)))
         self.h = h
-        self.n_params = self.lib.qcs_learned_param_count()
+        lt, rs, npar = C.c_int(0), C.c_int(0), C.c_int(0)
+        check(self.lib.qcs_learned_shape(h, C.byref(lt), C.byref(rs), C.byref(npar)))
+        self.loc_type, self.roi_size, self.n_params = lt.value, rs.value, npar.value
 
     def close(self):
         if self.h:
@@ -450,7 +465,7 @@ class LearnedNet:
     @staticmethod
     def features(para, d_rois, n, stream=0):
         import torch
-        feat = torch.empty((n, 64), dtype=torch.float32, device="cuda")
+        feat = torch.empty((n, learned_in_width(para.ROISize)), dtype=torch.float32, device="cuda")
         scale = torch.empty((n, 2), dtype=torch.float32, device="cuda")
         check(load().qcs_learned_features_device(C.byref(para), C.c_void_p(d_rois), int(n), C.c_void_p(feat.data_ptr()),
                                                  C.c_void_p(scale.data_ptr()), C.c_void_p(stream) if stream else None))
@@ -459,7 +474,7 @@ class LearnedNet:
     @staticmethod
     def targets(para, d_rois, d_rows, scale, n, stream=0):
         import torch
-        t = torch.empty((n, 5), dtype=torch.float32, device="cuda")
+        t = torch.empty((n, 6 if para.LocType == 1 else 5), dtype=torch.float32, device="cuda")
         v = torch.empty((n,), dtype=torch.float32, device="cuda")
         check(load().qcs_learned_targets_device(C.byref(para), C.c_void_p(d_rois), C.c_void_p(d_rows),
                                                 C.c_void_p(scale.data_ptr()), int(n), C.c_void_p(t.data_ptr()),
@@ -510,7 +525,7 @@ class LearnedNet:
 
     def start(self, para, d_rois, n, stream=0):
         import torch
-        st = torch.empty((n, 5), dtype=torch.float32, device="cuda")
+        st = torch.empty((n, learned_start_width(self.loc_type)), dtype=torch.float32, device="cuda")
         work = torch.empty((int(self.lib.qcs_learned_work_bytes(int(n))) // 4 + 1,), dtype=torch.float32,
                            device="cuda")
         check(self.lib.qcs_learned_start_device(self.h, C.byref(para), C.c_void_p(d_rois), int(n),

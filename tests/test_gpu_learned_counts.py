@@ -79,7 +79,8 @@ def test_count_loss_gradient_and_classes_match_oracle(cuda_ok):
     import torch
     s = torch.cuda.Stream()
     rows, _, labels = plain_multi(ctx, d, n, s)
-    t, v = qlib.LearnedNet.targets(para, d.data_ptr(), to_dev(rows[:n].astype(np.float32)).data_ptr(), scale, n)
+    d_rows = to_dev(rows[:n].astype(np.float32))  # kept alive while the kernel reads it
+    t, v = qlib.LearnedNet.targets(para, d.data_ptr(), d_rows.data_ptr(), scale, n)
     cls = np.random.default_rng(0).integers(-1, 3, n).astype(np.float32)
     d_cls = to_dev(cls)
     net = qlib.LearnedNet(batch=512, seed=3)
