@@ -539,6 +539,127 @@ def learned_measure(args, streams, ctxs, para, d_batches, h_batches, rec0, truth
     }
 
 
+SHAPE_RECORDS = 100_000    # records per call of the other learned workloads
+SHAPE_TRAIN = 200_000
+SHAPE_STEPS = 20
+
+
+def multi_truth_match(rows, rec, truth, R, first_frame=1):
+    """Each localization's distance (px) to the nearest true emitter of its
+    record (record = frame - first_frame), in ROI coordinates."""
+    rows = rows[rows[:, 0] > 0]
+    rid = rows[:, 11].astype(np.int64) - first_frame
+    fx = rows[:, 1] - rec[rid, R * R].astype(np.float64) + R // 2
+    fy = rows[:, 2] - rec[rid, R * R + 1].astype(np.float64) + R // 2
+    dx = truth["x"][rid] - fx[:, None]
+    dy = truth["y"][rid] - fy[:, None]
+    d = np.sqrt(np.nanmin(dx * dx + dy * dy, axis=1))
+    ok = d < 1.0
+    return {"localizations": int(rows.shape[0]), "matched": int(ok.sum()),
+            "rmse_px": float(np.sqrt(np.mean(d[ok] ** 2)))}
+
+
+def shape_accuracy(kind, plain, learned, rec, truth, R):
+    """Plain against learned on the same records: AS3D x/y (px) and z (nm)
+    RMSE over the records both accept; multi-emitter localizations within
+    1 px of a true emitter and their RMSE."""
+    if kind == "multi":
+        return {"plain": multi_truth_match(plain, rec, truth, R), "learned": multi_truth_match(learned, rec, truth, R),
+                "basis": "localizations within 1 px of a true emitter of their record"}
+    both = (plain[:, 0] > 0) & (learned[:, 0] > 0)
+
+    def rm(rows):
+        fx = rows[both, 1] + R // 2 - rec[both, R * R].astype(np.float64)
+        fy = rows[both, 2] + R // 2 - rec[both, R * R + 1].astype(np.float64)
+        xy = float(np.sqrt(np.mean((fx - truth["x"][both]) ** 2 + (fy - truth["y"][both]) ** 2) / 2))
+        z = float(np.sqrt(np.mean((rows[both, 3] - truth["z"][both]) ** 2)))
+        return {"rmse_px": xy, "z_rmse_nm": z, "accepted": float((rows[:, 0] > 0).mean())}
+    return {"plain": rm(plain), "learned": rm(learned), "compared": int(both.sum()),
+            "basis": "records accepted by both; ground truth of the generator"}
+
+
+def learned_shapes_measure(streams, dist, world, rank):
+    """The learned path on the other configurations' generators, each against
+    plain fitting of the same device-resident records with two contexts in
+    turn: astigmatic 3D 9x9 ROIs (single-emitter fits from sigma_x / sigma_y
+    start points, 3 iterations of 6 line-search steps against the reference's
+    11 of 11) and 1-3 emitter 11x11 ROIs with multi-emitter fitting (learned
+    single-emitter stage, 2 x 6, and emitter-count classes routing records
+    straight to the 2E / 3E fits).  Networks trained on the GPU on
+    SHAPE_TRAIN records of other seeds labelled by plain fitting."""
+    import torch
+    from qcstorm_b200 import lib, synth
+    s0 = streams[0]
+    sh = s0.cuda_stream
+    out = {}
+    for kind, gen, R, iters, bis in (("as3d", synth.as3d_rois, 9, 3, 6), ("multi", synth.multi_rois, 11, 2, 6)):
+        t0 = time.perf_counter()
+        tr, para, _ = gen(SHAPE_TRAIN, R=R, seed=7000 + 10 * rank)
+        d_tr = torch.from_numpy(tr.view(np.int16)).cuda()
+        ctx_tr = lib.LocContext(para, capacity=SHAPE_TRAIN)
+        ctx_tr.localize_device(d_tr.data_ptr(), SHAPE_TRAIN, 0, sh)
+        labels = lib.count_labels(ctx_tr, SHAPE_TRAIN, sh) if kind == "multi" else None
+        feat, scale = lib.LearnedNet.features(para, d_tr.data_ptr(), SHAPE_TRAIN, stream=sh)
+        tgt, valid = lib.LearnedNet.targets(para, d_tr.data_ptr(), ctx_tr.device_rows(), scale, SHAPE_TRAIN,
+                                            stream=sh)
+        s0.synchronize()
+        if labels is not None:
+            valid = valid * (labels == 0).float()
+        torch.cuda.synchronize()
+        net = lib.LearnedNet(batch=4096, seed=5, loc_type=para.LocType, roi_size=R)
+        net.train(feat, tgt, valid, epochs=TRAIN_EPOCHS, lr=2e-3, stream=sh, classes=labels)
+        if kind == "multi":
+            net.set_count_threshold(0.5)
+        torch.cuda.synchronize()
+        ctx_tr.close()
+        del d_tr, feat, scale, tgt, valid, labels
+        train_s = time.perf_counter() - t0
+
+        recs, truths, d_b = [], [], []
+        for b in range(2):
+            rec, _, truth = gen(SHAPE_RECORDS, R=R, seed=8000 + 10 * rank + b)
+            recs.append(rec)
+            truths.append(truth)
+            d_b.append(torch.from_numpy(rec.view(np.int16)).cuda())
+        ctxs = [lib.LocContext(para, capacity=SHAPE_RECORDS) for _ in range(2)]
+
+        def plain(k, s, c=None):
+            (c or ctxs[k % 2]).localize_device(d_b[k % 2].data_ptr(), SHAPE_RECORDS, 0, s.cuda_stream)
+
+        def learned(k, s, c=None):
+            net.localize(c or ctxs[k % 2], d_b[k % 2].data_ptr(), SHAPE_RECORDS, iters=iters, bisections=bis,
+                         stream=s.cuda_stream)
+
+        ms_p = device_timed(SHAPE_STEPS, 3, plain, streams, dist)
+        ms_l = device_timed(SHAPE_STEPS, 3, learned, streams, dist)
+        plain(0, s0, ctxs[0])
+        rows_p, ratios_p = ctxs[0].read_rows(sh)
+        learned(0, s0, ctxs[0])
+        rows_l, ratios_l = ctxs[0].read_rows(sh)
+        refits = net.refits(ctxs[0])
+        net.fused_status()
+        out[kind] = {
+            "workload": ("astigmatic 3D 9x9 ROIs, z U(-600,600) nm, photons log-U[1000,8000], background U(20,150), "
+                         "camera ADU (offset 100, 0.45 e-/ADU)" if kind == "as3d" else
+                         "11x11 ROIs with 1/2/3 emitters (p 0.5/0.3/0.2) 1-3 px apart, multi-emitter fitting on"),
+            "records_per_call": SHAPE_RECORDS,
+            "plain_fits_per_s": job_rate(SHAPE_STEPS, SHAPE_RECORDS, world, ms_p),
+            "learned_fits_per_s": job_rate(SHAPE_STEPS, SHAPE_RECORDS, world, ms_l),
+            "vs_plain": ms_p / ms_l,
+            "schedule": "%d BFGS iterations x %d line-search steps (plain: the reference's %s)" % (
+                iters, bis, "11 x 11" if kind == "as3d" else "8 x 11 single, 13 x 11 2E, 16 x 11 3E"),
+            "refits_per_call": refits,
+            "single_emitter_fits_per_call": {"plain": int(round(float(ratios_p[0]) * SHAPE_RECORDS)),
+                                             "learned": int(round(float(ratios_l[0]) * SHAPE_RECORDS))},
+            "accuracy": shape_accuracy(kind, rows_p, rows_l, recs[0], truths[0], R),
+            "train": {"records": SHAPE_TRAIN, "epochs": TRAIN_EPOCHS, "seconds": train_s},
+        }
+        for c in ctxs:
+            c.close()
+        net.close()
+    return out
+
+
 def profile_learned(n, stream):
     """Three learned-start localization calls over n records inside the NVTX
     range "learned" (for ncu --nvtx-include learned/), after training."""
@@ -718,6 +839,10 @@ def main():
     if not args.no_learned:
         learned = learned_measure(args, streams, ctxs, para, d_batches, h_batches, rec0, truth0, value, world, dist)
 
+    shapes = None
+    if not args.no_learned:
+        shapes = learned_shapes_measure(streams, dist, world, rank)
+
     frames = None
     if not args.no_frames:
         fsteps = min(max(args.steps // 40, 5), 40)
@@ -746,7 +871,8 @@ def main():
                          "kernel_ms": fit_ms,
                          "algorithmic": "%d px-evals x %d MUFU per fit; peak = measured __expf/__logf rate" % (
                              PX_EVALS_PER_FIT, MUFU_PER_PX_EVAL)},
-            "cpu_baseline": cpu, "clocks": clocks, "learned": learned, "frames": frames,
+            "cpu_baseline": cpu, "clocks": clocks, "learned": learned, "learned_other_configs": shapes,
+            "frames": frames,
         }
         print(json.dumps(line), flush=True)
     for c in ctxs:

@@ -429,7 +429,7 @@ size_t qcs_learned_work_bytes(int n);
  * `bisections` line-search steps each (<= 0: the reference's 11; schedules:
  * 2..4 iterations of 6 steps or 3 of 11; GS2D 7x7 also 2..5 or 8 of 11 and 2
  * or 3 of 4 or 8) and the loss's analytic gradient; fits that are not
- * accepted or whose Poisson deviance exceeds dev_th (<= 0: 100) are refitted
+ * accepted or whose Poisson deviance exceeds dev_th (<= 0: 2 R^2 + 2, 100 for 7x7) are refitted
  * by the plain kernel; then CRLB.  Rows in the context (n).  With
  * p->MultiEmitterFitEn the single-emitter fit is the first stage of the
  * reference's cascade (bfgs_top.cu:26-204): it runs over the single-emitter

@@ -278,6 +278,10 @@ int learned_kind(const qcs_loc_para *p) {
     if (p->LocType == QCS_LOCTYPE_AS3D && !p->MultiEmitterFitEn) return qcs::kAS3D;
     return -1;
 }
+// Deviance bound of the learned fits' judge: a good fit's unweighted Poisson
+// deviance is near a chi-square with about R*R degrees of freedom, so the
+// bound scales with the pixel count (100 for 7x7 ROIs).
+float default_dev_th(int R) { return 2.0f * (float)(R * R) + 2.0f; }
 const char *kLearnedShapes = "start-point fits: GS2D or AS3D, ROISize 7, 9 or 11 (multi-emitter fitting: GS2D)";
 const char *kLearnedSchedules =
     "schedule: 2..4 iterations of 6 bisections or 3 of 11 (GS2D 7x7 also 2..5 or 8 of 11, 2 or 3 of 4 or 8)";
@@ -351,7 +355,7 @@ int qcs_fit_from_start_classes_device(qcs_loc_data *c, const uint16_t *d_rois, c
     if (!qcs::learned_schedule_supported(kind, p->ROISize, iters, bisections)) return fail(QCS_ERR_ARG, kLearnedSchedules);
     if (n == 0) return QCS_OK;
     if (!d_rois || !d_start) return fail(QCS_ERR_ARG, "null pointer");
-    if (!(dev_th > 0.0f)) dev_th = 100.0f;
+    if (!(dev_th > 0.0f)) dev_th = default_dev_th(p->ROISize);
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
     const float *wle = d_wle;
     if (!wle) {
@@ -434,7 +438,7 @@ int qcs_learned_localize_device_n(qcs_loc_data *c, qcs_learned_net *net, const u
     if (bisections <= 0) bisections = 11;
     if (!qcs::learned_schedule_supported(qcs::kGS2D, p->ROISize, iters, bisections))
         return fail(QCS_ERR_ARG, kLearnedSchedules);
-    if (!(dev_th > 0.0f)) dev_th = 100.0f;
+    if (!(dev_th > 0.0f)) dev_th = default_dev_th(p->ROISize);
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
     uint8_t *cls = qcs_learned_count_threshold(net) > 0.0f ? c->d_cls : nullptr;
     if (max_n == 0) return QCS_OK;
