@@ -49,7 +49,7 @@ template <int R>
 __device__ __forceinline__ void record_range(const uint16_t *r, float offset, float kadc, float &lo, float &rng) {
     float hi = -1e30f;
     lo = 1e30f;
-#pragma unroll 7
+#pragma unroll
     for (int k = 0; k < R * R; ++k) {
         const float e = fmaxf(((float)r[k] - offset) * kadc, 1.0f);
         lo = fminf(lo, e);
@@ -521,7 +521,41 @@ __global__ void __launch_bounds__(128, 1) mlp_tc_kernel(const uint16_t *__restri
         }
         // features of this thread's ROI into A1 (row tid)
         float lo = 1.0f, rng = 1.0f;
-        {
+        if constexpr (R == 7) {
+            // 7x7: the 56-word record in registers (seven 16-byte loads from
+            // shared memory), features in one pass
+            float f[KIN];
+#pragma unroll
+            for (int k = 0; k < KIN; ++k) f[k] = 0.0f;
+            if (tid < rows) {
+                uint16_t px[WHOLE];
+                if (BULK) {
+                    const uint4 *r4 = reinterpret_cast<const uint4 *>(srec + (size_t)tid * WHOLE);
+#pragma unroll
+                    for (int q = 0; q < WHOLE / 8; ++q) {
+                        const uint4 u = r4[q];
+                        const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+                        for (int h = 0; h < 4; ++h) {
+                            px[q * 8 + 2 * h] = (uint16_t)(w[h] & 0xFFFFu);
+                            px[q * 8 + 2 * h + 1] = (uint16_t)(w[h] >> 16);
+                        }
+                    }
+                } else {
+                    const uint16_t *r = rois + (size_t)i * WHOLE;
+#pragma unroll
+                    for (int k = 0; k < R * R; ++k) px[k] = r[k];
+                }
+                record_range<R>(px, offset, kadc, lo, rng);
+                const float inv = 1.0f / rng;
+                const float f_rng = logf(rng) * 0.125f, f_lo = logf(lo) * 0.125f;
+#pragma unroll
+                for (int k = 0; k < R * R + 2; ++k) f[k] = feature<R>(px, k, offset, kadc, lo, inv, f_rng, f_lo);
+            }
+#pragma unroll
+            for (int kg = 0; kg < KIN / 8; ++kg)
+                *reinterpret_cast<uint4 *>(base + L::OFF_A1 + (size_t)(kg * kM + tid) * 16) = pack8(f + 8 * kg);
+        } else {
             const uint16_t *r = BULK ? srec + (size_t)tid * WHOLE : rois + (size_t)i * WHOLE;
             float inv = 0.0f, f_rng = 0.0f, f_lo = 0.0f;
             const bool live = tid < rows;
