@@ -367,6 +367,28 @@ def frame_pipeline(stream, steps, warmup, e2e=True, dist=None, world=1, net=None
     e1.record(stream)
     torch.cuda.synchronize()
     ms = max_over_ranks(e0.elapsed_time(e1), dist) / steps
+    # the same call sequence captured once in a CUDA graph and replayed
+    # (every frame pointer repeats each call: 32 frames per call over 8 distinct)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g, stream=stream, capture_error_mode="relaxed"):
+        step(0)
+    with torch.cuda.stream(stream):
+        for _ in range(warmup):
+            g.replay()
+    torch.cuda.synchronize()
+    g0 = torch.cuda.Event(enable_timing=True)
+    g1 = torch.cuda.Event(enable_timing=True)
+    g0.record(stream)
+    with torch.cuda.stream(stream):
+        for _ in range(steps):
+            g.replay()
+    g1.record(stream)
+    torch.cuda.synchronize()
+    ms_graph = max_over_ranks(g0.elapsed_time(g1), dist) / steps
+    rows_g, _ = loc.read_rows(sh)
+    assert rows_g.shape == rows0.shape
+    del g
     e2e_steps = max(3, steps // 4) if e2e else 1
     t0 = time.perf_counter()
     out_rows = 0
@@ -385,6 +407,9 @@ def frame_pipeline(stream, steps, warmup, e2e=True, dist=None, world=1, net=None
         "frames_per_s": world * FRAMES_PER_CALL * 1e3 / ms, "ms_per_call": ms, "frames_per_call": FRAMES_PER_CALL,
         "records_per_call": recs0, "rows_per_call": int(rows0.shape[0]),
         "single_emitter_fits_per_call": int(round(float(ratios0[0]) * recs0)),
+        "graph": {"frames_per_s": world * FRAMES_PER_CALL * 1e3 / ms_graph, "ms_per_call": ms_graph,
+                  "note": "one call (reset, %d extractions, localization) captured in a CUDA graph and replayed"
+                          % FRAMES_PER_CALL},
         "localizations_per_s": world * rows0.shape[0] * 1e3 / ms, "steps": steps,
         "accuracy": dict(accuracy, basis="first call's localizations against the generator's emitters of their "
                                          "frames (nearest within 1 px)"),

@@ -840,16 +840,28 @@ cudaError_t fused_start_points(qcs_learned_net *net, const qcs_loc_para *p, cons
         const int per_sm = Lay::SMEM <= 113 * 1024 ? 2 : 1;
         const int grid = tiles < per_sm * sms ? tiles : per_sm * sms;
         // the weight image is rebuilt only after a parameter change; calls on
-        // other streams wait for the build that made the current one
+        // other streams wait for the build that made the current one.  Under
+        // stream capture a stale image is rebuilt inside the graph (and again
+        // by the next call outside it), and a current one must have been
+        // built already: an event recorded outside a capture cannot be waited
+        // on inside it.
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        e2 = cudaStreamIsCapturing(s, &cs);
+        if (e2 != cudaSuccess) return e2;
+        const bool capturing = cs != cudaStreamCaptureStatusNone;
         if (net->wimg_version != net->version) {
             L::tc::weight_image_kernel<Lay::KIN><<<blocks(Lay::W1 + Lay::W2 + Lay::W3), 256, 0, s>>>(net->d_par,
                                                                                                   net->d_wimg);
-            e2 = cudaEventRecord(net->wimg_ready, s);
-            if (e2 != cudaSuccess) return e2;
-            net->wimg_version = net->version;
-        } else {
+            if (!capturing) {
+                e2 = cudaEventRecord(net->wimg_ready, s);
+                if (e2 != cudaSuccess) return e2;
+                net->wimg_version = net->version;
+            }
+        } else if (!capturing) {
             e2 = cudaStreamWaitEvent(s, net->wimg_ready, 0);
             if (e2 != cudaSuccess) return e2;
+        } else if (cudaEventQuery(net->wimg_ready) != cudaSuccess) {
+            return cudaErrorNotReady;  // the build is still in flight: synchronize before capturing
         }
         kern<<<grid, 128, Lay::SMEM, s>>>(d_rois, n, p->Offset, p->KAdc, reinterpret_cast<const uint4 *>(net->d_wimg),
                                           w.b1, w.b2, w.b3, start, cls, th, n_dev, net->d_err);
