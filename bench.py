@@ -685,6 +685,51 @@ def learned_shapes_measure(streams, dist, world, rank):
     return out
 
 
+CONSEC_FRAMES_PER_GROUP = 32
+CONSEC_GROUPS = 8
+
+
+def consec_measure(stream, dist, world):
+    """Consecutive-frame merging (qcs_consec_fit_device) of localization rows
+    of blinking molecules, ~3,000 rows per 2048 x 2048 frame, groups of
+    CONSEC_FRAMES_PER_GROUP frames as the plug-ins write them (each call
+    merges the previous group with the new one and CRLBs the rows that
+    leave): rows/s over CONSEC_GROUPS calls, CUDA events on the call's
+    stream (the call synchronizes at its end, as the reference's does)."""
+    import torch
+    from qcstorm_b200 import lib, synth
+    from qcstorm_b200.abi import default_para
+    rows, counts = synth.blinking_rows(n_emitters=7500, frames=CONSEC_FRAMES_PER_GROUP * 2, seed=3, width=2048)
+    sizes = synth.group_sizes(counts, CONSEC_FRAMES_PER_GROUP)
+    para = default_para(LocType=0, ConsecFit_DistanceTh_nm=80.0, PixelSize=100.0, QE=0.72)
+    cap = int(sizes.max())
+    cf = lib.ConsecFit(capacity=cap)
+    d = [torch.from_numpy(rows[o:o + k].copy()).cuda() for o, k in zip(np.r_[0, np.cumsum(sizes)[:-1]], sizes)]
+    sh = stream.cuda_stream
+    torch.cuda.synchronize()
+    for g in range(3):
+        cf.fit_device(d[g % 2].data_ptr(), int(sizes[g % 2]), para, stream=sh)
+    merged = cf.fit_device(d[1].data_ptr(), int(sizes[1]), para, stream=sh)
+    zeroed = int((cf.read_rows()[:, 0] == 0).sum())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    total = 0
+    for g in range(CONSEC_GROUPS):
+        cf.fit_device(d[g % 2].data_ptr(), int(sizes[g % 2]), para, stream=sh)
+        total += int(sizes[g % 2])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), dist) / CONSEC_GROUPS
+    cf.close()
+    return {"workload": "rows of 7,500 blinking molecules over 2048 x 2048 frames (~%d rows per frame), %d frames "
+                        "per call, threshold 80 nm at 100 nm pixels" % (int(counts.mean()), CONSEC_FRAMES_PER_GROUP),
+            "rows_per_call": int(total / CONSEC_GROUPS), "ms_per_call": ms,
+            "rows_per_s": world * total / (ms * 1e-3 * CONSEC_GROUPS),
+            "rows_zeroed_per_call": zeroed, "rows_out_per_call": merged,
+            "call": "qcs_consec_fit_device (link by sorted (frame, y) search, merge, remove, CRLB)"}
+
+
 def profile_learned(n, stream):
     """Three learned-start localization calls over n records inside the NVTX
     range "learned" (for ncu --nvtx-include learned/), after training."""
@@ -864,6 +909,8 @@ def main():
     if not args.no_learned:
         learned = learned_measure(args, streams, ctxs, para, d_batches, h_batches, rec0, truth0, value, world, dist)
 
+    consec = consec_measure(stream, dist, world)
+
     shapes = None
     if not args.no_learned:
         shapes = learned_shapes_measure(streams, dist, world, rank)
@@ -897,6 +944,7 @@ def main():
                          "algorithmic": "%d px-evals x %d MUFU per fit; peak = measured __expf/__logf rate" % (
                              PX_EVALS_PER_FIT, MUFU_PER_PX_EVAL)},
             "cpu_baseline": cpu, "clocks": clocks, "learned": learned, "learned_other_configs": shapes,
+            "consecutive_fit": consec,
             "frames": frames,
         }
         print(json.dumps(line), flush=True)

@@ -315,6 +315,37 @@ int qcs_zero_valid_num(const qcs_zero_data *c);
 int qcs_zero_remove_device(qcs_zero_data *c, const float *d_rows, int n, const int *d_n, int sort_frame_en,
                            int first_frame, int end_frame, float *d_out, int *d_nvalid, void *stream);
 
+/* ---- consecutive-frame merging: ConsecutiveFit_TypeDef -------------------- */
+#define QCS_ONTIME_BINS 10 /* MaxOnTimeConsecutiveNum (StatisticsInfo/statisticsInfo.h:53) */
+typedef struct qcs_consec qcs_consec;
+/* ConsecutiveFit_TypeDef::Init (ConsecutiveFit/ConsecutiveFit_top.cu:101-131):
+ * groups of at most `capacity` rows (<= 0: 2 x QCS_MAX_POINT_NUM). */
+int qcs_consec_init(int capacity, qcs_consec **out);
+int qcs_consec_deinit(qcs_consec *c);
+/* ConsecutiveFit_TypeDef::ConsecutiveFit_WeightedAvg (ConsecutiveFit_top.cu:22-98):
+ * merges the n frame-sorted host rows of this group (RemoveZeroLocalizations
+ * with frame sorting leaves them so) with the previous call's group: rows in
+ * consecutive frames whose integer positions are closer than
+ * ConsecFit_DistanceTh_nm / PixelSize pixels form chains; each chain's first
+ * row takes the summed photons and background and the averages of x, y, z and
+ * the widths weighted by 10 / CRLB_x, the other rows are zeroed; CRLB
+ * recomputed for the rows that leave.  Output (qcs_consec_h_out_loc_arry,
+ * qcs_consec_out_num rows): the previous group, or with is_end everything.
+ * QCS_ERR_CAPACITY above the capacity.  Synchronous, like the reference. */
+int qcs_consec_fit(qcs_consec *c, const float *h_rows, int n, int is_end, const qcs_loc_para *p, void *stream);
+/* The same with the group's rows in device memory; the output rows stay on
+ * the device (qcs_consec_d_out_loc_arry). */
+int qcs_consec_fit_device(qcs_consec *c, const float *d_rows, int n, int is_end, const qcs_loc_para *p,
+                          void *stream);
+int qcs_consec_out_num(const qcs_consec *c);                 /* OutFluoNum */
+const float *qcs_consec_h_out_loc_arry(const qcs_consec *c); /* h_OutLocArry (pinned, valid until the next call) */
+const float *qcs_consec_d_out_loc_arry(const qcs_consec *c);
+/* Copies the last call's qcs_consec_out_num output rows from the device into h_out. */
+int qcs_consec_read_rows(qcs_consec *c, float *h_out);
+/* h_OntimeRatio of the last call: chains starting in the new group by length
+ * 1..10 frames (the last bin: 10 or more), over their number. */
+int qcs_consec_ontime_ratio(const qcs_consec *c, float *out10);
+
 /* ---- WLE pre-pass: WLEParameterEstimation_TypeDef ---------------------- */
 /* WLEParameterEstimation_TypeDef::WLEParameterEstimate (WLEParaEstimation.h:41,
  * WLEParaEstimation.cpp:20-40): PSF width, same-frame nearest neighbour and

@@ -5,7 +5,7 @@ Compiles the reference's own CUDA sources (MLEbfgs/bfgs_MLE_dll x64/bfgsMLE_dll/
 bfgsMLE_dll/) with g++ against the host shim in oracle/refshim/, links them with
 oracle/ref_harness.cpp and writes oracle/_ref/libqcs_ref_host.so.  The result
 runs the reference's fit kernels, WLE pre-pass, CRLB, cascade orchestration,
-ROI extraction and super-resolution render on the CPU, one emulated CUDA block
+ROI extraction, super-resolution render and consecutive-frame merging on the CPU, one emulated CUDA block
 at a time; it is the checker
 the CPU oracle (oracle/qcs_oracle.c) is pinned against.
 
@@ -53,7 +53,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 # Reference sub-directories and translation units of the localization path.
 DIRS = ["bfgsMLE_Loc_LD", "bfgsMLE_Loc_HD", "bfgsMLE_Loc_top", "WLEParaEstimation",
-        "SubregionExtraction", "cudaWrapper", "ImgRender"]
+        "SubregionExtraction", "cudaWrapper", "ImgRender", "ConsecutiveFit", "StatisticsInfo"]
 UNITS = [
     "bfgsMLE_Loc_LD/bfgs_base.cu",
     "bfgsMLE_Loc_LD/bfgsMLE_Single_Emitter_Fit.cu",
@@ -71,6 +71,8 @@ UNITS = [
     "ImgRender/ImageRender_3d.cu",
     "ImgRender/ImageRender_top.cu",
     "ImgRender/ImageRerender_rc.cu",
+    "ConsecutiveFit/ConsecutiveFit.cu",
+    "ConsecutiveFit/ConsecutiveFit_top.cu",
 ]
 
 LAUNCH = re.compile(

@@ -73,6 +73,12 @@ int qcso_render(const qcs_loc_para *p, const float *rows, int n, int mode, float
 int qcso_zero_remove(const float *rows, int n, int sort_frame, int first_frame, int end_frame, float *out,
                      int *n_out);
 
+/* ConsecutiveFit_WeightedAvg over n_groups groups of sizes[g] rows in turn (is_end[g]: the call's
+ * IsEndProc); each call's output rows back to back in out, their count in out_n[g], its 10 on-time
+ * ratios at ontime[10 g]; gpu_rounding: fused weighted sums and GPU float-to-int truncation. */
+int qcso_consec(const qcs_loc_para *p, const float *rows, const int *sizes, const int *is_end, int n_groups,
+                int gpu_rounding, float *out, int *out_n, float *ontime);
+
 #ifdef __cplusplus
 }
 #endif

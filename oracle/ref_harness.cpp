@@ -10,6 +10,7 @@
 //   qcsref_crlb        GaussianCRLB_Calc_top (LocPrecCalc_GaussianCRLB.h:65-128)
 //   qcsref_wle         WLEParameterEstimation_TypeDef::WLEParameterEstimate
 //   qcsref_zero_remove ZeroLocalizationsRemovel_TypeDef::RemoveZeroLocalizations
+//   qcsref_consec      ConsecutiveFit_TypeDef::ConsecutiveFit_WeightedAvg over a sequence of groups
 //                      (WLEParaEstimation.cpp:20-40)
 //   qcsref_extract     LDROIExtractData_TypeDef::ExtractMolecules (LDROIExtraction.cu:30-80)
 #include <cstdio>
@@ -23,6 +24,7 @@
 #include "bfgsMLE_AS3D_core.h"
 #include "LocPrecCalc_GaussianCRLB.h"
 #include "ZeroLocalizationsRemove.h"
+#include "ConsecutiveFit.h"
 #include "ImageRender_2d.h"
 #include "ImageRender_3d.h"
 
@@ -245,6 +247,33 @@ int qcsref_zero_remove(const float *rows, int n, int sort_frame, int first_frame
     *n_out = z.ValidFluoNum;
     memcpy(out, z.h_LocArry, sizeof(float) * 12 * (size_t)z.ValidFluoNum);
     z.Deinit();
+    return 0;
+}
+
+// ConsecutiveFit_TypeDef::ConsecutiveFit_WeightedAvg (ConsecutiveFit_top.cu:22-98)
+// called once per group on one object: group g is sizes[g] rows (<= MaxPointNum)
+// taken in turn from rows, the call's IsEndProc is is_end[g]; each call's
+// OutFluoNum rows go to out back to back, their count to out_n[g] and the
+// call's h_OntimeRatio (MaxOnTimeConsecutiveNum floats) to ontime[g * 10].
+int qcsref_consec(const qcs_loc_para *p, const float *rows, const int *sizes, const int *is_end, int n_groups,
+                  float *out, int *out_n, float *ontime) {
+    for (int g = 0; g < n_groups; ++g)
+        if (sizes[g] < 0 || sizes[g] > MaxPointNum) return -1;
+    LocalizationPara r;
+    to_ref(p, r);
+    ConsecutiveFit_TypeDef cf;
+    cf.Init();
+    size_t off = 0, oo = 0;
+    for (int g = 0; g < n_groups; ++g) {
+        std::vector<float> in(rows + off * 12, rows + (off + (size_t)sizes[g]) * 12);
+        cf.ConsecutiveFit_WeightedAvg(in.data(), sizes[g], is_end[g], r, nullptr);
+        out_n[g] = cf.OutFluoNum;
+        memcpy(out + oo * 12, cf.h_OutLocArry, sizeof(float) * 12 * (size_t)cf.OutFluoNum);
+        memcpy(ontime + (size_t)g * MaxOnTimeConsecutiveNum, cf.h_OntimeRatio, sizeof(float) * MaxOnTimeConsecutiveNum);
+        oo += (size_t)cf.OutFluoNum;
+        off += (size_t)sizes[g];
+    }
+    cf.Deinit();
     return 0;
 }
 

@@ -12,6 +12,7 @@
 //   qcsrefg_wle         WLEParameterEstimation_TypeDef::WLEParameterEstimate
 //   qcsrefg_extract     LDROIExtractData_TypeDef::ExtractMolecules
 //   qcsrefg_zero_remove ZeroLocalizationsRemovel_TypeDef::RemoveZeroLocalizations
+//   qcsrefg_consec     ConsecutiveFit_TypeDef::ConsecutiveFit_WeightedAvg over a sequence of groups
 // Every entry point returns 0, or the CUDA error code of the first failure.
 #include <cstdio>
 #include <cstring>
@@ -27,6 +28,7 @@
 #include "bfgsMLE_AS3D_2Emitter_core.h"
 #include "LocPrecCalc_GaussianCRLB.h"
 #include "ZeroLocalizationsRemove.h"
+#include "ConsecutiveFit.h"
 #include "ImageRender_2d.h"
 #include "ImageRender_3d.h"
 
@@ -384,6 +386,38 @@ int qcsrefg_zero_remove(const float *rows, int n, int sort_frame, int first_fram
     cudaStreamDestroy(s);
     cudaFreeHost(pinned);
     z.Deinit();
+    return st;
+}
+
+// qcsref_consec on the GPU build.
+int qcsrefg_consec(const qcs_loc_para *p, const float *rows, const int *sizes, const int *is_end, int n_groups,
+                   float *out, int *out_n, float *ontime) {
+    for (int g = 0; g < n_groups; ++g)
+        if (sizes[g] < 0 || sizes[g] > MaxPointNum) return -1;
+    LocalizationPara r;
+    to_ref(p, r);
+    ConsecutiveFit_TypeDef cf;
+    cf.Init();
+    float *pinned = nullptr;
+    cudaMallocHost((void **)&pinned, sizeof(float) * 12 * (size_t)MaxPointNum);
+    cudaStream_t s;
+    cudaStreamCreate(&s);
+    size_t off = 0, oo = 0;
+    int st = 0;
+    for (int g = 0; g < n_groups && st == 0; ++g) {
+        memcpy(pinned, rows + off * 12, sizeof(float) * 12 * (size_t)sizes[g]);
+        cf.ConsecutiveFit_WeightedAvg(pinned, sizes[g], is_end[g], r, s);
+        cudaStreamSynchronize(s);
+        st = check();
+        out_n[g] = cf.OutFluoNum;
+        memcpy(out + oo * 12, cf.h_OutLocArry, sizeof(float) * 12 * (size_t)cf.OutFluoNum);
+        memcpy(ontime + (size_t)g * MaxOnTimeConsecutiveNum, cf.h_OntimeRatio, sizeof(float) * MaxOnTimeConsecutiveNum);
+        oo += (size_t)cf.OutFluoNum;
+        off += (size_t)sizes[g];
+    }
+    cudaStreamDestroy(s);
+    cudaFreeHost(pinned);
+    cf.Deinit();
     return st;
 }
 

@@ -121,6 +121,15 @@ _SIGS = {
                                                   C.c_void_p]),
     "qcs_loc_count_labels_device": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "qcs_learned_set_count_threshold": (C.c_int, [C.c_void_p, C.c_float]),
+    "qcs_consec_init": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
+    "qcs_consec_deinit": (C.c_int, [C.c_void_p]),
+    "qcs_consec_fit": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.POINTER(LocPara), C.c_void_p]),
+    "qcs_consec_fit_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.POINTER(LocPara), C.c_void_p]),
+    "qcs_consec_out_num": (C.c_int, [C.c_void_p]),
+    "qcs_consec_h_out_loc_arry": (C.c_void_p, [C.c_void_p]),
+    "qcs_consec_d_out_loc_arry": (C.c_void_p, [C.c_void_p]),
+    "qcs_consec_ontime_ratio": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "qcs_consec_read_rows": (C.c_int, [C.c_void_p, C.c_void_p]),
     "qcs_learned_create_for": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_ulonglong, C.POINTER(C.c_void_p)]),
     "qcs_learned_shape": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "qcs_learned_localize_device_n": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(LocPara),
@@ -580,6 +589,60 @@ def count_labels(ctx, n, stream=0):
     check(load().qcs_loc_count_labels_device(ctx.h, int(n), C.c_void_p(out.data_ptr()),
                                              C.c_void_p(stream) if stream else None))
     return out
+
+
+class ConsecFit:
+    """ConsecutiveFit_TypeDef (qcs_consec_*): merges localizations of one
+    molecule over consecutive frames, one group of frame-sorted rows per call."""
+
+    def __init__(self, capacity=0):
+        self.lib = load()
+        h = C.c_void_p()
+        check(self.lib.qcs_consec_init(int(capacity), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.lib.qcs_consec_deinit(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def fit(self, rows, para, is_end=False, stream=0):
+        """One group of host rows; returns (output rows, on-time ratios[10])."""
+        rows, pr = _host(rows, np.float32)
+        check(self.lib.qcs_consec_fit(self.h, pr, rows.shape[0] if rows.ndim == 2 else 0, int(bool(is_end)),
+                                      C.byref(para), C.c_void_p(stream) if stream else None))
+        return self._result()
+
+    def fit_device(self, d_rows, n, para, is_end=False, stream=0):
+        check(self.lib.qcs_consec_fit_device(self.h, C.c_void_p(d_rows), int(n), int(bool(is_end)), C.byref(para),
+                                             C.c_void_p(stream) if stream else None))
+        return self.lib.qcs_consec_out_num(self.h)
+
+    def _result(self):
+        n = self.lib.qcs_consec_out_num(self.h)
+        ptr = self.lib.qcs_consec_h_out_loc_arry(self.h)
+        rows = np.ctypeslib.as_array((C.c_float * (12 * n)).from_address(ptr)).reshape(n, 12).copy() if n else \
+            np.zeros((0, 12), np.float32)
+        on = np.zeros(10, np.float32)
+        check(self.lib.qcs_consec_ontime_ratio(self.h, C.c_void_p(on.ctypes.data)))
+        return rows, on
+
+    def device_rows(self):
+        return self.lib.qcs_consec_d_out_loc_arry(self.h)
+
+    def read_rows(self):
+        """The last call's output rows copied from the device."""
+        n = self.lib.qcs_consec_out_num(self.h)
+        out = np.zeros((n, 12), np.float32)
+        if n:
+            check(self.lib.qcs_consec_read_rows(self.h, C.c_void_p(out.ctypes.data)))
+        return out
 
 
 class RenderContext:

@@ -175,3 +175,48 @@ def frames(n_frames, width=2048, height=2048, density=3000, pair_frac=0.2, seed=
         truth.append(dict(x=x, y=y, sigma=sig, photons=ph, background=bgv))
     para = default_para(Offset=offset, KAdc=kadc, QE=1.0, ImageWidth=width, ImageHigh=height)
     return out, para, truth
+
+
+def blinking_rows(n_emitters=400, frames=12, seed=0, width=256, jitter=0.1, loc_type=0, first_frame=1):
+    """Rows (12 floats) of emitters that switch on and off (on -> on 0.6,
+    off -> on 0.25) over `frames` frames; each on-frame gives one row near the
+    emitter's position (Gaussian jitter in px).  Returns (rows, per-frame counts)."""
+    rng = np.random.default_rng(seed)
+    ex = rng.uniform(5, width - 5, n_emitters)
+    ey = rng.uniform(5, width - 5, n_emitters)
+    ez = rng.uniform(-400, 400, n_emitters)
+    on = rng.random(n_emitters) < 0.4
+    rows, counts = [], []
+    for f in range(frames):
+        if f:
+            stay = rng.random(n_emitters) < 0.6
+            come = rng.random(n_emitters) < 0.25
+            on = np.where(on, stay, come)
+        idx = np.nonzero(on)[0]
+        rng.shuffle(idx)
+        k = idx.size
+        r = np.zeros((k, 12), np.float32)
+        sig = rng.uniform(1.0, 1.5, k)
+        peak = np.exp(rng.uniform(np.log(200), np.log(2000), k))
+        bkg = rng.uniform(20, 80, k)
+        r[:, 0] = peak
+        r[:, 1] = ex[idx] + rng.normal(0, jitter, k)
+        r[:, 2] = ey[idx] + rng.normal(0, jitter, k)
+        r[:, 3] = ez[idx] + rng.normal(0, 20, k) if loc_type == 1 else 0.0
+        r[:, 4] = sig
+        r[:, 5] = sig * (rng.uniform(0.8, 1.25, k) if loc_type == 1 else 1.0)
+        r[:, 6] = peak * 2 * np.pi * r[:, 4] * r[:, 5]
+        r[:, 7] = bkg
+        r[:, 8] = peak / np.sqrt(peak + bkg)
+        r[:, 9] = rng.uniform(5, 30, k)
+        r[:, 10] = rng.uniform(5, 30, k)
+        r[:, 11] = first_frame + f
+        rows.append(r)
+        counts.append(k)
+    return np.concatenate(rows), np.array(counts)
+
+
+def group_sizes(counts, frames_per_group):
+    """Rows per group of `frames_per_group` consecutive frames."""
+    return np.array([counts[i:i + frames_per_group].sum() for i in range(0, counts.size, frames_per_group)],
+                    np.int32)

@@ -171,6 +171,37 @@ def zero_remove(rows, sort_frame=0, first_frame=0, end_frame=0, lib="oracle"):
     return out[:n.value].copy()
 
 
+def consec(para, rows, sizes, is_end=None, lib="oracle", gpu_rounding=0):
+    """ConsecutiveFit_WeightedAvg over groups of rows (sizes[g] rows each, in
+    turn) through the oracle ("oracle"; gpu_rounding 1: the GPU's roundings),
+    the host build of the reference ("ref") or its CUDA build ("ref_gpu").
+    Returns (list of per-call output rows, ontime ratios [groups, 10])."""
+    rows = np.ascontiguousarray(rows, np.float32)
+    sizes = np.ascontiguousarray(sizes, np.int32)
+    g = sizes.size
+    if is_end is None:
+        is_end = np.zeros(g, np.int32)
+        is_end[-1] = 1
+    is_end = np.ascontiguousarray(is_end, np.int32)
+    out = np.zeros((max(rows.shape[0], 1), 12), np.float32)
+    out_n = np.zeros(g, np.int32)
+    ontime = np.zeros((g, 10), np.float32)
+    pp = C.byref(para)
+    if lib == "oracle":
+        st = oracle().qcso_consec(pp, _p(rows), _p(sizes), _p(is_end), g, int(gpu_rounding), _p(out), _p(out_n),
+                                  _p(ontime))
+    elif lib == "ref":
+        st = ref_host().qcsref_consec(pp, _p(rows), _p(sizes), _p(is_end), g, _p(out), _p(out_n), _p(ontime))
+    else:
+        st = ref_gpu().qcsrefg_consec(pp, _p(rows), _p(sizes), _p(is_end), g, _p(out), _p(out_n), _p(ontime))
+    assert st == 0, st
+    res, o = [], 0
+    for k in out_n:
+        res.append(out[o:o + k].copy())
+        o += k
+    return res, ontime
+
+
 def render(para, rows, mode, fixed_prec=0.0, state=None, lib="oracle"):
     """Super-resolution render of rows through the oracle ("oracle"), the host
     build of the reference ("ref") or its CUDA build ("ref_gpu").  state:
