@@ -722,7 +722,25 @@ def consec_measure(stream, dist, world):
     torch.cuda.synchronize()
     ms = max_over_ranks(e0.elapsed_time(e1), dist) / CONSEC_GROUPS
     cf.close()
-    return {"workload": "rows of 7,500 blinking molecules over 2048 x 2048 frames (~%d rows per frame), %d frames "
+    # localization statistics (qcs_stat_get_statistical_inf_device) on the same groups
+    stt = lib.Statistics(capacity=cap)
+    for g in range(2):
+        stt.update_device(d[g % 2].data_ptr(), int(sizes[g % 2]), para, stream=sh)
+    torch.cuda.synchronize()
+    s0 = torch.cuda.Event(enable_timing=True)
+    s1 = torch.cuda.Event(enable_timing=True)
+    s0.record(stream)
+    for g in range(CONSEC_GROUPS):
+        _, means = stt.update_device(d[g % 2].data_ptr(), int(sizes[g % 2]), para, stream=sh)
+    s1.record(stream)
+    torch.cuda.synchronize()
+    ms_stat = max_over_ranks(s0.elapsed_time(s1), dist) / CONSEC_GROUPS
+    stt.close()
+    stat = {"rows_per_call": int(total / CONSEC_GROUPS), "ms_per_call": ms_stat,
+            "rows_per_s": world * total / (ms_stat * 1e-3 * CONSEC_GROUPS),
+            "activation_density_per_um2": float(means[6]), "mean_precision_nm": float(means[1]),
+            "call": "qcs_stat_get_statistical_inf_device (histograms, means, activation density over 30 frames)"}
+    return {"statistics": stat, "workload": "rows of 7,500 blinking molecules over 2048 x 2048 frames (~%d rows per frame), %d frames "
                         "per call, threshold 80 nm at 100 nm pixels" % (int(counts.mean()), CONSEC_FRAMES_PER_GROUP),
             "rows_per_call": int(total / CONSEC_GROUPS), "ms_per_call": ms,
             "rows_per_s": world * total / (ms * 1e-3 * CONSEC_GROUPS),

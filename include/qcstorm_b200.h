@@ -346,6 +346,54 @@ int qcs_consec_read_rows(qcs_consec *c, float *h_out);
  * 1..10 frames (the last bin: 10 or more), over their number. */
 int qcs_consec_ontime_ratio(const qcs_consec *c, float *out10);
 
+/* ---- localization statistics: FluoStatisticData_TypeDef ------------------ */
+#define QCS_STAT_HIST_LEN 1600 /* StatInf_Hist_DatLenMax (StatisticsInfo/statisticsInfo.h:37) */
+/* qcs_stat_means: MeanTotalPhoton, MeanLocPrecisionXY, MeanPeakSNR, MeanBackground,
+ * MeanPSFWidth, MeanPSFWidth_Ctl, MeanLocDensity2D, TimeVaryMean_TotalPhoton,
+ * TimeVaryMean_LocPrecisionXY, TimeVaryMean_PeakSNR (statisticsInfo.h:63-86) */
+#define QCS_STAT_MEANS 10
+#define QCS_STAT_MEAN_PHOTON 0
+#define QCS_STAT_MEAN_PREC 1
+#define QCS_STAT_MEAN_SNR 2
+#define QCS_STAT_MEAN_BKG 3
+#define QCS_STAT_MEAN_PSF 4
+#define QCS_STAT_MEAN_PSF_CTL 5
+#define QCS_STAT_MEAN_DENSITY 6
+#define QCS_STAT_TV_PHOTON 7
+#define QCS_STAT_TV_PREC 8
+#define QCS_STAT_TV_SNR 9
+/* qcs_stat_series: TimeVary_TotalPhoton, _LocPrecisionXY, _PeakSNR, _Background,
+ * _PSFWidth, _PSFWidth_Ctl, _LocDensity2D (statisticsInfo.h:89-96) */
+#define QCS_STAT_SERIES 7
+#define QCS_STAT_SERIES_PHOTON 0
+#define QCS_STAT_SERIES_PREC 1
+#define QCS_STAT_SERIES_SNR 2
+#define QCS_STAT_SERIES_BKG 3
+#define QCS_STAT_SERIES_PSF 4
+#define QCS_STAT_SERIES_PSF_CTL 5
+#define QCS_STAT_SERIES_DENSITY 6
+typedef struct qcs_stat qcs_stat;
+/* FluoStatisticData_TypeDef::Init (statisticsInfo_top.cu:258): calls of at
+ * most `capacity` rows (<= 0: 2 x QCS_MAX_POINT_NUM); starts reset. */
+int qcs_stat_init(int capacity, qcs_stat **out);
+int qcs_stat_deinit(qcs_stat *st);
+/* ResetAllDat (statisticsInfo_top.cu:391): histograms, means and time series cleared. */
+int qcs_stat_reset_all(qcs_stat *st);
+/* GetStatisticalInf (statisticsInfo_top.cu:61) over n host rows: the four
+ * histograms (qcs_stat_histograms), the means and the activation density
+ * (qcs_stat_means), one more entry in each time series (qcs_stat_series).
+ * Synchronous, like the reference; n <= 0 changes nothing. */
+int qcs_stat_get_statistical_inf(qcs_stat *st, const float *h_rows, int n, const qcs_loc_para *p, void *stream);
+/* The same over n rows in device memory. */
+int qcs_stat_get_statistical_inf_device(qcs_stat *st, const float *d_rows, int n, const qcs_loc_para *p,
+                                        void *stream);
+/* The last call's histograms: total photons (bins of 25 photons), precision
+ * (0.15 nm), peak SNR (0.125), PSF width (0.0125 px), QCS_STAT_HIST_LEN each, in that order. */
+int qcs_stat_histograms(const qcs_stat *st, int *out4x1600);
+int qcs_stat_means(const qcs_stat *st, float *out10);
+/* Copies up to max_n entries of time series `which` into out (may be NULL); returns its length. */
+int qcs_stat_series(const qcs_stat *st, int which, float *out, int max_n);
+
 /* ---- WLE pre-pass: WLEParameterEstimation_TypeDef ---------------------- */
 /* WLEParameterEstimation_TypeDef::WLEParameterEstimate (WLEParaEstimation.h:41,
  * WLEParaEstimation.cpp:20-40): PSF width, same-frame nearest neighbour and

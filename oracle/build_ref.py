@@ -5,7 +5,8 @@ Compiles the reference's own CUDA sources (MLEbfgs/bfgs_MLE_dll x64/bfgsMLE_dll/
 bfgsMLE_dll/) with g++ against the host shim in oracle/refshim/, links them with
 oracle/ref_harness.cpp and writes oracle/_ref/libqcs_ref_host.so.  The result
 runs the reference's fit kernels, WLE pre-pass, CRLB, cascade orchestration,
-ROI extraction, super-resolution render and consecutive-frame merging on the CPU, one emulated CUDA block
+ROI extraction, super-resolution render, consecutive-frame merging and the
+localization statistics on the CPU, one emulated CUDA block
 at a time; it is the checker
 the CPU oracle (oracle/qcs_oracle.c) is pinned against.
 
@@ -26,6 +27,9 @@ reference source text is kept in the repository):
      barriers, so lane 0 would overwrite its entry before lane 1 reads it.
      A __syncthreads() is inserted after the read, which restores the
      lock-step order on the host and changes nothing the GPU computes.
+Every unit is also compiled with <cstring> included first: BFGS for curve
+fitting/BFGSOptimizer.h calls memset and memcpy without including it (MSVC's
+headers declare them on the way), which GCC rejects.
 Nothing else is changed.  Only the built .so lands in oracle/_ref/.
 
 With --gpu the same sources are compiled unmodified by nvcc for sm_100a
@@ -53,7 +57,8 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 # Reference sub-directories and translation units of the localization path.
 DIRS = ["bfgsMLE_Loc_LD", "bfgsMLE_Loc_HD", "bfgsMLE_Loc_top", "WLEParaEstimation",
-        "SubregionExtraction", "cudaWrapper", "ImgRender", "ConsecutiveFit", "StatisticsInfo"]
+        "SubregionExtraction", "cudaWrapper", "ImgRender", "ConsecutiveFit", "StatisticsInfo",
+        "BFGS for curve fitting"]
 UNITS = [
     "bfgsMLE_Loc_LD/bfgs_base.cu",
     "bfgsMLE_Loc_LD/bfgsMLE_Single_Emitter_Fit.cu",
@@ -73,6 +78,11 @@ UNITS = [
     "ImgRender/ImageRerender_rc.cu",
     "ConsecutiveFit/ConsecutiveFit.cu",
     "ConsecutiveFit/ConsecutiveFit_top.cu",
+    "StatisticsInfo/statisticsInfo.cu",
+    "StatisticsInfo/statisticsInfo_densityCalc.cu",
+    "StatisticsInfo/statisticsInfo_rc.cu",
+    "StatisticsInfo/statisticsInfo_top.cu",
+    "BFGS for curve fitting/CurveFitting.cpp",
 ]
 
 LAUNCH = re.compile(
@@ -137,7 +147,7 @@ def build_gpu(args):
         open(os.path.join(tmp, "stdafx.h"), "w").close()
         incs = ["-I" + tmp] + ["-I" + os.path.join(tmp, d) for d in DIRS]
         flags = ["-std=c++17", "-O3", "-gencode", "arch=compute_100a,code=sm_100a", "-Xcompiler", "-fPIC",
-                 "-w", "-D__declspec(x)=", "-x", "cu", "-rdc=false"]
+                 "-w", "-D__declspec(x)=", "-x", "cu", "-rdc=false", "--pre-include", "cstring"]
         units = [os.path.join(tmp, u) for u in UNITS] + [os.path.join(HERE, "ref_harness_gpu.cu")]
         objs, cmds = [], []
         for i, u in enumerate(units):
@@ -190,7 +200,7 @@ def main():
                 with open(os.path.join(dst, name), "w", encoding="latin-1") as f:
                     f.write(rewrite(text))
         incs = ["-I" + os.path.join(HERE, "refshim")] + ["-I" + os.path.join(tmp, d) for d in DIRS]
-        flags = ["-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-w", "-D__declspec(x)="]
+        flags = ["-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-w", "-D__declspec(x)=", "-include", "cstring"]
         objs = []
         units = [os.path.join(tmp, u) for u in UNITS]
         units += [os.path.join(HERE, "ref_harness.cpp"), os.path.join(HERE, "refshim", "simt_emu.cpp")]

@@ -79,6 +79,10 @@ int qcso_zero_remove(const float *rows, int n, int sort_frame, int first_frame, 
 int qcso_consec(const qcs_loc_para *p, const float *rows, const int *sizes, const int *is_end, int n_groups,
                 int gpu_rounding, float *out, int *out_n, float *ontime);
 
+/* GetStatisticalInf over n_groups groups of sizes[g] rows in turn (after ResetAllDat); after call g:
+ * hist[g * 6400 ..] the four 1600-bin histograms, means[g * 10 ..] the means (see qcs_oracle_stat.c). */
+int qcso_stat(const qcs_loc_para *p, const float *rows, const int *sizes, int n_groups, int *hist, float *means);
+
 #ifdef __cplusplus
 }
 #endif

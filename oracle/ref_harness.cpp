@@ -11,6 +11,7 @@
 //   qcsref_wle         WLEParameterEstimation_TypeDef::WLEParameterEstimate
 //   qcsref_zero_remove ZeroLocalizationsRemovel_TypeDef::RemoveZeroLocalizations
 //   qcsref_consec      ConsecutiveFit_TypeDef::ConsecutiveFit_WeightedAvg over a sequence of groups
+//   qcsref_stat        FluoStatisticData_TypeDef::GetStatisticalInf over a sequence of groups
 //                      (WLEParaEstimation.cpp:20-40)
 //   qcsref_extract     LDROIExtractData_TypeDef::ExtractMolecules (LDROIExtraction.cu:30-80)
 #include <cstdio>
@@ -25,6 +26,7 @@
 #include "LocPrecCalc_GaussianCRLB.h"
 #include "ZeroLocalizationsRemove.h"
 #include "ConsecutiveFit.h"
+#include "statisticsInfo.h"
 #include "ImageRender_2d.h"
 #include "ImageRender_3d.h"
 
@@ -274,6 +276,53 @@ int qcsref_consec(const qcs_loc_para *p, const float *rows, const int *sizes, co
         off += (size_t)sizes[g];
     }
     cf.Deinit();
+    return 0;
+}
+
+// copies the histograms and means of call g (see qcsref_stat)
+static void stat_out(const FluoStatisticData_TypeDef &sd, int g, int *hist, float *means) {
+    int *h = hist + (size_t)g * 4 * StatInf_Hist_DatLenMax;
+    memcpy(h, sd.h_Hist_TotalPhoton, sizeof(int) * StatInf_Hist_DatLenMax);
+    memcpy(h + StatInf_Hist_DatLenMax, sd.h_Hist_LocPrecisionXY, sizeof(int) * StatInf_Hist_DatLenMax);
+    memcpy(h + 2 * StatInf_Hist_DatLenMax, sd.h_Hist_PeakSNR, sizeof(int) * StatInf_Hist_DatLenMax);
+    memcpy(h + 3 * StatInf_Hist_DatLenMax, sd.h_Hist_PSFWidth, sizeof(int) * StatInf_Hist_DatLenMax);
+    float *m = means + (size_t)g * 10;
+    m[0] = sd.MeanTotalPhoton;
+    m[1] = sd.MeanLocPrecisionXY;
+    m[2] = sd.MeanPeakSNR;
+    m[3] = sd.MeanBackground;
+    m[4] = sd.MeanPSFWidth;
+    m[5] = sd.MeanPSFWidth_Ctl;
+    m[6] = sd.MeanLocDensity2D;
+    m[7] = sd.TimeVaryMean_TotalPhoton;
+    m[8] = sd.TimeVaryMean_LocPrecisionXY;
+    m[9] = sd.TimeVaryMean_PeakSNR;
+}
+
+// FluoStatisticData_TypeDef (StatisticsInfo/statisticsInfo_top.cu:61-255): Init,
+// ResetAllDat, then GetStatisticalInf once per group of sizes[g] rows (<=
+// MaxPointNum) taken in turn from rows.  After call g: hist[g * 4 * 1600 ..]
+// the four histograms (total photons, localization precision, peak SNR, PSF
+// width; StatInf_Hist_DatLenMax bins each) and means[g * 10 ..] MeanTotalPhoton,
+// MeanLocPrecisionXY, MeanPeakSNR, MeanBackground, MeanPSFWidth,
+// MeanPSFWidth_Ctl, MeanLocDensity2D, TimeVaryMean_TotalPhoton,
+// TimeVaryMean_LocPrecisionXY, TimeVaryMean_PeakSNR.
+int qcsref_stat(const qcs_loc_para *p, const float *rows, const int *sizes, int n_groups, int *hist, float *means) {
+    for (int g = 0; g < n_groups; ++g)
+        if (sizes[g] < 0 || sizes[g] > MaxPointNum) return -1;
+    LocalizationPara r;
+    to_ref(p, r);
+    FluoStatisticData_TypeDef sd;
+    sd.Init();
+    sd.ResetAllDat(nullptr);
+    size_t off = 0;
+    for (int g = 0; g < n_groups; ++g) {
+        std::vector<float> in(rows + off * 12, rows + (off + (size_t)sizes[g]) * 12);
+        sd.GetStatisticalInf(in.data(), r, sizes[g], nullptr);
+        stat_out(sd, g, hist, means);
+        off += (size_t)sizes[g];
+    }
+    sd.Deinit();
     return 0;
 }
 

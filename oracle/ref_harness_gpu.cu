@@ -13,6 +13,7 @@
 //   qcsrefg_extract     LDROIExtractData_TypeDef::ExtractMolecules
 //   qcsrefg_zero_remove ZeroLocalizationsRemovel_TypeDef::RemoveZeroLocalizations
 //   qcsrefg_consec     ConsecutiveFit_TypeDef::ConsecutiveFit_WeightedAvg over a sequence of groups
+//   qcsrefg_stat       FluoStatisticData_TypeDef::GetStatisticalInf over a sequence of groups
 // Every entry point returns 0, or the CUDA error code of the first failure.
 #include <cstdio>
 #include <cstring>
@@ -29,6 +30,7 @@
 #include "LocPrecCalc_GaussianCRLB.h"
 #include "ZeroLocalizationsRemove.h"
 #include "ConsecutiveFit.h"
+#include "statisticsInfo.h"
 #include "ImageRender_2d.h"
 #include "ImageRender_3d.h"
 
@@ -418,6 +420,55 @@ int qcsrefg_consec(const qcs_loc_para *p, const float *rows, const int *sizes, c
     cudaStreamDestroy(s);
     cudaFreeHost(pinned);
     cf.Deinit();
+    return st;
+}
+
+// copies the histograms and means of call g (see qcsref_stat)
+static void stat_out(const FluoStatisticData_TypeDef &sd, int g, int *hist, float *means) {
+    int *h = hist + (size_t)g * 4 * StatInf_Hist_DatLenMax;
+    memcpy(h, sd.h_Hist_TotalPhoton, sizeof(int) * StatInf_Hist_DatLenMax);
+    memcpy(h + StatInf_Hist_DatLenMax, sd.h_Hist_LocPrecisionXY, sizeof(int) * StatInf_Hist_DatLenMax);
+    memcpy(h + 2 * StatInf_Hist_DatLenMax, sd.h_Hist_PeakSNR, sizeof(int) * StatInf_Hist_DatLenMax);
+    memcpy(h + 3 * StatInf_Hist_DatLenMax, sd.h_Hist_PSFWidth, sizeof(int) * StatInf_Hist_DatLenMax);
+    float *m = means + (size_t)g * 10;
+    m[0] = sd.MeanTotalPhoton;
+    m[1] = sd.MeanLocPrecisionXY;
+    m[2] = sd.MeanPeakSNR;
+    m[3] = sd.MeanBackground;
+    m[4] = sd.MeanPSFWidth;
+    m[5] = sd.MeanPSFWidth_Ctl;
+    m[6] = sd.MeanLocDensity2D;
+    m[7] = sd.TimeVaryMean_TotalPhoton;
+    m[8] = sd.TimeVaryMean_LocPrecisionXY;
+    m[9] = sd.TimeVaryMean_PeakSNR;
+}
+
+// qcsref_stat on the GPU build.
+int qcsrefg_stat(const qcs_loc_para *p, const float *rows, const int *sizes, int n_groups, int *hist, float *means) {
+    for (int g = 0; g < n_groups; ++g)
+        if (sizes[g] < 0 || sizes[g] > MaxPointNum) return -1;
+    LocalizationPara r;
+    to_ref(p, r);
+    FluoStatisticData_TypeDef sd;
+    sd.Init();
+    cudaStream_t s;
+    cudaStreamCreate(&s);
+    sd.ResetAllDat(s);
+    float *pinned = nullptr;
+    cudaMallocHost((void **)&pinned, sizeof(float) * 12 * (size_t)MaxPointNum);
+    size_t off = 0;
+    int st = 0;
+    for (int g = 0; g < n_groups && st == 0; ++g) {
+        memcpy(pinned, rows + off * 12, sizeof(float) * 12 * (size_t)sizes[g]);
+        sd.GetStatisticalInf(pinned, r, sizes[g], s);
+        cudaStreamSynchronize(s);
+        st = check();
+        stat_out(sd, g, hist, means);
+        off += (size_t)sizes[g];
+    }
+    cudaFreeHost(pinned);
+    cudaStreamDestroy(s);
+    sd.Deinit();
     return st;
 }
 

@@ -130,6 +130,15 @@ _SIGS = {
     "qcs_consec_d_out_loc_arry": (C.c_void_p, [C.c_void_p]),
     "qcs_consec_ontime_ratio": (C.c_int, [C.c_void_p, C.c_void_p]),
     "qcs_consec_read_rows": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "qcs_stat_init": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
+    "qcs_stat_deinit": (C.c_int, [C.c_void_p]),
+    "qcs_stat_reset_all": (C.c_int, [C.c_void_p]),
+    "qcs_stat_get_statistical_inf": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(LocPara), C.c_void_p]),
+    "qcs_stat_get_statistical_inf_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(LocPara),
+                                                      C.c_void_p]),
+    "qcs_stat_histograms": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "qcs_stat_means": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "qcs_stat_series": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
     "qcs_learned_create_for": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_ulonglong, C.POINTER(C.c_void_p)]),
     "qcs_learned_shape": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "qcs_learned_localize_device_n": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(LocPara),
@@ -642,6 +651,57 @@ class ConsecFit:
         out = np.zeros((n, 12), np.float32)
         if n:
             check(self.lib.qcs_consec_read_rows(self.h, C.c_void_p(out.ctypes.data)))
+        return out
+
+
+class Statistics:
+    """FluoStatisticData_TypeDef (qcs_stat_*): histograms, means, activation
+    density and their time series over the localization rows of each call."""
+
+    def __init__(self, capacity=0):
+        self.lib = load()
+        h = C.c_void_p()
+        check(self.lib.qcs_stat_init(int(capacity), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.lib.qcs_stat_deinit(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def reset(self):
+        check(self.lib.qcs_stat_reset_all(self.h))
+
+    def update(self, rows, para, stream=0):
+        rows, pr = _host(rows, np.float32)
+        check(self.lib.qcs_stat_get_statistical_inf(self.h, pr, rows.shape[0], C.byref(para),
+                                                    C.c_void_p(stream) if stream else None))
+        return self.result()
+
+    def update_device(self, d_rows, n, para, stream=0):
+        check(self.lib.qcs_stat_get_statistical_inf_device(self.h, C.c_void_p(d_rows), int(n), C.byref(para),
+                                                           C.c_void_p(stream) if stream else None))
+        return self.result()
+
+    def result(self):
+        """(histograms [4, 1600], means [10])."""
+        hist = np.zeros((4, 1600), np.int32)
+        means = np.zeros(10, np.float32)
+        check(self.lib.qcs_stat_histograms(self.h, C.c_void_p(hist.ctypes.data)))
+        check(self.lib.qcs_stat_means(self.h, C.c_void_p(means.ctypes.data)))
+        return hist, means
+
+    def series(self, which):
+        n = self.lib.qcs_stat_series(self.h, int(which), None, 0)
+        out = np.zeros(max(n, 0), np.float32)
+        if n > 0:
+            self.lib.qcs_stat_series(self.h, int(which), C.c_void_p(out.ctypes.data), n)
         return out
 
 

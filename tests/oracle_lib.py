@@ -202,6 +202,26 @@ def consec(para, rows, sizes, is_end=None, lib="oracle", gpu_rounding=0):
     return res, ontime
 
 
+def stat(para, rows, sizes, lib="oracle"):
+    """GetStatisticalInf over groups of rows (sizes[g] each, in turn) through the
+    oracle ("oracle"), the host build of the reference ("ref") or its CUDA
+    build ("ref_gpu").  Returns (histograms [groups, 4, 1600], means [groups, 10])."""
+    rows = np.ascontiguousarray(rows, np.float32)
+    sizes = np.ascontiguousarray(sizes, np.int32)
+    g = sizes.size
+    hist = np.zeros((g, 4, 1600), np.int32)
+    means = np.zeros((g, 10), np.float32)
+    pp = C.byref(para)
+    if lib == "oracle":
+        st = oracle().qcso_stat(pp, _p(rows), _p(sizes), g, _p(hist), _p(means))
+    elif lib == "ref":
+        st = ref_host().qcsref_stat(pp, _p(rows), _p(sizes), g, _p(hist), _p(means))
+    else:
+        st = ref_gpu().qcsrefg_stat(pp, _p(rows), _p(sizes), g, _p(hist), _p(means))
+    assert st == 0, st
+    return hist, means
+
+
 def render(para, rows, mode, fixed_prec=0.0, state=None, lib="oracle"):
     """Super-resolution render of rows through the oracle ("oracle"), the host
     build of the reference ("ref") or its CUDA build ("ref_gpu").  state:
