@@ -165,7 +165,8 @@ int qcs_loc_init_capacity(const qcs_loc_para *p, int capacity, qcs_loc_data **ou
     if (e == cudaSuccess) e = A(&c->d_wle_scratch, c->wle_scratch);
     // cascade state in one allocation
     const size_t a_int = cap * sizeof(int), a_u8 = (cap + 255) / 256 * 256, a_row = cap * 12 * sizeof(float);
-    const size_t bytes = 3 * a_int + 3 * a_u8 + 2 * a_row + 256;
+    const size_t a_scan = ((size_t)qcs::cascade_scan_ints(capacity) * sizeof(int) + 255) / 256 * 256;
+    const size_t bytes = 3 * a_int + 3 * a_u8 + 2 * a_row + 256 + a_scan;
     if (e == cudaSuccess) e = A(&c->d_state, bytes);
     if (e == cudaSuccess) e = cudaMallocHost((void **)&c->h_loc, (size_t)c->max_rows * QCS_OUT_PARA_NUM * sizeof(float));
     if (e == cudaSuccess) e = cudaMallocHost((void **)&c->h_counters, qcs::kCntNum * sizeof(int));
@@ -191,7 +192,8 @@ int qcs_loc_init_capacity(const qcs_loc_para *p, int capacity, qcs_loc_data **ou
     c->st.res3 = reinterpret_cast<int8_t *>(s); s += a_u8;
     c->st.extra2 = reinterpret_cast<float *>(s); s += a_row;
     c->st.extra3 = reinterpret_cast<float *>(s); s += a_row;
-    c->st.counters = reinterpret_cast<int *>(s);
+    c->st.counters = reinterpret_cast<int *>(s); s += 256;
+    c->st.scan = reinterpret_cast<int *>(s);
     c->q_refit = reinterpret_cast<int *>(c->d_start + cap * 6);
     c->d_refit = reinterpret_cast<uint8_t *>(c->q_refit + cap);
     c->d_cls = c->d_refit + cap;

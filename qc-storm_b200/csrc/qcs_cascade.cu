@@ -44,120 +44,174 @@ __device__ __forceinline__ int block_scan(int pred, int *total) {
     return warp_sums[warp] + in_warp;
 }
 
-// Split records by WLE molecule type into the single-emitter queue
-// (MLEFit, WLEFit) and the two-emitter queue (MultiFit), both ascending
-// (bfgs_top_MoleculeClasify.cu:26-92).  With a predicted emitter-count class
-// per record (pred, learned path only: 0 one emitter, 1 the two-emitter
-// stage, 2 the three-emitter stage), class 2 goes straight to the 3E queue
-// and class 1 to the 2E queue, so neither pays for the fits that would have
-// rejected it; pred == null is the reference's split.
-__global__ void __launch_bounds__(kScanThreads) classify_queues_kernel(const float *__restrict__ wle, int n,
-                                                                       const int *__restrict__ n_dev, int multi,
-                                                                       const uint8_t *__restrict__ pred,
-                                                                       CascadeState st) {
+// The records' split (bfgs_top_MoleculeClasify.cu:26-92): by WLE molecule
+// type into the single-emitter queue (MLEFit, WLEFit) and the two-emitter
+// queue (MultiFit), both ascending.  With a predicted emitter-count class per
+// record (pred, learned path only: 0 one emitter, 1 the two-emitter stage, 2
+// the three-emitter stage), class 2 goes straight to the 3E queue and class 1
+// to the 2E queue, so neither pays for the fits that would have rejected it;
+// pred == null is the reference's split.  After the single-emitter fit its
+// rejects with SNR > 6 follow the classified records in the 2E queue, in
+// single-queue order (bfgsMLE_GS2D_core.h:279-298); after each multi-emitter
+// fit the queue slots are walked in order, second emitters appended after the
+// current rows and rejections routed to the next queue (3E) or counted.  All
+// three are order-preserving compactions (ClassifyStage, Append2EStage,
+// CompactStage below).
+
+// ---- order-preserving compaction over many blocks --------------------------
+// The queues above are built by one block walking all records, 1,024 at a
+// time (~100 serial steps for 100,000 records).  The same compactions run here
+// over one block per 1,024-element tile in two launches: every tile counts its
+// selected elements; then every tile adds the counts of the tiles before it to
+// its own prefix sums and scatters, and the last tile writes the totals.  The
+// positions are the one-block walk's exactly (ascending element order).  A
+// stage S gives the element count (on the device), NP predicates per element,
+// where a selected element goes, and the counters after the last element;
+// counters it reads and later overwrites are copied first (snapshot, by tile
+// 0 of the counting launch) so that no tile reads a value the last tile has
+// already replaced.  scan: kScanSnap snapshot ints, then NP counts per tile.
+constexpr int kScanSnap = 4;
+
+template <class S>
+__global__ void __launch_bounds__(kScanThreads) tile_count_kernel(S s, int *__restrict__ scan) {
+    const int n = s.count();
+    if (blockIdx.x == 0 && threadIdx.x == 0) s.snapshot(scan);
+    const int i = blockIdx.x * kScanThreads + threadIdx.x;
+    int f[S::NP];
+    s.flags(i, n, f);
+#pragma unroll
+    for (int p = 0; p < S::NP; ++p) {
+        const int c = __syncthreads_count(f[p]);
+        if (threadIdx.x == 0) scan[kScanSnap + blockIdx.x * S::NP + p] = c;
+    }
+}
+
+template <class S>
+__global__ void __launch_bounds__(kScanThreads) tile_scatter_kernel(S s, const int *__restrict__ scan) {
+    __shared__ int base[S::NP];
     __shared__ int tot;
-    if (n_dev) n = min(max(*n_dev, 0), n);
-    int n1 = 0, n2 = 0, n3 = 0;
-    for (int base = 0; base < n; base += kScanThreads) {
-        const int i = base + threadIdx.x;
-        const int valid = i < n;
+    if (threadIdx.x < 32) {
+        int acc[S::NP];
+#pragma unroll
+        for (int p = 0; p < S::NP; ++p) acc[p] = 0;
+        for (int t = threadIdx.x; t < (int)blockIdx.x; t += 32)
+#pragma unroll
+            for (int p = 0; p < S::NP; ++p) acc[p] += scan[kScanSnap + t * S::NP + p];
+#pragma unroll
+        for (int p = 0; p < S::NP; ++p) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc[p] += __shfl_down_sync(0xffffffffu, acc[p], o);
+            if (threadIdx.x == 0) base[p] = acc[p];
+        }
+    }
+    __syncthreads();
+    const int n = s.count();
+    const int i = blockIdx.x * kScanThreads + threadIdx.x;
+    int f[S::NP];
+    s.flags(i, n, f);
+    int total[S::NP];
+#pragma unroll
+    for (int p = 0; p < S::NP; ++p) {
+        const int pre = block_scan(f[p], &tot);
+        if (f[p]) s.emit(p, i, base[p] + pre, scan);
+        total[p] = base[p] + tot;
+    }
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) s.finish(total, scan, n);
+}
+
+// the classify split
+struct ClassifyStage {
+    enum { NP = 3 };
+    const float *wle;
+    int n;
+    const int *n_dev;
+    const uint8_t *pred;
+    CascadeState st;
+    __device__ int count() const { return n_dev ? min(max(*n_dev, 0), n) : n; }
+    __device__ void snapshot(int *) const {}
+    __device__ void flags(int i, int cnt, int (&f)[NP]) const {
+        const int valid = i < cnt;
         const int type = valid ? (int)wle[(size_t)i * QCS_WLE_PARA_NUM + 5] : 0;
         const int cls = (valid && pred) ? pred[i] : 0;
-        const int to_3e = valid && multi && cls == 2;
-        const int to_multi = valid && multi && !to_3e && (type > QCS_MOLECULE_WLEFIT || cls == 1);
-        const int to_single = valid && !to_multi && !to_3e;
-        int p1 = block_scan(to_single, &tot);
-        const int t1 = tot;
-        if (to_single) st.q_single[n1 + p1] = i;
-        int p2 = block_scan(to_multi, &tot);
-        const int t2 = tot;
-        if (to_multi) st.q2[n2 + p2] = i;
-        int p3 = block_scan(to_3e, &tot);
-        const int t3 = tot;
-        if (to_3e) st.q3[n3 + p3] = i;
-        n1 += t1;
-        n2 += t2;
-        n3 += t3;
+        const int to_3e = valid && cls == 2;
+        const int to_multi = valid && !to_3e && (type > QCS_MOLECULE_WLEFIT || cls == 1);
+        f[0] = valid && !to_multi && !to_3e;
+        f[1] = to_multi;
+        f[2] = to_3e;
     }
-    if (threadIdx.x == 0) {
-        st.counters[kCntSingle] = n1;
-        st.counters[kCnt2E] = n2;
-        st.counters[kCnt2EClassify] = n2;
-        st.counters[kCnt3E] = n3;
-        st.counters[kCnt3EClassify] = n3;
+    __device__ void emit(int p, int i, int pos, const int *) const {
+        if (p == 0) st.q_single[pos] = i;
+        else if (p == 1) st.q2[pos] = i;
+        else st.q3[pos] = i;
+    }
+    __device__ void finish(const int (&t)[NP], const int *, int cnt) const {
+        st.counters[kCntSingle] = t[0];
+        st.counters[kCnt2E] = t[1];
+        st.counters[kCnt2EClassify] = t[1];
+        st.counters[kCnt3E] = t[2];
+        st.counters[kCnt3EClassify] = t[2];
         st.counters[kCntRejected] = 0;
-        st.counters[kCntRows] = n;
+        st.counters[kCntRows] = cnt;
     }
-}
+};
 
-// Append single-emitter rejects with SNR > 6 to the two-emitter queue, in
-// single-queue order (bfgsMLE_GS2D_core.h:279-298).
-__global__ void __launch_bounds__(kScanThreads) append_2e_kernel(CascadeState st) {
-    __shared__ int tot;
-    const int ns = st.counters[kCntSingle];
-    int n2 = st.counters[kCnt2E];
-    for (int base = 0; base < ns; base += kScanThreads) {
-        const int k = base + threadIdx.x;
-        int id = 0, pred = 0;
-        if (k < ns) {
-            id = st.q_single[k];
-            pred = st.to2e[id];
-        }
-        const int p = block_scan(pred, &tot);
-        if (pred) st.q2[n2 + p] = id;
-        n2 += tot;
+// single-emitter rejects to the 2E queue
+struct Append2EStage {
+    enum { NP = 1 };
+    CascadeState st;
+    __device__ int count() const { return st.counters[kCntSingle]; }
+    __device__ void snapshot(int *snap) const { snap[0] = st.counters[kCnt2E]; }
+    __device__ void flags(int k, int cnt, int (&f)[NP]) const { f[0] = k < cnt ? st.to2e[st.q_single[k]] : 0; }
+    __device__ void emit(int, int k, int pos, const int *snap) const { st.q2[snap[0] + pos] = st.q_single[k]; }
+    __device__ void finish(const int (&t)[NP], const int *snap, int) const { st.counters[kCnt2E] = snap[0] + t[0]; }
+};
+
+// second emitters appended, rejects routed on
+struct CompactStage {
+    enum { NP = 2 };
+    CascadeState st;
+    float *loc;
+    int stage, route, max_rows;
+    __device__ int count() const { return stage == 2 ? st.counters[kCnt2E] : st.counters[kCnt3E]; }
+    __device__ void snapshot(int *snap) const {
+        snap[0] = st.counters[kCntRows];
+        snap[1] = stage == 2 ? st.counters[kCnt3E] : 0;
+        snap[2] = st.counters[kCntRejected];
     }
-    if (threadIdx.x == 0) st.counters[kCnt2E] = n2;
-}
-
-// Walk the multi-emitter queue slots in order: append second emitters after
-// the current rows, and route rejections to the next queue (3E) or the
-// rejected count.  stage 2 = after the 2E fit, 3 = after the 3E fit.
-__global__ void __launch_bounds__(kScanThreads) compact_multi_kernel(CascadeState st, float *__restrict__ loc,
-                                                                     int stage, int route_rejects_to_3e,
-                                                                     int max_rows) {
-    __shared__ int tot;
-    const int nslots = (stage == 2) ? st.counters[kCnt2E] : st.counters[kCnt3E];
-    const int8_t *res = (stage == 2) ? st.res2 : st.res3;
-    const float *extra = (stage == 2) ? st.extra2 : st.extra3;
-    const int *queue = (stage == 2) ? st.q2 : st.q3;
-    int rows = st.counters[kCntRows];
-    // after the 2E stage, rejects follow the records classified straight to 3E
-    int n3 = (stage == 2) ? st.counters[kCnt3E] : 0, rejected = st.counters[kCntRejected];
-    for (int base = 0; base < nslots; base += kScanThreads) {
-        const int k = base + threadIdx.x;
-        const int r = (k < nslots) ? res[k] : -1;
-        const int is2 = (r == 2);
-        const int is0 = (r == 0);
-        const int p2 = block_scan(is2, &tot);
-        const int t2 = tot;
-        if (is2) {
-            const int dst = rows + p2;
+    __device__ void flags(int k, int cnt, int (&f)[NP]) const {
+        const int r = k < cnt ? (stage == 2 ? st.res2[k] : st.res3[k]) : -1;
+        f[0] = r == 2;
+        f[1] = r == 0;
+    }
+    __device__ void emit(int p, int k, int pos, const int *snap) const {
+        if (p == 0) {
+            const int dst = snap[0] + pos;
             if (dst < max_rows) {
-                const float4 *s = reinterpret_cast<const float4 *>(extra + (size_t)k * 12);
+                const float4 *src = reinterpret_cast<const float4 *>((stage == 2 ? st.extra2 : st.extra3) + (size_t)k * 12);
                 float4 *d = reinterpret_cast<float4 *>(loc + (size_t)dst * 12);
-                d[0] = s[0];
-                d[1] = s[1];
-                d[2] = s[2];
+                d[0] = src[0];
+                d[1] = src[1];
+                d[2] = src[2];
             }
-        }
-        rows += t2;
-        const int p0 = block_scan(is0 && route_rejects_to_3e, &tot);
-        const int t0 = tot;
-        if (is0 && route_rejects_to_3e) st.q3[n3 + p0] = queue[k];
-        n3 += t0;
-        if (!route_rejects_to_3e) {
-            const int pr = block_scan(is0, &tot);
-            (void)pr;
-            rejected += tot;
+        } else if (route) {
+            st.q3[snap[1] + pos] = (stage == 2 ? st.q2 : st.q3)[k];
         }
     }
-    if (threadIdx.x == 0) {
+    __device__ void finish(const int (&t)[NP], const int *snap, int) const {
+        const int rows = snap[0] + t[0];
         st.counters[kCntRows] = rows;
-        st.counters[kCntRejected] = rejected;
-        if (stage == 2) st.counters[kCnt3E] = n3;
+        st.counters[kCntRejected] = snap[2] + (route ? 0 : t[1]);
+        if (stage == 2) st.counters[kCnt3E] = snap[1] + (route ? t[1] : 0);
         st.counters[kCntValid] = rows < max_rows ? rows : max_rows;
     }
+};
+
+template <class S>
+cudaError_t launch_compaction(const S &s, int max_count, const CascadeState &st, cudaStream_t stream) {
+    const int tiles = max_count > 0 ? (max_count + kScanThreads - 1) / kScanThreads : 1;
+    tile_count_kernel<S><<<tiles, kScanThreads, 0, stream>>>(s, st.scan);
+    tile_scatter_kernel<S><<<tiles, kScanThreads, 0, stream>>>(s, st.scan);
+    return cudaGetLastError();
 }
 
 __global__ void init_counters_kernel(CascadeState st, int n, const int *__restrict__ n_dev) {
@@ -179,10 +233,8 @@ __global__ void finish_kernel(CascadeState st, int max_rows) {
 }  // namespace
 
 cudaError_t cascade_classify(const CascadeArgs &a, const CascadeState &st) {
-    if (a.para.MultiEmitterFitEn)
-        classify_queues_kernel<<<1, kScanThreads, 0, a.stream>>>(a.wle, a.n, a.n_dev, 1, a.pred, st);
-    else
-        init_counters_kernel<<<1, 1, 0, a.stream>>>(st, a.n, a.n_dev);
+    if (a.para.MultiEmitterFitEn) return launch_compaction(ClassifyStage{a.wle, a.n, a.n_dev, a.pred, st}, a.n, st, a.stream);
+    init_counters_kernel<<<1, 1, 0, a.stream>>>(st, a.n, a.n_dev);
     return cudaGetLastError();
 }
 
@@ -212,8 +264,7 @@ cudaError_t cascade_tail(const CascadeArgs &a, const CascadeState &st) {
     cudaError_t e;
     FitLaunch f = cascade_single_launch(a, st);
     if (multi) {
-        append_2e_kernel<<<1, kScanThreads, 0, a.stream>>>(st);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if ((e = launch_compaction(Append2EStage{st}, n, st, a.stream)) != cudaSuccess) return e;
         const bool has2e = (p.LocType == QCS_LOCTYPE_GS2D) || as3d;
         if (has2e) {
             f.q = Queue{st.q2, st.counters + kCnt2E, 0};
@@ -221,14 +272,15 @@ cudaError_t cascade_tail(const CascadeArgs &a, const CascadeState &st) {
             f.to2e = nullptr;
             f.mo = MultiOut{st.res2, st.extra2};
             if ((e = launch_fit(as3d ? kAS3D2E : k2E, R, f)) != cudaSuccess) return e;
-            compact_multi_kernel<<<1, kScanThreads, 0, a.stream>>>(st, a.loc, 2, as3d ? 0 : 1, a.max_rows);
-            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+            if ((e = launch_compaction(CompactStage{st, a.loc, 2, as3d ? 0 : 1, a.max_rows}, n, st, a.stream)) !=
+                cudaSuccess)
+                return e;
             if (p.LocType == QCS_LOCTYPE_GS2D) {
                 f.q = Queue{st.q3, st.counters + kCnt3E, 0};
                 f.mo = MultiOut{st.res3, st.extra3};
                 if ((e = launch_fit(k3E, R, f)) != cudaSuccess) return e;
-                compact_multi_kernel<<<1, kScanThreads, 0, a.stream>>>(st, a.loc, 3, 0, a.max_rows);
-                if ((e = cudaGetLastError()) != cudaSuccess) return e;
+                if ((e = launch_compaction(CompactStage{st, a.loc, 3, 0, a.max_rows}, n, st, a.stream)) != cudaSuccess)
+                    return e;
             }
         }
     }

@@ -33,7 +33,11 @@ struct CascadeState {
     float *extra2;   // capacity x 12
     float *extra3;   // capacity x 12
     int *counters;   // kCntNum
+    int *scan;       // cascade_scan_ints(capacity): the multi-block compactions' tile counts
 };
+
+// ints of CascadeState::scan for `capacity` records
+constexpr int cascade_scan_ints(int capacity) { return 4 + 3 * ((capacity + 1023) / 1024 + 1); }
 
 struct CascadeArgs {
     qcs_loc_para para;

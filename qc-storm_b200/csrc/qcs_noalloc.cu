@@ -36,12 +36,13 @@ namespace {
 constexpr size_t kMax = QCS_NOALLOC_MAX_ROIS;
 constexpr size_t kAlign = 256;
 constexpr size_t al(size_t b) { return (b + kAlign - 1) / kAlign * kAlign; }
-// q_single, q2, q3 | to2e, res2, res3 | extra2, extra3 | counters
+// q_single, q2, q3 | to2e, res2, res3 | extra2, extra3 | counters | compaction tile counts
 constexpr size_t kOffQ = 0;
 constexpr size_t kOffFlags = kOffQ + 3 * al(kMax * sizeof(int));
 constexpr size_t kOffExtra = kOffFlags + 3 * al(kMax);
 constexpr size_t kOffCounters = kOffExtra + 2 * al(kMax * 12 * sizeof(float));
-constexpr size_t kScratchBytes = kOffCounters + al(qcs::kCntNum * sizeof(int));
+constexpr size_t kOffScan = kOffCounters + al(qcs::kCntNum * sizeof(int));
+constexpr size_t kScratchBytes = kOffScan + al(qcs::cascade_scan_ints((int)kMax) * sizeof(int));
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
@@ -99,6 +100,7 @@ extern "C" int qcs_localize_noalloc(const qcs_loc_para *p, const uint16_t *d_roi
     st.extra2 = reinterpret_cast<float *>(base + kOffExtra);
     st.extra3 = reinterpret_cast<float *>(base + kOffExtra + al(kMax * 12 * sizeof(float)));
     st.counters = reinterpret_cast<int *>(base + kOffCounters);
+    st.scan = reinterpret_cast<int *>(base + kOffScan);
     qcs::CascadeArgs a;
     a.para = *p;
     a.rois = d_rois;
