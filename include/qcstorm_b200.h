@@ -185,6 +185,10 @@ int qcs_extract_deinit(qcs_extract_data *c);
  * _CPU_NORMAL) or device memory (QCS_IMAGE_SOURCE_GPU, read in place, must
  * stay valid until the stream reaches this work).  Asynchronous on `stream`
  * (NULL: the context's own stream); the reference synchronises twice per call.
+ * Host frames are copied on the context's copy stream into one of two device
+ * buffers used in turn, so one call's copy runs while the previous call's
+ * kernels do (inside a stream capture the copy stays on `stream`); host
+ * frames must stay unchanged until this call's work has run.
  */
 int qcs_extract_molecules(qcs_extract_data *c, const uint16_t *img, int image_source, const qcs_loc_para *p,
                           int start_frame, int batched_num, void *stream);

@@ -547,6 +547,14 @@ struct qcs_extract_data {
     cudaStream_t stream = nullptr, last = nullptr;
     cudaEvent_t done = nullptr;  // recorded after the work of each call
     int first_frame = -1, end_frame = -1;
+    // host frames: two device buffers filled in turn on a copy stream, so the
+    // copy of one batch overlaps the kernels of the batch before it
+    uint16_t *d_raw2 = nullptr;
+    cudaStream_t copy = nullptr;
+    cudaEvent_t copied[2] = {nullptr, nullptr};    // a buffer's frames have arrived
+    cudaEvent_t consumed[2] = {nullptr, nullptr};  // the kernels that read a buffer are done
+    bool used[2] = {false, false};
+    int next_raw = 0;
 };
 
 namespace {
@@ -600,6 +608,13 @@ int qcs_extract_deinit(qcs_extract_data *c) {
     cudaFreeHost(c->h_wle);
     cudaFreeHost(c->h_state);
     if (c->done) cudaEventDestroy(c->done);
+    if (c->copy) cudaStreamSynchronize(c->copy);
+    cudaFree(c->d_raw2);
+    for (int b = 0; b < 2; ++b) {
+        if (c->copied[b]) cudaEventDestroy(c->copied[b]);
+        if (c->consumed[b]) cudaEventDestroy(c->consumed[b]);
+    }
+    if (c->copy) cudaStreamDestroy(c->copy);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return QCS_OK;
@@ -649,6 +664,12 @@ int qcs_extract_init_ex(const qcs_loc_para *p, int max_batched_num, int capacity
     if (e == cudaSuccess) e = cudaMallocHost((void **)&c->h_state, qcs::kStNum * sizeof(int));
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_raw2, px * sizeof(uint16_t));
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking);
+    for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
+        e = cudaEventCreateWithFlags(&c->copied[b], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->consumed[b], cudaEventDisableTiming);
+    }
     if (e == cudaSuccess) e = cudaMemsetAsync(c->d_state, 0, qcs::kStNum * sizeof(int), c->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(c->d_var_acc, 0, 4 * sizeof(unsigned long long), c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
@@ -678,10 +699,28 @@ int qcs_extract_molecules(qcs_extract_data *c, const uint16_t *img, int image_so
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
     QCS_CUDA(order_after_last(c, s), "order after the previous call");
     const uint16_t *raw = nullptr;
+    int buf = -1;  // the device frame buffer this call reads, for host frames outside a capture
     if (image_source == QCS_IMAGE_SOURCE_CPU_PINNED || image_source == QCS_IMAGE_SOURCE_CPU_NORMAL) {
-        QCS_CUDA(cudaMemcpyAsync(c->d_raw, img, (size_t)npx * sizeof(uint16_t), cudaMemcpyHostToDevice, s),
-                 "copy frames");
-        raw = c->d_raw;
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        QCS_CUDA(cudaStreamIsCapturing(s, &cs), "capture status");
+        if (cs != cudaStreamCaptureStatusNone) {
+            // under capture the copy stays on the captured stream
+            QCS_CUDA(cudaMemcpyAsync(c->d_raw, img, (size_t)npx * sizeof(uint16_t), cudaMemcpyHostToDevice, s),
+                     "copy frames");
+            raw = c->d_raw;
+        } else {
+            // the copy waits only for the kernels that last read its buffer (two
+            // calls ago), so it runs under the previous call's kernels
+            buf = c->next_raw;
+            c->next_raw ^= 1;
+            uint16_t *dst = buf ? c->d_raw2 : c->d_raw;
+            if (c->used[buf]) QCS_CUDA(cudaStreamWaitEvent(c->copy, c->consumed[buf], 0), "frame buffer reuse");
+            QCS_CUDA(cudaMemcpyAsync(dst, img, (size_t)npx * sizeof(uint16_t), cudaMemcpyHostToDevice, c->copy),
+                     "copy frames");
+            QCS_CUDA(cudaEventRecord(c->copied[buf], c->copy), "frames copied");
+            QCS_CUDA(cudaStreamWaitEvent(s, c->copied[buf], 0), "wait for the frames");
+            raw = dst;
+        }
     } else if (image_source == QCS_IMAGE_SOURCE_GPU) {
         raw = img;
     } else {
@@ -729,6 +768,10 @@ int qcs_extract_molecules(qcs_extract_data *c, const uint16_t *img, int image_so
     QCS_CUDA(qcs::launch_wle_presorted(c->d_rois, c->d_keys, c->d_state + qcs::kStBase, batch_max, c->R, p->LocType,
                                        c->d_wle, s),
              "WLE pre-pass");
+    if (buf >= 0) {
+        QCS_CUDA(cudaEventRecord(c->consumed[buf], s), "frame buffer read");
+        c->used[buf] = true;
+    }
     QCS_CUDA(mark_done(c, s), "record completion");
     return QCS_OK;
 }
