@@ -748,6 +748,39 @@ def consec_measure(stream, dist, world):
             "call": "qcs_consec_fit_device (link by sorted (frame, y) search, merge, remove, CRLB)"}
 
 
+def autotune_measure(stream, dist, world):
+    """The autotuner on small calls: qcs_loc_autotune's table for GS2D 7x7 and
+    the device time of 2,000-record calls (WLE pre-pass, fit, CRLB) with and
+    without it (the rows are identical)."""
+    import torch
+    from qcstorm_b200 import lib, synth
+    rec, para, _ = synth.gs2d_rois(20_000, R=R, seed=99)
+    d = torch.from_numpy(rec.view(np.int16)).cuda()
+    ctx = lib.LocContext(para, capacity=20_000)
+    wle = torch.from_numpy(ctx.wle(rec)).cuda()
+    sh = stream.cuda_stream
+    torch.cuda.synchronize()
+    table = ctx.autotune(d.data_ptr(), wle.data_ptr(), 20_000, stream=sh)
+    out = {"table": [{"records_up_to": a, "lanes_per_roi": b} for a, b in table]}
+    for m in (2000, 20_000):
+        res = {}
+        for name, tab in (("one_thread_per_roi", []), ("tuned", table)):
+            ctx.set_tuning(tab)
+            for _ in range(3):
+                ctx.localize_device(d.data_ptr(), m, 0, sh)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(20):
+                ctx.localize_device(d.data_ptr(), m, 0, sh)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            res[name + "_ms"] = max_over_ranks(e0.elapsed_time(e1), dist) / 20
+        out["call_%d_records" % m] = res
+    ctx.close()
+    return out
+
+
 def profile_learned(n, stream):
     """Three learned-start localization calls over n records inside the NVTX
     range "learned" (for ncu --nvtx-include learned/), after training."""
@@ -928,6 +961,7 @@ def main():
         learned = learned_measure(args, streams, ctxs, para, d_batches, h_batches, rec0, truth0, value, world, dist)
 
     consec = consec_measure(stream, dist, world)
+    tune = autotune_measure(stream, dist, world)
 
     shapes = None
     if not args.no_learned:
@@ -962,7 +996,7 @@ def main():
                          "algorithmic": "%d px-evals x %d MUFU per fit; peak = measured __expf/__logf rate" % (
                              PX_EVALS_PER_FIT, MUFU_PER_PX_EVAL)},
             "cpu_baseline": cpu, "clocks": clocks, "learned": learned, "learned_other_configs": shapes,
-            "consecutive_fit": consec,
+            "consecutive_fit": consec, "autotune": tune,
             "frames": frames,
         }
         print(json.dumps(line), flush=True)

@@ -422,6 +422,20 @@ int qcs_fit_single_device(int loc_type, const qcs_loc_para *p, const uint16_t *d
  * QCS_ERR_ARG otherwise. */
 int qcs_fit_single_group_device(int loc_type, const qcs_loc_para *p, const uint16_t *d_rois, const float *d_wle,
                                 int n, float *d_loc, int lanes, void *stream);
+/* Autotuner (no counterpart in the reference): times the single-emitter fit of
+ * the first m records of d_rois / d_wle (device, WLE rows given) for m = 256,
+ * 1,024, 4,096, ... up to n with one thread per ROI and with 8 lanes per ROI
+ * (also 4 and 16 for GS2D 7x7), and keeps in the context, per batch size,
+ * the fastest; qcs_loc_localize_device then fits a batch of n records with
+ * the lanes of the first entry whose size is >= n (larger batches: one
+ * thread per ROI).  Every choice gives the same rows bit for bit.  n >= 64
+ * records; overwrites the context's rows. */
+int qcs_loc_autotune(qcs_loc_data *c, const qcs_loc_para *p, const uint16_t *d_rois, const float *d_wle, int n,
+                     void *stream);
+/* The tuning table (returns its length; sizes / lanes may be NULL), or sets it
+ * (count 0..8 entries of (largest batch, lanes 1 / 4 / 8 / 16); 0 clears it). */
+int qcs_loc_tuning(const qcs_loc_data *c, int *sizes, int *lanes, int max_entries);
+int qcs_loc_set_tuning(qcs_loc_data *c, const int *sizes, const int *lanes, int count);
 /* LDLocData_TypeDef::LocPrecCalc_GaussianCRLB (bfgs_top.h:90,
  * LocPrecCalc_GaussianCRLB.cu:23-40): CRLB columns of n device rows. */
 int qcs_crlb_device(const qcs_loc_para *p, float *d_loc, int n, void *stream);

@@ -67,6 +67,11 @@ struct qcs_loc_data {
     int *q_refit = nullptr;         // learned multi-emitter path: records to refit plainly
     uint8_t *d_refit = nullptr;     //   their per-record flags
     uint8_t *d_cls = nullptr;       //   emitter-count class per record
+    // autotuned lanes per ROI of the single-emitter fit by batch size: batches of
+    // at most tune_n[k] records use tune_lanes[k] (first match); none: 1
+    int tune_count = 0;
+    int tune_n[8] = {0};
+    int tune_lanes[8] = {0};
     int pending = 0;                // an asynchronous host call awaits qcs_loc_finish
     int pending_n = 0;
     int valid = 0;
@@ -216,6 +221,12 @@ static int check_call(qcs_loc_data *c, const qcs_loc_para *p, int n) {
     return QCS_OK;
 }
 
+static int tuned_lanes(const qcs_loc_data *c, int n) {
+    for (int k = 0; k < c->tune_count; ++k)
+        if (n <= c->tune_n[k]) return c->tune_lanes[k];
+    return 1;
+}
+
 int qcs_loc_localize_device(qcs_loc_data *c, const uint16_t *d_rois, const float *d_wle, const qcs_loc_para *p,
                             int n, void *stream) {
     int st = check_call(c, p, n);
@@ -235,6 +246,7 @@ int qcs_loc_localize_device(qcs_loc_data *c, const uint16_t *d_rois, const float
     a.loc = c->d_loc;
     a.max_rows = c->max_rows;
     a.stream = s;
+    a.lanes = tuned_lanes(c, n);
     QCS_CUDA(qcs::run_cascade(a, c->st), "localization cascade");
     return QCS_OK;
 }
@@ -705,6 +717,96 @@ int qcs_fit_single_group_device(int loc_type, const qcs_loc_para *p, const uint1
     f.para = qcs::core_para(q);
     f.stream = static_cast<cudaStream_t>(stream);
     QCS_CUDA(qcs::launch_fit_group(kind, p->ROISize, lanes, f), "group fit launch");
+    return QCS_OK;
+}
+
+int qcs_loc_autotune(qcs_loc_data *c, const qcs_loc_para *p, const uint16_t *d_rois, const float *d_wle, int n,
+                     void *stream) {
+    int st = check_call(c, p, n);
+    if (st) return st;
+    if (!d_rois || !d_wle) return fail(QCS_ERR_ARG, "null pointer");
+    if (n < 64) return fail(QCS_ERR_ARG, "autotuning needs at least 64 records");
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+    const int kind = p->LocType == QCS_LOCTYPE_AS3D ? qcs::kAS3D : qcs::kGS2D;
+    c->tune_count = 0;
+    if (!qcs::group_fit_supported(kind, p->ROISize) || p->LocType == QCS_LOCTYPE_DH3D) return QCS_OK;
+    // lanes per ROI to try: 1 (one thread per ROI) and 8; 4 and 16 exist for GS2D 7x7 only
+    const int cand7[4] = {1, 4, 8, 16}, cand_other[2] = {1, 8};
+    const bool gs7 = kind == qcs::kGS2D && p->ROISize == 7;
+    const int *cand = gs7 ? cand7 : cand_other;
+    const int ncand = gs7 ? 4 : 2;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    QCS_CUDA(cudaEventCreate(&e0), "tuning events");
+    cudaError_t e = cudaEventCreate(&e1);
+    qcs_loc_para q = *p;
+    q.MultiEmitterFitEn = 0;
+    qcs::FitLaunch f;
+    f.rois = d_rois;
+    f.wle = d_wle;
+    f.loc = c->d_loc;
+    f.to2e = nullptr;
+    f.mo = qcs::MultiOut{nullptr, nullptr};
+    f.para = qcs::core_para(q);
+    f.stream = s;
+    int sizes[8], k = 0;
+    for (int m = 256; m < n && k < 7; m *= 4) sizes[k++] = m;
+    sizes[k++] = n;
+    for (int i = 0; i < k && e == cudaSuccess; ++i) {
+        const int m = sizes[i];
+        f.q = qcs::Queue{nullptr, nullptr, m};
+        f.max_count = m;
+        float best = 1e30f;
+        int best_lanes = 1;
+        for (int j = 0; j < ncand && e == cudaSuccess; ++j) {
+            const int lanes = cand[j];
+            auto run = [&]() {
+                return lanes == 1 ? qcs::launch_fit(kind, p->ROISize, f) : qcs::launch_fit_group(kind, p->ROISize, lanes, f);
+            };
+            e = run();  // warm-up
+            if (e == cudaSuccess) e = cudaEventRecord(e0, s);
+            for (int r = 0; r < 3 && e == cudaSuccess; ++r) e = run();
+            if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+            if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+            float ms = 0;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+            if (e == cudaSuccess && ms < best) {
+                best = ms;
+                best_lanes = lanes;
+            }
+        }
+        c->tune_n[i] = m;  // batches above the largest tuned size keep one thread per ROI
+        c->tune_lanes[i] = best_lanes;
+    }
+    if (e1) cudaEventDestroy(e1);
+    cudaEventDestroy(e0);
+    if (e != cudaSuccess) {
+        c->tune_count = 0;
+        return fail(QCS_ERR_CUDA, "autotuning", e);
+    }
+    c->tune_count = k;
+    return QCS_OK;
+}
+
+int qcs_loc_tuning(const qcs_loc_data *c, int *sizes, int *lanes, int max_entries) {
+    if (!c) return fail(QCS_ERR_ARG, "null context");
+    for (int i = 0; i < c->tune_count && i < max_entries; ++i) {
+        if (sizes) sizes[i] = c->tune_n[i];
+        if (lanes) lanes[i] = c->tune_lanes[i];
+    }
+    return c->tune_count;
+}
+
+int qcs_loc_set_tuning(qcs_loc_data *c, const int *sizes, const int *lanes, int count) {
+    if (!c) return fail(QCS_ERR_ARG, "null context");
+    if (count < 0 || count > 8 || (count > 0 && (!sizes || !lanes))) return fail(QCS_ERR_ARG, "0..8 entries");
+    for (int i = 0; i < count; ++i)
+        if (lanes[i] != 1 && lanes[i] != 4 && lanes[i] != 8 && lanes[i] != 16)
+            return fail(QCS_ERR_ARG, "lanes per ROI: 1, 4, 8 or 16");
+    for (int i = 0; i < count; ++i) {
+        c->tune_n[i] = sizes[i];
+        c->tune_lanes[i] = lanes[i];
+    }
+    c->tune_count = count;
     return QCS_OK;
 }
 

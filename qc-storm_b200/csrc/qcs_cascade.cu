@@ -294,7 +294,14 @@ cudaError_t run_cascade(const CascadeArgs &a, const CascadeState &st) {
     cudaError_t e = cascade_classify(a, st);
     if (e != cudaSuccess) return e;
     const bool as3d = (a.para.LocType == QCS_LOCTYPE_AS3D);
-    if ((e = launch_fit(as3d ? kAS3D : kGS2D, a.para.ROISize, cascade_single_launch(a, st))) != cudaSuccess) return e;
+    const int kind = as3d ? kAS3D : kGS2D;
+    // the lane-group kernel gives the one-thread kernel's rows bit for bit; which is faster depends on the batch
+    if (a.lanes > 1 && group_fit_supported(kind, a.para.ROISize))
+        e = launch_fit_group(kind, a.para.ROISize, (kind == kGS2D && a.para.ROISize == 7) ? a.lanes : 8,
+                             cascade_single_launch(a, st));
+    else
+        e = launch_fit(kind, a.para.ROISize, cascade_single_launch(a, st));
+    if (e != cudaSuccess) return e;
     return cascade_tail(a, st);
 }
 

@@ -49,6 +49,7 @@ struct CascadeArgs {
     int max_rows;
     cudaStream_t stream;
     const uint8_t *pred = nullptr;  // learned emitter-count class per record, or null (the reference's split)
+    int lanes = 1;  // lanes per ROI of the single-emitter fit: 1 (one thread per ROI) or 4 / 8 / 16 (group kernel)
 };
 
 // The whole localization call: queues, single-emitter fit, 2E / 3E fits,

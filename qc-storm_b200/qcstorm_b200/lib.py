@@ -130,6 +130,9 @@ _SIGS = {
     "qcs_consec_d_out_loc_arry": (C.c_void_p, [C.c_void_p]),
     "qcs_consec_ontime_ratio": (C.c_int, [C.c_void_p, C.c_void_p]),
     "qcs_consec_read_rows": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "qcs_loc_autotune": (C.c_int, [C.c_void_p, C.POINTER(LocPara), C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
+    "qcs_loc_tuning": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
+    "qcs_loc_set_tuning": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     "qcs_stat_init": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
     "qcs_stat_deinit": (C.c_int, [C.c_void_p]),
     "qcs_stat_reset_all": (C.c_int, [C.c_void_p]),
@@ -268,6 +271,25 @@ class LocContext:
         para = para or self.para
         check(self.lib.qcs_loc_localize_device_n(self.h, C.c_void_p(d_rois), C.c_void_p(d_wle), C.byref(para),
                                                  C.c_void_p(d_n), int(max_n), C.c_void_p(stream) if stream else None))
+
+    def autotune(self, d_rois, d_wle, n, para=None, stream=0):
+        """qcs_loc_autotune: lanes per ROI by batch size; returns the table [(largest batch, lanes)]."""
+        para = para or self.para
+        check(self.lib.qcs_loc_autotune(self.h, C.byref(para), C.c_void_p(d_rois), C.c_void_p(d_wle), int(n),
+                                        C.c_void_p(stream) if stream else None))
+        return self.tuning()
+
+    def tuning(self):
+        sizes = np.zeros(8, np.int32)
+        lanes = np.zeros(8, np.int32)
+        k = self.lib.qcs_loc_tuning(self.h, C.c_void_p(sizes.ctypes.data), C.c_void_p(lanes.ctypes.data), 8)
+        return [(int(sizes[i]), int(lanes[i])) for i in range(k)]
+
+    def set_tuning(self, table):
+        sizes = np.array([t[0] for t in table] or [0], np.int32)
+        lanes = np.array([t[1] for t in table] or [1], np.int32)
+        check(self.lib.qcs_loc_set_tuning(self.h, C.c_void_p(sizes.ctypes.data), C.c_void_p(lanes.ctypes.data),
+                                          len(table)))
 
     def read_rows(self, stream=0, para=None):
         """Rows of the last device call, on the host: (rows[n_valid, 12], ratios[7])."""
