@@ -156,7 +156,9 @@ struct SinglePrep {
 
 // PreEstimation_GS2D / PreEstimation_AS3D and the WLE mask widths: the start
 // point Ininf of the fit from the ROI's edge means and centre pixel.
-template <int R, int KIND>
+// PRE = false: the mask widths and bounds only, Ininf untouched (the
+// learned-start fit takes its start point from elsewhere).
+template <int R, int KIND, bool PRE = true>
 __device__ __forceinline__ SinglePrep single_prefit(const PixView &img, const float *pw, const CorePara &c,
                                                     float *Ininf) {
     SinglePrep sp;
@@ -170,7 +172,7 @@ __device__ __forceinline__ SinglePrep single_prefit(const PixView &img, const fl
         float WLE_SigmaX = fminf(SigmaL, SigmaU);
         WLE_SigmaX = fminf(WLE_SigmaX, R / 2.0f / 2.35f);
         // PreEstimation_GS2D
-        {
+        if constexpr (PRE) {
             const int CenterPos = R / 2;
             float Mean1, Mean2, Mean3, Mean4;
             edge_means<R>(img, Mean1, Mean2, Mean3, Mean4);
@@ -200,7 +202,7 @@ __device__ __forceinline__ SinglePrep single_prefit(const PixView &img, const fl
         float WLE_SigmaX = fminf(SigmaL, SigmaR);
         float WLE_SigmaY = fminf(SigmaU, SigmaD);
         // PreEstimation_AS3D
-        {
+        if constexpr (PRE) {
             const int CenterPos = R / 2;
             float Mean1, Mean2, Mean3, Mean4;
             edge_means<R>(img, Mean1, Mean2, Mean3, Mean4);
@@ -491,7 +493,7 @@ __global__ void __launch_bounds__(kTPB) fit_learned_kernel(const uint16_t *__res
     const RoiRef roi{s_img + tid, w, kTPB};
 
     float Ininf[P];
-    const SinglePrep sp = single_prefit<R, KIND>(img, pw, c, Ininf);  // mask widths (start replaced below)
+    const SinglePrep sp = single_prefit<R, KIND, false>(img, pw, c, Ininf);  // mask widths only
     wle_weights<R, MASK>(w, kTPB, sp.WLE_SigmaX, sp.WLE_SigmaY, sp.MoleculeType);
     const float *st = start + (size_t)id * P;
     Ininf[0] = st[0] * rAScalFactor;
