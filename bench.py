@@ -711,6 +711,7 @@ def consec_measure(stream, dist, world):
         cf.fit_device(d[g % 2].data_ptr(), int(sizes[g % 2]), para, stream=sh)
     merged = cf.fit_device(d[1].data_ptr(), int(sizes[1]), para, stream=sh)
     zeroed = int((cf.read_rows()[:, 0] == 0).sum())
+    on_ratios = cf.ontime_ratio()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
@@ -735,10 +736,17 @@ def consec_measure(stream, dist, world):
     s1.record(stream)
     torch.cuda.synchronize()
     ms_stat = max_over_ranks(s0.elapsed_time(s1), dist) / CONSEC_GROUPS
+    # the on-time fit the plug-ins run after each merge (host arithmetic, as in the reference)
+    t0 = time.perf_counter()
+    for _ in range(100):
+        mean_on, shown = stt.update_ontime(on_ratios)
+    us_on = (time.perf_counter() - t0) * 1e4
     stt.close()
     stat = {"rows_per_call": int(total / CONSEC_GROUPS), "ms_per_call": ms_stat,
             "rows_per_s": world * total / (ms_stat * 1e-3 * CONSEC_GROUPS),
             "activation_density_per_um2": float(means[6]), "mean_precision_nm": float(means[1]),
+            "ontime_fit": {"mean_ontime_frames": float(mean_on), "ratios_1_2_3_4plus": [float(v) for v in shown[:4]],
+                           "us_per_call": us_on, "call": "qcs_stat_update_ontime_ratio (host, 10 ratios)"},
             "call": "qcs_stat_get_statistical_inf_device (histograms, means, activation density over 30 frames)"}
     return {"statistics": stat, "workload": "rows of 7,500 blinking molecules over 2048 x 2048 frames (~%d rows per frame), %d frames "
                         "per call, threshold 80 nm at 100 nm pixels" % (int(counts.mean()), CONSEC_FRAMES_PER_GROUP),

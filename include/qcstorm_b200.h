@@ -367,8 +367,9 @@ int qcs_consec_ontime_ratio(const qcs_consec *c, float *out10);
 #define QCS_STAT_TV_PREC 8
 #define QCS_STAT_TV_SNR 9
 /* qcs_stat_series: TimeVary_TotalPhoton, _LocPrecisionXY, _PeakSNR, _Background,
- * _PSFWidth, _PSFWidth_Ctl, _LocDensity2D (statisticsInfo.h:89-96) */
-#define QCS_STAT_SERIES 7
+ * _PSFWidth, _PSFWidth_Ctl, _LocDensity2D (statisticsInfo.h:89-96), then
+ * TimeVary_OntimeF1Ratio .. F4Ratio (statisticsInfo.h:116-119) */
+#define QCS_STAT_SERIES 11
 #define QCS_STAT_SERIES_PHOTON 0
 #define QCS_STAT_SERIES_PREC 1
 #define QCS_STAT_SERIES_SNR 2
@@ -376,12 +377,17 @@ int qcs_consec_ontime_ratio(const qcs_consec *c, float *out10);
 #define QCS_STAT_SERIES_PSF 4
 #define QCS_STAT_SERIES_PSF_CTL 5
 #define QCS_STAT_SERIES_DENSITY 6
+#define QCS_STAT_SERIES_ONTIME_F1 7 /* ratios of on times of 1, 2, 3 and >= 4 frames */
+#define QCS_STAT_SERIES_ONTIME_F2 8
+#define QCS_STAT_SERIES_ONTIME_F3 9
+#define QCS_STAT_SERIES_ONTIME_F4 10
 typedef struct qcs_stat qcs_stat;
 /* FluoStatisticData_TypeDef::Init (statisticsInfo_top.cu:258): calls of at
  * most `capacity` rows (<= 0: 2 x QCS_MAX_POINT_NUM); starts reset. */
 int qcs_stat_init(int capacity, qcs_stat **out);
 int qcs_stat_deinit(qcs_stat *st);
-/* ResetAllDat (statisticsInfo_top.cu:391): histograms, means and time series cleared. */
+/* ResetAllDat (statisticsInfo_top.cu:391): histograms, means and time series
+ * cleared (the mean on time is kept, as the reference keeps MeanOntime). */
 int qcs_stat_reset_all(qcs_stat *st);
 /* GetStatisticalInf (statisticsInfo_top.cu:61) over n host rows: the four
  * histograms (qcs_stat_histograms), the means and the activation density
@@ -397,6 +403,18 @@ int qcs_stat_histograms(const qcs_stat *st, int *out4x1600);
 int qcs_stat_means(const qcs_stat *st, float *out10);
 /* Copies up to max_n entries of time series `which` into out (may be NULL); returns its length. */
 int qcs_stat_series(const qcs_stat *st, int which, float *out, int max_n);
+/* UpdateOntimeRatio (statisticsInfo_top.cu:23-57): takes the QCS_ONTIME_BINS
+ * on-time ratios of a consecutive-frame merge (qcs_consec_ontime_ratio), fits
+ * y = a * exp(b * i) to them by the reference's 2-parameter BFGS curve fit (BFGS
+ * for curve fitting/BFGSOptimizer.h, CurveFitting.cpp:27-58: 4 iterations, 11
+ * bisections), sets the mean on time 2 / (-log(1 - a) - b) frames, sums the
+ * ratios of 4 frames and more into entry 3, clamps entries 0..3 to [0, 1] and
+ * appends them to the series QCS_STAT_SERIES_ONTIME_F1..F4.  Host arithmetic,
+ * as in the reference: results equal its host build bit for bit. */
+int qcs_stat_update_ontime_ratio(qcs_stat *st, const float *ratios10);
+/* The mean on time (frames; 0 before the first update) and the QCS_ONTIME_BINS
+ * ratios of the last update as shown (entries 0..3 folded and clamped). */
+int qcs_stat_ontime(const qcs_stat *st, float *mean_ontime, float *ratios10);
 
 /* ---- WLE pre-pass: WLEParameterEstimation_TypeDef ---------------------- */
 /* WLEParameterEstimation_TypeDef::WLEParameterEstimate (WLEParaEstimation.h:41,

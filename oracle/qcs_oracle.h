@@ -82,6 +82,9 @@ int qcso_consec(const qcs_loc_para *p, const float *rows, const int *sizes, cons
 /* GetStatisticalInf over n_groups groups of sizes[g] rows in turn (after ResetAllDat); after call g:
  * hist[g * 6400 ..] the four 1600-bin histograms, means[g * 10 ..] the means (see qcs_oracle_stat.c). */
 int qcso_stat(const qcs_loc_para *p, const float *rows, const int *sizes, int n_groups, int *hist, float *means);
+/* UpdateOntimeRatio: the exponential fit of n (>= 4) on-time ratios, the mean on
+ * time, and the ratios with entries 4.. summed into entry 3 and 0..3 clamped. */
+int qcso_ontime(const float *ratios, int n, float *mean_ontime, float *out);
 
 #ifdef __cplusplus
 }

@@ -243,3 +243,126 @@ int qcso_stat(const qcs_loc_para *p, const float *rows, const int *sizes, int n_
     free(ts_snr);
     return QCS_OK;
 }
+
+/*
+ * On-time fit: FluoStatisticData_TypeDef::UpdateOntimeRatio
+ * (StatisticsInfo/statisticsInfo_top.cu:23-57) with the curve fit it runs,
+ * BFGSOptimizer<float, 2, 4, 11> over ExpFit_PreFitting / ExpFit_TargerF
+ * (BFGS for curve fitting/BFGSOptimizer.h:120-533, CurveFitting.cpp:27-58):
+ * least squares of y = a * exp(b * i), i = 0..n-1, from a = y0,
+ * b = log(y1 / y0) (0 unless y0, y1 > 0.01), in coordinates divided by
+ * max(|start|, 1); 4 quasi-Newton steps, each along the direction normalised
+ * to a mean |component| of 1 with the step length bracketed in [1e-5, 1] and
+ * halved 11 times; gradients by central differences of 0.002; the inverse
+ * Hessian updated by the BFGS formula.  Then the mean on time 2 / (k1 + k2),
+ * k1 = -log(1 - a), k2 = -b, and the ratios of on times of 4 frames and more
+ * summed into entry 3 and entries 0..3 clamped to [0, 1].  Every float
+ * operation separately rounded in the reference's order.
+ */
+static float ot_sse(const float *u, const float *scale, const float *y, int n)
+{
+    const float a = u[0] * scale[0], b = u[1] * scale[1];
+    float e = 0;
+    for (int i = 0; i < n; ++i) {
+        const float d = a * expf(b * i) - y[i];
+        e += d * d;
+    }
+    return e;
+}
+
+static void ot_grad(const float *u, const float *scale, const float *y, int n, float *g)
+{
+    float t[2] = {u[0], u[1]};
+    for (int k = 0; k < 2; ++k) {
+        t[k] = t[k] - 0.002f;
+        const float lo = ot_sse(t, scale, y, n);
+        t[k] = t[k] + 0.004f;
+        const float hi = ot_sse(t, scale, y, n);
+        g[k] = (hi - lo) * 250.0f;
+        t[k] = t[k] - 0.002f;
+    }
+}
+
+int qcso_ontime(const float *ratios, int n, float *mean_ontime, float *out)
+{
+    if (!ratios || !mean_ontime || !out || n < 4) return QCS_ERR_ARG;
+    float p[2], scale[2], g[2], d[2], H[4] = {1, 0, 0, 1};
+    p[0] = ratios[0];
+    p[1] = (ratios[0] > 0.01 && ratios[1] > 0.01) ? logf(ratios[1] / ratios[0]) : 0.0f;
+    for (int k = 0; k < 2; ++k) {
+        const float m = fabsf(p[k]);
+        scale[k] = m > 1.0f ? m : 1.0f;
+        p[k] = p[k] / scale[k];
+    }
+    ot_grad(p, scale, ratios, n, g);
+    d[0] = -g[0];
+    d[1] = -g[1];
+    for (int it = 0; it < 4; ++it) {
+        float tot = 0;
+        for (int k = 0; k < 2; ++k) tot += fabsf(d[k]);
+        tot = tot / 2;
+        for (int k = 0; k < 2; ++k) d[k] = d[k] / tot;
+        float pos[2] = {0.00001f, 1.0f}, x[4], f[2];
+        for (int k = 0; k < 2; ++k) {
+            x[k] = d[k] * 0.0001f + p[k];
+            x[2 + k] = d[k] * 1.0f + p[k];
+        }
+        f[0] = ot_sse(x, scale, ratios, n);
+        f[1] = ot_sse(x + 2, scale, ratios, n);
+        for (int b = 0; b < 11; ++b) {
+            const int sel = f[0] < f[1];
+            pos[sel] = (pos[0] + pos[1]) * 0.5f;
+            if (b < 10) {
+                for (int k = 0; k < 2; ++k) x[sel * 2 + k] = d[k] * pos[sel] + p[k];
+                f[sel] = ot_sse(x + sel * 2, scale, ratios, n);
+            }
+        }
+        const float step = (pos[0] + pos[1]) * 0.5f;
+        float s[2], yk[2], og[2];
+        for (int k = 0; k < 2; ++k) {
+            s[k] = d[k] * step;
+            p[k] = p[k] + s[k];
+        }
+        if (it < 3) {
+            og[0] = g[0];
+            og[1] = g[1];
+            ot_grad(p, scale, ratios, n, g);
+            for (int k = 0; k < 2; ++k) yk[k] = g[k] - og[k];
+            float sy = 0;
+            for (int k = 0; k < 2; ++k) sy += s[k] * yk[k];
+            sy = 1.0f / sy;
+            float ty[2], ts[2], A[4], S[4], T[4];
+            for (int k = 0; k < 2; ++k) {
+                ty[k] = yk[k] * sy;
+                ts[k] = s[k] * sy;
+            }
+            for (int r = 0; r < 2; ++r)
+                for (int c = 0; c < 2; ++c) {
+                    A[r * 2 + c] = (r == c ? 1.0f : 0.0f) - s[r] * ty[c];
+                    S[r * 2 + c] = s[r] * ts[c];
+                }
+            for (int r = 0; r < 2; ++r)
+                for (int c = 0; c < 2; ++c) {
+                    T[r * 2 + c] = 0;
+                    for (int k = 0; k < 2; ++k) T[r * 2 + c] += A[r * 2 + k] * H[k * 2 + c];
+                }
+            for (int r = 0; r < 2; ++r)
+                for (int c = 0; c < 2; ++c) {
+                    H[r * 2 + c] = 0;
+                    for (int k = 0; k < 2; ++k) H[r * 2 + c] += T[r * 2 + k] * A[c * 2 + k];
+                }
+            for (int k = 0; k < 4; ++k) H[k] = H[k] + S[k];
+            for (int r = 0; r < 2; ++r) {
+                d[r] = 0;
+                for (int c = 0; c < 2; ++c) d[r] -= H[r * 2 + c] * g[c];
+            }
+        }
+    }
+    const float a = p[0] * scale[0], b = p[1] * scale[1];
+    const float k1 = -logf(1 - a), k2 = -b;
+    *mean_ontime = 2 / (k1 + k2);
+    for (int i = 0; i < n; ++i) out[i] = ratios[i];
+    for (int i = 4; i < n; ++i) out[3] += out[i];
+    for (int i = 0; i < 4; ++i) out[i] = fminf(fmaxf(out[i], 0.0f), 1.0f);
+    return QCS_OK;
+}

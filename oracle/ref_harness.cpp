@@ -12,6 +12,7 @@
 //   qcsref_zero_remove ZeroLocalizationsRemovel_TypeDef::RemoveZeroLocalizations
 //   qcsref_consec      ConsecutiveFit_TypeDef::ConsecutiveFit_WeightedAvg over a sequence of groups
 //   qcsref_stat        FluoStatisticData_TypeDef::GetStatisticalInf over a sequence of groups
+//   qcsref_ontime      FluoStatisticData_TypeDef::UpdateOntimeRatio over a sequence of calls
 //                      (WLEParaEstimation.cpp:20-40)
 //   qcsref_extract     LDROIExtractData_TypeDef::ExtractMolecules (LDROIExtraction.cu:30-80)
 #include <cstdio>
@@ -323,6 +324,27 @@ int qcsref_stat(const qcs_loc_para *p, const float *rows, const int *sizes, int 
         off += (size_t)sizes[g];
     }
     sd.Deinit();
+    return 0;
+}
+
+// FluoStatisticData_TypeDef::UpdateOntimeRatio (StatisticsInfo/statisticsInfo_top.cu:23-57)
+// once per call c on ratios[c * MaxOnTimeConsecutiveNum ..] in turn, on one
+// object: after call c, mean[c] = MeanOntime and out[c * 10 ..] = h_OntimeRatio.
+// The function touches only h_OntimeRatio, MeanOntime and the four on-time time
+// series, so the object's device buffers are not set up.
+int qcsref_ontime(const float *ratios, int n_calls, float *mean, float *out) {
+    FluoStatisticData_TypeDef sd;
+    std::vector<float> buf(MaxOnTimeConsecutiveNum);
+    sd.h_OntimeRatio = buf.data();
+    for (int c = 0; c < n_calls; ++c) {
+        std::vector<float> in(ratios + (size_t)c * MaxOnTimeConsecutiveNum,
+                              ratios + (size_t)(c + 1) * MaxOnTimeConsecutiveNum);
+        sd.UpdateOntimeRatio(in.data());
+        mean[c] = sd.MeanOntime;
+        memcpy(out + (size_t)c * MaxOnTimeConsecutiveNum, sd.h_OntimeRatio, sizeof(float) * MaxOnTimeConsecutiveNum);
+    }
+    if ((int)sd.TimeVary_OntimeF1Ratio.size() != n_calls) return -2;
+    sd.h_OntimeRatio = nullptr;
     return 0;
 }
 

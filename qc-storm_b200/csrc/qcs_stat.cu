@@ -16,6 +16,7 @@
 // bins equal the reference's (same comparisons, separate roundings as its host
 // build); the four sums are reduced per block and then in block order
 // (deterministic; the reference adds them with float atomics in any order).
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <cub/device/device_radix_sort.cuh>
@@ -204,6 +205,125 @@ float series_mean(const std::vector<float> &v) {
     return mean;
 }
 
+// The on-time curve fit of UpdateOntimeRatio (statisticsInfo_top.cu:30-35):
+// least squares of y = a * exp(b * i) over the on-time ratios by the reference's
+// BFGSOptimizer<float, 2, 4, 11> with ExpFit_PreFitting / ExpFit_TargerF (BFGS
+// for curve fitting/BFGSOptimizer.h:120-533, CurveFitting.cpp:27-58).  The
+// parameters are searched divided by max(|start|, 1); each of the 4 steps
+// normalises the direction to a mean |component| of 1 and brackets the step
+// length in [1e-5, 1] (the lower end scored at 1e-4, as the reference does),
+// halving the bracket 11 times towards the lower loss; gradients are central
+// differences of 0.002 in the scaled coordinates; the inverse Hessian takes the
+// BFGS update (I - s y'/y's) H (I - y s'/y's) + s s'/y's.  A 10-point host
+// problem: every float operation is rounded separately in the reference's order
+// (host build, no contraction), so the result equals the reference's.
+struct DecayFit {
+    const float *y;
+    int n;
+    float scale[2];
+
+    float loss(const float *u) const {
+        const float a = u[0] * scale[0], b = u[1] * scale[1];
+        float e = 0;
+        for (int i = 0; i < n; ++i) {
+            const float r = a * expf(b * (float)i) - y[i];
+            e += r * r;
+        }
+        return e;
+    }
+    float loss_along(const float *p, const float *d, float t) const {
+        const float u[2] = {d[0] * t + p[0], d[1] * t + p[1]};
+        return loss(u);
+    }
+    void gradient(const float *p, float *g) const {
+        float u[2] = {p[0], p[1]};
+        for (int k = 0; k < 2; ++k) {
+            u[k] = u[k] - 0.002f;
+            const float below = loss(u);
+            u[k] = u[k] + 0.004f;
+            const float above = loss(u);
+            g[k] = (above - below) * 250.0f;
+            u[k] = u[k] - 0.002f;  // not exactly p[k] again: the next component sees it
+        }
+    }
+};
+
+void fit_decay(const float *y, int n, float *a, float *b) {
+    DecayFit f{y, n, {1.0f, 1.0f}};
+    float p[2];
+    p[0] = y[0];
+    p[1] = ((double)y[0] > 0.01 && (double)y[1] > 0.01) ? logf(y[1] / y[0]) : 0.0f;
+    for (int k = 0; k < 2; ++k) {
+        f.scale[k] = std::fabs(p[k]) > 1.0f ? std::fabs(p[k]) : 1.0f;
+        p[k] = p[k] / f.scale[k];
+    }
+    float g[2], d[2];
+    float h[2][2] = {{1.0f, 0.0f}, {0.0f, 1.0f}};
+    f.gradient(p, g);
+    d[0] = -g[0];
+    d[1] = -g[1];
+    constexpr int kSteps = 4, kHalvings = 11;
+    for (int step = 0; step < kSteps; ++step) {
+        float mean_abs = 0;
+        mean_abs += std::fabs(d[0]);
+        mean_abs += std::fabs(d[1]);
+        mean_abs = mean_abs / 2;
+        d[0] = d[0] / mean_abs;
+        d[1] = d[1] / mean_abs;
+        float lo = 0.00001f, hi = 1.0f;
+        float f_lo = f.loss_along(p, d, 0.0001f), f_hi = f.loss_along(p, d, 1.0f);
+        for (int k = 0; k < kHalvings; ++k) {
+            const float mid = (lo + hi) * 0.5f;
+            const bool last = k == kHalvings - 1;
+            if (f_lo < f_hi) {
+                hi = mid;
+                if (!last) f_hi = f.loss_along(p, d, hi);
+            } else {
+                lo = mid;
+                if (!last) f_lo = f.loss_along(p, d, lo);
+            }
+        }
+        const float t = (lo + hi) * 0.5f;
+        const float s[2] = {d[0] * t, d[1] * t};
+        p[0] = p[0] + s[0];
+        p[1] = p[1] + s[1];
+        if (step == kSteps - 1) break;
+        const float g0[2] = {g[0], g[1]};
+        f.gradient(p, g);
+        const float yk[2] = {g[0] - g0[0], g[1] - g0[1]};
+        float sy = 0;
+        sy += s[0] * yk[0];
+        sy += s[1] * yk[1];
+        const float inv = 1.0f / sy;
+        const float yi[2] = {yk[0] * inv, yk[1] * inv}, si[2] = {s[0] * inv, s[1] * inv};
+        float left[2][2], ss[2][2], lh[2][2];
+        for (int r = 0; r < 2; ++r)
+            for (int c = 0; c < 2; ++c) {
+                left[r][c] = (r == c ? 1.0f : 0.0f) - s[r] * yi[c];  // I - s y' / y's
+                ss[r][c] = s[r] * si[c];
+            }
+        for (int r = 0; r < 2; ++r)
+            for (int c = 0; c < 2; ++c) {
+                float acc = 0;
+                for (int k = 0; k < 2; ++k) acc += left[r][k] * h[k][c];
+                lh[r][c] = acc;
+            }
+        for (int r = 0; r < 2; ++r)
+            for (int c = 0; c < 2; ++c) {
+                float acc = 0;
+                for (int k = 0; k < 2; ++k) acc += lh[r][k] * left[c][k];  // right factor: the transpose
+                h[r][c] = acc + ss[r][c];
+            }
+        for (int r = 0; r < 2; ++r) {
+            float acc = 0;
+            for (int c = 0; c < 2; ++c) acc -= h[r][c] * g[c];
+            d[r] = acc;
+        }
+    }
+    *a = p[0] * f.scale[0];
+    *b = p[1] * f.scale[1];
+}
+
 }  // namespace
 
 struct qcs_stat {
@@ -221,6 +341,8 @@ struct qcs_stat {
     float *h_sums = nullptr;  // pinned, 5
     int *h_ints = nullptr;    // pinned, 5
     float means[QCS_STAT_MEANS] = {0};
+    float mean_ontime = 0;
+    float ontime[QCS_ONTIME_BINS] = {0};
     std::vector<float> series[QCS_STAT_SERIES];
     cudaStream_t stream = nullptr;
 };
@@ -405,6 +527,29 @@ int qcs_stat_histograms(const qcs_stat *st, int *out) {
 int qcs_stat_means(const qcs_stat *st, float *out) {
     if (!st || !out) return fail(QCS_ERR_ARG, "null argument");
     memcpy(out, st->means, sizeof(st->means));
+    return QCS_OK;
+}
+
+int qcs_stat_update_ontime_ratio(qcs_stat *st, const float *ratios) {
+    if (!st || !ratios) return fail(QCS_ERR_ARG, "null argument");
+    float *r = st->ontime;
+    memcpy(r, ratios, sizeof(st->ontime));
+    float a = 0, b = 0;
+    fit_decay(r, QCS_ONTIME_BINS, &a, &b);
+    const float k1 = -logf(1 - a), k2 = -b;
+    st->mean_ontime = 2 / (k1 + k2);
+    for (int i = 4; i < QCS_ONTIME_BINS; ++i) r[3] += r[i];
+    for (int i = 0; i < 4; ++i) {
+        r[i] = fminf(fmaxf(r[i], 0.0f), 1.0f);
+        st->series[QCS_STAT_SERIES_ONTIME_F1 + i].push_back(r[i]);
+    }
+    return QCS_OK;
+}
+
+int qcs_stat_ontime(const qcs_stat *st, float *mean_ontime, float *ratios) {
+    if (!st) return fail(QCS_ERR_ARG, "null statistics");
+    if (mean_ontime) *mean_ontime = st->mean_ontime;
+    if (ratios) memcpy(ratios, st->ontime, sizeof(st->ontime));
     return QCS_OK;
 }
 

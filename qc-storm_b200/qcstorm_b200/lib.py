@@ -142,6 +142,8 @@ _SIGS = {
     "qcs_stat_histograms": (C.c_int, [C.c_void_p, C.c_void_p]),
     "qcs_stat_means": (C.c_int, [C.c_void_p, C.c_void_p]),
     "qcs_stat_series": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int]),
+    "qcs_stat_update_ontime_ratio": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "qcs_stat_ontime": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_void_p]),
     "qcs_learned_create_for": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_ulonglong, C.POINTER(C.c_void_p)]),
     "qcs_learned_shape": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "qcs_learned_localize_device_n": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(LocPara),
@@ -660,9 +662,13 @@ class ConsecFit:
         ptr = self.lib.qcs_consec_h_out_loc_arry(self.h)
         rows = np.ctypeslib.as_array((C.c_float * (12 * n)).from_address(ptr)).reshape(n, 12).copy() if n else \
             np.zeros((0, 12), np.float32)
+        return rows, self.ontime_ratio()
+
+    def ontime_ratio(self):
+        """The last call's 10 on-time ratios (input of Statistics.update_ontime)."""
         on = np.zeros(10, np.float32)
         check(self.lib.qcs_consec_ontime_ratio(self.h, C.c_void_p(on.ctypes.data)))
-        return rows, on
+        return on
 
     def device_rows(self):
         return self.lib.qcs_consec_d_out_loc_arry(self.h)
@@ -674,6 +680,13 @@ class ConsecFit:
         if n:
             check(self.lib.qcs_consec_read_rows(self.h, C.c_void_p(out.ctypes.data)))
         return out
+
+
+# qcs_stat_series indices (QCS_STAT_SERIES_* in qcstorm_b200.h)
+STAT_SERIES_PHOTON, STAT_SERIES_PREC, STAT_SERIES_SNR, STAT_SERIES_BKG = 0, 1, 2, 3
+STAT_SERIES_PSF, STAT_SERIES_PSF_CTL, STAT_SERIES_DENSITY = 4, 5, 6
+STAT_SERIES_ONTIME_F1 = 7  # .. 10: ratios of on times of 1, 2, 3 and >= 4 frames
+STAT_SERIES = 11
 
 
 class Statistics:
@@ -718,6 +731,22 @@ class Statistics:
         check(self.lib.qcs_stat_histograms(self.h, C.c_void_p(hist.ctypes.data)))
         check(self.lib.qcs_stat_means(self.h, C.c_void_p(means.ctypes.data)))
         return hist, means
+
+    def update_ontime(self, ratios):
+        """UpdateOntimeRatio on the 10 on-time ratios of a consecutive-frame
+        merge (ConsecFit.fit's second result): (mean on time in frames, the 10
+        ratios as shown, entries 0..3 folded and clamped)."""
+        r = np.ascontiguousarray(ratios, np.float32).reshape(-1)
+        if r.size != 10:
+            raise ValueError("UpdateOntimeRatio takes 10 on-time ratios")
+        check(self.lib.qcs_stat_update_ontime_ratio(self.h, C.c_void_p(r.ctypes.data)))
+        return self.ontime()
+
+    def ontime(self):
+        m = C.c_float()
+        out = np.zeros(10, np.float32)
+        check(self.lib.qcs_stat_ontime(self.h, C.byref(m), C.c_void_p(out.ctypes.data)))
+        return m.value, out
 
     def series(self, which):
         n = self.lib.qcs_stat_series(self.h, int(which), None, 0)

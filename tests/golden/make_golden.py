@@ -35,9 +35,12 @@ def para_bytes(p):
 
 
 OUT = HERE
+ONLY = None
 
 
 def save(name, **arrays):
+    if ONLY and not name.startswith(ONLY):
+        return
     path = os.path.join(OUT, name + ".npz")
     np.savez_compressed(path, **arrays)
     print("wrote", path, os.path.getsize(path), "bytes")
@@ -56,9 +59,35 @@ def cases():
     return out
 
 
+def ontime_cases():
+    """On-time ratios: those of the reference's consecutive-frame merge over
+    blinking rows (one per call), noisy exponential decays, and edge cases (no
+    molecule, small or negative first ratios, ratios above 1, NaN from an empty
+    merge)."""
+    out = []
+    from qcstorm_b200.abi import default_para
+    for loc_type in (0, 1):
+        rows, counts = synth.blinking_rows(n_emitters=400, frames=24, seed=611 + loc_type, loc_type=loc_type)
+        para = default_para(LocType=loc_type, ConsecFit_DistanceTh_nm=80.0, PixelSize=100.0, QE=0.8)
+        _, on = O.consec(para, rows, synth.group_sizes(counts, 4), lib="ref")
+        out.extend(on)
+    rng = np.random.default_rng(612)
+    for k in range(48):
+        a, b = rng.uniform(0.2, 0.9), -rng.uniform(0.1, 3.0)
+        y = a * np.exp(b * np.arange(10)) * (1 + rng.normal(0, 0.1, 10))
+        out.append(y / y.sum() if k % 2 else y)
+    out += [np.zeros(10), np.r_[0.005, 0.5, np.zeros(8)], np.r_[0.5, 0.005, np.zeros(8)],
+            np.r_[1.2, 0.3, 0.1, np.zeros(7)], np.full(10, np.nan), np.r_[-0.1, 0.5, np.ones(8)],
+            np.r_[3.0, 2.0, np.ones(8)]]
+    return np.asarray(out, np.float32)
+
+
 def host():
     if O.ref_host() is None:
         sys.exit("oracle/_ref/libqcs_ref_host.so not built")
+    r = ontime_cases()
+    mean, shown = O.ontime(r, lib="ref")
+    save("ref_host_ontime", ratios=r, mean=mean, shown=shown)
     for name, rec, p in cases():
         wl = O.wle(p, rec, lib="ref")
         rows, ratios = O.localize(p, rec, wl, lib="ref")
@@ -114,8 +143,10 @@ if __name__ == "__main__":
     ap.add_argument("--host", action="store_true")
     ap.add_argument("--gpu", action="store_true")
     ap.add_argument("--out", default=HERE, help="directory for the fixtures (default: tests/golden)")
+    ap.add_argument("--only", default=None, help="write only the fixtures whose name starts with this")
     a = ap.parse_args()
     OUT = a.out
+    ONLY = a.only
     os.makedirs(OUT, exist_ok=True)
     if a.host:
         host()

@@ -222,6 +222,26 @@ def stat(para, rows, sizes, lib="oracle"):
     return hist, means
 
 
+def ontime(ratios, lib="oracle"):
+    """UpdateOntimeRatio over calls of 10 on-time ratios each (ratios [calls, 10])
+    through the oracle ("oracle") or the host build of the reference ("ref").
+    Returns (mean on time [calls], shown ratios [calls, 10])."""
+    ratios = np.ascontiguousarray(np.atleast_2d(ratios), np.float32)
+    c = ratios.shape[0]
+    mean = np.zeros(c, np.float32)
+    out = np.zeros((c, 10), np.float32)
+    if lib == "oracle":
+        for k in range(c):
+            m = C.c_float()
+            st = oracle().qcso_ontime(_p(ratios[k]), 10, C.byref(m), _p(out[k]))
+            assert st == 0, st
+            mean[k] = m.value
+    else:
+        st = ref_host().qcsref_ontime(_p(ratios), c, _p(mean), _p(out))
+        assert st == 0, st
+    return mean, out
+
+
 def render(para, rows, mode, fixed_prec=0.0, state=None, lib="oracle"):
     """Super-resolution render of rows through the oracle ("oracle"), the host
     build of the reference ("ref") or its CUDA build ("ref_gpu").  state:

@@ -84,6 +84,14 @@ def test_oracle_render_equals_reference_host(kind):
     same(hist, z["hist"])
 
 
+def test_oracle_ontime_equals_reference_host():
+    z = load("ref_host_ontime")
+    mean, shown = O.ontime(z["ratios"])
+    same(mean, z["mean"])
+    same(shown, z["shown"])
+    assert np.isnan(z["mean"]).sum() >= 1 and np.isfinite(z["mean"]).sum() > 50
+
+
 def product_fit(kind, p, rec, wl):
     import torch
     from qcstorm_b200 import lib as qlib

@@ -81,3 +81,56 @@ def test_stat_device_form_and_reset(cuda_ok):
     with pytest.raises(RuntimeError):
         st.update(np.zeros((int(max(sizes)) + 1, 12), np.float32), para)
     st.close()
+
+
+def test_ontime_fit_equals_reference(cuda_ok):
+    """qcs_stat_update_ontime_ratio against the reference's UpdateOntimeRatio
+    (golden outputs of its host build, and the oracle pinned to it): mean on
+    time and shown ratios bit for bit, call after call on one object; the four
+    on-time series follow the shown ratios; a reset clears them and keeps the
+    mean on time, as the reference does."""
+    import os
+    z = np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_host_ontime.npz"))
+    st = qlib.Statistics(capacity=16)
+    assert st.ontime()[0] == 0.0
+    means, shown = [], []
+    for r in z["ratios"]:
+        m, s = st.update_ontime(r)
+        means.append(m)
+        shown.append(s)
+    means = np.asarray(means, np.float32)
+    shown = np.asarray(shown, np.float32)
+    np.testing.assert_array_equal(means.view(np.uint32), z["mean"].view(np.uint32))
+    np.testing.assert_array_equal(shown.view(np.uint32), z["shown"].view(np.uint32))
+    for k in range(4):
+        np.testing.assert_array_equal(st.series(qlib.STAT_SERIES_ONTIME_F1 + k), shown[:, k])
+    last = st.ontime()[0]
+    st.reset()
+    assert st.series(qlib.STAT_SERIES_ONTIME_F1).size == 0
+    assert np.asarray(st.ontime()[0], np.float32).view(np.uint32) == np.asarray(last, np.float32).view(np.uint32)
+    with pytest.raises(ValueError):
+        st.update_ontime(np.zeros(9, np.float32))
+    st.close()
+
+
+def test_ontime_from_consecutive_fit(cuda_ok):
+    """The plug-ins' chain, ConsecutiveFit then UpdateOntimeRatio
+    (OnlineLocalizationLD.cpp:312): the product's on-time ratios fed to the
+    product's fit equal the oracle's fit of the same ratios."""
+    rows, counts = blinking_rows(n_emitters=1500, frames=20, seed=77, width=512)
+    para = default_para(LocType=0, ConsecFit_DistanceTh_nm=80.0, PixelSize=100.0, QE=0.8)
+    sizes = group_sizes(counts, 4)
+    cf = qlib.ConsecFit(capacity=int(max(sizes)))
+    st = qlib.Statistics(capacity=16)
+    o, ons = 0, []
+    for g, k in enumerate(sizes):
+        _, on = cf.fit(rows[o:o + k], para, is_end=g == len(sizes) - 1)
+        o += k
+        ons.append(on)
+        m, s = st.update_ontime(on)
+        m_o, s_o = O.ontime(on)
+        assert np.float32(m).view(np.uint32) == m_o.view(np.uint32)[0]
+        np.testing.assert_array_equal(s.view(np.uint32), s_o[0].view(np.uint32))
+    assert np.isfinite(m) and 0.1 < m < 20.0
+    cf.close()
+    st.close()

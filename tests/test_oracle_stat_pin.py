@@ -27,3 +27,23 @@ def test_stat_oracle_matches_reference_host_build(loc_type, multi):
     np.testing.assert_array_equal(h_ora, h_ref)
     np.testing.assert_array_equal(m_ora.view(np.uint32), m_ref.view(np.uint32))
     assert h_ref[0].sum() > 1000 and m_ref[0, 6] > 0
+
+
+def test_ontime_oracle_matches_reference_host_build():
+    """UpdateOntimeRatio: the exponential fit's mean on time and the folded,
+    clamped ratios, bit for bit (NaN where the reference gives NaN), on noisy
+    decays, normalised decays, flat and rising ratios and degenerate starts."""
+    rng = np.random.default_rng(41)
+    cases = []
+    for k in range(300):
+        a, b = rng.uniform(0.05, 1.0), -rng.uniform(0.02, 4.0)
+        y = a * np.exp(b * np.arange(10)) * (1 + rng.normal(0, 0.2, 10))
+        cases.append(y / y.sum() if k % 3 == 0 else y)
+    cases += [rng.uniform(0, 1, 10) for _ in range(40)]
+    cases += [np.zeros(10), np.r_[0.01, 0.01, np.zeros(8)], np.r_[0.011, 0.02, np.zeros(8)], np.ones(10)]
+    r = np.asarray(cases, np.float32)
+    m_ref, s_ref = O.ontime(r, lib="ref")
+    m_ora, s_ora = O.ontime(r, lib="oracle")
+    np.testing.assert_array_equal(m_ora.view(np.uint32), m_ref.view(np.uint32))
+    np.testing.assert_array_equal(s_ora.view(np.uint32), s_ref.view(np.uint32))
+    assert np.isfinite(m_ref).sum() > 250
