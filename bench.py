@@ -30,6 +30,7 @@ WLE + localization + CRLB) on all host cores, rank 0 only.
 import argparse
 import ctypes as C
 import json
+import math
 import os
 import statistics
 import subprocess
@@ -685,6 +686,188 @@ def learned_shapes_measure(streams, dist, world, rank):
     return out
 
 
+MIXED_TRAIN = 4_000_000    # training records of the mixed 7/9/11 workload (all three shapes)
+MIXED_EVAL = 10_000_000    # fresh evaluation records of it
+MIXED_CALL = 100_000       # records per localization call
+MIXED_EPOCHS = 2
+# (generator, ROI size, learned BFGS iterations, line-search steps)
+MIXED_SHAPES = (("gs2d", 7, 2, 6), ("as3d", 9, 3, 6), ("multi", 11, 2, 6))
+
+
+def _split(total, parts):
+    return [total // parts + (1 if i < total % parts else 0) for i in range(parts)]
+
+
+class _SingleAcc:
+    """Sums over calls for single-emitter shapes: position error (px), z error
+    (nm) and CRLB (px) over the records both modes accept."""
+
+    def __init__(self):
+        self.n = 0
+        self.se = {"plain": 0.0, "learned": 0.0}
+        self.sz = {"plain": 0.0, "learned": 0.0}
+        self.crlb = {"plain": 0.0, "learned": 0.0}
+        self.crlb_n = {"plain": 0, "learned": 0}
+        self.acc = {"plain": 0, "learned": 0}
+        self.total = 0
+
+    def add(self, rows, truth, o, R, pixel_nm):
+        rp, rl = rows["plain"], rows["learned"]
+        m = rp.shape[0]
+        both = (rp[:, 0] > 0) & (rl[:, 0] > 0)
+        self.n += int(both.sum())
+        self.total += m
+        tx, ty = truth["x"][o:o + m][both], truth["y"][o:o + m][both]
+        for mode, r in rows.items():
+            self.acc[mode] += int((r[:, 0] > 0).sum())
+            fx = r[both, 1].astype(np.float64) + R // 2 - 1024
+            fy = r[both, 2].astype(np.float64) + R // 2 - 1024
+            self.se[mode] += float(np.sum((fx - tx) ** 2 + (fy - ty) ** 2) / 2)
+            if "z" in truth:
+                self.sz[mode] += float(np.sum((r[both, 3].astype(np.float64) - truth["z"][o:o + m][both]) ** 2))
+            c = r[both, 9:11].astype(np.float64) / pixel_nm
+            c2 = (c[:, 0] ** 2 + c[:, 1] ** 2) / 2
+            fin = np.isfinite(c2)
+            self.crlb[mode] += float(np.sum(c2[fin]))
+            self.crlb_n[mode] += int(fin.sum())
+
+    def result(self, has_z):
+        out = {}
+        for mode in ("plain", "learned"):
+            d = {"rmse_px": math.sqrt(self.se[mode] / max(self.n, 1)),
+                 "crlb_px": math.sqrt(self.crlb[mode] / max(self.crlb_n[mode], 1)),
+                 "crlb_not_finite": self.n - self.crlb_n[mode],
+                 "accepted": self.acc[mode] / max(self.total, 1)}
+            if has_z:
+                d["z_rmse_nm"] = math.sqrt(self.sz[mode] / max(self.n, 1))
+            d["rmse_over_crlb"] = d["rmse_px"] / d["crlb_px"] if d["crlb_px"] > 0 else None
+            out[mode] = d
+        out["compared"] = self.n
+        out["basis"] = "records accepted by both; ground truth of the generator; CRLB = the rows' own (cols 9-10, finite ones)"
+        return out
+
+
+class _MultiAcc:
+    """Sums over calls for multi-emitter ROIs: localizations within 1 px of a
+    true emitter of their record, their squared distances."""
+
+    def __init__(self):
+        self.loc = {"plain": 0, "learned": 0}
+        self.hit = {"plain": 0, "learned": 0}
+        self.se = {"plain": 0.0, "learned": 0.0}
+
+    def add(self, rows, truth, o, R, pixel_nm):
+        for mode, r in rows.items():
+            r = r[r[:, 0] > 0]
+            rid = r[:, 11].astype(np.int64) - 1
+            fx = r[:, 1].astype(np.float64) + R // 2 - 1024
+            fy = r[:, 2].astype(np.float64) + R // 2 - 1024
+            dx = truth["x"][rid] - fx[:, None]
+            dy = truth["y"][rid] - fy[:, None]
+            d2 = np.nanmin(dx * dx + dy * dy, axis=1)
+            ok = d2 < 1.0
+            self.loc[mode] += int(r.shape[0])
+            self.hit[mode] += int(ok.sum())
+            self.se[mode] += float(d2[ok].sum())
+
+    def result(self, has_z):
+        out = {mode: {"localizations": self.loc[mode], "matched": self.hit[mode],
+                      "rmse_px": math.sqrt(self.se[mode] / max(self.hit[mode], 1))} for mode in ("plain", "learned")}
+        out["basis"] = "localizations within 1 px of a true emitter of their record"
+        return out
+
+
+def mixed_measure(streams, dist, world, rank):
+    """The learned path on the mixed 7x7 / 9x9 / 11x11 workload: the GS2D 7x7,
+    astigmatic 3D 9x9 and 1-3 emitter 11x11 generators in equal parts,
+    MIXED_TRAIN records (seeded, made on the GPU) labelled by plain fitting
+    train one network per ROI size, and MIXED_EVAL fresh records are localized
+    in calls of MIXED_CALL records of one size (the reference's API takes one
+    ROI size per call) plainly and with learned start points.  fits/s over the
+    whole evaluation stream (device time of every call, two contexts in turn),
+    accuracy against the generator's truth with the rows' own CRLB beside it."""
+    import torch
+    from qcstorm_b200 import lib, synth_torch as ST
+    s0 = streams[0]
+    sh = s0.cuda_stream
+    n_train = _split(MIXED_TRAIN, len(MIXED_SHAPES))
+    n_eval = _split(MIXED_EVAL, len(MIXED_SHAPES))
+    shapes = {}
+    tot_p = tot_l = 0.0
+    for i, (kind, R, iters, bis) in enumerate(MIXED_SHAPES):
+        para = ST.para(kind, R)
+        t0 = time.perf_counter()
+        d_tr, _ = ST.rois(kind, n_train[i], R, seed=20_000 + 100 * rank + i, device="cuda")
+        torch.cuda.synchronize()
+        ctx_tr = lib.LocContext(para, capacity=n_train[i])
+        ctx_tr.localize_device(d_tr.data_ptr(), n_train[i], 0, sh)
+        labels = lib.count_labels(ctx_tr, n_train[i], sh) if kind == "multi" else None
+        feat, scale = lib.LearnedNet.features(para, d_tr.data_ptr(), n_train[i], stream=sh)
+        tgt, valid = lib.LearnedNet.targets(para, d_tr.data_ptr(), ctx_tr.device_rows(), scale, n_train[i],
+                                            stream=sh)
+        s0.synchronize()
+        if labels is not None:
+            valid = valid * (labels == 0).float()
+        torch.cuda.synchronize()
+        net = lib.LearnedNet(batch=4096, seed=5, loc_type=para.LocType, roi_size=R)
+        net.train(feat, tgt, valid, epochs=MIXED_EPOCHS, lr=2e-3, stream=sh, classes=labels)
+        if kind == "multi":
+            net.set_count_threshold(0.5)
+        torch.cuda.synchronize()
+        ctx_tr.close()
+        del d_tr, feat, scale, tgt, valid, labels
+        train_s = time.perf_counter() - t0
+
+        d_ev, truth = ST.rois(kind, n_eval[i], R, seed=30_000 + 100 * rank + i, device="cuda")
+        torch.cuda.synchronize()
+        rb = R * (R + 1) * 2
+        base = d_ev.data_ptr()
+        calls = [(o, min(MIXED_CALL, n_eval[i] - o)) for o in range(0, n_eval[i], MIXED_CALL)]
+        ctxs = [lib.LocContext(para, capacity=MIXED_CALL) for _ in range(2)]
+
+        def plain(k, s, c=None):
+            o, m = calls[k % len(calls)]
+            (c or ctxs[k % 2]).localize_device(base + o * rb, m, 0, s.cuda_stream)
+
+        def learned(k, s, c=None):
+            o, m = calls[k % len(calls)]
+            net.localize(c or ctxs[k % 2], base + o * rb, m, iters=iters, bisections=bis, stream=s.cuda_stream)
+
+        ms_p = device_timed(len(calls), 3, plain, streams, dist)
+        ms_l = device_timed(len(calls), 3, learned, streams, dist)
+        tot_p += ms_p
+        tot_l += ms_l
+        truth_h = {k: v.cpu().numpy() for k, v in truth.items()}
+        acc = _MultiAcc() if kind == "multi" else _SingleAcc()
+        for k, (o, m) in enumerate(calls):
+            rows = {}
+            plain(k, s0, ctxs[0])
+            rows["plain"] = ctxs[0].read_rows(sh)[0]
+            learned(k, s0, ctxs[0])
+            rows["learned"] = ctxs[0].read_rows(sh)[0]
+            acc.add(rows, truth_h, o, R, para.PixelSize)
+        net.fused_status()
+        shapes["%s%d" % (kind, R)] = {
+            "train_records": n_train[i], "eval_records": n_eval[i], "calls": len(calls),
+            "plain_fits_per_s": n_eval[i] * world / (ms_p * 1e-3),
+            "learned_fits_per_s": n_eval[i] * world / (ms_l * 1e-3), "vs_plain": ms_p / ms_l,
+            "schedule": "learned %d x %d" % (iters, bis), "train_seconds": train_s,
+            "accuracy": acc.result(kind == "as3d")}
+        for c in ctxs:
+            c.close()
+        net.close()
+        del d_ev, truth, truth_h
+        torch.cuda.empty_cache()
+    return {"workload": "GS2D 7x7, astigmatic 3D 9x9 and 1-3 emitter 11x11 ROIs in equal parts (the three "
+                        "single-size generators), records made on the GPU from seeds",
+            "train_records": MIXED_TRAIN * world, "eval_records": MIXED_EVAL * world, "records_per_call": MIXED_CALL,
+            "train_epochs": MIXED_EPOCHS,
+            "plain_fits_per_s": MIXED_EVAL * world / (tot_p * 1e-3),
+            "learned_fits_per_s": MIXED_EVAL * world / (tot_l * 1e-3), "vs_plain": tot_p / tot_l,
+            "timing": "device time of every evaluation call, two contexts in turn, summed over the sizes",
+            "shapes": shapes}
+
+
 CONSEC_FRAMES_PER_GROUP = 32
 CONSEC_GROUPS = 8
 
@@ -855,6 +1038,8 @@ def main():
     ap.add_argument("--profile-learned", type=int, default=0, metavar="N",
                     help="only train the start-point network and run 3 learned-start calls on N records")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-start measurement")
+    ap.add_argument("--no-mixed", action="store_true",
+                    help="skip the mixed 7/9/11 learned measurement (4e6 training, 1e7 evaluation records)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -971,9 +1156,11 @@ def main():
     consec = consec_measure(stream, dist, world)
     tune = autotune_measure(stream, dist, world)
 
-    shapes = None
+    shapes = mixed = None
     if not args.no_learned:
         shapes = learned_shapes_measure(streams, dist, world, rank)
+        if not args.no_mixed:
+            mixed = mixed_measure(streams, dist, world, rank)
 
     frames = None
     if not args.no_frames:
@@ -1004,6 +1191,7 @@ def main():
                          "algorithmic": "%d px-evals x %d MUFU per fit; peak = measured __expf/__logf rate" % (
                              PX_EVALS_PER_FIT, MUFU_PER_PX_EVAL)},
             "cpu_baseline": cpu, "clocks": clocks, "learned": learned, "learned_other_configs": shapes,
+            "learned_mixed_7_9_11": mixed,
             "consecutive_fit": consec, "autotune": tune,
             "frames": frames,
         }

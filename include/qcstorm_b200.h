@@ -663,7 +663,8 @@ int qcs_locfile_close(qcs_locfile *f);
  * take the device-wide synchronisation of cudaMalloc/cudaFree mid-stream.
  * Same result as qcs_loc_localize_device (classify, single-emitter fit,
  * 2E/3E cascade, CRLB) on caller-owned device buffers: n records d_rois, WLE
- * rows d_wle (required), rows into d_rows (room for 2 x n rows), row count
+ * rows d_wle (required), rows into d_rows (room for 2 x n rows, 16-byte
+ * aligned, else QCS_ERR_ARG), row count
  * into *d_nvalid (device int, may be NULL).  Allocates nothing: its queues
  * and counters live in one fixed library array, so n is limited to
  * QCS_NOALLOC_MAX_ROIS (else QCS_ERR_CAPACITY).  The first call on a device

@@ -168,9 +168,11 @@ int qcs_loc_init_capacity(const qcs_loc_para *p, int capacity, qcs_loc_data **ou
     if (e == cudaSuccess) e = A((void **)&c->d_loc, (size_t)c->max_rows * QCS_OUT_PARA_NUM * sizeof(float));
     c->wle_scratch = qcs::wle_scratch_bytes(capacity);
     if (e == cudaSuccess) e = A(&c->d_wle_scratch, c->wle_scratch);
-    // cascade state in one allocation
-    const size_t a_int = cap * sizeof(int), a_u8 = (cap + 255) / 256 * 256, a_row = cap * 12 * sizeof(float);
-    const size_t a_scan = ((size_t)qcs::cascade_scan_ints(capacity) * sizeof(int) + 255) / 256 * 256;
+    // cascade state in one allocation; every part starts on a 256-byte boundary whatever the capacity (the
+    // kernels move 12-float rows as float4, which needs 16-byte alignment)
+    auto round256 = [](size_t b) { return (b + 255) / 256 * 256; };
+    const size_t a_int = round256(cap * sizeof(int)), a_u8 = round256(cap), a_row = round256(cap * 12 * sizeof(float));
+    const size_t a_scan = round256((size_t)qcs::cascade_scan_ints(capacity) * sizeof(int));
     const size_t bytes = 3 * a_int + 3 * a_u8 + 2 * a_row + 256 + a_scan;
     if (e == cudaSuccess) e = A(&c->d_state, bytes);
     if (e == cudaSuccess) e = cudaMallocHost((void **)&c->h_loc, (size_t)c->max_rows * QCS_OUT_PARA_NUM * sizeof(float));
@@ -183,7 +185,8 @@ int qcs_loc_init_capacity(const qcs_loc_para *p, int capacity, qcs_loc_data **ou
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
     if (e == cudaSuccess) e = qcs::wle_sorter_create(capacity, c->d_wle_scratch, &c->wle_sorter);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_done, cudaEventDisableTiming);
-    if (e == cudaSuccess) e = A((void **)&c->d_start, cap * (6 * sizeof(float) + sizeof(int) + 2));
+    const size_t b_start = round256(cap * 6 * sizeof(float)), b_refit = round256(cap * sizeof(int));
+    if (e == cudaSuccess) e = A((void **)&c->d_start, b_start + b_refit + 2 * round256(cap));
     if (e != cudaSuccess) {
         qcs_loc_deinit(c);
         return fail(e == cudaErrorMemoryAllocation ? QCS_ERR_NOMEM : QCS_ERR_CUDA, "qcs_loc_init", e);
@@ -199,9 +202,10 @@ int qcs_loc_init_capacity(const qcs_loc_para *p, int capacity, qcs_loc_data **ou
     c->st.extra3 = reinterpret_cast<float *>(s); s += a_row;
     c->st.counters = reinterpret_cast<int *>(s); s += 256;
     c->st.scan = reinterpret_cast<int *>(s);
-    c->q_refit = reinterpret_cast<int *>(c->d_start + cap * 6);
-    c->d_refit = reinterpret_cast<uint8_t *>(c->q_refit + cap);
-    c->d_cls = c->d_refit + cap;
+    char *b = reinterpret_cast<char *>(c->d_start);
+    c->q_refit = reinterpret_cast<int *>(b + b_start);
+    c->d_refit = reinterpret_cast<uint8_t *>(b + b_start + b_refit);
+    c->d_cls = c->d_refit + round256(cap);
     *out = c;
     return QCS_OK;
 }

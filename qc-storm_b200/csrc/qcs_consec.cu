@@ -268,12 +268,15 @@ int qcs_consec_init(int capacity, qcs_consec **out) {
     cudaError_t e = cudaMalloc((void **)&c->d_last, cap * 12 * sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_work, T * 12 * sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_fwd, 2 * T * sizeof(int));
-    if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_keys, 2 * T * sizeof(uint64_t) + 2 * T * sizeof(int));
+    // keys, sorted keys, values, sorted values, each from a 256-byte boundary
+    const size_t bk = (T * sizeof(uint64_t) + 255) / 256 * 256, bv = (T * sizeof(int) + 255) / 256 * 256;
+    if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_keys, 2 * bk + 2 * bv);
     if (e == cudaSuccess) {
         c->d_bwd = c->d_fwd + T;
-        c->d_skeys = c->d_keys + T;
-        c->d_vals = reinterpret_cast<int *>(c->d_keys + 2 * T);
-        c->d_svals = c->d_vals + T;
+        char *b = reinterpret_cast<char *>(c->d_keys);
+        c->d_skeys = reinterpret_cast<uint64_t *>(b + bk);
+        c->d_vals = reinterpret_cast<int *>(b + 2 * bk);
+        c->d_svals = reinterpret_cast<int *>(b + 2 * bk + bv);
         e = cub::DeviceRadixSort::SortPairs(nullptr, c->sort_bytes, c->d_keys, c->d_skeys, c->d_vals, c->d_svals,
                                             (int)T, 0, 64);
     }

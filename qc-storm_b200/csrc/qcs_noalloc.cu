@@ -65,6 +65,8 @@ extern "C" int qcs_localize_noalloc(const qcs_loc_para *p, const uint16_t *d_roi
     g_msg[0] = 0;
     if (!p || !d_rois || !d_wle || !d_rows || n < 0) return noalloc_fail(QCS_ERR_ARG, "null pointer or negative n");
     if (n > QCS_NOALLOC_MAX_ROIS) return noalloc_fail(QCS_ERR_CAPACITY, "n above QCS_NOALLOC_MAX_ROIS");
+    if (reinterpret_cast<uintptr_t>(d_rows) & 15)
+        return noalloc_fail(QCS_ERR_ARG, "d_rows must be 16-byte aligned (rows are written 16 bytes at a time)");
     const int R = p->ROISize;
     if (R < 5 || R > 17 || (R & 1) == 0 || (p->MultiEmitterFitEn && R > 13))
         return noalloc_fail(QCS_ERR_ROISIZE, "unsupported ROISize");

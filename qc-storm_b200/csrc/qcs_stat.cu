@@ -464,13 +464,16 @@ int qcs_stat_init(int capacity, qcs_stat **out) {
     cudaError_t e = cudaMalloc((void **)&st->d_rows, cap * 12 * sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc((void **)&st->d_hist, 4 * kLenMax * sizeof(int) + 16 * sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc((void **)&st->d_part, (nb * 5 + 8) * sizeof(float));
-    if (e == cudaSuccess) e = cudaMalloc((void **)&st->d_keys, 2 * cap * sizeof(uint64_t) + 2 * cap * sizeof(int));
+    // keys, sorted keys, values, sorted values, each from a 256-byte boundary
+    const size_t bk = (cap * sizeof(uint64_t) + 255) / 256 * 256, bv = (cap * sizeof(int) + 255) / 256 * 256;
+    if (e == cudaSuccess) e = cudaMalloc((void **)&st->d_keys, 2 * bk + 2 * bv);
     if (e == cudaSuccess) {
         st->d_ints = st->d_hist + 4 * kLenMax;
         st->d_sums = st->d_part + nb * 5;
-        st->d_skeys = st->d_keys + cap;
-        st->d_vals = reinterpret_cast<int *>(st->d_keys + 2 * cap);
-        st->d_svals = st->d_vals + cap;
+        char *b = reinterpret_cast<char *>(st->d_keys);
+        st->d_skeys = reinterpret_cast<uint64_t *>(b + bk);
+        st->d_vals = reinterpret_cast<int *>(b + 2 * bk);
+        st->d_svals = reinterpret_cast<int *>(b + 2 * bk + bv);
         e = cub::DeviceRadixSort::SortPairs(nullptr, st->sort_bytes, st->d_keys, st->d_skeys, st->d_vals, st->d_svals,
                                             capacity, 0, 64);
     }
