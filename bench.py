@@ -604,6 +604,22 @@ def shape_accuracy(kind, plain, learned, rec, truth, R):
             "basis": "records accepted by both; ground truth of the generator"}
 
 
+TWO_ITERS = 3  # BFGS iterations of the learned-start two-emitter fits (6 line-search steps)
+
+
+def train_two_emitter_net(ctx_tr, para, d_tr, feat, scale, n, R, epochs, stream):
+    """A two-emitter start-point network trained on the records whose plain
+    two-emitter fit (the plain multi-emitter call just made on ctx_tr) kept
+    both emitters."""
+    from qcstorm_b200 import lib
+    t2, v2 = lib.two_emitter_targets(ctx_tr, para, d_tr.data_ptr(), scale, n, stream.cuda_stream)
+    stream.synchronize()
+    net2 = lib.LearnedNet(batch=4096, seed=6, loc_type=lib.LEARNED_GS2D_2E, roi_size=R)
+    net2.train(feat, t2, v2, epochs=epochs, lr=2e-3, stream=stream.cuda_stream)
+    stream.synchronize()
+    return net2
+
+
 def learned_shapes_measure(streams, dist, world, rank):
     """The learned path on the other configurations' generators, each against
     plain fitting of the same device-resident records with two contexts in
@@ -634,8 +650,10 @@ def learned_shapes_measure(streams, dist, world, rank):
         torch.cuda.synchronize()
         net = lib.LearnedNet(batch=4096, seed=5, loc_type=para.LocType, roi_size=R)
         net.train(feat, tgt, valid, epochs=TRAIN_EPOCHS, lr=2e-3, stream=sh, classes=labels)
+        net2 = None
         if kind == "multi":
             net.set_count_threshold(0.5)
+            net2 = train_two_emitter_net(ctx_tr, para, d_tr, feat, scale, SHAPE_TRAIN, R, TRAIN_EPOCHS, s0)
         torch.cuda.synchronize()
         ctx_tr.close()
         del d_tr, feat, scale, tgt, valid, labels
@@ -664,6 +682,25 @@ def learned_shapes_measure(streams, dist, world, rank):
         rows_l, ratios_l = ctxs[0].read_rows(sh)
         refits = net.refits(ctxs[0])
         net.fused_status()
+        two = None
+        if net2 is not None:
+            net.set_two_emitter(net2, iters=TWO_ITERS, bisections=6)
+            ms_l2 = device_timed(SHAPE_STEPS, 3, learned, streams, dist)
+            learned(0, s0, ctxs[0])
+            rows_l2, _ = ctxs[0].read_rows(sh)
+            two = {"learned_fits_per_s": job_rate(SHAPE_STEPS, SHAPE_RECORDS, world, ms_l2), "vs_plain": ms_p / ms_l2,
+                   "schedule": "two-emitter fits from the network's start points, %d x 6 (plain: 13 x 11); poor ones "
+                               "on to the three-emitter fit" % TWO_ITERS,
+                   "accuracy": multi_truth_match(rows_l2, recs[0], truths[0], R)}
+            net.set_two_emitter(net2, iters=TWO_ITERS, bisections=6, fallback="plain")
+            ms_l3 = device_timed(SHAPE_STEPS, 3, learned, streams, dist)
+            learned(0, s0, ctxs[0])
+            rows_l3, _ = ctxs[0].read_rows(sh)
+            two["plain_refit"] = {"learned_fits_per_s": job_rate(SHAPE_STEPS, SHAPE_RECORDS, world, ms_l3),
+                                  "two_emitter_refits_per_call": net.refits_2e(ctxs[0]),
+                                  "accuracy": multi_truth_match(rows_l3, recs[0], truths[0], R)}
+            net.set_two_emitter(None)
+            net2.close()
         out[kind] = {
             "workload": ("astigmatic 3D 9x9 ROIs, z U(-600,600) nm, photons log-U[1000,8000], background U(20,150), "
                          "camera ADU (offset 100, 0.45 e-/ADU)" if kind == "as3d" else
@@ -680,6 +717,8 @@ def learned_shapes_measure(streams, dist, world, rank):
             "accuracy": shape_accuracy(kind, rows_p, rows_l, recs[0], truths[0], R),
             "train": {"records": SHAPE_TRAIN, "epochs": TRAIN_EPOCHS, "seconds": train_s},
         }
+        if two is not None:
+            out[kind]["with_two_emitter_starts"] = two
         for c in ctxs:
             c.close()
         net.close()
@@ -811,8 +850,11 @@ def mixed_measure(streams, dist, world, rank):
         torch.cuda.synchronize()
         net = lib.LearnedNet(batch=4096, seed=5, loc_type=para.LocType, roi_size=R)
         net.train(feat, tgt, valid, epochs=MIXED_EPOCHS, lr=2e-3, stream=sh, classes=labels)
+        net2 = None
         if kind == "multi":
             net.set_count_threshold(0.5)
+            net2 = train_two_emitter_net(ctx_tr, para, d_tr, feat, scale, n_train[i], R, MIXED_EPOCHS, s0)
+            net.set_two_emitter(net2, iters=TWO_ITERS, bisections=6)
         torch.cuda.synchronize()
         ctx_tr.close()
         del d_tr, feat, scale, tgt, valid, labels
@@ -851,10 +893,15 @@ def mixed_measure(streams, dist, world, rank):
             "train_records": n_train[i], "eval_records": n_eval[i], "calls": len(calls),
             "plain_fits_per_s": n_eval[i] * world / (ms_p * 1e-3),
             "learned_fits_per_s": n_eval[i] * world / (ms_l * 1e-3), "vs_plain": ms_p / ms_l,
-            "schedule": "learned %d x %d" % (iters, bis), "train_seconds": train_s,
+            "schedule": "learned %d x %d" % (iters, bis) + (
+                "; two-emitter fits from the network's start points, %d x 6" % TWO_ITERS if net2 else ""),
+            "train_seconds": train_s,
             "accuracy": acc.result(kind == "as3d")}
         for c in ctxs:
             c.close()
+        if net2 is not None:
+            net.set_two_emitter(None)
+            net2.close()
         net.close()
         del d_ev, truth, truth_h
         torch.cuda.empty_cache()

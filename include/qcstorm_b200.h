@@ -478,6 +478,10 @@ int qcs_learned_param_count(void);
 /* A network for loc_type (QCS_LOCTYPE_GS2D or QCS_LOCTYPE_AS3D) and ROISize 7,
  * 9 or 11 (else QCS_ERR_ROISIZE); batch: training batch size and inference
  * chunk (<= 0: 4096); seed of the initial weights. */
+/* Network kind for the start points of the GS2D two-emitter fit (the
+ * multi-emitter cascade's 2E stage): 8 outputs, dx, dy of emitter 0 and of
+ * emitter 1, log(peak / range) of each, sigma - 1.3, (background - min) / range. */
+#define QCS_LEARNED_GS2D_2E 16
 int qcs_learned_create_for(int loc_type, int roi_size, int batch, unsigned long long seed, qcs_learned_net **out);
 /* qcs_learned_create_for(QCS_LOCTYPE_GS2D, 7, batch, seed, out). */
 int qcs_learned_create(int batch, unsigned long long seed, qcs_learned_net **out);
@@ -525,6 +529,31 @@ int qcs_loc_count_labels_device(qcs_loc_data *c, int n, float *d_labels, void *s
  * the WLE classes alone, as the reference does.  QCS_ERR_ARG outside [0, 1]. */
 int qcs_learned_set_count_threshold(qcs_learned_net *net, float th);
 float qcs_learned_count_threshold(const qcs_learned_net *net);
+/* Attaches a QCS_LEARNED_GS2D_2E network `two` of the same ROI size to the
+ * GS2D network `net` (NULL detaches): learned localization calls with
+ * multi-emitter fitting on then start the cascade's two-emitter fits from
+ * its start points with `iters` BFGS iterations of `bisections` line-search
+ * steps (3 or 4 of 6, or the reference's 13 of 11) and the analytic gradient.
+ * A fit is poor when no emitter is kept or when the two-emitter model's
+ * Poisson deviance exceeds dev_th (0: 2 ROISize^2 + 2); poor fits go on to the
+ * three-emitter fit, as the reference's rejected two-emitter fits do
+ * (fallback QCS_TWO_FALLBACK_3E), or are fitted again by the reference's
+ * two-emitter fit (QCS_TWO_FALLBACK_PLAIN: one more pass of that fit). */
+#define QCS_TWO_FALLBACK_3E 0
+#define QCS_TWO_FALLBACK_PLAIN 1
+int qcs_learned_set_two_emitter(qcs_learned_net *net, qcs_learned_net *two, int iters, int bisections,
+                                float dev_th, int fallback);
+/* Two-emitter fits that the last learned call on c redid with the reference's
+ * two-emitter fit (synchronises the device). */
+int qcs_learned_refit_2e_num(qcs_loc_data *c, int *n);
+/* Training targets of a QCS_LEARNED_GS2D_2E network from the plain
+ * multi-emitter call just made on c over the same n records (GS2D, ROI size 7,
+ * 9 or 11): for each record whose two-emitter fit kept both emitters, 8 floats
+ * (dx, dy of the first emitter row and of the second, log(peak e- / range) of
+ * each, sigma - 1.3, (background e- - min) / range; ranges d_scale from
+ * qcs_learned_features_device) and valid = 1; zeros elsewhere. */
+int qcs_loc_two_emitter_targets_device(qcs_loc_data *c, const uint16_t *d_rois, const qcs_loc_para *p, int n,
+                                       const float *d_scale, float *d_targets, float *d_valid, void *stream);
 /* Start points (as qcs_learned_start_device) and emitter-count classes
  * (uint8 per record, at the routing threshold, or 0.5 when routing is off)
  * of n device records. */
@@ -532,8 +561,9 @@ int qcs_learned_classes_device(qcs_learned_net *net, const qcs_loc_para *p, cons
                                float *d_start, uint8_t *d_classes, void *stream);
 /* Start points of n device records (GS2D n x 5: peak e-, x, y, sigma,
  * background e-; AS3D n x 6: peak e-, x, y, sigma_x, sigma_y, background
- * e-); d_work holds qcs_learned_work_bytes(n) bytes (unused by the fused
- * path). */
+ * e-; QCS_LEARNED_GS2D_2E n x 8: peak e-, x, y of emitter 0, the same of
+ * emitter 1, sigma, background e-); d_work holds qcs_learned_work_bytes(n)
+ * bytes (unused by the fused path). */
 int qcs_learned_start_device(qcs_learned_net *net, const qcs_loc_para *p, const uint16_t *d_rois, int n,
                              float *d_start, float *d_work, void *stream);
 size_t qcs_learned_work_bytes(int n);

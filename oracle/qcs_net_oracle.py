@@ -19,6 +19,8 @@ CENTRE = R / 2.0
 SIGMA0 = 1.3
 N_IN, N_HID, N_OUT, N_USED = 64, 128, 8, 5   # the GS2D 7x7 network
 TARGET_WEIGHT = np.array([4.0, 4.0, 1.0, 1.0, 1.0, 1.0])  # GS2D uses the first 5, AS3D all 6
+TARGET_WEIGHT_2E = np.array([4.0, 4.0, 4.0, 4.0, 1.0, 1.0, 1.0, 1.0])  # the two-emitter start points
+LEARNED_2E = 16  # network kind of the two-emitter start points (QCS_LEARNED_GS2D_2E)
 
 
 def in_width(r):
@@ -27,7 +29,25 @@ def in_width(r):
 
 
 def used_outputs(loc_type):
-    return 6 if loc_type == 1 else 5
+    return 8 if loc_type == LEARNED_2E else (6 if loc_type == 1 else 5)
+
+
+def start_points_2e(y, lo, rng, r):
+    """Two-emitter start points (peak0, x0, y0, peak1, x1, y1, sigma,
+    background) from outputs y [n, 8] and the ROI scales, as the kernels map
+    them (positions held a pixel inside the ROI's edge)."""
+    y = np.asarray(y, np.float64)
+    c, w2 = r / 2.0, r / 2.0 - 1.0
+    st = np.zeros((y.shape[0], 8))
+    st[:, 0] = rng * np.exp(np.clip(y[:, 4], -6, 3))
+    st[:, 1] = c + np.clip(y[:, 0], -w2, w2)
+    st[:, 2] = c + np.clip(y[:, 1], -w2, w2)
+    st[:, 3] = rng * np.exp(np.clip(y[:, 5], -6, 3))
+    st[:, 4] = c + np.clip(y[:, 2], -w2, w2)
+    st[:, 5] = c + np.clip(y[:, 3], -w2, w2)
+    st[:, 6] = np.clip(SIGMA0 + y[:, 6], 0.6, 3.0)
+    st[:, 7] = np.maximum(lo + rng * y[:, 7], 1.0)
+    return st
 
 
 def param_count(n_in):
@@ -117,7 +137,7 @@ def loss_and_grad(params, x, t, valid, classes=None):
     n = x.shape[0]
     nu = t.shape[1]
     e = y[:, :nu] - t
-    tw = TARGET_WEIGHT[:nu]
+    tw = TARGET_WEIGHT_2E if nu == 8 else TARGET_WEIGHT[:nu]
     loss = float(np.sum(tw * e * e * valid[:, None]) / n)
     dy = np.zeros_like(y)
     dy[:, :nu] = 2.0 * tw * e * valid[:, None] / n

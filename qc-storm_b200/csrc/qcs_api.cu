@@ -67,6 +67,11 @@ struct qcs_loc_data {
     int *q_refit = nullptr;         // learned multi-emitter path: records to refit plainly
     uint8_t *d_refit = nullptr;     //   their per-record flags
     uint8_t *d_cls = nullptr;       //   emitter-count class per record
+    float *d_start2 = nullptr;      // two-emitter start points, capacity x 8 (one block with the three below)
+    uint8_t *d_refit2 = nullptr;    //   per 2E-queue slot refit flags
+    int *d_slots2 = nullptr;        //   slots and record ids of the two-emitter refits
+    int *d_ids2 = nullptr;
+    const qcs::TwoEmitterStart *two = nullptr;  // set for the duration of a learned call with a two-emitter net
     // autotuned lanes per ROI of the single-emitter fit by batch size: batches of
     // at most tune_n[k] records use tune_lanes[k] (first match); none: 1
     int tune_count = 0;
@@ -136,6 +141,7 @@ int qcs_loc_deinit(qcs_loc_data *c) {
     if (c->pending && c->ev_done) cudaEventSynchronize(c->ev_done);
     qcs::wle_sorter_destroy(c->wle_sorter);
     cudaFree(c->d_start);
+    cudaFree(c->d_start2);
     if (c->ev_done) cudaEventDestroy(c->ev_done);
     if (c->stream) cudaStreamDestroy(c->stream);
     if (c->side) cudaStreamDestroy(c->side);
@@ -187,6 +193,8 @@ int qcs_loc_init_capacity(const qcs_loc_para *p, int capacity, qcs_loc_data **ou
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_done, cudaEventDisableTiming);
     const size_t b_start = round256(cap * 6 * sizeof(float)), b_refit = round256(cap * sizeof(int));
     if (e == cudaSuccess) e = A((void **)&c->d_start, b_start + b_refit + 2 * round256(cap));
+    const size_t b_start2 = round256(cap * 8 * sizeof(float));
+    if (e == cudaSuccess) e = A((void **)&c->d_start2, b_start2 + round256(cap) + 2 * b_refit);
     if (e != cudaSuccess) {
         qcs_loc_deinit(c);
         return fail(e == cudaErrorMemoryAllocation ? QCS_ERR_NOMEM : QCS_ERR_CUDA, "qcs_loc_init", e);
@@ -206,6 +214,10 @@ int qcs_loc_init_capacity(const qcs_loc_para *p, int capacity, qcs_loc_data **ou
     c->q_refit = reinterpret_cast<int *>(b + b_start);
     c->d_refit = reinterpret_cast<uint8_t *>(b + b_start + b_refit);
     c->d_cls = c->d_refit + round256(cap);
+    char *b2 = reinterpret_cast<char *>(c->d_start2);
+    c->d_refit2 = reinterpret_cast<uint8_t *>(b2 + b_start2);
+    c->d_slots2 = reinterpret_cast<int *>(b2 + b_start2 + round256(cap));
+    c->d_ids2 = reinterpret_cast<int *>(b2 + b_start2 + round256(cap) + b_refit);
     *out = c;
     return QCS_OK;
 }
@@ -319,6 +331,34 @@ __global__ void labels_2e_kernel(qcs::CascadeState st, int n, float *__restrict_
     if (id >= 0 && id < n) cls[id] = st.res2[k] == 0 ? 2.0f : 1.0f;
 }
 
+// Two-emitter targets (QCS_LEARNED_GS2D_2E network outputs) of the records
+// whose plain two-emitter fit kept both emitters, read from the cascade state
+// of a plain multi-emitter call: the first emitter's row at loc[id], the
+// second's at extra2[slot].  valid[id] = 1 for those records (zero on entry).
+template <int R>
+__global__ void two_targets_kernel(qcs::CascadeState st, const uint16_t *__restrict__ rois,
+                                   const float *__restrict__ loc, const float *__restrict__ scale, int n, float qe,
+                                   float *__restrict__ tgt, float *__restrict__ valid) {
+    enum { PIX = R * R, WHOLE = R * (R + 1), HALF = R / 2 };
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= st.counters[qcs::kCnt2E]) return;
+    const int id = st.q2[k];
+    if (id < 0 || id >= n || st.res2[k] != 2) return;
+    const float *r0 = loc + (size_t)id * 12, *r1 = st.extra2 + (size_t)k * 12;
+    const uint16_t *h = rois + (size_t)id * WHOLE + PIX;
+    const float centre = R / 2.0f, lo = scale[2 * id], rng = scale[2 * id + 1];
+    float *t = tgt + (size_t)id * 8;
+    t[0] = r0[QCS_POS_XPOS] + (float)HALF - (float)h[0] - centre;
+    t[1] = r0[QCS_POS_YPOS] + (float)HALF - (float)h[1] - centre;
+    t[2] = r1[QCS_POS_XPOS] + (float)HALF - (float)h[0] - centre;
+    t[3] = r1[QCS_POS_YPOS] + (float)HALF - (float)h[1] - centre;
+    t[4] = logf(fmaxf(r0[QCS_POS_PPHO] * qe, 1e-3f) / rng);
+    t[5] = logf(fmaxf(r1[QCS_POS_PPHO] * qe, 1e-3f) / rng);
+    t[6] = r0[QCS_POS_SIGX] - 1.3f;
+    t[7] = (r0[QCS_POS_BAKG] * qe - lo) / rng;
+    valid[id] = 1.0f;
+}
+
 // The learned multi-emitter call: the cascade's queues (with the predicted
 // classes when cls is set), the learned-start single-emitter fit over the
 // single queue, a plain refit of the fits it flags (which also flags the
@@ -337,6 +377,7 @@ cudaError_t learned_multi(qcs_loc_data *c, const uint16_t *d_rois, const float *
     a.max_rows = c->max_rows;
     a.stream = s;
     a.pred = cls;
+    a.two = c->two;
     cudaError_t e;
     if ((e = qcs::cascade_classify(a, c->st)) != cudaSuccess) return e;
     qcs::FitLaunch f = qcs::cascade_single_launch(a, c->st);
@@ -349,6 +390,24 @@ cudaError_t learned_multi(qcs_loc_data *c, const uint16_t *d_rois, const float *
     f.q = qcs::Queue{c->q_refit, c->st.counters + qcs::kCntRefit, 0};
     if ((e = qcs::launch_fit_group(qcs::kGS2D, R, 8, f)) != cudaSuccess) return e;
     return qcs::cascade_tail(a, c->st);
+}
+
+// When the GS2D network has a two-emitter network attached: its start points
+// of the call's records into the context and the context's two-emitter stage
+// set to use them (cleared by the caller after the call).
+int two_emitter_starts(qcs_loc_data *c, const qcs_learned_net *net, const qcs_loc_para *p, const uint16_t *d_rois,
+                       int n, const int *n_dev, cudaStream_t s, qcs::TwoEmitterStart *two) {
+    c->two = nullptr;
+    int iters = 0, bisections = 0, to3e = 1;
+    float dev_th = 0.0f;
+    qcs_learned_net *net2 = qcs::learned::two_emitter(net, &iters, &bisections, &dev_th, &to3e);
+    if (!net2 || p->LocType != QCS_LOCTYPE_GS2D || !p->MultiEmitterFitEn || n <= 0) return QCS_OK;
+    QCS_CUDA(qcs::learned::start_points(net2, p, d_rois, n, c->d_start2, s, nullptr, n_dev),
+             "two-emitter start points");
+    *two = qcs::TwoEmitterStart{c->d_start2, iters, bisections, dev_th > 0.0f ? dev_th : default_dev_th(p->ROISize),
+                                to3e, c->d_refit2, c->d_slots2, c->d_ids2};
+    c->two = two;
+    return QCS_OK;
 }
 }  // namespace
 
@@ -437,7 +496,11 @@ int qcs_learned_localize_device(qcs_loc_data *c, qcs_learned_net *net, const uin
     // emitter-count routing: multi-emitter fitting on and a threshold set
     uint8_t *cls = (p->MultiEmitterFitEn && qcs_learned_count_threshold(net) > 0.0f) ? c->d_cls : nullptr;
     QCS_CUDA(qcs::learned::start_points(net, p, d_rois, n, c->d_start, s, cls), "learned start points");
-    return qcs_fit_from_start_classes_device(c, d_rois, d_wle, p, n, c->d_start, cls, iters, bisections, dev_th, s);
+    qcs::TwoEmitterStart two;
+    if (p->MultiEmitterFitEn && (st = two_emitter_starts(c, net, p, d_rois, n, nullptr, s, &two)) != QCS_OK) return st;
+    st = qcs_fit_from_start_classes_device(c, d_rois, d_wle, p, n, c->d_start, cls, iters, bisections, dev_th, s);
+    c->two = nullptr;
+    return st;
 }
 
 int qcs_learned_localize_device_n(qcs_loc_data *c, qcs_learned_net *net, const uint16_t *d_rois, const float *d_wle,
@@ -461,8 +524,11 @@ int qcs_learned_localize_device_n(qcs_loc_data *c, qcs_learned_net *net, const u
     uint8_t *cls = qcs_learned_count_threshold(net) > 0.0f ? c->d_cls : nullptr;
     if (max_n == 0) return QCS_OK;
     QCS_CUDA(qcs::learned::start_points(net, p, d_rois, max_n, c->d_start, s, cls, d_n), "learned start points");
-    QCS_CUDA(learned_multi(c, d_rois, d_wle, p, max_n, d_n, c->d_start, cls, iters, bisections, dev_th, s),
-             "learned multi-emitter localization");
+    qcs::TwoEmitterStart two;
+    if ((st = two_emitter_starts(c, net, p, d_rois, max_n, d_n, s, &two)) != QCS_OK) return st;
+    const cudaError_t e = learned_multi(c, d_rois, d_wle, p, max_n, d_n, c->d_start, cls, iters, bisections, dev_th, s);
+    c->two = nullptr;
+    QCS_CUDA(e, "learned multi-emitter localization");
     return QCS_OK;
 }
 
@@ -483,6 +549,38 @@ int qcs_loc_count_labels_device(qcs_loc_data *c, int n, float *d_labels, void *s
     labels_zero_kernel<<<(n + 255) / 256, 256, 0, s>>>(d_labels, n);
     labels_2e_kernel<<<(n + 255) / 256, 256, 0, s>>>(c->st, n, d_labels);
     QCS_CUDA(cudaGetLastError(), "count labels");
+    return QCS_OK;
+}
+
+int qcs_learned_refit_2e_num(qcs_loc_data *c, int *n) {
+    if (!c || !n) return fail(QCS_ERR_ARG, "null argument");
+    QCS_CUDA(cudaDeviceSynchronize(), "localization");
+    QCS_CUDA(cudaMemcpy(c->h_counters, c->st.counters, qcs::kCntNum * sizeof(int), cudaMemcpyDeviceToHost),
+             "read counters");
+    *n = c->h_counters[qcs::kCntRefit2E];
+    return QCS_OK;
+}
+
+int qcs_loc_two_emitter_targets_device(qcs_loc_data *c, const uint16_t *d_rois, const qcs_loc_para *p, int n,
+                                       const float *d_scale, float *d_targets, float *d_valid, void *stream) {
+    if (!c || !p || !d_rois || !d_scale || !d_targets || !d_valid) return fail(QCS_ERR_ARG, "null argument");
+    if (n < 0 || n > c->capacity) return fail(QCS_ERR_CAPACITY, "record count outside the context capacity");
+    if (p->LocType != QCS_LOCTYPE_GS2D || !p->MultiEmitterFitEn || p->ROISize != c->R ||
+        !(c->R == 7 || c->R == 9 || c->R == 11))
+        return fail(QCS_ERR_ARG, "two-emitter targets: GS2D 7/9/11 with multi-emitter fitting");
+    if (n == 0) return QCS_OK;
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+    QCS_CUDA(cudaMemsetAsync(d_targets, 0, (size_t)n * 8 * sizeof(float), s), "clear targets");
+    QCS_CUDA(cudaMemsetAsync(d_valid, 0, (size_t)n * sizeof(float), s), "clear valid");
+    const int grid = (n + 255) / 256;
+    const float qe = p->QE;
+    if (c->R == 7)
+        two_targets_kernel<7><<<grid, 256, 0, s>>>(c->st, d_rois, c->d_loc, d_scale, n, qe, d_targets, d_valid);
+    else if (c->R == 9)
+        two_targets_kernel<9><<<grid, 256, 0, s>>>(c->st, d_rois, c->d_loc, d_scale, n, qe, d_targets, d_valid);
+    else
+        two_targets_kernel<11><<<grid, 256, 0, s>>>(c->st, d_rois, c->d_loc, d_scale, n, qe, d_targets, d_valid);
+    QCS_CUDA(cudaGetLastError(), "two-emitter targets");
     return QCS_OK;
 }
 

@@ -271,7 +271,31 @@ cudaError_t cascade_tail(const CascadeArgs &a, const CascadeState &st) {
             f.max_count = n;
             f.to2e = nullptr;
             f.mo = MultiOut{st.res2, st.extra2};
-            if ((e = launch_fit(as3d ? kAS3D2E : k2E, R, f)) != cudaSuccess) return e;
+            if (a.two && !as3d) {
+                // learned starts; the plain refits write into the (still unused) 3E stage's arrays and are
+                // merged back into their slots
+                const TwoEmitterStart &t = *a.two;
+                if ((e = launch_fit_learned_2e(R, t.iters, t.bisections, f, t.start, t.dev_th, t.refit, t.to3e)) !=
+                    cudaSuccess)
+                    return e;
+                if (!t.to3e && (e = launch_flag_slots(t.refit, st.counters + kCnt2E, n, st.q2, t.slots, t.ids,
+                                           st.counters + kCntRefit2E, a.stream)) != cudaSuccess)
+                    return e;
+                if (t.to3e) {
+                    if ((e = cudaMemsetAsync(st.counters + kCntRefit2E, 0, sizeof(int), a.stream)) != cudaSuccess)
+                        return e;
+                } else {
+                    FitLaunch g = f;
+                    g.q = Queue{t.ids, st.counters + kCntRefit2E, 0};
+                    g.mo = MultiOut{st.res3, st.extra3};
+                    if ((e = launch_fit(k2E, R, g)) != cudaSuccess) return e;
+                    if ((e = launch_merge_refit(t.slots, st.counters + kCntRefit2E, n, st.res3, st.extra3, st.res2,
+                                                st.extra2, a.stream)) != cudaSuccess)
+                        return e;
+                }
+            } else if ((e = launch_fit(as3d ? kAS3D2E : k2E, R, f)) != cudaSuccess) {
+                return e;
+            }
             if ((e = launch_compaction(CompactStage{st, a.loc, 2, as3d ? 0 : 1, a.max_rows}, n, st, a.stream)) !=
                 cudaSuccess)
                 return e;

@@ -19,6 +19,7 @@ enum {
     kCntValid = 6,       // rows produced, capped at the row capacity
     kCnt3EClassify = 7,  // three-emitter queue entries that came from the classifier (learned classes)
     kCntRefit = 8,       // learned path: records refitted by the plain single-emitter fit
+    kCntRefit2E = 9,     // learned path: two-emitter fits redone by the plain two-emitter fit
     kCntNum = 16
 };
 
@@ -39,6 +40,22 @@ struct CascadeState {
 // ints of CascadeState::scan for `capacity` records
 constexpr int cascade_scan_ints(int capacity) { return 4 + 3 * ((capacity + 1023) / 1024 + 1); }
 
+// Learned start points of the GS2D two-emitter stage: the stage fits its
+// queue from start[8 id ..] with iters x bisections (launch_fit_learned_2e),
+// the plain two-emitter fit redoes the fits it judges poor (refit, per queue
+// slot; slots / ids: scratch of the queue's capacity) and their results go
+// back to the slots they came from, so the stages after it see the
+// reference's layout; or, with to3e, the poor fits go on to the three-emitter
+// fit as the reference's rejected two-emitter fits do.
+struct TwoEmitterStart {
+    const float *start;
+    int iters, bisections;
+    float dev_th;
+    int to3e;  // 1: poor fits go on to the three-emitter fit instead of a plain refit
+    uint8_t *refit;
+    int *slots, *ids;
+};
+
 struct CascadeArgs {
     qcs_loc_para para;
     const uint16_t *rois;  // device, n records
@@ -50,6 +67,7 @@ struct CascadeArgs {
     cudaStream_t stream;
     const uint8_t *pred = nullptr;  // learned emitter-count class per record, or null (the reference's split)
     int lanes = 1;  // lanes per ROI of the single-emitter fit: 1 (one thread per ROI) or 4 / 8 / 16 (group kernel)
+    const TwoEmitterStart *two = nullptr;  // learned two-emitter starts (GS2D), or null (the reference's)
 };
 
 // The whole localization call: queues, single-emitter fit, 2E / 3E fits,

@@ -572,119 +572,18 @@ cudaError_t launch_learned(const FitLaunch &a, const float *start, float dev_th,
 }
 
 // -------------------------------------------------------- multi emitter ---
-template <int R, int KIND, int DIST = ArithSpec<KIND, R>::DIST, int MASK = ArithSpec<KIND, R>::MASK,
-          int SUM2 = ArithSpec<KIND, R>::SUM2>
-__global__ void __launch_bounds__(kTPB) fit_multi_kernel(const uint16_t *__restrict__ rois,
-                                                         const float *__restrict__ wle, Queue q,
-                                                         float *__restrict__ loc, MultiOut mo, CorePara c) {
-    typedef SmemLayout<R, KIND> L;
-    enum { P = KindTraits<KIND>::P, PIX = R * R, WHOLE = R * (R + 1), ROISize_Half = R / 2 };
-    extern __shared__ float smem[];
-    const int n = queue_len(q);
-    const int base = blockIdx.x * kTPB;
-    if (base >= n) return;
-    const int cnt = min(kTPB, n - base);
-    float2 *s_img = reinterpret_cast<float2 *>(smem + L::IMG);
-    stage_rois<R>(s_img, rois, q, base, cnt, c.Offset, c.KAdc);
-    __syncthreads();
-    const int tid = threadIdx.x;
-    if (tid >= cnt) return;
-
-    const int slot = base + tid;
-    const int CurFluoID = queue_at(q, slot);
-    const PixView img{s_img + tid, kTPB};
-    float *w = smem + L::W + tid;
-    float *D = smem + L::D + tid;
-    const uint16_t *hdr = rois + (size_t)CurFluoID * WHOLE + PIX;
-    const int XOffset = hdr[0];
-    const int YOffset = hdr[1];
-    const int CurFrame = hdr[2] + 65536 * hdr[3];
+// Emitter selection, accept rules and output of the multi-emitter fits
+// (2Emitter_core.h:245-333, 3Emitter_core.h:247-347, AS3D_2Emitter_core.h:
+// 307-406) at the fitted parameters Ininf (fit units): the first emitter's row
+// into loc[CurFluoID] (or a zero row), the second's into mo.extra[slot] and the
+// stage result (0: none kept, 1: one, 2: both) into mo.result[slot].
+template <int R, int KIND>
+__device__ __forceinline__ void multi_finish(float *Ininf, const CorePara &c, int XOffset, int YOffset, int CurFrame,
+                                             float NearNeighborDistance, float *__restrict__ loc, int CurFluoID,
+                                             MultiOut mo, int slot) {
+    enum { P = KindTraits<KIND>::P, ROISize_Half = R / 2 };
     const float ROICenter = R / 2.0f;
     const float QE = c.QE;
-
-    float Ininf[P];
-    const RoiRef roi{s_img + tid, w, kTPB};
-    float NearNeighborDistance = 1000;
-
-    if (KIND == k2E) {
-        float WLE_SigmaX = R / 1.8f / 2.35f;
-        NearNeighborDistance = wle[(size_t)CurFluoID * QCS_WLE_PARA_NUM + 0];
-        // PreEstimation_GS2D_2E
-        {
-            float Mean1, Mean2, Mean3, Mean4;
-            edge_means<R>(img, Mean1, Mean2, Mean3, Mean4);
-            Mean1 = fminf(Mean1, Mean2);
-            Mean3 = fminf(Mean3, Mean4);
-            Mean1 = fminf(Mean1, Mean3);
-            const float Bkg = Mean1 / R;
-            const float Amp = img[ROISize_Half * R + ROISize_Half] - Bkg;
-            const float SigmaX = R / 2.2f / 2.35f;
-            const float SigmaX1 = (1.0f / (2.0f * SigmaX * SigmaX));
-            float xs[1], ys[1];
-            block_starts<R>(img, 1, xs, ys);
-            Ininf[0] = 0.8f * Amp * rAScalFactor;
-            Ininf[1] = ROICenter;
-            Ininf[2] = ROICenter;
-            Ininf[3] = 0.8f * Amp * rAScalFactor;
-            Ininf[4] = xs[0];
-            Ininf[5] = ys[0];
-            Ininf[6] = SigmaX1 * rSScalFactor;
-            Ininf[7] = 0.8f * Bkg * rBScalFactor;
-        }
-        if (c.WLEEn == 0) WLE_SigmaX = R;
-        wle_weights<R, MASK>(w, kTPB, WLE_SigmaX, WLE_SigmaX, QCS_MOLECULE_MULTIFIT);
-        mle_fit<R, k2E, DIST, SUM2>(roi, Ininf, D, kTPB);
-    } else if (KIND == k3E) {
-        // PreEstimation_GS2D_3E
-        float Mean1, Mean2, Mean3, Mean4;
-        edge_means<R>(img, Mean1, Mean2, Mean3, Mean4);
-        Mean1 = fminf(Mean1, Mean2);
-        Mean3 = fminf(Mean3, Mean4);
-        const float Bkg = (Mean1 + Mean3) / 2 / R;
-        const float Amp = img[ROISize_Half * R + ROISize_Half] - Bkg;
-        const float SigmaX = R / 2.2f / 2.35f;
-        const float SigmaX1 = (1.0f / (2.0f * SigmaX * SigmaX));
-        float xs[2], ys[2];
-        block_starts<R>(img, 2, xs, ys);
-        Ininf[0] = 0.7f * Amp * rAScalFactor;
-        Ininf[1] = ROICenter;
-        Ininf[2] = ROICenter;
-        Ininf[3] = 0.7f * Amp * rAScalFactor;
-        Ininf[4] = xs[0];
-        Ininf[5] = ys[0];
-        Ininf[6] = 0.3f * Amp * rAScalFactor;
-        Ininf[7] = xs[1];
-        Ininf[8] = ys[1];
-        Ininf[9] = SigmaX1 * rSScalFactor;
-        Ininf[10] = 0.8f * Bkg * rBScalFactor;
-        mle_fit<R, k3E, DIST, SUM2>(roi, Ininf, D, kTPB);
-    } else {  // kAS3D2E
-        float Mean1, Mean2, Mean3, Mean4;
-        edge_means<R>(img, Mean1, Mean2, Mean3, Mean4);
-        Mean1 = fminf(Mean1, Mean2);
-        Mean3 = fminf(Mean3, Mean4);
-        const float Bkg = (Mean1 + Mean3) / 2 / R;
-        const float Amp = img[ROISize_Half * R + ROISize_Half] - Bkg;
-        const float SigmaX = R / 2.2f / 2.35f;
-        const float SigmaY = R / 2.2f / 2.35f;
-        const float SigmaX1 = rSScalFactor * (0.5f / (SigmaX * SigmaX));
-        const float SigmaY1 = rSScalFactor * (0.5f / (SigmaY * SigmaY));
-        float xs[1], ys[1];
-        block_starts<R>(img, 1, xs, ys);
-        Ininf[0] = 0.7f * Amp * rAScalFactor;
-        Ininf[1] = ROICenter;
-        Ininf[2] = ROICenter;
-        Ininf[3] = SigmaX1;
-        Ininf[4] = SigmaY1;
-        Ininf[5] = 0.7f * Amp * rAScalFactor;
-        Ininf[6] = xs[0];
-        Ininf[7] = ys[0];
-        Ininf[8] = SigmaX1;
-        Ininf[9] = SigmaY1;
-        Ininf[10] = 0.8f * Bkg * rBScalFactor;
-        mle_fit<R, kAS3D2E, DIST, SUM2>(roi, Ininf, D, kTPB);
-    }
-
     // emitter selection (2Emitter_core.h:245-271, 3Emitter_core.h:247-280)
     enum { NE = (KIND == k3E) ? 3 : 2, STRIDE = (KIND == kAS3D2E) ? 5 : 3 };
     float row0[12], row1[12];
@@ -805,6 +704,255 @@ __global__ void __launch_bounds__(kTPB) fit_multi_kernel(const uint16_t *__restr
     mo.result[slot] = (int8_t)result;
 }
 
+template <int R, int KIND, int DIST = ArithSpec<KIND, R>::DIST, int MASK = ArithSpec<KIND, R>::MASK,
+          int SUM2 = ArithSpec<KIND, R>::SUM2>
+__global__ void __launch_bounds__(kTPB) fit_multi_kernel(const uint16_t *__restrict__ rois,
+                                                         const float *__restrict__ wle, Queue q,
+                                                         float *__restrict__ loc, MultiOut mo, CorePara c) {
+    typedef SmemLayout<R, KIND> L;
+    enum { P = KindTraits<KIND>::P, PIX = R * R, WHOLE = R * (R + 1), ROISize_Half = R / 2 };
+    extern __shared__ float smem[];
+    const int n = queue_len(q);
+    const int base = blockIdx.x * kTPB;
+    if (base >= n) return;
+    const int cnt = min(kTPB, n - base);
+    float2 *s_img = reinterpret_cast<float2 *>(smem + L::IMG);
+    stage_rois<R>(s_img, rois, q, base, cnt, c.Offset, c.KAdc);
+    __syncthreads();
+    const int tid = threadIdx.x;
+    if (tid >= cnt) return;
+
+    const int slot = base + tid;
+    const int CurFluoID = queue_at(q, slot);
+    const PixView img{s_img + tid, kTPB};
+    float *w = smem + L::W + tid;
+    float *D = smem + L::D + tid;
+    const uint16_t *hdr = rois + (size_t)CurFluoID * WHOLE + PIX;
+    const int XOffset = hdr[0];
+    const int YOffset = hdr[1];
+    const int CurFrame = hdr[2] + 65536 * hdr[3];
+    const float ROICenter = R / 2.0f;
+    const float QE = c.QE;
+
+    float Ininf[P];
+    const RoiRef roi{s_img + tid, w, kTPB};
+    float NearNeighborDistance = 1000;
+
+    if (KIND == k2E) {
+        float WLE_SigmaX = R / 1.8f / 2.35f;
+        NearNeighborDistance = wle[(size_t)CurFluoID * QCS_WLE_PARA_NUM + 0];
+        // PreEstimation_GS2D_2E
+        {
+            float Mean1, Mean2, Mean3, Mean4;
+            edge_means<R>(img, Mean1, Mean2, Mean3, Mean4);
+            Mean1 = fminf(Mean1, Mean2);
+            Mean3 = fminf(Mean3, Mean4);
+            Mean1 = fminf(Mean1, Mean3);
+            const float Bkg = Mean1 / R;
+            const float Amp = img[ROISize_Half * R + ROISize_Half] - Bkg;
+            const float SigmaX = R / 2.2f / 2.35f;
+            const float SigmaX1 = (1.0f / (2.0f * SigmaX * SigmaX));
+            float xs[1], ys[1];
+            block_starts<R>(img, 1, xs, ys);
+            Ininf[0] = 0.8f * Amp * rAScalFactor;
+            Ininf[1] = ROICenter;
+            Ininf[2] = ROICenter;
+            Ininf[3] = 0.8f * Amp * rAScalFactor;
+            Ininf[4] = xs[0];
+            Ininf[5] = ys[0];
+            Ininf[6] = SigmaX1 * rSScalFactor;
+            Ininf[7] = 0.8f * Bkg * rBScalFactor;
+        }
+        if (c.WLEEn == 0) WLE_SigmaX = R;
+        wle_weights<R, MASK>(w, kTPB, WLE_SigmaX, WLE_SigmaX, QCS_MOLECULE_MULTIFIT);
+        mle_fit<R, k2E, DIST, SUM2>(roi, Ininf, D, kTPB);
+    } else if (KIND == k3E) {
+        // PreEstimation_GS2D_3E
+        float Mean1, Mean2, Mean3, Mean4;
+        edge_means<R>(img, Mean1, Mean2, Mean3, Mean4);
+        Mean1 = fminf(Mean1, Mean2);
+        Mean3 = fminf(Mean3, Mean4);
+        const float Bkg = (Mean1 + Mean3) / 2 / R;
+        const float Amp = img[ROISize_Half * R + ROISize_Half] - Bkg;
+        const float SigmaX = R / 2.2f / 2.35f;
+        const float SigmaX1 = (1.0f / (2.0f * SigmaX * SigmaX));
+        float xs[2], ys[2];
+        block_starts<R>(img, 2, xs, ys);
+        Ininf[0] = 0.7f * Amp * rAScalFactor;
+        Ininf[1] = ROICenter;
+        Ininf[2] = ROICenter;
+        Ininf[3] = 0.7f * Amp * rAScalFactor;
+        Ininf[4] = xs[0];
+        Ininf[5] = ys[0];
+        Ininf[6] = 0.3f * Amp * rAScalFactor;
+        Ininf[7] = xs[1];
+        Ininf[8] = ys[1];
+        Ininf[9] = SigmaX1 * rSScalFactor;
+        Ininf[10] = 0.8f * Bkg * rBScalFactor;
+        mle_fit<R, k3E, DIST, SUM2>(roi, Ininf, D, kTPB);
+    } else {  // kAS3D2E
+        float Mean1, Mean2, Mean3, Mean4;
+        edge_means<R>(img, Mean1, Mean2, Mean3, Mean4);
+        Mean1 = fminf(Mean1, Mean2);
+        Mean3 = fminf(Mean3, Mean4);
+        const float Bkg = (Mean1 + Mean3) / 2 / R;
+        const float Amp = img[ROISize_Half * R + ROISize_Half] - Bkg;
+        const float SigmaX = R / 2.2f / 2.35f;
+        const float SigmaY = R / 2.2f / 2.35f;
+        const float SigmaX1 = rSScalFactor * (0.5f / (SigmaX * SigmaX));
+        const float SigmaY1 = rSScalFactor * (0.5f / (SigmaY * SigmaY));
+        float xs[1], ys[1];
+        block_starts<R>(img, 1, xs, ys);
+        Ininf[0] = 0.7f * Amp * rAScalFactor;
+        Ininf[1] = ROICenter;
+        Ininf[2] = ROICenter;
+        Ininf[3] = SigmaX1;
+        Ininf[4] = SigmaY1;
+        Ininf[5] = 0.7f * Amp * rAScalFactor;
+        Ininf[6] = xs[0];
+        Ininf[7] = ys[0];
+        Ininf[8] = SigmaX1;
+        Ininf[9] = SigmaY1;
+        Ininf[10] = 0.8f * Bkg * rBScalFactor;
+        mle_fit<R, kAS3D2E, DIST, SUM2>(roi, Ininf, D, kTPB);
+    }
+
+    multi_finish<R, KIND>(Ininf, c, XOffset, YOffset, CurFrame, NearNeighborDistance, loc, CurFluoID, mo, slot);
+}
+
+// -------------------------------------- learned-start two-emitter fits ---
+// The GS2D two-emitter fit of fit_multi_kernel<R, k2E> over the records of
+// its queue, started from a given point (start[8 id ..]: peak e- of emitter
+// 0, its x, y in ROI pixels, peak e- of emitter 1, its x, y, the shared sigma,
+// background e-) instead of the centre / 3x3-block pre-estimate, with ITERS
+// BFGS iterations of NB line-search steps and the analytic gradient
+// (AnalyticEval2E); the same weighted loss (fixed-width WLE mask), selection,
+// accept rules and output (multi_finish). A fit is judged poor when no
+// emitter is kept or when the unweighted Poisson deviance of the two-emitter
+// model exceeds dev_th; with to3e = 0, refit[slot] = 1 marks it for the plain
+// two-emitter fit, with to3e = 1 its rows are dropped and its stage result set
+// to 0, so the cascade hands it to the three-emitter fit as it hands on the
+// reference fit's rejects.
+template <int R, int ITERS, int NB, int DIST = ArithSpec<k2E, R>::DIST, int MASK = ArithSpec<k2E, R>::MASK>
+__global__ void __launch_bounds__(kTPB) fit_learned_2e_kernel(const uint16_t *__restrict__ rois,
+                                                              const float *__restrict__ wle,
+                                                              const float *__restrict__ start, Queue q,
+                                                              float *__restrict__ loc, MultiOut mo,
+                                                              uint8_t *__restrict__ refit, CorePara c, float dev_th,
+                                                              int to3e) {
+    typedef SmemLayout<R, k2E> L;
+    enum { P = 8, PIX = R * R, WHOLE = R * (R + 1) };
+    extern __shared__ float smem[];
+    const int n = queue_len(q);
+    const int base = blockIdx.x * kTPB;
+    if (base >= n) return;
+    const int cnt = min(kTPB, n - base);
+    float2 *s_img = reinterpret_cast<float2 *>(smem + L::IMG);
+    stage_rois<R>(s_img, rois, q, base, cnt, c.Offset, c.KAdc);
+    __syncthreads();
+    const int tid = threadIdx.x;
+    if (tid >= cnt) return;
+    const int slot = base + tid;
+    const int id = queue_at(q, slot);
+    float *w = smem + L::W + tid;
+    float *D = smem + L::D + tid;
+    const uint16_t *hdr = rois + (size_t)id * WHOLE + PIX;
+    const int XOffset = hdr[0], YOffset = hdr[1];
+    const int CurFrame = hdr[2] + 65536 * hdr[3];
+    const RoiRef roi{s_img + tid, w, kTPB};
+    const float NearNeighborDistance = wle[(size_t)id * QCS_WLE_PARA_NUM + 0];
+    float WLE_SigmaX = R / 1.8f / 2.35f;
+    if (c.WLEEn == 0) WLE_SigmaX = R;
+    wle_weights<R, MASK>(w, kTPB, WLE_SigmaX, WLE_SigmaX, QCS_MOLECULE_MULTIFIT);
+    const float *st = start + (size_t)id * P;
+    float Ininf[P];
+    Ininf[0] = st[0] * rAScalFactor;
+    Ininf[1] = st[1];
+    Ininf[2] = st[2];
+    Ininf[3] = st[3] * rAScalFactor;
+    Ininf[4] = st[4];
+    Ininf[5] = st[5];
+    Ininf[6] = (0.5f / (st[6] * st[6])) * rSScalFactor;
+    Ininf[7] = st[7] * rBScalFactor;
+    bfgs_fit<P, ITERS, AnalyticEval2E<R, DIST>, NB>(AnalyticEval2E<R, DIST>{roi}, Ininf, D, kTPB);
+    // goodness of fit at the final point (unweighted Poisson deviance of the two-emitter model)
+    float dev = 0.0f;
+    {
+        float v[P];
+#pragma unroll
+        for (int k = 0; k < P; k++) v[k] = Ininf[k] < 0.0f ? 0.0f : Ininf[k];
+        const float A0 = v[0] * QCS_ASCALE, A1 = v[3] * QCS_ASCALE, S01 = v[6] * QCS_SSCALE, B64 = v[7] * QCS_BSCALE;
+#pragma unroll 1
+        for (int r = 0; r < R; r++)
+            for (int col = 0; col < R; col++) {
+                const float2 pl = roi.img[(r * R + col) * roi.ld];
+                const float dx0 = col + 0.5f - v[1], dy0 = r + 0.5f - v[2];
+                const float dx1 = col + 0.5f - v[4], dy1 = r + 0.5f - v[5];
+                const float mu = A0 * __expf(-(dx0 * dx0 + dy0 * dy0) * S01) +
+                                 A1 * __expf(-(dx1 * dx1 + dy1 * dy1) * S01) + B64;
+                dev += mu - pl.x - pl.x * (__logf(mu) - pl.y);
+            }
+        dev *= 2.0f;
+    }
+    multi_finish<R, k2E>(Ininf, c, XOffset, YOffset, CurFrame, NearNeighborDistance, loc, id, mo, slot);
+    const bool poor = mo.result[slot] == 0 || !(dev <= dev_th);
+    if (to3e) {
+        if (poor && mo.result[slot] != 0) {
+            zero_row(loc, id);
+            mo.result[slot] = 0;
+        }
+        refit[slot] = 0;
+    } else {
+        refit[slot] = poor ? 1 : 0;
+    }
+}
+
+// slots[] / ids[]: the queue slots i < *n_dev with flags[i] != 0 and their
+// record ids q[i] (any order); *count = their number (zero on entry).
+__global__ void flag_slots_kernel(const uint8_t *__restrict__ flags, const int *__restrict__ n_dev, int max_n,
+                                  const int *__restrict__ q, int *__restrict__ slots, int *__restrict__ ids,
+                                  int *__restrict__ count) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = min(*n_dev, max_n);
+    const bool f = i < n && flags[i] != 0;
+    const unsigned m = __ballot_sync(0xffffffffu, f);
+    int b = 0;
+    if ((threadIdx.x & 31) == 0 && m) b = atomicAdd(count, __popc(m));
+    b = __shfl_sync(0xffffffffu, b, 0);
+    if (f) {
+        const int k = b + __popc(m & ((1u << (threadIdx.x & 31)) - 1u));
+        slots[k] = i;
+        ids[k] = q[i];
+    }
+}
+
+// The plain refits' stage results and second-emitter rows (indexed by refit
+// position k) back into the slots they were taken from.
+__global__ void merge_refit_kernel(const int *__restrict__ slots, const int *__restrict__ count, int max_n,
+                                   const int8_t *__restrict__ res_k, const float *__restrict__ extra_k,
+                                   int8_t *__restrict__ res, float *__restrict__ extra) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= min(*count, max_n)) return;
+    const int slot = slots[k];
+    res[slot] = res_k[k];
+    if (res_k[k] == 2) {
+#pragma unroll
+        for (int j = 0; j < 12; j++) extra[(size_t)slot * 12 + j] = extra_k[(size_t)k * 12 + j];
+    }
+}
+
+template <int R, int IT, int NB>
+cudaError_t launch_learned_2e(const FitLaunch &a, const float *start, float dev_th, uint8_t *refit, int to3e) {
+    const size_t smem = SmemLayout<R, k2E>::TOTAL * sizeof(float);
+    auto k = fit_learned_2e_kernel<R, IT, NB>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const int grid = (a.max_count + kTPB - 1) / kTPB;
+    if (grid == 0) return cudaSuccess;
+    k<<<grid, kTPB, smem, a.stream>>>(a.rois, a.wle, start, a.q, a.loc, a.mo, refit, a.para, dev_th, to3e);
+    return cudaGetLastError();
+}
+
 template <int R, int KIND>
 cudaError_t launch_single(const FitLaunch &a) {
     const size_t smem = SmemLayout<R, KIND>::TOTAL * sizeof(float);
@@ -897,6 +1045,44 @@ cudaError_t launch_fit_learned(int kind, int R, int iters, int bisections, const
         }
     }
     return cudaErrorInvalidValue;
+}
+
+// Learned-start two-emitter schedules: 3 or 4 iterations of 6 steps, and the
+// reference's 13 of 11; ROI sizes 7, 9, 11.
+bool learned_2e_supported(int R, int iters, int bisections) {
+    return (R == 7 || R == 9 || R == 11) &&
+           ((bisections == 6 && (iters == 3 || iters == 4)) || (bisections == kBisections && iters == 13));
+}
+
+cudaError_t launch_fit_learned_2e(int R, int iters, int bisections, const FitLaunch &a, const float *start,
+                                  float dev_th, uint8_t *refit, int to3e) {
+    if (!learned_2e_supported(R, iters, bisections)) return cudaErrorInvalidValue;
+#define QCS_L2E(RR)                                                                                   \
+    if (R == RR) {                                                                                  \
+        if (iters == 3 && bisections == 6) return launch_learned_2e<RR, 3, 6>(a, start, dev_th, refit, to3e); \
+        if (iters == 4 && bisections == 6) return launch_learned_2e<RR, 4, 6>(a, start, dev_th, refit, to3e); \
+        return launch_learned_2e<RR, 13, kBisections>(a, start, dev_th, refit, to3e);                       \
+    }
+    QCS_L2E(7)
+    QCS_L2E(9)
+    QCS_L2E(11)
+#undef QCS_L2E
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_flag_slots(const uint8_t *flags, const int *n_dev, int max_n, const int *q, int *slots, int *ids,
+                              int *count, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(count, 0, sizeof(int), s);
+    if (e != cudaSuccess || max_n <= 0) return e;
+    flag_slots_kernel<<<(max_n + 255) / 256, 256, 0, s>>>(flags, n_dev, max_n, q, slots, ids, count);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_merge_refit(const int *slots, const int *count, int max_n, const int8_t *res_k,
+                               const float *extra_k, int8_t *res, float *extra, cudaStream_t s) {
+    if (max_n <= 0) return cudaSuccess;
+    merge_refit_kernel<<<(max_n + 255) / 256, 256, 0, s>>>(slots, count, max_n, res_k, extra_k, res, extra);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_flag_queue(const uint8_t *flags, int n, int *ids, int *count, cudaStream_t s) {

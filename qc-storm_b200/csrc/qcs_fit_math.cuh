@@ -436,6 +436,58 @@ struct AnalyticEvalAS3D {
     }
 };
 
+
+// The two-emitter GS2D loss (shared S and B, the loss the 2E fit minimises)
+// with its analytic gradient: mu = 128 (A0 e0 + A1 e1) + 64 B,
+// ek = exp(-0.1 S rk^2), and with q = w (1 - n / mu)
+//   dA_k = 128 sum q ek, dX_k = 128 A_k 0.2 S sum q ek dx_k (same for Y),
+//   dS = -12.8 sum q (A0 e0 r0^2 + A1 e1 r1^2), dB = 64 sum q,
+// at the point clamped as the loss clamps it (parameters >= 0).
+template <int R, int DIST>
+struct AnalyticEval2E {
+    RoiRef roi;
+    __device__ __forceinline__ float loss(float *x) const {
+        return qcs::loss<R, k2E, DIST, ArithSpec<k2E, R>::SUM2>(roi, x);
+    }
+    __device__ __forceinline__ void gradient(const float *v, float *g) const {
+        float c[8];
+#pragma unroll
+        for (int k = 0; k < 8; k++) c[k] = v[k] < 0.0f ? 0.0f : v[k];
+        const float A0 = c[0] * QCS_ASCALE, A1 = c[3] * QCS_ASCALE, S01 = c[6] * QCS_SSCALE, B64 = c[7] * QCS_BSCALE;
+        float gA0 = 0, gX0 = 0, gY0 = 0, gA1 = 0, gX1 = 0, gY1 = 0, gS = 0, gB = 0;
+#pragma unroll 1
+        for (int row = 0; row < R; row++) {
+            const float dy0 = (row + 0.5f) - c[2], dy1 = (row + 0.5f) - c[5];
+#pragma unroll(R <= kUnrollMaxR ? R : 1)
+            for (int col = 0; col < R; col++) {
+                const float2 pl = roi.img[(row * R + col) * roi.ld];
+                const float w = roi.w[(row * R + col) * roi.ld];
+                const float dx0 = (col + 0.5f) - c[1], dx1 = (col + 0.5f) - c[4];
+                const float r0 = __fmaf_rn(dx0, dx0, dy0 * dy0), r1 = __fmaf_rn(dx1, dx1, dy1 * dy1);
+                const float e0 = __expf(-r0 * S01), e1 = __expf(-r1 * S01);
+                const float mu = __fmaf_rn(A0, e0, __fmaf_rn(A1, e1, B64));
+                const float q = w * (1.0f - __fdividef(pl.x, mu));
+                const float q0 = q * e0, q1 = q * e1;
+                gA0 += q0;
+                gX0 = __fmaf_rn(q0, dx0, gX0);
+                gY0 = __fmaf_rn(q0, dy0, gY0);
+                gA1 += q1;
+                gX1 = __fmaf_rn(q1, dx1, gX1);
+                gY1 = __fmaf_rn(q1, dy1, gY1);
+                gS = __fmaf_rn(A0 * q0, r0, __fmaf_rn(A1 * q1, r1, gS));
+                gB += q;
+            }
+        }
+        g[0] = QCS_ASCALE * gA0;
+        g[1] = A0 * 2.0f * S01 * gX0;
+        g[2] = A0 * 2.0f * S01 * gY0;
+        g[3] = QCS_ASCALE * gA1;
+        g[4] = A1 * 2.0f * S01 * gX1;
+        g[5] = A1 * 2.0f * S01 * gY1;
+        g[6] = -QCS_SSCALE * gS;
+        g[7] = QCS_BSCALE * gB;
+    }
+};
 // Loss and gradient of one single-emitter ROI (GS2D / AS3D) evaluated by a
 // group of G consecutive lanes of a warp, bit for bit equal to ThreadEval:
 //  - loss: the lanes compute the pixel terms k = lane, lane + G, ... (the

@@ -40,6 +40,22 @@ cudaError_t launch_fit_group(int kind, int R, int lanes, const FitLaunch &a);
 bool learned_schedule_supported(int kind, int R, int iters, int bisections);
 cudaError_t launch_fit_learned(int kind, int R, int iters, int bisections, const FitLaunch &a, const float *start,
                                float dev_th, uint8_t *refit);
+// Learned-start GS2D two-emitter fit (R = 7, 9, 11) of the records of a.q
+// (grid from a.max_count) from start[8 id ..] (peak e-, x, y of emitter 0 and
+// of emitter 1, sigma, background e-) with `iters` iterations of `bisections`
+// steps (learned_2e_supported): rows and stage results as launch_fit(k2E);
+// poor fits get refit[slot] = 1 (to3e = 0: to redo with the plain kernel) or
+// stage result 0 and no rows (to3e = 1: on to the three-emitter fit).
+bool learned_2e_supported(int R, int iters, int bisections);
+cudaError_t launch_fit_learned_2e(int R, int iters, int bisections, const FitLaunch &a, const float *start,
+                                  float dev_th, uint8_t *refit, int to3e);
+// slots[] / ids[]: the queue slots i < min(*n_dev, max_n) with flags[i] != 0
+// and q[i]; *count = their number.
+cudaError_t launch_flag_slots(const uint8_t *flags, const int *n_dev, int max_n, const int *q, int *slots, int *ids,
+                              int *count, cudaStream_t s);
+// res[slots[k]] = res_k[k] and, when 2, extra[slots[k]] = extra_k[k] (12 floats), k < min(*count, max_n).
+cudaError_t launch_merge_refit(const int *slots, const int *count, int max_n, const int8_t *res_k,
+                               const float *extra_k, int8_t *res, float *extra, cudaStream_t s);
 // ids[] = the indices i < n with flags[i] != 0 (any order), *count = their number.
 cudaError_t launch_flag_queue(const uint8_t *flags, int n, int *ids, int *count, cudaStream_t s);
 

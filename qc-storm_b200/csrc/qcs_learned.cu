@@ -23,6 +23,7 @@
 
 #include "../../include/qcstorm_b200.h"
 #include "qcs_error.h"
+#include "qcs_kernels.h"
 #include "qcs_learned.h"
 
 namespace qcs {
@@ -234,7 +235,8 @@ __global__ void colsum_kernel(const float *__restrict__ dZ, int rows, int cols, 
 // cls[i] >= 0 (GS2D networks), kCountWeight x the softmax cross-entropy of
 // the count logits against class cls[i]: loss and dY.
 __global__ void mse_kernel(const float *__restrict__ Y, const float *__restrict__ T, const float *__restrict__ valid,
-                           const float *__restrict__ cls, int rows, int nused, float inv_count, float *__restrict__ dY,
+                           const float *__restrict__ cls, int rows, int nused, int wrow, float inv_count,
+                           float *__restrict__ dY,
                            float *__restrict__ loss) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= rows) return;
@@ -246,8 +248,8 @@ __global__ void mse_kernel(const float *__restrict__ Y, const float *__restrict_
         float d = 0.0f;
         if (j < nused) {
             const float e = y[j] - T[(size_t)i * nused + j];
-            d = 2.0f * kTargetWeight[j] * e * v * inv_count;
-            l += kTargetWeight[j] * e * e * v;
+            d = 2.0f * kTargetWeight[wrow][j] * e * v * inv_count;
+            l += kTargetWeight[wrow][j] * e * e * v;
         }
         dY[(size_t)i * kOut + j] = d;
     }
@@ -291,6 +293,19 @@ __global__ void gather_rows_kernel(const float *__restrict__ src, const int *__r
 template <int R, int LT>
 __device__ __forceinline__ void start_from_outputs(const float *y, float lo, float rng, float *st) {
     const float centre = R / 2.0f;
+    if (LT == kTwo) {
+        // emitters anywhere up to a pixel inside the ROI's edge
+        const float w2 = R / 2.0f - 1.0f;
+        st[0] = rng * expf(fminf(fmaxf(y[4], -6.0f), 3.0f));
+        st[1] = centre + fminf(fmaxf(y[0], -w2), w2);
+        st[2] = centre + fminf(fmaxf(y[1], -w2), w2);
+        st[3] = rng * expf(fminf(fmaxf(y[5], -6.0f), 3.0f));
+        st[4] = centre + fminf(fmaxf(y[2], -w2), w2);
+        st[5] = centre + fminf(fmaxf(y[3], -w2), w2);
+        st[6] = fminf(fmaxf(kSigma0 + y[6], 0.6f), 3.0f);
+        st[7] = fmaxf(lo + rng * y[7], 1.0f);
+        return;
+    }
     const float win = LT == QCS_LOCTYPE_AS3D ? 2.5f : 1.5f;
     const float smax = LT == QCS_LOCTYPE_AS3D ? 4.0f : 3.0f;
     st[0] = rng * expf(fminf(fmaxf(y[3], -6.0f), 3.0f));
@@ -685,6 +700,10 @@ namespace L = qcs::learned;
 struct qcs_learned_net {
     int loc_type = QCS_LOCTYPE_GS2D;  // the shape the network is built for
     int R = 7;
+    // GS2D networks: the two-emitter network whose start points the 2E stage uses, and its schedule
+    qcs_learned_net *two = nullptr;
+    int two_iters = 3, two_bisections = 6, two_to3e = 1;
+    float two_dev_th = 0.0f;
     int kin = 64;                     // input width: in_width(R)
     int params = 0;                   // param_count(kin)
     // parameters (FP32 master copies), their gradients and Adam moments, in one block
@@ -812,6 +831,12 @@ cudaError_t by_shape(int loc_type, int R, F &&f) {
         case 9: return f(Shape<9, QCS_LOCTYPE_GS2D>{});
         case 11: return f(Shape<11, QCS_LOCTYPE_GS2D>{});
         }
+    } else if (loc_type == L::kTwo) {
+        switch (R) {
+        case 7: return f(Shape<7, L::kTwo>{});
+        case 9: return f(Shape<9, L::kTwo>{});
+        case 11: return f(Shape<11, L::kTwo>{});
+        }
     }
     return cudaErrorInvalidValue;
 }
@@ -871,12 +896,26 @@ cudaError_t fused_start_points(qcs_learned_net *net, const qcs_loc_para *p, cons
 
 // net's shape against the call's parameters
 int check_shape(const qcs_learned_net *net, const qcs_loc_para *p) {
-    if (p->ROISize != net->R || p->LocType != net->loc_type)
+    const int want = net->loc_type == L::kTwo ? QCS_LOCTYPE_GS2D : net->loc_type;
+    if (p->ROISize != net->R || p->LocType != want)
         return fail(QCS_ERR_ROISIZE, "the network was built for another localization type or ROI size");
     return QCS_OK;
 }
 
 }  // namespace
+
+namespace qcs {
+namespace learned {
+qcs_learned_net *two_emitter(const qcs_learned_net *net, int *iters, int *bisections, float *dev_th, int *to3e) {
+    if (!net || !net->two) return nullptr;
+    *to3e = net->two_to3e;
+    *iters = net->two_iters;
+    *bisections = net->two_bisections;
+    *dev_th = net->two_dev_th;
+    return net->two;
+}
+}  // namespace learned
+}  // namespace qcs
 
 extern "C" {
 
@@ -1069,6 +1108,7 @@ int qcs_learned_gradient_counts_device(qcs_learned_net *net, const float *d_feat
     QCS_CUDA(forward(net, net->d_x, n, net->d_z1, net->d_a1, net->d_z2, net->d_a2, net->d_y, s), "forward");
     QCS_CUDA(cudaMemsetAsync(net->d_loss, 0, sizeof(float), s), "clear loss");
     L::mse_kernel<<<blocks(n), 256, 0, s>>>(net->d_y, d_targets, d_valid, d_classes, n, L::used_outputs(net->loc_type),
+                                            net->loc_type == L::kTwo ? 1 : 0,
                                             1.0f / (float)n, net->d_dy, net->d_loss);
     QCS_CUDA(backward(net, n, s), "backward");
     if (h_loss) {
@@ -1123,7 +1163,8 @@ int qcs_learned_train_counts_device(qcs_learned_net *net, const float *d_feat, c
             e = forward(net, net->d_x, B, net->d_z1, net->d_a1, net->d_z2, net->d_a2, net->d_y, s);
             if (e != cudaSuccess) break;
             // per-batch mean loss and its gradient; the loss accumulates over the epoch
-            L::mse_kernel<<<blocks(B), 256, 0, s>>>(net->d_y, d_tb, d_vb, d_cb, B, nu, 1.0f / (float)B, net->d_dy,
+            L::mse_kernel<<<blocks(B), 256, 0, s>>>(net->d_y, d_tb, d_vb, d_cb, B, nu, net->loc_type == L::kTwo ? 1 : 0,
+                                                    1.0f / (float)B, net->d_dy,
                                                     net->d_loss);
             e = backward(net, B, s);
             if (e != cudaSuccess) break;
@@ -1197,6 +1238,29 @@ int qcs_learned_set_count_threshold(qcs_learned_net *net, float th) {
 }
 
 float qcs_learned_count_threshold(const qcs_learned_net *net) { return net ? net->count_th : 0.0f; }
+
+int qcs_learned_set_two_emitter(qcs_learned_net *net, qcs_learned_net *two, int iters, int bisections,
+                                float dev_th, int fallback) {
+    if (!net) return fail(QCS_ERR_ARG, "null network");
+    if (!two) {
+        net->two = nullptr;
+        return QCS_OK;
+    }
+    if (net->loc_type != QCS_LOCTYPE_GS2D || two->loc_type != L::kTwo || two->R != net->R)
+        return fail(QCS_ERR_ARG, "two-emitter start points: a QCS_LEARNED_GS2D_2E network of the GS2D network's ROI size");
+    if (bisections <= 0) bisections = 11;
+    if (!qcs::learned_2e_supported(net->R, iters, bisections))
+        return fail(QCS_ERR_ARG, "two-emitter schedules: 3 or 4 iterations of 6 line-search steps, or 13 of 11");
+    if (!(dev_th >= 0.0f)) return fail(QCS_ERR_ARG, "negative deviance bound");
+    if (fallback != QCS_TWO_FALLBACK_3E && fallback != QCS_TWO_FALLBACK_PLAIN)
+        return fail(QCS_ERR_ARG, "fallback: QCS_TWO_FALLBACK_3E or QCS_TWO_FALLBACK_PLAIN");
+    net->two_to3e = fallback == QCS_TWO_FALLBACK_3E ? 1 : 0;
+    net->two = two;
+    net->two_iters = iters;
+    net->two_bisections = bisections;
+    net->two_dev_th = dev_th;
+    return QCS_OK;
+}
 
 size_t qcs_learned_work_bytes(int n) {
     return (size_t)(n > 0 ? n : 0) * (L::in_width(11) + 2 + L::kOut) * sizeof(float);

@@ -12,7 +12,8 @@ namespace learned {
 constexpr float kSigma0 = 1.3f;         // sigma offset of the sigma outputs
 constexpr int kHidden = 128;
 constexpr int kOut = 8;                 // start-point outputs, then (GS2D) three emitter-count logits
-constexpr int kUsedMax = 6;             // start-point outputs of the widest kind (AS3D)
+constexpr int kUsedMax = 8;             // start-point outputs of the widest kind (two-emitter GS2D)
+constexpr int kTwo = QCS_LEARNED_GS2D_2E;  // network kind of the two-emitter start points
 constexpr int kCount0 = 5;              // GS2D: logits of the emitter-count classes 0, 1, 2 (outputs 5..7)
 constexpr int kClasses = 3;             // one emitter / two-emitter stage / three-emitter stage
 
@@ -21,21 +22,32 @@ constexpr int kClasses = 3;             // one emitter / two-emitter stage / thr
 // log(range) / 8, log(min) / 8, zero padding to 64 (7x7) or 128 (9x9, 11x11).
 __host__ __device__ constexpr int in_width(int R) { return R * R + 2 <= 64 ? 64 : 128; }
 // Outputs fitted to the targets: GS2D dx, dy, sigma - 1.3, log(peak / range),
-// (background - min) / range; AS3D the same with sigma_x and then sigma_y - 1.3.
-__host__ __device__ constexpr int used_outputs(int loc_type) { return loc_type == QCS_LOCTYPE_AS3D ? 6 : 5; }
+// (background - min) / range; AS3D the same with sigma_x and then sigma_y - 1.3;
+// two-emitter GS2D dx0, dy0, dx1, dy1, log(peak0 / range), log(peak1 / range),
+// sigma - 1.3, (background - min) / range.
+__host__ __device__ constexpr int used_outputs(int loc_type) {
+    return loc_type == kTwo ? 8 : (loc_type == QCS_LOCTYPE_AS3D ? 6 : 5);
+}
 // Start point per record: GS2D peak e-, x, y, sigma, background e-; AS3D
-// peak e-, x, y, sigma_x, sigma_y, background e- (the fit's parameter order).
-__host__ __device__ constexpr int start_width(int loc_type) { return loc_type == QCS_LOCTYPE_AS3D ? 6 : 5; }
+// peak e-, x, y, sigma_x, sigma_y, background e-; two-emitter GS2D peak e-,
+// x, y of emitter 0, the same of emitter 1, sigma, background e- (each fit's
+// parameter order).
+__host__ __device__ constexpr int start_width(int loc_type) {
+    return loc_type == kTwo ? 8 : (loc_type == QCS_LOCTYPE_AS3D ? 6 : 5);
+}
 constexpr int param_count(int kin) {
     return kin * kHidden + kHidden + kHidden * kHidden + kHidden + kHidden * kOut + kOut;
 }
 inline bool shape_supported(int loc_type, int R) {
-    return (loc_type == QCS_LOCTYPE_GS2D || loc_type == QCS_LOCTYPE_AS3D) && (R == 7 || R == 9 || R == 11);
+    return (loc_type == QCS_LOCTYPE_GS2D || loc_type == QCS_LOCTYPE_AS3D || loc_type == kTwo) &&
+           (R == 7 || R == 9 || R == 11);
 }
 
 // loss weight of each start-point output (positions matter most) and of the
 // emitter-count cross-entropy
-__constant__ const float kTargetWeight[kUsedMax] = {4.0f, 4.0f, 1.0f, 1.0f, 1.0f, 1.0f};
+// (row 0: single-emitter kinds, row 1: two-emitter GS2D)
+__constant__ const float kTargetWeight[2][kUsedMax] = {{4.0f, 4.0f, 1.0f, 1.0f, 1.0f, 1.0f, 0.0f, 0.0f},
+                                                       {4.0f, 4.0f, 4.0f, 4.0f, 1.0f, 1.0f, 1.0f, 1.0f}};
 constexpr float kCountWeight = 0.5f;
 
 // Emitter-count class from the three logits: 2 when p(class 2) >= th, else 1
@@ -56,5 +68,8 @@ __host__ __device__ inline int count_class(float l0, float l1, float l2, float t
 cudaError_t start_points(qcs_learned_net *net, const qcs_loc_para *p, const uint16_t *d_rois, int n, float *out,
                          cudaStream_t s, uint8_t *cls = nullptr, const int *n_dev = nullptr);
 
+// The two-emitter network attached to a GS2D network (qcs_learned_set_two_emitter),
+// its schedule and fallback (to3e: poor fits go on to the three-emitter fit), or null.
+qcs_learned_net *two_emitter(const qcs_learned_net *net, int *iters, int *bisections, float *dev_th, int *to3e);
 }  // namespace learned
 }  // namespace qcs

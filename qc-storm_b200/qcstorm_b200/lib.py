@@ -121,6 +121,10 @@ _SIGS = {
                                                   C.c_void_p]),
     "qcs_loc_count_labels_device": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "qcs_learned_set_count_threshold": (C.c_int, [C.c_void_p, C.c_float]),
+    "qcs_learned_set_two_emitter": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_int]),
+    "qcs_learned_refit_2e_num": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "qcs_loc_two_emitter_targets_device": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(LocPara), C.c_int, C.c_void_p,
+                                                     C.c_void_p, C.c_void_p, C.c_void_p]),
     "qcs_consec_init": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
     "qcs_consec_deinit": (C.c_int, [C.c_void_p]),
     "qcs_consec_fit": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.POINTER(LocPara), C.c_void_p]),
@@ -461,8 +465,8 @@ def learned_in_width(roi_size):
 
 
 def learned_start_width(loc_type):
-    """Start-point floats per record: GS2D 5, AS3D 6."""
-    return 6 if loc_type == 1 else 5
+    """Start-point floats per record: GS2D 5, AS3D 6, two-emitter GS2D 8."""
+    return 8 if loc_type == LEARNED_GS2D_2E else (6 if loc_type == 1 else 5)
 
 
 class LearnedNet:
@@ -552,6 +556,21 @@ class LearnedNet:
         """Emitter-count routing threshold (0: route by the WLE classes alone)."""
         check(self.lib.qcs_learned_set_count_threshold(self.h, C.c_float(th)))
 
+    def set_two_emitter(self, two, iters=3, bisections=6, dev_th=0.0, fallback="3e"):
+        """Start the two-emitter fits of learned multi-emitter calls from the
+        LEARNED_GS2D_2E network `two` (None detaches); poor fits go on to the
+        three-emitter fit (fallback "3e") or are refitted plainly ("plain")."""
+        if fallback not in ("3e", "plain"):
+            raise ValueError("fallback: '3e' or 'plain'")
+        check(self.lib.qcs_learned_set_two_emitter(self.h, two.h if two is not None else None, int(iters),
+                                                   int(bisections), C.c_float(dev_th), 0 if fallback == "3e" else 1))
+        self._two = two
+
+    def refits_2e(self, ctx):
+        k = C.c_int(0)
+        check(self.lib.qcs_learned_refit_2e_num(ctx.h, C.byref(k)))
+        return k.value
+
     def count_threshold(self):
         return float(self.lib.qcs_learned_count_threshold(self.h))
 
@@ -613,6 +632,21 @@ def fit_from_start(ctx, d_rois, n, d_start, d_wle=0, iters=3, dev_th=0.0, para=N
                                                    C.c_void_p(d_classes) if d_classes else None, int(iters),
                                                    int(bisections), C.c_float(dev_th),
                                                    C.c_void_p(stream) if stream else None))
+
+
+LEARNED_GS2D_2E = 16  # network kind of the two-emitter start points
+
+
+def two_emitter_targets(ctx, para, d_rois, scale, n, stream=0):
+    """Targets (n x 8) and valid flags of a LEARNED_GS2D_2E network from the
+    plain multi-emitter call just made on ctx over the same n records."""
+    import torch
+    t = torch.empty((n, 8), dtype=torch.float32, device="cuda")
+    v = torch.empty((n,), dtype=torch.float32, device="cuda")
+    check(load().qcs_loc_two_emitter_targets_device(ctx.h, C.c_void_p(d_rois), C.byref(para), int(n),
+                                                    C.c_void_p(scale.data_ptr()), C.c_void_p(t.data_ptr()),
+                                                    C.c_void_p(v.data_ptr()), C.c_void_p(stream) if stream else None))
+    return t, v
 
 
 def count_labels(ctx, n, stream=0):
