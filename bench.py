@@ -1041,6 +1041,53 @@ def profile_learned(n, stream):
     return 0
 
 
+def profile_multi(n, stream):
+    """The 1-3 emitter 11x11 workload for ncu: networks trained as in
+    learned_shapes_measure (count classes and two-emitter starts, SHAPE_TRAIN
+    records), then one plain localization call over n records inside the NVTX
+    range "plain" and three learned calls (two-emitter starts, poor fits on to
+    the three-emitter fit) inside "learned"."""
+    import torch
+    from qcstorm_b200 import lib, synth
+    Rm = 11
+    sh = stream.cuda_stream
+    tr, para, _ = synth.multi_rois(SHAPE_TRAIN, R=Rm, seed=7000)
+    d_tr = torch.from_numpy(tr.view(np.int16)).cuda()
+    ctx_tr = lib.LocContext(para, capacity=SHAPE_TRAIN)
+    ctx_tr.localize_device(d_tr.data_ptr(), SHAPE_TRAIN, 0, sh)
+    labels = lib.count_labels(ctx_tr, SHAPE_TRAIN, sh)
+    feat, scale = lib.LearnedNet.features(para, d_tr.data_ptr(), SHAPE_TRAIN, stream=sh)
+    tgt, valid = lib.LearnedNet.targets(para, d_tr.data_ptr(), ctx_tr.device_rows(), scale, SHAPE_TRAIN, stream=sh)
+    stream.synchronize()
+    valid = valid * (labels == 0).float()
+    torch.cuda.synchronize()
+    net = lib.LearnedNet(batch=4096, seed=5, loc_type=para.LocType, roi_size=Rm)
+    net.train(feat, tgt, valid, epochs=TRAIN_EPOCHS, lr=2e-3, stream=sh, classes=labels)
+    net.set_count_threshold(0.5)
+    net2 = train_two_emitter_net(ctx_tr, para, d_tr, feat, scale, SHAPE_TRAIN, Rm, TRAIN_EPOCHS, stream)
+    net.set_two_emitter(net2, iters=TWO_ITERS, bisections=6)
+    ctx_tr.close()
+    rec, _, _ = synth.multi_rois(n, R=Rm, seed=8000)
+    d = torch.from_numpy(rec.view(np.int16)).cuda()
+    ctx = lib.LocContext(para, capacity=n)
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("plain")
+    ctx.localize_device(d.data_ptr(), n, 0, sh)
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    torch.cuda.nvtx.range_push("learned")
+    for _ in range(3):
+        net.localize(ctx, d.data_ptr(), n, iters=2, bisections=6, stream=sh)
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    print(json.dumps({"profile_multi": n, "refits": net.refits(ctx)}))
+    ctx.close()
+    net.set_two_emitter(None)
+    net2.close()
+    net.close()
+    return 0
+
+
 def profile_fit(n):
     """Three launches of the single-emitter fit kernel over n records."""
     import torch
@@ -1082,6 +1129,9 @@ def main():
                     help="only run the single-emitter fit and CRLB kernels 3 times on N records (for ncu captures)")
     ap.add_argument("--profile-frames", type=int, default=0, metavar="K",
                     help="only run K calls of the whole-frame pipeline (for ncu captures)")
+    ap.add_argument("--profile-multi", type=int, default=0, metavar="N",
+                    help="trained 1-3 emitter 11x11 networks, then one plain and three learned calls over N records "
+                         "in the NVTX ranges plain and learned (for ncu)")
     ap.add_argument("--profile-learned", type=int, default=0, metavar="N",
                     help="only train the start-point network and run 3 learned-start calls on N records")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-start measurement")
@@ -1110,6 +1160,8 @@ def main():
         return profile_frames(args.profile_frames, stream)
     if args.profile_learned:
         return profile_learned(args.profile_learned, stream)
+    if args.profile_multi:
+        return profile_multi(args.profile_multi, stream)
     dist = None
     if world > 1:
         import datetime
