@@ -166,6 +166,21 @@ def device_timed(steps, warmup, enqueue, streams, dist):
     return max_over_ranks(e0.elapsed_time(e1), dist)
 
 
+MIN_TIMED_MS = 1000.0  # the K-step window is repeated until the device-timed total reaches this
+
+
+def device_timed_windows(steps, warmup, enqueue, streams, dist):
+    """device_timed over windows of exactly `steps` calls, repeated until the
+    windows add up to MIN_TIMED_MS of device time (so the clock sampler, which
+    polls every 200 ms, sees the timed region); returns (median window ms,
+    window count).  The count follows from the first window's slowest-rank
+    time, so every rank runs the same windows."""
+    first = device_timed(steps, warmup, enqueue, streams, dist)
+    more = 0 if first >= MIN_TIMED_MS else min(int(math.ceil(MIN_TIMED_MS / max(first, 1e-3))) - 1, 500)
+    windows = [first] + [device_timed(steps, 0, enqueue, streams, dist) for _ in range(more)]
+    return statistics.median(windows), len(windows)
+
+
 def job_rate(steps, per_step, world, ms):
     """Whole-job rate: every rank's records over the slowest rank's time."""
     return steps * per_step * world / (ms * 1e-3)
@@ -219,7 +234,7 @@ def run_reference_arm(args, rank):
     v = statistics.median(rates)
     base["value"] = v
     line = {
-        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": env_int("WORLD_SIZE", 1),
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * N_PER_STEP / v,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic", "config": config_dict(args),
@@ -520,7 +535,7 @@ def learned_measure(args, streams, ctxs, para, d_batches, h_batches, rec0, truth
         net.localize(c or ctxs[k % 2], d_batches[k % BATCHES].data_ptr(), N_PER_STEP, 0, iters=LEARNED_ITERS,
                      bisections=LEARNED_BISECTIONS, stream=s.cuda_stream)
 
-    ms = device_timed(args.steps, args.warmup, step, streams, dist)
+    ms, windows = device_timed_windows(args.steps, args.warmup, step, streams, dist)
     value = job_rate(args.steps, N_PER_STEP, world, ms)
     one_steps = min(args.steps, 200)
     ms1 = device_timed(one_steps, 3, lambda k, s: step(k, s, ctx), [stream], dist)
@@ -532,9 +547,13 @@ def learned_measure(args, streams, ctxs, para, d_batches, h_batches, rec0, truth
     step(0, stream, ctx)
     learned, _ = ctx.read_rows(sh)
     refits = net.refits(ctx)
-    both = (plain[:, 0] > 0) & (learned[:, 0] > 0)
+    acc_p, acc_l = plain[:, 0] > 0, learned[:, 0] > 0
+    both = acc_p & acc_l
     rp, pp, crlb = fit_accuracy(plain, rec0, truth0, both, para)
     rl, pl, _ = fit_accuracy(learned, rec0, truth0, both, para)
+    # each arm over its own accepted records (learned accepts more)
+    rp_own, pp_own, crlb_p_own = fit_accuracy(plain, rec0, truth0, acc_p, para)
+    rl_own, pl_own, crlb_l_own = fit_accuracy(learned, rec0, truth0, acc_l, para)
 
     # end to end: pinned host records in, rows out, through qcs_learned_localize_async
     e2e_pipelined(ctxs, streams, h_batches, 4, net=net)
@@ -544,6 +563,7 @@ def learned_measure(args, streams, ctxs, para, d_batches, h_batches, rec0, truth
     net.close()
     return {
         "value": value, "unit": UNIT, "ms_per_step": ms / args.steps, "vs_plain": value / plain_value,
+        "windows": windows,
         "value_one_stream": value1, "timing": "two contexts in turn on two streams (value_one_stream: one)",
         "iters": LEARNED_ITERS, "bisections": LEARNED_BISECTIONS, "refits_per_step": refits,
         # mlp_tc (features + network), WLE (5), fit_learned, flag_queue, group refit, refit CRLB, counters, CRLB
@@ -558,7 +578,11 @@ def learned_measure(args, streams, ctxs, para, d_batches, h_batches, rec0, truth
                      "crlb_px": crlb, "accepted": {"plain": float((plain[:, 0] > 0).mean()),
                                                    "learned": float((learned[:, 0] > 0).mean())},
                      "equal_rmse": bool(rl <= 1.02 * rp),
-                     "basis": "records accepted by both; ground truth of the generator"},
+                     "basis": "records accepted by both; ground truth of the generator",
+                     "own_accepted": {"rmse_px": {"plain": rp_own, "learned": rl_own},
+                                      "photon_rel_rmse": {"plain": pp_own, "learned": pl_own},
+                                      "crlb_px": {"plain": crlb_p_own, "learned": crlb_l_own},
+                                      "basis": "each arm over the records it accepts"}},
         "train": train,
         "network": "64-128-128-8 MLP on the 7x7 pixels (+2 scale features), BF16 operands, FP32 accumulation; "
                    "inference fused with the features in one tcgen05 kernel",
@@ -1117,6 +1141,23 @@ def profile_frames(calls, stream):
     return 0
 
 
+def free_port():
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        return so.getsockname()[1]
+
+
+def relaunch(n):
+    """`bench.py --gpus N` started without a launcher: run it again as N ranks
+    (one process per GPU) under torch.distributed.run on this node, bounded by
+    `timeout` well above the process group's own timeout."""
+    cmd = ["timeout", "-k", "60", "3600", sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           "--nproc-per-node", str(n), "--master-addr", "127.0.0.1", "--master-port", str(free_port()),
+           os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1139,8 +1180,11 @@ def main():
                     help="skip the mixed 7/9/11 learned measurement (4e6 training, 1e7 evaluation records)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return relaunch(args.gpus)
 
     world = env_int("WORLD_SIZE", 1)
+    args.gpus = world  # the line reports the ranks that actually ran
     rank = env_int("RANK", 0)
     local = env_int("LOCAL_RANK", 0)
     if args.impl == "reference":
@@ -1195,7 +1239,7 @@ def main():
     sampler, spath = start_clock_sampler(local)
     time.sleep(0.5)  # first nvidia-smi sample lands before the timed region
     t_start = time.time()
-    ms = device_timed(args.steps, args.warmup, step, streams, dist)
+    ms, windows = device_timed_windows(args.steps, args.warmup, step, streams, dist)
     t_end = time.time()
     clocks = stop_clock_sampler(sampler, spath, t_start, t_end)
     value = job_rate(args.steps, N_PER_STEP, world, ms)
@@ -1278,9 +1322,12 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config_dict(args),
+            "windows": windows, "window_note": "value = median over %d device-timed windows of exactly %d steps "
+                                              "(repeated to >= %.0f ms so the clock samples cover them)" % (
+                                                  windows, args.steps, MIN_TIMED_MS),
             "value_one_stream": value1, "timing": "two contexts in turn on two streams, CUDA events around both "
                                                   "(value_one_stream: one context, one stream)",
-            "e2e": e2e, "gpu_launches": launches_per_step * args.steps,
+            "e2e": e2e, "gpu_launches": launches_per_step * args.steps * windows,
             "roofline": {"bound": "sfu", "kernel": "fit_single_kernel<7,GS2D>", "achieved": achieved,
                          "peak": mufu_peak, "unit": "MUFU op/s", "frac": achieved / mufu_peak,
                          "traffic": DRAM_BYTES_PER_FIT * N_PER_STEP,
@@ -1294,6 +1341,24 @@ def main():
             "consecutive_fit": consec, "autotune": tune,
             "frames": frames,
         }
+        if learned:
+            a = learned["accuracy"]
+            line.update({
+                "learned_value": learned["value"], "learned_vs_plain": learned["vs_plain"],
+                "learned_e2e_value": learned["e2e"]["value"],
+                "learned_rmse_px": a["rmse_px"]["learned"], "plain_rmse_px": a["rmse_px"]["plain"],
+                "learned_rmse_px_own": a["own_accepted"]["rmse_px"]["learned"],
+                "plain_rmse_px_own": a["own_accepted"]["rmse_px"]["plain"],
+                "learned_accept": a["accepted"]["learned"], "plain_accept": a["accepted"]["plain"],
+                "learned_equal_rmse": a["equal_rmse"], "crlb_px": a["crlb_px"],
+            })
+        # short keys first: the headline survives a truncated tail of the line
+        head = ["metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
+                "vs_baseline", "dtype", "data", "learned_value", "learned_vs_plain", "learned_e2e_value",
+                "learned_rmse_px", "plain_rmse_px", "learned_rmse_px_own", "plain_rmse_px_own", "learned_accept",
+                "plain_accept", "learned_equal_rmse", "crlb_px", "gpu_launches", "windows", "clocks", "roofline",
+                "e2e", "cpu_baseline", "config"]
+        line = {**{k: line[k] for k in head if k in line}, **{k: v for k, v in line.items() if k not in head}}
         print(json.dumps(line), flush=True)
     for c in ctxs:
         c.close()

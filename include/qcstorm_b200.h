@@ -487,6 +487,10 @@ int qcs_learned_create_for(int loc_type, int roi_size, int batch, unsigned long 
 int qcs_learned_create(int batch, unsigned long long seed, qcs_learned_net **out);
 /* The network's localization type, ROI size and parameter count (any may be NULL). */
 int qcs_learned_shape(const qcs_learned_net *net, int *loc_type, int *roi_size, int *params);
+/* Frees the network.  A QCS_LEARNED_GS2D_2E network that is attached to a
+ * GS2D network (qcs_learned_set_two_emitter) is refused with QCS_ERR_STATE
+ * and left intact: detach it or destroy its owner first.  Destroying an owner
+ * detaches its two-emitter network. */
 int qcs_learned_destroy(qcs_learned_net *net);
 int qcs_learned_get_params(qcs_learned_net *net, float *h_params);
 int qcs_learned_set_params(qcs_learned_net *net, const float *h_params);
@@ -530,7 +534,10 @@ int qcs_loc_count_labels_device(qcs_loc_data *c, int n, float *d_labels, void *s
 int qcs_learned_set_count_threshold(qcs_learned_net *net, float th);
 float qcs_learned_count_threshold(const qcs_learned_net *net);
 /* Attaches a QCS_LEARNED_GS2D_2E network `two` of the same ROI size to the
- * GS2D network `net` (NULL detaches): learned localization calls with
+ * GS2D network `net` (NULL detaches).  `net` keeps a pointer to `two`, so
+ * `two` must stay alive while attached: qcs_learned_destroy(two) refuses
+ * (QCS_ERR_STATE) until it is detached or `net` is destroyed.  Learned
+ * localization calls with
  * multi-emitter fitting on then start the cascade's two-emitter fits from
  * its start points with `iters` BFGS iterations of `bisections` line-search
  * steps (3 or 4 of 6, or the reference's 13 of 11) and the analytic gradient.
@@ -698,7 +705,10 @@ int qcs_locfile_close(qcs_locfile *f);
  * into *d_nvalid (device int, may be NULL).  Allocates nothing: its queues
  * and counters live in one fixed library array, so n is limited to
  * QCS_NOALLOC_MAX_ROIS (else QCS_ERR_CAPACITY).  The first call on a device
- * looks up that array's address; make it before any stream capture.  All
+ * looks up that array's address; make it before any stream capture.  After a
+ * device reset the next call looks the address up again in the new context,
+ * so that call, too, must come before any capture.  QE <= 0 is refused
+ * (QCS_ERR_ARG) before any device work.  All
  * calls on a device share the array: calls that overlap on the GPU race and
  * must not be issued.  Asynchronous on `stream`.
  */

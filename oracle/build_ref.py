@@ -49,7 +49,22 @@ import sys
 import tempfile
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-DEFAULT_REF = "/root/reference/MLEbfgs/bfgs_MLE_dll x64/bfgsMLE_dll/bfgsMLE_dll"
+# The localization library inside the reference checkout; the checkout itself
+# is BASELINE.json's reference_path (or --ref names the library directory).
+LIB_SUBDIR = os.path.join("MLEbfgs", "bfgs_MLE_dll x64", "bfgsMLE_dll", "bfgsMLE_dll")
+
+
+def default_ref():
+    """The reference's localization library, from BASELINE.json's reference_path."""
+    import json
+    try:
+        with open(os.path.join(os.path.dirname(HERE), "BASELINE.json")) as f:
+            root = json.load(f).get("reference_path")
+    except (OSError, ValueError):
+        root = None
+    return os.path.join(root, LIB_SUBDIR) if root else None
+
+
 OUT_DIR = os.path.join(HERE, "_ref")
 OUT_SO = os.path.join(OUT_DIR, "libqcs_ref_host.so")
 OUT_GPU_SO = os.path.join(OUT_DIR, "libqcs_ref_gpu.so")
@@ -131,7 +146,7 @@ def run_parallel(cmds):
 
 
 def build_gpu(args):
-    if not os.path.isdir(args.ref):
+    if not args.ref or not os.path.isdir(args.ref):
         print("build_ref: reference tree not present, skipping")
         return 0
     ours = [os.path.join(HERE, "ref_harness_gpu.cu"), os.path.abspath(__file__),
@@ -169,13 +184,16 @@ def newest_mtime(paths):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default=DEFAULT_REF)
+    ap.add_argument("--ref", default=None, help="the reference's bfgsMLE_dll library directory "
+                    "(default: BASELINE.json's reference_path + " + LIB_SUBDIR + ")")
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--gpu", action="store_true")
     args = ap.parse_args()
+    if args.ref is None:
+        args.ref = default_ref()
     if args.gpu:
         return build_gpu(args)
-    if not os.path.isdir(args.ref):
+    if not args.ref or not os.path.isdir(args.ref):
         print("build_ref: reference tree not present, skipping")
         return 0
     ours = [os.path.join(HERE, "ref_harness.cpp"), os.path.join(HERE, "refshim", "cuda_runtime.h"),

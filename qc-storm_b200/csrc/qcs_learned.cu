@@ -520,7 +520,8 @@ __global__ void __launch_bounds__(128, 1) mlp_tc_kernel(const uint16_t *__restri
     uint32_t phase = 0, rec_phase = 0;
     bool ok = true, copy_pending = BULK && (int)blockIdx.x < ntiles;
     uint16_t *srec = reinterpret_cast<uint16_t *>(base + L::OFF_REC);
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    int tile = blockIdx.x;
+    for (; tile < ntiles; tile += gridDim.x) {
         const int i = tile * kM + tid;
         const int rows = tile_rows(tile, n);
         if (BULK) {
@@ -669,7 +670,21 @@ __global__ void __launch_bounds__(128, 1) mlp_tc_kernel(const uint16_t *__restri
     fence_after();
     if (warp == 0)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
-    if (!ok && tid == 0) atomicExch(err, 1);
+    if (!ok) {
+        // A wait gave up: this CTA's tiles from the failed one on get NaN start
+        // points (and the single-emitter class), so their fits are rejected and
+        // the deviance judge hands them to the plain refit instead of fitting
+        // from a previous call's start points.  The sticky error flag records it.
+        for (int t = tile; t < ntiles; t += gridDim.x) {
+            if (tid < tile_rows(t, n)) {
+                const int r = t * kM + tid;
+#pragma unroll
+                for (int j = 0; j < NST; ++j) start[(size_t)r * NST + j] = __int_as_float(0x7fc00000);
+                if (LT == QCS_LOCTYPE_GS2D && cls) cls[r] = 0;
+            }
+        }
+        if (tid == 0) atomicExch(err, 1);
+    }
 }
 
 // FP32 master weights -> BF16 operand images (W1 | W2 | W3, N x K K-major).
@@ -702,6 +717,7 @@ struct qcs_learned_net {
     int R = 7;
     // GS2D networks: the two-emitter network whose start points the 2E stage uses, and its schedule
     qcs_learned_net *two = nullptr;
+    int owners = 0;  // GS2D networks this (two-emitter) network is attached to
     int two_iters = 3, two_bisections = 6, two_to3e = 1;
     float two_dev_th = 0.0f;
     int kin = 64;                     // input width: in_width(R)
@@ -923,6 +939,13 @@ int qcs_learned_param_count(void) { return L::param_count(L::in_width(7)); }
 
 int qcs_learned_destroy(qcs_learned_net *net) {
     if (!net) return QCS_OK;
+    // a two-emitter network still attached to a GS2D network is in use by it:
+    // refuse instead of leaving the owner with a dangling pointer
+    if (net->owners > 0)
+        return fail(QCS_ERR_STATE, "the network is attached to a GS2D network: detach it first "
+                                   "(qcs_learned_set_two_emitter(owner, NULL, ...)) or destroy the owner");
+    if (net->two) net->two->owners--;
+    net->two = nullptr;
     if (net->stream) cudaStreamSynchronize(net->stream);
     cudaFree(net->d_par);
     cudaFree(net->d_x);
@@ -1243,6 +1266,7 @@ int qcs_learned_set_two_emitter(qcs_learned_net *net, qcs_learned_net *two, int 
                                 float dev_th, int fallback) {
     if (!net) return fail(QCS_ERR_ARG, "null network");
     if (!two) {
+        if (net->two) net->two->owners--;
         net->two = nullptr;
         return QCS_OK;
     }
@@ -1255,6 +1279,10 @@ int qcs_learned_set_two_emitter(qcs_learned_net *net, qcs_learned_net *two, int 
     if (fallback != QCS_TWO_FALLBACK_3E && fallback != QCS_TWO_FALLBACK_PLAIN)
         return fail(QCS_ERR_ARG, "fallback: QCS_TWO_FALLBACK_3E or QCS_TWO_FALLBACK_PLAIN");
     net->two_to3e = fallback == QCS_TWO_FALLBACK_3E ? 1 : 0;
+    if (net->two != two) {
+        if (net->two) net->two->owners--;
+        two->owners++;
+    }
     net->two = two;
     net->two_iters = iters;
     net->two_bisections = bisections;

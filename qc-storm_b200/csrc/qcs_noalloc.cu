@@ -16,7 +16,10 @@
 //   * at most QCS_NOALLOC_MAX_ROIS records per call (larger n: QCS_ERR_CAPACITY);
 //   * the first call on a device looks up the array's device address
 //     (cudaGetSymbolAddress) with that device current; make that first call
-//     before any stream capture;
+//     before any stream capture.  The address is kept per device together with
+//     the CUDA context it was looked up in; after a device reset (a new
+//     primary context) the next call looks it up again, so that call must
+//     also come before any capture;
 //   * every call on a device shares the one array, which keeps the previous
 //     call's contents: calls that overlap on the GPU (different streams, no
 //     ordering between them) race on it and must not be issued;
@@ -26,6 +29,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <mutex>
+#include <cuda.h>  // CUcontext / CUresult types only; the entry point is fetched through the runtime
 #include <cuda_runtime.h>
 
 #include "../../include/qcstorm_b200.h"
@@ -49,6 +53,25 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 constexpr int kMaxDevices = 64;
 std::mutex g_mutex;
 void *g_scratch_addr[kMaxDevices] = {nullptr};
+CUcontext g_scratch_ctx[kMaxDevices] = {nullptr};  // context each address was looked up in
+
+// The calling thread's current CUDA context (the library links only the
+// runtime, so the driver's cuCtxGetCurrent is fetched through it once).
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
+bool current_context(CUcontext *ctx) {
+    static CtxGetCurrentFn fn = nullptr;
+    static bool looked_up = false;
+    if (!looked_up) {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<CtxGetCurrentFn>(f);
+        looked_up = true;
+    }
+    *ctx = nullptr;
+    return fn && fn(ctx) == CUDA_SUCCESS && *ctx;
+}
 
 // Status codes carry the error (QCS_ERR_*); the message is kept for debuggers.
 thread_local char g_msg[160];
@@ -71,17 +94,22 @@ extern "C" int qcs_localize_noalloc(const qcs_loc_para *p, const uint16_t *d_roi
     if (R < 5 || R > 17 || (R & 1) == 0 || (p->MultiEmitterFitEn && R > 13))
         return noalloc_fail(QCS_ERR_ROISIZE, "unsupported ROISize");
     if (p->LocType < QCS_LOCTYPE_GS2D || p->LocType > QCS_LOCTYPE_DH3D) return noalloc_fail(QCS_ERR_ARG, "LocType");
+    if (!(p->QE > 0.0f)) return noalloc_fail(QCS_ERR_ARG, "QE must be positive");
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
         return noalloc_fail(QCS_ERR_CUDA, "no current CUDA device");
     unsigned char *base = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_mutex);
-        if (!g_scratch_addr[dev]) {
+        CUcontext ctx = nullptr;
+        const bool have_ctx = current_context(&ctx);
+        if (!g_scratch_addr[dev] || (have_ctx && ctx != g_scratch_ctx[dev])) {
             void *ptr = nullptr;
             cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
             if (e != cudaSuccess || !ptr) return noalloc_fail(QCS_ERR_CUDA, "cudaGetSymbolAddress of the scratch array");
             g_scratch_addr[dev] = ptr;
+            if (!have_ctx) current_context(&ctx);  // cudaGetSymbolAddress made the primary context current
+            g_scratch_ctx[dev] = ctx;
         }
         base = static_cast<unsigned char *>(g_scratch_addr[dev]);
     }

@@ -483,9 +483,12 @@ class LearnedNet:
         self.loc_type, self.roi_size, self.n_params = lt.value, rs.value, npar.value
 
     def close(self):
+        """Frees the network.  A two-emitter network still attached to a GS2D
+        network is refused (QcsError, QCS_ERR_STATE) and stays usable."""
         if self.h:
-            self.lib.qcs_learned_destroy(self.h)
+            check(self.lib.qcs_learned_destroy(self.h))
             self.h = None
+            self._two = None
 
     def __del__(self):
         try:

@@ -68,3 +68,14 @@ def test_no_device_fails_loudly():
     h = C.c_void_p()
     assert L.qcs_loc_init(C.byref(p), C.byref(h)) == 4  # QCS_ERR_CUDA
     assert b"no CPU fallback" in L.qcs_last_error()
+
+
+def test_noalloc_argument_checks_before_device():
+    # the allocation-free entry point refuses bad arguments before touching a device
+    L = qlib.load()
+    p = abi.default_para()
+    args = (C.c_void_p(16), C.c_void_p(16))
+    assert L.qcs_localize_noalloc(C.byref(p), *args, 8193, C.c_void_p(16), None, None) == 3  # capacity
+    assert L.qcs_localize_noalloc(C.byref(p), *args, 16, C.c_void_p(20), None, None) == 1  # unaligned rows
+    p.QE = 0.0
+    assert L.qcs_localize_noalloc(C.byref(p), *args, 16, C.c_void_p(16), None, None) == 1  # QE

@@ -190,3 +190,25 @@ def test_trained_two_emitter_starts_keep_accuracy(cuda_ok):
     ctx.close()
     net.close()
     net2.close()
+
+
+def test_attached_two_emitter_network_outlives_owner(cuda_ok):
+    # a GS2D network keeps a pointer to its attached two-emitter network:
+    # destroying the attached network is refused until it is detached or its
+    # owner is gone
+    net = qlib.LearnedNet(batch=256, seed=1, roi_size=R)
+    two = qlib.LearnedNet(batch=256, seed=2, loc_type=qlib.LEARNED_GS2D_2E, roi_size=R)
+    net.set_two_emitter(two)
+    with pytest.raises(qlib.QcsError) as e:
+        two.close()
+    assert e.value.code == 6  # QCS_ERR_STATE
+    assert two.h  # still alive and usable
+    net.set_two_emitter(None)
+    two.close()
+    assert not two.h
+    two = qlib.LearnedNet(batch=256, seed=3, loc_type=qlib.LEARNED_GS2D_2E, roi_size=R)
+    net.set_two_emitter(two)
+    net.set_two_emitter(two)  # attaching twice counts once
+    net.close()  # destroying the owner detaches
+    two.close()
+    assert not two.h

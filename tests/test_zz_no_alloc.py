@@ -88,3 +88,12 @@ def test_noalloc_refuses_unaligned_rows(cuda_ok):
     code = qlib.load().qcs_localize_noalloc(C.byref(para), C.c_void_p(16), C.c_void_p(16), 16, C.c_void_p(16 + 4),
                                             None, None)
     assert code == 1  # QCS_ERR_ARG: rows are written 16 bytes at a time; rejected before any device work
+
+
+def test_noalloc_refuses_nonpositive_qe(cuda_ok):
+    _, para, _ = synth.gs2d_rois(16, R=7, seed=1)
+    for qe in (0.0, -0.5, float("nan")):
+        para.QE = qe
+        code = qlib.load().qcs_localize_noalloc(C.byref(para), C.c_void_p(16), C.c_void_p(16), 16, C.c_void_p(16),
+                                                None, None)
+        assert code == 1  # QCS_ERR_ARG before any device work: the CRLB divides by QE
