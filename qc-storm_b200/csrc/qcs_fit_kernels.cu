@@ -316,28 +316,80 @@ __device__ __forceinline__ void single_finish(const float *Ininf, const CorePara
     row[10] = 0.0f;
 }
 
-template <int R, int KIND, int DIST = ArithSpec<KIND, R>::DIST, int MASK = ArithSpec<KIND, R>::MASK>
-__global__ void __launch_bounds__(kTPB) fit_single_kernel(const uint16_t *__restrict__ rois,
-                                                          const float *__restrict__ wle, Queue q,
-                                                          float *__restrict__ loc, uint8_t *__restrict__ to2e,
-                                                          CorePara c) {
-    typedef SmemLayout<R, KIND> L;
+// Shared memory of fit_single_kernel: per slot (thread) the pixels' (value,
+// log) pairs, [pixel][slot], and the mask's unique values, [chunk][slot]
+// (MaskShape); the BFGS inverse Hessian lives in registers.  Blocks per SM:
+// as many as the shared memory holds (228 KB per SM, 1 KB reserved per
+// block), at most 7 (at 7 the register budget is 146 per thread).
+template <int R, bool FULL>
+struct SingleLayout {
+    enum {
+        PIX = R * R,
+        IMG = 0,                  // float2 per pixel and slot
+        WU = 2 * PIX * kTPB,      // floats; a multiple of 4 (16-byte aligned)
+        TOTAL = WU + MaskShape<R, FULL>::FLOATS * kTPB,
+        BYTES = TOTAL * 4,
+        FIT = (228 * 1024) / (BYTES + 1024),
+        BLOCKS = FIT < 1 ? 1 : (FIT > 7 ? 7 : FIT),
+    };
+};
+
+// Stage a block's records: pixel k of slot s at s_img[k * kTPB + s] as
+// (max((adu - offset) * gain, 1), its __logf).  WORDS: the records are
+// 4-byte aligned and read two pixels per load; element (word, slot) is taken
+// slot-fastest so a warp's shared-memory stores fall in distinct banks.
+template <int R, bool WORDS>
+__device__ __forceinline__ void stage_single(float2 *s_img, const uint16_t *rois, const Queue &q, int base, int cnt,
+                                             float Offset, float KAdc) {
+    enum { PIX = R * R, WHOLE = R * (R + 1), WPR = (PIX + 1) / 2 };
+    if (WORDS) {
+        for (int idx = threadIdx.x; idx < cnt * WPR; idx += kTPB) {
+            const int wd = idx / cnt;
+            const int slot = idx - wd * cnt;
+            const int id = queue_at(q, base + slot);
+            const uint32_t u = __ldg(reinterpret_cast<const uint32_t *>(rois + (size_t)id * WHOLE) + wd);
+            const int k = 2 * wd;
+            const float v0 = fmaxf(((float)(u & 0xFFFFu) - Offset) * KAdc, 1.0f);
+            s_img[k * kTPB + slot] = make_float2(v0, __logf(v0));
+            if (k + 1 < PIX) {
+                const float v1 = fmaxf(((float)(u >> 16) - Offset) * KAdc, 1.0f);
+                s_img[(k + 1) * kTPB + slot] = make_float2(v1, __logf(v1));
+            }
+        }
+    } else {
+        for (int idx = threadIdx.x; idx < cnt * PIX; idx += kTPB) {
+            const int k = idx / cnt;
+            const int slot = idx - k * cnt;
+            const int id = queue_at(q, base + slot);
+            const uint16_t u = __ldg(rois + (size_t)id * WHOLE + k);
+            const float pixval = fmaxf((u - Offset) * KAdc, 1.0f);
+            s_img[k * kTPB + slot] = make_float2(pixval, __logf(pixval));
+        }
+    }
+}
+
+template <int R, int KIND, bool WORDS, int DIST = ArithSpec<KIND, R>::DIST, int MASK = ArithSpec<KIND, R>::MASK,
+          bool FULL = MASK == kCompiler>
+__global__ void __launch_bounds__(kTPB, (SingleLayout<R, FULL>::BLOCKS)) fit_single_kernel(
+    const uint16_t *__restrict__ rois, const float *__restrict__ wle, Queue q, float *__restrict__ loc,
+    uint8_t *__restrict__ to2e, CorePara c) {
+    typedef SingleLayout<R, FULL> L;
     enum { P = KindTraits<KIND>::P, PIX = R * R, WHOLE = R * (R + 1) };
-    extern __shared__ float smem[];
+    extern __shared__ __align__(16) float smem[];
     const int n = queue_len(q);
     const int base = blockIdx.x * kTPB;
     if (base >= n) return;
     const int cnt = min(kTPB, n - base);
     float2 *s_img = reinterpret_cast<float2 *>(smem + L::IMG);
-    stage_rois<R>(s_img, rois, q, base, cnt, c.Offset, c.KAdc);
+    stage_single<R, WORDS>(s_img, rois, q, base, cnt, c.Offset, c.KAdc);
     __syncthreads();
     const int tid = threadIdx.x;
     if (tid >= cnt) return;
 
     const int CurFluoID = queue_at(q, base + tid);
     const PixView img{s_img + tid, kTPB};
-    float *w = smem + L::W + tid;
-    float *D = smem + L::D + tid;
+    // the mask: FULL, pixel k at mask[k * kTPB]; else float4 chunk j at ((float4 *)mask)[j * kTPB]
+    float *mask = smem + L::WU + (FULL ? tid : 4 * tid);
     const uint16_t *hdr = rois + (size_t)CurFluoID * WHOLE + PIX;
     const int XOffset = hdr[0];
     const int YOffset = hdr[1];
@@ -346,8 +398,13 @@ __global__ void __launch_bounds__(kTPB) fit_single_kernel(const uint16_t *__rest
 
     float Ininf[P];
     const SinglePrep sp = single_prefit<R, KIND>(img, pw, c, Ininf);
-    wle_weights<R, MASK>(w, kTPB, sp.WLE_SigmaX, sp.WLE_SigmaY, sp.MoleculeType);
-    mle_fit<R, KIND, DIST>(RoiRef{s_img + tid, w, kTPB}, Ininf, D, kTPB);
+    if constexpr (FULL)
+        wle_weights<R, MASK>(mask, kTPB, sp.WLE_SigmaX, sp.WLE_SigmaY, sp.MoleculeType);
+    else
+        wle_weights_unique<R, MASK>(reinterpret_cast<float4 *>(mask), kTPB, sp.WLE_SigmaX, sp.WLE_SigmaY,
+                                    sp.MoleculeType);
+    float D[P * P];  // the inverse Hessian, in registers
+    bfgs_fit<P, KindTraits<KIND>::IT>(StagedEval<R, KIND, DIST, FULL>{s_img + tid, mask, kTPB}, Ininf, D, 1);
     float row[12];
     bool accepted;
     float CurSNR;
@@ -955,8 +1012,10 @@ cudaError_t launch_learned_2e(const FitLaunch &a, const float *start, float dev_
 
 template <int R, int KIND>
 cudaError_t launch_single(const FitLaunch &a) {
-    const size_t smem = SmemLayout<R, KIND>::TOTAL * sizeof(float);
-    auto k = fit_single_kernel<R, KIND>;
+    const size_t smem = SingleLayout<R, ArithSpec<KIND, R>::MASK == kCompiler>::BYTES;
+    // two pixels per load when every record starts on a 4-byte boundary
+    auto k = (reinterpret_cast<uintptr_t>(a.rois) & 3) == 0 ? fit_single_kernel<R, KIND, true>
+                                                             : fit_single_kernel<R, KIND, false>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const int grid = (a.max_count + kTPB - 1) / kTPB;

@@ -51,9 +51,13 @@ struct RoiRef {
     int ld;
 };
 
-// Pixel rows are unrolled up to this ROI size (7x7 and 9x9 cover the
-// high-throughput single-emitter cases); the row loop stays rolled.
-constexpr int kUnrollMaxR = 9;
+// Pixel rows are unrolled up to this ROI size; the row loop stays rolled.
+// Without the unrolled row a thread's pixel terms form one dependent chain
+// (exp -> model -> log -> deviance -> sum) with nothing to overlap it, which
+// made 11x11 fits four times slower per pixel than 9x9 ones.  Up to 13 the
+// roundings of the loss are fixed in the source (ArithSpec), so unrolling
+// changes no result.
+constexpr int kUnrollMaxR = 13;
 
 // Contraction of a sum of two products a*b + c*d, the only operand shape
 // whose fused multiply-add nvcc chooses from the surrounding code (use
@@ -607,6 +611,223 @@ struct GroupEval {
             const float tp = __shfl_sync(mask, tot[(2 * k + 1) / G], (2 * k + 1) % G, G);
             grad[k] = (tp - tn) * 250.0f;
         }
+    }
+};
+
+// ------------------------------------------ staged single-emitter eval ---
+// The weighted-MLE mask of an R x R ROI depends on |col - R/2| and
+// |row - R/2| only: its exponent holds the squared distances of the pixel
+// centre from the ROI centre, which are equal (exact small numbers) for
+// mirrored pixels.  A thread therefore keeps U x U values (U = R/2 + 1);
+// mask row ur is C4 float4 chunks, value (ur, uc) in chunk uc / 4, lane uc % 4.
+// That holds where the mask's contraction is fixed in the source (MASK !=
+// kCompiler).  Where nvcc chooses it, its choice differs between pixels (and
+// with the surrounding code), so mirrored pixels need not agree bit for bit:
+// there (FULL) the whole R x R mask of wle_weights is kept, pixel k at
+// k * ld floats, which reproduces the reference's values.
+template <int R, bool FULL = false>
+struct MaskShape {
+    enum { U = R / 2 + 1, C4 = (U + 3) / 4, FLOATS = FULL ? R * R : U * C4 * 4 };
+};
+
+__host__ __device__ constexpr int mirror_index(int k, int R) { return k < R / 2 ? R / 2 - k : k - R / 2; }
+
+// wle_weights for the pixels col, row >= R/2 (same expressions, so the same
+// values as at their mirror images), chunk c of mask row ur at wu[(ur * C4 + c) * ld].
+template <int R, int MASK = kCompiler>
+__device__ __forceinline__ void wle_weights_unique(float4 *wu, int ld, float WLE_SigmaX, float WLE_SigmaY,
+                                                   int MoleculeType) {
+    typedef MaskShape<R> M;
+    const float ROICenter = R / 2.0f;
+    const float WLE_SigmaX1 = 1.0f / (2.0f * WLE_SigmaX * WLE_SigmaX);
+    const float WLE_SigmaY1 = 1.0f / (2.0f * WLE_SigmaY * WLE_SigmaY);
+    for (int ur = 0; ur < M::U; ur++) {
+        const float rowpos = (R / 2 + ur) + 0.5f;
+        for (int c = 0; c < M::C4; c++) {
+            float v[4];
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const int uc = c * 4 + j;
+                const float colpos = (R / 2 + uc) + 0.5f;
+                if (MoleculeType == 0 || uc >= M::U)
+                    v[j] = 1.0f;
+                else
+                    v[j] = __expf(-sum_of_products<MASK>((colpos - ROICenter) * (colpos - ROICenter), WLE_SigmaX1,
+                                                         (rowpos - ROICenter) * (rowpos - ROICenter), WLE_SigmaY1));
+            }
+            wu[(ur * M::C4 + c) * ld] = make_float4(v[0], v[1], v[2], v[3]);
+        }
+    }
+}
+
+// Model exponential of single_expo from the pixel's offsets dx = col + 0.5 - x
+// and dy = row + 0.5 - y (the same roundings).
+template <int KIND, int DIST>
+__device__ __forceinline__ float single_expo_d(float dx, float dy, const float *v) {
+    if (KIND == kGS2D) return __expf(-(sum_of_products<DIST>(dx, dx, dy, dy)) * v[3] * QCS_SSCALE);
+    return __expf(-(sum_of_products<DIST>(dx * dx * v[3], QCS_SSCALE, dy * dy * v[4], QCS_SSCALE)));
+}
+
+// Loss and gradient of one single-emitter ROI (GS2D / AS3D) evaluated by its
+// own thread, with the pixels' (value, log) pairs at img[k * ld] and the
+// mask's unique values (MaskShape) at wu[(ur * C4 + c) * ld].  Same terms,
+// same order, same roundings as loss() / numerical_gradient_shared(), with
+// fewer instructions: one 16-byte mask load per row, the column offsets of
+// the position computed once per evaluation, the row centre kept as a float.
+template <int R, int KIND, int DIST, bool FULL = false>
+struct StagedEval {
+    typedef KindTraits<KIND> T;
+    typedef MaskShape<R> M;
+    enum { P = T::P, UNROLL = R <= kUnrollMaxR };
+    const float2 *img;
+    // the mask: unique values as float4 chunks at ((const float4 *)mask)[(ur * C4 + c) * ld] (16-byte
+    // aligned), or (FULL) the R x R values, pixel k at mask[k * ld]
+    const float *mask;
+    int ld;
+
+    // the mask values of `row`, indexed by mirror_index(col) (FULL: by col)
+    __device__ __forceinline__ void mask_row(int row, float (&w)[FULL ? R : M::C4 * 4]) const {
+        if constexpr (FULL) {
+#pragma unroll
+            for (int c = 0; c < R; c++) w[c] = mask[(row * R + c) * ld];
+        } else {
+            const int ur = mirror_index(row, R);
+            const float4 *wu = reinterpret_cast<const float4 *>(mask);
+#pragma unroll
+            for (int c = 0; c < M::C4; c++) {
+                const float4 q = wu[(ur * M::C4 + c) * ld];
+                w[4 * c] = q.x;
+                w[4 * c + 1] = q.y;
+                w[4 * c + 2] = q.z;
+                w[4 * c + 3] = q.w;
+            }
+        }
+    }
+    __device__ __forceinline__ static constexpr int wcol(int col) { return FULL ? col : mirror_index(col, R); }
+    __device__ __forceinline__ float mask_at(int row, int col) const {
+        if constexpr (FULL) return mask[(row * R + col) * ld];
+        const int ur = mirror_index(row, R), uc = mirror_index(col, R);
+        return mask[((ur * M::C4 + uc / 4) * ld) * 4 + uc % 4];
+    }
+
+    __device__ __forceinline__ float loss(float *Ininf) const {
+#pragma unroll
+        for (int k = 0; k < P; k++) {
+            if (T::CLAMP001) {
+                if (Ininf[k] < 0.01f) Ininf[k] = 0.01f;
+            } else {
+                if (Ininf[k] < 0.0f) Ininf[k] = 0.0f;
+            }
+        }
+        float TotalLoss = 0;
+        if constexpr (UNROLL) {
+            float dxs[R];
+#pragma unroll
+            for (int col = 0; col < R; col++) dxs[col] = (col + 0.5f) - Ininf[1];
+            float rowpos = 0.5f;
+            const float2 *pr = img;
+#pragma unroll 1
+            for (int row = 0; row < R; row++) {
+                float w[FULL ? R : M::C4 * 4];
+                mask_row(row, w);
+                const float dy = rowpos - Ininf[2];
+#pragma unroll
+                for (int col = 0; col < R; col++) {
+                    const float2 pl = pr[col * ld];
+                    const float Lt = single_term<KIND>(single_expo_d<KIND, DIST>(dxs[col], dy, Ininf), Ininf, pl.x,
+                                                       pl.y);
+                    TotalLoss = __fmaf_rn(w[wcol(col)], Lt, TotalLoss);
+                }
+                rowpos += 1.0f;
+                pr += R * ld;
+            }
+        } else {
+#pragma unroll 1
+            for (int row = 0; row < R; row++) {
+#pragma unroll 1
+                for (int col = 0; col < R; col++) {
+                    const float2 pl = img[(row * R + col) * ld];
+                    const float Lt = single_term<KIND>(
+                        single_expo<KIND, DIST>(col + 0.5f, row + 0.5f, Ininf), Ininf, pl.x, pl.y);
+                    TotalLoss = __fmaf_rn(mask_at(row, col), Lt, TotalLoss);
+                }
+            }
+        }
+        return TotalLoss;
+    }
+
+    // numerical_gradient_shared with this layout (and its point-by-point
+    // fallback through loss()).
+    __device__ __forceinline__ void gradient(const float *Ininf, float *grad) const {
+        enum { NE = 2 * P };
+        float v[NE][P];
+        {
+            float t[P];
+#pragma unroll
+            for (int k = 0; k < P; k++) t[k] = Ininf[k];
+#pragma unroll
+            for (int k = 0; k < P; k++) {
+                t[k] = t[k] - 0.002f;
+#pragma unroll
+                for (int c = 0; c < P; c++) {
+                    if (T::CLAMP001) { if (t[c] < 0.01f) t[c] = 0.01f; } else { if (t[c] < 0.0f) t[c] = 0.0f; }
+                    v[2 * k][c] = t[c];
+                }
+                t[k] = t[k] + 0.004f;
+#pragma unroll
+                for (int c = 0; c < P; c++) {
+                    if (T::CLAMP001) { if (t[c] < 0.01f) t[c] = 0.01f; } else { if (t[c] < 0.0f) t[c] = 0.0f; }
+                    v[2 * k + 1][c] = t[c];
+                }
+                t[k] = t[k] - 0.002f;
+            }
+        }
+        bool share = true;
+#pragma unroll
+        for (int c = 1; c < P - 1; c++) {
+            const unsigned b = __float_as_uint(v[0][c]);
+            share = share && (__float_as_uint(v[1][c]) == b) && (__float_as_uint(v[NE - 2][c]) == b) &&
+                    (__float_as_uint(v[NE - 1][c]) == b);
+        }
+        if (!__all_sync(__activemask(), share)) {
+            float tI[P];
+#pragma unroll
+            for (int c = 0; c < P; c++) tI[c] = Ininf[c];
+            for (int k = 0; k < P; k++) {
+                tI[k] = tI[k] - 0.002f;
+                const float tn = loss(tI);
+                tI[k] = tI[k] + 0.004f;
+                const float tp = loss(tI);
+                grad[k] = (tp - tn) * 250.0f;
+                tI[k] = tI[k] - 0.002f;
+            }
+            return;
+        }
+        float tot[NE];
+#pragma unroll
+        for (int j = 0; j < NE; j++) tot[j] = 0;
+        float rowpos = 0.5f;
+#pragma unroll 1
+        for (int row = 0; row < R; row++) {
+            float w[FULL ? R : M::C4 * 4];
+            if constexpr (UNROLL) mask_row(row, w);
+#pragma unroll(UNROLL ? R : 1)
+            for (int col = 0; col < R; col++) {
+                const float2 pl = img[(row * R + col) * ld];
+                const float wk = UNROLL ? w[wcol(col)] : mask_at(row, col);
+                const float colpos = col + 0.5f;
+                const float e_base = single_expo<KIND, DIST>(colpos, rowpos, v[0]);
+#pragma unroll
+                for (int j = 0; j < NE; j++) {
+                    const bool base = (j < 2) || (j >= NE - 2);
+                    const float e = base ? e_base : single_expo<KIND, DIST>(colpos, rowpos, v[j]);
+                    tot[j] = __fmaf_rn(wk, single_term<KIND>(e, v[j], pl.x, pl.y), tot[j]);
+                }
+            }
+            rowpos += 1.0f;
+        }
+#pragma unroll
+        for (int k = 0; k < P; k++) grad[k] = (tot[2 * k + 1] - tot[2 * k]) * 250.0f;
     }
 };
 
