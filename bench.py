@@ -527,6 +527,7 @@ def learned_measure(args, streams, ctxs, para, d_batches, h_batches, rec0, truth
     the fits the deviance judge rejects + CRLB (qcs_learned_localize_device),
     on the same device-resident batches as the plain step, WLE pre-pass
     included; accuracy of plain vs learned on batch 0 against ground truth."""
+    from qcstorm_b200 import lib
     stream, ctx = streams[0], ctxs[0]
     sh = stream.cuda_stream
     net, train = train_learned_net(para, stream)
@@ -554,6 +555,19 @@ def learned_measure(args, streams, ctxs, para, d_batches, h_batches, rec0, truth
     # each arm over its own accepted records (learned accepts more)
     rp_own, pp_own, crlb_p_own = fit_accuracy(plain, rec0, truth0, acc_p, para)
     rl_own, pl_own, crlb_l_own = fit_accuracy(learned, rec0, truth0, acc_l, para)
+    # the FP64 Fisher-matrix bound of each arm's own rows (emitters at their fitted positions)
+    fisher = {}
+    for name, rows in (("plain", plain), ("learned", learned)):
+        f = lib.crlb_fisher(para, rows[:N_PER_STEP], rec0)
+        sel = (rows[:N_PER_STEP, 0] > 0) & (f[:, 7] == 0)
+        rmse, _, _ = fit_accuracy(rows, rec0, truth0, sel, para)
+        bound = float(np.sqrt(np.mean((f[sel, 0] ** 2 + f[sel, 1] ** 2) / 2)) / para.PixelSize)
+        fisher[name] = {"rmse_px": rmse, "crlb_px": bound, "rmse_over_crlb": rmse / bound, "rows": int(sel.sum())}
+    fisher["learned_minus_plain_rmse_over_crlb"] = (fisher["learned"]["rmse_px"] - fisher["plain"]["rmse_px"]) / \
+        fisher["plain"]["crlb_px"]
+    fisher["equal_rmse_within_2pct_of_crlb"] = bool(fisher["learned_minus_plain_rmse_over_crlb"] <= 0.02)
+    fisher["basis"] = ("each arm's accepted rows; CRLB = qcs_crlb_fisher_fp64 (full Fisher matrix of the fitted "
+                       "model on the ROI's pixels, FP64), per axis")
 
     # end to end: pinned host records in, rows out, through qcs_learned_localize_async
     e2e_pipelined(ctxs, streams, h_batches, 4, net=net)
@@ -579,6 +593,7 @@ def learned_measure(args, streams, ctxs, para, d_batches, h_batches, rec0, truth
                                                    "learned": float((learned[:, 0] > 0).mean())},
                      "equal_rmse": bool(rl <= 1.02 * rp),
                      "basis": "records accepted by both; ground truth of the generator",
+                     "fisher_crlb": fisher,
                      "own_accepted": {"rmse_px": {"plain": rp_own, "learned": rl_own},
                                       "photon_rel_rmse": {"plain": pp_own, "learned": pl_own},
                                       "crlb_px": {"plain": crlb_p_own, "learned": crlb_l_own},
@@ -1351,12 +1366,18 @@ def main():
                 "plain_rmse_px_own": a["own_accepted"]["rmse_px"]["plain"],
                 "learned_accept": a["accepted"]["learned"], "plain_accept": a["accepted"]["plain"],
                 "learned_equal_rmse": a["equal_rmse"], "crlb_px": a["crlb_px"],
+                "fisher_crlb_px": a["fisher_crlb"]["plain"]["crlb_px"],
+                "plain_rmse_over_fisher_crlb": a["fisher_crlb"]["plain"]["rmse_over_crlb"],
+                "learned_rmse_over_fisher_crlb": a["fisher_crlb"]["learned"]["rmse_over_crlb"],
+                "learned_equal_rmse_within_2pct_of_crlb": a["fisher_crlb"]["equal_rmse_within_2pct_of_crlb"],
             })
         # short keys first: the headline survives a truncated tail of the line
         head = ["metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
                 "vs_baseline", "dtype", "data", "learned_value", "learned_vs_plain", "learned_e2e_value",
                 "learned_rmse_px", "plain_rmse_px", "learned_rmse_px_own", "plain_rmse_px_own", "learned_accept",
-                "plain_accept", "learned_equal_rmse", "crlb_px", "gpu_launches", "windows", "clocks", "roofline",
+                "plain_accept", "learned_equal_rmse", "crlb_px", "fisher_crlb_px", "plain_rmse_over_fisher_crlb",
+                "learned_rmse_over_fisher_crlb", "learned_equal_rmse_within_2pct_of_crlb", "gpu_launches", "windows",
+                "clocks", "roofline",
                 "e2e", "cpu_baseline", "config"]
         line = {**{k: line[k] for k in head if k in line}, **{k: v for k, v in line.items() if k not in head}}
         print(json.dumps(line), flush=True)

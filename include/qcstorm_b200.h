@@ -691,6 +691,43 @@ long long qcs_locfile_rows(const qcs_locfile *f);
 /* Waits for queued appends and closes; reports a failed write. */
 int qcs_locfile_close(qcs_locfile *f);
 
+/* ---- FP64 Fisher-matrix CRLB side output --------------------------------- */
+/*
+ * No counterpart in the reference, whose CRLB columns (9, 10) hold a diagonal
+ * x / y estimate (LocPrecCalc_GaussianCRLB.h:65-243: Fisher information of
+ * x alone from numerical second derivatives on a fixed grid, emitter at its
+ * centre); those columns are left as they are.  This bound uses the full
+ * Fisher information of the fitted single-emitter model on the ROI's R x R
+ * pixel centres: mu = N / (2 pi sx sy) exp(-dx^2/(2 sx^2) - dy^2/(2 sy^2)) + B
+ * in photoelectrons, parameters x, y, N, B and sigma (GS2D, DH3D) or sigma_x,
+ * sigma_y (AS3D), Poisson noise with read noise as extra variance
+ * (I_ij = sum dmu_i dmu_j / (mu + ReadNoise_e^2)), built and inverted
+ * (Cholesky) in FP64 on the GPU.  For n device rows (12 floats, as the
+ * localization writes them; rows with column 0 <= 0 are skipped) writes
+ * n x QCS_FISHER_COLS floats to d_out: the square roots of the inverse's
+ * diagonal (x, y in nm; photons and background in photons, i.e. divided by
+ * QE; widths in pixels; z in nm through the calibration polynomial's
+ * Jacobian, AS3D only) and a status.  d_rois (may be NULL): the first n_rois
+ * rows are the single-emitter rows of those records (row i from record i),
+ * which places the emitter at its fitted position in its ROI; other rows put
+ * it at the ROI centre, as the reference's estimate does.  Asynchronous on
+ * `stream`; allocates nothing.
+ */
+#define QCS_FISHER_COLS 8
+#define QCS_FISHER_X 0          /* nm */
+#define QCS_FISHER_Y 1          /* nm */
+#define QCS_FISHER_Z 2          /* nm, AS3D (0 otherwise) */
+#define QCS_FISHER_PHOTONS 3    /* total photons */
+#define QCS_FISHER_BACKGROUND 4 /* photons per pixel */
+#define QCS_FISHER_SIGMA_X 5    /* pixels */
+#define QCS_FISHER_SIGMA_Y 6    /* pixels */
+#define QCS_FISHER_STATUS 7     /* QCS_FISHER_OK / _INVALID / _SINGULAR */
+#define QCS_FISHER_OK 0
+#define QCS_FISHER_INVALID 1    /* rejected row, or photons / widths out of range */
+#define QCS_FISHER_SINGULAR 2   /* Fisher matrix not positive definite */
+int qcs_crlb_fisher_fp64(const qcs_loc_para *p, const float *d_rows, int n, const uint16_t *d_rois, int n_rois,
+                         float *d_out, void *stream);
+
 /* ---- allocation-free localization --------------------------------------- */
 /*
  * No counterpart in the reference.  For callers that cannot allocate device

@@ -45,6 +45,11 @@ int qcso_fit_single_f64(int kind, const qcs_loc_para *p, const uint16_t *rois, c
 /* CRLB columns 9/10 over n rows, in place. */
 int qcso_crlb(const qcs_loc_para *p, float *loc, int n);
 
+/* FP64 Fisher-matrix CRLB side output of n rows (qcs_crlb_fisher_fp64):
+ * out n x QCS_FISHER_COLS; rois / n_rois as in the product's entry point. */
+int qcso_crlb_fisher_f64(const qcs_loc_para *p, const float *rows, int n, const uint16_t *rois, int n_rois,
+                         float *out);
+
 /* ROI extraction over n_frames frames fed in batches of `batch` frames, as
  * consecutive ExtractMolecules calls; rois_out cap x R(R+1), wle_out cap x 6.
  * flags selects the arithmetic of the two steps whose rounding depends on how

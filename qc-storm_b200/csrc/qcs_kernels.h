@@ -90,4 +90,10 @@ cudaError_t launch_wle(const uint16_t *rois, int n, int R, int loc_type, float *
 cudaError_t launch_wle_presorted(const uint16_t *rois, const unsigned long long *keys, const int *d_span, int max_n,
                                  int R, int loc_type, float *wle, cudaStream_t s);
 
+// FP64 Fisher-matrix CRLB of localization rows (qcs_crlb_fisher_fp64): n
+// rows, or min(*n_dev, n) when n_dev is set; rois: the records of the first
+// n_rois rows (may be null); out: n x QCS_FISHER_COLS floats.
+cudaError_t launch_crlb_fisher(const qcs_loc_para &p, const float *rows, int n, const int *n_dev,
+                               const uint16_t *rois, int n_rois, float *out, cudaStream_t s);
+
 }  // namespace qcs

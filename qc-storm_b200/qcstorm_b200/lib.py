@@ -41,6 +41,8 @@ _SIGS = {
     "qcs_fit_single_device": (C.c_int, [C.c_int, C.POINTER(LocPara), C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
                                         C.c_void_p]),
     "qcs_crlb_device": (C.c_int, [C.POINTER(LocPara), C.c_void_p, C.c_int, C.c_void_p]),
+    "qcs_crlb_fisher_fp64": (C.c_int, [C.POINTER(LocPara), C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
+                                       C.c_void_p]),
     "qcs_fit_single_group_device": (C.c_int, [C.c_int, C.POINTER(LocPara), C.c_void_p, C.c_void_p, C.c_int,
                                               C.c_void_p, C.c_int, C.c_void_p]),
     "qcs_measure_mufu_rate": (C.c_int, [C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_double)]),
@@ -330,6 +332,36 @@ def fit_single_group_device(loc_type, para, d_rois, d_wle, n, d_loc, lanes=8, st
 
 def crlb_device(para, d_loc, n, stream=0):
     check(load().qcs_crlb_device(C.byref(para), C.c_void_p(d_loc), int(n), C.c_void_p(stream) if stream else None))
+
+
+FISHER_COLS = 8  # x nm, y nm, z nm, photons, background, sigma_x px, sigma_y px, status
+FISHER_NAMES = ["x_nm", "y_nm", "z_nm", "photons", "background", "sigma_x_px", "sigma_y_px", "status"]
+
+
+def crlb_fisher_device(para, d_rows, n, d_out, d_rois=0, n_rois=0, stream=0):
+    """qcs_crlb_fisher_fp64: the FP64 Fisher-matrix CRLB of n device rows into
+    d_out (n x FISHER_COLS floats); d_rois / n_rois place the first n_rois
+    rows' emitters at their fitted positions in their records."""
+    check(load().qcs_crlb_fisher_fp64(C.byref(para), C.c_void_p(d_rows), int(n),
+                                      C.c_void_p(d_rois) if d_rois else None, int(n_rois), C.c_void_p(d_out),
+                                      C.c_void_p(stream) if stream else None))
+
+
+def crlb_fisher(para, rows, rois=None):
+    """The same from host rows (and records), through device copies."""
+    import torch
+    rows = np.ascontiguousarray(rows, np.float32)
+    n = rows.shape[0]
+    d_rows = torch.from_numpy(rows).cuda()
+    d_out = torch.zeros((max(n, 1), FISHER_COLS), dtype=torch.float32, device="cuda")
+    d_rois = None
+    if rois is not None:
+        d_rois = torch.from_numpy(np.ascontiguousarray(rois, np.uint16).view(np.int16)).cuda()
+    s = torch.cuda.current_stream()
+    crlb_fisher_device(para, d_rows.data_ptr(), n, d_out.data_ptr(), d_rois.data_ptr() if d_rois is not None else 0,
+                       rois.shape[0] if rois is not None else 0, s.cuda_stream)
+    s.synchronize()
+    return d_out.cpu().numpy()[:n]
 
 
 def mufu_rate(iters=4000):

@@ -78,6 +78,21 @@ def crlb(para, loc, lib="oracle"):
     return out
 
 
+FISHER_COLS = 8
+
+
+def crlb_fisher(para, rows, rois=None):
+    """The FP64 Fisher-matrix CRLB oracle (qcso_crlb_fisher_f64): n x 8."""
+    rows = np.ascontiguousarray(rows, np.float32)
+    n = rows.shape[0]
+    out = np.zeros((max(n, 1), FISHER_COLS), np.float32)
+    r = np.ascontiguousarray(rois, np.uint16) if rois is not None else None
+    st = oracle().qcso_crlb_fisher_f64(C.byref(para), _p(rows), n, _p(r), r.shape[0] if r is not None else 0,
+                                       _p(out))
+    assert st == 0, st
+    return out[:n]
+
+
 EXTRACT_FMA_CONV = 1
 EXTRACT_EXACT_VARIANCE = 2
 
