@@ -226,6 +226,99 @@ def cpu_reference_rate(steps=1, per_thread=6000, threads=None):
                 per_thread, threads)}, rates
 
 
+# loss evaluations of the reference's fixed schedules (2P initial gradient, IT iterations of 12 line-search
+# evaluations, IT - 1 more gradients) and MUFU operations per pixel-evaluation (exps of the model + its log)
+SCHEDULE_EVALS = {"gs2d": 176, "as3d": 264, "2e": 364, "3e": 544}
+MUFU_PER_EVAL = {"gs2d": 2, "as3d": 2, "2e": 3, "3e": 4}
+
+
+def cascade_mufu_ops(R, single, n2=0, n3=0, single_kind="gs2d"):
+    """MUFU operations the fits of one localization call execute on the
+    reference schedule: queue lengths of the single-emitter, 2E and 3E stages."""
+    px = R * R
+    return px * (single * SCHEDULE_EVALS[single_kind] * MUFU_PER_EVAL[single_kind] +
+                 n2 * SCHEDULE_EVALS["2e"] * MUFU_PER_EVAL["2e"] + n3 * SCHEDULE_EVALS["3e"] * MUFU_PER_EVAL["3e"])
+
+
+def threaded_cpu_rate(make_sample, work, threads=None):
+    """Units per second of work(sample) run on one prepared sample per host
+    thread (ctypes releases the GIL, so the threads run in parallel)."""
+    threads = threads or os.cpu_count() or 1
+    samples = [make_sample(t) for t in range(threads)]
+    done = [0] * threads
+
+    def run(i):
+        done[i] = work(samples[i])
+
+    t0 = time.perf_counter()
+    ths = [threading.Thread(target=run, args=(i,)) for i in range(threads)]
+    for th in ths:
+        th.start()
+    for th in ths:
+        th.join()
+    return sum(done) / (time.perf_counter() - t0), threads
+
+
+def shape_cpu_baseline(kind, R, per_thread):
+    """The reference's code compiled for the host (oracle/_ref) on every host
+    core over a bounded sample of the workload: WLE + fit (+ cascade) + CRLB.
+    AS3D 9x9 runs the reference's 9x9 kernel directly (its own dispatcher
+    would run the 8x8 one)."""
+    import oracle_lib as O
+    from qcstorm_b200 import synth
+    if O.ref_host() is None:
+        return None
+    gen = synth.as3d_rois if kind == "as3d" else synth.multi_rois
+
+    def make(t):
+        rec, para, _ = gen(per_thread, R=R, seed=9500 + t)
+        return rec, para
+
+    def work(sample):
+        rec, para = sample
+        w = O.wle(para, rec, "ref")
+        if kind == "as3d":
+            O.crlb(para, O.fit_single(1, para, rec, w, lib="ref"), lib="ref")
+        else:
+            O.localize(para, rec, w, lib="ref")
+        return rec.shape[0]
+
+    rate, threads = threaded_cpu_rate(make, work)
+    return {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": "%d %s %dx%d records per host thread x %d threads (WLE + fit%s + CRLB)" % (
+                per_thread, kind, R, R, threads, "" if kind == "as3d" else " cascade")}
+
+
+def frame_cpu_baseline(frames_per_thread=1):
+    """frames/s of the frame pipeline on every host core, one frame per
+    thread: ROI extraction by the oracle port (bit-pinned to the reference's
+    host build, which runs its CUDA extraction kernels through a SIMT emulator
+    at ~26 s per 2048 x 2048 frame and would misstate a CPU's speed), then the
+    reference's host build for WLE + localization cascade + CRLB."""
+    import oracle_lib as O
+    from qcstorm_b200 import synth
+    if O.ref_host() is None:
+        return None
+    O.set_threads(1)
+
+    def make(t):
+        fr, para, _ = synth.frames(frames_per_thread, width=FRAME_W, height=FRAME_H, density=3000, seed=9700 + t)
+        para.MultiEmitterFitEn = 1
+        return fr, para
+
+    def work(sample):
+        fr, para = sample
+        rois, _, _, _ = O.extract(para, fr, 1, lib="oracle")
+        O.localize(para, rois, O.wle(para, rois, "ref"), lib="ref")
+        return fr.shape[0]
+
+    rate, threads = threaded_cpu_rate(make, work)
+    O.set_threads(0)
+    return {"value": rate, "unit": "frames/s", "cores": threads, "kind": "port+reference",
+            "sample": "%d 2048x2048 frame(s) per host thread x %d threads: extraction by the oracle port, WLE + "
+                      "localization cascade + CRLB by the reference's host build" % (frames_per_thread, threads)}
+
+
 def run_reference_arm(args, rank):
     if rank != 0:
         return 0
@@ -423,6 +516,8 @@ def frame_pipeline(stream, steps, warmup, e2e=True, dist=None, world=1, net=None
         "frames_per_s": world * FRAMES_PER_CALL * 1e3 / ms, "ms_per_call": ms, "frames_per_call": FRAMES_PER_CALL,
         "records_per_call": recs0, "rows_per_call": int(rows0.shape[0]),
         "single_emitter_fits_per_call": int(round(float(ratios0[0]) * recs0)),
+        "stages": {"single": int(round(float(ratios0[0]) * recs0)), "two_emitter": int(round(float(ratios0[1]) * recs0)),
+                   "three_emitter": int(round(float(ratios0[2]) * recs0))},
         "graph": {"frames_per_s": world * FRAMES_PER_CALL * 1e3 / ms_graph, "ms_per_call": ms_graph,
                   "note": "one call (reset, %d extractions, localization) captured in a CUDA graph and replayed"
                           % FRAMES_PER_CALL},
@@ -562,12 +657,20 @@ def learned_measure(args, streams, ctxs, para, d_batches, h_batches, rec0, truth
         sel = (rows[:N_PER_STEP, 0] > 0) & (f[:, 7] == 0)
         rmse, _, _ = fit_accuracy(rows, rec0, truth0, sel, para)
         bound = float(np.sqrt(np.mean((f[sel, 0] ** 2 + f[sel, 1] ** 2) / 2)) / para.PixelSize)
-        fisher[name] = {"rmse_px": rmse, "crlb_px": bound, "rmse_over_crlb": rmse / bound, "rows": int(sel.sum())}
+        # each record's error over its own bound: arms that accept different records compare fairly
+        ex = rows[sel, 1] + R // 2 - rec0[sel, R * R].astype(np.float64) - truth0["x"][sel]
+        ey = rows[sel, 2] + R // 2 - rec0[sel, R * R + 1].astype(np.float64) - truth0["y"][sel]
+        norm = float(np.sqrt(np.mean(((ex / f[sel, 0]) ** 2 + (ey / f[sel, 1]) ** 2) / 2) * para.PixelSize ** 2))
+        fisher[name] = {"rmse_px": rmse, "crlb_px": bound, "rmse_over_crlb": rmse / bound,
+                        "rms_error_over_own_crlb": norm, "rows": int(sel.sum())}
     fisher["learned_minus_plain_rmse_over_crlb"] = (fisher["learned"]["rmse_px"] - fisher["plain"]["rmse_px"]) / \
         fisher["plain"]["crlb_px"]
-    fisher["equal_rmse_within_2pct_of_crlb"] = bool(fisher["learned_minus_plain_rmse_over_crlb"] <= 0.02)
+    fisher["equal_rmse_within_2pct_of_crlb"] = bool(
+        fisher["learned"]["rms_error_over_own_crlb"] <= 1.02 * fisher["plain"]["rms_error_over_own_crlb"])
     fisher["basis"] = ("each arm's accepted rows; CRLB = qcs_crlb_fisher_fp64 (full Fisher matrix of the fitted "
-                       "model on the ROI's pixels, FP64), per axis")
+                       "model on the ROI's pixels, FP64), per axis; rms_error_over_own_crlb = sqrt(mean((error / "
+                       "that record's bound)^2)), the criterion of equal_rmse_within_2pct_of_crlb (learned accepts "
+                       "more, harder records, which raise its plain RMSE over its own accepted set)")
 
     # end to end: pinned host records in, rows out, through qcs_learned_localize_async
     e2e_pipelined(ctxs, streams, h_batches, 4, net=net)
@@ -659,7 +762,7 @@ def train_two_emitter_net(ctx_tr, para, d_tr, feat, scale, n, R, epochs, stream)
     return net2
 
 
-def learned_shapes_measure(streams, dist, world, rank):
+def learned_shapes_measure(streams, dist, world, rank, mufu_peak=None, cpu_baseline=True):
     """The learned path on the other configurations' generators, each against
     plain fitting of the same device-resident records with two contexts in
     turn: astigmatic 3D 9x9 ROIs (single-emitter fits from sigma_x / sigma_y
@@ -717,6 +820,42 @@ def learned_shapes_measure(streams, dist, world, rank):
         ms_l = device_timed(SHAPE_STEPS, 3, learned, streams, dist)
         plain(0, s0, ctxs[0])
         rows_p, ratios_p = ctxs[0].read_rows(sh)
+        # roofline of the plain call: MUFU operations of its fits (reference schedule) over its time, and
+        # its single-emitter stage's kernel alone (the dominant kernel) on the same records
+        roof = None
+        if mufu_peak:
+            n = SHAPE_RECORDS
+            single = int(round(float(ratios_p[0]) * n))
+            n2, n3 = int(round(float(ratios_p[1]) * n)), int(round(float(ratios_p[2]) * n))
+            ops = cascade_mufu_ops(R, single, n2, n3, single_kind="as3d" if kind == "as3d" else "gs2d")
+            call_ms = ms_p / SHAPE_STEPS
+            wle_b = torch.empty((n, 6), dtype=torch.float32, device="cuda")
+            lib.check(lib.load().qcs_wle_estimate_device(ctxs[0].h, C.c_void_p(d_b[0].data_ptr()), n, C.byref(para),
+                                                         C.c_void_p(wle_b.data_ptr()), C.c_void_p(sh)))
+            d_loc = torch.empty((n, 12), dtype=torch.float32, device="cuda")
+            for _ in range(2):
+                lib.fit_single_device(para.LocType, para, d_b[0].data_ptr(), wle_b.data_ptr(), n, d_loc.data_ptr(), sh)
+            kt = []
+            for _ in range(10):
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(s0)
+                lib.fit_single_device(para.LocType, para, d_b[0].data_ptr(), wle_b.data_ptr(), n, d_loc.data_ptr(),
+                                      sh)
+                b.record(s0)
+                kt.append((a, b))
+            torch.cuda.synchronize()
+            k_ms = statistics.mean(a.elapsed_time(b) for a, b in kt)
+            k_ops = cascade_mufu_ops(R, n, single_kind="as3d" if kind == "as3d" else "gs2d")
+            roof = {"bound": "sfu", "unit": "MUFU op/s", "peak": mufu_peak,
+                    "call": {"achieved": ops / (call_ms * 1e-3), "frac": ops / (call_ms * 1e-3) / mufu_peak,
+                             "ms": call_ms, "stages": {"single": single, "two_emitter": n2, "three_emitter": n3},
+                             "scope": "whole plain call (WLE + fit cascade + CRLB), two contexts in turn; fits counted "
+                                      "on the reference schedule"},
+                    "kernel": {"name": "fit_single_kernel<%d,%s>" % (R, "AS3D" if kind == "as3d" else "GS2D"),
+                               "achieved": k_ops / (k_ms * 1e-3), "frac": k_ops / (k_ms * 1e-3) / mufu_peak,
+                               "ms": k_ms, "records": n}}
+            del wle_b, d_loc
         learned(0, s0, ctxs[0])
         rows_l, ratios_l = ctxs[0].read_rows(sh)
         refits = net.refits(ctxs[0])
@@ -758,6 +897,10 @@ def learned_shapes_measure(streams, dist, world, rank):
         }
         if two is not None:
             out[kind]["with_two_emitter_starts"] = two
+        if roof is not None:
+            out[kind]["plain_roofline"] = roof
+        if cpu_baseline and rank == 0:
+            out[kind]["cpu_baseline"] = shape_cpu_baseline(kind, R, 1500 if kind == "as3d" else 600)
         for c in ctxs:
             c.close()
         net.close()
@@ -1316,7 +1459,8 @@ def main():
 
     shapes = mixed = None
     if not args.no_learned:
-        shapes = learned_shapes_measure(streams, dist, world, rank)
+        shapes = learned_shapes_measure(streams, dist, world, rank, mufu_peak=mufu_peak,
+                                        cpu_baseline=not args.no_cpu_baseline)
         if not args.no_mixed:
             mixed = mixed_measure(streams, dist, world, rank)
 
@@ -1324,6 +1468,16 @@ def main():
     if not args.no_frames:
         fsteps = min(max(args.steps // 40, 5), 40)
         frames = frame_pipeline(stream, steps=fsteps, warmup=3, dist=dist, world=world)
+        st = frames["stages"]
+        ops = cascade_mufu_ops(R, st["single"], st["two_emitter"], st["three_emitter"])
+        frames["roofline"] = {
+            "bound": "sfu", "unit": "MUFU op/s", "peak": mufu_peak,
+            "achieved": ops / (frames["ms_per_call"] * 1e-3), "frac": ops / (frames["ms_per_call"] * 1e-3) / mufu_peak,
+            "scope": "whole call (32 extractions + localization cascade + CRLB); fits counted on the reference "
+                     "schedule; frames read once from HBM: %.1f GB/s" % (
+                         FRAMES_PER_CALL * FRAME_W * FRAME_H * 2 / (frames["ms_per_call"] * 1e-3) / 1e9)}
+        if rank == 0 and not args.no_cpu_baseline:
+            frames["cpu_baseline"] = frame_cpu_baseline()
         if not args.no_learned:
             frames["learned"] = frame_pipeline_learned(stream, fsteps, 3, dist=dist, world=world)
             frames["learned"]["vs_plain"] = frames["learned"]["frames_per_s"] / frames["frames_per_s"]
@@ -1367,8 +1521,8 @@ def main():
                 "learned_accept": a["accepted"]["learned"], "plain_accept": a["accepted"]["plain"],
                 "learned_equal_rmse": a["equal_rmse"], "crlb_px": a["crlb_px"],
                 "fisher_crlb_px": a["fisher_crlb"]["plain"]["crlb_px"],
-                "plain_rmse_over_fisher_crlb": a["fisher_crlb"]["plain"]["rmse_over_crlb"],
-                "learned_rmse_over_fisher_crlb": a["fisher_crlb"]["learned"]["rmse_over_crlb"],
+                "plain_rmse_over_fisher_crlb": a["fisher_crlb"]["plain"]["rms_error_over_own_crlb"],
+                "learned_rmse_over_fisher_crlb": a["fisher_crlb"]["learned"]["rms_error_over_own_crlb"],
                 "learned_equal_rmse_within_2pct_of_crlb": a["fisher_crlb"]["equal_rmse_within_2pct_of_crlb"],
             })
         # short keys first: the headline survives a truncated tail of the line

@@ -425,6 +425,16 @@ __global__ void __launch_bounds__(kTPB, (SingleLayout<R, FULL>::BLOCKS)) fit_sin
 // thread's serial fit.  Each ROI's pixels, weights and loss terms are
 // contiguous in shared memory (rows padded to 4 floats); D per lane.
 constexpr int kGroupTPB = 128;
+// Lanes per ROI of the multi-emitter group kernel: one central-difference
+// point per lane (2E: 16 points; 3E, AS3D-2E: 22 points).
+__host__ __device__ constexpr int multi_lanes(int kind) { return kind == k2E ? 16 : 32; }
+
+// Multi-emitter kinds and sizes whose roundings (pixel distance and the first
+// two emitters' model sum) are fixed in the source: there the group kernel's
+// rows equal the thread kernel's bit for bit.
+__host__ __device__ constexpr bool multi_group_supported(int kind, int R) {
+    return ((kind == k2E || kind == k3E) && (R == 7 || R == 11)) || (kind == kAS3D2E && R == 7);
+}
 
 template <int R, int KIND>
 struct GroupLayout {
@@ -761,70 +771,39 @@ __device__ __forceinline__ void multi_finish(float *Ininf, const CorePara &c, in
     mo.result[slot] = (int8_t)result;
 }
 
-template <int R, int KIND, int DIST = ArithSpec<KIND, R>::DIST, int MASK = ArithSpec<KIND, R>::MASK,
-          int SUM2 = ArithSpec<KIND, R>::SUM2>
-__global__ void __launch_bounds__(kTPB) fit_multi_kernel(const uint16_t *__restrict__ rois,
-                                                         const float *__restrict__ wle, Queue q,
-                                                         float *__restrict__ loc, MultiOut mo, CorePara c) {
-    typedef SmemLayout<R, KIND> L;
-    enum { P = KindTraits<KIND>::P, PIX = R * R, WHOLE = R * (R + 1), ROISize_Half = R / 2 };
-    extern __shared__ float smem[];
-    const int n = queue_len(q);
-    const int base = blockIdx.x * kTPB;
-    if (base >= n) return;
-    const int cnt = min(kTPB, n - base);
-    float2 *s_img = reinterpret_cast<float2 *>(smem + L::IMG);
-    stage_rois<R>(s_img, rois, q, base, cnt, c.Offset, c.KAdc);
-    __syncthreads();
-    const int tid = threadIdx.x;
-    if (tid >= cnt) return;
-
-    const int slot = base + tid;
-    const int CurFluoID = queue_at(q, slot);
-    const PixView img{s_img + tid, kTPB};
-    float *w = smem + L::W + tid;
-    float *D = smem + L::D + tid;
-    const uint16_t *hdr = rois + (size_t)CurFluoID * WHOLE + PIX;
-    const int XOffset = hdr[0];
-    const int YOffset = hdr[1];
-    const int CurFrame = hdr[2] + 65536 * hdr[3];
+// Start point of a multi-emitter fit (PreEstimation_GS2D_2E, _3E and
+// PreEstimation_AS3D_2E: 2Emitter_core.h:596-698, 3Emitter_core.h:593-710,
+// AS3D_2Emitter_core.h:648-750) from the ROI's pixels, and the weighted-MLE
+// mask width of the 2E fit (a fixed R / 1.8 / 2.35, or R without WLE; the
+// other kinds are unweighted).
+template <int R, int KIND>
+__device__ __forceinline__ void multi_prefit(const PixView &img, const CorePara &c, float *Ininf, float &WLE_SigmaX) {
+    enum { ROISize_Half = R / 2 };
     const float ROICenter = R / 2.0f;
-    const float QE = c.QE;
-
-    float Ininf[P];
-    const RoiRef roi{s_img + tid, w, kTPB};
-    float NearNeighborDistance = 1000;
-
+    WLE_SigmaX = R;
     if (KIND == k2E) {
-        float WLE_SigmaX = R / 1.8f / 2.35f;
-        NearNeighborDistance = wle[(size_t)CurFluoID * QCS_WLE_PARA_NUM + 0];
-        // PreEstimation_GS2D_2E
-        {
-            float Mean1, Mean2, Mean3, Mean4;
-            edge_means<R>(img, Mean1, Mean2, Mean3, Mean4);
-            Mean1 = fminf(Mean1, Mean2);
-            Mean3 = fminf(Mean3, Mean4);
-            Mean1 = fminf(Mean1, Mean3);
-            const float Bkg = Mean1 / R;
-            const float Amp = img[ROISize_Half * R + ROISize_Half] - Bkg;
-            const float SigmaX = R / 2.2f / 2.35f;
-            const float SigmaX1 = (1.0f / (2.0f * SigmaX * SigmaX));
-            float xs[1], ys[1];
-            block_starts<R>(img, 1, xs, ys);
-            Ininf[0] = 0.8f * Amp * rAScalFactor;
-            Ininf[1] = ROICenter;
-            Ininf[2] = ROICenter;
-            Ininf[3] = 0.8f * Amp * rAScalFactor;
-            Ininf[4] = xs[0];
-            Ininf[5] = ys[0];
-            Ininf[6] = SigmaX1 * rSScalFactor;
-            Ininf[7] = 0.8f * Bkg * rBScalFactor;
-        }
+        WLE_SigmaX = R / 1.8f / 2.35f;
+        float Mean1, Mean2, Mean3, Mean4;
+        edge_means<R>(img, Mean1, Mean2, Mean3, Mean4);
+        Mean1 = fminf(Mean1, Mean2);
+        Mean3 = fminf(Mean3, Mean4);
+        Mean1 = fminf(Mean1, Mean3);
+        const float Bkg = Mean1 / R;
+        const float Amp = img[ROISize_Half * R + ROISize_Half] - Bkg;
+        const float SigmaX = R / 2.2f / 2.35f;
+        const float SigmaX1 = (1.0f / (2.0f * SigmaX * SigmaX));
+        float xs[1], ys[1];
+        block_starts<R>(img, 1, xs, ys);
+        Ininf[0] = 0.8f * Amp * rAScalFactor;
+        Ininf[1] = ROICenter;
+        Ininf[2] = ROICenter;
+        Ininf[3] = 0.8f * Amp * rAScalFactor;
+        Ininf[4] = xs[0];
+        Ininf[5] = ys[0];
+        Ininf[6] = SigmaX1 * rSScalFactor;
+        Ininf[7] = 0.8f * Bkg * rBScalFactor;
         if (c.WLEEn == 0) WLE_SigmaX = R;
-        wle_weights<R, MASK>(w, kTPB, WLE_SigmaX, WLE_SigmaX, QCS_MOLECULE_MULTIFIT);
-        mle_fit<R, k2E, DIST, SUM2>(roi, Ininf, D, kTPB);
     } else if (KIND == k3E) {
-        // PreEstimation_GS2D_3E
         float Mean1, Mean2, Mean3, Mean4;
         edge_means<R>(img, Mean1, Mean2, Mean3, Mean4);
         Mean1 = fminf(Mean1, Mean2);
@@ -846,7 +825,6 @@ __global__ void __launch_bounds__(kTPB) fit_multi_kernel(const uint16_t *__restr
         Ininf[8] = ys[1];
         Ininf[9] = SigmaX1 * rSScalFactor;
         Ininf[10] = 0.8f * Bkg * rBScalFactor;
-        mle_fit<R, k3E, DIST, SUM2>(roi, Ininf, D, kTPB);
     } else {  // kAS3D2E
         float Mean1, Mean2, Mean3, Mean4;
         edge_means<R>(img, Mean1, Mean2, Mean3, Mean4);
@@ -871,10 +849,124 @@ __global__ void __launch_bounds__(kTPB) fit_multi_kernel(const uint16_t *__restr
         Ininf[8] = SigmaX1;
         Ininf[9] = SigmaY1;
         Ininf[10] = 0.8f * Bkg * rBScalFactor;
-        mle_fit<R, kAS3D2E, DIST, SUM2>(roi, Ininf, D, kTPB);
     }
+}
+
+template <int R, int KIND, int DIST = ArithSpec<KIND, R>::DIST, int MASK = ArithSpec<KIND, R>::MASK,
+          int SUM2 = ArithSpec<KIND, R>::SUM2>
+__global__ void __launch_bounds__(kTPB) fit_multi_kernel(const uint16_t *__restrict__ rois,
+                                                         const float *__restrict__ wle, Queue q,
+                                                         float *__restrict__ loc, MultiOut mo, CorePara c) {
+    typedef SmemLayout<R, KIND> L;
+    enum { P = KindTraits<KIND>::P, PIX = R * R, WHOLE = R * (R + 1) };
+    extern __shared__ float smem[];
+    const int n = queue_len(q);
+    const int base = blockIdx.x * kTPB;
+    if (base >= n) return;
+    const int cnt = min(kTPB, n - base);
+    float2 *s_img = reinterpret_cast<float2 *>(smem + L::IMG);
+    stage_rois<R>(s_img, rois, q, base, cnt, c.Offset, c.KAdc);
+    __syncthreads();
+    const int tid = threadIdx.x;
+    if (tid >= cnt) return;
+
+    const int slot = base + tid;
+    const int CurFluoID = queue_at(q, slot);
+    const PixView img{s_img + tid, kTPB};
+    float *w = smem + L::W + tid;
+    float *D = smem + L::D + tid;
+    const uint16_t *hdr = rois + (size_t)CurFluoID * WHOLE + PIX;
+    const int XOffset = hdr[0];
+    const int YOffset = hdr[1];
+    const int CurFrame = hdr[2] + 65536 * hdr[3];
+
+    float Ininf[P];
+    const RoiRef roi{s_img + tid, w, kTPB};
+    // the 2E fit's selection reads the nearest-neighbour distance of the WLE pre-pass
+    const float NearNeighborDistance = KIND == k2E ? wle[(size_t)CurFluoID * QCS_WLE_PARA_NUM + 0] : 1000.0f;
+    float WLE_SigmaX;
+    multi_prefit<R, KIND>(img, c, Ininf, WLE_SigmaX);
+    if (KIND == k2E) wle_weights<R, MASK>(w, kTPB, WLE_SigmaX, WLE_SigmaX, QCS_MOLECULE_MULTIFIT);
+    mle_fit<R, KIND, DIST, SUM2>(roi, Ininf, D, kTPB);
 
     multi_finish<R, KIND>(Ininf, c, XOffset, YOffset, CurFrame, NearNeighborDistance, loc, CurFluoID, mo, slot);
+}
+
+// The multi-emitter fit of fit_multi_kernel with G lanes per ROI
+// (MultiGroupEval): bit for bit the same rows, stage results and second
+// emitters.  The thread kernel runs a stage's queue with one thread per ROI at
+// ~255 registers (two warps per SM), so a queue shorter than a wave (the
+// usual 2E / 3E queue) takes as long as one thread's whole fit; here a ROI's
+// pixel terms and gradient points are spread over G lanes.  Per slot: the
+// ROI's (value, log) pairs, its mask and loss terms contiguous (rows padded to
+// 4 floats); the inverse Hessian per lane.
+template <int R, int KIND>
+struct MultiGroupLayout {
+    enum {
+        P = KindTraits<KIND>::P,
+        PIX = R * R,
+        PIXP = (PIX + 3) / 4 * 4,
+        SLOTS = kGroupTPB / multi_lanes(KIND),
+        IMG = 0,                       // float2 per pixel
+        W = IMG + 2 * PIXP * SLOTS,    // floats
+        PART = W + PIXP * SLOTS,
+        D = PART + PIXP * SLOTS,
+        TOTAL = D + P * P * kGroupTPB,
+    };
+};
+
+template <int R, int KIND, int DIST = ArithSpec<KIND, R>::DIST, int MASK = ArithSpec<KIND, R>::MASK,
+          int SUM2 = ArithSpec<KIND, R>::SUM2>
+__global__ void __launch_bounds__(kGroupTPB) fit_multi_group_kernel(const uint16_t *__restrict__ rois,
+                                                                    const float *__restrict__ wle, Queue q,
+                                                                    float *__restrict__ loc, MultiOut mo,
+                                                                    CorePara c) {
+    typedef MultiGroupLayout<R, KIND> L;
+    enum { G = multi_lanes(KIND), P = KindTraits<KIND>::P, PIX = R * R, PIXP = L::PIXP, WHOLE = R * (R + 1),
+           SLOTS = L::SLOTS };
+    static_assert(DIST != kCompiler && SUM2 != kCompiler, "the group sums equal the thread kernel's only for "
+                                                          "roundings fixed in the source");
+    extern __shared__ __align__(16) float smem[];
+    const int n = queue_len(q);
+    const int base = blockIdx.x * SLOTS;
+    if (base >= n) return;
+    const int cnt = min(SLOTS, n - base);
+    float2 *s_img = reinterpret_cast<float2 *>(smem + L::IMG);
+    for (int idx = threadIdx.x; idx < cnt * PIX; idx += kGroupTPB) {
+        const int sl = idx / PIX;
+        const int k = idx - sl * PIX;
+        const int id = queue_at(q, base + sl);
+        const uint16_t u = __ldg(rois + (size_t)id * WHOLE + k);
+        const float pixval = fmaxf((u - c.Offset) * c.KAdc, 1.0f);
+        s_img[sl * PIXP + k] = make_float2(pixval, __logf(pixval));
+    }
+    __syncthreads();
+    const int sl = threadIdx.x / G;
+    const int lane = threadIdx.x % G;
+    if (sl >= cnt) return;
+    const unsigned mask = G == 32 ? 0xffffffffu : ((1u << (G % 32)) - 1u) << ((threadIdx.x & 31) & ~(G - 1));
+
+    const int slot = base + sl;
+    const int CurFluoID = queue_at(q, slot);
+    const float2 *img2 = s_img + sl * PIXP;
+    float *w = smem + L::W + sl * PIXP;
+    float *part = smem + L::PART + sl * PIXP;
+    float *D = smem + L::D + threadIdx.x;
+    const uint16_t *hdr = rois + (size_t)CurFluoID * WHOLE + PIX;
+    const int XOffset = hdr[0];
+    const int YOffset = hdr[1];
+    const int CurFrame = hdr[2] + 65536 * hdr[3];
+    const float NearNeighborDistance = KIND == k2E ? wle[(size_t)CurFluoID * QCS_WLE_PARA_NUM + 0] : 1000.0f;
+
+    float Ininf[P];
+    float WLE_SigmaX;
+    multi_prefit<R, KIND>(PixView{img2, 1}, c, Ininf, WLE_SigmaX);
+    if (KIND == k2E && lane == 0) wle_weights<R, MASK>(w, 1, WLE_SigmaX, WLE_SigmaX, QCS_MOLECULE_MULTIFIT);
+    __syncwarp(mask);
+    bfgs_fit<P, KindTraits<KIND>::IT>(MultiGroupEval<R, KIND, DIST, SUM2, G>{img2, w, part, lane, mask}, Ininf, D,
+                                      kGroupTPB);
+    if (lane == 0)
+        multi_finish<R, KIND>(Ininf, c, XOffset, YOffset, CurFrame, NearNeighborDistance, loc, CurFluoID, mo, slot);
 }
 
 // -------------------------------------- learned-start two-emitter fits ---
@@ -1039,14 +1131,27 @@ cudaError_t launch_single_group(const FitLaunch &a) {
 
 template <int R, int KIND>
 cudaError_t launch_multi(const FitLaunch &a) {
-    const size_t smem = SmemLayout<R, KIND>::TOTAL * sizeof(float);
-    auto k = fit_multi_kernel<R, KIND>;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    const int grid = (a.max_count + kTPB - 1) / kTPB;
-    if (grid == 0) return cudaSuccess;
-    k<<<grid, kTPB, smem, a.stream>>>(a.rois, a.wle, a.q, a.loc, a.mo, a.para);
-    return cudaGetLastError();
+    if constexpr (multi_group_supported(KIND, R)) {
+        // G lanes per ROI: the same rows bit for bit, a fraction of the latency
+        typedef MultiGroupLayout<R, KIND> L;
+        const size_t smem = L::TOTAL * sizeof(float);
+        auto k = fit_multi_group_kernel<R, KIND>;
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        const int grid = (a.max_count + L::SLOTS - 1) / L::SLOTS;
+        if (grid == 0) return cudaSuccess;
+        k<<<grid, kGroupTPB, smem, a.stream>>>(a.rois, a.wle, a.q, a.loc, a.mo, a.para);
+        return cudaGetLastError();
+    } else {
+        const size_t smem = SmemLayout<R, KIND>::TOTAL * sizeof(float);
+        auto k = fit_multi_kernel<R, KIND>;
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        const int grid = (a.max_count + kTPB - 1) / kTPB;
+        if (grid == 0) return cudaSuccess;
+        k<<<grid, kTPB, smem, a.stream>>>(a.rois, a.wle, a.q, a.loc, a.mo, a.para);
+        return cudaGetLastError();
+    }
 }
 
 }  // namespace

@@ -614,6 +614,172 @@ struct GroupEval {
     }
 };
 
+// Poisson deviance term of one pixel of the multi-emitter kinds at the
+// parameters v: the expressions of loss(), term for term.
+template <int KIND, int DIST, int SUM2>
+__device__ __forceinline__ float multi_term(float colpos, float rowpos, const float *v, float pixval, float logpix) {
+    if (KIND == k2E) {
+        const float dx0 = colpos - v[1], dy0 = rowpos - v[2];
+        const float dx1 = colpos - v[4], dy1 = rowpos - v[5];
+        const float A0 = v[0] * QCS_ASCALE, A1 = v[3] * QCS_ASCALE;
+        const float e0 = __expf(-(sum_of_products<DIST>(dx0, dx0, dy0, dy0)) * v[6] * QCS_SSCALE);
+        const float e1 = __expf(-(sum_of_products<DIST>(dx1, dx1, dy1, dy1)) * v[6] * QCS_SSCALE);
+        float IVal_all = sum_of_products<SUM2>(A0, e0, A1, e1) + v[7] * QCS_BSCALE;
+        return IVal_all - pixval - pixval * (__logf(IVal_all) - logpix);
+    } else if (KIND == k3E) {
+        const float dx0 = colpos - v[1], dy0 = rowpos - v[2];
+        const float dx1 = colpos - v[4], dy1 = rowpos - v[5];
+        const float dx2 = colpos - v[7], dy2 = rowpos - v[8];
+        const float A0 = v[0] * QCS_ASCALE, A1 = v[3] * QCS_ASCALE, A2 = v[6] * QCS_ASCALE;
+        const float e0 = __expf(-(sum_of_products<DIST>(dx0, dx0, dy0, dy0)) * v[9] * QCS_SSCALE);
+        const float e1 = __expf(-(sum_of_products<DIST>(dx1, dx1, dy1, dy1)) * v[9] * QCS_SSCALE);
+        const float e2 = __expf(-(sum_of_products<DIST>(dx2, dx2, dy2, dy2)) * v[9] * QCS_SSCALE);
+        float IVal_all = sum_of_products<SUM2>(A0, e0, A1, e1) + A2 * e2 + v[10] * QCS_BSCALE;
+        return IVal_all - pixval - pixval * (__logf(IVal_all) - logpix);
+    } else {  // kAS3D2E
+        const float dx0 = colpos - v[1], dy0 = rowpos - v[2];
+        const float dx1 = colpos - v[6], dy1 = rowpos - v[7];
+        const float A0 = v[0] * QCS_ASCALE, A1 = v[5] * QCS_ASCALE;
+        const float e0 = __expf(-(sum_of_products<DIST>(dx0 * dx0 * v[3], QCS_SSCALE, dy0 * dy0 * v[4], QCS_SSCALE)));
+        const float e1 = __expf(-(sum_of_products<DIST>(dx1 * dx1 * v[8], QCS_SSCALE, dy1 * dy1 * v[9], QCS_SSCALE)));
+        float IVal_all = sum_of_products<SUM2>(A0, e0, A1, e1) + v[10] * QCS_BSCALE;
+        return IVal_all - pixval - pixval * (__logf(IVal_all) - logpix);
+    }
+}
+
+// Loss and gradient of one multi-emitter ROI (2E, 3E, AS3D-2E) evaluated by
+// a group of G consecutive lanes, bit for bit equal to ThreadEval:
+//  - loss: lane l computes the pixel terms k = l, l + G, ... (multi_term)
+//    into the ROI's scratch row; then every lane sums the row in pixel order
+//    with the thread kernel's operations (the weighted 2E fit: fused
+//    multiply-adds with the mask; 3E and AS3D-2E: plain adds);
+//  - gradient: the 2P central-difference points are replayed as
+//    numerical_gradient produces them (each loss call clamps its point in
+//    place and the next point starts from the clamped values); lane l sums
+//    points l, l + G, ... over all pixels in pixel order, and the lanes
+//    exchange the sums.
+// img / w / part: the ROI's pixels, mask and scratch, contiguous and 16-byte
+// aligned; mask: the group's lanes.  Only for roundings fixed in the source
+// (DIST, SUM2 != kCompiler).
+template <int R, int KIND, int DIST, int SUM2, int G>
+struct MultiGroupEval {
+    const float2 *img;
+    const float *w;
+    float *part;
+    int lane;
+    unsigned mask;
+
+    __device__ __forceinline__ float loss(float *Ininf) const {
+        typedef KindTraits<KIND> T;
+        enum { PIX = R * R };
+#pragma unroll
+        for (int k = 0; k < T::P; k++) {
+            if (T::CLAMP001) {
+                if (Ininf[k] < 0.01f) Ininf[k] = 0.01f;
+            } else {
+                if (Ininf[k] < 0.0f) Ininf[k] = 0.0f;
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < (PIX + G - 1) / G; i++) {
+            const int k = lane + i * G;
+            if (k < PIX) {
+                const int row = k / R, col = k - (k / R) * R;
+                const float2 pl = img[k];
+                part[k] = multi_term<KIND, DIST, SUM2>(col + 0.5f, row + 0.5f, Ininf, pl.x, pl.y);
+            }
+        }
+        __syncwarp(mask);
+        float TotalLoss = 0;
+        const float4 *p4 = reinterpret_cast<const float4 *>(part);
+        if (T::WEIGHTED) {
+            const float4 *w4 = reinterpret_cast<const float4 *>(w);
+#pragma unroll 8
+            for (int q = 0; q < PIX / 4; q++) {
+                const float4 a = w4[q], t = p4[q];
+                TotalLoss = __fmaf_rn(a.x, t.x, TotalLoss);
+                TotalLoss = __fmaf_rn(a.y, t.y, TotalLoss);
+                TotalLoss = __fmaf_rn(a.z, t.z, TotalLoss);
+                TotalLoss = __fmaf_rn(a.w, t.w, TotalLoss);
+            }
+#pragma unroll
+            for (int k = PIX / 4 * 4; k < PIX; k++) TotalLoss = __fmaf_rn(w[k], part[k], TotalLoss);
+        } else {
+#pragma unroll 8
+            for (int q = 0; q < PIX / 4; q++) {
+                const float4 t = p4[q];
+                TotalLoss = __fadd_rn(TotalLoss, t.x);
+                TotalLoss = __fadd_rn(TotalLoss, t.y);
+                TotalLoss = __fadd_rn(TotalLoss, t.z);
+                TotalLoss = __fadd_rn(TotalLoss, t.w);
+            }
+#pragma unroll
+            for (int k = PIX / 4 * 4; k < PIX; k++) TotalLoss = __fadd_rn(TotalLoss, part[k]);
+        }
+        __syncwarp(mask);
+        return TotalLoss;
+    }
+
+    __device__ __forceinline__ void gradient(const float *Ininf, float *grad) const {
+        typedef KindTraits<KIND> T;
+        enum { P = T::P, NE = 2 * P, NC = (NE + G - 1) / G, PIX = R * R };
+        float v[NC][P] = {};
+        {
+            float t[P];
+#pragma unroll
+            for (int k = 0; k < P; k++) t[k] = Ininf[k];
+#pragma unroll
+            for (int k = 0; k < P; k++) {
+                t[k] = t[k] - 0.002f;
+#pragma unroll
+                for (int c = 0; c < P; c++) {
+                    if (T::CLAMP001) { if (t[c] < 0.01f) t[c] = 0.01f; } else { if (t[c] < 0.0f) t[c] = 0.0f; }
+                }
+#pragma unroll
+                for (int j = 0; j < NC; j++)
+                    if (lane + j * G == 2 * k)
+#pragma unroll
+                        for (int c = 0; c < P; c++) v[j][c] = t[c];
+                t[k] = t[k] + 0.004f;
+#pragma unroll
+                for (int c = 0; c < P; c++) {
+                    if (T::CLAMP001) { if (t[c] < 0.01f) t[c] = 0.01f; } else { if (t[c] < 0.0f) t[c] = 0.0f; }
+                }
+#pragma unroll
+                for (int j = 0; j < NC; j++)
+                    if (lane + j * G == 2 * k + 1)
+#pragma unroll
+                        for (int c = 0; c < P; c++) v[j][c] = t[c];
+                t[k] = t[k] - 0.002f;
+            }
+        }
+        float tot[NC];
+#pragma unroll
+        for (int j = 0; j < NC; j++) tot[j] = 0;
+#pragma unroll 1
+        for (int row = 0; row < R; row++) {
+#pragma unroll(R <= kUnrollMaxR ? R : 1)
+            for (int col = 0; col < R; col++) {
+                const float2 pl = img[row * R + col];
+                const float wk = T::WEIGHTED ? w[row * R + col] : 1.0f;
+#pragma unroll
+                for (int j = 0; j < NC; j++) {
+                    if (lane + j * G < NE) {
+                        const float Lt = multi_term<KIND, DIST, SUM2>(col + 0.5f, row + 0.5f, v[j], pl.x, pl.y);
+                        tot[j] = T::WEIGHTED ? __fmaf_rn(wk, Lt, tot[j]) : __fadd_rn(tot[j], Lt);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < P; k++) {
+            const float tn = __shfl_sync(mask, tot[(2 * k) / G], (2 * k) % G, G);
+            const float tp = __shfl_sync(mask, tot[(2 * k + 1) / G], (2 * k + 1) % G, G);
+            grad[k] = (tp - tn) * 250.0f;
+        }
+    }
+};
+
 // ------------------------------------------ staged single-emitter eval ---
 // The weighted-MLE mask of an R x R ROI depends on |col - R/2| and
 // |row - R/2| only: its exponent holds the squared distances of the pixel
