@@ -454,6 +454,26 @@ int qcs_loc_autotune(qcs_loc_data *c, const qcs_loc_para *p, const uint16_t *d_r
  * (count 0..8 entries of (largest batch, lanes 1 / 4 / 8 / 16); 0 clears it). */
 int qcs_loc_tuning(const qcs_loc_data *c, int *sizes, int *lanes, int max_entries);
 int qcs_loc_set_tuning(qcs_loc_data *c, const int *sizes, const int *lanes, int count);
+/* Model selection of multi-emitter calls (no counterpart in the reference,
+ * whose selection is its SNR / validity cascade, bfgsMLE_GS2D_core.h:279-298,
+ * bfgsMLE_GS2D_2Emitter_core.h:296-348; QCS_SELECT_CASCADE, the default and
+ * the parity mode).  QCS_SELECT_LR, for GS2D and DH3D calls with
+ * MultiEmitterFitEn: every record is fitted with one, two and three emitters
+ * (the reference's fits, schedules and accept rules), each fitted model's
+ * unweighted Poisson log-likelihood sum(n ln mu - mu) is accumulated in FP64,
+ * and a record keeps the smallest accepted model unless a larger accepted one
+ * raises 2 ln L by more than `threshold` per added emitter (three parameters
+ * per emitter; 0 picks QCS_SELECT_LR_DEFAULT_TH).  The rows are the chosen
+ * model's, at most two emitters per record as the reference writes them, in
+ * the cascade's layout (records, then appended second emitters) with CRLB.
+ * Fit ratios: 1, 2, 3 = all records; 4, 5, 6 = fractions keeping one, two,
+ * three emitters; 7 = no model accepted.  About three times the fitting work
+ * of the cascade.  Allocates the mode's scratch (capacity x 108 bytes) once. */
+#define QCS_SELECT_CASCADE 0
+#define QCS_SELECT_LR 1
+#define QCS_SELECT_LR_DEFAULT_TH 10.0f
+int qcs_loc_set_model_selection(qcs_loc_data *c, int mode, float threshold);
+int qcs_loc_model_selection(const qcs_loc_data *c, int *mode, float *threshold);
 /* LDLocData_TypeDef::LocPrecCalc_GaussianCRLB (bfgs_top.h:90,
  * LocPrecCalc_GaussianCRLB.cu:23-40): CRLB columns of n device rows. */
 int qcs_crlb_device(const qcs_loc_para *p, float *d_loc, int n, void *stream);

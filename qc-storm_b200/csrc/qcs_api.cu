@@ -77,6 +77,11 @@ struct qcs_loc_data {
     int tune_count = 0;
     int tune_n[8] = {0};
     int tune_lanes[8] = {0};
+    // model selection of multi-emitter calls: QCS_SELECT_CASCADE (the reference's) or QCS_SELECT_LR
+    int sel_mode = QCS_SELECT_CASCADE;
+    float sel_th = QCS_SELECT_LR_DEFAULT_TH;
+    void *d_lr = nullptr;           // QCS_SELECT_LR scratch: loc2 / loc3 rows, three log-likelihood arrays
+    int lr_stats = 0;               // the last call ran the likelihood-ratio selection
     int pending = 0;                // an asynchronous host call awaits qcs_loc_finish
     int pending_n = 0;
     int valid = 0;
@@ -142,6 +147,7 @@ int qcs_loc_deinit(qcs_loc_data *c) {
     qcs::wle_sorter_destroy(c->wle_sorter);
     cudaFree(c->d_start);
     cudaFree(c->d_start2);
+    cudaFree(c->d_lr);
     if (c->ev_done) cudaEventDestroy(c->ev_done);
     if (c->stream) cudaStreamDestroy(c->stream);
     if (c->side) cudaStreamDestroy(c->side);
@@ -237,6 +243,33 @@ static int check_call(qcs_loc_data *c, const qcs_loc_para *p, int n) {
     return QCS_OK;
 }
 
+// The call runs the likelihood-ratio selection: the mode is set and the
+// parameters ask for GS2D (or DH3D) multi-emitter fitting.
+static bool use_lr(const qcs_loc_data *c, const qcs_loc_para *p) {
+    return c->sel_mode == QCS_SELECT_LR && c->d_lr && p->MultiEmitterFitEn &&
+           (p->LocType == QCS_LOCTYPE_GS2D || p->LocType == QCS_LOCTYPE_DH3D);
+}
+
+static qcs::LrScratch lr_scratch(const qcs_loc_data *c) {
+    const size_t cap = (size_t)c->capacity;
+    qcs::LrScratch lr;
+    char *b = static_cast<char *>(c->d_lr);
+    lr.loc2 = reinterpret_cast<float *>(b);
+    lr.loc3 = lr.loc2 + cap * 12;
+    lr.ll1 = reinterpret_cast<double *>(lr.loc3 + cap * 12);  // 2 x cap x 48 bytes: 8-byte aligned
+    lr.ll2 = lr.ll1 + cap;
+    lr.ll3 = lr.ll2 + cap;
+    lr.threshold = c->sel_th;
+    return lr;
+}
+
+// The call's localization: the reference's cascade, or the likelihood-ratio selection.
+static cudaError_t run_localization(qcs_loc_data *c, const qcs::CascadeArgs &a) {
+    c->lr_stats = use_lr(c, &a.para) ? 1 : 0;
+    if (c->lr_stats) return qcs::run_cascade_lr(a, c->st, lr_scratch(c));
+    return qcs::run_cascade(a, c->st);
+}
+
 static int tuned_lanes(const qcs_loc_data *c, int n) {
     for (int k = 0; k < c->tune_count; ++k)
         if (n <= c->tune_n[k]) return c->tune_lanes[k];
@@ -263,7 +296,7 @@ int qcs_loc_localize_device(qcs_loc_data *c, const uint16_t *d_rois, const float
     a.max_rows = c->max_rows;
     a.stream = s;
     a.lanes = tuned_lanes(c, n);
-    QCS_CUDA(qcs::run_cascade(a, c->st), "localization cascade");
+    QCS_CUDA(run_localization(c, a), "localization cascade");
     return QCS_OK;
 }
 
@@ -282,7 +315,7 @@ int qcs_loc_localize_device_n(qcs_loc_data *c, const uint16_t *d_rois, const flo
     a.loc = c->d_loc;
     a.max_rows = c->max_rows;
     a.stream = s;
-    QCS_CUDA(qcs::run_cascade(a, c->st), "localization cascade");
+    QCS_CUDA(run_localization(c, a), "localization cascade");
     return QCS_OK;
 }
 
@@ -602,6 +635,16 @@ static void compute_ratios(qcs_loc_data *c, const qcs_loc_para *p, int n) {
     const int single = k[qcs::kCntSingle];
     c->ratios[0] = (float)single / div;
     c->ratios[3] = (float)single / div;
+    if (c->lr_stats) {
+        // every record fitted with one, two and three emitters; the final
+        // ratios are the models the likelihood-ratio test kept
+        c->ratios[1] = c->ratios[2] = c->ratios[0];
+        c->ratios[3] = (float)k[qcs::kCntSel1] / div;
+        c->ratios[4] = (float)k[qcs::kCntSel2] / div;
+        c->ratios[5] = (float)k[qcs::kCntSel3] / div;
+        c->ratios[6] = (float)k[qcs::kCntRejected] / div;
+        return;
+    }
     if (p->MultiEmitterFitEn) {
         const int n2 = k[qcs::kCnt2E], n2c = k[qcs::kCnt2EClassify], n3 = k[qcs::kCnt3E], rej = k[qcs::kCntRejected];
         const int n3c = k[qcs::kCnt3EClassify];  // learned classes only: records sent straight to 3E
@@ -914,6 +957,29 @@ int qcs_loc_set_tuning(qcs_loc_data *c, const int *sizes, const int *lanes, int 
         c->tune_lanes[i] = lanes[i];
     }
     c->tune_count = count;
+    return QCS_OK;
+}
+
+int qcs_loc_set_model_selection(qcs_loc_data *c, int mode, float threshold) {
+    if (!c) return fail(QCS_ERR_ARG, "null context");
+    if (mode != QCS_SELECT_CASCADE && mode != QCS_SELECT_LR)
+        return fail(QCS_ERR_ARG, "mode: QCS_SELECT_CASCADE or QCS_SELECT_LR");
+    if (threshold < 0.0f || threshold != threshold) return fail(QCS_ERR_ARG, "threshold must be >= 0");
+    if (c->pending) return fail(QCS_ERR_STATE, "an asynchronous call on this context awaits qcs_loc_finish");
+    if (mode == QCS_SELECT_LR && !c->d_lr) {
+        const size_t cap = (size_t)c->capacity;
+        const size_t bytes = 2 * cap * 12 * sizeof(float) + 3 * cap * sizeof(double);
+        QCS_CUDA(cudaMalloc(&c->d_lr, bytes > 0 ? bytes : 16), "likelihood-ratio scratch");
+    }
+    c->sel_mode = mode;
+    c->sel_th = threshold > 0.0f ? threshold : QCS_SELECT_LR_DEFAULT_TH;
+    return QCS_OK;
+}
+
+int qcs_loc_model_selection(const qcs_loc_data *c, int *mode, float *threshold) {
+    if (!c) return fail(QCS_ERR_ARG, "null context");
+    if (mode) *mode = c->sel_mode;
+    if (threshold) *threshold = c->sel_th;
     return QCS_OK;
 }
 

@@ -225,6 +225,65 @@ __global__ void init_counters_kernel(CascadeState st, int n, const int *__restri
     st.counters[kCntRows] = n;
 }
 
+// Likelihood-ratio selection of each record's model (run_cascade_lr); the
+// chosen model's first row replaces loc[i], its second emitter (if any) goes
+// to extra2[i] with res2[i] = 1 or 2 (0: no model accepted), which the
+// cascade's append compaction then reads as a two-emitter stage over all
+// records.
+__global__ void lr_select_kernel(CascadeState st, float *__restrict__ loc, LrScratch lr, int n,
+                                 const int *__restrict__ n_dev) {
+    __shared__ int cnt[3];
+    if (threadIdx.x < 3) cnt[threadIdx.x] = 0;
+    __syncthreads();
+    if (n_dev) n = min(max(*n_dev, 0), n);
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const bool a1 = loc[(size_t)i * 12] > 0.0f, a2 = st.res2[i] >= 1, a3 = st.res3[i] >= 1;
+        const double l1 = lr.ll1[i], l2 = lr.ll2[i], l3 = lr.ll3[i];
+        const double th = lr.threshold;
+        int best = a1 ? 1 : 0;
+        double lb = l1;
+        if (a2 && (best == 0 || 2.0 * (l2 - lb) > th * (2 - best))) {
+            best = 2;
+            lb = l2;
+        }
+        if (a3 && (best == 0 || 2.0 * (l3 - lb) > th * (3 - best))) best = 3;
+        float4 *dst = reinterpret_cast<float4 *>(loc + (size_t)i * 12);
+        if (best >= 2) {
+            const float4 *src = reinterpret_cast<const float4 *>((best == 2 ? lr.loc2 : lr.loc3) + (size_t)i * 12);
+            dst[0] = src[0];
+            dst[1] = src[1];
+            dst[2] = src[2];
+        }
+        if (best == 3) {
+            const float4 *src = reinterpret_cast<const float4 *>(st.extra3 + (size_t)i * 12);
+            float4 *x = reinterpret_cast<float4 *>(st.extra2 + (size_t)i * 12);
+            x[0] = src[0];
+            x[1] = src[1];
+            x[2] = src[2];
+        }
+        st.res2[i] = (int8_t)(best == 0 ? 0 : (best == 1 ? 1 : (best == 2 ? st.res2[i] : st.res3[i])));
+        if (best > 0) atomicAdd(&cnt[best - 1], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x < 3 && cnt[threadIdx.x]) atomicAdd(st.counters + kCntSel1 + threadIdx.x, cnt[threadIdx.x]);
+}
+
+// counters of run_cascade_lr: every record is in each stage's (identity) queue
+__global__ void lr_counters_kernel(CascadeState st, int n, const int *__restrict__ n_dev) {
+    if (n_dev) n = min(max(*n_dev, 0), n);
+    st.counters[kCntSingle] = n;
+    st.counters[kCnt2E] = n;
+    st.counters[kCnt2EClassify] = 0;
+    st.counters[kCnt3E] = n;
+    st.counters[kCnt3EClassify] = 0;
+    st.counters[kCntRejected] = 0;
+    st.counters[kCntRows] = n;
+    st.counters[kCntSel1] = 0;
+    st.counters[kCntSel2] = 0;
+    st.counters[kCntSel3] = 0;
+}
+
 __global__ void finish_kernel(CascadeState st, int max_rows) {
     const int rows = st.counters[kCntRows];
     st.counters[kCntValid] = rows < max_rows ? rows : max_rows;
@@ -312,6 +371,42 @@ cudaError_t cascade_tail(const CascadeArgs &a, const CascadeState &st) {
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     return launch_crlb(a.loc, st.counters + kCntValid, 0, multi ? a.max_rows : n, p.LocType, p.ReadNoise_e, p.QE,
                        p.PixelSize, a.stream);
+}
+
+cudaError_t run_cascade_lr(const CascadeArgs &a, const CascadeState &st, const LrScratch &lr) {
+    const qcs_loc_para &p = a.para;
+    const int n = a.n, R = p.ROISize;
+    cudaError_t e;
+    lr_counters_kernel<<<1, 1, 0, a.stream>>>(st, n, a.n_dev);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    FitLaunch f;
+    f.rois = a.rois;
+    f.wle = a.wle;
+    f.q = Queue{nullptr, st.counters + kCntSingle, 0};  // identity over the call's records
+    f.max_count = n;
+    f.loc = a.loc;
+    f.to2e = nullptr;
+    f.mo = MultiOut{nullptr, nullptr};
+    f.para = core_para(p);
+    f.stream = a.stream;
+    f.ll = lr.ll1;
+    if ((e = launch_fit(kGS2D, R, f)) != cudaSuccess) return e;
+    f.loc = lr.loc2;
+    f.mo = MultiOut{st.res2, st.extra2};
+    f.ll = lr.ll2;
+    if ((e = launch_fit(k2E, R, f)) != cudaSuccess) return e;
+    f.loc = lr.loc3;
+    f.mo = MultiOut{st.res3, st.extra3};
+    f.ll = lr.ll3;
+    if ((e = launch_fit(k3E, R, f)) != cudaSuccess) return e;
+    if (n > 0) lr_select_kernel<<<(n + 255) / 256, 256, 0, a.stream>>>(st, a.loc, lr, n, a.n_dev);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    // second emitters appended after the records, in record order; records with no model counted as rejected
+    if ((e = launch_compaction(CompactStage{st, a.loc, 2, 0, a.max_rows}, n, st, a.stream)) != cudaSuccess) return e;
+    finish_kernel<<<1, 1, 0, a.stream>>>(st, a.max_rows);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    return launch_crlb(a.loc, st.counters + kCntValid, 0, a.max_rows, p.LocType, p.ReadNoise_e, p.QE, p.PixelSize,
+                       a.stream);
 }
 
 cudaError_t run_cascade(const CascadeArgs &a, const CascadeState &st) {

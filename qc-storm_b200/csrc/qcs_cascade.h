@@ -20,6 +20,9 @@ enum {
     kCnt3EClassify = 7,  // three-emitter queue entries that came from the classifier (learned classes)
     kCntRefit = 8,       // learned path: records refitted by the plain single-emitter fit
     kCntRefit2E = 9,     // learned path: two-emitter fits redone by the plain two-emitter fit
+    kCntSel1 = 10,       // likelihood-ratio selection: records that keep the one-emitter model
+    kCntSel2 = 11,       //   ... the two-emitter model
+    kCntSel3 = 12,       //   ... the three-emitter model
     kCntNum = 16
 };
 
@@ -73,6 +76,21 @@ struct CascadeArgs {
 // The whole localization call: queues, single-emitter fit, 2E / 3E fits,
 // CRLB.
 cudaError_t run_cascade(const CascadeArgs &a, const CascadeState &st);
+
+// Likelihood-ratio model selection (a selectable mode in place of the
+// reference's SNR cascade; GS2D or DH3D with multi-emitter fitting): every
+// record is fitted with one, two and three emitters (the reference's fits,
+// schedules and accept rules), the unweighted Poisson log-likelihood of each
+// fitted model is summed in FP64, and a record keeps the smallest accepted
+// model unless a larger accepted one raises 2 ln L by more than `threshold`
+// per added emitter.  Its rows (the chosen model's, up to two emitters as the
+// reference writes them) then take the cascade's output layout and CRLB.
+struct LrScratch {
+    float *loc2, *loc3;      // capacity x 12: rows of the two- and three-emitter fits
+    double *ll1, *ll2, *ll3;  // capacity: their log-likelihoods
+    float threshold;
+};
+cudaError_t run_cascade_lr(const CascadeArgs &a, const CascadeState &st, const LrScratch &lr);
 
 // Its phases, for callers that replace the single-emitter fit (the learned
 // path): the queues; the single-emitter launch run_cascade makes over them;

@@ -372,7 +372,7 @@ template <int R, int KIND, bool WORDS, int DIST = ArithSpec<KIND, R>::DIST, int 
           bool FULL = MASK == kCompiler>
 __global__ void __launch_bounds__(kTPB, (SingleLayout<R, FULL>::BLOCKS)) fit_single_kernel(
     const uint16_t *__restrict__ rois, const float *__restrict__ wle, Queue q, float *__restrict__ loc,
-    uint8_t *__restrict__ to2e, CorePara c) {
+    uint8_t *__restrict__ to2e, CorePara c, double *__restrict__ ll) {
     typedef SingleLayout<R, FULL> L;
     enum { P = KindTraits<KIND>::P, PIX = R * R, WHOLE = R * (R + 1) };
     extern __shared__ __align__(16) float smem[];
@@ -405,6 +405,7 @@ __global__ void __launch_bounds__(kTPB, (SingleLayout<R, FULL>::BLOCKS)) fit_sin
                                     sp.MoleculeType);
     float D[P * P];  // the inverse Hessian, in registers
     bfgs_fit<P, KindTraits<KIND>::IT>(StagedEval<R, KIND, DIST, FULL>{s_img + tid, mask, kTPB}, Ininf, D, 1);
+    if (ll) ll[CurFluoID] = model_loglik<R, KIND, DIST, kCompiler>(s_img + tid, kTPB, Ininf, 0, 1);
     float row[12];
     bool accepted;
     float CurSNR;
@@ -856,7 +857,8 @@ template <int R, int KIND, int DIST = ArithSpec<KIND, R>::DIST, int MASK = Arith
           int SUM2 = ArithSpec<KIND, R>::SUM2>
 __global__ void __launch_bounds__(kTPB) fit_multi_kernel(const uint16_t *__restrict__ rois,
                                                          const float *__restrict__ wle, Queue q,
-                                                         float *__restrict__ loc, MultiOut mo, CorePara c) {
+                                                         float *__restrict__ loc, MultiOut mo, CorePara c,
+                                                         double *__restrict__ ll) {
     typedef SmemLayout<R, KIND> L;
     enum { P = KindTraits<KIND>::P, PIX = R * R, WHOLE = R * (R + 1) };
     extern __shared__ float smem[];
@@ -888,6 +890,7 @@ __global__ void __launch_bounds__(kTPB) fit_multi_kernel(const uint16_t *__restr
     multi_prefit<R, KIND>(img, c, Ininf, WLE_SigmaX);
     if (KIND == k2E) wle_weights<R, MASK>(w, kTPB, WLE_SigmaX, WLE_SigmaX, QCS_MOLECULE_MULTIFIT);
     mle_fit<R, KIND, DIST, SUM2>(roi, Ininf, D, kTPB);
+    if (ll) ll[CurFluoID] = model_loglik<R, KIND, DIST, SUM2>(s_img + tid, kTPB, Ininf, 0, 1);
 
     multi_finish<R, KIND>(Ininf, c, XOffset, YOffset, CurFrame, NearNeighborDistance, loc, CurFluoID, mo, slot);
 }
@@ -920,7 +923,7 @@ template <int R, int KIND, int DIST = ArithSpec<KIND, R>::DIST, int MASK = Arith
 __global__ void __launch_bounds__(kGroupTPB) fit_multi_group_kernel(const uint16_t *__restrict__ rois,
                                                                     const float *__restrict__ wle, Queue q,
                                                                     float *__restrict__ loc, MultiOut mo,
-                                                                    CorePara c) {
+                                                                    CorePara c, double *__restrict__ ll) {
     typedef MultiGroupLayout<R, KIND> L;
     enum { G = multi_lanes(KIND), P = KindTraits<KIND>::P, PIX = R * R, PIXP = L::PIXP, WHOLE = R * (R + 1),
            SLOTS = L::SLOTS };
@@ -965,6 +968,12 @@ __global__ void __launch_bounds__(kGroupTPB) fit_multi_group_kernel(const uint16
     __syncwarp(mask);
     bfgs_fit<P, KindTraits<KIND>::IT>(MultiGroupEval<R, KIND, DIST, SUM2, G>{img2, w, part, lane, mask}, Ininf, D,
                                       kGroupTPB);
+    if (ll) {  // the lanes' pixel sums, combined in a fixed order
+        double s = model_loglik<R, KIND, DIST, SUM2>(img2, 1, Ininf, lane, G);
+#pragma unroll
+        for (int o = G / 2; o > 0; o >>= 1) s += __shfl_xor_sync(mask, s, o, G);
+        if (lane == 0) ll[CurFluoID] = s;
+    }
     if (lane == 0)
         multi_finish<R, KIND>(Ininf, c, XOffset, YOffset, CurFrame, NearNeighborDistance, loc, CurFluoID, mo, slot);
 }
@@ -1112,7 +1121,7 @@ cudaError_t launch_single(const FitLaunch &a) {
     if (e != cudaSuccess) return e;
     const int grid = (a.max_count + kTPB - 1) / kTPB;
     if (grid == 0) return cudaSuccess;
-    k<<<grid, kTPB, smem, a.stream>>>(a.rois, a.wle, a.q, a.loc, a.to2e, a.para);
+    k<<<grid, kTPB, smem, a.stream>>>(a.rois, a.wle, a.q, a.loc, a.to2e, a.para, a.ll);
     return cudaGetLastError();
 }
 
@@ -1140,7 +1149,7 @@ cudaError_t launch_multi(const FitLaunch &a) {
         if (e != cudaSuccess) return e;
         const int grid = (a.max_count + L::SLOTS - 1) / L::SLOTS;
         if (grid == 0) return cudaSuccess;
-        k<<<grid, kGroupTPB, smem, a.stream>>>(a.rois, a.wle, a.q, a.loc, a.mo, a.para);
+        k<<<grid, kGroupTPB, smem, a.stream>>>(a.rois, a.wle, a.q, a.loc, a.mo, a.para, a.ll);
         return cudaGetLastError();
     } else {
         const size_t smem = SmemLayout<R, KIND>::TOTAL * sizeof(float);
@@ -1149,7 +1158,7 @@ cudaError_t launch_multi(const FitLaunch &a) {
         if (e != cudaSuccess) return e;
         const int grid = (a.max_count + kTPB - 1) / kTPB;
         if (grid == 0) return cudaSuccess;
-        k<<<grid, kTPB, smem, a.stream>>>(a.rois, a.wle, a.q, a.loc, a.mo, a.para);
+        k<<<grid, kTPB, smem, a.stream>>>(a.rois, a.wle, a.q, a.loc, a.mo, a.para, a.ll);
         return cudaGetLastError();
     }
 }

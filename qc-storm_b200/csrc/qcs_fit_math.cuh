@@ -780,6 +780,60 @@ struct MultiGroupEval {
     }
 };
 
+// Expected photoelectrons of pixel (colpos, rowpos) under the model at the
+// parameters v (fit units): the model value of loss(), expression for
+// expression.
+template <int KIND, int DIST, int SUM2>
+__device__ __forceinline__ float model_value(float colpos, float rowpos, const float *v) {
+    if (KIND == kGS2D || KIND == kAS3D) {
+        const float e = single_expo<KIND, DIST>(colpos, rowpos, v);
+        return sum_of_products<kModelSum>(v[0] * QCS_ASCALE, e, v[KindTraits<KIND>::P - 1], QCS_BSCALE);
+    } else if (KIND == k2E) {
+        const float dx0 = colpos - v[1], dy0 = rowpos - v[2];
+        const float dx1 = colpos - v[4], dy1 = rowpos - v[5];
+        const float A0 = v[0] * QCS_ASCALE, A1 = v[3] * QCS_ASCALE;
+        const float e0 = __expf(-(sum_of_products<DIST>(dx0, dx0, dy0, dy0)) * v[6] * QCS_SSCALE);
+        const float e1 = __expf(-(sum_of_products<DIST>(dx1, dx1, dy1, dy1)) * v[6] * QCS_SSCALE);
+        return sum_of_products<SUM2>(A0, e0, A1, e1) + v[7] * QCS_BSCALE;
+    } else if (KIND == k3E) {
+        const float dx0 = colpos - v[1], dy0 = rowpos - v[2];
+        const float dx1 = colpos - v[4], dy1 = rowpos - v[5];
+        const float dx2 = colpos - v[7], dy2 = rowpos - v[8];
+        const float A0 = v[0] * QCS_ASCALE, A1 = v[3] * QCS_ASCALE, A2 = v[6] * QCS_ASCALE;
+        const float e0 = __expf(-(sum_of_products<DIST>(dx0, dx0, dy0, dy0)) * v[9] * QCS_SSCALE);
+        const float e1 = __expf(-(sum_of_products<DIST>(dx1, dx1, dy1, dy1)) * v[9] * QCS_SSCALE);
+        const float e2 = __expf(-(sum_of_products<DIST>(dx2, dx2, dy2, dy2)) * v[9] * QCS_SSCALE);
+        return sum_of_products<SUM2>(A0, e0, A1, e1) + A2 * e2 + v[10] * QCS_BSCALE;
+    } else {  // kAS3D2E
+        const float dx0 = colpos - v[1], dy0 = rowpos - v[2];
+        const float dx1 = colpos - v[6], dy1 = rowpos - v[7];
+        const float A0 = v[0] * QCS_ASCALE, A1 = v[5] * QCS_ASCALE;
+        const float e0 = __expf(-(sum_of_products<DIST>(dx0 * dx0 * v[3], QCS_SSCALE, dy0 * dy0 * v[4], QCS_SSCALE)));
+        const float e1 = __expf(-(sum_of_products<DIST>(dx1 * dx1 * v[8], QCS_SSCALE, dy1 * dy1 * v[9], QCS_SSCALE)));
+        return sum_of_products<SUM2>(A0, e0, A1, e1) + v[10] * QCS_BSCALE;
+    }
+}
+
+// Unweighted Poisson log-likelihood of the model at the fitted parameters Ininf
+// over pixels k0, k0 + step, ... of the ROI (pixel k's (value, log) pair at
+// img[k * ld]): sum n ln(mu) - mu, accumulated in FP64 (the data's ln n!
+// term is common to every model of the ROI and left out).  The parameters are
+// clamped as the loss clamps them.
+template <int R, int KIND, int DIST, int SUM2>
+__device__ __forceinline__ double model_loglik(const float2 *img, int ld, const float *Ininf, int k0, int step) {
+    typedef KindTraits<KIND> T;
+    float v[T::P];
+#pragma unroll
+    for (int k = 0; k < T::P; k++) v[k] = T::CLAMP001 ? fmaxf(Ininf[k], 0.01f) : fmaxf(Ininf[k], 0.0f);
+    double s = 0.0;
+    for (int k = k0; k < R * R; k += step) {
+        const int row = k / R, col = k - (k / R) * R;
+        const double mu = (double)model_value<KIND, DIST, SUM2>(col + 0.5f, row + 0.5f, v);
+        s += (double)img[k * ld].x * log(mu) - mu;
+    }
+    return s;
+}
+
 // ------------------------------------------ staged single-emitter eval ---
 // The weighted-MLE mask of an R x R ROI depends on |col - R/2| and
 // |row - R/2| only: its exponent holds the squared distances of the pixel

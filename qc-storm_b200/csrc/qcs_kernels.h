@@ -19,6 +19,10 @@ struct FitLaunch {
     MultiOut mo;           // multi-emitter kinds: per-slot result + second-emitter row
     CorePara para;
     cudaStream_t stream;
+    // when set: the unweighted Poisson log-likelihood sum(n ln mu - mu) of the
+    // fitted model, FP64, per record id (one-thread and multi-emitter group
+    // kernels; the likelihood-ratio model selection)
+    double *ll = nullptr;
 };
 
 // kind: FitKind (qcs_fit_math.cuh); R: ROI size.

@@ -41,6 +41,8 @@ _SIGS = {
     "qcs_fit_single_device": (C.c_int, [C.c_int, C.POINTER(LocPara), C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
                                         C.c_void_p]),
     "qcs_crlb_device": (C.c_int, [C.POINTER(LocPara), C.c_void_p, C.c_int, C.c_void_p]),
+    "qcs_loc_set_model_selection": (C.c_int, [C.c_void_p, C.c_int, C.c_float]),
+    "qcs_loc_model_selection": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_float)]),
     "qcs_crlb_fisher_fp64": (C.c_int, [C.POINTER(LocPara), C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p,
                                        C.c_void_p]),
     "qcs_fit_single_group_device": (C.c_int, [C.c_int, C.POINTER(LocPara), C.c_void_p, C.c_void_p, C.c_int,
@@ -241,6 +243,18 @@ class LocContext:
         out = np.zeros((rois.shape[0], 6), np.float32)
         check(self.lib.qcs_wle_estimate(self.h, pr, rois.shape[0], C.byref(para), C.c_void_p(out.ctypes.data)))
         return out
+
+    def set_model_selection(self, mode="lr", threshold=0.0):
+        """Multi-emitter model selection: "cascade" (the reference's, default)
+        or "lr" (FP64 likelihood-ratio test over 1, 2, 3 emitter fits)."""
+        if mode not in ("cascade", "lr"):
+            raise ValueError("mode: 'cascade' or 'lr'")
+        check(self.lib.qcs_loc_set_model_selection(self.h, 1 if mode == "lr" else 0, C.c_float(threshold)))
+
+    def model_selection(self):
+        m, t = C.c_int(0), C.c_float(0)
+        check(self.lib.qcs_loc_model_selection(self.h, C.byref(m), C.byref(t)))
+        return ("lr" if m.value == 1 else "cascade"), t.value
 
     def localize_async(self, h_rois_ptr, n, h_wle_ptr=0, stream=0, para=None, net=None, iters=2, dev_th=0.0,
                        bisections=0):

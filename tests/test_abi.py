@@ -79,3 +79,9 @@ def test_noalloc_argument_checks_before_device():
     assert L.qcs_localize_noalloc(C.byref(p), *args, 16, C.c_void_p(20), None, None) == 1  # unaligned rows
     p.QE = 0.0
     assert L.qcs_localize_noalloc(C.byref(p), *args, 16, C.c_void_p(16), None, None) == 1  # QE
+
+
+def test_model_selection_needs_a_context():
+    L = qlib.load()
+    assert L.qcs_loc_set_model_selection(None, 1, 0.0) == 1
+    assert L.qcs_loc_model_selection(None, None, None) == 1
