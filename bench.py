@@ -712,6 +712,17 @@ SHAPE_TRAIN = 200_000
 SHAPE_STEPS = 20
 
 
+def emitter_confusion(rows, truth, n, first_frame=1):
+    """Localizations per record (its own row, plus an appended second
+    emitter) against the generator's emitter count: 3 x 3 counts."""
+    count = (rows[:n, 0] > 0).astype(np.int64)
+    extra = rows[n:, 11].astype(np.int64) - first_frame
+    count[extra[(extra >= 0) & (extra < n)]] += 1
+    conf = np.zeros((3, 3), np.int64)
+    np.add.at(conf, (truth["k"] - 1, np.minimum(count, 2)), 1)
+    return conf.tolist()
+
+
 def multi_truth_match(rows, rec, truth, R, first_frame=1):
     """Each localization's distance (px) to the nearest true emitter of its
     record (record = frame - first_frame), in ROI coordinates."""
@@ -899,6 +910,28 @@ def learned_shapes_measure(streams, dist, world, rank, mufu_peak=None, cpu_basel
             out[kind]["with_two_emitter_starts"] = two
         if roof is not None:
             out[kind]["plain_roofline"] = roof
+        if kind == "multi":
+            # the FP64 likelihood-ratio model selection on the same records, against the reference's cascade:
+            # fits/s and localizations per record against the generator's emitter count
+            for c in ctxs:
+                c.set_model_selection("lr")
+            lr_th = ctxs[0].model_selection()[1]
+            ms_lr = device_timed(SHAPE_STEPS, 3, plain, streams, dist)
+            plain(0, s0, ctxs[0])
+            rows_lr, ratios_lr = ctxs[0].read_rows(sh)
+            for c in ctxs:
+                c.set_model_selection("cascade")
+            out[kind]["lr_selection"] = {
+                "fits_per_s": job_rate(SHAPE_STEPS, SHAPE_RECORDS, world, ms_lr), "vs_cascade": ms_p / ms_lr,
+                "threshold": lr_th,
+                "kept_1_2_3_emitters": [float(x) for x in ratios_lr[3:6]],
+                "localizations_per_record_by_true_count": {
+                    "cascade": emitter_confusion(rows_p, truths[0], SHAPE_RECORDS),
+                    "lr": emitter_confusion(rows_lr, truths[0], SHAPE_RECORDS)},
+                "accuracy": {"cascade": multi_truth_match(rows_p, recs[0], truths[0], R),
+                             "lr": multi_truth_match(rows_lr, recs[0], truths[0], R)},
+                "basis": "rows: true emitters 1..3, columns: localizations 0..2 (at most two per record, as the "
+                         "reference writes them)"}
         if cpu_baseline and rank == 0:
             out[kind]["cpu_baseline"] = shape_cpu_baseline(kind, R, 1500 if kind == "as3d" else 600)
         for c in ctxs:
