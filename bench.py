@@ -890,6 +890,16 @@ def learned_shapes_measure(streams, dist, world, rank, mufu_peak=None, cpu_basel
                                   "accuracy": multi_truth_match(rows_l3, recs[0], truths[0], R)}
             net.set_two_emitter(None)
             net2.close()
+            # poor bright single fits straight to the two-emitter fit (no plain refit first)
+            net.set_direct_two_emitter(True)
+            ms_d = device_timed(SHAPE_STEPS, 3, learned, streams, dist)
+            learned(0, s0, ctxs[0])
+            rows_d, _ = ctxs[0].read_rows(sh)
+            net.set_direct_two_emitter(False)
+            two["direct_two_emitter"] = {"learned_fits_per_s": job_rate(SHAPE_STEPS, SHAPE_RECORDS, world, ms_d),
+                                         "vs_plain": ms_p / ms_d,
+                                         "accuracy": multi_truth_match(rows_d, recs[0], truths[0], R),
+                                         "note": "without the two-emitter starts; qcs_learned_set_direct_two_emitter"}
         out[kind] = {
             "workload": ("astigmatic 3D 9x9 ROIs, z U(-600,600) nm, photons log-U[1000,8000], background U(20,150), "
                          "camera ADU (offset 100, 0.45 e-/ADU)" if kind == "as3d" else
@@ -1069,7 +1079,7 @@ def mixed_measure(streams, dist, world, rank):
         if kind == "multi":
             net.set_count_threshold(0.5)
             net2 = train_two_emitter_net(ctx_tr, para, d_tr, feat, scale, n_train[i], R, MIXED_EPOCHS, s0)
-            net.set_two_emitter(net2, iters=TWO_ITERS, bisections=6)
+            net.set_two_emitter(net2, iters=TWO_ITERS, bisections=6, fallback="plain")
         torch.cuda.synchronize()
         ctx_tr.close()
         del d_tr, feat, scale, tgt, valid, labels

@@ -566,6 +566,14 @@ float qcs_learned_count_threshold(const qcs_learned_net *net);
  * three-emitter fit, as the reference's rejected two-emitter fits do
  * (fallback QCS_TWO_FALLBACK_3E), or are fitted again by the reference's
  * two-emitter fit (QCS_TWO_FALLBACK_PLAIN: one more pass of that fit). */
+/* Multi-emitter learned calls: a learned single-emitter fit that is rejected
+ * or judged poor by the deviance bound and has SNR > 6 goes straight to the
+ * two-emitter fit (the reference's rule for its rejected single fits, applied
+ * to the learned fit) instead of being refitted plainly first (on != 0; GS2D
+ * networks; default off).  More localizations and lower RMSE on records with
+ * several emitters, at the cost of a longer two-emitter queue.  No
+ * counterpart in the reference. */
+int qcs_learned_set_direct_two_emitter(qcs_learned_net *net, int on);
 #define QCS_TWO_FALLBACK_3E 0
 #define QCS_TWO_FALLBACK_PLAIN 1
 int qcs_learned_set_two_emitter(qcs_learned_net *net, qcs_learned_net *two, int iters, int bisections,

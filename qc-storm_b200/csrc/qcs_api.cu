@@ -397,9 +397,13 @@ __global__ void two_targets_kernel(qcs::CascadeState st, const uint16_t *__restr
 // single queue, a plain refit of the fits it flags (which also flags the
 // rejects that go on to the 2E fit), then the reference's 2E / 3E stages and
 // the CRLB.
+// direct2e (qcs_learned_set_direct_two_emitter, network-driven calls only):
+// bright ROIs whose learned single fit is rejected or judged poor go straight
+// to the two-emitter stage, without a plain refit first; otherwise every
+// flagged fit is refitted plainly, which reproduces the reference's decisions.
 cudaError_t learned_multi(qcs_loc_data *c, const uint16_t *d_rois, const float *wle, const qcs_loc_para *p, int n,
                           const int *n_dev, const float *d_start, const uint8_t *cls, int iters, int bisections,
-                          float dev_th, cudaStream_t s) {
+                          float dev_th, cudaStream_t s, bool direct2e = false) {
     qcs::CascadeArgs a;
     a.para = *p;
     a.rois = d_rois;
@@ -414,6 +418,7 @@ cudaError_t learned_multi(qcs_loc_data *c, const uint16_t *d_rois, const float *
     cudaError_t e;
     if ((e = qcs::cascade_classify(a, c->st)) != cudaSuccess) return e;
     qcs::FitLaunch f = qcs::cascade_single_launch(a, c->st);
+    f.direct2e = direct2e ? 1 : 0;
     if ((e = cudaMemsetAsync(c->d_refit, 0, (size_t)n, s)) != cudaSuccess) return e;
     const int R = p->ROISize;
     if ((e = qcs::launch_fit_learned(qcs::kGS2D, R, iters, bisections, f, d_start, dev_th, c->d_refit)) != cudaSuccess)
@@ -421,7 +426,9 @@ cudaError_t learned_multi(qcs_loc_data *c, const uint16_t *d_rois, const float *
     if ((e = qcs::launch_flag_queue(c->d_refit, n, c->q_refit, c->st.counters + qcs::kCntRefit, s)) != cudaSuccess)
         return e;
     f.q = qcs::Queue{c->q_refit, c->st.counters + qcs::kCntRefit, 0};
-    if ((e = qcs::launch_fit_group(qcs::kGS2D, R, 8, f)) != cudaSuccess) return e;
+    // multi-emitter records refit by the thousands (every poor single fit of a ROI with several emitters):
+    // a throughput-bound queue, one thread per ROI (the rows are the group kernel's bit for bit)
+    if ((e = qcs::launch_fit(qcs::kGS2D, R, f)) != cudaSuccess) return e;
     return qcs::cascade_tail(a, c->st);
 }
 
@@ -447,6 +454,10 @@ int two_emitter_starts(qcs_loc_data *c, const qcs_learned_net *net, const qcs_lo
     c->two = two;
     return QCS_OK;
 }
+
+int fit_from_start(qcs_loc_data *c, const uint16_t *d_rois, const float *d_wle, const qcs_loc_para *p, int n,
+                   const float *d_start, const uint8_t *d_classes, int iters, int bisections, float dev_th,
+                   void *stream, bool direct2e);
 }  // namespace
 
 extern "C" {
@@ -460,6 +471,17 @@ int qcs_fit_from_start_device(qcs_loc_data *c, const uint16_t *d_rois, const flo
 int qcs_fit_from_start_classes_device(qcs_loc_data *c, const uint16_t *d_rois, const float *d_wle,
                                       const qcs_loc_para *p, int n, const float *d_start, const uint8_t *d_classes,
                                       int iters, int bisections, float dev_th, void *stream) {
+    return fit_from_start(c, d_rois, d_wle, p, n, d_start, d_classes, iters, bisections, dev_th, stream, false);
+}
+
+}  // extern "C"
+
+namespace {
+// qcs_fit_from_start_classes_device; direct2e as in learned_multi (on for the
+// network-driven calls)
+int fit_from_start(qcs_loc_data *c, const uint16_t *d_rois, const float *d_wle, const qcs_loc_para *p, int n,
+                   const float *d_start, const uint8_t *d_classes, int iters, int bisections, float dev_th,
+                   void *stream, bool direct2e) {
     int st = check_call(c, p, n);
     if (st) return st;
     const int kind = learned_kind(p);
@@ -478,7 +500,8 @@ int qcs_fit_from_start_classes_device(qcs_loc_data *c, const uint16_t *d_rois, c
         wle = c->d_wle;
     }
     if (p->MultiEmitterFitEn) {
-        QCS_CUDA(learned_multi(c, d_rois, wle, p, n, nullptr, d_start, d_classes, iters, bisections, dev_th, s),
+        QCS_CUDA(learned_multi(c, d_rois, wle, p, n, nullptr, d_start, d_classes, iters, bisections, dev_th, s,
+                               direct2e),
                  "learned multi-emitter localization");
         return QCS_OK;
     }
@@ -517,6 +540,9 @@ int qcs_fit_from_start_classes_device(qcs_loc_data *c, const uint16_t *d_rois, c
     QCS_CUDA(cudaStreamWaitEvent(s, c->ev_join, 0), "join");
     return QCS_OK;
 }
+}  // namespace
+
+extern "C" {
 
 int qcs_learned_localize_device(qcs_loc_data *c, qcs_learned_net *net, const uint16_t *d_rois, const float *d_wle,
                                 const qcs_loc_para *p, int n, int iters, int bisections, float dev_th, void *stream) {
@@ -536,7 +562,8 @@ int qcs_learned_localize_device(qcs_loc_data *c, qcs_learned_net *net, const uin
     QCS_CUDA(qcs::learned::start_points(net, p, d_rois, n, c->d_start, s, cls), "learned start points");
     qcs::TwoEmitterStart two;
     if (p->MultiEmitterFitEn && (st = two_emitter_starts(c, net, p, d_rois, n, nullptr, s, &two)) != QCS_OK) return st;
-    st = qcs_fit_from_start_classes_device(c, d_rois, d_wle, p, n, c->d_start, cls, iters, bisections, dev_th, s);
+    st = fit_from_start(c, d_rois, d_wle, p, n, c->d_start, cls, iters, bisections, dev_th, s,
+                        qcs::learned::direct_two_emitter(net));
     c->two = nullptr;
     return st;
 }
@@ -564,7 +591,9 @@ int qcs_learned_localize_device_n(qcs_loc_data *c, qcs_learned_net *net, const u
     QCS_CUDA(qcs::learned::start_points(net, p, d_rois, max_n, c->d_start, s, cls, d_n), "learned start points");
     qcs::TwoEmitterStart two;
     if ((st = two_emitter_starts(c, net, p, d_rois, max_n, d_n, s, &two)) != QCS_OK) return st;
-    const cudaError_t e = learned_multi(c, d_rois, d_wle, p, max_n, d_n, c->d_start, cls, iters, bisections, dev_th, s);
+    const cudaError_t e =
+        learned_multi(c, d_rois, d_wle, p, max_n, d_n, c->d_start, cls, iters, bisections, dev_th, s,
+                      qcs::learned::direct_two_emitter(net));
     c->two = nullptr;
     QCS_CUDA(e, "learned multi-emitter localization");
     return QCS_OK;

@@ -391,6 +391,8 @@ cudaError_t run_cascade_lr(const CascadeArgs &a, const CascadeState &st, const L
     f.stream = a.stream;
     f.ll = lr.ll1;
     if ((e = launch_fit(kGS2D, R, f)) != cudaSuccess) return e;
+    // every record goes through the 2E and 3E fits: throughput-bound queues, one thread per ROI
+    f.thread_per_roi = 1;
     f.loc = lr.loc2;
     f.mo = MultiOut{st.res2, st.extra2};
     f.ll = lr.ll2;

@@ -536,7 +536,8 @@ __global__ void __launch_bounds__(kTPB) fit_learned_kernel(const uint16_t *__res
                                                            const float *__restrict__ wle,
                                                            const float *__restrict__ start, Queue q,
                                                            float *__restrict__ loc, uint8_t *__restrict__ refit,
-                                                           uint8_t *__restrict__ to2e, CorePara c, float dev_th) {
+                                                           uint8_t *__restrict__ to2e, CorePara c, float dev_th,
+                                                           int direct2e) {
     typedef SmemLayout<R, KIND> L;
     enum { P = KindTraits<KIND>::P, PIX = R * R, WHOLE = R * (R + 1) };
     typedef typename std::conditional<KIND == kGS2D, AnalyticEvalGS2D<R, DIST>, AnalyticEvalAS3D<R, DIST>>::type Eval;
@@ -592,7 +593,15 @@ __global__ void __launch_bounds__(kTPB) fit_learned_kernel(const uint16_t *__res
             dev += single_term<KIND>(e, Ininf, pl.x, pl.y);
         }
     dev *= 2.0f;
-    refit[id] = (!accepted || !(dev <= dev_th)) ? 1 : 0;
+    const bool poor = !accepted || !(dev <= dev_th);
+    if (direct2e && to2e && poor && IsFittingValid && CurSNR > 6.0f) {
+        // a bright ROI the single model does not fit: on to the two-emitter fit
+        refit[id] = 0;
+        to2e[id] = 1;
+        zero_row(loc, id);
+        return;
+    }
+    refit[id] = poor ? 1 : 0;
     if (to2e) to2e[id] = 0;  // a kept fit is final; a refit sets the flag again
     if (accepted)
         store_row(loc, id, row);
@@ -608,7 +617,7 @@ cudaError_t launch_learned(const FitLaunch &a, const float *start, float dev_th,
     if (e != cudaSuccess) return e;
     const int grid = (a.max_count + kTPB - 1) / kTPB;
     if (grid == 0) return cudaSuccess;
-    k<<<grid, kTPB, smem, a.stream>>>(a.rois, a.wle, start, a.q, a.loc, refit, a.to2e, a.para, dev_th);
+    k<<<grid, kTPB, smem, a.stream>>>(a.rois, a.wle, start, a.q, a.loc, refit, a.to2e, a.para, dev_th, a.direct2e);
     return cudaGetLastError();
 }
 
@@ -625,18 +634,6 @@ __global__ void flag_queue_kernel(const uint8_t *__restrict__ flags, int n, int 
     if (lane == 0 && ballot) base = atomicAdd(count, __popc(ballot));
     base = __shfl_sync(0xffffffffu, base, 0);
     if (f) ids[base + __popc(ballot & ((1u << lane) - 1u))] = i;
-}
-
-template <int R, int ITERS, int NB>
-cudaError_t launch_learned(const FitLaunch &a, const float *start, float dev_th, uint8_t *refit) {
-    const size_t smem = SmemLayout<R, kGS2D>::TOTAL * sizeof(float);
-    auto k = fit_learned_kernel<R, ITERS, NB>;
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    const int grid = (a.max_count + kTPB - 1) / kTPB;
-    if (grid == 0) return cudaSuccess;
-    k<<<grid, kTPB, smem, a.stream>>>(a.rois, a.wle, start, a.q, a.loc, refit, a.to2e, a.para, dev_th);
-    return cudaGetLastError();
 }
 
 // -------------------------------------------------------- multi emitter ---
@@ -858,11 +855,12 @@ template <int R, int KIND, int DIST = ArithSpec<KIND, R>::DIST, int MASK = Arith
 __global__ void __launch_bounds__(kTPB) fit_multi_kernel(const uint16_t *__restrict__ rois,
                                                          const float *__restrict__ wle, Queue q,
                                                          float *__restrict__ loc, MultiOut mo, CorePara c,
-                                                         double *__restrict__ ll) {
+                                                         double *__restrict__ ll, int min_n) {
     typedef SmemLayout<R, KIND> L;
     enum { P = KindTraits<KIND>::P, PIX = R * R, WHOLE = R * (R + 1) };
     extern __shared__ float smem[];
     const int n = queue_len(q);
+    if (n <= min_n) return;  // a queue this short is the lane-group kernel's
     const int base = blockIdx.x * kTPB;
     if (base >= n) return;
     const int cnt = min(kTPB, n - base);
@@ -923,7 +921,7 @@ template <int R, int KIND, int DIST = ArithSpec<KIND, R>::DIST, int MASK = Arith
 __global__ void __launch_bounds__(kGroupTPB) fit_multi_group_kernel(const uint16_t *__restrict__ rois,
                                                                     const float *__restrict__ wle, Queue q,
                                                                     float *__restrict__ loc, MultiOut mo,
-                                                                    CorePara c, double *__restrict__ ll) {
+                                                                    CorePara c, double *__restrict__ ll, int max_n) {
     typedef MultiGroupLayout<R, KIND> L;
     enum { G = multi_lanes(KIND), P = KindTraits<KIND>::P, PIX = R * R, PIXP = L::PIXP, WHOLE = R * (R + 1),
            SLOTS = L::SLOTS };
@@ -931,6 +929,7 @@ __global__ void __launch_bounds__(kGroupTPB) fit_multi_group_kernel(const uint16
                                                           "roundings fixed in the source");
     extern __shared__ __align__(16) float smem[];
     const int n = queue_len(q);
+    if (n > max_n) return;  // a longer queue is the one-thread-per-ROI kernel's
     const int base = blockIdx.x * SLOTS;
     if (base >= n) return;
     const int cnt = min(SLOTS, n - base);
@@ -1138,29 +1137,56 @@ cudaError_t launch_single_group(const FitLaunch &a) {
     return cudaGetLastError();
 }
 
+// Queue lengths up to which the lane-group kernel fits a multi-emitter stage:
+// about three waves of the ROIs it holds at once.  Beyond that the lanes'
+// repeated pixel sums cost more than the latency they save, and the
+// one-thread-per-ROI kernel (whose single wave holds far more ROIs) is faster.
+template <int R, int KIND>
+int group_queue_limit() {
+    static int limit = -2;
+    if (limit == -2) {
+        typedef MultiGroupLayout<R, KIND> L;
+        int dev = 0, sms = 0, blocks = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaFuncSetAttribute(fit_multi_group_kernel<R, KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(L::TOTAL * sizeof(float)));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, fit_multi_group_kernel<R, KIND>, kGroupTPB,
+                                                      L::TOTAL * sizeof(float));
+        limit = 3 * sms * (blocks > 0 ? blocks : 1) * L::SLOTS;
+    }
+    return limit;
+}
+
+// Both kernels are launched; each reads the stage's queue length on the
+// device and only one of them fits it (no host synchronisation).
 template <int R, int KIND>
 cudaError_t launch_multi(const FitLaunch &a) {
+    int min_n = -1;
     if constexpr (multi_group_supported(KIND, R)) {
-        // G lanes per ROI: the same rows bit for bit, a fraction of the latency
-        typedef MultiGroupLayout<R, KIND> L;
-        const size_t smem = L::TOTAL * sizeof(float);
-        auto k = fit_multi_group_kernel<R, KIND>;
-        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        const int grid = (a.max_count + L::SLOTS - 1) / L::SLOTS;
-        if (grid == 0) return cudaSuccess;
-        k<<<grid, kGroupTPB, smem, a.stream>>>(a.rois, a.wle, a.q, a.loc, a.mo, a.para, a.ll);
-        return cudaGetLastError();
-    } else {
-        const size_t smem = SmemLayout<R, KIND>::TOTAL * sizeof(float);
-        auto k = fit_multi_kernel<R, KIND>;
-        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        const int grid = (a.max_count + kTPB - 1) / kTPB;
-        if (grid == 0) return cudaSuccess;
-        k<<<grid, kTPB, smem, a.stream>>>(a.rois, a.wle, a.q, a.loc, a.mo, a.para, a.ll);
-        return cudaGetLastError();
+        if (!a.thread_per_roi) {
+            typedef MultiGroupLayout<R, KIND> L;
+            const size_t smem = L::TOTAL * sizeof(float);
+            auto k = fit_multi_group_kernel<R, KIND>;
+            cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+            min_n = group_queue_limit<R, KIND>();
+            const int grid = (min(a.max_count, min_n) + L::SLOTS - 1) / L::SLOTS;
+            if (grid > 0) {
+                k<<<grid, kGroupTPB, smem, a.stream>>>(a.rois, a.wle, a.q, a.loc, a.mo, a.para, a.ll, min_n);
+                if ((e = cudaGetLastError()) != cudaSuccess) return e;
+            }
+            if (a.max_count <= min_n) return cudaSuccess;  // the queue cannot outgrow the group kernel
+        }
     }
+    const size_t smem = SmemLayout<R, KIND>::TOTAL * sizeof(float);
+    auto k = fit_multi_kernel<R, KIND>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const int grid = (a.max_count + kTPB - 1) / kTPB;
+    if (grid == 0) return cudaSuccess;
+    k<<<grid, kTPB, smem, a.stream>>>(a.rois, a.wle, a.q, a.loc, a.mo, a.para, a.ll, min_n);
+    return cudaGetLastError();
 }
 
 }  // namespace

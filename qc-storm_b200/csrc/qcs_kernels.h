@@ -23,6 +23,15 @@ struct FitLaunch {
     // fitted model, FP64, per record id (one-thread and multi-emitter group
     // kernels; the likelihood-ratio model selection)
     double *ll = nullptr;
+    // learned-start single fits with multi-emitter fitting (to2e set): a fit
+    // that is rejected or judged poor and has SNR > 6 goes straight to the
+    // two-emitter queue (the reference's rule for rejected single fits) instead
+    // of a plain refit; fits with SNR <= 6 are still refitted
+    int direct2e = 0;
+    // multi-emitter kinds: the one-thread-per-ROI kernel even where the lane-group
+    // kernel exists (queues of every record, where throughput, not one ROI's
+    // latency, sets the time)
+    int thread_per_roi = 0;
 };
 
 // kind: FitKind (qcs_fit_math.cuh); R: ROI size.

@@ -718,6 +718,7 @@ struct qcs_learned_net {
     // GS2D networks: the two-emitter network whose start points the 2E stage uses, and its schedule
     qcs_learned_net *two = nullptr;
     int owners = 0;  // GS2D networks this (two-emitter) network is attached to
+    int direct_2e = 0;  // multi-emitter calls: poor bright single fits straight to the 2E stage
     int two_iters = 3, two_bisections = 6, two_to3e = 1;
     float two_dev_th = 0.0f;
     int kin = 64;                     // input width: in_width(R)
@@ -922,6 +923,8 @@ int check_shape(const qcs_learned_net *net, const qcs_loc_para *p) {
 
 namespace qcs {
 namespace learned {
+bool direct_two_emitter(const qcs_learned_net *net) { return net && net->direct_2e; }
+
 qcs_learned_net *two_emitter(const qcs_learned_net *net, int *iters, int *bisections, float *dev_th, int *to3e) {
     if (!net || !net->two) return nullptr;
     *to3e = net->two_to3e;
@@ -1287,6 +1290,13 @@ int qcs_learned_set_two_emitter(qcs_learned_net *net, qcs_learned_net *two, int 
     net->two_iters = iters;
     net->two_bisections = bisections;
     net->two_dev_th = dev_th;
+    return QCS_OK;
+}
+
+int qcs_learned_set_direct_two_emitter(qcs_learned_net *net, int on) {
+    if (!net) return fail(QCS_ERR_ARG, "null network");
+    if (on && net->loc_type != QCS_LOCTYPE_GS2D) return fail(QCS_ERR_ARG, "direct two-emitter routing: GS2D networks");
+    net->direct_2e = on ? 1 : 0;
     return QCS_OK;
 }
 

@@ -71,5 +71,7 @@ cudaError_t start_points(qcs_learned_net *net, const qcs_loc_para *p, const uint
 // The two-emitter network attached to a GS2D network (qcs_learned_set_two_emitter),
 // its schedule and fallback (to3e: poor fits go on to the three-emitter fit), or null.
 qcs_learned_net *two_emitter(const qcs_learned_net *net, int *iters, int *bisections, float *dev_th, int *to3e);
+// qcs_learned_set_direct_two_emitter's setting
+bool direct_two_emitter(const qcs_learned_net *net);
 }  // namespace learned
 }  // namespace qcs

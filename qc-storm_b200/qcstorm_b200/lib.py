@@ -126,6 +126,7 @@ _SIGS = {
     "qcs_loc_count_labels_device": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "qcs_learned_set_count_threshold": (C.c_int, [C.c_void_p, C.c_float]),
     "qcs_learned_set_two_emitter": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_int]),
+    "qcs_learned_set_direct_two_emitter": (C.c_int, [C.c_void_p, C.c_int]),
     "qcs_learned_refit_2e_num": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "qcs_loc_two_emitter_targets_device": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(LocPara), C.c_int, C.c_void_p,
                                                      C.c_void_p, C.c_void_p, C.c_void_p]),
@@ -614,6 +615,10 @@ class LearnedNet:
         check(self.lib.qcs_learned_set_two_emitter(self.h, two.h if two is not None else None, int(iters),
                                                    int(bisections), C.c_float(dev_th), 0 if fallback == "3e" else 1))
         self._two = two
+
+    def set_direct_two_emitter(self, on=True):
+        """Multi-emitter calls: poor bright single fits straight to the two-emitter fit."""
+        check(self.lib.qcs_learned_set_direct_two_emitter(self.h, 1 if on else 0))
 
     def refits_2e(self, ctx):
         k = C.c_int(0)
