@@ -626,6 +626,8 @@ def learned_measure(args, streams, ctxs, para, d_batches, h_batches, rec0, truth
     stream, ctx = streams[0], ctxs[0]
     sh = stream.cuda_stream
     net, train = train_learned_net(para, stream)
+    # the iteration cap the tuner picks on these records (informational; the timed schedule is fixed)
+    tuned_schedule = net.autotune(ctx, d_batches[0].data_ptr(), N_PER_STEP, stream=sh)
 
     def step(k, s, c=None):
         net.localize(c or ctxs[k % 2], d_batches[k % BATCHES].data_ptr(), N_PER_STEP, 0, iters=LEARNED_ITERS,
@@ -683,6 +685,9 @@ def learned_measure(args, streams, ctxs, para, d_batches, h_batches, rec0, truth
         "windows": windows,
         "value_one_stream": value1, "timing": "two contexts in turn on two streams (value_one_stream: one)",
         "iters": LEARNED_ITERS, "bisections": LEARNED_BISECTIONS, "refits_per_step": refits,
+        "autotuned_schedule": {"iters": tuned_schedule[0], "bisections": tuned_schedule[1],
+                               "rule": "qcs_learned_autotune: fastest schedule with acceptance within 0.5 points of "
+                                       "the best"},
         # mlp_tc (features + network), WLE (5), fit_learned, flag_queue, group refit, refit CRLB, counters, CRLB
         "gpu_launches_per_step": 12,
         "e2e": {"value": e2e_steps * N_PER_STEP * world / e2e_s, "unit": UNIT,
@@ -1240,6 +1245,18 @@ def autotune_measure(stream, dist, world):
             torch.cuda.synchronize()
             res[name + "_ms"] = max_over_ranks(e0.elapsed_time(e1), dist) / 20
         out["call_%d_records" % m] = res
+    ctx.close()
+    # the multi-emitter stages: lane groups against one thread per ROI, by queue length (11x11, 1-3 emitters)
+    rec, para, _ = synth.multi_rois(50_000, R=11, seed=98)
+    d = torch.from_numpy(rec.view(np.int16)).cuda()
+    ctx = lib.LocContext(para, capacity=50_000)
+    wle = torch.from_numpy(ctx.wle(rec)).cuda()
+    torch.cuda.synchronize()
+    ctx.autotune(d.data_ptr(), wle.data_ptr(), 50_000, stream=sh)
+    l2, l3 = ctx.tuning_multi()
+    out["multi_emitter_11x11"] = {"lane_group_queue_limit_2e": l2, "lane_group_queue_limit_3e": l3,
+                                  "note": "longest stage queue for which the lane-group kernel beat one thread per "
+                                          "ROI on the caller's records (-1: never)"}
     ctx.close()
     return out
 

@@ -454,6 +454,23 @@ int qcs_loc_autotune(qcs_loc_data *c, const qcs_loc_para *p, const uint16_t *d_r
  * (count 0..8 entries of (largest batch, lanes 1 / 4 / 8 / 16); 0 clears it). */
 int qcs_loc_tuning(const qcs_loc_data *c, int *sizes, int *lanes, int max_entries);
 int qcs_loc_set_tuning(qcs_loc_data *c, const int *sizes, const int *lanes, int count);
+/* With multi-emitter fitting, qcs_loc_autotune also times each multi-emitter
+ * stage (2E or AS3D-2E, and 3E) on queues of the caller's first 64, 256,
+ * 1,024, ... records with the lane-group kernel and with one thread per ROI,
+ * and keeps the longest queue for which the lane groups are faster: a stage
+ * whose queue (read on the device) is at most that long uses them.  The
+ * limits (-1: one thread per ROI always; 0: the built-in default, about three
+ * waves of the lane-group kernel), read or set here.  The rows are the same
+ * either way. */
+int qcs_loc_tuning_multi(const qcs_loc_data *c, int *limit_2e, int *limit_3e);
+int qcs_loc_set_tuning_multi(qcs_loc_data *c, int limit_2e, int limit_3e);
+/* Per-GPU tuning cache: writes the context's tuning (lanes table and
+ * multi-emitter limits) to a text file tagged with the GPU's name, ROI size,
+ * localization type and multi-emitter setting; loading sets the context's
+ * tuning from such a file and refuses (QCS_ERR_STATE) one written for another
+ * GPU model or shape, so a caller tunes once per machine and reloads. */
+int qcs_loc_save_tuning(const qcs_loc_data *c, const char *path);
+int qcs_loc_load_tuning(qcs_loc_data *c, const char *path);
 /* Model selection of multi-emitter calls (no counterpart in the reference,
  * whose selection is its SNR / validity cascade, bfgsMLE_GS2D_core.h:279-298,
  * bfgsMLE_GS2D_2Emitter_core.h:296-348; QCS_SELECT_CASCADE, the default and
@@ -574,6 +591,15 @@ float qcs_learned_count_threshold(const qcs_learned_net *net);
  * several emitters, at the cost of a longer two-emitter queue.  No
  * counterpart in the reference. */
 int qcs_learned_set_direct_two_emitter(qcs_learned_net *net, int on);
+/* Iteration cap of the learned-start fits (no counterpart in the reference):
+ * runs qcs_learned_localize_device on the caller's n device records with
+ * every schedule compiled for the network's shape (BFGS iterations x
+ * line-search steps) and returns the fastest whose fraction of accepted
+ * records is within 0.5 points of the best schedule's (ground truth is not
+ * needed: a schedule too short for the data shows as rejected and refitted
+ * records).  Overwrites the context's rows; n >= 64. */
+int qcs_learned_autotune(qcs_loc_data *c, qcs_learned_net *net, const uint16_t *d_rois, const float *d_wle,
+                         const qcs_loc_para *p, int n, int *iters, int *bisections, void *stream);
 #define QCS_TWO_FALLBACK_3E 0
 #define QCS_TWO_FALLBACK_PLAIN 1
 int qcs_learned_set_two_emitter(qcs_learned_net *net, qcs_learned_net *two, int iters, int bisections,

@@ -77,6 +77,8 @@ struct qcs_loc_data {
     int tune_count = 0;
     int tune_n[8] = {0};
     int tune_lanes[8] = {0};
+    // tuned longest queues the lane-group multi-emitter kernels fit (2E / AS3D-2E, 3E; 0: their default)
+    int tune_limit2 = 0, tune_limit3 = 0;
     // model selection of multi-emitter calls: QCS_SELECT_CASCADE (the reference's) or QCS_SELECT_LR
     int sel_mode = QCS_SELECT_CASCADE;
     float sel_th = QCS_SELECT_LR_DEFAULT_TH;
@@ -296,6 +298,8 @@ int qcs_loc_localize_device(qcs_loc_data *c, const uint16_t *d_rois, const float
     a.max_rows = c->max_rows;
     a.stream = s;
     a.lanes = tuned_lanes(c, n);
+    a.group_limit2 = c->tune_limit2;
+    a.group_limit3 = c->tune_limit3;
     QCS_CUDA(run_localization(c, a), "localization cascade");
     return QCS_OK;
 }
@@ -315,6 +319,8 @@ int qcs_loc_localize_device_n(qcs_loc_data *c, const uint16_t *d_rois, const flo
     a.loc = c->d_loc;
     a.max_rows = c->max_rows;
     a.stream = s;
+    a.group_limit2 = c->tune_limit2;
+    a.group_limit3 = c->tune_limit3;
     QCS_CUDA(run_localization(c, a), "localization cascade");
     return QCS_OK;
 }
@@ -415,6 +421,8 @@ cudaError_t learned_multi(qcs_loc_data *c, const uint16_t *d_rois, const float *
     a.stream = s;
     a.pred = cls;
     a.two = c->two;
+    a.group_limit2 = c->tune_limit2;
+    a.group_limit3 = c->tune_limit3;
     cudaError_t e;
     if ((e = qcs::cascade_classify(a, c->st)) != cudaSuccess) return e;
     qcs::FitLaunch f = qcs::cascade_single_launch(a, c->st);
@@ -813,6 +821,63 @@ int qcs_loc_read_rows(qcs_loc_data *c, const qcs_loc_para *p, void *stream) {
     return QCS_OK;
 }
 
+int qcs_learned_autotune(qcs_loc_data *c, qcs_learned_net *net, const uint16_t *d_rois, const float *d_wle,
+                         const qcs_loc_para *p, int n, int *iters, int *bisections, void *stream) {
+    if (!iters || !bisections) return fail(QCS_ERR_ARG, "null output");
+    int st = check_call(c, p, n);
+    if (st) return st;
+    if (!net || !d_rois) return fail(QCS_ERR_ARG, "null argument");
+    if (n < 64) return fail(QCS_ERR_ARG, "autotuning needs at least 64 records");
+    const int kind = learned_kind(p);
+    if (kind < 0) return fail(QCS_ERR_ARG, kLearnedShapes);
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+    // every schedule compiled for the shape; the fastest whose acceptance stays within 0.5 points of the
+    // best schedule's (refits and rejected fits are what a too-short schedule costs)
+    const int sched[][2] = {{2, 4}, {2, 6}, {2, 8}, {3, 4}, {3, 6}, {3, 8}, {4, 6}, {2, 11}, {3, 11}, {4, 11}, {5, 11},
+                            {8, 11}};
+    float ms[12] = {0};
+    double acc[12] = {0};
+    bool ran[12] = {false};
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    QCS_CUDA(cudaEventCreate(&e0), "tuning events");
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return fail(QCS_ERR_CUDA, "tuning events");
+    }
+    int rc = QCS_OK;
+    for (int i = 0; i < 12 && rc == QCS_OK; ++i) {
+        const int it = sched[i][0], nb = sched[i][1];
+        if (!qcs::learned_schedule_supported(kind, p->ROISize, it, nb)) continue;
+        rc = qcs_learned_localize_device(c, net, d_rois, d_wle, p, n, it, nb, 0.0f, s);  // warm-up
+        if (rc == QCS_OK && cudaEventRecord(e0, s) != cudaSuccess) rc = fail(QCS_ERR_CUDA, "tuning");
+        for (int r = 0; r < 2 && rc == QCS_OK; ++r)
+            rc = qcs_learned_localize_device(c, net, d_rois, d_wle, p, n, it, nb, 0.0f, s);
+        if (rc == QCS_OK && (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                             cudaEventElapsedTime(&ms[i], e0, e1) != cudaSuccess))
+            rc = fail(QCS_ERR_CUDA, "tuning");
+        if (rc == QCS_OK) rc = qcs_loc_read_rows(c, p, s);
+        if (rc == QCS_OK) {
+            long kept = 0;
+            for (int r = 0; r < c->valid; ++r) kept += c->h_loc[(size_t)r * QCS_OUT_PARA_NUM] > 0.0f;
+            acc[i] = (double)kept / n;
+            ran[i] = true;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != QCS_OK) return rc;
+    double best_acc = 0;
+    for (int i = 0; i < 12; ++i)
+        if (ran[i] && acc[i] > best_acc) best_acc = acc[i];
+    int pick = -1;
+    for (int i = 0; i < 12; ++i)
+        if (ran[i] && acc[i] >= best_acc - 0.005 && (pick < 0 || ms[i] < ms[pick])) pick = i;
+    if (pick < 0) return fail(QCS_ERR_ARG, kLearnedSchedules);
+    *iters = sched[pick][0];
+    *bisections = sched[pick][1];
+    return QCS_OK;
+}
+
 const float *qcs_loc_h_loc_arry(const qcs_loc_data *c) { return c ? c->h_loc : nullptr; }
 int qcs_loc_valid_num(const qcs_loc_data *c) { return c ? c->valid : 0; }
 
@@ -908,7 +973,12 @@ int qcs_loc_autotune(qcs_loc_data *c, const qcs_loc_para *p, const uint16_t *d_r
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
     const int kind = p->LocType == QCS_LOCTYPE_AS3D ? qcs::kAS3D : qcs::kGS2D;
     c->tune_count = 0;
-    if (!qcs::group_fit_supported(kind, p->ROISize) || p->LocType == QCS_LOCTYPE_DH3D) return QCS_OK;
+    c->tune_limit2 = c->tune_limit3 = 0;
+    // the single-emitter lanes exist for the sizes with a lane-group kernel; the multi-emitter stages for GS2D
+    // and AS3D calls with multi-emitter fitting (DH3D has no two-emitter stage)
+    const bool single_ok = qcs::group_fit_supported(kind, p->ROISize) && p->LocType != QCS_LOCTYPE_DH3D;
+    const bool multi_ok = p->MultiEmitterFitEn && p->LocType != QCS_LOCTYPE_DH3D;
+    if (!single_ok && !multi_ok) return QCS_OK;
     // lanes per ROI to try: 1 (one thread per ROI) and 8; 4 and 16 exist for GS2D 7x7 only
     const int cand7[4] = {1, 4, 8, 16}, cand_other[2] = {1, 8};
     const bool gs7 = kind == qcs::kGS2D && p->ROISize == 7;
@@ -928,8 +998,10 @@ int qcs_loc_autotune(qcs_loc_data *c, const qcs_loc_para *p, const uint16_t *d_r
     f.para = qcs::core_para(q);
     f.stream = s;
     int sizes[8], k = 0;
-    for (int m = 256; m < n && k < 7; m *= 4) sizes[k++] = m;
-    sizes[k++] = n;
+    if (single_ok) {
+        for (int m = 256; m < n && k < 7; m *= 4) sizes[k++] = m;
+        sizes[k++] = n;
+    }
     for (int i = 0; i < k && e == cudaSuccess; ++i) {
         const int m = sizes[i];
         f.q = qcs::Queue{nullptr, nullptr, m};
@@ -956,13 +1028,121 @@ int qcs_loc_autotune(qcs_loc_data *c, const qcs_loc_para *p, const uint16_t *d_r
         c->tune_n[i] = m;  // batches above the largest tuned size keep one thread per ROI
         c->tune_lanes[i] = best_lanes;
     }
+    // Multi-emitter stages: the longest queue for which the lane-group kernel beats one thread per ROI,
+    // timed on queues of the caller's first m records (the rows are the same either way).
+    if (e == cudaSuccess && multi_ok) {
+        const int kinds[2] = {p->LocType == QCS_LOCTYPE_AS3D ? qcs::kAS3D2E : qcs::k2E,
+                              p->LocType == QCS_LOCTYPE_GS2D ? qcs::k3E : -1};
+        int *limits[2] = {&c->tune_limit2, &c->tune_limit3};
+        qcs::FitLaunch g;
+        g.rois = d_rois;
+        g.wle = d_wle;
+        g.loc = c->d_loc;
+        g.to2e = nullptr;
+        g.mo = qcs::MultiOut{c->st.res2, c->st.extra2};
+        g.para = qcs::core_para(*p);
+        g.stream = s;
+        for (int st2 = 0; st2 < 2 && e == cudaSuccess; ++st2) {
+            const int kind2 = kinds[st2];
+            *limits[st2] = 0;
+            if (kind2 < 0 || !qcs::multi_group_available(kind2, p->ROISize)) continue;
+            int limit = 0;
+            bool group_wins_all = true;
+            for (int m = 64; e == cudaSuccess; m *= 4) {
+                const int mm = m < n ? m : n;
+                g.q = qcs::Queue{nullptr, nullptr, mm};
+                g.max_count = mm;
+                float t[2] = {0, 0};
+                for (int mode = 0; mode < 2 && e == cudaSuccess; ++mode) {
+                    g.thread_per_roi = mode;           // 0: lane groups for any length, 1: one thread per ROI
+                    g.group_limit = mode ? 0 : (1 << 30);
+                    e = qcs::launch_fit(kind2, p->ROISize, g);  // warm-up
+                    if (e == cudaSuccess) e = cudaEventRecord(e0, s);
+                    for (int r = 0; r < 2 && e == cudaSuccess; ++r) e = qcs::launch_fit(kind2, p->ROISize, g);
+                    if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+                    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+                    if (e == cudaSuccess) e = cudaEventElapsedTime(&t[mode], e0, e1);
+                }
+                if (t[0] < t[1])
+                    limit = mm;
+                else
+                    group_wins_all = false;
+                if (!group_wins_all || mm == n) break;
+            }
+            // lane groups still ahead at the largest queue tried: keep the larger of it and the default
+            if (group_wins_all) {
+                const int d = qcs::multi_group_default_limit(kind2, p->ROISize);
+                limit = limit > d ? limit : d;
+            }
+            *limits[st2] = limit > 0 ? limit : -1;  // -1: always one thread per ROI
+        }
+    }
     if (e1) cudaEventDestroy(e1);
     cudaEventDestroy(e0);
     if (e != cudaSuccess) {
         c->tune_count = 0;
+        c->tune_limit2 = c->tune_limit3 = 0;
         return fail(QCS_ERR_CUDA, "autotuning", e);
     }
     c->tune_count = k;
+    return QCS_OK;
+}
+
+// the current GPU's name with blanks as underscores (the cache's tag)
+static std::string gpu_tag() {
+    int dev = 0;
+    cudaDeviceProp prop;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return "unknown";
+    std::string name(prop.name);
+    for (char &ch : name)
+        if (ch == ' ' || ch == '\t' || ch == '\n') ch = '_';
+    return name;
+}
+
+int qcs_loc_save_tuning(const qcs_loc_data *c, const char *path) {
+    if (!c || !path) return fail(QCS_ERR_ARG, "null argument");
+    FILE *f = fopen(path, "w");
+    if (!f) return fail(QCS_ERR_ARG, "cannot open the tuning file for writing");
+    fprintf(f, "qcstorm_b200_tuning 1\ngpu %s\nroi_size %d\nloc_type %d\nmulti %d\nlanes %d", gpu_tag().c_str(),
+            c->para.ROISize, c->para.LocType, c->para.MultiEmitterFitEn, c->tune_count);
+    for (int i = 0; i < c->tune_count; ++i) fprintf(f, " %d %d", c->tune_n[i], c->tune_lanes[i]);
+    fprintf(f, "\nlimits %d %d\n", c->tune_limit2, c->tune_limit3);
+    const bool ok = fclose(f) == 0;
+    return ok ? QCS_OK : fail(QCS_ERR_ARG, "writing the tuning file failed");
+}
+
+int qcs_loc_load_tuning(qcs_loc_data *c, const char *path) {
+    if (!c || !path) return fail(QCS_ERR_ARG, "null argument");
+    FILE *f = fopen(path, "r");
+    if (!f) return fail(QCS_ERR_ARG, "cannot open the tuning file");
+    char gpu[256] = {0};
+    int version = 0, R = 0, lt = 0, multi = 0, count = 0, sizes[8], lanes[8], l2 = 0, l3 = 0;
+    bool ok = fscanf(f, " qcstorm_b200_tuning %d gpu %255s roi_size %d loc_type %d multi %d lanes %d", &version, gpu,
+                     &R, &lt, &multi, &count) == 6 &&
+              version == 1 && count >= 0 && count <= 8;
+    for (int i = 0; ok && i < count; ++i) ok = fscanf(f, " %d %d", &sizes[i], &lanes[i]) == 2;
+    ok = ok && fscanf(f, " limits %d %d", &l2, &l3) == 2;
+    fclose(f);
+    if (!ok) return fail(QCS_ERR_ARG, "not a tuning file");
+    if (gpu_tag() != gpu || R != c->para.ROISize || lt != c->para.LocType || multi != c->para.MultiEmitterFitEn)
+        return fail(QCS_ERR_STATE, "the tuning file was written for another GPU model or ROI shape");
+    int st = qcs_loc_set_tuning(c, sizes, lanes, count);
+    if (st) return st;
+    return qcs_loc_set_tuning_multi(c, l2, l3);
+}
+
+int qcs_loc_tuning_multi(const qcs_loc_data *c, int *limit_2e, int *limit_3e) {
+    if (!c) return fail(QCS_ERR_ARG, "null context");
+    if (limit_2e) *limit_2e = c->tune_limit2;
+    if (limit_3e) *limit_3e = c->tune_limit3;
+    return QCS_OK;
+}
+
+int qcs_loc_set_tuning_multi(qcs_loc_data *c, int limit_2e, int limit_3e) {
+    if (!c) return fail(QCS_ERR_ARG, "null context");
+    if (limit_2e < -1 || limit_3e < -1) return fail(QCS_ERR_ARG, "limits: -1 (one thread per ROI), 0 (default) or > 0");
+    c->tune_limit2 = limit_2e;
+    c->tune_limit3 = limit_3e;
     return QCS_OK;
 }
 

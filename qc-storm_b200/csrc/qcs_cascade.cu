@@ -330,6 +330,7 @@ cudaError_t cascade_tail(const CascadeArgs &a, const CascadeState &st) {
             f.max_count = n;
             f.to2e = nullptr;
             f.mo = MultiOut{st.res2, st.extra2};
+            f.group_limit = a.group_limit2;
             if (a.two && !as3d) {
                 // learned starts; the plain refits write into the (still unused) 3E stage's arrays and are
                 // merged back into their slots
@@ -361,6 +362,7 @@ cudaError_t cascade_tail(const CascadeArgs &a, const CascadeState &st) {
             if (p.LocType == QCS_LOCTYPE_GS2D) {
                 f.q = Queue{st.q3, st.counters + kCnt3E, 0};
                 f.mo = MultiOut{st.res3, st.extra3};
+                f.group_limit = a.group_limit3;
                 if ((e = launch_fit(k3E, R, f)) != cudaSuccess) return e;
                 if ((e = launch_compaction(CompactStage{st, a.loc, 3, 0, a.max_rows}, n, st, a.stream)) != cudaSuccess)
                     return e;

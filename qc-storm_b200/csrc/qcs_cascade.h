@@ -71,6 +71,7 @@ struct CascadeArgs {
     const uint8_t *pred = nullptr;  // learned emitter-count class per record, or null (the reference's split)
     int lanes = 1;  // lanes per ROI of the single-emitter fit: 1 (one thread per ROI) or 4 / 8 / 16 (group kernel)
     const TwoEmitterStart *two = nullptr;  // learned two-emitter starts (GS2D), or null (the reference's)
+    int group_limit2 = 0, group_limit3 = 0;  // tuned lane-group queue limits of the 2E / 3E stages (0: default)
 };
 
 // The whole localization call: queues, single-emitter fit, 2E / 3E fits,

@@ -1158,6 +1158,21 @@ int group_queue_limit() {
     return limit;
 }
 
+}  // namespace
+
+int multi_group_default_limit(int kind, int R) {
+    if (kind == k2E && R == 7) return group_queue_limit<7, k2E>();
+    if (kind == k2E && R == 11) return group_queue_limit<11, k2E>();
+    if (kind == k3E && R == 7) return group_queue_limit<7, k3E>();
+    if (kind == k3E && R == 11) return group_queue_limit<11, k3E>();
+    if (kind == kAS3D2E && R == 7) return group_queue_limit<7, kAS3D2E>();
+    return 0;
+}
+
+bool multi_group_available(int kind, int R) { return multi_group_supported(kind, R); }
+
+namespace {
+
 // Both kernels are launched; each reads the stage's queue length on the
 // device and only one of them fits it (no host synchronisation).
 template <int R, int KIND>
@@ -1170,7 +1185,8 @@ cudaError_t launch_multi(const FitLaunch &a) {
             auto k = fit_multi_group_kernel<R, KIND>;
             cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if (e != cudaSuccess) return e;
-            min_n = group_queue_limit<R, KIND>();
+            // group_limit > 0: tuned; < 0: one thread per ROI always; 0: the default
+            min_n = a.group_limit > 0 ? a.group_limit : (a.group_limit < 0 ? -1 : group_queue_limit<R, KIND>());
             const int grid = (min(a.max_count, min_n) + L::SLOTS - 1) / L::SLOTS;
             if (grid > 0) {
                 k<<<grid, kGroupTPB, smem, a.stream>>>(a.rois, a.wle, a.q, a.loc, a.mo, a.para, a.ll, min_n);

@@ -32,10 +32,17 @@ struct FitLaunch {
     // kernel exists (queues of every record, where throughput, not one ROI's
     // latency, sets the time)
     int thread_per_roi = 0;
+    // multi-emitter kinds: the longest queue the lane-group kernel fits (0: the
+    // default, about three of its waves; the autotuner measures it)
+    int group_limit = 0;
 };
 
 // kind: FitKind (qcs_fit_math.cuh); R: ROI size.
 cudaError_t launch_fit(int kind, int R, const FitLaunch &a);
+// Multi-emitter kinds and sizes with a lane-group kernel, and the default
+// queue-length limit up to which it fits a stage (0 where there is none).
+bool multi_group_available(int kind, int R);
+int multi_group_default_limit(int kind, int R);
 
 // Single-emitter kinds with `lanes` lanes per ROI (8; also 4 and 16 for GS2D
 // 7x7): the rows of launch_fit bit for bit, lower latency.  Sizes: GS2D 7, 9,

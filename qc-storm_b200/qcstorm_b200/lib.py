@@ -142,6 +142,12 @@ _SIGS = {
     "qcs_loc_autotune": (C.c_int, [C.c_void_p, C.POINTER(LocPara), C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]),
     "qcs_loc_tuning": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
     "qcs_loc_set_tuning": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
+    "qcs_loc_tuning_multi": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "qcs_loc_set_tuning_multi": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "qcs_loc_save_tuning": (C.c_int, [C.c_void_p, C.c_char_p]),
+    "qcs_learned_autotune": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(LocPara), C.c_int,
+                                       C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_void_p]),
+    "qcs_loc_load_tuning": (C.c_int, [C.c_void_p, C.c_char_p]),
     "qcs_stat_init": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
     "qcs_stat_deinit": (C.c_int, [C.c_void_p]),
     "qcs_stat_reset_all": (C.c_int, [C.c_void_p]),
@@ -313,6 +319,21 @@ class LocContext:
         lanes = np.array([t[1] for t in table] or [1], np.int32)
         check(self.lib.qcs_loc_set_tuning(self.h, C.c_void_p(sizes.ctypes.data), C.c_void_p(lanes.ctypes.data),
                                           len(table)))
+
+    def tuning_multi(self):
+        """(2E limit, 3E limit) of the multi-emitter stages' lane-group kernels."""
+        a, b = C.c_int(0), C.c_int(0)
+        check(self.lib.qcs_loc_tuning_multi(self.h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def set_tuning_multi(self, limit_2e, limit_3e):
+        check(self.lib.qcs_loc_set_tuning_multi(self.h, int(limit_2e), int(limit_3e)))
+
+    def save_tuning(self, path):
+        check(self.lib.qcs_loc_save_tuning(self.h, str(path).encode()))
+
+    def load_tuning(self, path):
+        check(self.lib.qcs_loc_load_tuning(self.h, str(path).encode()))
 
     def read_rows(self, stream=0, para=None):
         """Rows of the last device call, on the host: (rows[n_valid, 12], ratios[7])."""
@@ -615,6 +636,16 @@ class LearnedNet:
         check(self.lib.qcs_learned_set_two_emitter(self.h, two.h if two is not None else None, int(iters),
                                                    int(bisections), C.c_float(dev_th), 0 if fallback == "3e" else 1))
         self._two = two
+
+    def autotune(self, ctx, d_rois, n, d_wle=0, para=None, stream=0):
+        """qcs_learned_autotune: (iterations, line-search steps) of the fastest schedule whose acceptance is
+        within 0.5 points of the best."""
+        para = para or ctx.para
+        it, nb = C.c_int(0), C.c_int(0)
+        check(self.lib.qcs_learned_autotune(ctx.h, self.h, C.c_void_p(d_rois), C.c_void_p(d_wle) if d_wle else None,
+                                            C.byref(para), int(n), C.byref(it), C.byref(nb),
+                                            C.c_void_p(stream) if stream else None))
+        return it.value, nb.value
 
     def set_direct_two_emitter(self, on=True):
         """Multi-emitter calls: poor bright single fits straight to the two-emitter fit."""
