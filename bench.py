@@ -53,10 +53,10 @@ R = 7
 PX_EVALS_PER_FIT = 176 * R * R  # reference schedule: 176 loss evaluations of R*R pixels
 MUFU_PER_PX_EVAL = 2            # exp of the model, log of the model (log of the data is invariant)
 # DRAM bytes (read + write) per fit of fit_single_kernel<7, GS2D>, from one ncu capture of
-# `bench.py --profile-fit 1200000` (profiles/fit_single_gs2d7_crlb9_1.2M_records.md:
-# 163.41 MB read + 37.19 MB written for 1.2 M fits); algorithmic: 112 B record + 24 B WLE row
-# read, 48 B row written.
-DRAM_BYTES_PER_FIT = (163.412480e6 + 37.192192e6) / 1.2e6
+# `bench.py --profile-fit 200000` (profiles/fit_single_gs2d7_200k_full.md: 27.28 MB read, 0 B
+# written for 200 k fits: the rows stay in L2 during the launch); algorithmic: 112 B record +
+# 24 B WLE row read, 48 B row written.
+DRAM_BYTES_PER_FIT = (27.277056e6 + 0.0) / 2e5
 ALGO_BYTES_PER_FIT = 112 + 24 + 48
 
 
@@ -1561,7 +1561,7 @@ def main():
                          "peak": mufu_peak, "unit": "MUFU op/s", "frac": achieved / mufu_peak,
                          "traffic": DRAM_BYTES_PER_FIT * N_PER_STEP,
                          "traffic_algorithmic": ALGO_BYTES_PER_FIT * N_PER_STEP,
-                         "traffic_note": "DRAM bytes per launch from ncu on 1.2 M records, scaled to %d" % N_PER_STEP,
+                         "traffic_note": "DRAM bytes per launch from ncu on 200 k records, scaled to %d" % N_PER_STEP,
                          "kernel_ms": fit_ms,
                          "algorithmic": "%d px-evals x %d MUFU per fit; peak = measured __expf/__logf rate" % (
                              PX_EVALS_PER_FIT, MUFU_PER_PX_EVAL)},
