@@ -455,8 +455,8 @@ int qcs_loc_autotune(qcs_loc_data *c, const qcs_loc_para *p, const uint16_t *d_r
 int qcs_loc_tuning(const qcs_loc_data *c, int *sizes, int *lanes, int max_entries);
 int qcs_loc_set_tuning(qcs_loc_data *c, const int *sizes, const int *lanes, int count);
 /* With multi-emitter fitting, qcs_loc_autotune also times each multi-emitter
- * stage (2E or AS3D-2E, and 3E) on queues of the caller's first 64, 256,
- * 1,024, ... records with the lane-group kernel and with one thread per ROI,
+ * stage (2E or AS3D-2E, and 3E) on queues of the caller's first 64, 128,
+ * 256, ... records with the lane-group kernel and with one thread per ROI,
  * and keeps the longest queue for which the lane groups are faster: a stage
  * whose queue (read on the device) is at most that long uses them.  The
  * limits (-1: one thread per ROI always; 0: the built-in default, about three

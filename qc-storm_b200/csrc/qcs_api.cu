@@ -1048,7 +1048,7 @@ int qcs_loc_autotune(qcs_loc_data *c, const qcs_loc_para *p, const uint16_t *d_r
             if (kind2 < 0 || !qcs::multi_group_available(kind2, p->ROISize)) continue;
             int limit = 0;
             bool group_wins_all = true;
-            for (int m = 64; e == cudaSuccess; m *= 4) {
+            for (int m = 64; e == cudaSuccess; m *= 2) {
                 const int mm = m < n ? m : n;
                 g.q = qcs::Queue{nullptr, nullptr, mm};
                 g.max_count = mm;

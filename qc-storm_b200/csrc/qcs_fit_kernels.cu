@@ -900,25 +900,33 @@ __global__ void __launch_bounds__(kTPB) fit_multi_kernel(const uint16_t *__restr
 // usual 2E / 3E queue) takes as long as one thread's whole fit; here a ROI's
 // pixel terms and gradient points are spread over G lanes.  Per slot: the
 // ROI's (value, log) pairs, its mask and loss terms contiguous (rows padded to
-// 4 floats); the inverse Hessian per lane.
+// 4 floats), and one inverse Hessian with its update scratch and the search
+// direction, which the group's first lane alone updates (bfgs_fit_shared).
 template <int R, int KIND>
 struct MultiGroupLayout {
     enum {
         P = KindTraits<KIND>::P,
         PIX = R * R,
         PIXP = (PIX + 3) / 4 * 4,
+        HP = (2 * P * P + P + 3) / 4 * 4,  // D, T and the direction per slot
         SLOTS = kGroupTPB / multi_lanes(KIND),
         IMG = 0,                       // float2 per pixel
         W = IMG + 2 * PIXP * SLOTS,    // floats
         PART = W + PIXP * SLOTS,
-        D = PART + PIXP * SLOTS,
-        TOTAL = D + P * P * kGroupTPB,
+        H = PART + PIXP * SLOTS,
+        TOTAL = H + HP * SLOTS,
     };
 };
 
+// The shared inverse Hessian's last update: nvcc fuses the separately
+// computed s s'/(y's) product of bfgs_update into the final sum (found by
+// building both forms against the reference's multi-emitter cascades: only
+// the fused one gives their rows bit for bit).
+constexpr bool kSkskFused = true;
+
 template <int R, int KIND, int DIST = ArithSpec<KIND, R>::DIST, int MASK = ArithSpec<KIND, R>::MASK,
           int SUM2 = ArithSpec<KIND, R>::SUM2>
-__global__ void __launch_bounds__(kGroupTPB) fit_multi_group_kernel(const uint16_t *__restrict__ rois,
+__global__ void __launch_bounds__(kGroupTPB, 4) fit_multi_group_kernel(const uint16_t *__restrict__ rois,
                                                                     const float *__restrict__ wle, Queue q,
                                                                     float *__restrict__ loc, MultiOut mo,
                                                                     CorePara c, double *__restrict__ ll, int max_n) {
@@ -953,7 +961,7 @@ __global__ void __launch_bounds__(kGroupTPB) fit_multi_group_kernel(const uint16
     const float2 *img2 = s_img + sl * PIXP;
     float *w = smem + L::W + sl * PIXP;
     float *part = smem + L::PART + sl * PIXP;
-    float *D = smem + L::D + threadIdx.x;
+    float *hess = smem + L::H + sl * L::HP;  // D (P x P), T (P x P), direction (P)
     const uint16_t *hdr = rois + (size_t)CurFluoID * WHOLE + PIX;
     const int XOffset = hdr[0];
     const int YOffset = hdr[1];
@@ -965,8 +973,9 @@ __global__ void __launch_bounds__(kGroupTPB) fit_multi_group_kernel(const uint16
     multi_prefit<R, KIND>(PixView{img2, 1}, c, Ininf, WLE_SigmaX);
     if (KIND == k2E && lane == 0) wle_weights<R, MASK>(w, 1, WLE_SigmaX, WLE_SigmaX, QCS_MOLECULE_MULTIFIT);
     __syncwarp(mask);
-    bfgs_fit<P, KindTraits<KIND>::IT>(MultiGroupEval<R, KIND, DIST, SUM2, G>{img2, w, part, lane, mask}, Ininf, D,
-                                      kGroupTPB);
+    bfgs_fit_shared<P, KindTraits<KIND>::IT, MultiGroupEval<R, KIND, DIST, SUM2, G>, kSkskFused>(
+        MultiGroupEval<R, KIND, DIST, SUM2, G>{img2, w, part, lane, mask}, Ininf, hess, hess + P * P,
+        hess + 2 * P * P, lane, mask);
     if (ll) {  // the lanes' pixel sums, combined in a fixed order
         double s = model_loglik<R, KIND, DIST, SUM2>(img2, 1, Ininf, lane, G);
 #pragma unroll

@@ -1136,6 +1136,143 @@ __device__ __forceinline__ void bfgs_fit(const Eval &ev, float *Ininf, float *D,
     }
 }
 
+// bfgs_update with few live registers, for one lane that updates an inverse
+// Hessian shared by a lane group: D (row-major P x P) and the scratch T
+// (P x P) in shared memory.  The same values as bfgs_update, operation for
+// operation: its P x P temporaries are recomputed from sk and the scaled
+// vectors with the roundings nvcc gives their expressions (one fused
+// multiply-add or separate product each), the left product kept in T.
+// SKSK_FUSED: the final D + sk sk'/(y's) fused into one multiply-add (nvcc
+// may contract the separately computed product into the sum).
+template <int P, bool SKSK_FUSED>
+__device__ __forceinline__ void bfgs_update_light(float *D, float *T, const float *sk, const float *yk) {
+    float divdat = 0;
+#pragma unroll
+    for (int cnt = 0; cnt < P; cnt++) divdat = __fmaf_rn(sk[cnt], yk[cnt], divdat);
+    divdat = 1.0f / divdat;
+    float tdat10[P], tdat20[P];
+#pragma unroll
+    for (int cnt = 0; cnt < P; cnt++) {
+        tdat10[cnt] = __fmul_rn(yk[cnt], divdat);
+        tdat20[cnt] = __fmul_rn(sk[cnt], divdat);
+    }
+    // skyk(r, c) = [r == c] - sk[r] tdat10[c], one rounding
+    auto skyk = [&](int r, int c) { return __fmaf_rn(-sk[r], tdat10[c], r == c ? 1.0f : 0.0f); };
+#pragma unroll 1
+    for (int row = 0; row < P; row++) {
+#pragma unroll
+        for (int col = 0; col < P; col++) {
+            float acc = 0;
+#pragma unroll
+            for (int cnt = 0; cnt < P; cnt++) acc = __fmaf_rn(skyk(row, cnt), D[cnt * P + col], acc);
+            T[row * P + col] = acc;
+        }
+    }
+#pragma unroll 1
+    for (int row = 0; row < P; row++) {
+#pragma unroll
+        for (int col = 0; col < P; col++) {
+            float acc = 0;
+#pragma unroll
+            for (int cnt = 0; cnt < P; cnt++) acc = __fmaf_rn(T[row * P + cnt], skyk(col, cnt), acc);
+            D[row * P + col] = SKSK_FUSED ? __fmaf_rn(sk[row], tdat20[col], acc)
+                                          : __fadd_rn(acc, __fmul_rn(sk[row], tdat20[col]));
+        }
+    }
+}
+
+// bfgs_fit for a lane group that shares one inverse Hessian per ROI: every
+// lane runs the line search and the evaluations (which need all lanes), the
+// group's first lane alone updates D (bfgs_update_light) and the new search
+// direction, which the others then read from dbuf.  D, T: P x P, dbuf: P
+// floats of shared memory per ROI.  The same values as bfgs_fit.
+template <int P, int IT, class Eval, bool SKSK_FUSED, int NB = kBisections>
+__device__ __forceinline__ void bfgs_fit_shared(const Eval &ev, float *Ininf, float *D, float *T, float *dbuf,
+                                                int lane, unsigned mask) {
+    float grad[P], d0[P], td0[P], sk[P], yk[P], tgrad[P];
+    float ddat[2], dpos[2];
+    if (lane == 0) {
+#pragma unroll
+        for (int r = 0; r < P; r++) {
+#pragma unroll
+            for (int c = 0; c < P; c++) D[r * P + c] = (r == c) ? 1.0f : 0.0f;
+        }
+    }
+    ev.gradient(Ininf, grad);
+#pragma unroll
+    for (int rcnt = 0; rcnt < P; rcnt++) d0[rcnt] = -grad[rcnt];
+
+    for (int itcnt = 0; itcnt < IT; itcnt++) {
+        float td0_total = 0;
+#pragma unroll
+        for (int rcnt = 0; rcnt < P; rcnt++) {
+            td0[rcnt] = fabsf(d0[rcnt]);
+            td0_total += td0[rcnt];
+        }
+        td0_total = ((float)P) / td0_total;
+#pragma unroll
+        for (int rcnt = 0; rcnt < P; rcnt++) d0[rcnt] = d0[rcnt] * td0_total;
+
+        dpos[0] = 0.00001f;
+        dpos[1] = 1.0f;
+        {
+            float xlo[P], xhi[P];
+#pragma unroll
+            for (int cnt = 0; cnt < P; cnt++) xlo[cnt] = d0[cnt] * 0.0001f + Ininf[cnt];
+#pragma unroll
+            for (int cnt = 0; cnt < P; cnt++) xhi[cnt] = d0[cnt] * 1.0f + Ininf[cnt];
+            ddat[0] = ev.loss(xlo);
+            ddat[1] = ev.loss(xhi);
+        }
+        for (int cnt = 0; cnt < NB; cnt++) {
+            const int xdsel = (ddat[0] < ddat[1]);
+            const float mid = (dpos[0] + dpos[1]) * 0.5f;
+            dpos[0] = xdsel ? dpos[0] : mid;
+            dpos[1] = xdsel ? mid : dpos[1];
+            if (cnt < NB - 1) {
+                const float dsel = xdsel ? dpos[1] : dpos[0];
+                float xn[P];
+#pragma unroll
+                for (int k = 0; k < P; k++) xn[k] = d0[k] * dsel + Ininf[k];
+                const float f = ev.loss(xn);
+                ddat[0] = xdsel ? ddat[0] : f;
+                ddat[1] = xdsel ? f : ddat[1];
+            }
+        }
+        const float scale = (dpos[0] + dpos[1]) * 0.5f;
+#pragma unroll
+        for (int rcnt = 0; rcnt < P; rcnt++) {
+            sk[rcnt] = d0[rcnt] * scale;
+            Ininf[rcnt] = Ininf[rcnt] + sk[rcnt];
+        }
+#pragma unroll
+        for (int cnt = 0; cnt < P; cnt++)
+            if (Ininf[cnt] < 0.01f) Ininf[cnt] = 0.01f;
+
+        if (itcnt < IT - 1) {
+#pragma unroll
+            for (int rcnt = 0; rcnt < P; rcnt++) tgrad[rcnt] = grad[rcnt];
+            ev.gradient(Ininf, grad);
+            if (lane == 0) {
+#pragma unroll
+                for (int rcnt = 0; rcnt < P; rcnt++) yk[rcnt] = grad[rcnt] - tgrad[rcnt];
+                bfgs_update_light<P, SKSK_FUSED>(D, T, sk, yk);
+#pragma unroll
+                for (int row = 0; row < P; row++) {
+                    float acc = 0;
+#pragma unroll
+                    for (int cnt = 0; cnt < P; cnt++) acc = __fmaf_rn(-D[row * P + cnt], grad[cnt], acc);
+                    dbuf[row] = acc;
+                }
+            }
+            __syncwarp(mask);
+#pragma unroll
+            for (int row = 0; row < P; row++) d0[row] = dbuf[row];
+            __syncwarp(mask);
+        }
+    }
+}
+
 template <int R, int KIND, int DIST = ArithSpec<KIND, R>::DIST, int SUM2 = ArithSpec<KIND, R>::SUM2,
           int ITERS = KindTraits<KIND>::IT>
 __device__ __forceinline__ void mle_fit(const RoiRef &roi, float *Ininf, float *D, int ld) {
