@@ -508,6 +508,9 @@ int qcs_crlb_device(const qcs_loc_para *p, float *d_loc, int n, void *stream);
  * outcome.  One network per localization type and ROI size.
  * Parameters: W1 Kx128, b1, W2 128x128, b2, W3 128x8, b3, row-major [in][out]
  * (qcs_learned_shape gives the count).
+ * Every `stream` argument of these entry points is a cudaStream_t, NULL for
+ * the default stream; the calls are asynchronous on it unless they return a
+ * host value (a loss).
  */
 typedef struct qcs_learned_net qcs_learned_net;
 /* Parameter count of the GS2D 7x7 network (K = 64). */

@@ -165,3 +165,132 @@ def loss_and_grad(params, x, t, valid, classes=None):
     gb1 = d1.sum(axis=0)
     grad = np.concatenate([g.ravel() for g in (gW1, gb1, gW2, gb2, gW3, gb3)])
     return loss, grad, y
+
+
+# ---------------------------------------------------------------- conv net
+# The convolutional start-point network (QCS_LEARNED_ARCH_CONV in
+# qc-storm_b200/csrc/qcs_convnet.cu): the R x R scaled pixels (the first R*R
+# features) -> 3x3 conv, 32 channels, zero 'same' padding, ReLU -> 3x3 conv,
+# 64 channels, ReLU -> fully connected 256 over the flattened map (position
+# major, channel minor) and the two scale features, ReLU -> 8 outputs (the
+# MLP's outputs).  Parameters, row-major [in][out]: W1 [9][32] (tap t = 3 *
+# (dy + 1) + (dx + 1)), b1, W2 [9 * 32][64] (row t * 32 + input channel), b2,
+# W3 [R*R*64 + 2][256], b3, W4 [256][8], b4.
+CONV_C1, CONV_C2, CONV_FC = 32, 64, 256
+
+
+def conv_param_count(r):
+    return 9 * CONV_C1 + CONV_C1 + 9 * CONV_C1 * CONV_C2 + CONV_C2 + (r * r * CONV_C2 + 2) * CONV_FC + CONV_FC + \
+        CONV_FC * N_OUT + N_OUT
+
+
+def conv_split_params(p, r):
+    p = np.asarray(p, np.float64)
+    shapes = ((9, CONV_C1), (CONV_C1,), (9 * CONV_C1, CONV_C2), (CONV_C2,), (r * r * CONV_C2 + 2, CONV_FC),
+              (CONV_FC,), (CONV_FC, N_OUT), (N_OUT,))
+    out, o = [], 0
+    for shape in shapes:
+        size = int(np.prod(shape))
+        out.append(p[o:o + size].reshape(shape))
+        o += size
+    assert o == p.size
+    return out
+
+
+def im2col(a, r):
+    """[n, r, r, c] -> [n * r * r, 9 * c]: for each position the 3x3
+    neighbourhood (tap-major, channel-minor), zeros outside the ROI."""
+    n, c = a.shape[0], a.shape[3]
+    pad = np.zeros((n, r + 2, r + 2, c))
+    pad[:, 1:-1, 1:-1] = a
+    cols = [pad[:, dy:dy + r, dx:dx + r, :] for dy in range(3) for dx in range(3)]
+    return np.concatenate(cols, axis=3).reshape(n * r * r, 9 * c)
+
+
+def col2im(d, n, r, c):
+    """Adjoint of im2col: [n * r * r, 9 * c] -> [n * r * r, c]."""
+    d = d.reshape(n, r, r, 9, c)
+    pad = np.zeros((n, r + 2, r + 2, c))
+    for dy in range(3):
+        for dx in range(3):
+            pad[:, dy:dy + r, dx:dx + r, :] += d[:, :, :, dy * 3 + dx, :]
+    return pad[:, 1:-1, 1:-1, :].reshape(n * r * r, c)
+
+
+def conv_forward(params, x, r, exact=False):
+    """Outputs [n, 8] of feature rows x (in_width(r) wide).  GEMM operands are
+    rounded to bfloat16 as the GPU rounds them, unless exact."""
+    rb = (lambda a: np.asarray(a, np.float64)) if exact else bf16
+    W1, b1, W2, b2, W3, b3, W4, b4 = conv_split_params(params, r)
+    x = np.asarray(x, np.float64)
+    n, pix = x.shape[0], r * r
+    X1 = im2col(x[:, :pix].reshape(n, r, r, 1), r)
+    z1 = rb(X1) @ rb(W1) + b1
+    a1 = np.maximum(z1, 0)
+    X2 = im2col(a1.reshape(n, r, r, CONV_C1), r)
+    z2 = rb(X2) @ rb(W2) + b2
+    a2 = np.maximum(z2, 0)
+    H = np.concatenate([a2.reshape(n, pix * CONV_C2), x[:, pix:pix + 2]], axis=1)
+    z3 = rb(H) @ rb(W3) + b3
+    a3 = np.maximum(z3, 0)
+    y = rb(a3) @ rb(W4) + b4
+    return y, (X1, z1, X2, z2, H, z3, a3)
+
+
+def _loss_dy(y, t, valid, classes):
+    """Masked weighted MSE (+ count cross-entropy) over the batch and dL/dy."""
+    n, nu = y.shape[0], t.shape[1]
+    e = y[:, :nu] - t
+    tw = TARGET_WEIGHT_2E if nu == 8 else TARGET_WEIGHT[:nu]
+    loss = float(np.sum(tw * e * e * valid[:, None]) / n)
+    dy = np.zeros_like(y)
+    dy[:, :nu] = 2.0 * tw * e * valid[:, None] / n
+    if classes is not None:
+        c = np.asarray(classes).astype(np.int64)
+        lab = c >= 0
+        lg = y[:, COUNT0:COUNT0 + CLASSES]
+        p = np.exp(lg - lg.max(axis=1, keepdims=True))
+        p /= p.sum(axis=1, keepdims=True)
+        rows = np.nonzero(lab)[0]
+        loss += float(COUNT_WEIGHT * np.sum(-np.log(p[rows, c[rows]])) / n)
+        onehot = np.zeros_like(p)
+        onehot[rows, c[rows]] = 1.0
+        dy[:, COUNT0:COUNT0 + CLASSES] = COUNT_WEIGHT * (p - onehot) * lab[:, None] / n
+    return loss, dy
+
+
+def conv_loss_and_grad(params, x, t, valid, r, classes=None, exact=False):
+    """Loss and parameter gradient of the conv net, with the GPU's bfloat16
+    rounding of every GEMM operand of the backward pass unless exact."""
+    rb = (lambda a: np.asarray(a, np.float64)) if exact else bf16
+    W1, b1, W2, b2, W3, b3, W4, b4 = conv_split_params(params, r)
+    y, (X1, z1, X2, z2, H, z3, a3) = conv_forward(params, x, r, exact)
+    n, pix = y.shape[0], r * r
+    loss, dy = _loss_dy(y, np.asarray(t, np.float64), np.asarray(valid, np.float64), classes)
+    gW4 = rb(a3).T @ rb(dy)
+    gb4 = dy.sum(axis=0)
+    d3 = (rb(dy) @ rb(W4).T) * (z3 > 0)
+    gW3 = rb(H).T @ rb(d3)
+    gb3 = d3.sum(axis=0)
+    d2 = (rb(d3) @ rb(W3[:pix * CONV_C2]).T).reshape(n * pix, CONV_C2) * (z2 > 0)
+    gW2 = rb(X2).T @ rb(d2)
+    gb2 = d2.sum(axis=0)
+    d1 = col2im(rb(d2) @ rb(W2).T, n, r, CONV_C1) * (z1 > 0)
+    gW1 = rb(X1).T @ rb(d1)
+    gb1 = d1.sum(axis=0)
+    grad = np.concatenate([g.ravel() for g in (gW1, gb1, gW2, gb2, gW3, gb3, gW4, gb4)])
+    return loss, grad, y
+
+
+def conv_init(r, seed):
+    """He-style uniform initial parameters (a test helper; the library draws its own)."""
+    rng = np.random.default_rng(seed)
+    parts = []
+    for fan_in, shape in ((9, (9, CONV_C1)), (None, (CONV_C1,)), (9 * CONV_C1, (9 * CONV_C1, CONV_C2)),
+                          (None, (CONV_C2,)), (r * r * CONV_C2 + 2, (r * r * CONV_C2 + 2, CONV_FC)),
+                          (None, (CONV_FC,)), (CONV_FC, (CONV_FC, N_OUT)), (None, (N_OUT,))):
+        if fan_in is None:
+            parts.append(np.zeros(shape))
+        else:
+            parts.append(rng.uniform(-1, 1, shape) * np.sqrt(6.0 / fan_in))
+    return np.concatenate([a.ravel() for a in parts])

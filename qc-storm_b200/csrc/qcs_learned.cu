@@ -13,8 +13,8 @@
 // (background - min) / range, sigma_y - 1.3.
 // Features: the R*R photoelectron pixels max((adu - offset) * gain, 1) scaled
 // to [0, 1] by the ROI's min and range, log(range) / 8, log(min) / 8, zeros.
-// Training and inference GEMMs run on the tensor cores in BF16 with FP32
-// accumulation (mma.sync m16n8k16); master weights and Adam moments are FP32.
+// Training and inference GEMMs run on the tensor cores (tcgen05) in BF16 with
+// FP32 accumulation; master weights and Adam moments are FP32.
 // Labels are the converged plain MLEbfgs fits of the same ROIs.
 #include <cstdint>
 #include <cstring>
@@ -25,12 +25,12 @@
 #include "qcs_error.h"
 #include "qcs_kernels.h"
 #include "qcs_learned.h"
+#include "qcs_tc.cuh"
 
 namespace qcs {
 namespace learned {
 
-constexpr int kGemmThreads = 128;  // 4 warps, 64 x 64 block tile, k step 16
-constexpr int kTile = 64;
+constexpr int kGemmThreads = 128;  // 4 warps: one tcgen05 GEMM tile of 128 rows
 
 // One feature of record r (R x R pixels then header words): feature k of
 // in_width(R), given the record's photoelectron min lo, 1 / range inv and the
@@ -108,99 +108,184 @@ __global__ void targets_kernel(const uint16_t *__restrict__ rois, const float *_
 }
 
 // ------------------------------------------------------------------- GEMM
-__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
-    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
-    return *reinterpret_cast<const uint32_t *>(&v);
-}
-
 // C(m, n) = beta * C(m, n) + sum_k A(m, k) B(k, n), M x N x K, with
 // A(m, k) = A[m * sam + k * sak], B(k, n) = B[k * sbk + n * sbn] (FP32 in
 // memory, rounded to BF16 for the tensor cores), C row-major with ldc.
-// mma.sync.m16n8k16 fragment layouts (PTX ISA, bf16): lane = 4 g + t;
-// A: {(g, 2t..2t+1), (g+8, 2t..), (g, 2t+8..), (g+8, 2t+8..)};
-// B: {(k = 2t..2t+1, n = g), (k = 2t+8..2t+9, n = g)};
-// C: {(g, 2t..2t+1), (g+8, 2t..2t+1)}.
-__global__ void __launch_bounds__(kGemmThreads) gemm_bf16_kernel(int M, int N, int K, const float *__restrict__ A,
-                                                                 int sam, int sak, const float *__restrict__ B,
-                                                                 int sbk, int sbn, float *__restrict__ Cm, int ldc,
-                                                                 float beta) {
-    __shared__ __nv_bfloat16 As[kTile][16 + 8];
-    __shared__ __nv_bfloat16 Bs[16][kTile + 8];
-    const int m0 = blockIdx.y * kTile, n0 = blockIdx.x * kTile;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int g = lane >> 2, t = lane & 3;
-    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
-    float acc[2][4][4];
-#pragma unroll
-    for (int a = 0; a < 2; ++a)
-#pragma unroll
-        for (int b = 0; b < 4; ++b)
-#pragma unroll
-            for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.0f;
-    for (int k0 = 0; k0 < K; k0 += 16) {
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const int idx = threadIdx.x + j * kGemmThreads;  // 0..1023
-            const int r = idx >> 4, c = idx & 15;             // A tile 64 x 16
-            const int gm = m0 + r, gk = k0 + c;
-            As[r][c] = __float2bfloat16_rn((gm < M && gk < K) ? A[(size_t)gm * sam + (size_t)gk * sak] : 0.0f);
-            const int kr = idx >> 6, nc = idx & 63;           // B tile 16 x 64
-            const int bk = k0 + kr, bn = n0 + nc;
-            Bs[kr][nc] = __float2bfloat16_rn((bk < K && bn < N) ? B[(size_t)bk * sbk + (size_t)bn * sbn] : 0.0f);
-        }
-        __syncthreads();
-        uint32_t af[2][4], bfr[4][2];
-#pragma unroll
-        for (int mi = 0; mi < 2; ++mi) {
-            const int r = wm + mi * 16 + g;
-            af[mi][0] = *reinterpret_cast<const uint32_t *>(&As[r][2 * t]);
-            af[mi][1] = *reinterpret_cast<const uint32_t *>(&As[r + 8][2 * t]);
-            af[mi][2] = *reinterpret_cast<const uint32_t *>(&As[r][2 * t + 8]);
-            af[mi][3] = *reinterpret_cast<const uint32_t *>(&As[r + 8][2 * t + 8]);
-        }
-#pragma unroll
-        for (int ni = 0; ni < 4; ++ni) {
-            const int c = wn + ni * 8 + g;
-            const __nv_bfloat162 b01 = __halves2bfloat162(Bs[2 * t][c], Bs[2 * t + 1][c]);
-            const __nv_bfloat162 b23 = __halves2bfloat162(Bs[2 * t + 8][c], Bs[2 * t + 9][c]);
-            bfr[ni][0] = *reinterpret_cast<const uint32_t *>(&b01);
-            bfr[ni][1] = *reinterpret_cast<const uint32_t *>(&b23);
-        }
-#pragma unroll
-        for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-            for (int ni = 0; ni < 4; ++ni)
-                asm volatile(
-                    "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
-                    "{%8, %9}, {%0, %1, %2, %3};\n"
-                    : "+f"(acc[mi][ni][0]), "+f"(acc[mi][ni][1]), "+f"(acc[mi][ni][2]), "+f"(acc[mi][ni][3])
-                    : "r"(af[mi][0]), "r"(af[mi][1]), "r"(af[mi][2]), "r"(af[mi][3]), "r"(bfr[ni][0]),
-                      "r"(bfr[ni][1]));
-        __syncthreads();
+// One CTA of 128 threads per 128 x bn tile (bn <= 256, a multiple of 16) and
+// K range: the threads stage 64-deep K chunks of both operands into shared
+// memory in the UMMA layout (double-buffered), one thread issues four
+// tcgen05.mma (M = 128, K = 16) per chunk into an FP32 accumulator in tensor
+// memory, and each warp reads its 32 rows back with tcgen05.ld.  With split-K
+// (gridDim.z > 1) CTA z sums K range [z kper, (z + 1) kper) into
+// part[z][M][N] and gemm_reduce_kernel adds the splits in order, so results
+// do not depend on scheduling.
+constexpr int kGemmM = 128, kGemmK = 64;
+
+__global__ void __launch_bounds__(kGemmThreads, 1)
+    gemm_tc_kernel(int M, int N, int K, int bn, const float *__restrict__ A, long long sam, long long sak,
+                   const float *__restrict__ B, long long sbk, long long sbn, float *__restrict__ Cm, int ldc,
+                   float beta, int kper, float *__restrict__ part, int *__restrict__ err) {
+    extern __shared__ uint8_t smem_raw[];
+    const uint32_t raw = (uint32_t)__cvta_generic_to_shared(smem_raw);
+    const uint32_t sbase = (raw + 127u) & ~127u;
+    uint8_t *base = smem_raw + (sbase - raw);
+    const uint32_t a_bytes = kGemmM * kGemmK * 2, b_bytes = (uint32_t)bn * kGemmK * 2;
+    const uint32_t sA = sbase, sB = sbase + 2 * a_bytes, sBar = sB + 2 * b_bytes, sTmem = sBar + 16;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.y * kGemmM, n0 = blockIdx.x * bn;
+    const int kb = blockIdx.z * kper, ke = min(K, kb + kper);
+    const int nchunks = ke > kb ? (ke - kb + kGemmK - 1) / kGemmK : 0;
+    uint32_t cols = 32;
+    while ((int)cols < bn) cols <<= 1;
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(sBar) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(sBar + 8) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sTmem), "r"(cols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    const uint32_t tmem = *reinterpret_cast<volatile uint32_t *>(base + (sTmem - sbase));
+    const uint32_t idesc = tc::instr_desc(kGemmM, bn);
+    bool ok = true;
+    int issued = 0;  // chunks whose MMAs were issued
+    for (int c = 0; c < nchunks; ++c) {
+        const int buf = c & 1, k0 = kb + c * kGemmK;
+        if (c >= 2) {  // the MMAs of chunk c - 2 have read this buffer
+            ok = __syncthreads_and(tc::mbar_wait(sBar + 8 * buf, ((c - 2) >> 1) & 1));
+            if (!ok) break;
+        }
+        uint8_t *a_img = base + buf * a_bytes, *b_img = base + 2 * a_bytes + buf * b_bytes;
+        // A: row tid, K groups 0..7 of the chunk
+        const int gm = m0 + tid;
+#pragma unroll 2
+        for (int kg = 0; kg < kGemmK / 8; ++kg) {
+            float v[8];
 #pragma unroll
-    for (int mi = 0; mi < 2; ++mi)
+            for (int e = 0; e < 8; ++e) {
+                const int gk = k0 + kg * 8 + e;
+                v[e] = (gm < M && gk < ke) ? __ldg(A + (long long)gm * sam + (long long)gk * sak) : 0.0f;
+            }
+            *reinterpret_cast<uint4 *>(a_img + (size_t)(kg * kGemmM + tid) * 16) = tc::pack8(v);
+        }
+        // B: bn rows (n) x 8 K groups
+        for (int u = tid; u < bn * (kGemmK / 8); u += kGemmThreads) {
+            const int kg = u / bn, nn = u - kg * bn, gn = n0 + nn;
+            float v[8];
 #pragma unroll
-        for (int ni = 0; ni < 4; ++ni)
+            for (int e = 0; e < 8; ++e) {
+                const int gk = k0 + kg * 8 + e;
+                v[e] = (gn < N && gk < ke) ? __ldg(B + (long long)gk * sbk + (long long)gn * sbn) : 0.0f;
+            }
+            *reinterpret_cast<uint4 *>(b_img + (size_t)(kg * bn + nn) * 16) = tc::pack8(v);
+        }
+        tc::fence_async_smem();
+        tc::fence_before();
+        __syncthreads();
+        tc::fence_after();
+        if (tid == 0) {
+            const uint32_t a0 = sA + buf * a_bytes, b0 = sB + buf * b_bytes;
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int r = m0 + wm + mi * 16 + g + h * 8;
-                const int c = n0 + wn + ni * 8 + 2 * t;
-                if (r >= M) continue;
+            for (int ks = 0; ks < kGemmK / 16; ++ks)
+                tc::mma_bf16(tmem, tc::smem_desc(a0 + ks * 2 * kGemmM * 16, kGemmM * 16, 128),
+                             tc::smem_desc(b0 + ks * 2 * bn * 16, bn * 16, 128), idesc, (c > 0 || ks > 0) ? 1u : 0u);
+            tc::mma_commit(sBar + 8 * buf);
+        }
+        issued = c + 1;
+    }
+    // the last commit covers every MMA issued before it; after a wait gave up
+    // this (bounded) wait still lets the issued MMAs end before the memory is released
+    if (issued > 0) {
+        const bool done = __syncthreads_and(tc::mbar_wait(sBar + 8 * ((issued - 1) & 1), ((issued - 1) >> 1) & 1));
+        ok = ok && done;
+    }
+    tc::fence_after();
+    const int row = m0 + warp * 32 + lane;
+    if (ok) {
+        for (int c0 = 0; c0 < bn; c0 += 16) {
+            float v[16];
+            if (issued > 0) {
+                tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + c0, v);
+            } else {
 #pragma unroll
-                for (int q = 0; q < 2; ++q) {
-                    if (c + q >= N) continue;
-                    float *dst = Cm + (size_t)r * ldc + c + q;
-                    const float v = acc[mi][ni][2 * h + q];
-                    *dst = (beta == 0.0f) ? v : beta * (*dst) + v;
+                for (int j = 0; j < 16; ++j) v[j] = 0.0f;
+            }
+            if (row >= M) continue;
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const int col = n0 + c0 + j;
+                if (col >= N) continue;
+                if (part) {
+                    part[((size_t)blockIdx.z * M + row) * N + col] = v[j];
+                } else {
+                    float *dst = Cm + (size_t)row * ldc + col;
+                    *dst = (beta == 0.0f) ? v[j] : beta * (*dst) + v[j];
                 }
             }
+        }
+    } else if (tid == 0 && err) {
+        atomicExch(err, 1);
+    }
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(cols) : "memory");
 }
 
-cudaError_t gemm(int M, int N, int K, const float *A, int sam, int sak, const float *B, int sbk, int sbn, float *C,
-                 int ldc, float beta, cudaStream_t s) {
-    dim3 grid((N + kTile - 1) / kTile, (M + kTile - 1) / kTile);
-    gemm_bf16_kernel<<<grid, kGemmThreads, 0, s>>>(M, N, K, A, sam, sak, B, sbk, sbn, C, ldc, beta);
+// C = beta C + sum over the splits z = 0, 1, ... of part[z] (in that order).
+__global__ void gemm_reduce_kernel(const float *__restrict__ part, int splits, int M, int N, float *__restrict__ Cm,
+                                   int ldc, float beta) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (long long)M * N) return;
+    const int r = (int)(i / N), c = (int)(i - (long long)r * N);
+    float s = 0.0f;
+    for (int z = 0; z < splits; ++z) s += part[(size_t)z * M * N + i];
+    float *dst = Cm + (size_t)r * ldc + c;
+    *dst = (beta == 0.0f) ? s : beta * (*dst) + s;
+}
+
+size_t gemm_smem_bytes(int bn) { return 2 * (size_t)(kGemmM + bn) * kGemmK * 2 + 32 + 128; }
+
+// Split count for an M x N x K GEMM: enough CTAs to cover the SMs, at least
+// four K chunks per split, and partials within `ws_floats`.
+int gemm_splits(int M, int N, int K, int bn, size_t ws_floats) {
+    const int tiles = ((M + kGemmM - 1) / kGemmM) * ((N + bn - 1) / bn);
+    int s = 148 / tiles;
+    const int by_k = K / (4 * kGemmK);
+    if (s > by_k) s = by_k;
+    if (s > 64) s = 64;
+    while (s > 1 && (size_t)s * M * N > ws_floats) --s;
+    return s < 1 ? 1 : s;
+}
+
+cudaError_t gemm(int M, int N, int K, const float *A, long long sam, long long sak, const float *B, long long sbk,
+                 long long sbn, float *C, int ldc, float beta, cudaStream_t s, float *ws, size_t ws_floats, int *err) {
+    if (M <= 0 || N <= 0) return cudaSuccess;
+    int bn = ((N + 15) / 16) * 16;
+    if (bn > 256) bn = 256;
+    const int splits = ws ? gemm_splits(M, N, K, bn, ws_floats) : 1;
+    int kper = (K + splits - 1) / splits;
+    kper = ((kper + kGemmK - 1) / kGemmK) * kGemmK;
+    const int z = kper > 0 ? (K + kper - 1) / kper : 1;
+    const size_t smem = gemm_smem_bytes(bn);
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)gemm_smem_bytes(256));
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    dim3 grid((N + bn - 1) / bn, (M + kGemmM - 1) / kGemmM, z > 1 ? z : 1);
+    float *part = z > 1 ? ws : nullptr;
+    gemm_tc_kernel<<<grid, kGemmThreads, smem, s>>>(M, N, K, bn, A, sam, sak, B, sbk, sbn, C, ldc, beta,
+                                                    z > 1 ? kper : (K > 0 ? K : 0), part, err);
+    if (z > 1)
+        gemm_reduce_kernel<<<(int)(((long long)M * N + 255) / 256), 256, 0, s>>>(part, z, M, N, C, ldc, beta);
     return cudaGetLastError();
 }
 
@@ -287,39 +372,6 @@ __global__ void gather_rows_kernel(const float *__restrict__ src, const int *__r
     dst[i] = src[(size_t)idx[r] * cols + c];
 }
 
-// Network outputs y (bias included) -> the fit's start point st
-// (start_width(LT) floats: peak e-, x, y, sigma(s), background e-), with
-// positions held inside the kind's accept window and widths in range.
-template <int R, int LT>
-__device__ __forceinline__ void start_from_outputs(const float *y, float lo, float rng, float *st) {
-    const float centre = R / 2.0f;
-    if (LT == kTwo) {
-        // emitters anywhere up to a pixel inside the ROI's edge
-        const float w2 = R / 2.0f - 1.0f;
-        st[0] = rng * expf(fminf(fmaxf(y[4], -6.0f), 3.0f));
-        st[1] = centre + fminf(fmaxf(y[0], -w2), w2);
-        st[2] = centre + fminf(fmaxf(y[1], -w2), w2);
-        st[3] = rng * expf(fminf(fmaxf(y[5], -6.0f), 3.0f));
-        st[4] = centre + fminf(fmaxf(y[2], -w2), w2);
-        st[5] = centre + fminf(fmaxf(y[3], -w2), w2);
-        st[6] = fminf(fmaxf(kSigma0 + y[6], 0.6f), 3.0f);
-        st[7] = fmaxf(lo + rng * y[7], 1.0f);
-        return;
-    }
-    const float win = LT == QCS_LOCTYPE_AS3D ? 2.5f : 1.5f;
-    const float smax = LT == QCS_LOCTYPE_AS3D ? 4.0f : 3.0f;
-    st[0] = rng * expf(fminf(fmaxf(y[3], -6.0f), 3.0f));
-    st[1] = centre + fminf(fmaxf(y[0], -win), win);
-    st[2] = centre + fminf(fmaxf(y[1], -win), win);
-    st[3] = fminf(fmaxf(kSigma0 + y[2], 0.6f), smax);
-    if (LT == QCS_LOCTYPE_AS3D) {
-        st[4] = fminf(fmaxf(kSigma0 + y[5], 0.6f), smax);
-        st[5] = fmaxf(lo + rng * y[4], 1.0f);
-    } else {
-        st[4] = fmaxf(lo + rng * y[4], 1.0f);
-    }
-}
-
 // Predictions -> fit start and, with cls set (GS2D), the emitter-count class
 // at threshold th.
 template <int R, int LT>
@@ -338,16 +390,13 @@ __global__ void start_kernel(const float *__restrict__ Y, const float *__restric
 // kept on chip.  The three GEMMs are tcgen05.mma (M = 128, kind::f16, BF16
 // operands in shared memory, FP32 accumulators in tensor memory), issued by
 // one thread and completed through an mbarrier; each warp reads its 32
-// accumulator rows back with tcgen05.ld.  Operands use the K-major,
-// no-swizzle UMMA layout: 8-row x 16-byte core matrices, 8-row groups 128 B
-// apart (SBO), 8-element K groups rows x 16 B apart (LBO).
+// accumulator rows back with tcgen05.ld.
 namespace tc {
 
 constexpr int kM = 128;        // ROIs per tile (the MMA's M)
 constexpr int kN3 = 16;        // layer-3 N padded to the M = 128 minimum
 constexpr int kAlign = 128;
 constexpr int kTmemCols = 256;                     // layer 1 / 3 at column 0, layer 2 at column 128
-constexpr int kWaitPolls = 1 << 22;                // bound of every barrier wait
 
 // Shared memory of one CTA for R x R records and KIN features: the weight
 // images, the layer-2 operand (the layer-1 operand lives in its first part:
@@ -373,82 +422,6 @@ struct Layout {
     static_assert(OFF_A1 + kM * KIN * 2 <= OFF_REC, "layer-1 operand inside the layer-2 buffer");
     static_assert(REC_BYTES % 16 == 0 && OFF_REC % 16 == 0, "a full tile is a whole number of 16-byte blocks");
 };
-
-// element (n, k) of an N x K K-major operand image, in bf16 elements
-__host__ __device__ constexpr int img_index(int n, int k, int N) { return ((k >> 3) * N + n) * 8 + (k & 7); }
-
-// UMMA shared-memory descriptor: start address, leading (K-group) and stride
-// (8-row group) byte offsets, version 1, no swizzle.
-__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
-    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
-           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
-}
-
-// instruction descriptor: FP32 accumulate, BF16 A and B, both K-major, N, M
-__host__ __device__ constexpr uint32_t instr_desc(int M, int N) {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
-}
-
-__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
-        :
-        : "r"(tmem_d), "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
-}
-
-__device__ __forceinline__ void mma_commit(uint32_t bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
-}
-
-// Bounded wait for the barrier phase; false when it did not complete.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
-    for (int it = 0; it < kWaitPolls; ++it) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.b32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(done)
-            : "r"(bar), "r"(phase)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
-}
-
-// Bulk copy (TMA, no multicast) of `bytes` contiguous global bytes into this
-// CTA's shared memory, completing on `bar` (which expects the bytes).
-__device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-                 "l"(src), "r"(bytes), "r"(bar)
-                 : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
-    uint32_t r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15}, [%16];\n"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
-          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
-}
-
-__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
-__device__ __forceinline__ uint4 pack8(const float *v) {
-    uint4 u;
-    u.x = pack_bf16(v[0], v[1]);
-    u.y = pack_bf16(v[2], v[3]);
-    u.z = pack_bf16(v[4], v[5]);
-    u.w = pack_bf16(v[6], v[7]);
-    return u;
-}
 
 // Relu(D + bias) of this thread's accumulator row (ncols columns from tmem
 // column col0) into the next layer's A operand (row tid).
@@ -732,7 +705,8 @@ struct qcs_learned_net {
     float *d_start = nullptr;  // start points and feature work of the last localization call
     size_t start_cap = 0;
     __nv_bfloat16 *d_wimg = nullptr;  // BF16 operand images of the weights (fused inference)
-    int *d_err = nullptr;             // set by the fused kernel when an MMA wait gives up
+    int *d_err = nullptr;             // set by a tensor-core kernel when an MMA wait gives up
+    float *d_ws = nullptr;            // split-K partial sums of the training GEMMs
     unsigned version = 1;             // bumped whenever the parameters change
     unsigned wimg_version = 0;        // parameter version d_wimg was built from
     cudaEvent_t wimg_ready = nullptr; // recorded after d_wimg was built
@@ -740,7 +714,6 @@ struct qcs_learned_net {
     float count_th = 0.0f;            // emitter-count routing threshold; 0 = no routing
     int batch = 0;
     long long step = 0;
-    cudaStream_t stream = nullptr;
 };
 
 namespace {
@@ -761,6 +734,8 @@ Views views(float *p, int kin) {
 
 inline int blocks(long long n, int t = 256) { return (int)((n + t - 1) / t); }
 
+constexpr size_t kWsFloats = (size_t)1 << 21;  // split-K workspace per network (8 MB)
+
 // threshold of the class outputs: the routing threshold, or 0.5 when routing is off
 inline float class_threshold(const qcs_learned_net *net) { return net->count_th > 0.0f ? net->count_th : 0.5f; }
 
@@ -769,13 +744,13 @@ cudaError_t forward(qcs_learned_net *net, const float *x, int rows, float *z1, f
                     float *y, cudaStream_t s) {
     const Views w = views(net->d_par, net->kin);
     cudaError_t e;
-    if ((e = L::gemm(rows, L::kHidden, net->kin, x, net->kin, 1, w.W1, L::kHidden, 1, z1, L::kHidden, 0.0f, s)))
+    if ((e = L::gemm(rows, L::kHidden, net->kin, x, net->kin, 1, w.W1, L::kHidden, 1, z1, L::kHidden, 0.0f, s, net->d_ws, kWsFloats, net->d_err)))
         return e;
     L::bias_relu_kernel<<<blocks((long long)rows * L::kHidden), 256, 0, s>>>(z1, w.b1, rows, L::kHidden, a1, 1);
-    if ((e = L::gemm(rows, L::kHidden, L::kHidden, a1, L::kHidden, 1, w.W2, L::kHidden, 1, z2, L::kHidden, 0.0f, s)))
+    if ((e = L::gemm(rows, L::kHidden, L::kHidden, a1, L::kHidden, 1, w.W2, L::kHidden, 1, z2, L::kHidden, 0.0f, s, net->d_ws, kWsFloats, net->d_err)))
         return e;
     L::bias_relu_kernel<<<blocks((long long)rows * L::kHidden), 256, 0, s>>>(z2, w.b2, rows, L::kHidden, a2, 1);
-    if ((e = L::gemm(rows, L::kOut, L::kHidden, a2, L::kHidden, 1, w.W3, L::kOut, 1, y, L::kOut, 0.0f, s))) return e;
+    if ((e = L::gemm(rows, L::kOut, L::kHidden, a2, L::kHidden, 1, w.W3, L::kOut, 1, y, L::kOut, 0.0f, s, net->d_ws, kWsFloats, net->d_err))) return e;
     L::bias_relu_kernel<<<blocks((long long)rows * L::kOut), 256, 0, s>>>(y, w.b3, rows, L::kOut, y, 0);
     return cudaGetLastError();
 }
@@ -787,27 +762,27 @@ cudaError_t backward(qcs_learned_net *net, int rows, cudaStream_t s) {
     cudaError_t e;
     // layer 3: dW3 = a2^T dy, db3 = colsum(dy), d2 = dy W3^T
     if ((e = L::gemm(L::kHidden, L::kOut, rows, net->d_a2, 1, L::kHidden, net->d_dy, L::kOut, 1, g.W3, L::kOut, 0.0f,
-                     s)))
+                     s, net->d_ws, kWsFloats, net->d_err)))
         return e;
     L::colsum_kernel<<<1, L::kOut, 0, s>>>(net->d_dy, rows, L::kOut, g.b3);
     if ((e = L::gemm(rows, L::kHidden, L::kOut, net->d_dy, L::kOut, 1, w.W3, 1, L::kOut, net->d_d2, L::kHidden, 0.0f,
-                     s)))
+                     s, net->d_ws, kWsFloats, net->d_err)))
         return e;
     L::relu_back_kernel<<<blocks((long long)rows * L::kHidden), 256, 0, s>>>(net->d_d2, net->d_z2,
                                                                            (long long)rows * L::kHidden);
     // layer 2
     if ((e = L::gemm(L::kHidden, L::kHidden, rows, net->d_a1, 1, L::kHidden, net->d_d2, L::kHidden, 1, g.W2,
-                     L::kHidden, 0.0f, s)))
+                     L::kHidden, 0.0f, s, net->d_ws, kWsFloats, net->d_err)))
         return e;
     L::colsum_kernel<<<1, L::kHidden, 0, s>>>(net->d_d2, rows, L::kHidden, g.b2);
     if ((e = L::gemm(rows, L::kHidden, L::kHidden, net->d_d2, L::kHidden, 1, w.W2, 1, L::kHidden, net->d_d1,
-                     L::kHidden, 0.0f, s)))
+                     L::kHidden, 0.0f, s, net->d_ws, kWsFloats, net->d_err)))
         return e;
     L::relu_back_kernel<<<blocks((long long)rows * L::kHidden), 256, 0, s>>>(net->d_d1, net->d_z1,
                                                                            (long long)rows * L::kHidden);
     // layer 1
     if ((e = L::gemm(net->kin, L::kHidden, rows, net->d_x, 1, net->kin, net->d_d1, L::kHidden, 1, g.W1, L::kHidden,
-                     0.0f, s)))
+                     0.0f, s, net->d_ws, kWsFloats, net->d_err)))
         return e;
     L::colsum_kernel<<<1, L::kHidden, 0, s>>>(net->d_d1, rows, L::kHidden, g.b1);
     return cudaGetLastError();
@@ -949,15 +924,15 @@ int qcs_learned_destroy(qcs_learned_net *net) {
                                    "(qcs_learned_set_two_emitter(owner, NULL, ...)) or destroy the owner");
     if (net->two) net->two->owners--;
     net->two = nullptr;
-    if (net->stream) cudaStreamSynchronize(net->stream);
+    cudaDeviceSynchronize();  // no call of this network still in flight
     cudaFree(net->d_par);
     cudaFree(net->d_x);
     cudaFree(net->d_idx);
     cudaFree(net->d_start);
     cudaFree(net->d_wimg);
     cudaFree(net->d_err);
+    cudaFree(net->d_ws);
     if (net->wimg_ready) cudaEventDestroy(net->wimg_ready);
-    if (net->stream) cudaStreamDestroy(net->stream);
     delete net;
     return QCS_OK;
 }
@@ -987,8 +962,8 @@ int qcs_learned_create_for(int loc_type, int roi_size, int batch, unsigned long 
     if (e == cudaSuccess) e = cudaMalloc((void **)&net->d_idx, B * sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc((void **)&net->d_wimg, wimg_bytes);
     if (e == cudaSuccess) e = cudaMalloc((void **)&net->d_err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&net->d_ws, kWsFloats * sizeof(float));
     if (e == cudaSuccess) e = cudaMemset(net->d_err, 0, sizeof(int));
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&net->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&net->wimg_ready, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         qcs_learned_destroy(net);
@@ -1107,7 +1082,7 @@ int qcs_learned_targets_device(const qcs_loc_para *p, const uint16_t *d_rois, co
 
 int qcs_learned_forward_device(qcs_learned_net *net, const float *d_feat, int n, float *d_out, void *stream) {
     if (!net || !d_feat || !d_out) return fail(QCS_ERR_ARG, "null argument");
-    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : net->stream;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
     for (int r0 = 0; r0 < n; r0 += net->batch) {
         const int rows = (n - r0) < net->batch ? (n - r0) : net->batch;
         QCS_CUDA(forward(net, d_feat + (size_t)r0 * net->kin, rows, net->d_z1, net->d_a1, net->d_z2, net->d_a2,
@@ -1128,7 +1103,7 @@ int qcs_learned_gradient_counts_device(qcs_learned_net *net, const float *d_feat
     if (!net || !d_feat || !d_targets || !d_valid) return fail(QCS_ERR_ARG, "null argument");
     if (n <= 0 || n > net->batch) return fail(QCS_ERR_CAPACITY, "gradient batch must be 1..batch rows");
     if (d_classes && net->loc_type != QCS_LOCTYPE_GS2D) return fail(QCS_ERR_ARG, "count classes: GS2D networks only");
-    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : net->stream;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
     QCS_CUDA(cudaMemcpyAsync(net->d_x, d_feat, (size_t)n * net->kin * sizeof(float), cudaMemcpyDeviceToDevice, s),
              "copy features");
     QCS_CUDA(forward(net, net->d_x, n, net->d_z1, net->d_a1, net->d_z2, net->d_a2, net->d_y, s), "forward");
@@ -1163,7 +1138,7 @@ int qcs_learned_train_counts_device(qcs_learned_net *net, const float *d_feat, c
     if (!net || !d_feat || !d_targets || !d_valid) return fail(QCS_ERR_ARG, "null argument");
     if (n < net->batch) return fail(QCS_ERR_ARG, "fewer training rows than one batch");
     if (d_classes && net->loc_type != QCS_LOCTYPE_GS2D) return fail(QCS_ERR_ARG, "count classes: GS2D networks only");
-    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : net->stream;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int B = net->batch;
     const int steps = n / B;
     const int kin = net->kin, nu = L::used_outputs(net->loc_type);
@@ -1223,7 +1198,7 @@ int qcs_learned_start_device(qcs_learned_net *net, const qcs_loc_para *p, const 
     int st = check_shape(net, p);
     if (st) return st;
     if (n <= 0) return QCS_OK;
-    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : net->stream;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
     if (net->use_tc) {
         QCS_CUDA(fused_start_points(net, p, d_rois, n, nullptr, d_start, nullptr, s), "fused start points");
         return QCS_OK;
@@ -1250,7 +1225,7 @@ int qcs_learned_classes_device(qcs_learned_net *net, const qcs_loc_para *p, cons
     if (net->loc_type != QCS_LOCTYPE_GS2D) return fail(QCS_ERR_ARG, "count classes: GS2D networks only");
     if (n <= 0) return QCS_OK;
     if (!d_rois) return fail(QCS_ERR_ARG, "null ROI pointer");
-    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : net->stream;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
     QCS_CUDA(L::start_points(net, p, d_rois, n, d_start, s, d_classes), "start points and classes");
     return QCS_OK;
 }

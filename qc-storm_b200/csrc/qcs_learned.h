@@ -61,6 +61,47 @@ __host__ __device__ inline int count_class(float l0, float l1, float l2, float t
     return 0;
 }
 
+// Network outputs y (bias included) -> the fit's start point st
+// (start_width(LT) floats: peak e-, x, y, sigma(s), background e-), with
+// positions held inside the kind's accept window and widths in range.
+template <int R, int LT>
+__device__ __forceinline__ void start_from_outputs(const float *y, float lo, float rng, float *st) {
+    const float centre = R / 2.0f;
+    if (LT == kTwo) {
+        // emitters anywhere up to a pixel inside the ROI's edge
+        const float w2 = R / 2.0f - 1.0f;
+        st[0] = rng * expf(fminf(fmaxf(y[4], -6.0f), 3.0f));
+        st[1] = centre + fminf(fmaxf(y[0], -w2), w2);
+        st[2] = centre + fminf(fmaxf(y[1], -w2), w2);
+        st[3] = rng * expf(fminf(fmaxf(y[5], -6.0f), 3.0f));
+        st[4] = centre + fminf(fmaxf(y[2], -w2), w2);
+        st[5] = centre + fminf(fmaxf(y[3], -w2), w2);
+        st[6] = fminf(fmaxf(kSigma0 + y[6], 0.6f), 3.0f);
+        st[7] = fmaxf(lo + rng * y[7], 1.0f);
+        return;
+    }
+    const float win = LT == QCS_LOCTYPE_AS3D ? 2.5f : 1.5f;
+    const float smax = LT == QCS_LOCTYPE_AS3D ? 4.0f : 3.0f;
+    st[0] = rng * expf(fminf(fmaxf(y[3], -6.0f), 3.0f));
+    st[1] = centre + fminf(fmaxf(y[0], -win), win);
+    st[2] = centre + fminf(fmaxf(y[1], -win), win);
+    st[3] = fminf(fmaxf(kSigma0 + y[2], 0.6f), smax);
+    if (LT == QCS_LOCTYPE_AS3D) {
+        st[4] = fminf(fmaxf(kSigma0 + y[5], 0.6f), smax);
+        st[5] = fmaxf(lo + rng * y[4], 1.0f);
+    } else {
+        st[4] = fmaxf(lo + rng * y[4], 1.0f);
+    }
+}
+
+// C = beta C + A B on the tensor cores (tcgen05, BF16 operands rounded from
+// the FP32 ones, FP32 accumulation): M x N x K, A(m, k) = A[m sam + k sak],
+// B(k, n) = B[k sbk + n sbn], C row-major with ldc.  ws (ws_floats floats,
+// may be null): split-K partial sums, reduced in a fixed order.  err: set
+// when an MMA wait gave up.
+cudaError_t gemm(int M, int N, int K, const float *A, long long sam, long long sak, const float *B, long long sbk,
+                 long long sbn, float *C, int ldc, float beta, cudaStream_t s, float *ws, size_t ws_floats, int *err);
+
 // Start points (start_width floats per record) of n device records into out;
 // with cls set (GS2D networks), also each record's emitter-count class at the
 // network's count threshold.  With n_dev set the fused kernel reads the
