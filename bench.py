@@ -556,10 +556,11 @@ TRAIN_RECORDS = 200_000    # training records, same generator, seeds disjoint fr
 TRAIN_EPOCHS = 8
 
 
-def train_learned_net(para, stream, seed=4242):
-    """Train the start-point network on the GPU: TRAIN_RECORDS fresh records
-    labelled by plain fits, features and targets on the device, Adam over
-    TRAIN_EPOCHS epochs (qcs_learned_train_device).  Returns (net, info)."""
+def train_learned_net(para, stream, seed=4242, arch="mlp", lr=2e-3):
+    """Train the start-point network (arch "mlp" or "conv") on the GPU:
+    TRAIN_RECORDS fresh records labelled by plain fits, features and targets
+    on the device, Adam over TRAIN_EPOCHS epochs (qcs_learned_train_device).
+    Returns (net, info)."""
     import torch
     from qcstorm_b200 import lib, synth
     sh = stream.cuda_stream
@@ -571,10 +572,13 @@ def train_learned_net(para, stream, seed=4242):
     stream.synchronize()
     feat, scale = lib.LearnedNet.features(para, d_tr.data_ptr(), TRAIN_RECORDS, stream=sh)
     tgt, valid = lib.LearnedNet.targets(para, d_tr.data_ptr(), ctx.device_rows(), scale, TRAIN_RECORDS, stream=sh)
-    net = lib.LearnedNet(batch=4096, seed=5)
-    losses = net.train(feat, tgt, valid, epochs=TRAIN_EPOCHS, lr=2e-3, stream=sh)
+    net = lib.LearnedNet(batch=4096, seed=5, arch=arch)
+    stream.synchronize()
+    t1 = time.perf_counter()
+    losses = net.train(feat, tgt, valid, epochs=TRAIN_EPOCHS, lr=lr, stream=sh)
     stream.synchronize()
     info = {"records": TRAIN_RECORDS, "epochs": TRAIN_EPOCHS, "seconds": time.perf_counter() - t0,
+            "training_seconds": time.perf_counter() - t1, "lr": lr,
             "loss_first_epoch": float(losses[0]), "loss_last_epoch": float(losses[-1]),
             "labels": "plain MLEbfgs fits of the training records on this GPU"}
     ctx.close()
@@ -679,7 +683,9 @@ def learned_measure(args, streams, ctxs, para, d_batches, h_batches, rec0, truth
     e2e_steps = E2E_STEPS
     e2e_s, _ = e2e_pipelined(ctxs, streams, h_batches, e2e_steps, net=net)
     e2e_s = max_over_ranks(e2e_s * 1e3, dist) * 1e-3
+    start_ms = start_point_ms(net, para, d_batches, stream, dist)
     net.close()
+    conv = conv_arm(args, streams, ctxs, para, d_batches, rec0, truth0, plain_value, value, start_ms, world, dist)
     return {
         "value": value, "unit": UNIT, "ms_per_step": ms / args.steps, "vs_plain": value / plain_value,
         "windows": windows,
@@ -709,7 +715,69 @@ def learned_measure(args, streams, ctxs, para, d_batches, h_batches, rec0, truth
         "train": train,
         "network": "64-128-128-8 MLP on the 7x7 pixels (+2 scale features), BF16 operands, FP32 accumulation; "
                    "inference fused with the features in one tcgen05 kernel",
+        "start_points_ms_per_step": start_ms,
+        "conv": conv,
     }
+
+
+def start_point_ms(net, para, d_batches, stream, dist, steps=20):
+    """Device time of the start points alone (network inference) per
+    N_PER_STEP-record step."""
+    import torch
+    st = torch.empty((N_PER_STEP, 5), dtype=torch.float32, device="cuda")
+    work = torch.empty((N_PER_STEP * 200,), dtype=torch.float32, device="cuda")
+    from qcstorm_b200 import lib
+    import ctypes as C
+
+    def step(k, s):
+        lib.check(lib.load().qcs_learned_start_device(net.h, C.byref(para), C.c_void_p(d_batches[k % BATCHES].data_ptr()),
+                                                      N_PER_STEP, C.c_void_p(st.data_ptr()), C.c_void_p(work.data_ptr()),
+                                                      C.c_void_p(s.cuda_stream)))
+    return device_timed(steps, 3, step, [stream], dist) / steps
+
+
+def conv_arm(args, streams, ctxs, para, d_batches, rec0, truth0, plain_value, mlp_value, mlp_start_ms, world, dist):
+    """The convolutional start-point network (3x3 conv 32 -> 3x3 conv 64 ->
+    FC 256 -> the same outputs; qcs_learned_create_arch(QCS_LEARNED_ARCH_CONV))
+    trained on the same records and timed on the same batches with the same
+    schedule as the MLP: fits/s, start-point time and accuracy."""
+    stream, ctx = streams[0], ctxs[0]
+    sh = stream.cuda_stream
+    net, train = train_learned_net(para, stream, arch="conv", lr=1e-3)
+
+    def step(k, s, c=None):
+        net.localize(c or ctxs[k % 2], d_batches[k % BATCHES].data_ptr(), N_PER_STEP, 0, iters=LEARNED_ITERS,
+                     bisections=LEARNED_BISECTIONS, stream=s.cuda_stream)
+
+    steps = min(args.steps, 200)
+    ms = device_timed(steps, 3, step, streams, dist)
+    value = job_rate(steps, N_PER_STEP, world, ms)
+    start_ms = start_point_ms(net, para, d_batches, stream, dist)
+    ctx.localize_device(d_batches[0].data_ptr(), N_PER_STEP, 0, sh)
+    plain, _ = ctx.read_rows(sh)
+    step(0, stream, ctx)
+    rows, _ = ctx.read_rows(sh)
+    refits = net.refits(ctx)
+    net.fused_status()
+    net.close()
+    acc_p, acc_c = plain[:, 0] > 0, rows[:, 0] > 0
+    both = acc_p & acc_c
+    rp, pp, _ = fit_accuracy(plain, rec0, truth0, both, para)
+    rc, pc, _ = fit_accuracy(rows, rec0, truth0, both, para)
+    rc_own, _, _ = fit_accuracy(rows, rec0, truth0, acc_c, para)
+    return {"value": value, "unit": UNIT, "vs_plain": value / plain_value, "vs_mlp": value / mlp_value,
+            "steps": steps, "start_points_ms_per_step": start_ms, "mlp_start_points_ms_per_step": mlp_start_ms,
+            "iters": LEARNED_ITERS, "bisections": LEARNED_BISECTIONS, "refits_per_step": refits,
+            "accuracy": {"rmse_px": {"plain": rp, "conv": rc}, "photon_rel_rmse": {"plain": pp, "conv": pc},
+                         "rmse_px_own_accepted": rc_own, "accepted": {"plain": float(acc_p.mean()),
+                                                                      "conv": float(acc_c.mean())},
+                         "basis": "batch 0; records accepted by both (own_accepted: the conv arm's own)"},
+            "train": train,
+            "flops_per_record": 2 * (49 * 9 * 32 + 49 * 288 * 64 + (49 * 64 + 2) * 256 + 256 * 8),
+            "network": "conv 3x3x32 -> conv 3x3x64 -> FC 256 -> 8 outputs on the 7x7 pixels (+2 scale features into "
+                       "FC), BF16 operands, FP32 accumulation; inference: conv_tc_kernel (padded-grid implicit GEMM, "
+                       "tcgen05) + fc_tc_kernel (bulk-copy ring, tcgen05)",
+            "default": "mlp (the faster of the two at equal schedule and accuracy)"}
 
 
 SHAPE_RECORDS = 100_000    # records per call of the other learned workloads
@@ -1584,13 +1652,16 @@ def main():
                 "plain_rmse_over_fisher_crlb": a["fisher_crlb"]["plain"]["rms_error_over_own_crlb"],
                 "learned_rmse_over_fisher_crlb": a["fisher_crlb"]["learned"]["rms_error_over_own_crlb"],
                 "learned_equal_rmse_within_2pct_of_crlb": a["fisher_crlb"]["equal_rmse_within_2pct_of_crlb"],
+                "learned_conv_value": learned["conv"]["value"], "learned_conv_vs_plain": learned["conv"]["vs_plain"],
+                "learned_conv_rmse_px": learned["conv"]["accuracy"]["rmse_px"]["conv"],
             })
         # short keys first: the headline survives a truncated tail of the line
         head = ["metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better", "scaling",
                 "vs_baseline", "dtype", "data", "learned_value", "learned_vs_plain", "learned_e2e_value",
                 "learned_rmse_px", "plain_rmse_px", "learned_rmse_px_own", "plain_rmse_px_own", "learned_accept",
                 "plain_accept", "learned_equal_rmse", "crlb_px", "fisher_crlb_px", "plain_rmse_over_fisher_crlb",
-                "learned_rmse_over_fisher_crlb", "learned_equal_rmse_within_2pct_of_crlb", "gpu_launches", "windows",
+                "learned_rmse_over_fisher_crlb", "learned_equal_rmse_within_2pct_of_crlb", "learned_conv_value",
+                "learned_conv_vs_plain", "learned_conv_rmse_px", "gpu_launches", "windows",
                 "clocks", "roofline",
                 "e2e", "cpu_baseline", "config"]
         line = {**{k: line[k] for k in head if k in line}, **{k: v for k, v in line.items() if k not in head}}

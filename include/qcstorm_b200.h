@@ -523,6 +523,23 @@ int qcs_learned_param_count(void);
  * emitter 1, log(peak / range) of each, sigma - 1.3, (background - min) / range. */
 #define QCS_LEARNED_GS2D_2E 16
 int qcs_learned_create_for(int loc_type, int roi_size, int batch, unsigned long long seed, qcs_learned_net **out);
+/* Network architectures: the MLP above, and a convolutional network
+ * (3x3 conv, 32 channels, zero 'same' padding, ReLU -> 3x3 conv, 64 channels,
+ * ReLU -> fully connected 256 over the flattened 64 x R x R map (position
+ * major, channel minor) and the two scale features, ReLU -> the same eight
+ * outputs) on the first R*R features taken as the R x R image.  Same
+ * features, targets, loss, training and start-point entry points; its
+ * parameters, row-major [in][out]: W1 [9][32] (tap 3 (dy + 1) + (dx + 1)),
+ * b1, W2 [9 * 32][64] (row tap * 32 + input channel), b2, W3 [R*R*64 + 2][256],
+ * b3, W4 [256][8], b4.  Inference runs two tensor-core kernels per chunk of
+ * 65,536 records (0.4-1 GB of device memory per conv network for the
+ * flattened maps). */
+#define QCS_LEARNED_ARCH_MLP 0
+#define QCS_LEARNED_ARCH_CONV 1
+int qcs_learned_create_arch(int arch, int loc_type, int roi_size, int batch, unsigned long long seed,
+                            qcs_learned_net **out);
+/* QCS_LEARNED_ARCH_MLP or QCS_LEARNED_ARCH_CONV (-1 for NULL). */
+int qcs_learned_arch(const qcs_learned_net *net);
 /* qcs_learned_create_for(QCS_LOCTYPE_GS2D, 7, batch, seed, out). */
 int qcs_learned_create(int batch, unsigned long long seed, qcs_learned_net **out);
 /* The network's localization type, ROI size and parameter count (any may be NULL). */

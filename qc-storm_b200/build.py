@@ -24,7 +24,7 @@ FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2,-ffp-contrac
 
 UNITS = ["qcs_fit_kernels.cu", "qcs_crlb.cu", "qcs_wle.cu", "qcs_cascade.cu", "qcs_api.cu", "qcs_diag.cu", "qcs_noalloc.cu",
          "qcs_extract.cu", "qcs_post.cu", "qcs_learned.cu", "qcs_render.cu",
-         "qcs_locfile.cu", "qcs_consec.cu", "qcs_stat.cu", "qcs_crlb_fisher.cu"]
+         "qcs_locfile.cu", "qcs_consec.cu", "qcs_stat.cu", "qcs_crlb_fisher.cu", "qcs_convnet.cu"]
 
 
 def deps():

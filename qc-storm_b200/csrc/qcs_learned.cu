@@ -707,6 +707,9 @@ struct qcs_learned_net {
     __nv_bfloat16 *d_wimg = nullptr;  // BF16 operand images of the weights (fused inference)
     int *d_err = nullptr;             // set by a tensor-core kernel when an MMA wait gives up
     float *d_ws = nullptr;            // split-K partial sums of the training GEMMs
+    size_t ws_floats = 0;
+    int arch = QCS_LEARNED_ARCH_MLP;
+    qcs::learned::conv::State *conv = nullptr;  // QCS_LEARNED_ARCH_CONV: activations and inference buffers
     unsigned version = 1;             // bumped whenever the parameters change
     unsigned wimg_version = 0;        // parameter version d_wimg was built from
     cudaEvent_t wimg_ready = nullptr; // recorded after d_wimg was built
@@ -742,47 +745,52 @@ inline float class_threshold(const qcs_learned_net *net) { return net->count_th 
 // Forward over `rows` feature rows into net->d_y (and the hidden activations).
 cudaError_t forward(qcs_learned_net *net, const float *x, int rows, float *z1, float *a1, float *z2, float *a2,
                     float *y, cudaStream_t s) {
+    if (net->conv)
+        return L::conv::forward(net->conv, net->d_par, x, rows, net->kin, y, s, net->d_ws, net->ws_floats, net->d_err);
     const Views w = views(net->d_par, net->kin);
     cudaError_t e;
-    if ((e = L::gemm(rows, L::kHidden, net->kin, x, net->kin, 1, w.W1, L::kHidden, 1, z1, L::kHidden, 0.0f, s, net->d_ws, kWsFloats, net->d_err)))
+    if ((e = L::gemm(rows, L::kHidden, net->kin, x, net->kin, 1, w.W1, L::kHidden, 1, z1, L::kHidden, 0.0f, s, net->d_ws, net->ws_floats, net->d_err)))
         return e;
     L::bias_relu_kernel<<<blocks((long long)rows * L::kHidden), 256, 0, s>>>(z1, w.b1, rows, L::kHidden, a1, 1);
-    if ((e = L::gemm(rows, L::kHidden, L::kHidden, a1, L::kHidden, 1, w.W2, L::kHidden, 1, z2, L::kHidden, 0.0f, s, net->d_ws, kWsFloats, net->d_err)))
+    if ((e = L::gemm(rows, L::kHidden, L::kHidden, a1, L::kHidden, 1, w.W2, L::kHidden, 1, z2, L::kHidden, 0.0f, s, net->d_ws, net->ws_floats, net->d_err)))
         return e;
     L::bias_relu_kernel<<<blocks((long long)rows * L::kHidden), 256, 0, s>>>(z2, w.b2, rows, L::kHidden, a2, 1);
-    if ((e = L::gemm(rows, L::kOut, L::kHidden, a2, L::kHidden, 1, w.W3, L::kOut, 1, y, L::kOut, 0.0f, s, net->d_ws, kWsFloats, net->d_err))) return e;
+    if ((e = L::gemm(rows, L::kOut, L::kHidden, a2, L::kHidden, 1, w.W3, L::kOut, 1, y, L::kOut, 0.0f, s, net->d_ws, net->ws_floats, net->d_err))) return e;
     L::bias_relu_kernel<<<blocks((long long)rows * L::kOut), 256, 0, s>>>(y, w.b3, rows, L::kOut, y, 0);
     return cudaGetLastError();
 }
 
 // Backward of the masked MSE for one batch already forwarded; fills d_grad.
 cudaError_t backward(qcs_learned_net *net, int rows, cudaStream_t s) {
+    if (net->conv)
+        return L::conv::backward(net->conv, net->d_par, net->d_grad, net->d_x, rows, net->kin, net->d_dy, s, net->d_ws,
+                                 net->ws_floats, net->d_err);
     const Views w = views(net->d_par, net->kin);
     const Views g = views(net->d_grad, net->kin);
     cudaError_t e;
     // layer 3: dW3 = a2^T dy, db3 = colsum(dy), d2 = dy W3^T
     if ((e = L::gemm(L::kHidden, L::kOut, rows, net->d_a2, 1, L::kHidden, net->d_dy, L::kOut, 1, g.W3, L::kOut, 0.0f,
-                     s, net->d_ws, kWsFloats, net->d_err)))
+                     s, net->d_ws, net->ws_floats, net->d_err)))
         return e;
     L::colsum_kernel<<<1, L::kOut, 0, s>>>(net->d_dy, rows, L::kOut, g.b3);
     if ((e = L::gemm(rows, L::kHidden, L::kOut, net->d_dy, L::kOut, 1, w.W3, 1, L::kOut, net->d_d2, L::kHidden, 0.0f,
-                     s, net->d_ws, kWsFloats, net->d_err)))
+                     s, net->d_ws, net->ws_floats, net->d_err)))
         return e;
     L::relu_back_kernel<<<blocks((long long)rows * L::kHidden), 256, 0, s>>>(net->d_d2, net->d_z2,
                                                                            (long long)rows * L::kHidden);
     // layer 2
     if ((e = L::gemm(L::kHidden, L::kHidden, rows, net->d_a1, 1, L::kHidden, net->d_d2, L::kHidden, 1, g.W2,
-                     L::kHidden, 0.0f, s, net->d_ws, kWsFloats, net->d_err)))
+                     L::kHidden, 0.0f, s, net->d_ws, net->ws_floats, net->d_err)))
         return e;
     L::colsum_kernel<<<1, L::kHidden, 0, s>>>(net->d_d2, rows, L::kHidden, g.b2);
     if ((e = L::gemm(rows, L::kHidden, L::kHidden, net->d_d2, L::kHidden, 1, w.W2, 1, L::kHidden, net->d_d1,
-                     L::kHidden, 0.0f, s, net->d_ws, kWsFloats, net->d_err)))
+                     L::kHidden, 0.0f, s, net->d_ws, net->ws_floats, net->d_err)))
         return e;
     L::relu_back_kernel<<<blocks((long long)rows * L::kHidden), 256, 0, s>>>(net->d_d1, net->d_z1,
                                                                            (long long)rows * L::kHidden);
     // layer 1
     if ((e = L::gemm(net->kin, L::kHidden, rows, net->d_x, 1, net->kin, net->d_d1, L::kHidden, 1, g.W1, L::kHidden,
-                     0.0f, s, net->d_ws, kWsFloats, net->d_err)))
+                     0.0f, s, net->d_ws, net->ws_floats, net->d_err)))
         return e;
     L::colsum_kernel<<<1, L::kHidden, 0, s>>>(net->d_d1, rows, L::kHidden, g.b1);
     return cudaGetLastError();
@@ -840,6 +848,9 @@ cudaError_t by_shape(int loc_type, int R, F &&f) {
 cudaError_t fused_start_points(qcs_learned_net *net, const qcs_loc_para *p, const uint16_t *d_rois, int n,
                                const int *n_dev, float *start, uint8_t *cls, cudaStream_t s) {
     if (n <= 0) return cudaSuccess;
+    if (net->conv)
+        return L::conv::start_points(net->conv, net->d_par, net->version, net->loc_type, p, d_rois, n, n_dev, start, cls,
+                                     class_threshold(net), s, net->d_err);
     const int tiles = (n + L::tc::kM - 1) / L::tc::kM;
     int dev = 0, sms = 148;
     cudaError_t e = cudaGetDevice(&dev);
@@ -932,14 +943,24 @@ int qcs_learned_destroy(qcs_learned_net *net) {
     cudaFree(net->d_wimg);
     cudaFree(net->d_err);
     cudaFree(net->d_ws);
+    L::conv::destroy(net->conv);
     if (net->wimg_ready) cudaEventDestroy(net->wimg_ready);
     delete net;
     return QCS_OK;
 }
 
 int qcs_learned_create_for(int loc_type, int roi_size, int batch, unsigned long long seed, qcs_learned_net **out) {
+    return qcs_learned_create_arch(QCS_LEARNED_ARCH_MLP, loc_type, roi_size, batch, seed, out);
+}
+
+int qcs_learned_arch(const qcs_learned_net *net) { return net ? net->arch : -1; }
+
+int qcs_learned_create_arch(int arch, int loc_type, int roi_size, int batch, unsigned long long seed,
+                            qcs_learned_net **out) {
     if (!out) return fail(QCS_ERR_ARG, "null output handle");
     *out = nullptr;
+    if (arch != QCS_LEARNED_ARCH_MLP && arch != QCS_LEARNED_ARCH_CONV)
+        return fail(QCS_ERR_ARG, "architecture: QCS_LEARNED_ARCH_MLP or QCS_LEARNED_ARCH_CONV");
     if (!L::shape_supported(loc_type, roi_size))
         return fail(QCS_ERR_ROISIZE, "learned start points: GS2D or AS3D, ROISize 7, 9 or 11");
     if (batch <= 0) batch = 4096;
@@ -950,7 +971,9 @@ int qcs_learned_create_for(int loc_type, int roi_size, int batch, unsigned long 
     net->loc_type = loc_type;
     net->R = roi_size;
     net->kin = L::in_width(roi_size);
-    net->params = L::param_count(net->kin);
+    net->arch = arch;
+    net->params = arch == QCS_LEARNED_ARCH_CONV ? L::conv::param_count(roi_size) : L::param_count(net->kin);
+    net->ws_floats = arch == QCS_LEARNED_ARCH_CONV ? 4 * kWsFloats : kWsFloats;
     net->batch = batch;
     const int kin = net->kin;
     const size_t P = net->params;
@@ -962,7 +985,8 @@ int qcs_learned_create_for(int loc_type, int roi_size, int batch, unsigned long 
     if (e == cudaSuccess) e = cudaMalloc((void **)&net->d_idx, B * sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc((void **)&net->d_wimg, wimg_bytes);
     if (e == cudaSuccess) e = cudaMalloc((void **)&net->d_err, sizeof(int));
-    if (e == cudaSuccess) e = cudaMalloc((void **)&net->d_ws, kWsFloats * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&net->d_ws, net->ws_floats * sizeof(float));
+    if (e == cudaSuccess && arch == QCS_LEARNED_ARCH_CONV) e = L::conv::create(roi_size, batch, &net->conv);
     if (e == cudaSuccess) e = cudaMemset(net->d_err, 0, sizeof(int));
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&net->wimg_ready, cudaEventDisableTiming);
     if (e != cudaSuccess) {
@@ -1003,13 +1027,17 @@ int qcs_learned_create_for(int loc_type, int roi_size, int batch, unsigned long 
         st ^= st << 17;
         return (float)((st >> 11) * (1.0 / 9007199254740992.0)) * 2.0f - 1.0f;
     };
-    const Views hv = views(h, kin);
-    for (int i = 0; i < kin * L::kHidden; ++i) hv.W1[i] = uni() * sqrtf(6.0f / kin);
-    for (int i = 0; i < L::kHidden; ++i) hv.b1[i] = 0.0f;
-    for (int i = 0; i < L::kHidden * L::kHidden; ++i) hv.W2[i] = uni() * sqrtf(6.0f / L::kHidden);
-    for (int i = 0; i < L::kHidden; ++i) hv.b2[i] = 0.0f;
-    for (int i = 0; i < L::kHidden * L::kOut; ++i) hv.W3[i] = uni() * sqrtf(3.0f / L::kHidden);
-    for (int i = 0; i < L::kOut; ++i) hv.b3[i] = 0.0f;
+    if (net->conv) {
+        L::conv::init_params(h, roi_size, seed);
+    } else {
+        const Views hv = views(h, kin);
+        for (int i = 0; i < kin * L::kHidden; ++i) hv.W1[i] = uni() * sqrtf(6.0f / kin);
+        for (int i = 0; i < L::kHidden; ++i) hv.b1[i] = 0.0f;
+        for (int i = 0; i < L::kHidden * L::kHidden; ++i) hv.W2[i] = uni() * sqrtf(6.0f / L::kHidden);
+        for (int i = 0; i < L::kHidden; ++i) hv.b2[i] = 0.0f;
+        for (int i = 0; i < L::kHidden * L::kOut; ++i) hv.W3[i] = uni() * sqrtf(3.0f / L::kHidden);
+        for (int i = 0; i < L::kOut; ++i) hv.b3[i] = 0.0f;
+    }
     e = cudaMemcpy(net->d_par, h, P * sizeof(float), cudaMemcpyHostToDevice);
     delete[] h;
     if (e == cudaSuccess) e = cudaMemset(net->d_m, 0, 2 * P * sizeof(float));
@@ -1318,7 +1346,14 @@ cudaError_t qcs::learned::start_points(qcs_learned_net *net, const qcs_loc_para 
     return by_shape(net->loc_type, net->R, [&](auto sh) -> cudaError_t {
         constexpr int R = decltype(sh)::R, LT = decltype(sh)::LT;
         L::features_kernel<R><<<blocks(n), 256, 0, s>>>(d_rois, n, p->Offset, p->KAdc, feat, scale);
-        cudaError_t e = forward(net, feat, n, h1, h1, h2, h2, y, s);
+        cudaError_t e = cudaSuccess;
+        if (net->conv) {  // the conv net's activations hold one batch
+            for (int r0 = 0; r0 < n && e == cudaSuccess; r0 += net->batch)
+                e = forward(net, feat + (size_t)r0 * kin, n - r0 < net->batch ? n - r0 : net->batch, nullptr, nullptr,
+                            nullptr, nullptr, y + (size_t)r0 * L::kOut, s);
+        } else {
+            e = forward(net, feat, n, h1, h1, h2, h2, y, s);
+        }
         if (e != cudaSuccess) return e;
         L::start_kernel<R, LT><<<blocks(n), 256, 0, s>>>(y, scale, n, out, LT == QCS_LOCTYPE_GS2D ? cls : nullptr, th);
         return cudaGetLastError();

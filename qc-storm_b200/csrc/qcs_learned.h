@@ -109,6 +109,25 @@ cudaError_t gemm(int M, int N, int K, const float *A, long long sam, long long s
 cudaError_t start_points(qcs_learned_net *net, const qcs_loc_para *p, const uint16_t *d_rois, int n, float *out,
                          cudaStream_t s, uint8_t *cls = nullptr, const int *n_dev = nullptr);
 
+// The convolutional network (qcs_convnet.cu): parameter count, training
+// activations and inference buffers (State), forward / backward of one
+// batch of feature rows, and the start points of n records through its two
+// tcgen05 kernels (weight images rebuilt when `version` changes).
+namespace conv {
+struct State;
+int param_count(int R);
+cudaError_t create(int R, int batch, State **out);
+void destroy(State *st);
+void init_params(float *h, int R, unsigned long long seed);
+cudaError_t forward(State *st, const float *par, const float *feat, int rows, int kin, float *y, cudaStream_t s,
+                    float *ws, size_t wsf, int *err);
+cudaError_t backward(State *st, const float *par, float *grad, const float *feat, int rows, int kin, const float *dy,
+                     cudaStream_t s, float *ws, size_t wsf, int *err);
+cudaError_t start_points(State *st, const float *par, unsigned version, int loc_type, const qcs_loc_para *p,
+                         const uint16_t *rois, int n, const int *n_dev, float *out, uint8_t *cls, float th,
+                         cudaStream_t s, int *err);
+}  // namespace conv
+
 // The two-emitter network attached to a GS2D network (qcs_learned_set_two_emitter),
 // its schedule and fallback (to3e: poor fits go on to the three-emitter fit), or null.
 qcs_learned_net *two_emitter(const qcs_learned_net *net, int *iters, int *bisections, float *dev_th, int *to3e);

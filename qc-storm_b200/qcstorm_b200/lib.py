@@ -160,6 +160,8 @@ _SIGS = {
     "qcs_stat_update_ontime_ratio": (C.c_int, [C.c_void_p, C.c_void_p]),
     "qcs_stat_ontime": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_void_p]),
     "qcs_learned_create_for": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_ulonglong, C.POINTER(C.c_void_p)]),
+    "qcs_learned_create_arch": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_ulonglong, C.POINTER(C.c_void_p)]),
+    "qcs_learned_arch": (C.c_int, [C.c_void_p]),
     "qcs_learned_shape": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "qcs_learned_localize_device_n": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(LocPara),
                                                 C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_void_p]),
@@ -537,15 +539,21 @@ def learned_start_width(loc_type):
     return 8 if loc_type == LEARNED_GS2D_2E else (6 if loc_type == 1 else 5)
 
 
+LEARNED_ARCH = {"mlp": 0, "conv": 1}  # QCS_LEARNED_ARCH_MLP, QCS_LEARNED_ARCH_CONV
+
+
 class LearnedNet:
     """Learned start points (qcs_learned_*) for one localization type and ROI
-    size (GS2D or AS3D; 7, 9 or 11): device tensors are torch CUDA tensors."""
+    size (GS2D or AS3D; 7, 9 or 11): device tensors are torch CUDA tensors.
+    arch: "mlp" (the default network) or "conv" (the convolutional one)."""
 
-    def __init__(self, batch=4096, seed=1, loc_type=0, roi_size=7):
+    def __init__(self, batch=4096, seed=1, loc_type=0, roi_size=7, arch="mlp"):
         self.lib = load()
         h = C.c_void_p()
-        check(self.lib.qcs_learned_create_for(int(loc_type), int(roi_size), int(batch), int(seed), C.byref(h)))
+        check(self.lib.qcs_learned_create_arch(LEARNED_ARCH[arch], int(loc_type), int(roi_size), int(batch), int(seed),
+                                               C.byref(h)))
         self.h = h
+        self.arch = arch
         lt, rs, npar = C.c_int(0), C.c_int(0), C.c_int(0)
         check(self.lib.qcs_learned_shape(h, C.byref(lt), C.byref(rs), C.byref(npar)))
         self.loc_type, self.roi_size, self.n_params = lt.value, rs.value, npar.value
