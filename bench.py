@@ -1351,6 +1351,47 @@ def profile_learned(n, stream):
     return 0
 
 
+def profile_conv(n, stream):
+    """The convolutional start-point network's inference (conv_tc_kernel +
+    fc_tc_kernel) three times over n GS2D 7x7 records, untrained weights
+    (the kernels' work does not depend on the values), for ncu."""
+    import torch
+    from qcstorm_b200 import lib, synth
+    rec, para, _ = synth.gs2d_rois(n, R=R, seed=5)
+    d = torch.from_numpy(rec.view(np.int16)).cuda()
+    net = lib.LearnedNet(batch=1024, seed=4, arch="conv")
+    for _ in range(3):
+        net.start(para, d.data_ptr(), n, stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    net.fused_status()
+    print(json.dumps({"profile_conv": n}))
+    net.close()
+    return 0
+
+
+def profile_train(n, stream):
+    """One training epoch of the MLP and of the conv start-point network over
+    n GS2D 7x7 records labelled by plain fits (tcgen05 GEMMs), for ncu."""
+    import torch
+    from qcstorm_b200 import lib, synth
+    rec, para, _ = synth.gs2d_rois(n, R=R, seed=5)
+    d = torch.from_numpy(rec.view(np.int16)).cuda()
+    sh = stream.cuda_stream
+    ctx = lib.LocContext(para, capacity=n)
+    ctx.localize_device(d.data_ptr(), n, 0, sh)
+    feat, scale = lib.LearnedNet.features(para, d.data_ptr(), n, stream=sh)
+    tgt, valid = lib.LearnedNet.targets(para, d.data_ptr(), ctx.device_rows(), scale, n, stream=sh)
+    out = {}
+    for arch in ("mlp", "conv"):
+        net = lib.LearnedNet(batch=4096, seed=5, arch=arch)
+        out[arch] = float(net.train(feat, tgt, valid, epochs=1, lr=1e-3, stream=sh)[0])
+        net.fused_status()
+        net.close()
+    ctx.close()
+    print(json.dumps({"profile_train": n, "loss": out}))
+    return 0
+
+
 def profile_multi(n, stream):
     """The 1-3 emitter 11x11 workload for ncu: networks trained as in
     learned_shapes_measure (count classes and two-emitter starts, SHAPE_TRAIN
@@ -1461,6 +1502,10 @@ def main():
                          "in the NVTX ranges plain and learned (for ncu)")
     ap.add_argument("--profile-learned", type=int, default=0, metavar="N",
                     help="only train the start-point network and run 3 learned-start calls on N records")
+    ap.add_argument("--profile-conv", type=int, default=0, metavar="N",
+                    help="only run the conv start-point network's inference 3 times on N records (for ncu)")
+    ap.add_argument("--profile-train", type=int, default=0, metavar="N",
+                    help="only run one training epoch of each start-point network on N records (for ncu)")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-start measurement")
     ap.add_argument("--no-mixed", action="store_true",
                     help="skip the mixed 7/9/11 learned measurement (4e6 training, 1e7 evaluation records)")
@@ -1492,6 +1537,10 @@ def main():
         return profile_learned(args.profile_learned, stream)
     if args.profile_multi:
         return profile_multi(args.profile_multi, stream)
+    if args.profile_conv:
+        return profile_conv(args.profile_conv, stream)
+    if args.profile_train:
+        return profile_train(args.profile_train, stream)
     dist = None
     if world > 1:
         import datetime

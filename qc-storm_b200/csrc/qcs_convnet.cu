@@ -146,36 +146,6 @@ __global__ void relu_back_kernel(float *__restrict__ d, const float *__restrict_
     if (i < total && !(z[i] > 0.0f)) d[i] = 0.0f;
 }
 
-// Column sums of d (rows x cols), two passes with a fixed order: block
-// (x, z) sums split z's rows of 32 columns into part[z][cols]; then
-// colsum_final adds the splits in order.
-constexpr int kSumSplits = 128;
-__global__ void colsum_part_kernel(const float *__restrict__ d, long long rows, int cols, float *__restrict__ part) {
-    __shared__ float acc[8][33];
-    const int c = blockIdx.x * 32 + threadIdx.x;
-    const long long per = (rows + gridDim.y - 1) / gridDim.y;
-    const long long r0 = (long long)blockIdx.y * per, r1 = r0 + per < rows ? r0 + per : rows;
-    float s = 0.0f;
-    if (c < cols)
-        for (long long r = r0 + threadIdx.y; r < r1; r += 8) s += d[r * cols + c];
-    acc[threadIdx.y][threadIdx.x] = s;
-    __syncthreads();
-    if (threadIdx.y == 0 && c < cols) {
-        float t = 0.0f;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) t += acc[k][threadIdx.x];
-        part[(size_t)blockIdx.y * cols + c] = t;
-    }
-}
-
-__global__ void colsum_final_kernel(const float *__restrict__ part, int splits, int cols, float *__restrict__ g) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= cols) return;
-    float s = 0.0f;
-    for (int z = 0; z < splits; ++z) s += part[(size_t)z * cols + c];
-    g[c] = s;
-}
-
 // ----------------------------------------------------- inference kernels
 // Shape of a conv_tc_kernel group for R x R ROIs: T ROIs per group on a
 // padded grid of rows (pitch PR = R + 1, PB = PR^2 rows per ROI, front
@@ -720,7 +690,7 @@ cudaError_t create(int R, int batch, State **out) {
     st->batch = batch;
     const size_t P = (size_t)batch * R * R;
     const size_t fl = P * (kTaps + 2 * kC1 + kTaps * kC1 + 2 * kC2) + (size_t)batch * 3 * kFc +
-                      (size_t)kSumSplits * kFc;
+                      (size_t)kColsumSplits * kFc;
     cudaError_t e = cudaMalloc((void **)&st->x1, fl * sizeof(float));
     if (e == cudaSuccess) {
         float *a = st->x1 + P * kTaps;
@@ -776,15 +746,6 @@ void init_params(float *h, int R, unsigned long long seed) {
     for (size_t i = o.W4; i < o.b4; ++i) h[i] = uni() * sqrtf(3.0f / kFc);
 }
 
-static cudaError_t colsum(const float *d, long long rows, int cols, float *g, float *part, cudaStream_t s) {
-    int splits = (int)((rows + 255) / 256);
-    if (splits > kSumSplits) splits = kSumSplits;
-    if (splits < 1) splits = 1;
-    colsum_part_kernel<<<dim3((cols + 31) / 32, splits), dim3(32, 8), 0, s>>>(d, rows, cols, part);
-    colsum_final_kernel<<<(cols + 127) / 128, 128, 0, s>>>(part, splits, cols, g);
-    return cudaGetLastError();
-}
-
 cudaError_t forward(State *st, const float *par, const float *feat, int rows, int kin, float *y, cudaStream_t s,
                     float *ws, size_t wsf, int *err) {
     const int R = st->R;
@@ -817,7 +778,7 @@ cudaError_t backward(State *st, const float *par, float *grad, const float *feat
     cudaError_t e;
     // head
     if ((e = gemm(kFc, kOut, rows, st->a3, 1, kFc, dy, kOut, 1, grad + o.W4, kOut, 0.0f, s, ws, wsf, err))) return e;
-    if ((e = colsum(dy, rows, kOut, grad + o.b4, st->part, s))) return e;
+    if ((e = column_sums(dy, rows, kOut, grad + o.b4, st->part, s))) return e;
     if ((e = gemm(rows, kFc, kOut, dy, kOut, 1, par + o.W4, 1, kOut, st->d3, kFc, 0.0f, s, ws, wsf, err))) return e;
     relu_back_kernel<<<nblk((long long)rows * kFc), 256, 0, s>>>(st->d3, st->z3, (long long)rows * kFc);
     // FC: map rows and the two scale rows of W3
@@ -825,7 +786,7 @@ cudaError_t backward(State *st, const float *par, float *grad, const float *feat
     if ((e = gemm(2, kFc, rows, feat + R * R, 1, kin, st->d3, kFc, 1, grad + o.W3 + (size_t)K0 * kFc, kFc, 0.0f, s, ws,
                   wsf, err)))
         return e;
-    if ((e = colsum(st->d3, rows, kFc, grad + o.b3, st->part, s))) return e;
+    if ((e = column_sums(st->d3, rows, kFc, grad + o.b3, st->part, s))) return e;
     // dA2 = d3 W3[map rows]^T, over a2 (no longer needed)
     if ((e = gemm(rows, K0, kFc, st->d3, kFc, 1, par + o.W3, 1, kFc, st->a2, K0, 0.0f, s, ws, wsf, err))) return e;
     relu_back_kernel<<<nblk(P * kC2), 256, 0, s>>>(st->a2, st->z2, P * kC2);
@@ -833,7 +794,7 @@ cudaError_t backward(State *st, const float *par, float *grad, const float *feat
     if ((e = gemm(kTaps * kC1, kC2, (int)P, st->x2, 1, kTaps * kC1, st->a2, kC2, 1, grad + o.W2, kC2, 0.0f, s, ws, wsf,
                   err)))
         return e;
-    if ((e = colsum(st->a2, P, kC2, grad + o.b2, st->part, s))) return e;
+    if ((e = column_sums(st->a2, P, kC2, grad + o.b2, st->part, s))) return e;
     // dX2 = dZ2 W2^T over x2, then dA1 over a1
     if ((e = gemm((int)P, kTaps * kC1, kC2, st->a2, kC2, 1, par + o.W2, 1, kC2, st->x2, kTaps * kC1, 0.0f, s, ws, wsf,
                   err)))
@@ -843,7 +804,7 @@ cudaError_t backward(State *st, const float *par, float *grad, const float *feat
     // conv1
     if ((e = gemm(kTaps, kC1, (int)P, st->x1, 1, kTaps, st->a1, kC1, 1, grad + o.W1, kC1, 0.0f, s, ws, wsf, err)))
         return e;
-    if ((e = colsum(st->a1, P, kC1, grad + o.b1, st->part, s))) return e;
+    if ((e = column_sums(st->a1, P, kC1, grad + o.b1, st->part, s))) return e;
     return cudaGetLastError();
 }
 

@@ -163,7 +163,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         uint8_t *a_img = base + buf * a_bytes, *b_img = base + 2 * a_bytes + buf * b_bytes;
         // A: row tid, K groups 0..7 of the chunk
         const int gm = m0 + tid;
-#pragma unroll 2
+#pragma unroll
         for (int kg = 0; kg < kGemmK / 8; ++kg) {
             float v[8];
 #pragma unroll
@@ -174,6 +174,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
             *reinterpret_cast<uint4 *>(a_img + (size_t)(kg * kGemmM + tid) * 16) = tc::pack8(v);
         }
         // B: bn rows (n) x 8 K groups
+#pragma unroll 4
         for (int u = tid; u < bn * (kGemmK / 8); u += kGemmThreads) {
             const int kg = u / bn, nn = u - kg * bn, gn = n0 + nn;
             float v[8];
@@ -205,28 +206,42 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         ok = ok && done;
     }
     tc::fence_after();
-    const int row = m0 + warp * 32 + lane;
     if (ok) {
-        for (int c0 = 0; c0 < bn; c0 += 16) {
-            float v[16];
-            if (issued > 0) {
-                tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + c0, v);
-            } else {
+        // 64 columns at a time through shared memory (the operand buffers are
+        // free once the last MMA has ended): each thread stores its row, then
+        // each warp writes whole rows, lanes along the columns (coalesced)
+        float *stage = reinterpret_cast<float *>(base);  // [128][65]
+        float *out = part ? part + (size_t)blockIdx.z * M * N : Cm;
+        const long long ld = part ? N : ldc;
+        const float b = part ? 0.0f : beta;
+        for (int c0 = 0; c0 < bn; c0 += 64) {
 #pragma unroll
-                for (int j = 0; j < 16; ++j) v[j] = 0.0f;
-            }
-            if (row >= M) continue;
-#pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                const int col = n0 + c0 + j;
-                if (col >= N) continue;
-                if (part) {
-                    part[((size_t)blockIdx.z * M + row) * N + col] = v[j];
+            for (int q = 0; q < 64; q += 16) {
+                float v[16];
+                if (issued > 0) {
+                    tc::tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + c0 + q, v);
                 } else {
-                    float *dst = Cm + (size_t)row * ldc + col;
-                    *dst = (beta == 0.0f) ? v[j] : beta * (*dst) + v[j];
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) v[j] = 0.0f;
+                }
+#pragma unroll
+                for (int j = 0; j < 16; ++j) stage[tid * 65 + q + j] = v[j];
+            }
+            __syncthreads();
+            for (int r = warp * 32; r < warp * 32 + 32; ++r) {
+                const int row = m0 + r;
+                if (row >= M) break;
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int c = c0 + h * 32 + lane, col = n0 + c;
+                    if (c < bn && col < N) {
+                        float *dst = out + (size_t)row * ld + col;
+                        const float v = stage[r * 65 + h * 32 + lane];
+                        *dst = (b == 0.0f) ? v : b * (*dst) + v;
+                    }
                 }
             }
+            __syncthreads();
         }
     } else if (tid == 0 && err) {
         atomicExch(err, 1);
@@ -307,13 +322,42 @@ __global__ void relu_back_kernel(float *__restrict__ dA, const float *__restrict
     if (!(Z[i] > 0.0f)) dA[i] = 0.0f;
 }
 
-// Column sums of dZ (rows x cols) into g (bias gradient), one block per column group.
-__global__ void colsum_kernel(const float *__restrict__ dZ, int rows, int cols, float *__restrict__ g) {
+// Column sums of d (rows x cols), two passes with a fixed order: block
+// (x, z) sums split z's rows of 32 columns into part[z][cols]; then
+// colsum_final adds the splits in order.
+__global__ void colsum_part_kernel(const float *__restrict__ d, long long rows, int cols, float *__restrict__ part) {
+    __shared__ float acc[8][33];
+    const int c = blockIdx.x * 32 + threadIdx.x;
+    const long long per = (rows + gridDim.y - 1) / gridDim.y;
+    const long long r0 = (long long)blockIdx.y * per, r1 = r0 + per < rows ? r0 + per : rows;
+    float s = 0.0f;
+    if (c < cols)
+        for (long long r = r0 + threadIdx.y; r < r1; r += 8) s += d[r * cols + c];
+    acc[threadIdx.y][threadIdx.x] = s;
+    __syncthreads();
+    if (threadIdx.y == 0 && c < cols) {
+        float t = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) t += acc[k][threadIdx.x];
+        part[(size_t)blockIdx.y * cols + c] = t;
+    }
+}
+
+__global__ void colsum_final_kernel(const float *__restrict__ part, int splits, int cols, float *__restrict__ g) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= cols) return;
     float s = 0.0f;
-    for (int r = 0; r < rows; ++r) s += dZ[(size_t)r * cols + c];
+    for (int z = 0; z < splits; ++z) s += part[(size_t)z * cols + c];
     g[c] = s;
+}
+
+cudaError_t column_sums(const float *d, long long rows, int cols, float *g, float *part, cudaStream_t s) {
+    int splits = (int)((rows + 255) / 256);
+    if (splits > kColsumSplits) splits = kColsumSplits;
+    if (splits < 1) splits = 1;
+    colsum_part_kernel<<<dim3((cols + 31) / 32, splits), dim3(32, 8), 0, s>>>(d, rows, cols, part);
+    colsum_final_kernel<<<(cols + 127) / 128, 128, 0, s>>>(part, splits, cols, g);
+    return cudaGetLastError();
 }
 
 // Masked weighted MSE on the first nused outputs plus, where cls is set and
@@ -772,7 +816,7 @@ cudaError_t backward(qcs_learned_net *net, int rows, cudaStream_t s) {
     if ((e = L::gemm(L::kHidden, L::kOut, rows, net->d_a2, 1, L::kHidden, net->d_dy, L::kOut, 1, g.W3, L::kOut, 0.0f,
                      s, net->d_ws, net->ws_floats, net->d_err)))
         return e;
-    L::colsum_kernel<<<1, L::kOut, 0, s>>>(net->d_dy, rows, L::kOut, g.b3);
+    if ((e = L::column_sums(net->d_dy, rows, L::kOut, g.b3, net->d_ws, s))) return e;
     if ((e = L::gemm(rows, L::kHidden, L::kOut, net->d_dy, L::kOut, 1, w.W3, 1, L::kOut, net->d_d2, L::kHidden, 0.0f,
                      s, net->d_ws, net->ws_floats, net->d_err)))
         return e;
@@ -782,7 +826,7 @@ cudaError_t backward(qcs_learned_net *net, int rows, cudaStream_t s) {
     if ((e = L::gemm(L::kHidden, L::kHidden, rows, net->d_a1, 1, L::kHidden, net->d_d2, L::kHidden, 1, g.W2,
                      L::kHidden, 0.0f, s, net->d_ws, net->ws_floats, net->d_err)))
         return e;
-    L::colsum_kernel<<<1, L::kHidden, 0, s>>>(net->d_d2, rows, L::kHidden, g.b2);
+    if ((e = L::column_sums(net->d_d2, rows, L::kHidden, g.b2, net->d_ws, s))) return e;
     if ((e = L::gemm(rows, L::kHidden, L::kHidden, net->d_d2, L::kHidden, 1, w.W2, 1, L::kHidden, net->d_d1,
                      L::kHidden, 0.0f, s, net->d_ws, net->ws_floats, net->d_err)))
         return e;
@@ -792,7 +836,7 @@ cudaError_t backward(qcs_learned_net *net, int rows, cudaStream_t s) {
     if ((e = L::gemm(net->kin, L::kHidden, rows, net->d_x, 1, net->kin, net->d_d1, L::kHidden, 1, g.W1, L::kHidden,
                      0.0f, s, net->d_ws, net->ws_floats, net->d_err)))
         return e;
-    L::colsum_kernel<<<1, L::kHidden, 0, s>>>(net->d_d1, rows, L::kHidden, g.b1);
+    if ((e = L::column_sums(net->d_d1, rows, L::kHidden, g.b1, net->d_ws, s))) return e;
     return cudaGetLastError();
 }
 

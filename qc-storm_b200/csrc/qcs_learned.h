@@ -102,6 +102,12 @@ __device__ __forceinline__ void start_from_outputs(const float *y, float lo, flo
 cudaError_t gemm(int M, int N, int K, const float *A, long long sam, long long sak, const float *B, long long sbk,
                  long long sbn, float *C, int ldc, float beta, cudaStream_t s, float *ws, size_t ws_floats, int *err);
 
+// g[c] = sum over rows r of d[r * cols + c], FP32, in a fixed order (two
+// passes: up to kColsumSplits row splits into part, then their sum); part
+// holds kColsumSplits * cols floats.
+constexpr int kColsumSplits = 128;
+cudaError_t column_sums(const float *d, long long rows, int cols, float *g, float *part, cudaStream_t s);
+
 // Start points (start_width floats per record) of n device records into out;
 // with cls set (GS2D networks), also each record's emitter-count class at the
 // network's count threshold.  With n_dev set the fused kernel reads the
