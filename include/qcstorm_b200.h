@@ -522,6 +522,11 @@ int qcs_learned_param_count(void);
  * multi-emitter cascade's 2E stage): 8 outputs, dx, dy of emitter 0 and of
  * emitter 1, log(peak / range) of each, sigma - 1.3, (background - min) / range. */
 #define QCS_LEARNED_GS2D_2E 16
+/* Network kind for the start points of the GS2D three-emitter fit (the
+ * cascade's 3E stage): 16 outputs, of which 11 are used: dx, dy of emitters 0,
+ * 1, 2, log(peak / range) of each, sigma - 1.3, (background - min) / range;
+ * W3 128x16, b3 16.  MLP networks only. */
+#define QCS_LEARNED_GS2D_3E 17
 int qcs_learned_create_for(int loc_type, int roi_size, int batch, unsigned long long seed, qcs_learned_net **out);
 /* Network architectures: the MLP above, and a convolutional network
  * (3x3 conv, 32 channels, zero 'same' padding, ReLU -> 3x3 conv, 64 channels,
@@ -559,7 +564,7 @@ int qcs_learned_features_device(const qcs_loc_para *p, const uint16_t *d_rois, i
  * plain-fit rows of the same records. */
 int qcs_learned_targets_device(const qcs_loc_para *p, const uint16_t *d_rois, const float *d_rows,
                                const float *d_scale, int n, float *d_targets, float *d_valid, void *stream);
-/* Network outputs (n x 8) of n feature rows. */
+/* Network outputs (n x 8; n x 16 for QCS_LEARNED_GS2D_3E networks) of n feature rows. */
 int qcs_learned_forward_device(qcs_learned_net *net, const float *d_feat, int n, float *d_out, void *stream);
 /* Loss and parameter gradient of one batch (n <= batch); gradients via qcs_learned_get_grads. */
 int qcs_learned_gradient_device(qcs_learned_net *net, const float *d_feat, const float *d_targets,
@@ -603,6 +608,35 @@ float qcs_learned_count_threshold(const qcs_learned_net *net);
  * three-emitter fit, as the reference's rejected two-emitter fits do
  * (fallback QCS_TWO_FALLBACK_3E), or are fitted again by the reference's
  * two-emitter fit (QCS_TWO_FALLBACK_PLAIN: one more pass of that fit). */
+/* Attaches a QCS_LEARNED_GS2D_3E network `three` of the same ROI size to the
+ * GS2D network `net` (NULL detaches): learned multi-emitter calls with `net`
+ * then start the three-emitter stage's fits from its start points, with
+ * `iters` BFGS iterations of `bisections` line-search steps (4 or 6 of 6, or
+ * 16 of 11; bisections <= 0: 6), and refit plainly every fit that keeps no
+ * emitter or whose unweighted Poisson deviance exceeds dev_th (0: 2 R^2 + 2).
+ * `three` stays owned by the caller and must outlive the attachment
+ * (qcs_learned_destroy refuses it while attached).  The context allocates
+ * 97 bytes per record of capacity for the three-emitter stage on the first
+ * such call, which must not be inside a stream capture. */
+int qcs_learned_set_three_emitter(qcs_learned_net *net, qcs_learned_net *three, int iters, int bisections,
+                                  float dev_th);
+/* Three-emitter fits of the last learned call redone by the plain three-emitter fit. */
+int qcs_learned_refit_3e_num(qcs_loc_data *ctx, int *n);
+/* Training data of a QCS_LEARNED_GS2D_3E network.  With capture on, each
+ * plain multi-emitter call of the context also keeps the final fitted
+ * parameters of its three-emitter fits (11 floats per 3E-queue slot, fit
+ * units; qcs_loc_device_three_emitter_params); the rows are unchanged.  Turning
+ * it on allocates the context's three-emitter buffers (97 bytes per record of
+ * capacity). */
+int qcs_loc_set_three_emitter_capture(qcs_loc_data *ctx, int on);
+const float *qcs_loc_device_three_emitter_params(const qcs_loc_data *ctx);
+/* Targets (n x 11: dx, dy of emitters 0..2, log(peak / range) of each,
+ * sigma - 1.3, (background - min) / range; emitters ordered by peak x (R -
+ * distance from the ROI centre)) and validity (n) of the records whose plain
+ * three-emitter fit in the last capturing call kept an emitter; d_scale from
+ * qcs_learned_features_device. */
+int qcs_loc_three_emitter_targets_device(qcs_loc_data *ctx, const uint16_t *d_rois, const qcs_loc_para *p, int n,
+                                         const float *d_scale, float *d_targets, float *d_valid, void *stream);
 /* Multi-emitter learned calls: a learned single-emitter fit that is rejected
  * or judged poor by the deviance bound and has SNR > 6 goes straight to the
  * two-emitter fit (the reference's rule for its rejected single fits, applied

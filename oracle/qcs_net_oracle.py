@@ -20,7 +20,9 @@ SIGMA0 = 1.3
 N_IN, N_HID, N_OUT, N_USED = 64, 128, 8, 5   # the GS2D 7x7 network
 TARGET_WEIGHT = np.array([4.0, 4.0, 1.0, 1.0, 1.0, 1.0])  # GS2D uses the first 5, AS3D all 6
 TARGET_WEIGHT_2E = np.array([4.0, 4.0, 4.0, 4.0, 1.0, 1.0, 1.0, 1.0])  # the two-emitter start points
+TARGET_WEIGHT_3E = np.array([4.0, 4.0, 4.0, 4.0, 4.0, 4.0, 1.0, 1.0, 1.0, 1.0, 1.0])  # the three-emitter ones
 LEARNED_2E = 16  # network kind of the two-emitter start points (QCS_LEARNED_GS2D_2E)
+LEARNED_3E = 17  # network kind of the three-emitter start points (QCS_LEARNED_GS2D_3E; 16 outputs)
 
 
 def in_width(r):
@@ -29,7 +31,27 @@ def in_width(r):
 
 
 def used_outputs(loc_type):
-    return 8 if loc_type == LEARNED_2E else (6 if loc_type == 1 else 5)
+    return 11 if loc_type == LEARNED_3E else (8 if loc_type == LEARNED_2E else (6 if loc_type == 1 else 5))
+
+
+def out_width(loc_type):
+    return 16 if loc_type == LEARNED_3E else N_OUT
+
+
+def start_points_3e(y, lo, rng, r):
+    """Three-emitter start points (peak, x, y of emitters 0..2, sigma,
+    background) from outputs y [n, 16] and the ROI scales, as the kernels map
+    them (positions held a pixel inside the ROI's edge)."""
+    y = np.asarray(y, np.float64)
+    c, w2 = r / 2.0, r / 2.0 - 1.0
+    st = np.zeros((y.shape[0], 11))
+    for e in range(3):
+        st[:, 3 * e] = rng * np.exp(np.clip(y[:, 6 + e], -6, 3))
+        st[:, 3 * e + 1] = c + np.clip(y[:, 2 * e], -w2, w2)
+        st[:, 3 * e + 2] = c + np.clip(y[:, 2 * e + 1], -w2, w2)
+    st[:, 9] = np.clip(SIGMA0 + y[:, 9], 0.6, 3.0)
+    st[:, 10] = np.maximum(lo + rng * y[:, 10], 1.0)
+    return st
 
 
 def start_points_2e(y, lo, rng, r):
@@ -50,8 +72,9 @@ def start_points_2e(y, lo, rng, r):
     return st
 
 
-def param_count(n_in):
-    return n_in * N_HID + N_HID + N_HID * N_HID + N_HID + N_HID * N_OUT + N_OUT
+def param_count(n_in, n_out=None):
+    n_out = N_OUT if n_out is None else n_out
+    return n_in * N_HID + N_HID + N_HID * N_HID + N_HID + N_HID * n_out + n_out
 COUNT0, CLASSES, COUNT_WEIGHT = 5, 3, 0.5  # outputs 5..7: emitter-count logits
 N_PARAMS = N_IN * N_HID + N_HID + N_HID * N_HID + N_HID + N_HID * N_OUT + N_OUT
 
@@ -64,12 +87,13 @@ def bf16(a):
     return rounded.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
-def split_params(p):
+def split_params(p, n_out=None):
+    n_out = N_OUT if n_out is None else n_out
     p = np.asarray(p, np.float64)
-    n_in = (p.size - param_count(0)) // N_HID
+    n_in = (p.size - param_count(0, n_out)) // N_HID
     o = 0
     out = []
-    for shape in ((n_in, N_HID), (N_HID,), (N_HID, N_HID), (N_HID,), (N_HID, N_OUT), (N_OUT,)):
+    for shape in ((n_in, N_HID), (N_HID,), (N_HID, N_HID), (N_HID,), (N_HID, n_out), (n_out,)):
         size = int(np.prod(shape))
         out.append(p[o:o + size].reshape(shape))
         o += size
@@ -108,8 +132,8 @@ def targets(rois, rows, scale, qe, r=R, loc_type=0):
     return t, ok.astype(np.float32)
 
 
-def forward(params, x):
-    W1, b1, W2, b2, W3, b3 = split_params(params)
+def forward(params, x, n_out=None):
+    W1, b1, W2, b2, W3, b3 = split_params(params, n_out)
     z1 = bf16(x) @ bf16(W1) + b1
     a1 = np.maximum(z1, 0)
     z2 = bf16(a1) @ bf16(W2) + b2
@@ -128,16 +152,16 @@ def count_class(logits, th):
     return np.where(e[:, 2] >= th * s, 2, np.where(e[:, 1] + e[:, 2] >= th * s, 1, 0)).astype(np.uint8)
 
 
-def loss_and_grad(params, x, t, valid, classes=None):
+def loss_and_grad(params, x, t, valid, classes=None, n_out=None):
     """Mean over the batch of sum_j w_j (y_j - t_j)^2 * valid plus, for rows
     with a class label c >= 0, COUNT_WEIGHT * (-log softmax(logits)[c]); and
     its gradient."""
-    W1, b1, W2, b2, W3, b3 = split_params(params)
-    y, (x, z1, a1, z2, a2) = forward(params, x)
+    W1, b1, W2, b2, W3, b3 = split_params(params, n_out)
+    y, (x, z1, a1, z2, a2) = forward(params, x, n_out)
     n = x.shape[0]
     nu = t.shape[1]
     e = y[:, :nu] - t
-    tw = TARGET_WEIGHT_2E if nu == 8 else TARGET_WEIGHT[:nu]
+    tw = TARGET_WEIGHT_3E if nu == 11 else (TARGET_WEIGHT_2E if nu == 8 else TARGET_WEIGHT[:nu])
     loss = float(np.sum(tw * e * e * valid[:, None]) / n)
     dy = np.zeros_like(y)
     dy[:, :nu] = 2.0 * tw * e * valid[:, None] / n

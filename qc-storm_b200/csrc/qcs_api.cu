@@ -72,6 +72,13 @@ struct qcs_loc_data {
     int *d_slots2 = nullptr;        //   slots and record ids of the two-emitter refits
     int *d_ids2 = nullptr;
     const qcs::TwoEmitterStart *two = nullptr;  // set for the duration of a learned call with a two-emitter net
+    // three-emitter block (allocated on first use): start points (capacity x 11), refit flags, refit slots and
+    // ids, and the captured parameters of the plain three-emitter fits (capacity x 11)
+    float *d_start3 = nullptr, *d_params3 = nullptr;
+    uint8_t *d_refit3 = nullptr;
+    int *d_slots3 = nullptr, *d_ids3 = nullptr;
+    int capture3 = 0;  // qcs_loc_set_three_emitter_capture
+    const qcs::ThreeEmitterStart *three = nullptr;  // set for the duration of a learned call with a 3E net
     // autotuned lanes per ROI of the single-emitter fit by batch size: batches of
     // at most tune_n[k] records use tune_lanes[k] (first match); none: 1
     int tune_count = 0;
@@ -149,6 +156,7 @@ int qcs_loc_deinit(qcs_loc_data *c) {
     qcs::wle_sorter_destroy(c->wle_sorter);
     cudaFree(c->d_start);
     cudaFree(c->d_start2);
+    cudaFree(c->d_start3);
     cudaFree(c->d_lr);
     if (c->ev_done) cudaEventDestroy(c->ev_done);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -269,7 +277,31 @@ static qcs::LrScratch lr_scratch(const qcs_loc_data *c) {
 static cudaError_t run_localization(qcs_loc_data *c, const qcs::CascadeArgs &a) {
     c->lr_stats = use_lr(c, &a.para) ? 1 : 0;
     if (c->lr_stats) return qcs::run_cascade_lr(a, c->st, lr_scratch(c));
+    if (c->capture3 && c->d_params3) {
+        qcs::CascadeArgs b = a;
+        b.params3 = c->d_params3;
+        return qcs::run_cascade(b, c->st);
+    }
     return qcs::run_cascade(a, c->st);
+}
+
+// The context's three-emitter block, allocated on first use (outside any
+// stream capture: an allocation cannot be captured).
+static int ensure_three(qcs_loc_data *c) {
+    if (c->d_start3) return QCS_OK;
+    auto round256 = [](size_t b) { return (b + 255) / 256 * 256; };
+    const size_t cap = (size_t)c->capacity;
+    const size_t b_par = round256(cap * 11 * sizeof(float)), b_int = round256(cap * sizeof(int));
+    char *b = nullptr;
+    const cudaError_t e = cudaMalloc((void **)&b, 2 * b_par + round256(cap) + 2 * b_int);
+    if (e != cudaSuccess)
+        return fail(e == cudaErrorMemoryAllocation ? QCS_ERR_NOMEM : QCS_ERR_CUDA, "three-emitter buffers", e);
+    c->d_start3 = reinterpret_cast<float *>(b);
+    c->d_params3 = reinterpret_cast<float *>(b + b_par);
+    c->d_refit3 = reinterpret_cast<uint8_t *>(b + 2 * b_par);
+    c->d_slots3 = reinterpret_cast<int *>(b + 2 * b_par + round256(cap));
+    c->d_ids3 = reinterpret_cast<int *>(b + 2 * b_par + round256(cap) + b_int);
+    return QCS_OK;
 }
 
 static int tuned_lanes(const qcs_loc_data *c, int n) {
@@ -398,6 +430,49 @@ __global__ void two_targets_kernel(qcs::CascadeState st, const uint16_t *__restr
     valid[id] = 1.0f;
 }
 
+// Three-emitter targets (QCS_LEARNED_GS2D_3E network outputs) of the records
+// whose plain three-emitter fit kept an emitter, from the parameters that
+// fit captured (qcs_loc_set_three_emitter_capture): dx, dy of the three
+// emitters, log(peak / range) of each, sigma - 1.3, (background - min) /
+// range, the emitters ordered by peak x (R - distance from the centre), the
+// order of the fit's own emitter selection.  valid[id] = 1 for those records.
+template <int R>
+__global__ void three_targets_kernel(qcs::CascadeState st, const float *__restrict__ params,
+                                     const float *__restrict__ scale, int n, float *__restrict__ tgt,
+                                     float *__restrict__ valid) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= st.counters[qcs::kCnt3E]) return;
+    const int id = st.q3[k];
+    if (id < 0 || id >= n || st.res3[k] == 0) return;
+    const float *v = params + (size_t)k * 11;
+    const float centre = R / 2.0f, lo = scale[2 * id], rng = scale[2 * id + 1];
+    float key[3];
+    int order[3] = {0, 1, 2};
+    for (int e = 0; e < 3; ++e) {  // the fit's selection key (positions outside the ROI count as far away)
+        float x = v[3 * e + 1], y = v[3 * e + 2];
+        if (fabsf(x - centre) >= R / 2) x = -100.0f;
+        if (fabsf(y - centre) >= R / 2) y = -100.0f;
+        key[e] = v[3 * e] * (R - sqrtf((x - centre) * (x - centre) + (y - centre) * (y - centre)));
+    }
+    for (int a = 0; a < 2; ++a)  // three elements: sort by key, descending
+        for (int b = 0; b < 2 - a; ++b)
+            if (key[order[b]] < key[order[b + 1]]) {
+                const int t = order[b];
+                order[b] = order[b + 1];
+                order[b + 1] = t;
+            }
+    float *t = tgt + (size_t)id * 11;
+    for (int j = 0; j < 3; ++j) {
+        const int e = order[j];
+        t[2 * j] = v[3 * e + 1] - centre;
+        t[2 * j + 1] = v[3 * e + 2] - centre;
+        t[6 + j] = logf(fmaxf(v[3 * e] * QCS_ASCALE, 1e-3f) / rng);
+    }
+    t[9] = sqrtf(0.5f / (fmaxf(v[9], 1e-6f) * QCS_SSCALE)) - 1.3f;
+    t[10] = (v[10] * QCS_BSCALE - lo) / rng;
+    valid[id] = 1.0f;
+}
+
 // The learned multi-emitter call: the cascade's queues (with the predicted
 // classes when cls is set), the learned-start single-emitter fit over the
 // single queue, a plain refit of the fits it flags (which also flags the
@@ -421,6 +496,7 @@ cudaError_t learned_multi(qcs_loc_data *c, const uint16_t *d_rois, const float *
     a.stream = s;
     a.pred = cls;
     a.two = c->two;
+    a.three = c->three;
     a.group_limit2 = c->tune_limit2;
     a.group_limit3 = c->tune_limit3;
     cudaError_t e;
@@ -460,6 +536,33 @@ int two_emitter_starts(qcs_loc_data *c, const qcs_learned_net *net, const qcs_lo
     *two = qcs::TwoEmitterStart{c->d_start2, iters, bisections, dev_th > 0.0f ? dev_th : default_dev_th(p->ROISize),
                                 to3e, c->d_refit2, c->d_slots2, c->d_ids2};
     c->two = two;
+    return QCS_OK;
+}
+
+// When the GS2D network has a three-emitter network attached: its start
+// points of the call's records (all n, as for the two-emitter network) and the
+// context's three-emitter stage set to use them (cleared by the caller).
+int three_emitter_starts(qcs_loc_data *c, const qcs_learned_net *net, const qcs_loc_para *p, const uint16_t *d_rois,
+                         int n, const int *n_dev, cudaStream_t s, qcs::ThreeEmitterStart *three) {
+    c->three = nullptr;
+    int iters = 0, bisections = 0;
+    float dev_th = 0.0f;
+    qcs_learned_net *net3 = qcs::learned::three_emitter(net, &iters, &bisections, &dev_th);
+    if (!net3 || p->LocType != QCS_LOCTYPE_GS2D || !p->MultiEmitterFitEn || n <= 0) return QCS_OK;
+    if (!c->d_start3) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        QCS_CUDA(cudaStreamIsCapturing(s, &cs), "capture status");
+        if (cs != cudaStreamCaptureStatusNone)
+            return fail(QCS_ERR_STATE, "three-emitter start points: make one call outside a stream capture first");
+        const int st = ensure_three(c);
+        if (st) return st;
+    }
+    QCS_CUDA(qcs::learned::start_points(net3, p, d_rois, n, c->d_start3, s, nullptr, n_dev),
+             "three-emitter start points");
+    *three = qcs::ThreeEmitterStart{c->d_start3, iters, bisections,
+                                    dev_th > 0.0f ? dev_th : default_dev_th(p->ROISize), c->d_refit3, c->d_slots3,
+                                    c->d_ids3};
+    c->three = three;
     return QCS_OK;
 }
 
@@ -569,10 +672,16 @@ int qcs_learned_localize_device(qcs_loc_data *c, qcs_learned_net *net, const uin
     uint8_t *cls = (p->MultiEmitterFitEn && qcs_learned_count_threshold(net) > 0.0f) ? c->d_cls : nullptr;
     QCS_CUDA(qcs::learned::start_points(net, p, d_rois, n, c->d_start, s, cls), "learned start points");
     qcs::TwoEmitterStart two;
+    qcs::ThreeEmitterStart three;
     if (p->MultiEmitterFitEn && (st = two_emitter_starts(c, net, p, d_rois, n, nullptr, s, &two)) != QCS_OK) return st;
+    if (p->MultiEmitterFitEn && (st = three_emitter_starts(c, net, p, d_rois, n, nullptr, s, &three)) != QCS_OK) {
+        c->two = nullptr;
+        return st;
+    }
     st = fit_from_start(c, d_rois, d_wle, p, n, c->d_start, cls, iters, bisections, dev_th, s,
                         qcs::learned::direct_two_emitter(net));
     c->two = nullptr;
+    c->three = nullptr;
     return st;
 }
 
@@ -598,11 +707,17 @@ int qcs_learned_localize_device_n(qcs_loc_data *c, qcs_learned_net *net, const u
     if (max_n == 0) return QCS_OK;
     QCS_CUDA(qcs::learned::start_points(net, p, d_rois, max_n, c->d_start, s, cls, d_n), "learned start points");
     qcs::TwoEmitterStart two;
+    qcs::ThreeEmitterStart three;
     if ((st = two_emitter_starts(c, net, p, d_rois, max_n, d_n, s, &two)) != QCS_OK) return st;
+    if ((st = three_emitter_starts(c, net, p, d_rois, max_n, d_n, s, &three)) != QCS_OK) {
+        c->two = nullptr;
+        return st;
+    }
     const cudaError_t e =
         learned_multi(c, d_rois, d_wle, p, max_n, d_n, c->d_start, cls, iters, bisections, dev_th, s,
                       qcs::learned::direct_two_emitter(net));
     c->two = nullptr;
+    c->three = nullptr;
     QCS_CUDA(e, "learned multi-emitter localization");
     return QCS_OK;
 }
@@ -633,6 +748,51 @@ int qcs_learned_refit_2e_num(qcs_loc_data *c, int *n) {
     QCS_CUDA(cudaMemcpy(c->h_counters, c->st.counters, qcs::kCntNum * sizeof(int), cudaMemcpyDeviceToHost),
              "read counters");
     *n = c->h_counters[qcs::kCntRefit2E];
+    return QCS_OK;
+}
+
+int qcs_learned_refit_3e_num(qcs_loc_data *c, int *n) {
+    if (!c || !n) return fail(QCS_ERR_ARG, "null argument");
+    QCS_CUDA(cudaDeviceSynchronize(), "localization");
+    QCS_CUDA(cudaMemcpy(c->h_counters, c->st.counters, qcs::kCntNum * sizeof(int), cudaMemcpyDeviceToHost),
+             "read counters");
+    *n = c->h_counters[qcs::kCntRefit3E];
+    return QCS_OK;
+}
+
+int qcs_loc_set_three_emitter_capture(qcs_loc_data *c, int on) {
+    if (!c) return fail(QCS_ERR_ARG, "null context");
+    if (on) {
+        const int st = ensure_three(c);
+        if (st) return st;
+    }
+    c->capture3 = on ? 1 : 0;
+    return QCS_OK;
+}
+
+const float *qcs_loc_device_three_emitter_params(const qcs_loc_data *c) { return c ? c->d_params3 : nullptr; }
+
+int qcs_loc_three_emitter_targets_device(qcs_loc_data *c, const uint16_t *d_rois, const qcs_loc_para *p, int n,
+                                         const float *d_scale, float *d_targets, float *d_valid, void *stream) {
+    if (!c || !p || !d_rois || !d_scale || !d_targets || !d_valid) return fail(QCS_ERR_ARG, "null argument");
+    if (n < 0 || n > c->capacity) return fail(QCS_ERR_CAPACITY, "record count outside the context capacity");
+    if (p->LocType != QCS_LOCTYPE_GS2D || !p->MultiEmitterFitEn || p->ROISize != c->R ||
+        !(c->R == 7 || c->R == 9 || c->R == 11))
+        return fail(QCS_ERR_ARG, "three-emitter targets: GS2D 7/9/11 with multi-emitter fitting");
+    if (!c->capture3 || !c->d_params3)
+        return fail(QCS_ERR_STATE, "three-emitter targets: set qcs_loc_set_three_emitter_capture before the plain call");
+    if (n == 0) return QCS_OK;
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
+    QCS_CUDA(cudaMemsetAsync(d_targets, 0, (size_t)n * 11 * sizeof(float), s), "clear targets");
+    QCS_CUDA(cudaMemsetAsync(d_valid, 0, (size_t)n * sizeof(float), s), "clear valid");
+    const int grid = (n + 255) / 256;
+    if (c->R == 7)
+        three_targets_kernel<7><<<grid, 256, 0, s>>>(c->st, c->d_params3, d_scale, n, d_targets, d_valid);
+    else if (c->R == 9)
+        three_targets_kernel<9><<<grid, 256, 0, s>>>(c->st, c->d_params3, d_scale, n, d_targets, d_valid);
+    else
+        three_targets_kernel<11><<<grid, 256, 0, s>>>(c->st, c->d_params3, d_scale, n, d_targets, d_valid);
+    QCS_CUDA(cudaGetLastError(), "three-emitter targets");
     return QCS_OK;
 }
 

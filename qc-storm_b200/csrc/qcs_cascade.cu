@@ -151,6 +151,7 @@ struct ClassifyStage {
         st.counters[kCnt3E] = t[2];
         st.counters[kCnt3EClassify] = t[2];
         st.counters[kCntRejected] = 0;
+        st.counters[kCntRefit3E] = 0;
         st.counters[kCntRows] = cnt;
     }
 };
@@ -223,6 +224,7 @@ __global__ void init_counters_kernel(CascadeState st, int n, const int *__restri
     st.counters[kCnt3EClassify] = 0;
     st.counters[kCntRejected] = 0;
     st.counters[kCntRows] = n;
+    st.counters[kCntRefit3E] = 0;
 }
 
 // Likelihood-ratio selection of each record's model (run_cascade_lr); the
@@ -361,9 +363,28 @@ cudaError_t cascade_tail(const CascadeArgs &a, const CascadeState &st) {
                 return e;
             if (p.LocType == QCS_LOCTYPE_GS2D) {
                 f.q = Queue{st.q3, st.counters + kCnt3E, 0};
-                f.mo = MultiOut{st.res3, st.extra3};
+                f.mo = MultiOut{st.res3, st.extra3, a.params3};
                 f.group_limit = a.group_limit3;
-                if ((e = launch_fit(k3E, R, f)) != cudaSuccess) return e;
+                if (a.three) {
+                    // learned starts; the plain refits write into the 2E stage's arrays (consumed by its
+                    // compaction above) and are merged back into their slots
+                    const ThreeEmitterStart &t = *a.three;
+                    if ((e = launch_fit_learned_3e(R, t.iters, t.bisections, f, t.start, t.dev_th, t.refit)) !=
+                        cudaSuccess)
+                        return e;
+                    if ((e = launch_flag_slots(t.refit, st.counters + kCnt3E, n, st.q3, t.slots, t.ids,
+                                               st.counters + kCntRefit3E, a.stream)) != cudaSuccess)
+                        return e;
+                    FitLaunch g = f;
+                    g.q = Queue{t.ids, st.counters + kCntRefit3E, 0};
+                    g.mo = MultiOut{st.res2, st.extra2};
+                    if ((e = launch_fit(k3E, R, g)) != cudaSuccess) return e;
+                    if ((e = launch_merge_refit(t.slots, st.counters + kCntRefit3E, n, st.res2, st.extra2, st.res3,
+                                                st.extra3, a.stream)) != cudaSuccess)
+                        return e;
+                } else if ((e = launch_fit(k3E, R, f)) != cudaSuccess) {
+                    return e;
+                }
                 if ((e = launch_compaction(CompactStage{st, a.loc, 3, 0, a.max_rows}, n, st, a.stream)) != cudaSuccess)
                     return e;
             }

@@ -23,6 +23,7 @@ enum {
     kCntSel1 = 10,       // likelihood-ratio selection: records that keep the one-emitter model
     kCntSel2 = 11,       //   ... the two-emitter model
     kCntSel3 = 12,       //   ... the three-emitter model
+    kCntRefit3E = 13,    // learned path: three-emitter fits redone by the plain three-emitter fit
     kCntNum = 16
 };
 
@@ -59,6 +60,17 @@ struct TwoEmitterStart {
     int *slots, *ids;
 };
 
+// Learned starts of the GS2D three-emitter stage: start points (11 per
+// record), schedule, deviance bound; per 3E-queue slot refit flags, and the
+// slots and record ids of the plain refits.
+struct ThreeEmitterStart {
+    const float *start;
+    int iters, bisections;
+    float dev_th;
+    uint8_t *refit;
+    int *slots, *ids;
+};
+
 struct CascadeArgs {
     qcs_loc_para para;
     const uint16_t *rois;  // device, n records
@@ -71,6 +83,8 @@ struct CascadeArgs {
     const uint8_t *pred = nullptr;  // learned emitter-count class per record, or null (the reference's split)
     int lanes = 1;  // lanes per ROI of the single-emitter fit: 1 (one thread per ROI) or 4 / 8 / 16 (group kernel)
     const TwoEmitterStart *two = nullptr;  // learned two-emitter starts (GS2D), or null (the reference's)
+    const ThreeEmitterStart *three = nullptr;  // learned three-emitter starts (GS2D), or null (the reference's)
+    float *params3 = nullptr;  // when set: the plain three-emitter fits' parameters, 11 per 3E-queue slot
     int group_limit2 = 0, group_limit3 = 0;  // tuned lane-group queue limits of the 2E / 3E stages (0: default)
 };
 

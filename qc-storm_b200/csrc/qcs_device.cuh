@@ -54,6 +54,10 @@ __device__ __forceinline__ int queue_at(const Queue &q, int i) { return q.ids ? 
 struct MultiOut {
     int8_t *result;
     float *extra;  // 12 floats per queue slot
+    // three-emitter kind only, when set: each slot's final fitted parameters
+    // (11 floats, fit units: peak / 128, x, y per emitter, 1/(2 sigma^2) / 0.1,
+    // background / 64), written before the emitter selection
+    float *params = nullptr;
 };
 
 }  // namespace qcs

@@ -889,6 +889,10 @@ __global__ void __launch_bounds__(kTPB) fit_multi_kernel(const uint16_t *__restr
     if (KIND == k2E) wle_weights<R, MASK>(w, kTPB, WLE_SigmaX, WLE_SigmaX, QCS_MOLECULE_MULTIFIT);
     mle_fit<R, KIND, DIST, SUM2>(roi, Ininf, D, kTPB);
     if (ll) ll[CurFluoID] = model_loglik<R, KIND, DIST, SUM2>(s_img + tid, kTPB, Ininf, 0, 1);
+    if (KIND == k3E && mo.params) {
+#pragma unroll
+        for (int k = 0; k < P; k++) mo.params[(size_t)slot * P + k] = Ininf[k];
+    }
 
     multi_finish<R, KIND>(Ininf, c, XOffset, YOffset, CurFrame, NearNeighborDistance, loc, CurFluoID, mo, slot);
 }
@@ -982,6 +986,10 @@ __global__ void __launch_bounds__(kGroupTPB, 4) fit_multi_group_kernel(const uin
         for (int o = G / 2; o > 0; o >>= 1) s += __shfl_xor_sync(mask, s, o, G);
         if (lane == 0) ll[CurFluoID] = s;
     }
+    if (KIND == k3E && mo.params && lane == 0) {
+#pragma unroll
+        for (int k = 0; k < P; k++) mo.params[(size_t)slot * P + k] = Ininf[k];
+    }
     if (lane == 0)
         multi_finish<R, KIND>(Ininf, c, XOffset, YOffset, CurFrame, NearNeighborDistance, loc, CurFluoID, mo, slot);
 }
@@ -1073,6 +1081,76 @@ __global__ void __launch_bounds__(kTPB) fit_learned_2e_kernel(const uint16_t *__
     }
 }
 
+// ------------------------------------ learned-start three-emitter fits ---
+// The GS2D three-emitter fit of fit_multi_kernel<R, k3E> over the records of
+// its queue, started from a given point (start[11 id ..]: peak e-, x, y in
+// ROI pixels of emitters 0, 1, 2, the shared sigma, background e-) instead of
+// the reference's pre-estimate (bfgsMLE_GS2D_3Emitter_core.h:593-710), with
+// ITERS BFGS iterations of NB line-search steps and the analytic gradient
+// (AnalyticEval3E); the same loss, selection of the two kept emitters, accept
+// rules and output (multi_finish). A fit is judged poor when no emitter is
+// kept or when its unweighted Poisson deviance exceeds dev_th: refit[slot] = 1
+// marks it for the plain three-emitter fit.
+template <int R, int ITERS, int NB, int DIST = ArithSpec<k3E, R>::DIST>
+__global__ void __launch_bounds__(kTPB) fit_learned_3e_kernel(const uint16_t *__restrict__ rois,
+                                                              const float *__restrict__ start, Queue q,
+                                                              float *__restrict__ loc, MultiOut mo,
+                                                              uint8_t *__restrict__ refit, CorePara c, float dev_th) {
+    typedef SmemLayout<R, k3E> L;
+    enum { P = 11, PIX = R * R, WHOLE = R * (R + 1) };
+    extern __shared__ float smem[];
+    const int n = queue_len(q);
+    const int base = blockIdx.x * kTPB;
+    if (base >= n) return;
+    const int cnt = min(kTPB, n - base);
+    float2 *s_img = reinterpret_cast<float2 *>(smem + L::IMG);
+    stage_rois<R>(s_img, rois, q, base, cnt, c.Offset, c.KAdc);
+    __syncthreads();
+    const int tid = threadIdx.x;
+    if (tid >= cnt) return;
+    const int slot = base + tid;
+    const int id = queue_at(q, slot);
+    float *D = smem + L::D + tid;
+    const uint16_t *hdr = rois + (size_t)id * WHOLE + PIX;
+    const int XOffset = hdr[0], YOffset = hdr[1];
+    const int CurFrame = hdr[2] + 65536 * hdr[3];
+    const RoiRef roi{s_img + tid, nullptr, kTPB};  // the three-emitter loss is unweighted
+    const float *st = start + (size_t)id * P;
+    float Ininf[P];
+#pragma unroll
+    for (int e = 0; e < 3; e++) {
+        Ininf[3 * e] = st[3 * e] * rAScalFactor;
+        Ininf[3 * e + 1] = st[3 * e + 1];
+        Ininf[3 * e + 2] = st[3 * e + 2];
+    }
+    Ininf[9] = (0.5f / (st[9] * st[9])) * rSScalFactor;
+    Ininf[10] = st[10] * rBScalFactor;
+    bfgs_fit<P, ITERS, AnalyticEval3E<R, DIST>, NB>(AnalyticEval3E<R, DIST>{roi}, Ininf, D, kTPB);
+    // goodness of fit at the final point (unweighted Poisson deviance of the three-emitter model)
+    float dev = 0.0f;
+    {
+        float v[P];
+#pragma unroll
+        for (int k = 0; k < P; k++) v[k] = Ininf[k] < 0.0f ? 0.0f : Ininf[k];
+        const float A0 = v[0] * QCS_ASCALE, A1 = v[3] * QCS_ASCALE, A2 = v[6] * QCS_ASCALE;
+        const float S = v[9] * QCS_SSCALE, B64 = v[10] * QCS_BSCALE;
+#pragma unroll 1
+        for (int r = 0; r < R; r++)
+            for (int col = 0; col < R; col++) {
+                const float2 pl = roi.img[(r * R + col) * roi.ld];
+                const float dx0 = col + 0.5f - v[1], dy0 = r + 0.5f - v[2];
+                const float dx1 = col + 0.5f - v[4], dy1 = r + 0.5f - v[5];
+                const float dx2 = col + 0.5f - v[7], dy2 = r + 0.5f - v[8];
+                const float mu = A0 * __expf(-(dx0 * dx0 + dy0 * dy0) * S) + A1 * __expf(-(dx1 * dx1 + dy1 * dy1) * S) +
+                                 A2 * __expf(-(dx2 * dx2 + dy2 * dy2) * S) + B64;
+                dev += mu - pl.x - pl.x * (__logf(mu) - pl.y);
+            }
+        dev *= 2.0f;
+    }
+    multi_finish<R, k3E>(Ininf, c, XOffset, YOffset, CurFrame, 1000.0f, loc, id, mo, slot);
+    refit[slot] = (mo.result[slot] == 0 || !(dev <= dev_th)) ? 1 : 0;
+}
+
 // slots[] / ids[]: the queue slots i < *n_dev with flags[i] != 0 and their
 // record ids q[i] (any order); *count = their number (zero on entry).
 __global__ void flag_slots_kernel(const uint8_t *__restrict__ flags, const int *__restrict__ n_dev, int max_n,
@@ -1116,6 +1194,18 @@ cudaError_t launch_learned_2e(const FitLaunch &a, const float *start, float dev_
     const int grid = (a.max_count + kTPB - 1) / kTPB;
     if (grid == 0) return cudaSuccess;
     k<<<grid, kTPB, smem, a.stream>>>(a.rois, a.wle, start, a.q, a.loc, a.mo, refit, a.para, dev_th, to3e);
+    return cudaGetLastError();
+}
+
+template <int R, int IT, int NB>
+cudaError_t launch_learned_3e(const FitLaunch &a, const float *start, float dev_th, uint8_t *refit) {
+    const size_t smem = SmemLayout<R, k3E>::TOTAL * sizeof(float);
+    auto k = fit_learned_3e_kernel<R, IT, NB>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const int grid = (a.max_count + kTPB - 1) / kTPB;
+    if (grid == 0) return cudaSuccess;
+    k<<<grid, kTPB, smem, a.stream>>>(a.rois, start, a.q, a.loc, a.mo, refit, a.para, dev_th);
     return cudaGetLastError();
 }
 
@@ -1291,6 +1381,27 @@ cudaError_t launch_fit_learned_2e(int R, int iters, int bisections, const FitLau
     QCS_L2E(9)
     QCS_L2E(11)
 #undef QCS_L2E
+    return cudaErrorInvalidValue;
+}
+
+bool learned_3e_supported(int R, int iters, int bisections) {
+    return (R == 7 || R == 9 || R == 11) &&
+           ((bisections == 6 && (iters == 4 || iters == 6)) || (bisections == kBisections && iters == 16));
+}
+
+cudaError_t launch_fit_learned_3e(int R, int iters, int bisections, const FitLaunch &a, const float *start,
+                                  float dev_th, uint8_t *refit) {
+    if (!learned_3e_supported(R, iters, bisections)) return cudaErrorInvalidValue;
+#define QCS_L3E(RR)                                                                          \
+    if (R == RR) {                                                                         \
+        if (iters == 4 && bisections == 6) return launch_learned_3e<RR, 4, 6>(a, start, dev_th, refit); \
+        if (iters == 6 && bisections == 6) return launch_learned_3e<RR, 6, 6>(a, start, dev_th, refit); \
+        return launch_learned_3e<RR, 16, kBisections>(a, start, dev_th, refit);                        \
+    }
+    QCS_L3E(7)
+    QCS_L3E(9)
+    QCS_L3E(11)
+#undef QCS_L3E
     return cudaErrorInvalidValue;
 }
 

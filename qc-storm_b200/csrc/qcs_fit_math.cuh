@@ -492,6 +492,63 @@ struct AnalyticEval2E {
         g[7] = QCS_BSCALE * gB;
     }
 };
+// Loss of the GS2D three-emitter fit (the plain kernel's, unweighted) with
+// the analytic gradient of that Poisson deviance: d/d mu = 1 - n / mu per
+// pixel, chained through the three Gaussians sharing 1/(2 sigma^2) and the
+// background (the learned-start three-emitter fit; no central differences).
+template <int R, int DIST>
+struct AnalyticEval3E {
+    RoiRef roi;
+    __device__ __forceinline__ float loss(float *x) const {
+        return qcs::loss<R, k3E, DIST, ArithSpec<k3E, R>::SUM2>(roi, x);
+    }
+    __device__ __forceinline__ void gradient(const float *v, float *g) const {
+        float c[11];
+#pragma unroll
+        for (int k = 0; k < 11; k++) c[k] = v[k] < 0.0f ? 0.0f : v[k];
+        const float A0 = c[0] * QCS_ASCALE, A1 = c[3] * QCS_ASCALE, A2 = c[6] * QCS_ASCALE;
+        const float S = c[9] * QCS_SSCALE, B64 = c[10] * QCS_BSCALE;
+        float gA0 = 0, gX0 = 0, gY0 = 0, gA1 = 0, gX1 = 0, gY1 = 0, gA2 = 0, gX2 = 0, gY2 = 0, gS = 0, gB = 0;
+#pragma unroll 1
+        for (int row = 0; row < R; row++) {
+            const float dy0 = (row + 0.5f) - c[2], dy1 = (row + 0.5f) - c[5], dy2 = (row + 0.5f) - c[8];
+#pragma unroll(R <= kUnrollMaxR ? R : 1)
+            for (int col = 0; col < R; col++) {
+                const float2 pl = roi.img[(row * R + col) * roi.ld];
+                const float dx0 = (col + 0.5f) - c[1], dx1 = (col + 0.5f) - c[4], dx2 = (col + 0.5f) - c[7];
+                const float r0 = __fmaf_rn(dx0, dx0, dy0 * dy0), r1 = __fmaf_rn(dx1, dx1, dy1 * dy1);
+                const float r2 = __fmaf_rn(dx2, dx2, dy2 * dy2);
+                const float e0 = __expf(-r0 * S), e1 = __expf(-r1 * S), e2 = __expf(-r2 * S);
+                const float mu = __fmaf_rn(A0, e0, __fmaf_rn(A1, e1, __fmaf_rn(A2, e2, B64)));
+                const float q = 1.0f - __fdividef(pl.x, mu);
+                const float q0 = q * e0, q1 = q * e1, q2 = q * e2;
+                gA0 += q0;
+                gX0 = __fmaf_rn(q0, dx0, gX0);
+                gY0 = __fmaf_rn(q0, dy0, gY0);
+                gA1 += q1;
+                gX1 = __fmaf_rn(q1, dx1, gX1);
+                gY1 = __fmaf_rn(q1, dy1, gY1);
+                gA2 += q2;
+                gX2 = __fmaf_rn(q2, dx2, gX2);
+                gY2 = __fmaf_rn(q2, dy2, gY2);
+                gS = __fmaf_rn(A0 * q0, r0, __fmaf_rn(A1 * q1, r1, __fmaf_rn(A2 * q2, r2, gS)));
+                gB += q;
+            }
+        }
+        g[0] = QCS_ASCALE * gA0;
+        g[1] = A0 * 2.0f * S * gX0;
+        g[2] = A0 * 2.0f * S * gY0;
+        g[3] = QCS_ASCALE * gA1;
+        g[4] = A1 * 2.0f * S * gX1;
+        g[5] = A1 * 2.0f * S * gY1;
+        g[6] = QCS_ASCALE * gA2;
+        g[7] = A2 * 2.0f * S * gX2;
+        g[8] = A2 * 2.0f * S * gY2;
+        g[9] = -QCS_SSCALE * gS;
+        g[10] = QCS_BSCALE * gB;
+    }
+};
+
 // Loss and gradient of one single-emitter ROI (GS2D / AS3D) evaluated by a
 // group of G consecutive lanes of a warp, bit for bit equal to ThreadEval:
 //  - loss: the lanes compute the pixel terms k = lane, lane + G, ... (the

@@ -69,6 +69,14 @@ cudaError_t launch_fit_learned(int kind, int R, int iters, int bisections, const
 bool learned_2e_supported(int R, int iters, int bisections);
 cudaError_t launch_fit_learned_2e(int R, int iters, int bisections, const FitLaunch &a, const float *start,
                                   float dev_th, uint8_t *refit, int to3e);
+// Learned-start GS2D three-emitter fit (R = 7, 9, 11) of the records of a.q
+// (grid from a.max_count) from start[11 id ..] (peak e-, x, y of emitters 0,
+// 1, 2, sigma, background e-) with `iters` iterations of `bisections` steps
+// (learned_3e_supported): rows and stage results as launch_fit(k3E); poor fits
+// get refit[slot] = 1 (to redo with the plain kernel).
+bool learned_3e_supported(int R, int iters, int bisections);
+cudaError_t launch_fit_learned_3e(int R, int iters, int bisections, const FitLaunch &a, const float *start,
+                                  float dev_th, uint8_t *refit);
 // slots[] / ids[]: the queue slots i < min(*n_dev, max_n) with flags[i] != 0
 // and q[i]; *count = their number.
 cudaError_t launch_flag_slots(const uint8_t *flags, const int *n_dev, int max_n, const int *q, int *slots, int *ids,

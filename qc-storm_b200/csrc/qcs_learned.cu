@@ -364,23 +364,22 @@ cudaError_t column_sums(const float *d, long long rows, int cols, float *g, floa
 // cls[i] >= 0 (GS2D networks), kCountWeight x the softmax cross-entropy of
 // the count logits against class cls[i]: loss and dY.
 __global__ void mse_kernel(const float *__restrict__ Y, const float *__restrict__ T, const float *__restrict__ valid,
-                           const float *__restrict__ cls, int rows, int nused, int wrow, float inv_count,
+                           const float *__restrict__ cls, int rows, int nout, int nused, int wrow, float inv_count,
                            float *__restrict__ dY,
                            float *__restrict__ loss) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= rows) return;
     const float v = valid[i];
-    const float *y = Y + (size_t)i * kOut;
+    const float *y = Y + (size_t)i * nout;
     float l = 0.0f;
-#pragma unroll
-    for (int j = 0; j < kOut; ++j) {
+    for (int j = 0; j < nout; ++j) {
         float d = 0.0f;
         if (j < nused) {
             const float e = y[j] - T[(size_t)i * nused + j];
             d = 2.0f * kTargetWeight[wrow][j] * e * v * inv_count;
             l += kTargetWeight[wrow][j] * e * e * v;
         }
-        dY[(size_t)i * kOut + j] = d;
+        dY[(size_t)i * nout + j] = d;
     }
     const int label = cls ? (int)cls[i] : -1;
     if (label >= 0 && label < kClasses) {
@@ -391,7 +390,7 @@ __global__ void mse_kernel(const float *__restrict__ Y, const float *__restrict_
         l += kCountWeight * (logf(sum) - (y[kCount0 + label] - m));
 #pragma unroll
         for (int j = 0; j < kClasses; ++j)
-            dY[(size_t)i * kOut + kCount0 + j] = kCountWeight * (e[j] / sum - (j == label ? 1.0f : 0.0f)) * inv_count;
+            dY[(size_t)i * nout + kCount0 + j] = kCountWeight * (e[j] / sum - (j == label ? 1.0f : 0.0f)) * inv_count;
     }
     atomicAdd(loss, l * inv_count);
 }
@@ -423,7 +422,7 @@ __global__ void start_kernel(const float *__restrict__ Y, const float *__restric
                              float *__restrict__ start, uint8_t *__restrict__ cls, float th) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const float *y = Y + (size_t)i * kOut;
+    const float *y = Y + (size_t)i * out_width(LT);
     if (cls) cls[i] = (uint8_t)count_class(y[kCount0], y[kCount0 + 1], y[kCount0 + 2], th);
     start_from_outputs<R, LT>(y, scale[2 * i], scale[2 * i + 1], start + (size_t)i * start_width(LT));
 }
@@ -670,7 +669,7 @@ __global__ void __launch_bounds__(128, 1) mlp_tc_kernel(const uint16_t *__restri
         tmem_ld16(tmem + row_lane, y);
         if (tid < rows) {
 #pragma unroll
-            for (int j = 0; j < kOut; ++j) y[j] += __ldg(b3 + j);
+            for (int j = 0; j < out_width(LT); ++j) y[j] += __ldg(b3 + j);
             start_from_outputs<R, LT>(y, lo, rng, start + (size_t)i * NST);
             if (LT == QCS_LOCTYPE_GS2D && cls)
                 cls[i] = (uint8_t)count_class(y[kCount0], y[kCount0 + 1], y[kCount0 + 2], count_th);
@@ -705,7 +704,7 @@ __global__ void __launch_bounds__(128, 1) mlp_tc_kernel(const uint16_t *__restri
 }
 
 // FP32 master weights -> BF16 operand images (W1 | W2 | W3, N x K K-major).
-template <int KIN>
+template <int KIN, int NOUT>
 __global__ void weight_image_kernel(const float *__restrict__ par, __nv_bfloat16 *__restrict__ img) {
     constexpr int W1 = kHidden * KIN, W2 = kHidden * kHidden, W3 = kN3 * kHidden;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -718,7 +717,7 @@ __global__ void weight_image_kernel(const float *__restrict__ par, __nv_bfloat16
         img[W1 + img_index(nn, k, kHidden)] = __float2bfloat16_rn(pW2[j]);
     } else if (i < W1 + W2 + W3) {
         const int j = i - W1 - W2, k = j / kN3, nn = j % kN3;
-        img[W1 + W2 + img_index(nn, k, kN3)] = __float2bfloat16_rn(nn < kOut ? pW3[k * kOut + nn] : 0.0f);
+        img[W1 + W2 + img_index(nn, k, kN3)] = __float2bfloat16_rn(nn < NOUT ? pW3[k * NOUT + nn] : 0.0f);
     }
 }
 
@@ -738,7 +737,12 @@ struct qcs_learned_net {
     int direct_2e = 0;  // multi-emitter calls: poor bright single fits straight to the 2E stage
     int two_iters = 3, two_bisections = 6, two_to3e = 1;
     float two_dev_th = 0.0f;
+    // GS2D networks: the three-emitter network whose start points the 3E stage uses, and its schedule
+    qcs_learned_net *three = nullptr;
+    int three_iters = 4, three_bisections = 6;
+    float three_dev_th = 0.0f;
     int kin = 64;                     // input width: in_width(R)
+    int nout = 8;                     // outputs per record: out_width(loc_type)
     int params = 0;                   // param_count(kin)
     // parameters (FP32 master copies), their gradients and Adam moments, in one block
     float *d_par = nullptr, *d_grad = nullptr, *d_m = nullptr, *d_v = nullptr;
@@ -768,14 +772,14 @@ namespace {
 struct Views {
     float *W1, *b1, *W2, *b2, *W3, *b3;
 };
-Views views(float *p, int kin) {
+Views views(float *p, int kin, int nout = L::kOut) {
     Views v;
     v.W1 = p;
     v.b1 = v.W1 + kin * L::kHidden;
     v.W2 = v.b1 + L::kHidden;
     v.b2 = v.W2 + L::kHidden * L::kHidden;
     v.W3 = v.b2 + L::kHidden;
-    v.b3 = v.W3 + L::kHidden * L::kOut;
+    v.b3 = v.W3 + L::kHidden * nout;
     return v;
 }
 
@@ -791,7 +795,7 @@ cudaError_t forward(qcs_learned_net *net, const float *x, int rows, float *z1, f
                     float *y, cudaStream_t s) {
     if (net->conv)
         return L::conv::forward(net->conv, net->d_par, x, rows, net->kin, y, s, net->d_ws, net->ws_floats, net->d_err);
-    const Views w = views(net->d_par, net->kin);
+    const Views w = views(net->d_par, net->kin, net->nout);
     cudaError_t e;
     if ((e = L::gemm(rows, L::kHidden, net->kin, x, net->kin, 1, w.W1, L::kHidden, 1, z1, L::kHidden, 0.0f, s, net->d_ws, net->ws_floats, net->d_err)))
         return e;
@@ -799,8 +803,11 @@ cudaError_t forward(qcs_learned_net *net, const float *x, int rows, float *z1, f
     if ((e = L::gemm(rows, L::kHidden, L::kHidden, a1, L::kHidden, 1, w.W2, L::kHidden, 1, z2, L::kHidden, 0.0f, s, net->d_ws, net->ws_floats, net->d_err)))
         return e;
     L::bias_relu_kernel<<<blocks((long long)rows * L::kHidden), 256, 0, s>>>(z2, w.b2, rows, L::kHidden, a2, 1);
-    if ((e = L::gemm(rows, L::kOut, L::kHidden, a2, L::kHidden, 1, w.W3, L::kOut, 1, y, L::kOut, 0.0f, s, net->d_ws, net->ws_floats, net->d_err))) return e;
-    L::bias_relu_kernel<<<blocks((long long)rows * L::kOut), 256, 0, s>>>(y, w.b3, rows, L::kOut, y, 0);
+    const int no = net->nout;
+    if ((e = L::gemm(rows, no, L::kHidden, a2, L::kHidden, 1, w.W3, no, 1, y, no, 0.0f, s, net->d_ws, net->ws_floats,
+                     net->d_err)))
+        return e;
+    L::bias_relu_kernel<<<blocks((long long)rows * no), 256, 0, s>>>(y, w.b3, rows, no, y, 0);
     return cudaGetLastError();
 }
 
@@ -809,15 +816,16 @@ cudaError_t backward(qcs_learned_net *net, int rows, cudaStream_t s) {
     if (net->conv)
         return L::conv::backward(net->conv, net->d_par, net->d_grad, net->d_x, rows, net->kin, net->d_dy, s, net->d_ws,
                                  net->ws_floats, net->d_err);
-    const Views w = views(net->d_par, net->kin);
-    const Views g = views(net->d_grad, net->kin);
+    const Views w = views(net->d_par, net->kin, net->nout);
+    const Views g = views(net->d_grad, net->kin, net->nout);
     cudaError_t e;
     // layer 3: dW3 = a2^T dy, db3 = colsum(dy), d2 = dy W3^T
-    if ((e = L::gemm(L::kHidden, L::kOut, rows, net->d_a2, 1, L::kHidden, net->d_dy, L::kOut, 1, g.W3, L::kOut, 0.0f,
+    const int no = net->nout;
+    if ((e = L::gemm(L::kHidden, no, rows, net->d_a2, 1, L::kHidden, net->d_dy, no, 1, g.W3, no, 0.0f,
                      s, net->d_ws, net->ws_floats, net->d_err)))
         return e;
-    if ((e = L::column_sums(net->d_dy, rows, L::kOut, g.b3, net->d_ws, s))) return e;
-    if ((e = L::gemm(rows, L::kHidden, L::kOut, net->d_dy, L::kOut, 1, w.W3, 1, L::kOut, net->d_d2, L::kHidden, 0.0f,
+    if ((e = L::column_sums(net->d_dy, rows, no, g.b3, net->d_ws, s))) return e;
+    if ((e = L::gemm(rows, L::kHidden, no, net->d_dy, no, 1, w.W3, 1, no, net->d_d2, L::kHidden, 0.0f,
                      s, net->d_ws, net->ws_floats, net->d_err)))
         return e;
     L::relu_back_kernel<<<blocks((long long)rows * L::kHidden), 256, 0, s>>>(net->d_d2, net->d_z2,
@@ -881,6 +889,12 @@ cudaError_t by_shape(int loc_type, int R, F &&f) {
         case 9: return f(Shape<9, L::kTwo>{});
         case 11: return f(Shape<11, L::kTwo>{});
         }
+    } else if (loc_type == L::kThree) {
+        switch (R) {
+        case 7: return f(Shape<7, L::kThree>{});
+        case 9: return f(Shape<9, L::kThree>{});
+        case 11: return f(Shape<11, L::kThree>{});
+        }
     }
     return cudaErrorInvalidValue;
 }
@@ -901,7 +915,7 @@ cudaError_t fused_start_points(qcs_learned_net *net, const qcs_loc_para *p, cons
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
     const bool bulk = (reinterpret_cast<uintptr_t>(d_rois) & 15) == 0;
-    const Views w = views(net->d_par, net->kin);
+    const Views w = views(net->d_par, net->kin, net->nout);
     const float th = class_threshold(net);
     return by_shape(net->loc_type, net->R, [&](auto sh) -> cudaError_t {
         constexpr int R = decltype(sh)::R, LT = decltype(sh)::LT;
@@ -922,7 +936,7 @@ cudaError_t fused_start_points(qcs_learned_net *net, const qcs_loc_para *p, cons
         if (e2 != cudaSuccess) return e2;
         const bool capturing = cs != cudaStreamCaptureStatusNone;
         if (net->wimg_version != net->version) {
-            L::tc::weight_image_kernel<Lay::KIN><<<blocks(Lay::W1 + Lay::W2 + Lay::W3), 256, 0, s>>>(net->d_par,
+            L::tc::weight_image_kernel<Lay::KIN, L::out_width(LT)><<<blocks(Lay::W1 + Lay::W2 + Lay::W3), 256, 0, s>>>(net->d_par,
                                                                                                   net->d_wimg);
             if (!capturing) {
                 e2 = cudaEventRecord(net->wimg_ready, s);
@@ -943,7 +957,7 @@ cudaError_t fused_start_points(qcs_learned_net *net, const qcs_loc_para *p, cons
 
 // net's shape against the call's parameters
 int check_shape(const qcs_learned_net *net, const qcs_loc_para *p) {
-    const int want = net->loc_type == L::kTwo ? QCS_LOCTYPE_GS2D : net->loc_type;
+    const int want = (net->loc_type == L::kTwo || net->loc_type == L::kThree) ? QCS_LOCTYPE_GS2D : net->loc_type;
     if (p->ROISize != net->R || p->LocType != want)
         return fail(QCS_ERR_ROISIZE, "the network was built for another localization type or ROI size");
     return QCS_OK;
@@ -954,6 +968,14 @@ int check_shape(const qcs_learned_net *net, const qcs_loc_para *p) {
 namespace qcs {
 namespace learned {
 bool direct_two_emitter(const qcs_learned_net *net) { return net && net->direct_2e; }
+
+qcs_learned_net *three_emitter(const qcs_learned_net *net, int *iters, int *bisections, float *dev_th) {
+    if (!net || !net->three) return nullptr;
+    *iters = net->three_iters;
+    *bisections = net->three_bisections;
+    *dev_th = net->three_dev_th;
+    return net->three;
+}
 
 qcs_learned_net *two_emitter(const qcs_learned_net *net, int *iters, int *bisections, float *dev_th, int *to3e) {
     if (!net || !net->two) return nullptr;
@@ -979,6 +1001,8 @@ int qcs_learned_destroy(qcs_learned_net *net) {
                                    "(qcs_learned_set_two_emitter(owner, NULL, ...)) or destroy the owner");
     if (net->two) net->two->owners--;
     net->two = nullptr;
+    if (net->three) net->three->owners--;
+    net->three = nullptr;
     cudaDeviceSynchronize();  // no call of this network still in flight
     cudaFree(net->d_par);
     cudaFree(net->d_x);
@@ -1005,6 +1029,8 @@ int qcs_learned_create_arch(int arch, int loc_type, int roi_size, int batch, uns
     *out = nullptr;
     if (arch != QCS_LEARNED_ARCH_MLP && arch != QCS_LEARNED_ARCH_CONV)
         return fail(QCS_ERR_ARG, "architecture: QCS_LEARNED_ARCH_MLP or QCS_LEARNED_ARCH_CONV");
+    if (arch == QCS_LEARNED_ARCH_CONV && loc_type == L::kThree)
+        return fail(QCS_ERR_ARG, "three-emitter start points: MLP networks only");
     if (!L::shape_supported(loc_type, roi_size))
         return fail(QCS_ERR_ROISIZE, "learned start points: GS2D or AS3D, ROISize 7, 9 or 11");
     if (batch <= 0) batch = 4096;
@@ -1016,13 +1042,14 @@ int qcs_learned_create_arch(int arch, int loc_type, int roi_size, int batch, uns
     net->R = roi_size;
     net->kin = L::in_width(roi_size);
     net->arch = arch;
-    net->params = arch == QCS_LEARNED_ARCH_CONV ? L::conv::param_count(roi_size) : L::param_count(net->kin);
+    net->nout = L::out_width(loc_type);
+    net->params = arch == QCS_LEARNED_ARCH_CONV ? L::conv::param_count(roi_size) : L::param_count(net->kin, net->nout);
     net->ws_floats = arch == QCS_LEARNED_ARCH_CONV ? 4 * kWsFloats : kWsFloats;
     net->batch = batch;
     const int kin = net->kin;
     const size_t P = net->params;
     const size_t B = (size_t)batch;
-    const size_t acts = B * (kin + 4 * L::kHidden + L::kOut + L::kUsedMax + 1 + L::kOut + 2 * L::kHidden) + 4;
+    const size_t acts = B * (kin + 4 * L::kHidden + L::kOutMax + L::kUsedMax + 1 + L::kOutMax + 2 * L::kHidden) + 4;
     const size_t wimg_bytes = (size_t)(L::kHidden * kin + L::kHidden * L::kHidden + L::tc::kN3 * L::kHidden) * 2;
     cudaError_t e = cudaMalloc((void **)&net->d_par, 4 * P * sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc((void **)&net->d_x, acts * sizeof(float));
@@ -1050,13 +1077,13 @@ int qcs_learned_create_arch(int arch, int loc_type, int roi_size, int batch, uns
     net->d_a2 = a;
     a += B * L::kHidden;
     net->d_y = a;
-    a += B * L::kOut;
+    a += B * L::kOutMax;
     net->d_t = a;
     a += B * L::kUsedMax;
     net->d_valid = a;
     a += B;
     net->d_dy = a;
-    a += B * L::kOut;
+    a += B * L::kOutMax;
     net->d_d2 = a;
     a += B * L::kHidden;
     net->d_d1 = a;
@@ -1074,13 +1101,13 @@ int qcs_learned_create_arch(int arch, int loc_type, int roi_size, int batch, uns
     if (net->conv) {
         L::conv::init_params(h, roi_size, seed);
     } else {
-        const Views hv = views(h, kin);
+        const Views hv = views(h, kin, net->nout);
         for (int i = 0; i < kin * L::kHidden; ++i) hv.W1[i] = uni() * sqrtf(6.0f / kin);
         for (int i = 0; i < L::kHidden; ++i) hv.b1[i] = 0.0f;
         for (int i = 0; i < L::kHidden * L::kHidden; ++i) hv.W2[i] = uni() * sqrtf(6.0f / L::kHidden);
         for (int i = 0; i < L::kHidden; ++i) hv.b2[i] = 0.0f;
-        for (int i = 0; i < L::kHidden * L::kOut; ++i) hv.W3[i] = uni() * sqrtf(3.0f / L::kHidden);
-        for (int i = 0; i < L::kOut; ++i) hv.b3[i] = 0.0f;
+        for (int i = 0; i < L::kHidden * net->nout; ++i) hv.W3[i] = uni() * sqrtf(3.0f / L::kHidden);
+        for (int i = 0; i < net->nout; ++i) hv.b3[i] = 0.0f;
     }
     e = cudaMemcpy(net->d_par, h, P * sizeof(float), cudaMemcpyHostToDevice);
     delete[] h;
@@ -1158,7 +1185,7 @@ int qcs_learned_forward_device(qcs_learned_net *net, const float *d_feat, int n,
     for (int r0 = 0; r0 < n; r0 += net->batch) {
         const int rows = (n - r0) < net->batch ? (n - r0) : net->batch;
         QCS_CUDA(forward(net, d_feat + (size_t)r0 * net->kin, rows, net->d_z1, net->d_a1, net->d_z2, net->d_a2,
-                         d_out + (size_t)r0 * L::kOut, s),
+                         d_out + (size_t)r0 * net->nout, s),
                  "forward");
     }
     return QCS_OK;
@@ -1180,8 +1207,8 @@ int qcs_learned_gradient_counts_device(qcs_learned_net *net, const float *d_feat
              "copy features");
     QCS_CUDA(forward(net, net->d_x, n, net->d_z1, net->d_a1, net->d_z2, net->d_a2, net->d_y, s), "forward");
     QCS_CUDA(cudaMemsetAsync(net->d_loss, 0, sizeof(float), s), "clear loss");
-    L::mse_kernel<<<blocks(n), 256, 0, s>>>(net->d_y, d_targets, d_valid, d_classes, n, L::used_outputs(net->loc_type),
-                                            net->loc_type == L::kTwo ? 1 : 0,
+    L::mse_kernel<<<blocks(n), 256, 0, s>>>(net->d_y, d_targets, d_valid, d_classes, n, net->nout,
+                                            L::used_outputs(net->loc_type), L::weight_row(net->loc_type),
                                             1.0f / (float)n, net->d_dy, net->d_loss);
     QCS_CUDA(backward(net, n, s), "backward");
     if (h_loss) {
@@ -1236,7 +1263,8 @@ int qcs_learned_train_counts_device(qcs_learned_net *net, const float *d_feat, c
             e = forward(net, net->d_x, B, net->d_z1, net->d_a1, net->d_z2, net->d_a2, net->d_y, s);
             if (e != cudaSuccess) break;
             // per-batch mean loss and its gradient; the loss accumulates over the epoch
-            L::mse_kernel<<<blocks(B), 256, 0, s>>>(net->d_y, d_tb, d_vb, d_cb, B, nu, net->loc_type == L::kTwo ? 1 : 0,
+            L::mse_kernel<<<blocks(B), 256, 0, s>>>(net->d_y, d_tb, d_vb, d_cb, B, net->nout, nu,
+                                                    L::weight_row(net->loc_type),
                                                     1.0f / (float)B, net->d_dy,
                                                     net->d_loss);
             e = backward(net, B, s);
@@ -1340,6 +1368,32 @@ int qcs_learned_set_two_emitter(qcs_learned_net *net, qcs_learned_net *two, int 
     return QCS_OK;
 }
 
+int qcs_learned_set_three_emitter(qcs_learned_net *net, qcs_learned_net *three, int iters, int bisections,
+                                  float dev_th) {
+    if (!net) return fail(QCS_ERR_ARG, "null network");
+    if (!three) {
+        if (net->three) net->three->owners--;
+        net->three = nullptr;
+        return QCS_OK;
+    }
+    if (net->loc_type != QCS_LOCTYPE_GS2D || three->loc_type != L::kThree || three->R != net->R)
+        return fail(QCS_ERR_ARG,
+                    "three-emitter start points: a QCS_LEARNED_GS2D_3E network of the GS2D network's ROI size");
+    if (bisections <= 0) bisections = 6;
+    if (!qcs::learned_3e_supported(net->R, iters, bisections))
+        return fail(QCS_ERR_ARG, "three-emitter schedules: 4 or 6 iterations of 6 line-search steps, or 16 of 11");
+    if (!(dev_th >= 0.0f)) return fail(QCS_ERR_ARG, "negative deviance bound");
+    if (net->three != three) {
+        if (net->three) net->three->owners--;
+        three->owners++;
+    }
+    net->three = three;
+    net->three_iters = iters;
+    net->three_bisections = bisections;
+    net->three_dev_th = dev_th;
+    return QCS_OK;
+}
+
 int qcs_learned_set_direct_two_emitter(qcs_learned_net *net, int on) {
     if (!net) return fail(QCS_ERR_ARG, "null network");
     if (on && net->loc_type != QCS_LOCTYPE_GS2D) return fail(QCS_ERR_ARG, "direct two-emitter routing: GS2D networks");
@@ -1348,7 +1402,7 @@ int qcs_learned_set_direct_two_emitter(qcs_learned_net *net, int on) {
 }
 
 size_t qcs_learned_work_bytes(int n) {
-    return (size_t)(n > 0 ? n : 0) * (L::in_width(11) + 2 + L::kOut) * sizeof(float);
+    return (size_t)(n > 0 ? n : 0) * (L::in_width(11) + 2 + L::kOutMax) * sizeof(float);
 }
 
 int qcs_learned_set_inference(qcs_learned_net *net, int fused) {
@@ -1375,7 +1429,7 @@ cudaError_t qcs::learned::start_points(qcs_learned_net *net, const qcs_loc_para 
                                        float *out, cudaStream_t s, uint8_t *cls, const int *n_dev) {
     if (net->use_tc) return fused_start_points(net, p, d_rois, n, n_dev, out, cls, s);
     const int kin = net->kin;
-    const size_t need = (size_t)n * (kin + 2 + 2 * L::kHidden + L::kOut);
+    const size_t need = (size_t)n * (kin + 2 + 2 * L::kHidden + L::kOutMax);
     if (need > net->start_cap) {
         cudaFree(net->d_start);
         net->d_start = nullptr;
@@ -1394,7 +1448,7 @@ cudaError_t qcs::learned::start_points(qcs_learned_net *net, const qcs_loc_para 
         if (net->conv) {  // the conv net's activations hold one batch
             for (int r0 = 0; r0 < n && e == cudaSuccess; r0 += net->batch)
                 e = forward(net, feat + (size_t)r0 * kin, n - r0 < net->batch ? n - r0 : net->batch, nullptr, nullptr,
-                            nullptr, nullptr, y + (size_t)r0 * L::kOut, s);
+                            nullptr, nullptr, y + (size_t)r0 * net->nout, s);
         } else {
             e = forward(net, feat, n, h1, h1, h2, h2, y, s);
         }

@@ -12,8 +12,10 @@ namespace learned {
 constexpr float kSigma0 = 1.3f;         // sigma offset of the sigma outputs
 constexpr int kHidden = 128;
 constexpr int kOut = 8;                 // start-point outputs, then (GS2D) three emitter-count logits
-constexpr int kUsedMax = 8;             // start-point outputs of the widest kind (two-emitter GS2D)
-constexpr int kTwo = QCS_LEARNED_GS2D_2E;  // network kind of the two-emitter start points
+constexpr int kOutMax = 16;             // outputs of the widest kind (three-emitter GS2D: 11 used)
+constexpr int kUsedMax = 11;            // start-point outputs of the widest kind (three-emitter GS2D)
+constexpr int kTwo = QCS_LEARNED_GS2D_2E;    // network kind of the two-emitter start points
+constexpr int kThree = QCS_LEARNED_GS2D_3E;  // network kind of the three-emitter start points
 constexpr int kCount0 = 5;              // GS2D: logits of the emitter-count classes 0, 1, 2 (outputs 5..7)
 constexpr int kClasses = 3;             // one emitter / two-emitter stage / three-emitter stage
 
@@ -24,30 +26,36 @@ __host__ __device__ constexpr int in_width(int R) { return R * R + 2 <= 64 ? 64 
 // Outputs fitted to the targets: GS2D dx, dy, sigma - 1.3, log(peak / range),
 // (background - min) / range; AS3D the same with sigma_x and then sigma_y - 1.3;
 // two-emitter GS2D dx0, dy0, dx1, dy1, log(peak0 / range), log(peak1 / range),
-// sigma - 1.3, (background - min) / range.
+// sigma - 1.3, (background - min) / range; three-emitter GS2D dx0, dy0, dx1,
+// dy1, dx2, dy2, log(peak0..2 / range), sigma - 1.3, (background - min) / range.
 __host__ __device__ constexpr int used_outputs(int loc_type) {
-    return loc_type == kTwo ? 8 : (loc_type == QCS_LOCTYPE_AS3D ? 6 : 5);
+    return loc_type == kThree ? 11 : (loc_type == kTwo ? 8 : (loc_type == QCS_LOCTYPE_AS3D ? 6 : 5));
 }
+// Network outputs per record: 8, or 16 for the three-emitter kind.
+__host__ __device__ constexpr int out_width(int loc_type) { return loc_type == kThree ? kOutMax : kOut; }
 // Start point per record: GS2D peak e-, x, y, sigma, background e-; AS3D
-// peak e-, x, y, sigma_x, sigma_y, background e-; two-emitter GS2D peak e-,
-// x, y of emitter 0, the same of emitter 1, sigma, background e- (each fit's
+// peak e-, x, y, sigma_x, sigma_y, background e-; two- and three-emitter
+// GS2D peak e-, x, y of each emitter, then sigma, background e- (each fit's
 // parameter order).
 __host__ __device__ constexpr int start_width(int loc_type) {
-    return loc_type == kTwo ? 8 : (loc_type == QCS_LOCTYPE_AS3D ? 6 : 5);
+    return loc_type == kThree ? 11 : (loc_type == kTwo ? 8 : (loc_type == QCS_LOCTYPE_AS3D ? 6 : 5));
 }
-constexpr int param_count(int kin) {
-    return kin * kHidden + kHidden + kHidden * kHidden + kHidden + kHidden * kOut + kOut;
+constexpr int param_count(int kin, int nout = kOut) {
+    return kin * kHidden + kHidden + kHidden * kHidden + kHidden + kHidden * nout + nout;
 }
 inline bool shape_supported(int loc_type, int R) {
-    return (loc_type == QCS_LOCTYPE_GS2D || loc_type == QCS_LOCTYPE_AS3D || loc_type == kTwo) &&
+    return (loc_type == QCS_LOCTYPE_GS2D || loc_type == QCS_LOCTYPE_AS3D || loc_type == kTwo || loc_type == kThree) &&
            (R == 7 || R == 9 || R == 11);
 }
 
 // loss weight of each start-point output (positions matter most) and of the
 // emitter-count cross-entropy
-// (row 0: single-emitter kinds, row 1: two-emitter GS2D)
-__constant__ const float kTargetWeight[2][kUsedMax] = {{4.0f, 4.0f, 1.0f, 1.0f, 1.0f, 1.0f, 0.0f, 0.0f},
-                                                       {4.0f, 4.0f, 4.0f, 4.0f, 1.0f, 1.0f, 1.0f, 1.0f}};
+// (row 0: single-emitter kinds, row 1: two-emitter GS2D, row 2: three-emitter GS2D)
+__constant__ const float kTargetWeight[3][kUsedMax] = {
+    {4.0f, 4.0f, 1.0f, 1.0f, 1.0f, 1.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f},
+    {4.0f, 4.0f, 4.0f, 4.0f, 1.0f, 1.0f, 1.0f, 1.0f, 0.0f, 0.0f, 0.0f},
+    {4.0f, 4.0f, 4.0f, 4.0f, 4.0f, 4.0f, 1.0f, 1.0f, 1.0f, 1.0f, 1.0f}};
+__host__ __device__ constexpr int weight_row(int loc_type) { return loc_type == kThree ? 2 : (loc_type == kTwo ? 1 : 0); }
 constexpr float kCountWeight = 0.5f;
 
 // Emitter-count class from the three logits: 2 when p(class 2) >= th, else 1
@@ -67,6 +75,19 @@ __host__ __device__ inline int count_class(float l0, float l1, float l2, float t
 template <int R, int LT>
 __device__ __forceinline__ void start_from_outputs(const float *y, float lo, float rng, float *st) {
     const float centre = R / 2.0f;
+    if (LT == kThree) {
+        // emitters anywhere up to a pixel inside the ROI's edge
+        const float w2 = R / 2.0f - 1.0f;
+#pragma unroll
+        for (int e = 0; e < 3; ++e) {
+            st[3 * e] = rng * expf(fminf(fmaxf(y[6 + e], -6.0f), 3.0f));
+            st[3 * e + 1] = centre + fminf(fmaxf(y[2 * e], -w2), w2);
+            st[3 * e + 2] = centre + fminf(fmaxf(y[2 * e + 1], -w2), w2);
+        }
+        st[9] = fminf(fmaxf(kSigma0 + y[9], 0.6f), 3.0f);
+        st[10] = fmaxf(lo + rng * y[10], 1.0f);
+        return;
+    }
     if (LT == kTwo) {
         // emitters anywhere up to a pixel inside the ROI's edge
         const float w2 = R / 2.0f - 1.0f;
@@ -137,6 +158,9 @@ cudaError_t start_points(State *st, const float *par, unsigned version, int loc_
 // The two-emitter network attached to a GS2D network (qcs_learned_set_two_emitter),
 // its schedule and fallback (to3e: poor fits go on to the three-emitter fit), or null.
 qcs_learned_net *two_emitter(const qcs_learned_net *net, int *iters, int *bisections, float *dev_th, int *to3e);
+// The three-emitter network attached to a GS2D network (qcs_learned_set_three_emitter)
+// and its schedule, or null.
+qcs_learned_net *three_emitter(const qcs_learned_net *net, int *iters, int *bisections, float *dev_th);
 // qcs_learned_set_direct_two_emitter's setting
 bool direct_two_emitter(const qcs_learned_net *net);
 }  // namespace learned

@@ -128,6 +128,12 @@ _SIGS = {
     "qcs_learned_set_two_emitter": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_int]),
     "qcs_learned_set_direct_two_emitter": (C.c_int, [C.c_void_p, C.c_int]),
     "qcs_learned_refit_2e_num": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "qcs_learned_set_three_emitter": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_float]),
+    "qcs_learned_refit_3e_num": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
+    "qcs_loc_set_three_emitter_capture": (C.c_int, [C.c_void_p, C.c_int]),
+    "qcs_loc_device_three_emitter_params": (C.c_void_p, [C.c_void_p]),
+    "qcs_loc_three_emitter_targets_device": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(LocPara), C.c_int,
+                                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "qcs_loc_two_emitter_targets_device": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(LocPara), C.c_int, C.c_void_p,
                                                      C.c_void_p, C.c_void_p, C.c_void_p]),
     "qcs_consec_init": (C.c_int, [C.c_int, C.POINTER(C.c_void_p)]),
@@ -535,8 +541,13 @@ def learned_in_width(roi_size):
 
 
 def learned_start_width(loc_type):
-    """Start-point floats per record: GS2D 5, AS3D 6, two-emitter GS2D 8."""
-    return 8 if loc_type == LEARNED_GS2D_2E else (6 if loc_type == 1 else 5)
+    """Start-point floats per record: GS2D 5, AS3D 6, two-emitter GS2D 8, three-emitter GS2D 11."""
+    return 11 if loc_type == LEARNED_GS2D_3E else (8 if loc_type == LEARNED_GS2D_2E else (6 if loc_type == 1 else 5))
+
+
+def learned_out_width(loc_type):
+    """Network outputs per record: 8, or 16 for the three-emitter kind."""
+    return 16 if loc_type == LEARNED_GS2D_3E else 8
 
 
 LEARNED_ARCH = {"mlp": 0, "conv": 1}  # QCS_LEARNED_ARCH_MLP, QCS_LEARNED_ARCH_CONV
@@ -565,6 +576,7 @@ class LearnedNet:
             check(self.lib.qcs_learned_destroy(self.h))
             self.h = None
             self._two = None
+            self._three = None
 
     def __del__(self):
         try:
@@ -609,7 +621,7 @@ class LearnedNet:
     def forward(self, feat, stream=0):
         import torch
         n = feat.shape[0]
-        out = torch.empty((n, 8), dtype=torch.float32, device="cuda")
+        out = torch.empty((n, learned_out_width(self.loc_type)), dtype=torch.float32, device="cuda")
         check(self.lib.qcs_learned_forward_device(self.h, C.c_void_p(feat.data_ptr()), int(n),
                                                   C.c_void_p(out.data_ptr()), C.c_void_p(stream) if stream else None))
         return out
@@ -654,6 +666,18 @@ class LearnedNet:
                                             C.byref(para), int(n), C.byref(it), C.byref(nb),
                                             C.c_void_p(stream) if stream else None))
         return it.value, nb.value
+
+    def set_three_emitter(self, three, iters=4, bisections=6, dev_th=0.0):
+        """Start the three-emitter fits of learned multi-emitter calls from the
+        LEARNED_GS2D_3E network `three` (None detaches); poor fits are refitted plainly."""
+        check(self.lib.qcs_learned_set_three_emitter(self.h, three.h if three is not None else None, int(iters),
+                                                     int(bisections), C.c_float(dev_th)))
+        self._three = three
+
+    def refits_3e(self, ctx):
+        k = C.c_int(0)
+        check(self.lib.qcs_learned_refit_3e_num(ctx.h, C.byref(k)))
+        return k.value
 
     def set_direct_two_emitter(self, on=True):
         """Multi-emitter calls: poor bright single fits straight to the two-emitter fit."""
@@ -728,6 +752,29 @@ def fit_from_start(ctx, d_rois, n, d_start, d_wle=0, iters=3, dev_th=0.0, para=N
 
 
 LEARNED_GS2D_2E = 16  # network kind of the two-emitter start points
+LEARNED_GS2D_3E = 17  # network kind of the three-emitter start points
+
+
+def set_three_emitter_capture(ctx, on=True):
+    """Keep the plain three-emitter fits' parameters of the following calls on ctx."""
+    check(load().qcs_loc_set_three_emitter_capture(ctx.h, 1 if on else 0))
+
+
+def three_emitter_params(ctx):
+    """Device pointer of the captured three-emitter parameters (11 floats per 3E-queue slot)."""
+    return load().qcs_loc_device_three_emitter_params(ctx.h)
+
+
+def three_emitter_targets(ctx, para, d_rois, scale, n, stream=0):
+    """Targets (n x 11) and valid flags of a LEARNED_GS2D_3E network from the
+    plain multi-emitter call just made, with capture on, on ctx over the same n records."""
+    import torch
+    t = torch.empty((n, 11), dtype=torch.float32, device="cuda")
+    v = torch.empty((n,), dtype=torch.float32, device="cuda")
+    check(load().qcs_loc_three_emitter_targets_device(ctx.h, C.c_void_p(d_rois), C.byref(para), int(n),
+                                                      C.c_void_p(scale.data_ptr()), C.c_void_p(t.data_ptr()),
+                                                      C.c_void_p(v.data_ptr()), C.c_void_p(stream) if stream else None))
+    return t, v
 
 
 def two_emitter_targets(ctx, para, d_rois, scale, n, stream=0):
