@@ -846,6 +846,22 @@ def train_two_emitter_net(ctx_tr, para, d_tr, feat, scale, n, R, epochs, stream)
     return net2
 
 
+def train_three_emitter_net(ctx_tr, para, d_tr, feat, scale, n, R, epochs, stream):
+    """A three-emitter start-point network trained on the parameters the
+    plain three-emitter fit converged to (captured in the plain call just made
+    on ctx_tr) for the records where it kept an emitter."""
+    from qcstorm_b200 import lib
+    t3, v3 = lib.three_emitter_targets(ctx_tr, para, d_tr.data_ptr(), scale, n, stream.cuda_stream)
+    stream.synchronize()
+    net3 = lib.LearnedNet(batch=4096, seed=7, loc_type=lib.LEARNED_GS2D_3E, roi_size=R)
+    net3.train(feat, t3, v3, epochs=epochs, lr=2e-3, stream=stream.cuda_stream)
+    stream.synchronize()
+    return net3
+
+
+THREE_ITERS = 4  # three-emitter fits from the network's start points: 4 x 6 (plain 16 x 11)
+
+
 def learned_shapes_measure(streams, dist, world, rank, mufu_peak=None, cpu_baseline=True):
     """The learned path on the other configurations' generators, each against
     plain fitting of the same device-resident records with two contexts in
@@ -865,6 +881,8 @@ def learned_shapes_measure(streams, dist, world, rank, mufu_peak=None, cpu_basel
         tr, para, _ = gen(SHAPE_TRAIN, R=R, seed=7000 + 10 * rank)
         d_tr = torch.from_numpy(tr.view(np.int16)).cuda()
         ctx_tr = lib.LocContext(para, capacity=SHAPE_TRAIN)
+        if kind == "multi":
+            lib.set_three_emitter_capture(ctx_tr)  # the three-emitter network's targets
         ctx_tr.localize_device(d_tr.data_ptr(), SHAPE_TRAIN, 0, sh)
         labels = lib.count_labels(ctx_tr, SHAPE_TRAIN, sh) if kind == "multi" else None
         feat, scale = lib.LearnedNet.features(para, d_tr.data_ptr(), SHAPE_TRAIN, stream=sh)
@@ -876,10 +894,11 @@ def learned_shapes_measure(streams, dist, world, rank, mufu_peak=None, cpu_basel
         torch.cuda.synchronize()
         net = lib.LearnedNet(batch=4096, seed=5, loc_type=para.LocType, roi_size=R)
         net.train(feat, tgt, valid, epochs=TRAIN_EPOCHS, lr=2e-3, stream=sh, classes=labels)
-        net2 = None
+        net2 = net3 = None
         if kind == "multi":
             net.set_count_threshold(0.5)
             net2 = train_two_emitter_net(ctx_tr, para, d_tr, feat, scale, SHAPE_TRAIN, R, TRAIN_EPOCHS, s0)
+            net3 = train_three_emitter_net(ctx_tr, para, d_tr, feat, scale, SHAPE_TRAIN, R, TRAIN_EPOCHS, s0)
         torch.cuda.synchronize()
         ctx_tr.close()
         del d_tr, feat, scale, tgt, valid, labels
@@ -961,6 +980,23 @@ def learned_shapes_measure(streams, dist, world, rank, mufu_peak=None, cpu_basel
             two["plain_refit"] = {"learned_fits_per_s": job_rate(SHAPE_STEPS, SHAPE_RECORDS, world, ms_l3),
                                   "two_emitter_refits_per_call": net.refits_2e(ctxs[0]),
                                   "accuracy": multi_truth_match(rows_l3, recs[0], truths[0], R)}
+            # and the three-emitter fits from their network's start points (QCS_LEARNED_GS2D_3E)
+            three = {"schedule": "three-emitter fits from the network's start points, %d x 6 (plain: 16 x 11); poor "
+                                 "ones refitted plainly" % THREE_ITERS}
+            for fb in ("3e", "plain"):
+                net.set_two_emitter(net2, iters=TWO_ITERS, bisections=6, fallback=fb)
+                net.set_three_emitter(net3, iters=THREE_ITERS, bisections=6)
+                ms_t = device_timed(SHAPE_STEPS, 3, learned, streams, dist)
+                learned(0, s0, ctxs[0])
+                rows_t, _ = ctxs[0].read_rows(sh)
+                three["two_emitter_fallback_" + fb] = {
+                    "learned_fits_per_s": job_rate(SHAPE_STEPS, SHAPE_RECORDS, world, ms_t), "vs_plain": ms_p / ms_t,
+                    "two_emitter_refits_per_call": net.refits_2e(ctxs[0]),
+                    "three_emitter_refits_per_call": net.refits_3e(ctxs[0]),
+                    "accuracy": multi_truth_match(rows_t, recs[0], truths[0], R)}
+            net.set_three_emitter(None)
+            net3.close()
+            two["with_three_emitter_starts"] = three
             net.set_two_emitter(None)
             net2.close()
             # poor bright single fits straight to the two-emitter fit (no plain refit first)

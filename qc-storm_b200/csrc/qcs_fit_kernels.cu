@@ -1095,11 +1095,13 @@ template <int R, int ITERS, int NB, int DIST = ArithSpec<k3E, R>::DIST>
 __global__ void __launch_bounds__(kTPB) fit_learned_3e_kernel(const uint16_t *__restrict__ rois,
                                                               const float *__restrict__ start, Queue q,
                                                               float *__restrict__ loc, MultiOut mo,
-                                                              uint8_t *__restrict__ refit, CorePara c, float dev_th) {
+                                                              uint8_t *__restrict__ refit, CorePara c, float dev_th,
+                                                              int min_n) {
     typedef SmemLayout<R, k3E> L;
     enum { P = 11, PIX = R * R, WHOLE = R * (R + 1) };
     extern __shared__ float smem[];
     const int n = queue_len(q);
+    if (n <= min_n) return;  // a queue this short is the one-warp-per-ROI kernel's
     const int base = blockIdx.x * kTPB;
     if (base >= n) return;
     const int cnt = min(kTPB, n - base);
@@ -1151,6 +1153,85 @@ __global__ void __launch_bounds__(kTPB) fit_learned_3e_kernel(const uint16_t *__
     refit[slot] = (mo.result[slot] == 0 || !(dev <= dev_th)) ? 1 : 0;
 }
 
+// The same fit with one warp per ROI (AnalyticWarpEval3E: the pixels spread
+// over the lanes, one shared inverse Hessian per ROI updated by lane 0,
+// bfgs_fit_shared) for queues of at most max_n records, where one ROI's
+// latency, not throughput, sets the stage's time.
+template <int R, int ITERS, int NB>
+__global__ void __launch_bounds__(kGroupTPB) fit_learned_3e_warp_kernel(const uint16_t *__restrict__ rois,
+                                                                       const float *__restrict__ start, Queue q,
+                                                                       float *__restrict__ loc, MultiOut mo,
+                                                                       uint8_t *__restrict__ refit, CorePara c,
+                                                                       float dev_th, int max_n) {
+    typedef MultiGroupLayout<R, k3E> L;
+    enum { P = 11, PIX = R * R, PIXP = L::PIXP, WHOLE = R * (R + 1), SLOTS = kGroupTPB / 32 };
+    static_assert(L::SLOTS == SLOTS, "one warp per slot");
+    extern __shared__ __align__(16) float smem[];
+    const int n = queue_len(q);
+    if (n > max_n) return;  // a longer queue is the one-thread-per-ROI kernel's
+    const int base = blockIdx.x * SLOTS;
+    if (base >= n) return;
+    const int cnt = min((int)SLOTS, n - base);
+    float2 *s_img = reinterpret_cast<float2 *>(smem + L::IMG);
+    for (int idx = threadIdx.x; idx < cnt * PIX; idx += kGroupTPB) {
+        const int sl = idx / PIX;
+        const int k = idx - sl * PIX;
+        const int id = queue_at(q, base + sl);
+        const uint16_t u = __ldg(rois + (size_t)id * WHOLE + k);
+        const float pixval = fmaxf((u - c.Offset) * c.KAdc, 1.0f);
+        s_img[sl * PIXP + k] = make_float2(pixval, __logf(pixval));
+    }
+    __syncthreads();
+    const int sl = threadIdx.x / 32, lane = threadIdx.x % 32;
+    if (sl >= cnt) return;
+    const unsigned mask = 0xffffffffu;
+    const int slot = base + sl;
+    const int id = queue_at(q, slot);
+    const float2 *img2 = s_img + sl * PIXP;
+    float *hess = smem + L::H + sl * L::HP;  // D (P x P), T (P x P), direction (P)
+    const uint16_t *hdr = rois + (size_t)id * WHOLE + PIX;
+    const int XOffset = hdr[0], YOffset = hdr[1];
+    const int CurFrame = hdr[2] + 65536 * hdr[3];
+    const float *st = start + (size_t)id * P;
+    float Ininf[P];
+#pragma unroll
+    for (int e = 0; e < 3; e++) {
+        Ininf[3 * e] = st[3 * e] * rAScalFactor;
+        Ininf[3 * e + 1] = st[3 * e + 1];
+        Ininf[3 * e + 2] = st[3 * e + 2];
+    }
+    Ininf[9] = (0.5f / (st[9] * st[9])) * rSScalFactor;
+    Ininf[10] = st[10] * rBScalFactor;
+    const AnalyticWarpEval3E<R> ev{img2, lane, mask};
+    bfgs_fit_shared<P, ITERS, AnalyticWarpEval3E<R>, kSkskFused, NB>(ev, Ininf, hess, hess + P * P, hess + 2 * P * P,
+                                                                     lane, mask);
+    // goodness of fit at the final point (unweighted Poisson deviance of the three-emitter model)
+    float dev;
+    {
+        float v[P];
+#pragma unroll
+        for (int k = 0; k < P; k++) v[k] = Ininf[k] < 0.0f ? 0.0f : Ininf[k];
+        const float A0 = v[0] * QCS_ASCALE, A1 = v[3] * QCS_ASCALE, A2 = v[6] * QCS_ASCALE;
+        const float S = v[9] * QCS_SSCALE, B64 = v[10] * QCS_BSCALE;
+        float part = 0.0f;
+        for (int k = lane; k < PIX; k += 32) {
+            const int r = k / R, col = k - r * R;
+            const float2 pl = img2[k];
+            const float dx0 = col + 0.5f - v[1], dy0 = r + 0.5f - v[2];
+            const float dx1 = col + 0.5f - v[4], dy1 = r + 0.5f - v[5];
+            const float dx2 = col + 0.5f - v[7], dy2 = r + 0.5f - v[8];
+            const float mu = A0 * __expf(-(dx0 * dx0 + dy0 * dy0) * S) + A1 * __expf(-(dx1 * dx1 + dy1 * dy1) * S) +
+                             A2 * __expf(-(dx2 * dx2 + dy2 * dy2) * S) + B64;
+            part += mu - pl.x - pl.x * (__logf(mu) - pl.y);
+        }
+        dev = 2.0f * ev.uniform_sum(part);
+    }
+    if (lane == 0) {
+        multi_finish<R, k3E>(Ininf, c, XOffset, YOffset, CurFrame, 1000.0f, loc, id, mo, slot);
+        refit[slot] = (mo.result[slot] == 0 || !(dev <= dev_th)) ? 1 : 0;
+    }
+}
+
 // slots[] / ids[]: the queue slots i < *n_dev with flags[i] != 0 and their
 // record ids q[i] (any order); *count = their number (zero on entry).
 __global__ void flag_slots_kernel(const uint8_t *__restrict__ flags, const int *__restrict__ n_dev, int max_n,
@@ -1197,15 +1278,32 @@ cudaError_t launch_learned_2e(const FitLaunch &a, const float *start, float dev_
     return cudaGetLastError();
 }
 
+// Learned-start three-emitter queues up to this length run one warp per ROI.
+constexpr int kLearned3EWarpLimit = 4096;
+
+// Both kernels are launched; each reads the stage's queue length on the
+// device and only one of them fits it.
 template <int R, int IT, int NB>
 cudaError_t launch_learned_3e(const FitLaunch &a, const float *start, float dev_th, uint8_t *refit) {
+    if (a.max_count <= 0) return cudaSuccess;
+    {
+        typedef MultiGroupLayout<R, k3E> L;
+        const size_t smem = L::TOTAL * sizeof(float);
+        auto k = fit_learned_3e_warp_kernel<R, IT, NB>;
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        const int m = a.max_count < kLearned3EWarpLimit ? a.max_count : kLearned3EWarpLimit;
+        k<<<(m + L::SLOTS - 1) / L::SLOTS, kGroupTPB, smem, a.stream>>>(a.rois, start, a.q, a.loc, a.mo, refit,
+                                                                        a.para, dev_th, kLearned3EWarpLimit);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+    if (a.max_count <= kLearned3EWarpLimit) return cudaSuccess;
     const size_t smem = SmemLayout<R, k3E>::TOTAL * sizeof(float);
     auto k = fit_learned_3e_kernel<R, IT, NB>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const int grid = (a.max_count + kTPB - 1) / kTPB;
-    if (grid == 0) return cudaSuccess;
-    k<<<grid, kTPB, smem, a.stream>>>(a.rois, start, a.q, a.loc, a.mo, refit, a.para, dev_th);
+    k<<<grid, kTPB, smem, a.stream>>>(a.rois, start, a.q, a.loc, a.mo, refit, a.para, dev_th, kLearned3EWarpLimit);
     return cudaGetLastError();
 }
 

@@ -704,6 +704,74 @@ __device__ __forceinline__ float multi_term(float colpos, float rowpos, const fl
     }
 }
 
+// The same loss and analytic gradient evaluated by one warp: lane l sums the
+// pixels l, l + 32, ...; each sum is reduced by a shuffle tree and lane 0's
+// total broadcast, so every lane holds the same value (the lanes' BFGS steps
+// stay identical).  img: the ROI's PIX (value, log) pairs, contiguous.
+template <int R>
+struct AnalyticWarpEval3E {
+    const float2 *img;
+    int lane;
+    unsigned mask;
+    __device__ __forceinline__ float uniform_sum(float v) const {
+#pragma unroll
+        for (int m = 16; m > 0; m >>= 1) v += __shfl_xor_sync(mask, v, m);
+        return __shfl_sync(mask, v, 0);
+    }
+    __device__ __forceinline__ float loss(float *x) const {
+#pragma unroll
+        for (int k = 0; k < 11; k++)
+            if (x[k] < 0.0f) x[k] = 0.0f;
+        float s = 0.0f;
+        for (int k = lane; k < R * R; k += 32) {
+            const int row = k / R, col = k - row * R;
+            const float2 pl = img[k];
+            s += multi_term<k3E, ArithSpec<k3E, R>::DIST, ArithSpec<k3E, R>::SUM2>(col + 0.5f, row + 0.5f, x, pl.x,
+                                                                                  pl.y);
+        }
+        return uniform_sum(s);
+    }
+    __device__ __forceinline__ void gradient(const float *v, float *g) const {
+        float c[11];
+#pragma unroll
+        for (int k = 0; k < 11; k++) c[k] = v[k] < 0.0f ? 0.0f : v[k];
+        const float A[3] = {c[0] * QCS_ASCALE, c[3] * QCS_ASCALE, c[6] * QCS_ASCALE};
+        const float S = c[9] * QCS_SSCALE, B64 = c[10] * QCS_BSCALE;
+        float gA[3] = {0, 0, 0}, gX[3] = {0, 0, 0}, gY[3] = {0, 0, 0}, gS = 0, gB = 0;
+        for (int k = lane; k < R * R; k += 32) {
+            const int row = k / R, col = k - row * R;
+            const float2 pl = img[k];
+            float dx[3], dy[3], r[3], e[3];
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                dx[j] = (col + 0.5f) - c[3 * j + 1];
+                dy[j] = (row + 0.5f) - c[3 * j + 2];
+                r[j] = __fmaf_rn(dx[j], dx[j], dy[j] * dy[j]);
+                e[j] = __expf(-r[j] * S);
+            }
+            const float mu = __fmaf_rn(A[0], e[0], __fmaf_rn(A[1], e[1], __fmaf_rn(A[2], e[2], B64)));
+            const float q = 1.0f - __fdividef(pl.x, mu);
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                const float qj = q * e[j];
+                gA[j] += qj;
+                gX[j] = __fmaf_rn(qj, dx[j], gX[j]);
+                gY[j] = __fmaf_rn(qj, dy[j], gY[j]);
+                gS = __fmaf_rn(A[j] * qj, r[j], gS);
+            }
+            gB += q;
+        }
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            g[3 * j] = QCS_ASCALE * uniform_sum(gA[j]);
+            g[3 * j + 1] = A[j] * 2.0f * S * uniform_sum(gX[j]);
+            g[3 * j + 2] = A[j] * 2.0f * S * uniform_sum(gY[j]);
+        }
+        g[9] = -QCS_SSCALE * uniform_sum(gS);
+        g[10] = QCS_BSCALE * uniform_sum(gB);
+    }
+};
+
 // Loss and gradient of one multi-emitter ROI (2E, 3E, AS3D-2E) evaluated by
 // a group of G consecutive lanes, bit for bit equal to ThreadEval:
 //  - loss: lane l computes the pixel terms k = l, l + G, ... (multi_term)
