@@ -983,13 +983,13 @@ def learned_shapes_measure(streams, dist, world, rank, mufu_peak=None, cpu_basel
             # and the three-emitter fits from their network's start points (QCS_LEARNED_GS2D_3E)
             three = {"schedule": "three-emitter fits from the network's start points, %d x 6 (plain: 16 x 11); poor "
                                  "ones refitted plainly" % THREE_ITERS}
-            for fb in ("3e", "plain"):
+            for fb, th in (("3e", 0.0), ("plain", 0.0), ("plain", -1.0)):
                 net.set_two_emitter(net2, iters=TWO_ITERS, bisections=6, fallback=fb)
-                net.set_three_emitter(net3, iters=THREE_ITERS, bisections=6)
+                net.set_three_emitter(net3, iters=THREE_ITERS, bisections=6, dev_th=th)
                 ms_t = device_timed(SHAPE_STEPS, 3, learned, streams, dist)
                 learned(0, s0, ctxs[0])
                 rows_t, _ = ctxs[0].read_rows(sh)
-                three["two_emitter_fallback_" + fb] = {
+                three["two_emitter_fallback_" + fb + ("_no_3e_refits" if th < 0 else "")] = {
                     "learned_fits_per_s": job_rate(SHAPE_STEPS, SHAPE_RECORDS, world, ms_t), "vs_plain": ms_p / ms_t,
                     "two_emitter_refits_per_call": net.refits_2e(ctxs[0]),
                     "three_emitter_refits_per_call": net.refits_3e(ctxs[0]),
@@ -1173,6 +1173,8 @@ def mixed_measure(streams, dist, world, rank):
         d_tr, _ = ST.rois(kind, n_train[i], R, seed=20_000 + 100 * rank + i, device="cuda")
         torch.cuda.synchronize()
         ctx_tr = lib.LocContext(para, capacity=n_train[i])
+        if kind == "multi":
+            lib.set_three_emitter_capture(ctx_tr)  # the three-emitter network's targets
         ctx_tr.localize_device(d_tr.data_ptr(), n_train[i], 0, sh)
         labels = lib.count_labels(ctx_tr, n_train[i], sh) if kind == "multi" else None
         feat, scale = lib.LearnedNet.features(para, d_tr.data_ptr(), n_train[i], stream=sh)
@@ -1184,11 +1186,13 @@ def mixed_measure(streams, dist, world, rank):
         torch.cuda.synchronize()
         net = lib.LearnedNet(batch=4096, seed=5, loc_type=para.LocType, roi_size=R)
         net.train(feat, tgt, valid, epochs=MIXED_EPOCHS, lr=2e-3, stream=sh, classes=labels)
-        net2 = None
+        net2 = net3 = None
         if kind == "multi":
             net.set_count_threshold(0.5)
             net2 = train_two_emitter_net(ctx_tr, para, d_tr, feat, scale, n_train[i], R, MIXED_EPOCHS, s0)
             net.set_two_emitter(net2, iters=TWO_ITERS, bisections=6, fallback="plain")
+            net3 = train_three_emitter_net(ctx_tr, para, d_tr, feat, scale, n_train[i], R, MIXED_EPOCHS, s0)
+            net.set_three_emitter(net3, iters=THREE_ITERS, bisections=6, dev_th=-1.0)  # no plain 3E refits
         torch.cuda.synchronize()
         ctx_tr.close()
         del d_tr, feat, scale, tgt, valid, labels
@@ -1228,7 +1232,8 @@ def mixed_measure(streams, dist, world, rank):
             "plain_fits_per_s": n_eval[i] * world / (ms_p * 1e-3),
             "learned_fits_per_s": n_eval[i] * world / (ms_l * 1e-3), "vs_plain": ms_p / ms_l,
             "schedule": "learned %d x %d" % (iters, bis) + (
-                "; two-emitter fits from the network's start points, %d x 6" % TWO_ITERS if net2 else ""),
+                "; two-emitter fits from the network's start points, %d x 6, poor ones refitted plainly; "
+                "three-emitter fits from theirs, %d x 6, no refits" % (TWO_ITERS, THREE_ITERS) if net2 else ""),
             "train_seconds": train_s,
             "accuracy": acc.result(kind == "as3d")}
         for c in ctxs:
@@ -1236,6 +1241,9 @@ def mixed_measure(streams, dist, world, rank):
         if net2 is not None:
             net.set_two_emitter(None)
             net2.close()
+        if net3 is not None:
+            net.set_three_emitter(None)
+            net3.close()
         net.close()
         del d_ev, truth, truth_h
         torch.cuda.empty_cache()

@@ -613,7 +613,9 @@ float qcs_learned_count_threshold(const qcs_learned_net *net);
  * then start the three-emitter stage's fits from its start points, with
  * `iters` BFGS iterations of `bisections` line-search steps (4 or 6 of 6, or
  * 16 of 11; bisections <= 0: 6), and refit plainly every fit that keeps no
- * emitter or whose unweighted Poisson deviance exceeds dev_th (0: 2 R^2 + 2).
+ * emitter or whose unweighted Poisson deviance exceeds dev_th (0: 2 R^2 + 2;
+ * negative: no plain refits, the learned fits' results stand).  A plain refit
+ * pass, even of a few ROIs, costs the plain three-emitter schedule's latency.
  * `three` stays owned by the caller and must outlive the attachment
  * (qcs_learned_destroy refuses it while attached).  The context allocates
  * 97 bytes per record of capacity for the three-emitter stage on the first

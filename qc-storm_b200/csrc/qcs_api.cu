@@ -560,7 +560,7 @@ int three_emitter_starts(qcs_loc_data *c, const qcs_learned_net *net, const qcs_
     QCS_CUDA(qcs::learned::start_points(net3, p, d_rois, n, c->d_start3, s, nullptr, n_dev),
              "three-emitter start points");
     *three = qcs::ThreeEmitterStart{c->d_start3, iters, bisections,
-                                    dev_th > 0.0f ? dev_th : default_dev_th(p->ROISize), c->d_refit3, c->d_slots3,
+                                    dev_th != 0.0f ? dev_th : default_dev_th(p->ROISize), c->d_refit3, c->d_slots3,
                                     c->d_ids3};
     c->three = three;
     return QCS_OK;

@@ -369,19 +369,25 @@ cudaError_t cascade_tail(const CascadeArgs &a, const CascadeState &st) {
                     // learned starts; the plain refits write into the 2E stage's arrays (consumed by its
                     // compaction above) and are merged back into their slots
                     const ThreeEmitterStart &t = *a.three;
-                    if ((e = launch_fit_learned_3e(R, t.iters, t.bisections, f, t.start, t.dev_th, t.refit)) !=
-                        cudaSuccess)
+                    const bool refits = t.dev_th >= 0.0f;
+                    if ((e = launch_fit_learned_3e(R, t.iters, t.bisections, f, t.start, refits ? t.dev_th : 0.0f,
+                                                   t.refit)) != cudaSuccess)
                         return e;
-                    if ((e = launch_flag_slots(t.refit, st.counters + kCnt3E, n, st.q3, t.slots, t.ids,
+                    if (!refits) {
+                        if ((e = cudaMemsetAsync(st.counters + kCntRefit3E, 0, sizeof(int), a.stream)) != cudaSuccess)
+                            return e;
+                    } else if ((e = launch_flag_slots(t.refit, st.counters + kCnt3E, n, st.q3, t.slots, t.ids,
                                                st.counters + kCntRefit3E, a.stream)) != cudaSuccess)
                         return e;
-                    FitLaunch g = f;
-                    g.q = Queue{t.ids, st.counters + kCntRefit3E, 0};
-                    g.mo = MultiOut{st.res2, st.extra2};
-                    if ((e = launch_fit(k3E, R, g)) != cudaSuccess) return e;
-                    if ((e = launch_merge_refit(t.slots, st.counters + kCntRefit3E, n, st.res2, st.extra2, st.res3,
-                                                st.extra3, a.stream)) != cudaSuccess)
-                        return e;
+                    if (refits) {
+                        FitLaunch g = f;
+                        g.q = Queue{t.ids, st.counters + kCntRefit3E, 0};
+                        g.mo = MultiOut{st.res2, st.extra2};
+                        if ((e = launch_fit(k3E, R, g)) != cudaSuccess) return e;
+                        if ((e = launch_merge_refit(t.slots, st.counters + kCntRefit3E, n, st.res2, st.extra2, st.res3,
+                                                    st.extra3, a.stream)) != cudaSuccess)
+                            return e;
+                    }
                 } else if ((e = launch_fit(k3E, R, f)) != cudaSuccess) {
                     return e;
                 }

@@ -66,7 +66,7 @@ struct TwoEmitterStart {
 struct ThreeEmitterStart {
     const float *start;
     int iters, bisections;
-    float dev_th;
+    float dev_th;  // < 0: no plain refits (the learned fits' results stand)
     uint8_t *refit;
     int *slots, *ids;
 };

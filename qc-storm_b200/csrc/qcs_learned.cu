@@ -1382,7 +1382,7 @@ int qcs_learned_set_three_emitter(qcs_learned_net *net, qcs_learned_net *three, 
     if (bisections <= 0) bisections = 6;
     if (!qcs::learned_3e_supported(net->R, iters, bisections))
         return fail(QCS_ERR_ARG, "three-emitter schedules: 4 or 6 iterations of 6 line-search steps, or 16 of 11");
-    if (!(dev_th >= 0.0f)) return fail(QCS_ERR_ARG, "negative deviance bound");
+    if (dev_th != dev_th) return fail(QCS_ERR_ARG, "deviance bound is not a number");
     if (net->three != three) {
         if (net->three) net->three->owners--;
         three->owners++;

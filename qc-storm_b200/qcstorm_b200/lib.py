@@ -669,7 +669,8 @@ class LearnedNet:
 
     def set_three_emitter(self, three, iters=4, bisections=6, dev_th=0.0):
         """Start the three-emitter fits of learned multi-emitter calls from the
-        LEARNED_GS2D_3E network `three` (None detaches); poor fits are refitted plainly."""
+        LEARNED_GS2D_3E network `three` (None detaches); poor fits are refitted
+        plainly (dev_th < 0: no refits, the learned fits' results stand)."""
         check(self.lib.qcs_learned_set_three_emitter(self.h, three.h if three is not None else None, int(iters),
                                                      int(bisections), C.c_float(dev_th)))
         self._three = three

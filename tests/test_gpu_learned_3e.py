@@ -194,16 +194,21 @@ def test_trained_three_emitter_starts_keep_accuracy(cuda_ok):
     net.localize(ctx, d.data_ptr(), m, iters=2, bisections=6, stream=s.cuda_stream)
     three, _ = ctx.read_rows(s.cuda_stream)
     k3 = net.refits_3e(ctx)
+    net.set_three_emitter(net3, iters=4, bisections=6, dev_th=-1.0)  # no plain refits
+    net.localize(ctx, d.data_ptr(), m, iters=2, bisections=6, stream=s.cuda_stream)
+    three_nr, _ = ctx.read_rows(s.cuda_stream)
+    assert net.refits_3e(ctx) == 0
     res = {}
-    for name, rows in (("plain", plain), ("learned", one), ("learned_3e", three)):
+    for name, rows in (("plain", plain), ("learned", one), ("learned_3e", three), ("learned_3e_no_refit", three_nr)):
         dd = match_truth(rows, ev, truth)
         ok = dd < 1.0
         res[name] = (int(ok.sum()), float(np.sqrt(np.mean(dd[ok] ** 2))), rows.shape[0])
     print("matched / rmse / rows", res, "three-emitter refits", k3)
     tp_p, rm_p, _ = res["plain"]
-    tp_3, rm_3, _ = res["learned_3e"]
-    assert tp_3 >= 0.97 * tp_p
-    assert rm_3 <= 1.05 * rm_p
+    for name in ("learned_3e", "learned_3e_no_refit"):
+        tp_3, rm_3, _ = res[name]
+        assert tp_3 >= 0.97 * tp_p, name
+        assert rm_3 <= 1.05 * rm_p, name
     ctx.close()
     net.close()
     net3.close()
