@@ -1438,10 +1438,11 @@ def profile_train(n, stream):
 
 def profile_multi(n, stream):
     """The 1-3 emitter 11x11 workload for ncu: networks trained as in
-    learned_shapes_measure (count classes and two-emitter starts, SHAPE_TRAIN
-    records), then one plain localization call over n records inside the NVTX
-    range "plain" and three learned calls (two-emitter starts, poor fits on to
-    the three-emitter fit) inside "learned"."""
+    learned_shapes_measure (count classes, two- and three-emitter starts,
+    SHAPE_TRAIN records), then one plain localization call over n records
+    inside the NVTX range "plain" and three learned calls (two-emitter starts
+    with plain refits of the poor fits, three-emitter starts without refits:
+    the fastest variant) inside "learned"."""
     import torch
     from qcstorm_b200 import lib, synth
     Rm = 11
@@ -1449,6 +1450,7 @@ def profile_multi(n, stream):
     tr, para, _ = synth.multi_rois(SHAPE_TRAIN, R=Rm, seed=7000)
     d_tr = torch.from_numpy(tr.view(np.int16)).cuda()
     ctx_tr = lib.LocContext(para, capacity=SHAPE_TRAIN)
+    lib.set_three_emitter_capture(ctx_tr)
     ctx_tr.localize_device(d_tr.data_ptr(), SHAPE_TRAIN, 0, sh)
     labels = lib.count_labels(ctx_tr, SHAPE_TRAIN, sh)
     feat, scale = lib.LearnedNet.features(para, d_tr.data_ptr(), SHAPE_TRAIN, stream=sh)
@@ -1460,7 +1462,9 @@ def profile_multi(n, stream):
     net.train(feat, tgt, valid, epochs=TRAIN_EPOCHS, lr=2e-3, stream=sh, classes=labels)
     net.set_count_threshold(0.5)
     net2 = train_two_emitter_net(ctx_tr, para, d_tr, feat, scale, SHAPE_TRAIN, Rm, TRAIN_EPOCHS, stream)
-    net.set_two_emitter(net2, iters=TWO_ITERS, bisections=6)
+    net.set_two_emitter(net2, iters=TWO_ITERS, bisections=6, fallback="plain")
+    net3 = train_three_emitter_net(ctx_tr, para, d_tr, feat, scale, SHAPE_TRAIN, Rm, TRAIN_EPOCHS, stream)
+    net.set_three_emitter(net3, iters=THREE_ITERS, bisections=6, dev_th=-1.0)
     ctx_tr.close()
     rec, _, _ = synth.multi_rois(n, R=Rm, seed=8000)
     d = torch.from_numpy(rec.view(np.int16)).cuda()
@@ -1479,6 +1483,8 @@ def profile_multi(n, stream):
     ctx.close()
     net.set_two_emitter(None)
     net2.close()
+    net.set_three_emitter(None)
+    net3.close()
     net.close()
     return 0
 

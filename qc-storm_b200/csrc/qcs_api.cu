@@ -62,6 +62,11 @@ struct qcs_loc_data {
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;  // high-priority stream for work overlapped with the main stream
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    // the two- / three-emitter start points of a learned call run on their own stream, overlapping the
+    // single-emitter stage; the multi-emitter stages wait for ev_sready
+    cudaStream_t starts = nullptr;
+    cudaEvent_t ev_sfork = nullptr, ev_sready = nullptr;
+    cudaEvent_t starts_ready = nullptr;  // set for the duration of such a call
     cudaEvent_t ev_done = nullptr;  // end of the last asynchronous host call
     float *d_start = nullptr;       // learned start points, capacity x 6 (one block with the three below)
     int *q_refit = nullptr;         // learned multi-emitter path: records to refit plainly
@@ -163,6 +168,9 @@ int qcs_loc_deinit(qcs_loc_data *c) {
     if (c->side) cudaStreamDestroy(c->side);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
     if (c->ev_join) cudaEventDestroy(c->ev_join);
+    if (c->starts) cudaStreamDestroy(c->starts);
+    if (c->ev_sfork) cudaEventDestroy(c->ev_sfork);
+    if (c->ev_sready) cudaEventDestroy(c->ev_sready);
     delete c;
     return QCS_OK;
 }
@@ -205,6 +213,9 @@ int qcs_loc_init_capacity(const qcs_loc_para *p, int capacity, qcs_loc_data **ou
     if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&c->side, cudaStreamNonBlocking, prio_greatest);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->starts, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_sfork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_sready, cudaEventDisableTiming);
     if (e == cudaSuccess) e = qcs::wle_sorter_create(capacity, c->d_wle_scratch, &c->wle_sorter);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_done, cudaEventDisableTiming);
     const size_t b_start = round256(cap * 6 * sizeof(float)), b_refit = round256(cap * sizeof(int));
@@ -497,6 +508,7 @@ cudaError_t learned_multi(qcs_loc_data *c, const uint16_t *d_rois, const float *
     a.pred = cls;
     a.two = c->two;
     a.three = c->three;
+    a.starts_ready = c->starts_ready;
     a.group_limit2 = c->tune_limit2;
     a.group_limit3 = c->tune_limit3;
     cudaError_t e;
@@ -563,6 +575,37 @@ int three_emitter_starts(qcs_loc_data *c, const qcs_learned_net *net, const qcs_
                                     dev_th != 0.0f ? dev_th : default_dev_th(p->ROISize), c->d_refit3, c->d_slots3,
                                     c->d_ids3};
     c->three = three;
+    return QCS_OK;
+}
+
+// The two- and three-emitter start points of a learned multi-emitter call
+// (those of the networks attached to net), on the context's start-point
+// stream forked from s: they overlap the single-emitter stage, and the
+// cascade's multi-emitter stages wait for c->starts_ready (cleared by the
+// caller after the call).
+int multi_starts(qcs_loc_data *c, const qcs_learned_net *net, const qcs_loc_para *p, const uint16_t *d_rois, int n,
+                 const int *n_dev, cudaStream_t s, qcs::TwoEmitterStart *two, qcs::ThreeEmitterStart *three) {
+    c->starts_ready = nullptr;
+    c->two = nullptr;
+    c->three = nullptr;
+    int i2 = 0, b2 = 0, i3 = 0, b3 = 0, t3 = 0;
+    float d2 = 0.0f, d3 = 0.0f;
+    const bool any = qcs::learned::two_emitter(net, &i2, &b2, &d2, &t3) != nullptr ||
+                     qcs::learned::three_emitter(net, &i3, &b3, &d3) != nullptr;
+    if (!any || p->LocType != QCS_LOCTYPE_GS2D || !p->MultiEmitterFitEn || n <= 0) return QCS_OK;
+    QCS_CUDA(cudaEventRecord(c->ev_sfork, s), "fork");
+    QCS_CUDA(cudaStreamWaitEvent(c->starts, c->ev_sfork, 0), "fork");
+    int st = two_emitter_starts(c, net, p, d_rois, n, n_dev, c->starts, two);
+    if (st == QCS_OK) st = three_emitter_starts(c, net, p, d_rois, n, n_dev, c->starts, three);
+    // joined even after an error, so that a capture in progress stays well formed
+    QCS_CUDA(cudaEventRecord(c->ev_sready, c->starts), "join");
+    if (st != QCS_OK) {
+        QCS_CUDA(cudaStreamWaitEvent(s, c->ev_sready, 0), "join");
+        c->two = nullptr;
+        c->three = nullptr;
+        return st;
+    }
+    c->starts_ready = c->ev_sready;
     return QCS_OK;
 }
 
@@ -673,15 +716,14 @@ int qcs_learned_localize_device(qcs_loc_data *c, qcs_learned_net *net, const uin
     QCS_CUDA(qcs::learned::start_points(net, p, d_rois, n, c->d_start, s, cls), "learned start points");
     qcs::TwoEmitterStart two;
     qcs::ThreeEmitterStart three;
-    if (p->MultiEmitterFitEn && (st = two_emitter_starts(c, net, p, d_rois, n, nullptr, s, &two)) != QCS_OK) return st;
-    if (p->MultiEmitterFitEn && (st = three_emitter_starts(c, net, p, d_rois, n, nullptr, s, &three)) != QCS_OK) {
-        c->two = nullptr;
+    if (p->MultiEmitterFitEn && (st = multi_starts(c, net, p, d_rois, n, nullptr, s, &two, &three)) != QCS_OK)
         return st;
-    }
     st = fit_from_start(c, d_rois, d_wle, p, n, c->d_start, cls, iters, bisections, dev_th, s,
                         qcs::learned::direct_two_emitter(net));
+    if (c->starts_ready && st != QCS_OK) cudaStreamWaitEvent(s, c->starts_ready, 0);  // joined on every path
     c->two = nullptr;
     c->three = nullptr;
+    c->starts_ready = nullptr;
     return st;
 }
 
@@ -708,16 +750,14 @@ int qcs_learned_localize_device_n(qcs_loc_data *c, qcs_learned_net *net, const u
     QCS_CUDA(qcs::learned::start_points(net, p, d_rois, max_n, c->d_start, s, cls, d_n), "learned start points");
     qcs::TwoEmitterStart two;
     qcs::ThreeEmitterStart three;
-    if ((st = two_emitter_starts(c, net, p, d_rois, max_n, d_n, s, &two)) != QCS_OK) return st;
-    if ((st = three_emitter_starts(c, net, p, d_rois, max_n, d_n, s, &three)) != QCS_OK) {
-        c->two = nullptr;
-        return st;
-    }
+    if ((st = multi_starts(c, net, p, d_rois, max_n, d_n, s, &two, &three)) != QCS_OK) return st;
     const cudaError_t e =
         learned_multi(c, d_rois, d_wle, p, max_n, d_n, c->d_start, cls, iters, bisections, dev_th, s,
                       qcs::learned::direct_two_emitter(net));
+    if (c->starts_ready && e != cudaSuccess) cudaStreamWaitEvent(s, c->starts_ready, 0);  // joined on every path
     c->two = nullptr;
     c->three = nullptr;
+    c->starts_ready = nullptr;
     QCS_CUDA(e, "learned multi-emitter localization");
     return QCS_OK;
 }

@@ -325,6 +325,7 @@ cudaError_t cascade_tail(const CascadeArgs &a, const CascadeState &st) {
     cudaError_t e;
     FitLaunch f = cascade_single_launch(a, st);
     if (multi) {
+        if (a.starts_ready && (e = cudaStreamWaitEvent(a.stream, a.starts_ready, 0)) != cudaSuccess) return e;
         if ((e = launch_compaction(Append2EStage{st}, n, st, a.stream)) != cudaSuccess) return e;
         const bool has2e = (p.LocType == QCS_LOCTYPE_GS2D) || as3d;
         if (has2e) {

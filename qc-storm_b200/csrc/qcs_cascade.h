@@ -85,6 +85,9 @@ struct CascadeArgs {
     const TwoEmitterStart *two = nullptr;  // learned two-emitter starts (GS2D), or null (the reference's)
     const ThreeEmitterStart *three = nullptr;  // learned three-emitter starts (GS2D), or null (the reference's)
     float *params3 = nullptr;  // when set: the plain three-emitter fits' parameters, 11 per 3E-queue slot
+    // when set: recorded after the two- / three-emitter start points, computed on another stream; the
+    // multi-emitter stages wait for it
+    cudaEvent_t starts_ready = nullptr;
     int group_limit2 = 0, group_limit3 = 0;  // tuned lane-group queue limits of the 2E / 3E stages (0: default)
 };
 
