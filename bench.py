@@ -983,13 +983,17 @@ def learned_shapes_measure(streams, dist, world, rank, mufu_peak=None, cpu_basel
             # and the three-emitter fits from their network's start points (QCS_LEARNED_GS2D_3E)
             three = {"schedule": "three-emitter fits from the network's start points, %d x 6 (plain: 16 x 11); poor "
                                  "ones refitted plainly" % THREE_ITERS}
-            for fb, th in (("3e", 0.0), ("plain", 0.0), ("plain", -1.0)):
+            for fb, th, direct in (("3e", 0.0, False), ("plain", 0.0, False), ("plain", -1.0, False),
+                                   ("plain", -1.0, True)):
                 net.set_two_emitter(net2, iters=TWO_ITERS, bisections=6, fallback=fb)
                 net.set_three_emitter(net3, iters=THREE_ITERS, bisections=6, dev_th=th)
+                net.set_direct_two_emitter(direct)
                 ms_t = device_timed(SHAPE_STEPS, 3, learned, streams, dist)
                 learned(0, s0, ctxs[0])
                 rows_t, _ = ctxs[0].read_rows(sh)
-                three["two_emitter_fallback_" + fb + ("_no_3e_refits" if th < 0 else "")] = {
+                net.set_direct_two_emitter(False)
+                three["two_emitter_fallback_" + fb + ("_no_3e_refits" if th < 0 else "") +
+                      ("_direct_two_emitter" if direct else "")] = {
                     "learned_fits_per_s": job_rate(SHAPE_STEPS, SHAPE_RECORDS, world, ms_t), "vs_plain": ms_p / ms_t,
                     "two_emitter_refits_per_call": net.refits_2e(ctxs[0]),
                     "three_emitter_refits_per_call": net.refits_3e(ctxs[0]),
