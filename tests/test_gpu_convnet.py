@@ -128,3 +128,28 @@ def test_conv_tensor_core_start_points(cuda_ok, loc_type, R, n):
     assert_start_close(fused, layered, sc, 2e-3 * y_scale)
     assert_start_close(fused[:k], start_from_y(y_o, sc[:k], R, loc_type), sc[:k], 2e-3 * y_scale)
     net.close()
+
+
+def test_conv_network_localize_equals_fit_from_its_start_points(cuda_ok):
+    """The learned localization call with a conv network is the fit from that
+    network's start points: its rows equal, bit for bit, those of
+    qcs_fit_from_start_classes_device given the same start points."""
+    import torch
+    n = 20_000
+    rec, para, _, d, feat, scale, t, v, _keep = data(0, 7, n, 71)
+    net = qlib.LearnedNet(batch=4096, seed=4, arch="conv")
+    net.train(feat, t, v, epochs=2, lr=1e-3)
+    s = torch.cuda.Stream()
+    st = net.start(para, d.data_ptr(), n, stream=s.cuda_stream)
+    s.synchronize()
+    ctx = qlib.LocContext(para, capacity=n)
+    net.localize(ctx, d.data_ptr(), n, iters=2, bisections=6, stream=s.cuda_stream)
+    a, ra = ctx.read_rows(s.cuda_stream)
+    qlib.fit_from_start(ctx, d.data_ptr(), n, st.data_ptr(), iters=2, bisections=6, stream=s.cuda_stream)
+    b, rb = ctx.read_rows(s.cuda_stream)
+    net.fused_status()
+    assert (a[:, 0] > 0).mean() > 0.9
+    np.testing.assert_array_equal(a.view(np.uint32), b.view(np.uint32))
+    np.testing.assert_array_equal(ra, rb)
+    ctx.close()
+    net.close()

@@ -138,18 +138,20 @@ def test_three_emitter_fused_start_points(cuda_ok, n):
     net3.close()
 
 
-def test_three_emitter_stage_with_every_fit_redone_gives_plain_stage(cuda_ok):
+@pytest.mark.parametrize("r", [R, 11])
+def test_three_emitter_stage_with_every_fit_redone_gives_plain_stage(cuda_ok, r):
     """With a deviance bound of ~0 every learned three-emitter fit is redone by
     the reference's fit and merged back into its slot: the call's rows equal,
     bit for bit and in order, those of the same learned call without the
-    three-emitter network."""
+    three-emitter network (7x7 and 11x11, the three-emitter queue short
+    enough for the warp-per-ROI kernel)."""
     import torch
-    rec, para, _ = synth.multi_rois(3000, R=R, seed=55)
+    rec, para, _ = synth.multi_rois(3000, R=r, seed=55)
     n = rec.shape[0]
     d = to_dev(rec)
     s = torch.cuda.Stream()
-    net = qlib.LearnedNet(batch=512, seed=5, loc_type=0, roi_size=R)  # routes by the WLE classes
-    net3 = qlib.LearnedNet(batch=512, seed=6, loc_type=qlib.LEARNED_GS2D_3E, roi_size=R)
+    net = qlib.LearnedNet(batch=512, seed=5, loc_type=0, roi_size=r)  # routes by the WLE classes
+    net3 = qlib.LearnedNet(batch=512, seed=6, loc_type=qlib.LEARNED_GS2D_3E, roi_size=r)
     ctx = qlib.LocContext(para, capacity=n)
     net.localize(ctx, d.data_ptr(), n, iters=2, bisections=6, stream=s.cuda_stream)
     ref, ref_r = ctx.read_rows(s.cuda_stream)
