@@ -144,13 +144,18 @@ def test_three_emitter_stage_with_every_fit_redone_gives_plain_stage(cuda_ok, r)
     the reference's fit and merged back into its slot: the call's rows equal,
     bit for bit and in order, those of the same learned call without the
     three-emitter network (7x7 and 11x11, the three-emitter queue short
-    enough for the warp-per-ROI kernel)."""
+    enough for the warp-per-ROI kernel).  The plain 11x11 cascade sends
+    almost no record to the three-emitter fit (~18 per 100,000), so at 11x11
+    the learned count classes route every record there (a class threshold of
+    0.01 on an untrained network)."""
     import torch
     rec, para, _ = synth.multi_rois(3000, R=r, seed=55)
     n = rec.shape[0]
     d = to_dev(rec)
     s = torch.cuda.Stream()
-    net = qlib.LearnedNet(batch=512, seed=5, loc_type=0, roi_size=r)  # routes by the WLE classes
+    net = qlib.LearnedNet(batch=512, seed=5, loc_type=0, roi_size=r)  # 7x7: routes by the WLE classes
+    if r == 11:
+        net.set_count_threshold(0.01)
     net3 = qlib.LearnedNet(batch=512, seed=6, loc_type=qlib.LEARNED_GS2D_3E, roi_size=r)
     ctx = qlib.LocContext(para, capacity=n)
     net.localize(ctx, d.data_ptr(), n, iters=2, bisections=6, stream=s.cuda_stream)
@@ -159,7 +164,7 @@ def test_three_emitter_stage_with_every_fit_redone_gives_plain_stage(cuda_ok, r)
     net.localize(ctx, d.data_ptr(), n, iters=2, bisections=6, stream=s.cuda_stream)
     got, got_r = ctx.read_rows(s.cuda_stream)
     k3 = net.refits_3e(ctx)
-    assert k3 > 0.02 * n
+    assert k3 > (0.02 if r == 7 else 0.5) * n  # every fit of the three-emitter stage redone
     assert got.shape == ref.shape
     np.testing.assert_array_equal(got.view(np.uint32), ref.view(np.uint32))
     np.testing.assert_array_equal(got_r, ref_r)
