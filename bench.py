@@ -984,7 +984,7 @@ def learned_shapes_measure(streams, dist, world, rank, mufu_peak=None, cpu_basel
             three = {"schedule": "three-emitter fits from the network's start points, %d x 6 (plain: 16 x 11); poor "
                                  "ones refitted plainly" % THREE_ITERS}
             for fb, th, direct in (("3e", 0.0, False), ("plain", 0.0, False), ("plain", -1.0, False),
-                                   ("plain", -1.0, True)):
+                                   ("none", -1.0, False), ("plain", -1.0, True)):
                 net.set_two_emitter(net2, iters=TWO_ITERS, bisections=6, fallback=fb)
                 net.set_three_emitter(net3, iters=THREE_ITERS, bisections=6, dev_th=th)
                 net.set_direct_two_emitter(direct)

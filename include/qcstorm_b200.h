@@ -606,8 +606,11 @@ float qcs_learned_count_threshold(const qcs_learned_net *net);
  * A fit is poor when no emitter is kept or when the two-emitter model's
  * Poisson deviance exceeds dev_th (0: 2 ROISize^2 + 2); poor fits go on to the
  * three-emitter fit, as the reference's rejected two-emitter fits do
- * (fallback QCS_TWO_FALLBACK_3E), or are fitted again by the reference's
- * two-emitter fit (QCS_TWO_FALLBACK_PLAIN: one more pass of that fit). */
+ * (fallback QCS_TWO_FALLBACK_3E), are fitted again by the reference's
+ * two-emitter fit (QCS_TWO_FALLBACK_PLAIN: one more pass of that fit), or
+ * keep their own result under the reference's accept rules
+ * (QCS_TWO_FALLBACK_NONE: no refit; a plain refit pass, even of a few ROIs,
+ * costs the plain two-emitter schedule's latency). */
 /* Attaches a QCS_LEARNED_GS2D_3E network `three` of the same ROI size to the
  * GS2D network `net` (NULL detaches): learned multi-emitter calls with `net`
  * then start the three-emitter stage's fits from its start points, with
@@ -658,6 +661,7 @@ int qcs_learned_autotune(qcs_loc_data *c, qcs_learned_net *net, const uint16_t *
                          const qcs_loc_para *p, int n, int *iters, int *bisections, void *stream);
 #define QCS_TWO_FALLBACK_3E 0
 #define QCS_TWO_FALLBACK_PLAIN 1
+#define QCS_TWO_FALLBACK_NONE 2
 int qcs_learned_set_two_emitter(qcs_learned_net *net, qcs_learned_net *two, int iters, int bisections,
                                 float dev_th, int fallback);
 /* Two-emitter fits that the last learned call on c redid with the reference's

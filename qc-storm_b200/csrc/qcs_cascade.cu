@@ -338,13 +338,13 @@ cudaError_t cascade_tail(const CascadeArgs &a, const CascadeState &st) {
                 // learned starts; the plain refits write into the (still unused) 3E stage's arrays and are
                 // merged back into their slots
                 const TwoEmitterStart &t = *a.two;
-                if ((e = launch_fit_learned_2e(R, t.iters, t.bisections, f, t.start, t.dev_th, t.refit, t.to3e)) !=
-                    cudaSuccess)
+                if ((e = launch_fit_learned_2e(R, t.iters, t.bisections, f, t.start, t.dev_th, t.refit,
+                                               t.to3e == 1 ? 1 : 0)) != cudaSuccess)
                     return e;
                 if (!t.to3e && (e = launch_flag_slots(t.refit, st.counters + kCnt2E, n, st.q2, t.slots, t.ids,
                                            st.counters + kCntRefit2E, a.stream)) != cudaSuccess)
                     return e;
-                if (t.to3e) {
+                if (t.to3e) {  // to the 3E fit, or no refit
                     if ((e = cudaMemsetAsync(st.counters + kCntRefit2E, 0, sizeof(int), a.stream)) != cudaSuccess)
                         return e;
                 } else {

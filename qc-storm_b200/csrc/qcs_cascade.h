@@ -55,7 +55,7 @@ struct TwoEmitterStart {
     const float *start;
     int iters, bisections;
     float dev_th;
-    int to3e;  // 1: poor fits go on to the three-emitter fit instead of a plain refit
+    int to3e;  // 1: poor fits go on to the three-emitter fit; 0: plain refit; 2: no refit (their results stand)
     uint8_t *refit;
     int *slots, *ids;
 };

@@ -1354,9 +1354,9 @@ int qcs_learned_set_two_emitter(qcs_learned_net *net, qcs_learned_net *two, int 
     if (!qcs::learned_2e_supported(net->R, iters, bisections))
         return fail(QCS_ERR_ARG, "two-emitter schedules: 3 or 4 iterations of 6 line-search steps, or 13 of 11");
     if (!(dev_th >= 0.0f)) return fail(QCS_ERR_ARG, "negative deviance bound");
-    if (fallback != QCS_TWO_FALLBACK_3E && fallback != QCS_TWO_FALLBACK_PLAIN)
-        return fail(QCS_ERR_ARG, "fallback: QCS_TWO_FALLBACK_3E or QCS_TWO_FALLBACK_PLAIN");
-    net->two_to3e = fallback == QCS_TWO_FALLBACK_3E ? 1 : 0;
+    if (fallback != QCS_TWO_FALLBACK_3E && fallback != QCS_TWO_FALLBACK_PLAIN && fallback != QCS_TWO_FALLBACK_NONE)
+        return fail(QCS_ERR_ARG, "fallback: QCS_TWO_FALLBACK_3E, QCS_TWO_FALLBACK_PLAIN or QCS_TWO_FALLBACK_NONE");
+    net->two_to3e = fallback == QCS_TWO_FALLBACK_3E ? 1 : (fallback == QCS_TWO_FALLBACK_NONE ? 2 : 0);
     if (net->two != two) {
         if (net->two) net->two->owners--;
         two->owners++;

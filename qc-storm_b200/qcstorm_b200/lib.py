@@ -650,11 +650,13 @@ class LearnedNet:
     def set_two_emitter(self, two, iters=3, bisections=6, dev_th=0.0, fallback="3e"):
         """Start the two-emitter fits of learned multi-emitter calls from the
         LEARNED_GS2D_2E network `two` (None detaches); poor fits go on to the
-        three-emitter fit (fallback "3e") or are refitted plainly ("plain")."""
-        if fallback not in ("3e", "plain"):
-            raise ValueError("fallback: '3e' or 'plain'")
+        three-emitter fit (fallback "3e"), are refitted plainly ("plain"), or keep
+        their own result ("none")."""
+        modes = {"3e": 0, "plain": 1, "none": 2}  # QCS_TWO_FALLBACK_3E, _PLAIN, _NONE
+        if fallback not in modes:
+            raise ValueError("fallback: '3e', 'plain' or 'none'")
         check(self.lib.qcs_learned_set_two_emitter(self.h, two.h if two is not None else None, int(iters),
-                                                   int(bisections), C.c_float(dev_th), 0 if fallback == "3e" else 1))
+                                                   int(bisections), C.c_float(dev_th), modes[fallback]))
         self._two = two
 
     def autotune(self, ctx, d_rois, n, d_wle=0, para=None, stream=0):

@@ -176,14 +176,19 @@ def test_trained_two_emitter_starts_keep_accuracy(cuda_ok):
     net.localize(ctx, d.data_ptr(), m, iters=2, bisections=6, stream=s.cuda_stream)
     two, _ = ctx.read_rows(s.cuda_stream)
     assert net.refits_2e(ctx) == 0
+    net.set_two_emitter(net2, iters=3, bisections=6, fallback="none")  # poor fits keep their own result
+    net.localize(ctx, d.data_ptr(), m, iters=2, bisections=6, stream=s.cuda_stream)
+    two_n, _ = ctx.read_rows(s.cuda_stream)
+    assert net.refits_2e(ctx) == 0
     res = {}
-    for name, rows in (("plain", plain), ("learned", one), ("learned_2e_refit", two_p), ("learned_2e", two)):
+    for name, rows in (("plain", plain), ("learned", one), ("learned_2e_refit", two_p), ("learned_2e", two),
+                       ("learned_2e_none", two_n)):
         dd = match_truth(rows, ev, truth)
         ok = dd < 1.0
         res[name] = (int(ok.sum()), float(np.sqrt(np.mean(dd[ok] ** 2))), rows.shape[0])
     print("matched / rmse / rows", res, "two-emitter refits", k2)
     tp_p, rm_p, _ = res["plain"]
-    for name in ("learned_2e_refit", "learned_2e"):
+    for name in ("learned_2e_refit", "learned_2e", "learned_2e_none"):
         tp_2, rm_2, _ = res[name]
         assert tp_2 >= 0.97 * tp_p, name
         assert rm_2 <= 1.05 * rm_p, name
