@@ -378,12 +378,14 @@ def frame_truth_match(rows, truth, radius=1.0):
             "rmse_px": float(np.sqrt(np.mean(dist[ok] ** 2))) if ok.any() else None}
 
 
-def train_frame_net(para, stream, seed=9001):
+def train_frame_net(para, stream, seed=9001, multi_starts=False):
     """The network of the learned frame pipeline, trained on the GPU on the
     records that extraction cuts from TRAIN_FRAMES fresh frames (same
     generator, other seeds): start-point targets from the records the plain
     multi-emitter cascade kept single, emitter-count classes from its outcome
-    (qcs_loc_count_labels_device).  Returns (net, info)."""
+    (qcs_loc_count_labels_device).  With multi_starts, also two- and
+    three-emitter start-point networks on the same records, attached.
+    Returns (net, info, extra networks)."""
     import torch
     from qcstorm_b200 import lib, synth
     sh = stream.cuda_stream
@@ -398,6 +400,8 @@ def train_frame_net(para, stream, seed=9001):
         ex.extract_device(d_fr.data_ptr() + f * fb, 1, f, stream=sh)
     n = ex.accumulated()
     d_rois, d_wle, _ = ex.device_records()
+    if multi_starts:
+        lib.set_three_emitter_capture(loc)
     loc.localize_device(d_rois, n, d_wle, sh)
     labels = lib.count_labels(loc, n, sh)
     feat, scale = lib.LearnedNet.features(para, d_rois, n, stream=sh)
@@ -409,6 +413,15 @@ def train_frame_net(para, stream, seed=9001):
     net = lib.LearnedNet(batch=4096, seed=5)
     losses = net.train(feat, tgt, valid, epochs=TRAIN_EPOCHS, lr=2e-3, stream=sh, classes=labels)
     stream.synchronize()
+    extra = []
+    if multi_starts:
+        dr = _DevPtr(d_rois)
+        net2 = train_two_emitter_net(loc, para, dr, feat, scale, n, R, TRAIN_EPOCHS, stream)
+        net3 = train_three_emitter_net(loc, para, dr, feat, scale, n, R, TRAIN_EPOCHS, stream)
+        net.set_two_emitter(net2, iters=TWO_ITERS, bisections=6, fallback="none")
+        net.set_three_emitter(net3, iters=THREE_ITERS, bisections=6, dev_th=-1.0)
+        net.set_direct_two_emitter(True)
+        extra = [net2, net3]
     info = {"frames": TRAIN_FRAMES, "records": n, "epochs": TRAIN_EPOCHS, "seconds": time.perf_counter() - t0,
             "loss_first_epoch": float(losses[0]), "loss_last_epoch": float(losses[-1]),
             "class_counts": counts,
@@ -416,7 +429,17 @@ def train_frame_net(para, stream, seed=9001):
                       "outcome per record (0: kept single, 1: kept by the 2E fit, 2: passed on to the 3E fit)"}
     ex.close()
     loc.close()
-    return net, info
+    return net, info, extra
+
+
+class _DevPtr:
+    """A raw device address where a helper expects a tensor's data_ptr()."""
+
+    def __init__(self, ptr):
+        self.ptr = ptr
+
+    def data_ptr(self):
+        return self.ptr
 
 
 def frame_pipeline(stream, steps, warmup, e2e=True, dist=None, world=1, net=None):
@@ -532,17 +555,21 @@ def frame_pipeline(stream, steps, warmup, e2e=True, dist=None, world=1, net=None
     }
 
 
-def frame_pipeline_learned(stream, steps, warmup, dist=None, world=1):
+def frame_pipeline_learned(stream, steps, warmup, dist=None, world=1, multi_starts=False):
     """The frame pipeline with the learned localization call, after training
-    its network on records of other frames."""
+    its network on records of other frames; with multi_starts, also two- and
+    three-emitter start points, poor bright single fits routed straight to
+    the two-emitter fit and no plain refits of the multi-emitter stages."""
     from qcstorm_b200.abi import default_para
     # the camera of synth.frames, multi-emitter fitting on (as in frame_pipeline)
     para = default_para(Offset=100.0, KAdc=0.45, QE=1.0, ImageWidth=FRAME_W, ImageHigh=FRAME_H, MultiEmitterFitEn=1)
-    net, info = train_frame_net(para, stream)
+    net, info, extra = train_frame_net(para, stream, multi_starts=multi_starts)
     net.set_count_threshold(COUNT_TH)
     r = frame_pipeline(stream, steps, warmup, e2e=True, dist=dist, world=world, net=net)
     net.fused_status()
     net.close()
+    for x in extra:
+        x.close()
     r["train"] = info
     r["count_threshold"] = COUNT_TH
     r["schedule"] = "%d BFGS iterations x %d line-search steps from the network's start points" % (
@@ -1716,6 +1743,10 @@ def main():
         if not args.no_learned:
             frames["learned"] = frame_pipeline_learned(stream, fsteps, 3, dist=dist, world=world)
             frames["learned"]["vs_plain"] = frames["learned"]["frames_per_s"] / frames["frames_per_s"]
+            frames["learned_multi_starts"] = frame_pipeline_learned(stream, fsteps, 3, dist=dist, world=world,
+                                                                    multi_starts=True)
+            frames["learned_multi_starts"]["vs_plain"] = (frames["learned_multi_starts"]["frames_per_s"] /
+                                                          frames["frames_per_s"])
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
