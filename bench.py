@@ -711,6 +711,24 @@ def learned_measure(args, streams, ctxs, para, d_batches, h_batches, rec0, truth
     e2e_s, _ = e2e_pipelined(ctxs, streams, h_batches, e2e_steps, net=net)
     e2e_s = max_over_ranks(e2e_s * 1e3, dist) * 1e-3
     start_ms = start_point_ms(net, para, d_batches, stream, dist)
+    # the same call without the plain refits of the rejected or poor learned fits (qcs_learned_set_single_refits)
+    net.set_single_refits(False)
+    nr_steps = min(args.steps, 200)
+    ms_nr = device_timed(nr_steps, 3, step, streams, dist)
+    step(0, stream, ctx)
+    rows_nr, _ = ctx.read_rows(sh)
+    net.set_single_refits(True)
+    acc_nr = rows_nr[:, 0] > 0
+    both_nr = acc_p & acc_nr
+    rp_nr, _, _ = fit_accuracy(plain, rec0, truth0, both_nr, para)
+    rn, pn, _ = fit_accuracy(rows_nr, rec0, truth0, both_nr, para)
+    rn_own, _, _ = fit_accuracy(rows_nr, rec0, truth0, acc_nr, para)
+    no_refit = {"value": job_rate(nr_steps, N_PER_STEP, world, ms_nr), "unit": UNIT,
+                "vs_plain": job_rate(nr_steps, N_PER_STEP, world, ms_nr) / plain_value,
+                "rmse_px": {"plain": rp_nr, "no_refit": rn}, "photon_rel_rmse_no_refit": pn,
+                "rmse_px_own_accepted": rn_own, "accepted": float(acc_nr.mean()),
+                "basis": "batch 0; records accepted by both plain and this variant (own: its own accepted records)",
+                "call": "qcs_learned_set_single_refits(net, 0): the learned fits' results stand"}
     net.close()
     conv = conv_arm(args, streams, ctxs, para, d_batches, rec0, truth0, plain_value, value, start_ms, world, dist)
     return {
@@ -743,6 +761,7 @@ def learned_measure(args, streams, ctxs, para, d_batches, h_batches, rec0, truth
         "network": "64-128-128-8 MLP on the 7x7 pixels (+2 scale features), BF16 operands, FP32 accumulation; "
                    "inference fused with the features in one tcgen05 kernel",
         "start_points_ms_per_step": start_ms,
+        "no_refit": no_refit,
         "conv": conv,
     }
 
@@ -1790,6 +1809,10 @@ def main():
                 "plain_rmse_over_fisher_crlb": a["fisher_crlb"]["plain"]["rms_error_over_own_crlb"],
                 "learned_rmse_over_fisher_crlb": a["fisher_crlb"]["learned"]["rms_error_over_own_crlb"],
                 "learned_equal_rmse_within_2pct_of_crlb": a["fisher_crlb"]["equal_rmse_within_2pct_of_crlb"],
+                "learned_no_refit_value": learned["no_refit"]["value"],
+                "learned_no_refit_vs_plain": learned["no_refit"]["vs_plain"],
+                "learned_no_refit_rmse_px": learned["no_refit"]["rmse_px"]["no_refit"],
+                "learned_no_refit_accept": learned["no_refit"]["accepted"],
                 "learned_conv_value": learned["conv"]["value"], "learned_conv_vs_plain": learned["conv"]["vs_plain"],
                 "learned_conv_rmse_px": learned["conv"]["accuracy"]["rmse_px"]["conv"],
             })
@@ -1798,7 +1821,8 @@ def main():
                 "vs_baseline", "dtype", "data", "learned_value", "learned_vs_plain", "learned_e2e_value",
                 "learned_rmse_px", "plain_rmse_px", "learned_rmse_px_own", "plain_rmse_px_own", "learned_accept",
                 "plain_accept", "learned_equal_rmse", "crlb_px", "fisher_crlb_px", "plain_rmse_over_fisher_crlb",
-                "learned_rmse_over_fisher_crlb", "learned_equal_rmse_within_2pct_of_crlb", "learned_conv_value",
+                "learned_rmse_over_fisher_crlb", "learned_equal_rmse_within_2pct_of_crlb", "learned_no_refit_value",
+                "learned_no_refit_vs_plain", "learned_no_refit_rmse_px", "learned_no_refit_accept", "learned_conv_value",
                 "learned_conv_vs_plain", "learned_conv_rmse_px", "gpu_launches", "windows",
                 "clocks", "roofline",
                 "e2e", "cpu_baseline", "config"]

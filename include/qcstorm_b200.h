@@ -642,6 +642,13 @@ const float *qcs_loc_device_three_emitter_params(const qcs_loc_data *ctx);
  * qcs_learned_features_device. */
 int qcs_loc_three_emitter_targets_device(qcs_loc_data *ctx, const uint16_t *d_rois, const qcs_loc_para *p, int n,
                                          const float *d_scale, float *d_targets, float *d_valid, void *stream);
+/* Learned calls without multi-emitter fitting refit plainly every learned fit
+ * that is not accepted or whose deviance exceeds dev_th (on, the default).
+ * With on = 0 the learned fits' results stand: no refit pass and rejected
+ * fits stay rejected (the plain fit might have accepted some of them).
+ * Multi-emitter calls always route the poor single fits by a plain refit or,
+ * with qcs_learned_set_direct_two_emitter, to the two-emitter fit. */
+int qcs_learned_set_single_refits(qcs_learned_net *net, int on);
 /* Multi-emitter learned calls: a learned single-emitter fit that is rejected
  * or judged poor by the deviance bound and has SNR > 6 goes straight to the
  * two-emitter fit (the reference's rule for its rejected single fits, applied

@@ -611,7 +611,7 @@ int multi_starts(qcs_loc_data *c, const qcs_learned_net *net, const qcs_loc_para
 
 int fit_from_start(qcs_loc_data *c, const uint16_t *d_rois, const float *d_wle, const qcs_loc_para *p, int n,
                    const float *d_start, const uint8_t *d_classes, int iters, int bisections, float dev_th,
-                   void *stream, bool direct2e);
+                   void *stream, bool direct2e, bool refits = true);
 }  // namespace
 
 extern "C" {
@@ -635,7 +635,7 @@ namespace {
 // network-driven calls)
 int fit_from_start(qcs_loc_data *c, const uint16_t *d_rois, const float *d_wle, const qcs_loc_para *p, int n,
                    const float *d_start, const uint8_t *d_classes, int iters, int bisections, float dev_th,
-                   void *stream, bool direct2e) {
+                   void *stream, bool direct2e, bool refits) {
     int st = check_call(c, p, n);
     if (st) return st;
     const int kind = learned_kind(p);
@@ -671,6 +671,15 @@ int fit_from_start(qcs_loc_data *c, const uint16_t *d_rois, const float *d_wle, 
     f.stream = s;
     QCS_CUDA(qcs::launch_fit_learned(kind, p->ROISize, iters, bisections, f, d_start, dev_th, c->st.to2e),
              "start-point fit");
+    if (!refits) {
+        // the learned fits' results stand: no refit queue, the CRLB of every row
+        QCS_CUDA(cudaMemsetAsync(c->st.counters + qcs::kCntSingle, 0, sizeof(int), s), "refit count");
+        learned_counters_kernel<<<1, 1, 0, s>>>(c->st, n);
+        QCS_CUDA(cudaGetLastError(), "counters");
+        QCS_CUDA(qcs::launch_crlb(c->d_loc, nullptr, n, n, p->LocType, p->ReadNoise_e, p->QE, p->PixelSize, s),
+                 "CRLB");
+        return QCS_OK;
+    }
     // plain refit of the flagged records
     QCS_CUDA(qcs::launch_flag_queue(c->st.to2e, n, c->st.q_single, c->st.counters + qcs::kCntSingle, s),
              "refit queue");
@@ -719,7 +728,7 @@ int qcs_learned_localize_device(qcs_loc_data *c, qcs_learned_net *net, const uin
     if (p->MultiEmitterFitEn && (st = multi_starts(c, net, p, d_rois, n, nullptr, s, &two, &three)) != QCS_OK)
         return st;
     st = fit_from_start(c, d_rois, d_wle, p, n, c->d_start, cls, iters, bisections, dev_th, s,
-                        qcs::learned::direct_two_emitter(net));
+                        qcs::learned::direct_two_emitter(net), qcs::learned::single_refits(net));
     if (c->starts_ready && st != QCS_OK) cudaStreamWaitEvent(s, c->starts_ready, 0);  // joined on every path
     c->two = nullptr;
     c->three = nullptr;

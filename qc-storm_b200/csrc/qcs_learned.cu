@@ -735,6 +735,7 @@ struct qcs_learned_net {
     qcs_learned_net *two = nullptr;
     int owners = 0;  // GS2D networks this (two-emitter) network is attached to
     int direct_2e = 0;  // multi-emitter calls: poor bright single fits straight to the 2E stage
+    int single_refits = 1;  // single-emitter calls: plain refits of the rejected or poor learned fits
     int two_iters = 3, two_bisections = 6, two_to3e = 1;
     float two_dev_th = 0.0f;
     // GS2D networks: the three-emitter network whose start points the 3E stage uses, and its schedule
@@ -968,6 +969,7 @@ int check_shape(const qcs_learned_net *net, const qcs_loc_para *p) {
 namespace qcs {
 namespace learned {
 bool direct_two_emitter(const qcs_learned_net *net) { return net && net->direct_2e; }
+bool single_refits(const qcs_learned_net *net) { return !net || net->single_refits; }
 
 qcs_learned_net *three_emitter(const qcs_learned_net *net, int *iters, int *bisections, float *dev_th) {
     if (!net || !net->three) return nullptr;
@@ -1391,6 +1393,12 @@ int qcs_learned_set_three_emitter(qcs_learned_net *net, qcs_learned_net *three, 
     net->three_iters = iters;
     net->three_bisections = bisections;
     net->three_dev_th = dev_th;
+    return QCS_OK;
+}
+
+int qcs_learned_set_single_refits(qcs_learned_net *net, int on) {
+    if (!net) return fail(QCS_ERR_ARG, "null network");
+    net->single_refits = on ? 1 : 0;
     return QCS_OK;
 }
 

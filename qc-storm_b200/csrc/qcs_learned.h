@@ -161,6 +161,8 @@ qcs_learned_net *two_emitter(const qcs_learned_net *net, int *iters, int *bisect
 // The three-emitter network attached to a GS2D network (qcs_learned_set_three_emitter)
 // and its schedule, or null.
 qcs_learned_net *three_emitter(const qcs_learned_net *net, int *iters, int *bisections, float *dev_th);
+// qcs_learned_set_single_refits's setting
+bool single_refits(const qcs_learned_net *net);
 // qcs_learned_set_direct_two_emitter's setting
 bool direct_two_emitter(const qcs_learned_net *net);
 }  // namespace learned

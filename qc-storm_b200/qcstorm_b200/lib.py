@@ -127,6 +127,7 @@ _SIGS = {
     "qcs_learned_set_count_threshold": (C.c_int, [C.c_void_p, C.c_float]),
     "qcs_learned_set_two_emitter": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_int]),
     "qcs_learned_set_direct_two_emitter": (C.c_int, [C.c_void_p, C.c_int]),
+    "qcs_learned_set_single_refits": (C.c_int, [C.c_void_p, C.c_int]),
     "qcs_learned_refit_2e_num": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "qcs_learned_set_three_emitter": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_float]),
     "qcs_learned_refit_3e_num": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
@@ -681,6 +682,10 @@ class LearnedNet:
         k = C.c_int(0)
         check(self.lib.qcs_learned_refit_3e_num(ctx.h, C.byref(k)))
         return k.value
+
+    def set_single_refits(self, on=True):
+        """Single-emitter learned calls: plain refits of the rejected or poor fits (off: their results stand)."""
+        check(self.lib.qcs_learned_set_single_refits(self.h, 1 if on else 0))
 
     def set_direct_two_emitter(self, on=True):
         """Multi-emitter calls: poor bright single fits straight to the two-emitter fit."""
