@@ -238,5 +238,17 @@ def test_trained_start_points_reach_plain_rmse_with_fewer_iterations(cuda_ok, bi
     assert r_naive > 1.05 * r_plain
     assert refits <= 0.10 * m
     assert (learned[:, 0] > 0).mean() >= (plain[:, 0] > 0).mean() - 0.005
+    # without the plain refits (qcs_learned_set_single_refits): no refit pass, the same accuracy
+    net.set_single_refits(False)
+    net.localize(ctx, d_ev.data_ptr(), m, iters=2, bisections=bisections, stream=s.cuda_stream)
+    nr, _ = ctx.read_rows(s.cuda_stream)
+    assert net.refits(ctx) == 0
+    both_nr = (plain[:, 0] > 0) & (nr[:, 0] > 0)
+    assert rmse_xy(nr, ev, truth, both_nr) <= 1.02 * rmse_xy(plain, ev, truth, both_nr)
+    assert (nr[:, 0] > 0).mean() >= (plain[:, 0] > 0).mean() - 0.005
+    # rows the default call did not refit are the no-refit call's bit for bit
+    same = (learned[:, 0] > 0) & (nr[:, 0] > 0)
+    assert np.mean(np.all(learned[same].view(np.uint32) == nr[same].view(np.uint32), axis=1)) >= 1.0 - refits / m
+    net.set_single_refits(True)
     ctx.close()
     net.close()
