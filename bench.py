@@ -1237,6 +1237,8 @@ def mixed_measure(streams, dist, world, rank):
         net = lib.LearnedNet(batch=4096, seed=5, loc_type=para.LocType, roi_size=R)
         net.train(feat, tgt, valid, epochs=MIXED_EPOCHS, lr=2e-3, stream=sh, classes=labels)
         net2 = net3 = None
+        if kind != "multi":
+            net.set_single_refits(False)  # the learned fits' results stand (accuracy below)
         if kind == "multi":
             net.set_count_threshold(0.5)
             net2 = train_two_emitter_net(ctx_tr, para, d_tr, feat, scale, n_train[i], R, MIXED_EPOCHS, s0)
@@ -1284,7 +1286,7 @@ def mixed_measure(streams, dist, world, rank):
             "train_records": n_train[i], "eval_records": n_eval[i], "calls": len(calls),
             "plain_fits_per_s": n_eval[i] * world / (ms_p * 1e-3),
             "learned_fits_per_s": n_eval[i] * world / (ms_l * 1e-3), "vs_plain": ms_p / ms_l,
-            "schedule": "learned %d x %d" % (iters, bis) + (
+            "schedule": "learned %d x %d" % (iters, bis) + ("; no plain refits" if kind != "multi" else "") + (
                 "; poor bright single fits straight to the two-emitter fit; two-emitter fits from the network's start "
                 "points, %d x 6, and three-emitter fits from theirs, %d x 6, without plain refits (more emitters "
                 "found than the plain cascade, see accuracy)" % (TWO_ITERS, THREE_ITERS) if net2 else ""),
