@@ -530,18 +530,20 @@ __global__ void __launch_bounds__(kGroupTPB) fit_single_group_kernel(const uint1
 // deviance 2 sum(mu - n - n ln(mu / n)) exceeds dev_th: those ROIs are
 // refitted by the plain kernel, which also decides whether a rejected one
 // goes on to the two-emitter fit (to2e).
+// Layout of fit_single_kernel: the pixels' (value, log) pairs and the mask's
+// unique values (the full mask where its rounding is nvcc's per pixel) in
+// shared memory, the inverse Hessian in registers.
 template <int KIND, int R, int ITERS, int NB, int DIST = ArithSpec<KIND, R>::DIST,
-          int MASK = ArithSpec<KIND, R>::MASK>
-__global__ void __launch_bounds__(kTPB) fit_learned_kernel(const uint16_t *__restrict__ rois,
-                                                           const float *__restrict__ wle,
-                                                           const float *__restrict__ start, Queue q,
-                                                           float *__restrict__ loc, uint8_t *__restrict__ refit,
-                                                           uint8_t *__restrict__ to2e, CorePara c, float dev_th,
-                                                           int direct2e) {
-    typedef SmemLayout<R, KIND> L;
+          int MASK = ArithSpec<KIND, R>::MASK, bool FULL = (ArithSpec<KIND, R>::MASK == kCompiler)>
+__global__ void __launch_bounds__(kTPB, (SingleLayout<R, FULL>::BLOCKS))
+    fit_learned_kernel(const uint16_t *__restrict__ rois, const float *__restrict__ wle,
+                       const float *__restrict__ start, Queue q, float *__restrict__ loc,
+                       uint8_t *__restrict__ refit, uint8_t *__restrict__ to2e, CorePara c, float dev_th,
+                       int direct2e) {
+    typedef SingleLayout<R, FULL> L;
     enum { P = KindTraits<KIND>::P, PIX = R * R, WHOLE = R * (R + 1) };
-    typedef typename std::conditional<KIND == kGS2D, AnalyticEvalGS2D<R, DIST>, AnalyticEvalAS3D<R, DIST>>::type Eval;
-    extern __shared__ float smem[];
+    typedef StagedAnalyticEval<R, KIND, DIST, FULL> Eval;
+    extern __shared__ __align__(16) float smem[];
     const int n = queue_len(q);
     const int base = blockIdx.x * kTPB;
     if (base >= n) return;
@@ -552,18 +554,21 @@ __global__ void __launch_bounds__(kTPB) fit_learned_kernel(const uint16_t *__res
     const int tid = threadIdx.x;
     if (tid >= cnt) return;
     const int id = queue_at(q, base + tid);
-    float *w = smem + L::W + tid;
-    float *D = smem + L::D + tid;
+    // the mask: FULL, pixel k at mask[k * kTPB]; else float4 chunk j at ((float4 *)mask)[j * kTPB]
+    float *mask = smem + L::WU + (FULL ? tid : 4 * tid);
     const uint16_t *hdr = rois + (size_t)id * WHOLE + PIX;
     const int XOffset = hdr[0], YOffset = hdr[1];
     const int CurFrame = hdr[2] + 65536 * hdr[3];
     const float *pw = wle + (size_t)id * QCS_WLE_PARA_NUM;
     const PixView img{s_img + tid, kTPB};
-    const RoiRef roi{s_img + tid, w, kTPB};
 
     float Ininf[P];
     const SinglePrep sp = single_prefit<R, KIND, false>(img, pw, c, Ininf);  // mask widths only
-    wle_weights<R, MASK>(w, kTPB, sp.WLE_SigmaX, sp.WLE_SigmaY, sp.MoleculeType);
+    if constexpr (FULL)
+        wle_weights<R, MASK>(mask, kTPB, sp.WLE_SigmaX, sp.WLE_SigmaY, sp.MoleculeType);
+    else
+        wle_weights_unique<R, MASK>(reinterpret_cast<float4 *>(mask), kTPB, sp.WLE_SigmaX, sp.WLE_SigmaY,
+                                    sp.MoleculeType);
     const float *st = start + (size_t)id * P;
     Ininf[0] = st[0] * rAScalFactor;
     Ininf[1] = st[1];
@@ -575,7 +580,8 @@ __global__ void __launch_bounds__(kTPB) fit_learned_kernel(const uint16_t *__res
         Ininf[4] = (0.5f / (st[4] * st[4])) * rSScalFactor;
         Ininf[P - 1] = st[5] * rBScalFactor;
     }
-    bfgs_fit<P, ITERS, Eval, NB>(Eval{roi}, Ininf, D, kTPB);
+    float D[P * P];  // the inverse Hessian, in registers
+    bfgs_fit<P, ITERS, Eval, NB>(Eval{{s_img + tid, mask, kTPB}}, Ininf, D, 1);
 
     float row[12];
     bool accepted;
@@ -588,7 +594,7 @@ __global__ void __launch_bounds__(kTPB) fit_learned_kernel(const uint16_t *__res
 #pragma unroll 1
     for (int r = 0; r < R; r++)
         for (int col = 0; col < R; col++) {
-            const float2 pl = roi.img[(r * R + col) * roi.ld];
+            const float2 pl = s_img[tid + (r * R + col) * kTPB];
             const float e = single_expo<KIND, DIST>(col + 0.5f, r + 0.5f, Ininf);
             dev += single_term<KIND>(e, Ininf, pl.x, pl.y);
         }
@@ -611,7 +617,7 @@ __global__ void __launch_bounds__(kTPB) fit_learned_kernel(const uint16_t *__res
 
 template <int KIND, int R, int ITERS, int NB>
 cudaError_t launch_learned(const FitLaunch &a, const float *start, float dev_th, uint8_t *refit) {
-    const size_t smem = SmemLayout<R, KIND>::TOTAL * sizeof(float);
+    const size_t smem = SingleLayout<R, ArithSpec<KIND, R>::MASK == kCompiler>::BYTES;
     auto k = fit_learned_kernel<KIND, R, ITERS, NB>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;

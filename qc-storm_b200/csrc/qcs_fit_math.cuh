@@ -1176,6 +1176,90 @@ struct StagedEval {
     }
 };
 
+// The learned-start single fit's loss and analytic gradient over the staged
+// layout of fit_single_kernel (pixels as (value, log) pairs, the mask's unique
+// values): StagedEval's loss, the gradient of AnalyticEvalGS2D /
+// AnalyticEvalAS3D term for term (the mask values are the same, so the
+// results are those of the full-mask evaluators).
+template <int R, int KIND, int DIST, bool FULL = false>
+struct StagedAnalyticEval : StagedEval<R, KIND, DIST, FULL> {
+    typedef StagedEval<R, KIND, DIST, FULL> B;
+    __device__ __forceinline__ void gradient(const float *v, float *g) const {
+        enum { NW = FULL ? R : B::M::C4 * 4 };
+        if constexpr (KIND == kGS2D) {
+            float c[5];
+#pragma unroll
+            for (int k = 0; k < 5; k++) c[k] = v[k] < 0.0f ? 0.0f : v[k];
+            const float A128 = c[0] * QCS_ASCALE, B64 = c[4] * QCS_BSCALE, S01 = c[3] * QCS_SSCALE;
+            float gA = 0, gX = 0, gY = 0, gS = 0, gB = 0;
+#pragma unroll 1
+            for (int row = 0; row < R; row++) {
+                float wr[NW];
+                this->mask_row(row, wr);
+                const float dy = (row + 0.5f) - c[2];
+#pragma unroll(R <= kUnrollMaxR ? R : 1)
+                for (int col = 0; col < R; col++) {
+                    const float2 pl = this->img[(row * R + col) * this->ld];
+                    const float w = wr[B::wcol(col)];
+                    const float dx = (col + 0.5f) - c[1];
+                    const float r2 = __fmaf_rn(dx, dx, dy * dy);
+                    const float e = __expf(-r2 * S01);
+                    const float mu = __fmaf_rn(A128, e, B64);
+                    const float q = w * (1.0f - __fdividef(pl.x, mu));
+                    const float qe = q * e;
+                    gA += qe;
+                    gX = __fmaf_rn(qe, dx, gX);
+                    gY = __fmaf_rn(qe, dy, gY);
+                    gS = __fmaf_rn(qe, r2, gS);
+                    gB += q;
+                }
+            }
+            g[0] = QCS_ASCALE * gA;
+            g[1] = A128 * 2.0f * S01 * gX;
+            g[2] = A128 * 2.0f * S01 * gY;
+            g[3] = -A128 * QCS_SSCALE * gS;
+            g[4] = QCS_BSCALE * gB;
+        } else {
+            float c[6];
+#pragma unroll
+            for (int k = 0; k < 6; k++) c[k] = v[k] < 0.01f ? 0.01f : v[k];
+            const float A128 = c[0] * QCS_ASCALE, B64 = c[5] * QCS_BSCALE;
+            const float Sx = c[3] * QCS_SSCALE, Sy = c[4] * QCS_SSCALE;
+            float gA = 0, gX = 0, gY = 0, gSx = 0, gSy = 0, gB = 0;
+#pragma unroll 1
+            for (int row = 0; row < R; row++) {
+                float wr[NW];
+                this->mask_row(row, wr);
+                const float dy = (row + 0.5f) - c[2];
+                const float qy = dy * dy;
+#pragma unroll(R <= kUnrollMaxR ? R : 1)
+                for (int col = 0; col < R; col++) {
+                    const float2 pl = this->img[(row * R + col) * this->ld];
+                    const float w = wr[B::wcol(col)];
+                    const float dx = (col + 0.5f) - c[1];
+                    const float qx = dx * dx;
+                    const float e = __expf(-__fmaf_rn(qx, Sx, qy * Sy));
+                    const float mu = __fmaf_rn(A128, e, B64);
+                    const float q = w * (1.0f - __fdividef(pl.x, mu));
+                    const float qe = q * e;
+                    gA += qe;
+                    gX = __fmaf_rn(qe, dx, gX);
+                    gY = __fmaf_rn(qe, dy, gY);
+                    gSx = __fmaf_rn(qe, qx, gSx);
+                    gSy = __fmaf_rn(qe, qy, gSy);
+                    gB += q;
+                }
+            }
+            g[0] = QCS_ASCALE * gA;
+            g[1] = A128 * 2.0f * Sx * gX;
+            g[2] = A128 * 2.0f * Sy * gY;
+            g[3] = -A128 * QCS_SSCALE * gSx;
+            g[4] = -A128 * QCS_SSCALE * gSy;
+            g[5] = QCS_BSCALE * gB;
+        }
+    }
+};
+
 // Fixed schedule: IT quasi-Newton iterations, each with an NB-step bisection
 // of the step length in [1e-5, 1] (the reference: 11); no convergence test.
 // D: P x P scratch at D[(r * P + c) * ld]; ev evaluates the loss and the
