@@ -1313,6 +1313,71 @@ def mixed_measure(streams, dist, world, rank):
             "shapes": shapes}
 
 
+def mixed_persistent_measure(streams, dist, world, rank):
+    """Plain fitting of the mixed 7/9/11 evaluation stream (mixed_measure's
+    records, same seeds) two ways over the same chunks: one
+    qcs_loc_localize_mixed_device call per MIXED_CALL records of each size
+    (the three sizes' single-emitter fits in one persistent launch), and the
+    same chunks as three qcs_loc_localize_device calls in a row.  Device time
+    of every call, two sets of contexts in turn; the rows of one chunk are
+    compared bit for bit."""
+    import torch
+    from qcstorm_b200 import lib, synth_torch as ST
+    n_eval = _split(MIXED_EVAL, len(MIXED_SHAPES))
+    data = []
+    for i, (kind, R, _, _) in enumerate(MIXED_SHAPES):
+        d_ev, _ = ST.rois(kind, n_eval[i], R, seed=30_000 + 100 * rank + i, device="cuda")
+        data.append((R, ST.para(kind, R), d_ev, n_eval[i]))
+    torch.cuda.synchronize()
+    ncalls = max((n + MIXED_CALL - 1) // MIXED_CALL for _, _, _, n in data)
+    ctxs = [[lib.LocContext(para, capacity=MIXED_CALL) for _, para, _, _ in data] for _ in range(2)]
+
+    def chunks(k, cs):
+        out = []
+        for j, (R, para, d, n) in enumerate(data):
+            o = (k % ncalls) * MIXED_CALL
+            m = min(MIXED_CALL, n - o)
+            if m > 0:
+                out.append((cs[j], d.data_ptr() + o * R * (R + 1) * 2, m))
+        return out
+
+    def mixed(k, s, cs=None):
+        lib.localize_mixed_device(chunks(k, cs or ctxs[k % 2]), s.cuda_stream)
+
+    def per_size(k, s, cs=None):
+        for c, ptr, m in chunks(k, cs or ctxs[k % 2]):
+            c.localize_device(ptr, m, 0, s.cuda_stream)
+
+    ms_m = device_timed(ncalls, 3, mixed, streams, dist)
+    ms_s = device_timed(ncalls, 3, per_size, streams, dist)
+    sh = streams[0].cuda_stream
+    # chunk 0 through both paths, one size at a time and all three, one stream
+    per_entry = {}
+    first = chunks(0, ctxs[0])
+    for name, sub in [("R%d" % data[j][0], [first[j]]) for j in range(len(first))] + [("all", first)]:
+        t_m = device_timed(5, 2, lambda k, s: lib.localize_mixed_device(sub, s.cuda_stream), streams[:1], dist)
+        t_s = device_timed(5, 2, lambda k, s: [c.localize_device(p, m, 0, s.cuda_stream) for c, p, m in sub],
+                           streams[:1], dist)
+        per_entry[name] = {"persistent_ms": t_m / 5, "per_size_ms": t_s / 5}
+    per_size(0, streams[0], ctxs[0])
+    base = [c.read_rows(sh)[0] for c in ctxs[0]]
+    mixed(0, streams[0], ctxs[0])
+    equal = all(np.array_equal(c.read_rows(sh)[0].view(np.uint32), b.view(np.uint32)) for c, b in zip(ctxs[0], base))
+    for cs in ctxs:
+        for c in cs:
+            c.close()
+    del data
+    torch.cuda.empty_cache()
+    return {"workload": "the mixed 7/9/11 evaluation records (GS2D 7x7, astigmatic 3D 9x9, 1-3 emitter 11x11), plain "
+                        "fitting, %d records of each size per call" % MIXED_CALL,
+            "calls": ncalls, "eval_records": MIXED_EVAL * world,
+            "persistent_fits_per_s": MIXED_EVAL * world / (ms_m * 1e-3),
+            "per_size_fits_per_s": MIXED_EVAL * world / (ms_s * 1e-3), "persistent_vs_per_size": ms_s / ms_m,
+            "rows_equal": bool(equal), "per_entry": per_entry,
+            "timing": "device time of every call, two sets of contexts in turn; per_entry: one chunk of each size "
+                      "alone and all three, one stream, 5 calls after 2 warm-ups"}
+
+
 CONSEC_FRAMES_PER_GROUP = 32
 CONSEC_GROUPS = 8
 
@@ -1612,6 +1677,8 @@ def main():
                     help="only run the conv start-point network's inference 3 times on N records (for ncu)")
     ap.add_argument("--profile-train", type=int, default=0, metavar="N",
                     help="only run one training epoch of each start-point network on N records (for ncu)")
+    ap.add_argument("--mixed-persistent", action="store_true",
+                    help="only run the plain mixed 7/9/11 measurement (persistent launch against per-size calls)")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-start measurement")
     ap.add_argument("--no-mixed", action="store_true",
                     help="skip the mixed 7/9/11 learned measurement (4e6 training, 1e7 evaluation records)")
@@ -1647,6 +1714,9 @@ def main():
         return profile_conv(args.profile_conv, stream)
     if args.profile_train:
         return profile_train(args.profile_train, stream)
+    if args.mixed_persistent:
+        print(json.dumps(mixed_persistent_measure([stream, torch.cuda.Stream()], None, 1, 0)))
+        return 0
     dist = None
     if world > 1:
         import datetime
@@ -1746,6 +1816,7 @@ def main():
                                         cpu_baseline=not args.no_cpu_baseline)
         if not args.no_mixed:
             mixed = mixed_measure(streams, dist, world, rank)
+            mixed["plain_persistent"] = mixed_persistent_measure(streams, dist, world, rank)
 
     frames = None
     if not args.no_frames:

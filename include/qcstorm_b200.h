@@ -284,6 +284,22 @@ int qcs_loc_fit_ratios(const qcs_loc_data *c, float *out7);
  */
 int qcs_loc_localize_device(qcs_loc_data *c, const uint16_t *d_rois, const float *d_wle,
                             const qcs_loc_para *p, int n, void *stream);
+/* Several device-resident calls of different ROI sizes at once (a stream
+ * of 7x7, 9x9 and 11x11 records): entry i is qcs_loc_localize_device(ctx[i],
+ * d_rois[i], d_wle[i], &p[i], n[i], stream) with the same rows, counters and
+ * 2E / 3E stages in ctx[i], but the single-emitter fits of all entries run in
+ * one persistent launch whose blocks take tiles of any size from one work
+ * list (the larger ROIs first).  count 1..QCS_MIXED_MAX, distinct contexts;
+ * LocType GS2D, AS3D or DH3D with ROISize 7, 9 or 11 (else QCS_ERR_ROISIZE);
+ * records on a 4-byte boundary and no likelihood-ratio selection on any
+ * context (else QCS_ERR_ARG).  d_wle[i] may be NULL (the WLE pre-pass runs
+ * into ctx[i]); the stream NULL means ctx[0]'s.  No counterpart in the
+ * reference, which launches one kernel per ROI size and fit stage
+ * (bfgsMLE_Single_Emitter_Fit.cu:40-67). */
+#define QCS_MIXED_MAX 6
+int qcs_loc_localize_mixed_device(qcs_loc_data *const *ctx, const uint16_t *const *d_rois,
+                                  const float *const *d_wle, const qcs_loc_para *p, const int *n, int count,
+                                  void *stream);
 /* The same with the record count read on the device: *d_n (clamped to
  * [0, max_n], max_n <= capacity), e.g. qcs_extract_device_roi_num, so that
  * frames -> extraction -> localization runs with no host round trip.  d_wle is

@@ -347,6 +347,58 @@ int qcs_loc_localize_device(qcs_loc_data *c, const uint16_t *d_rois, const float
     return QCS_OK;
 }
 
+int qcs_loc_localize_mixed_device(qcs_loc_data *const *ctx, const uint16_t *const *d_rois,
+                                  const float *const *d_wle, const qcs_loc_para *p, const int *n, int count,
+                                  void *stream) {
+    static_assert(QCS_MIXED_MAX == qcs::kMixedMax, "mixed-size entries");
+    if (!ctx || !d_rois || !d_wle || !p || !n) return fail(QCS_ERR_ARG, "null argument");
+    if (count < 1 || count > QCS_MIXED_MAX) return fail(QCS_ERR_ARG, "entry count outside 1..QCS_MIXED_MAX");
+    int kind[QCS_MIXED_MAX], R[QCS_MIXED_MAX];
+    for (int i = 0; i < count; ++i) {
+        int st = check_call(ctx[i], &p[i], n[i]);
+        if (st) return st;
+        for (int j = 0; j < i; ++j)
+            if (ctx[j] == ctx[i]) return fail(QCS_ERR_ARG, "a context appears twice");
+        if (use_lr(ctx[i], &p[i])) return fail(QCS_ERR_ARG, "likelihood-ratio selection runs per call");
+        if (p[i].LocType != QCS_LOCTYPE_GS2D && p[i].LocType != QCS_LOCTYPE_AS3D && p[i].LocType != QCS_LOCTYPE_DH3D)
+            return fail(QCS_ERR_ROISIZE, "fit kind outside GS2D / AS3D / DH3D");
+        kind[i] = p[i].LocType == QCS_LOCTYPE_AS3D ? qcs::kAS3D : qcs::kGS2D;
+        R[i] = p[i].ROISize;
+        if (!qcs::mixed_fit_supported(kind[i], R[i])) return fail(QCS_ERR_ROISIZE, "ROI size outside 7, 9, 11");
+        if (n[i] > 0 && !d_rois[i]) return fail(QCS_ERR_ARG, "null ROI pointer");
+        if ((reinterpret_cast<uintptr_t>(d_rois[i]) & 3) != 0)
+            return fail(QCS_ERR_ARG, "records must start on a 4-byte boundary");
+    }
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx[0]->stream;
+    qcs::CascadeArgs a[QCS_MIXED_MAX];
+    qcs::FitLaunch f[QCS_MIXED_MAX];
+    for (int i = 0; i < count; ++i) {
+        qcs_loc_data *c = ctx[i];
+        const float *wle = d_wle[i];
+        if (!wle && n[i] > 0) {
+            QCS_CUDA(qcs::launch_wle_ctx(c->wle_sorter, d_rois[i], n[i], c->R, p[i].LocType, c->d_wle, s),
+                     "WLE pre-pass");
+            wle = c->d_wle;
+        }
+        c->lr_stats = 0;
+        a[i].para = p[i];
+        a[i].rois = d_rois[i];
+        a[i].wle = wle;
+        a[i].n = n[i];
+        a[i].loc = c->d_loc;
+        a[i].max_rows = c->max_rows;
+        a[i].stream = s;
+        a[i].group_limit2 = c->tune_limit2;
+        a[i].group_limit3 = c->tune_limit3;
+        QCS_CUDA(qcs::cascade_classify(a[i], c->st), "queues");
+        f[i] = qcs::cascade_single_launch(a[i], c->st);
+    }
+    QCS_CUDA(qcs::launch_fit_mixed(f, kind, R, count, ctx[0]->st.counters + qcs::kCntMixedNext, s),
+             "mixed-size single-emitter fit");
+    for (int i = 0; i < count; ++i) QCS_CUDA(qcs::cascade_tail(a[i], ctx[i]->st), "localization cascade");
+    return QCS_OK;
+}
+
 int qcs_loc_localize_device_n(qcs_loc_data *c, const uint16_t *d_rois, const float *d_wle, const qcs_loc_para *p,
                               const int *d_n, int max_n, void *stream) {
     int st = check_call(c, p, max_n);

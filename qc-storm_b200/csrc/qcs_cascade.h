@@ -24,6 +24,7 @@ enum {
     kCntSel2 = 11,       //   ... the two-emitter model
     kCntSel3 = 12,       //   ... the three-emitter model
     kCntRefit3E = 13,    // learned path: three-emitter fits redone by the plain three-emitter fit
+    kCntMixedNext = 14,  // mixed-size call (first context): the persistent launch's next tile
     kCntNum = 16
 };
 

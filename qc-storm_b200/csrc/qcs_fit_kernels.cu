@@ -18,6 +18,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 #include <type_traits>
+#include <utility>
 
 #include "qcs_device.cuh"
 #include "qcs_fit_math.cuh"
@@ -320,25 +321,27 @@ __device__ __forceinline__ void single_finish(const float *Ininf, const CorePara
 // log) pairs, [pixel][slot], and the mask's unique values, [chunk][slot]
 // (MaskShape); the BFGS inverse Hessian lives in registers.  Blocks per SM:
 // as many as the shared memory holds (228 KB per SM, 1 KB reserved per
-// block), at most 7 (at 7 the register budget is 146 per thread).
-template <int R, bool FULL>
+// block), at most 7 (at 7 the register budget is 146 per thread).  S slots
+// per block: kTPB, or fewer in the mixed-size kernel (an even count, so the
+// mask starts on a 16-byte boundary).
+template <int R, bool FULL, int S = kTPB>
 struct SingleLayout {
     enum {
         PIX = R * R,
         IMG = 0,                  // float2 per pixel and slot
-        WU = 2 * PIX * kTPB,      // floats; a multiple of 4 (16-byte aligned)
-        TOTAL = WU + MaskShape<R, FULL>::FLOATS * kTPB,
+        WU = 2 * PIX * S,         // floats; a multiple of 4 (16-byte aligned)
+        TOTAL = WU + MaskShape<R, FULL>::FLOATS * S,
         BYTES = TOTAL * 4,
         FIT = (228 * 1024) / (BYTES + 1024),
         BLOCKS = FIT < 1 ? 1 : (FIT > 7 ? 7 : FIT),
     };
 };
 
-// Stage a block's records: pixel k of slot s at s_img[k * kTPB + s] as
+// Stage a block's records: pixel k of slot s at s_img[k * S + s] as
 // (max((adu - offset) * gain, 1), its __logf).  WORDS: the records are
 // 4-byte aligned and read two pixels per load; element (word, slot) is taken
 // slot-fastest so a warp's shared-memory stores fall in distinct banks.
-template <int R, bool WORDS>
+template <int R, bool WORDS, int S = kTPB>
 __device__ __forceinline__ void stage_single(float2 *s_img, const uint16_t *rois, const Queue &q, int base, int cnt,
                                              float Offset, float KAdc) {
     enum { PIX = R * R, WHOLE = R * (R + 1), WPR = (PIX + 1) / 2 };
@@ -350,10 +353,10 @@ __device__ __forceinline__ void stage_single(float2 *s_img, const uint16_t *rois
             const uint32_t u = __ldg(reinterpret_cast<const uint32_t *>(rois + (size_t)id * WHOLE) + wd);
             const int k = 2 * wd;
             const float v0 = fmaxf(((float)(u & 0xFFFFu) - Offset) * KAdc, 1.0f);
-            s_img[k * kTPB + slot] = make_float2(v0, __logf(v0));
+            s_img[k * S + slot] = make_float2(v0, __logf(v0));
             if (k + 1 < PIX) {
                 const float v1 = fmaxf(((float)(u >> 16) - Offset) * KAdc, 1.0f);
-                s_img[(k + 1) * kTPB + slot] = make_float2(v1, __logf(v1));
+                s_img[(k + 1) * S + slot] = make_float2(v1, __logf(v1));
             }
         }
     } else {
@@ -363,32 +366,32 @@ __device__ __forceinline__ void stage_single(float2 *s_img, const uint16_t *rois
             const int id = queue_at(q, base + slot);
             const uint16_t u = __ldg(rois + (size_t)id * WHOLE + k);
             const float pixval = fmaxf((u - Offset) * KAdc, 1.0f);
-            s_img[k * kTPB + slot] = make_float2(pixval, __logf(pixval));
+            s_img[k * S + slot] = make_float2(pixval, __logf(pixval));
         }
     }
 }
 
-template <int R, int KIND, bool WORDS, int DIST = ArithSpec<KIND, R>::DIST, int MASK = ArithSpec<KIND, R>::MASK,
-          bool FULL = MASK == kCompiler>
-__global__ void __launch_bounds__(kTPB, (SingleLayout<R, FULL>::BLOCKS)) fit_single_kernel(
-    const uint16_t *__restrict__ rois, const float *__restrict__ wle, Queue q, float *__restrict__ loc,
-    uint8_t *__restrict__ to2e, CorePara c, double *__restrict__ ll) {
-    typedef SingleLayout<R, FULL> L;
+// One block's tile of the single-emitter fit: queue entries base .. base+S-1
+// (those below n), one thread per ROI, S slots of SingleLayout<R, FULL, S>
+// in smem.  Every thread of the block calls it (it synchronises the block
+// once, after staging).
+template <int R, int KIND, bool WORDS, int DIST, int MASK, bool FULL, int S>
+__device__ __forceinline__ void single_tile(float *smem, int base, int n, const uint16_t *__restrict__ rois,
+                                            const float *__restrict__ wle, const Queue &q, float *__restrict__ loc,
+                                            uint8_t *__restrict__ to2e, const CorePara &c, double *__restrict__ ll) {
+    typedef SingleLayout<R, FULL, S> L;
     enum { P = KindTraits<KIND>::P, PIX = R * R, WHOLE = R * (R + 1) };
-    extern __shared__ __align__(16) float smem[];
-    const int n = queue_len(q);
-    const int base = blockIdx.x * kTPB;
     if (base >= n) return;
-    const int cnt = min(kTPB, n - base);
+    const int cnt = min(S, n - base);
     float2 *s_img = reinterpret_cast<float2 *>(smem + L::IMG);
-    stage_single<R, WORDS>(s_img, rois, q, base, cnt, c.Offset, c.KAdc);
+    stage_single<R, WORDS, S>(s_img, rois, q, base, cnt, c.Offset, c.KAdc);
     __syncthreads();
     const int tid = threadIdx.x;
     if (tid >= cnt) return;
 
     const int CurFluoID = queue_at(q, base + tid);
-    const PixView img{s_img + tid, kTPB};
-    // the mask: FULL, pixel k at mask[k * kTPB]; else float4 chunk j at ((float4 *)mask)[j * kTPB]
+    const PixView img{s_img + tid, S};
+    // the mask: FULL, pixel k at mask[k * S]; else float4 chunk j at ((float4 *)mask)[j * S]
     float *mask = smem + L::WU + (FULL ? tid : 4 * tid);
     const uint16_t *hdr = rois + (size_t)CurFluoID * WHOLE + PIX;
     const int XOffset = hdr[0];
@@ -399,13 +402,13 @@ __global__ void __launch_bounds__(kTPB, (SingleLayout<R, FULL>::BLOCKS)) fit_sin
     float Ininf[P];
     const SinglePrep sp = single_prefit<R, KIND>(img, pw, c, Ininf);
     if constexpr (FULL)
-        wle_weights<R, MASK>(mask, kTPB, sp.WLE_SigmaX, sp.WLE_SigmaY, sp.MoleculeType);
+        wle_weights<R, MASK>(mask, S, sp.WLE_SigmaX, sp.WLE_SigmaY, sp.MoleculeType);
     else
-        wle_weights_unique<R, MASK>(reinterpret_cast<float4 *>(mask), kTPB, sp.WLE_SigmaX, sp.WLE_SigmaY,
+        wle_weights_unique<R, MASK>(reinterpret_cast<float4 *>(mask), S, sp.WLE_SigmaX, sp.WLE_SigmaY,
                                     sp.MoleculeType);
     float D[P * P];  // the inverse Hessian, in registers
-    bfgs_fit<P, KindTraits<KIND>::IT>(StagedEval<R, KIND, DIST, FULL>{s_img + tid, mask, kTPB}, Ininf, D, 1);
-    if (ll) ll[CurFluoID] = model_loglik<R, KIND, DIST, kCompiler>(s_img + tid, kTPB, Ininf, 0, 1);
+    bfgs_fit<P, KindTraits<KIND>::IT>(StagedEval<R, KIND, DIST, FULL>{s_img + tid, mask, S}, Ininf, D, 1);
+    if (ll) ll[CurFluoID] = model_loglik<R, KIND, DIST, kCompiler>(s_img + tid, S, Ininf, 0, 1);
     float row[12];
     bool accepted;
     float CurSNR;
@@ -417,6 +420,107 @@ __global__ void __launch_bounds__(kTPB, (SingleLayout<R, FULL>::BLOCKS)) fit_sin
     else
         zero_row(loc, CurFluoID);
     if (to2e) to2e[CurFluoID] = (!accepted && c.MultiEmitterFitEn && IsFittingValid && (CurSNR > 6.0f)) ? 1 : 0;
+}
+
+template <int R, int KIND, bool WORDS, int DIST = ArithSpec<KIND, R>::DIST, int MASK = ArithSpec<KIND, R>::MASK,
+          bool FULL = MASK == kCompiler>
+__global__ void __launch_bounds__(kTPB, (SingleLayout<R, FULL>::BLOCKS)) fit_single_kernel(
+    const uint16_t *__restrict__ rois, const float *__restrict__ wle, Queue q, float *__restrict__ loc,
+    uint8_t *__restrict__ to2e, CorePara c, double *__restrict__ ll) {
+    extern __shared__ __align__(16) float smem[];
+    single_tile<R, KIND, WORDS, DIST, MASK, FULL, kTPB>(smem, blockIdx.x * kTPB, queue_len(q), rois, wle, q, loc,
+                                                         to2e, c, ll);
+}
+
+// ------------------------------------------------ mixed-size single fits ---
+// One persistent launch fits the single-emitter queues of several calls of
+// different ROI sizes (GS2D / AS3D 7x7, 9x9, 11x11): each block takes the
+// next tile of the shared work list with an atomic counter and fits it with
+// that size's single_tile, so no block waits on another and the last tiles of
+// every size spread over all SMs.  Every block has the same shared memory
+// (kMixedBlocks blocks per SM); a tile holds 64 ROIs, else 32 where those fit
+// (so no warp runs partly filled), else an even count, one thread each.  The
+// tiles of the larger ROIs come first in the list, so the longest fits start
+// first.  The arithmetic is fit_single_kernel's: the rows are the per-size
+// launches' rows bit for bit.  One launch has one register count: 6 blocks
+// per SM allow 168 registers a thread, which the 7x7 (128) and GS2D 9x9 (168)
+// fits need, while the per-size GS2D 11x11 and AS3D 9x9 / 11x11 kernels use
+// 180 to 254; those fits run slower here than in their own launches.
+constexpr int kMixedBlocks = 6;
+// floats of dynamic shared memory per block: 228 KB per SM less 1 KB reserved and the kernel's static
+// shared memory per block, in 16-byte units
+constexpr int kMixedBudget = ((228 * 1024 / kMixedBlocks - 1024 - 64) / 4) & ~3;
+
+template <int R, int KIND>
+struct MixedShape {
+    enum {
+        MASK = ArithSpec<KIND, R>::MASK,
+        FULL = MASK == kCompiler,
+        PER = 2 * R * R + MaskShape<R, (bool)FULL>::FLOATS,  // floats per ROI
+        FIT = kMixedBudget / PER,
+        S = FIT >= kTPB ? kTPB : (FIT >= 32 ? 32 : FIT & ~1),
+    };
+    static_assert(S >= 2, "a mixed-size tile holds at least two ROIs");
+};
+
+__host__ __device__ constexpr int mixed_code(int kind, int R) { return kind * 32 + R; }
+
+struct MixedSeg {
+    const uint16_t *rois;
+    const float *wle;
+    Queue q;
+    float *loc;
+    uint8_t *to2e;
+    CorePara c;
+    int code;   // mixed_code(kind, R)
+    int slots;  // ROIs per tile
+};
+
+struct MixedArgs {
+    MixedSeg seg[kMixedMax];
+    int count;
+    int *next;  // zero at launch: the next tile to take
+};
+
+template <int R, int KIND>
+__device__ __forceinline__ void mixed_tile(float *smem, int base, int n, const MixedSeg &g) {
+    typedef MixedShape<R, KIND> M;
+    single_tile<R, KIND, true, ArithSpec<KIND, R>::DIST, M::MASK, (bool)M::FULL, M::S>(smem, base, n, g.rois, g.wle,
+                                                                                     g.q, g.loc, g.to2e, g.c, nullptr);
+}
+
+__global__ void __launch_bounds__(kTPB, kMixedBlocks) fit_mixed_kernel(const __grid_constant__ MixedArgs a) {
+    extern __shared__ __align__(16) float smem[];
+    __shared__ int s_len[kMixedMax], s_end[kMixedMax], s_tile;
+    if (threadIdx.x == 0) {
+        int end = 0;
+        for (int i = 0; i < a.count; ++i) {
+            const int n = queue_len(a.seg[i].q);
+            s_len[i] = n;
+            end += (n + a.seg[i].slots - 1) / a.seg[i].slots;
+            s_end[i] = end;
+        }
+    }
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = atomicAdd(a.next, 1);
+        __syncthreads();
+        int t = s_tile;
+        if (t >= s_end[a.count - 1]) return;  // the same for every thread of the block
+        int i = 0;
+        while (t >= s_end[i]) ++i;
+        if (i > 0) t -= s_end[i - 1];
+        const MixedSeg &g = a.seg[i];
+        const int base = t * g.slots, n = s_len[i];
+        switch (g.code) {
+        case mixed_code(kGS2D, 7): mixed_tile<7, kGS2D>(smem, base, n, g); break;
+        case mixed_code(kGS2D, 9): mixed_tile<9, kGS2D>(smem, base, n, g); break;
+        case mixed_code(kGS2D, 11): mixed_tile<11, kGS2D>(smem, base, n, g); break;
+        case mixed_code(kAS3D, 7): mixed_tile<7, kAS3D>(smem, base, n, g); break;
+        case mixed_code(kAS3D, 9): mixed_tile<9, kAS3D>(smem, base, n, g); break;
+        case mixed_code(kAS3D, 11): mixed_tile<11, kAS3D>(smem, base, n, g); break;
+        }
+        __syncthreads();  // the tile's shared memory and s_tile are free again
+    }
 }
 
 // The same fit with G lanes per ROI (GroupEval): bit for bit the rows of
@@ -1557,6 +1661,63 @@ cudaError_t launch_fit_group(int kind, int R, int lanes, const FitLaunch &a) {
     case 13: return launch_single_group<13, kGS2D, 8>(a);
     }
     return cudaErrorInvalidValue;
+}
+
+bool mixed_fit_supported(int kind, int R) { return (kind == kGS2D || kind == kAS3D) && (R == 7 || R == 9 || R == 11); }
+
+namespace {
+int mixed_slots(int kind, int R) {
+    switch (mixed_code(kind, R)) {
+    case mixed_code(kGS2D, 7): return MixedShape<7, kGS2D>::S;
+    case mixed_code(kGS2D, 9): return MixedShape<9, kGS2D>::S;
+    case mixed_code(kGS2D, 11): return MixedShape<11, kGS2D>::S;
+    case mixed_code(kAS3D, 7): return MixedShape<7, kAS3D>::S;
+    case mixed_code(kAS3D, 9): return MixedShape<9, kAS3D>::S;
+    case mixed_code(kAS3D, 11): return MixedShape<11, kAS3D>::S;
+    }
+    return 0;
+}
+}  // namespace
+
+cudaError_t launch_fit_mixed(const FitLaunch *f, const int *kind, const int *R, int count, int *d_next,
+                             cudaStream_t s) {
+    if (count < 1 || count > kMixedMax || !d_next) return cudaErrorInvalidValue;
+    MixedArgs a{};
+    a.count = count;
+    a.next = d_next;
+    // larger ROIs first (their fits take longest); ties keep the caller's order
+    int order[kMixedMax];
+    for (int i = 0; i < count; ++i) order[i] = i;
+    for (int i = 1; i < count; ++i)
+        for (int j = i; j > 0 && R[order[j]] > R[order[j - 1]]; --j) std::swap(order[j], order[j - 1]);
+    long long tiles = 0;
+    for (int k = 0; k < count; ++k) {
+        const int i = order[k];
+        if (!mixed_fit_supported(kind[i], R[i]) || f[i].ll || (reinterpret_cast<uintptr_t>(f[i].rois) & 3) != 0)
+            return cudaErrorInvalidValue;
+        MixedSeg &g = a.seg[k];
+        g.rois = f[i].rois;
+        g.wle = f[i].wle;
+        g.q = f[i].q;
+        g.loc = f[i].loc;
+        g.to2e = f[i].to2e;
+        g.c = f[i].para;
+        g.code = mixed_code(kind[i], R[i]);
+        g.slots = mixed_slots(kind[i], R[i]);
+        tiles += (f[i].max_count + g.slots - 1) / g.slots;
+    }
+    cudaError_t e = cudaMemsetAsync(d_next, 0, sizeof(int), s);
+    if (e != cudaSuccess || tiles == 0) return e;
+    const size_t smem = kMixedBudget * sizeof(float);
+    int dev = 0, sms = 0, per_sm = 0;
+    if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fit_mixed_kernel, kTPB, smem)) != cudaSuccess)
+        return e;
+    const long long resident = (long long)sms * (per_sm > 0 ? per_sm : 1);
+    const int grid = (int)(tiles < resident ? tiles : resident);
+    fit_mixed_kernel<<<grid, kTPB, smem, s>>>(a);
+    return cudaGetLastError();
 }
 
 // ROI sizes: odd 5..17 for single emitter, 5..13 for multi emitter (the

@@ -50,6 +50,16 @@ int multi_group_default_limit(int kind, int R);
 bool group_fit_supported(int kind, int R);
 cudaError_t launch_fit_group(int kind, int R, int lanes, const FitLaunch &a);
 
+// Single-emitter fits (GS2D / AS3D, ROI sizes 7, 9, 11; the fit kinds of
+// launch_fit) of up to kMixedMax launches of different ROI sizes in one
+// persistent launch: rows and 2E flags of each launch_fit(kind[i], R[i],
+// f[i]) bit for bit.  Records must start on a 4-byte boundary; ll unused.
+// d_next: one device int of scratch (set to zero on the stream first).
+constexpr int kMixedMax = 6;
+bool mixed_fit_supported(int kind, int R);
+cudaError_t launch_fit_mixed(const FitLaunch *f, const int *kind, const int *R, int count, int *d_next,
+                             cudaStream_t s);
+
 // Single-emitter fit (kind kGS2D or kAS3D; R = 7, 9, 11) of the records of
 // a.q (grid from a.max_count) started from start[P * id] (GS2D P = 5: peak
 // e-, x, y, sigma, background e-; AS3D P = 6: peak e-, x, y, sigma_x,

@@ -31,6 +31,8 @@ _SIGS = {
                                           C.c_void_p]),
     "qcs_loc_localize_device_n": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(LocPara), C.c_void_p,
                                             C.c_int, C.c_void_p]),
+    "qcs_loc_localize_mixed_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                                C.c_void_p]),
     "qcs_loc_device_rows": (C.c_void_p, [C.c_void_p]),
     "qcs_loc_device_valid_num": (C.c_void_p, [C.c_void_p]),
     "qcs_loc_device_roi_buffer": (C.c_void_p, [C.c_void_p]),
@@ -210,6 +212,21 @@ def check(code):
 def _host(a, dtype):
     a = np.ascontiguousarray(a, dtype=dtype)
     return a, C.c_void_p(a.ctypes.data)
+
+
+def localize_mixed_device(entries, stream=0):
+    """qcs_loc_localize_mixed_device: entries = [(LocContext, d_rois, n, d_wle or 0, para or None), ...] of
+    different ROI sizes; their single-emitter fits run in one persistent launch, rows stay in each context."""
+    lib = load()
+    k = len(entries)
+    ctx = (C.c_void_p * k)(*[e[0].h for e in entries])
+    rois = (C.c_void_p * k)(*[e[1] for e in entries])
+    wle = (C.c_void_p * k)(*[(e[3] if len(e) > 3 and e[3] else None) for e in entries])
+    para = (LocPara * k)(*[(e[4] if len(e) > 4 and e[4] is not None else e[0].para) for e in entries])
+    n = (C.c_int * k)(*[int(e[2]) for e in entries])
+    check(lib.qcs_loc_localize_mixed_device(C.cast(ctx, C.c_void_p), C.cast(rois, C.c_void_p), C.cast(wle, C.c_void_p),
+                                            C.cast(para, C.c_void_p), C.cast(n, C.c_void_p), k,
+                                            C.c_void_p(stream) if stream else None))
 
 
 class LocContext:
