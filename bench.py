@@ -1516,6 +1516,33 @@ def profile_learned(n, stream):
     return 0
 
 
+def profile_mixed(n, stream):
+    """One mixed-size call (qcs_loc_localize_mixed_device) over n records of
+    each size of the mixed 7/9/11 workload, then the same records as three
+    per-size calls, twice, inside the NVTX range "mixed" (for ncu)."""
+    import torch
+    from qcstorm_b200 import lib, synth_torch as ST
+    data = []
+    for i, (kind, R_, _, _) in enumerate(MIXED_SHAPES):
+        d, _ = ST.rois(kind, n, R_, seed=30_000 + i, device="cuda")
+        data.append((ST.para(kind, R_), d))
+    ctxs = [lib.LocContext(p, capacity=n) for p, _ in data]
+    ents = [(c, d.data_ptr(), n) for c, (_, d) in zip(ctxs, data)]
+    sh = stream.cuda_stream
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("mixed")
+    for _ in range(2):
+        lib.localize_mixed_device(ents, sh)
+        for c, ptr, m in ents:
+            c.localize_device(ptr, m, 0, sh)
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    print(json.dumps({"profile_mixed": n}))
+    for c in ctxs:
+        c.close()
+    return 0
+
+
 def profile_conv(n, stream):
     """The convolutional start-point network's inference (conv_tc_kernel +
     fc_tc_kernel) three times over n GS2D 7x7 records, untrained weights
@@ -1677,6 +1704,9 @@ def main():
                     help="only run the conv start-point network's inference 3 times on N records (for ncu)")
     ap.add_argument("--profile-train", type=int, default=0, metavar="N",
                     help="only run one training epoch of each start-point network on N records (for ncu)")
+    ap.add_argument("--profile-mixed", type=int, default=0, metavar="N",
+                    help="one mixed-size call and the same records as per-size calls, twice, N records per size "
+                         "(for ncu)")
     ap.add_argument("--mixed-persistent", action="store_true",
                     help="only run the plain mixed 7/9/11 measurement (persistent launch against per-size calls)")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-start measurement")
@@ -1714,6 +1744,8 @@ def main():
         return profile_conv(args.profile_conv, stream)
     if args.profile_train:
         return profile_train(args.profile_train, stream)
+    if args.profile_mixed:
+        return profile_mixed(args.profile_mixed, stream)
     if args.mixed_persistent:
         print(json.dumps(mixed_persistent_measure([stream, torch.cuda.Stream()], None, 1, 0)))
         return 0
