@@ -12,11 +12,12 @@ U(1.0,1.6) px, photons log-U[500,5000], background U(20,100) e-/px, Poisson),
 frames -> extraction -> multi-emitter localization -> CRLB) in frames/s.
 
 Printed JSON line (rank 0): `value` is device-timed fits/s with records
-resident in HBM, two localization contexts used in turn on two streams (one
-call's latency-bound tail overlaps the next call's kernels; `value_one_stream`
-is one context on one stream); `e2e` is the same metric through the
-asynchronous host-buffer calls (qcs_loc_localize_async + qcs_loc_finish on two
-contexts in turn: pinned host records in, rows and counters out, every copy
+resident in HBM, three localization contexts used in turn on three streams
+(one call's latency-bound tail overlaps the next calls' kernels;
+`value_one_stream` is one context on one stream); `e2e` is the same metric
+through the asynchronous host-buffer calls (qcs_loc_localize_async +
+qcs_loc_finish on three contexts in turn, so one call stays queued while the
+host reads another's rows: pinned host records in, rows and counters out, every copy
 inside the timed region; `e2e.sync_value`: the synchronous
 qcs_loc_bfgs_mle_localization, one call at a time); `roofline` is the fit kernel against the measured
 special-function-unit rate (the loss is exp/log bound, not HBM or tensor
@@ -613,27 +614,32 @@ def train_learned_net(para, stream, seed=4242, arch="mlp", lr=2e-3):
 
 
 E2E_STEPS = 40  # end-to-end steps (each ~1 ms)
+# calls in flight in the main measurements (value, e2e, learned): with two, call k+2 is enqueued only after call k's
+# rows are read, and the GPU idles on the host between calls; a third keeps one call queued
+IN_FLIGHT = 3
 
 
 def e2e_pipelined(ctxs, streams, h_batches, steps, net=None):
     """`steps` calls of the asynchronous host-buffer localization
-    (qcs_loc_localize_async, or qcs_learned_localize_async with net) over two
-    contexts used in turn on their own streams: call k's record copy and row
-    copy overlap call k-1's kernels.  Every call copies its pinned records in
-    and its rows and counters out; qcs_loc_finish waits for it.  Returns
-    (seconds, rows read)."""
+    (qcs_loc_localize_async, or qcs_learned_localize_async with net) over the
+    contexts used in turn, each on its stream: call k's record copy and row
+    copy overlap the kernels of the calls before it, and up to len(ctxs) calls
+    are in flight.  Every call copies its pinned records in and its rows and
+    counters out; qcs_loc_finish waits for it.  Returns (seconds, rows read)."""
     import torch
+    depth = len(ctxs)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     rows = 0
     for k in range(steps):
-        c = ctxs[k % 2]
-        if k >= 2:
+        c = ctxs[k % depth]
+        if k >= depth:
             rows += c.finish(copy=False)[0].shape[0]
-        c.localize_async(h_batches[k % len(h_batches)].data_ptr(), N_PER_STEP, stream=streams[k % 2].cuda_stream,
-                         net=net, iters=LEARNED_ITERS, bisections=LEARNED_BISECTIONS)
-    for k in range(max(0, steps - 2), steps):
-        rows += ctxs[k % 2].finish(copy=False)[0].shape[0]
+        c.localize_async(h_batches[k % len(h_batches)].data_ptr(), N_PER_STEP,
+                         stream=streams[k % len(streams)].cuda_stream, net=net, iters=LEARNED_ITERS,
+                         bisections=LEARNED_BISECTIONS)
+    for k in range(max(0, steps - depth), steps):
+        rows += ctxs[k % depth].finish(copy=False)[0].shape[0]
     return time.perf_counter() - t0, rows
 
 
@@ -661,7 +667,7 @@ def learned_measure(args, streams, ctxs, para, d_batches, h_batches, rec0, truth
     tuned_schedule = net.autotune(ctx, d_batches[0].data_ptr(), N_PER_STEP, stream=sh)
 
     def step(k, s, c=None):
-        net.localize(c or ctxs[k % 2], d_batches[k % BATCHES].data_ptr(), N_PER_STEP, 0, iters=LEARNED_ITERS,
+        net.localize(c or ctxs[k % len(ctxs)], d_batches[k % BATCHES].data_ptr(), N_PER_STEP, 0, iters=LEARNED_ITERS,
                      bisections=LEARNED_BISECTIONS, stream=s.cuda_stream)
 
     ms, windows = device_timed_windows(args.steps, args.warmup, step, streams, dist)
@@ -734,7 +740,7 @@ def learned_measure(args, streams, ctxs, para, d_batches, h_batches, rec0, truth
     return {
         "value": value, "unit": UNIT, "ms_per_step": ms / args.steps, "vs_plain": value / plain_value,
         "windows": windows,
-        "value_one_stream": value1, "timing": "two contexts in turn on two streams (value_one_stream: one)",
+        "value_one_stream": value1, "timing": "three contexts in turn on three streams (value_one_stream: one)",
         "iters": LEARNED_ITERS, "bisections": LEARNED_BISECTIONS, "refits_per_step": refits,
         "autotuned_schedule": {"iters": tuned_schedule[0], "bisections": tuned_schedule[1],
                                "rule": "qcs_learned_autotune: fastest schedule with acceptance within 0.5 points of "
@@ -744,7 +750,7 @@ def learned_measure(args, streams, ctxs, para, d_batches, h_batches, rec0, truth
         "e2e": {"value": e2e_steps * N_PER_STEP * world / e2e_s, "unit": UNIT,
                 "h2d_bytes_per_step": N_PER_STEP * R * (R + 1) * 2,
                 "d2h_bytes_per_step": N_PER_STEP * 48 + 32,
-                "call": "qcs_learned_localize_async + qcs_loc_finish on two contexts in turn (pinned records in, "
+                "call": "qcs_learned_localize_async + qcs_loc_finish on three contexts in turn (pinned records in, "
                         "rows and counters out every step)"},
         "accuracy": {"records": N_PER_STEP, "compared": int(both.sum()),
                      "rmse_px": {"plain": rp, "learned": rl}, "photon_rel_rmse": {"plain": pp, "learned": pl},
@@ -792,7 +798,7 @@ def conv_arm(args, streams, ctxs, para, d_batches, rec0, truth0, plain_value, ml
     net, train = train_learned_net(para, stream, arch="conv", lr=1e-3)
 
     def step(k, s, c=None):
-        net.localize(c or ctxs[k % 2], d_batches[k % BATCHES].data_ptr(), N_PER_STEP, 0, iters=LEARNED_ITERS,
+        net.localize(c or ctxs[k % len(ctxs)], d_batches[k % BATCHES].data_ptr(), N_PER_STEP, 0, iters=LEARNED_ITERS,
                      bisections=LEARNED_BISECTIONS, stream=s.cuda_stream)
 
     steps = min(args.steps, 200)
@@ -1767,22 +1773,24 @@ def main():
         h_batches.append(h)
         d_batches.append(h.cuda())
     ctx = lib.LocContext(para, capacity=N_PER_STEP)
-    ctxs = [ctx, lib.LocContext(para, capacity=N_PER_STEP)]
+    # IN_FLIGHT contexts in turn, each call on its own stream (the other measurements: two)
+    ctxs = [ctx] + [lib.LocContext(para, capacity=N_PER_STEP) for _ in range(IN_FLIGHT - 1)]
     streams = [stream, torch.cuda.Stream()]
+    streams_main = streams + [torch.cuda.Stream() for _ in range(IN_FLIGHT - 2)]
     sh = stream.cuda_stream
 
     def step(k, s, c=None):
-        (c or ctxs[k % 2]).localize_device(d_batches[k % BATCHES].data_ptr(), N_PER_STEP, 0, s.cuda_stream)
+        (c or ctxs[k % IN_FLIGHT]).localize_device(d_batches[k % BATCHES].data_ptr(), N_PER_STEP, 0, s.cuda_stream)
 
     # psf_width, nn_keys_flag, the sort's condition kernel (the sort itself only for out-of-order records),
     # nn_scan_select, classify, init_counters, fit, finish, crlb
     launches_per_step = 9
 
-    # ---- device-timed steps: two contexts in turn on two streams
+    # ---- device-timed steps: IN_FLIGHT contexts in turn on their streams
     sampler, spath = start_clock_sampler(local)
     time.sleep(0.5)  # first nvidia-smi sample lands before the timed region
     t_start = time.time()
-    ms, windows = device_timed_windows(args.steps, args.warmup, step, streams, dist)
+    ms, windows = device_timed_windows(args.steps, args.warmup, step, streams_main, dist)
     t_end = time.time()
     clocks = stop_clock_sampler(sampler, spath, t_start, t_end)
     value = job_rate(args.steps, N_PER_STEP, world, ms)
@@ -1814,9 +1822,9 @@ def main():
     achieved = N_PER_STEP * PX_EVALS_PER_FIT * MUFU_PER_PX_EVAL / (fit_ms * 1e-3)
 
     # ---- end to end through the host-buffer calls (pinned records in, rows out every step)
-    e2e_pipelined(ctxs, streams, h_batches, 4)
+    e2e_pipelined(ctxs, streams_main, h_batches, 4)
     e2e_steps = E2E_STEPS
-    e2e_s, rows = e2e_pipelined(ctxs, streams, h_batches, e2e_steps)
+    e2e_s, rows = e2e_pipelined(ctxs, streams_main, h_batches, e2e_steps)
     e2e_s = max_over_ranks(e2e_s * 1e3, dist) * 1e-3
     # the synchronous reference-shaped call, one at a time
     sync_steps = 10
@@ -1830,14 +1838,15 @@ def main():
     e2e = {"value": e2e_steps * N_PER_STEP * world / e2e_s, "unit": UNIT,
            "h2d_bytes_per_step": N_PER_STEP * R * (R + 1) * 2,
            "d2h_bytes_per_step": int(rows / e2e_steps) * 48 + 32,
-           "call": "qcs_loc_localize_async + qcs_loc_finish on two contexts in turn (pinned host records in, rows "
+           "call": "qcs_loc_localize_async + qcs_loc_finish on three contexts in turn (pinned host records in, rows "
                    "and counters out every step, WLE on device)",
            "sync_value": sync_steps * N_PER_STEP * world / sync_s,
            "sync_call": "qcs_loc_bfgs_mle_localization, one call at a time"}
 
     learned = None
     if not args.no_learned:
-        learned = learned_measure(args, streams, ctxs, para, d_batches, h_batches, rec0, truth0, value, world, dist)
+        learned = learned_measure(args, streams_main, ctxs, para, d_batches, h_batches, rec0, truth0, value, world,
+                                  dist)
 
     consec = consec_measure(stream, dist, world)
     tune = autotune_measure(stream, dist, world)
@@ -1884,7 +1893,7 @@ def main():
             "windows": windows, "window_note": "value = median over %d device-timed windows of exactly %d steps "
                                               "(repeated to >= %.0f ms so the clock samples cover them)" % (
                                                   windows, args.steps, MIN_TIMED_MS),
-            "value_one_stream": value1, "timing": "two contexts in turn on two streams, CUDA events around both "
+            "value_one_stream": value1, "timing": "three contexts in turn on three streams, CUDA events around all "
                                                   "(value_one_stream: one context, one stream)",
             "e2e": e2e, "gpu_launches": launches_per_step * args.steps * windows,
             "roofline": {"bound": "sfu", "kernel": "fit_single_kernel<7,GS2D>", "achieved": achieved,
