@@ -138,9 +138,9 @@ def max_over_ranks(ms, dist):
 
 def device_timed(steps, warmup, enqueue, streams, dist):
     """Device time (ms, the slowest rank's) of `steps` calls enqueue(k, stream)
-    after `warmup` untimed ones.  With two streams the calls alternate between
-    them (two contexts in turn), so one call's latency-bound tail overlaps the
-    next call's kernels; the CUDA events bracket every stream."""
+    after `warmup` untimed ones.  With several streams the calls rotate over
+    them (as many contexts in turn), so one call's latency-bound tail overlaps
+    the next calls' kernels; the CUDA events bracket every stream."""
     import torch
     for k in range(warmup):
         enqueue(k, streams[k % len(streams)])
@@ -962,13 +962,13 @@ def learned_shapes_measure(streams, dist, world, rank, mufu_peak=None, cpu_basel
             recs.append(rec)
             truths.append(truth)
             d_b.append(torch.from_numpy(rec.view(np.int16)).cuda())
-        ctxs = [lib.LocContext(para, capacity=SHAPE_RECORDS) for _ in range(2)]
+        ctxs = [lib.LocContext(para, capacity=SHAPE_RECORDS) for _ in range(len(streams))]
 
         def plain(k, s, c=None):
-            (c or ctxs[k % 2]).localize_device(d_b[k % 2].data_ptr(), SHAPE_RECORDS, 0, s.cuda_stream)
+            (c or ctxs[k % len(ctxs)]).localize_device(d_b[k % 2].data_ptr(), SHAPE_RECORDS, 0, s.cuda_stream)
 
         def learned(k, s, c=None):
-            net.localize(c or ctxs[k % 2], d_b[k % 2].data_ptr(), SHAPE_RECORDS, iters=iters, bisections=bis,
+            net.localize(c or ctxs[k % len(ctxs)], d_b[k % 2].data_ptr(), SHAPE_RECORDS, iters=iters, bisections=bis,
                          stream=s.cuda_stream)
 
         ms_p = device_timed(SHAPE_STEPS, 3, plain, streams, dist)
@@ -1005,7 +1005,7 @@ def learned_shapes_measure(streams, dist, world, rank, mufu_peak=None, cpu_basel
             roof = {"bound": "sfu", "unit": "MUFU op/s", "peak": mufu_peak,
                     "call": {"achieved": ops / (call_ms * 1e-3), "frac": ops / (call_ms * 1e-3) / mufu_peak,
                              "ms": call_ms, "stages": {"single": single, "two_emitter": n2, "three_emitter": n3},
-                             "scope": "whole plain call (WLE + fit cascade + CRLB), two contexts in turn; fits counted "
+                             "scope": "whole plain call (WLE + fit cascade + CRLB), three contexts in turn; fits counted "
                                       "on the reference schedule"},
                     "kernel": {"name": "fit_single_kernel<%d,%s>" % (R, "AS3D" if kind == "as3d" else "GS2D"),
                                "achieved": k_ops / (k_ms * 1e-3), "frac": k_ops / (k_ms * 1e-3) / mufu_peak,
@@ -1213,7 +1213,7 @@ def mixed_measure(streams, dist, world, rank):
     train one network per ROI size, and MIXED_EVAL fresh records are localized
     in calls of MIXED_CALL records of one size (the reference's API takes one
     ROI size per call) plainly and with learned start points.  fits/s over the
-    whole evaluation stream (device time of every call, two contexts in turn),
+    whole evaluation stream (device time of every call, three contexts in turn),
     accuracy against the generator's truth with the rows' own CRLB beside it."""
     import torch
     from qcstorm_b200 import lib, synth_torch as ST
@@ -1264,15 +1264,15 @@ def mixed_measure(streams, dist, world, rank):
         rb = R * (R + 1) * 2
         base = d_ev.data_ptr()
         calls = [(o, min(MIXED_CALL, n_eval[i] - o)) for o in range(0, n_eval[i], MIXED_CALL)]
-        ctxs = [lib.LocContext(para, capacity=MIXED_CALL) for _ in range(2)]
+        ctxs = [lib.LocContext(para, capacity=MIXED_CALL) for _ in range(len(streams))]
 
         def plain(k, s, c=None):
             o, m = calls[k % len(calls)]
-            (c or ctxs[k % 2]).localize_device(base + o * rb, m, 0, s.cuda_stream)
+            (c or ctxs[k % len(ctxs)]).localize_device(base + o * rb, m, 0, s.cuda_stream)
 
         def learned(k, s, c=None):
             o, m = calls[k % len(calls)]
-            net.localize(c or ctxs[k % 2], base + o * rb, m, iters=iters, bisections=bis, stream=s.cuda_stream)
+            net.localize(c or ctxs[k % len(ctxs)], base + o * rb, m, iters=iters, bisections=bis, stream=s.cuda_stream)
 
         ms_p = device_timed(len(calls), 3, plain, streams, dist)
         ms_l = device_timed(len(calls), 3, learned, streams, dist)
@@ -1315,7 +1315,7 @@ def mixed_measure(streams, dist, world, rank):
             "train_epochs": MIXED_EPOCHS,
             "plain_fits_per_s": MIXED_EVAL * world / (tot_p * 1e-3),
             "learned_fits_per_s": MIXED_EVAL * world / (tot_l * 1e-3), "vs_plain": tot_p / tot_l,
-            "timing": "device time of every evaluation call, two contexts in turn, summed over the sizes",
+            "timing": "device time of every evaluation call, three contexts in turn, summed over the sizes",
             "shapes": shapes}
 
 
@@ -1325,7 +1325,7 @@ def mixed_persistent_measure(streams, dist, world, rank):
     qcs_loc_localize_mixed_device call per MIXED_CALL records of each size
     (the three sizes' single-emitter fits in one persistent launch), and the
     same chunks as three qcs_loc_localize_device calls in a row.  Device time
-    of every call, two sets of contexts in turn; the rows of one chunk are
+    of every call, three sets of contexts in turn; the rows of one chunk are
     compared bit for bit."""
     import torch
     from qcstorm_b200 import lib, synth_torch as ST
@@ -1336,7 +1336,7 @@ def mixed_persistent_measure(streams, dist, world, rank):
         data.append((R, ST.para(kind, R), d_ev, n_eval[i]))
     torch.cuda.synchronize()
     ncalls = max((n + MIXED_CALL - 1) // MIXED_CALL for _, _, _, n in data)
-    ctxs = [[lib.LocContext(para, capacity=MIXED_CALL) for _, para, _, _ in data] for _ in range(2)]
+    ctxs = [[lib.LocContext(para, capacity=MIXED_CALL) for _, para, _, _ in data] for _ in range(len(streams))]
 
     def chunks(k, cs):
         out = []
@@ -1348,10 +1348,10 @@ def mixed_persistent_measure(streams, dist, world, rank):
         return out
 
     def mixed(k, s, cs=None):
-        lib.localize_mixed_device(chunks(k, cs or ctxs[k % 2]), s.cuda_stream)
+        lib.localize_mixed_device(chunks(k, cs or ctxs[k % len(ctxs)]), s.cuda_stream)
 
     def per_size(k, s, cs=None):
-        for c, ptr, m in chunks(k, cs or ctxs[k % 2]):
+        for c, ptr, m in chunks(k, cs or ctxs[k % len(ctxs)]):
             c.localize_device(ptr, m, 0, s.cuda_stream)
 
     ms_m = device_timed(ncalls, 3, mixed, streams, dist)
@@ -1380,7 +1380,7 @@ def mixed_persistent_measure(streams, dist, world, rank):
             "persistent_fits_per_s": MIXED_EVAL * world / (ms_m * 1e-3),
             "per_size_fits_per_s": MIXED_EVAL * world / (ms_s * 1e-3), "persistent_vs_per_size": ms_s / ms_m,
             "rows_equal": bool(equal), "per_entry": per_entry,
-            "timing": "device time of every call, two sets of contexts in turn; per_entry: one chunk of each size "
+            "timing": "device time of every call, three sets of contexts in turn; per_entry: one chunk of each size "
                       "alone and all three, one stream, 5 calls after 2 warm-ups"}
 
 
@@ -1753,7 +1753,8 @@ def main():
     if args.profile_mixed:
         return profile_mixed(args.profile_mixed, stream)
     if args.mixed_persistent:
-        print(json.dumps(mixed_persistent_measure([stream, torch.cuda.Stream()], None, 1, 0)))
+        print(json.dumps(mixed_persistent_measure([stream] + [torch.cuda.Stream() for _ in range(IN_FLIGHT - 1)], None,
+                                                  1, 0)))
         return 0
     dist = None
     if world > 1:
@@ -1853,11 +1854,11 @@ def main():
 
     shapes = mixed = None
     if not args.no_learned:
-        shapes = learned_shapes_measure(streams, dist, world, rank, mufu_peak=mufu_peak,
+        shapes = learned_shapes_measure(streams_main, dist, world, rank, mufu_peak=mufu_peak,
                                         cpu_baseline=not args.no_cpu_baseline)
         if not args.no_mixed:
-            mixed = mixed_measure(streams, dist, world, rank)
-            mixed["plain_persistent"] = mixed_persistent_measure(streams, dist, world, rank)
+            mixed = mixed_measure(streams_main, dist, world, rank)
+            mixed["plain_persistent"] = mixed_persistent_measure(streams_main, dist, world, rank)
 
     frames = None
     if not args.no_frames:
