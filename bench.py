@@ -467,22 +467,25 @@ def frame_pipeline(stream, steps, warmup, e2e=True, dist=None, world=1, net=None
     d_fr = torch.from_numpy(fr.view(np.int16)).cuda()
     h_fr = torch.from_numpy(fr.view(np.int16)).pin_memory()
     sh = stream.cuda_stream
-    d_rois, d_wle, d_n = ex.device_records()
     frame_bytes = FRAME_W * FRAME_H * 2
 
-    def step(k, host=False):
-        ex.reset(sh)
+    def call(k, e, l, s, host):
+        """Call k on extraction context e, localization context l, stream handle s."""
+        rois, wle, n = e.device_records()
+        e.reset(s)
         for j in range(FRAMES_PER_CALL):
             f = k * FRAMES_PER_CALL + j
             if host:
-                ex.extract_device(h_fr.data_ptr() + (f % FRAMES) * frame_bytes, 1, f, stream=sh, source="pinned")
+                e.extract_device(h_fr.data_ptr() + (f % FRAMES) * frame_bytes, 1, f, stream=s, source="pinned")
             else:
-                ex.extract_device(d_fr.data_ptr() + (f % FRAMES) * frame_bytes, 1, f, stream=sh)
+                e.extract_device(d_fr.data_ptr() + (f % FRAMES) * frame_bytes, 1, f, stream=s)
         if net is None:
-            loc.localize_device_n(d_rois, d_wle, d_n, MAX_POINT_NUM, sh)
+            l.localize_device_n(rois, wle, n, MAX_POINT_NUM, s)
         else:
-            net.localize_n(loc, d_rois, d_wle, d_n, MAX_POINT_NUM, iters=LEARNED_ITERS, bisections=LEARNED_BISECTIONS,
-                           stream=sh)
+            net.localize_n(l, rois, wle, n, MAX_POINT_NUM, iters=LEARNED_ITERS, bisections=LEARNED_BISECTIONS, stream=s)
+
+    def step(k, host=False):
+        call(k, ex, loc, sh, host)
 
     step(0)
     rows0, ratios0 = loc.read_rows(sh)
@@ -522,17 +525,32 @@ def frame_pipeline(stream, steps, warmup, e2e=True, dist=None, world=1, net=None
     rows_g, _ = loc.read_rows(sh)
     assert rows_g.shape == rows0.shape
     del g
-    e2e_steps = max(3, steps // 4) if e2e else 1
+    # end to end: IN_FLIGHT (extraction, localization) context pairs on their own streams, so that the next calls'
+    # frame copies and extractions run while a call localizes and its rows are read
+    e2e_steps = max(6, steps // 4) if e2e else 1
+    more = [(lib.ExtractContext(para, max_batched_num=1, capacity=MAX_POINT_NUM),
+             lib.LocContext(para, capacity=MAX_POINT_NUM), torch.cuda.Stream()) for _ in range(IN_FLIGHT - 1)]
+    pairs = [(ex, loc, sh)] + [(e, l, st.cuda_stream) for e, l, st in more]
+    depth = len(pairs)
+    for k in range(depth):
+        call(k, *pairs[k], True)
+        pairs[k][1].read_rows(pairs[k][2])
+    torch.cuda.synchronize()
     t0 = time.perf_counter()
     out_rows = 0
     for k in range(e2e_steps):
-        step(k, host=True)
-        r, _ = loc.read_rows(sh)
-        out_rows += r.shape[0]
+        if k >= depth:
+            _, l, s = pairs[k % depth]
+            out_rows += l.read_rows(s)[0].shape[0]
+        call(k, *pairs[k % depth], True)
+    for k in range(max(0, e2e_steps - depth), e2e_steps):
+        _, l, s = pairs[k % depth]
+        out_rows += l.read_rows(s)[0].shape[0]
     e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3, dist) / e2e_steps
-    ex.close()
-    loc.close()
-    call = "qcs_loc_localize_device_n" if net is None else "qcs_learned_localize_device_n"
+    for e, l, _ in pairs:
+        e.close()
+        l.close()
+    call_name = "qcs_loc_localize_device_n" if net is None else "qcs_learned_localize_device_n"
     return {
         "workload": "2048x2048 uint16 frames, ~3000 emitters/frame (20%% in pairs < 3 px), GS2D 7x7, multi-emitter "
                     "fitting on; %d frames per localization call, %d distinct frames rotated" % (
@@ -551,8 +569,8 @@ def frame_pipeline(stream, steps, warmup, e2e=True, dist=None, world=1, net=None
         "e2e": {"frames_per_s": world * FRAMES_PER_CALL * 1e3 / e2e_ms, "ms_per_call": e2e_ms,
                 "h2d_bytes_per_call": FRAMES_PER_CALL * frame_bytes,
                 "d2h_bytes_per_call": int(out_rows / e2e_steps) * 48 + 32,
-                "calls": "%d x qcs_extract_molecules (pinned frame) -> %s -> qcs_loc_read_rows" % (
-                    FRAMES_PER_CALL, call)},
+                "calls": "%d x qcs_extract_molecules (pinned frame) -> %s -> qcs_loc_read_rows, %d context pairs "
+                         "on their streams in turn" % (FRAMES_PER_CALL, call_name, IN_FLIGHT)},
     }
 
 
