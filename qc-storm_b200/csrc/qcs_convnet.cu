@@ -671,6 +671,7 @@ struct State {
     float2 *scale = nullptr;
     unsigned img_version = 0;
     cudaEvent_t img_ready = nullptr;
+    cudaEvent_t scratch_free = nullptr;  // recorded after the last inference call's use of fc_in and scale
     int sms = 148;
 };
 
@@ -680,6 +681,7 @@ void destroy(State *st) {
     cudaFree(st->img);
     cudaFree(st->fc_in);
     if (st->img_ready) cudaEventDestroy(st->img_ready);
+    if (st->scratch_free) cudaEventDestroy(st->scratch_free);
     delete st;
 }
 
@@ -718,6 +720,7 @@ cudaError_t create(int R, int batch, State **out) {
         e = cudaMalloc((void **)&st->fc_in, tiles * (size_t)kf_of(R) * 128 * 2 + (size_t)kChunk * sizeof(float2));
     if (e == cudaSuccess) st->scale = reinterpret_cast<float2 *>(st->fc_in + tiles * (size_t)kf_of(R) * 128 * 2);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&st->img_ready, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&st->scratch_free, cudaEventDisableTiming);
     int dev = 0;
     if (e == cudaSuccess) e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&st->sms, cudaDevAttrMultiProcessorCount, dev);
@@ -862,10 +865,16 @@ cudaError_t start_points(State *st, const float *par, unsigned version, int loc_
     } else if (cudaEventQuery(st->img_ready) != cudaSuccess) {
         return cudaErrorNotReady;
     }
+    // fc_in and scale hold one call's intermediate results: a call on another stream waits until the call before
+    // it has used them (outside stream capture: a graph holding this call must not run beside another call of the
+    // same network)
+    if (!capturing && (e = cudaStreamWaitEvent(s, st->scratch_free, 0)) != cudaSuccess) return e;
     const int R = st->R;
-#define QCS_CONV_CASE(RR, LTT)                                                                        \
-    if (R == RR && loc_type == LTT)                                                                   \
-        return launch_chunks<RR, LTT>(st, par, p, rois, n, n_dev, out, cls, th, s, err);
+    e = cudaErrorInvalidValue;
+#define QCS_CONV_CASE(RR, LTT) \
+    else if (R == RR && loc_type == LTT) e = launch_chunks<RR, LTT>(st, par, p, rois, n, n_dev, out, cls, th, s, err);
+    if (false) {
+    }
     QCS_CONV_CASE(7, QCS_LOCTYPE_GS2D)
     QCS_CONV_CASE(9, QCS_LOCTYPE_GS2D)
     QCS_CONV_CASE(11, QCS_LOCTYPE_GS2D)
@@ -876,7 +885,8 @@ cudaError_t start_points(State *st, const float *par, unsigned version, int loc_
     QCS_CONV_CASE(9, kTwo)
     QCS_CONV_CASE(11, kTwo)
 #undef QCS_CONV_CASE
-    return cudaErrorInvalidValue;
+    if (e != cudaSuccess || capturing) return e;
+    return cudaEventRecord(st->scratch_free, s);
 }
 
 }  // namespace conv

@@ -762,6 +762,7 @@ struct qcs_learned_net {
     unsigned version = 1;             // bumped whenever the parameters change
     unsigned wimg_version = 0;        // parameter version d_wimg was built from
     cudaEvent_t wimg_ready = nullptr; // recorded after d_wimg was built
+    cudaEvent_t start_free = nullptr;  // recorded after the last unfused start-point call used d_start
     bool use_tc = true;
     float count_th = 0.0f;            // emitter-count routing threshold; 0 = no routing
     int batch = 0;
@@ -1015,6 +1016,7 @@ int qcs_learned_destroy(qcs_learned_net *net) {
     cudaFree(net->d_ws);
     L::conv::destroy(net->conv);
     if (net->wimg_ready) cudaEventDestroy(net->wimg_ready);
+    if (net->start_free) cudaEventDestroy(net->start_free);
     delete net;
     return QCS_OK;
 }
@@ -1062,6 +1064,7 @@ int qcs_learned_create_arch(int arch, int loc_type, int roi_size, int batch, uns
     if (e == cudaSuccess && arch == QCS_LEARNED_ARCH_CONV) e = L::conv::create(roi_size, batch, &net->conv);
     if (e == cudaSuccess) e = cudaMemset(net->d_err, 0, sizeof(int));
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&net->wimg_ready, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&net->start_free, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         qcs_learned_destroy(net);
         return fail(e == cudaErrorMemoryAllocation ? QCS_ERR_NOMEM : QCS_ERR_CUDA, "qcs_learned_create", e);
@@ -1449,7 +1452,14 @@ cudaError_t qcs::learned::start_points(qcs_learned_net *net, const qcs_loc_para 
     float *feat = net->d_start, *scale = feat + (size_t)n * kin;
     float *h1 = scale + 2 * (size_t)n, *h2 = h1 + (size_t)n * L::kHidden, *y = h2 + (size_t)n * L::kHidden;
     const float th = class_threshold(net);
-    return by_shape(net->loc_type, net->R, [&](auto sh) -> cudaError_t {
+    // d_start holds one call's features and activations: a call on another stream waits until the call before it
+    // has used them (outside stream capture: a graph holding this call must not run beside another call of the net)
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaError_t e0 = cudaStreamIsCapturing(s, &cs);
+    if (e0 != cudaSuccess) return e0;
+    const bool capturing = cs != cudaStreamCaptureStatusNone;
+    if (!capturing && (e0 = cudaStreamWaitEvent(s, net->start_free, 0)) != cudaSuccess) return e0;
+    e0 = by_shape(net->loc_type, net->R, [&](auto sh) -> cudaError_t {
         constexpr int R = decltype(sh)::R, LT = decltype(sh)::LT;
         L::features_kernel<R><<<blocks(n), 256, 0, s>>>(d_rois, n, p->Offset, p->KAdc, feat, scale);
         cudaError_t e = cudaSuccess;
@@ -1464,4 +1474,6 @@ cudaError_t qcs::learned::start_points(qcs_learned_net *net, const qcs_loc_para 
         L::start_kernel<R, LT><<<blocks(n), 256, 0, s>>>(y, scale, n, out, LT == QCS_LOCTYPE_GS2D ? cls : nullptr, th);
         return cudaGetLastError();
     });
+    if (e0 != cudaSuccess || capturing) return e0;
+    return cudaEventRecord(net->start_free, s);
 }

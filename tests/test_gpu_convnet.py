@@ -153,3 +153,34 @@ def test_conv_network_localize_equals_fit_from_its_start_points(cuda_ok):
     np.testing.assert_array_equal(ra, rb)
     ctx.close()
     net.close()
+
+
+@pytest.mark.parametrize("arch,fused", [("conv", True), ("conv", False), ("mlp", True), ("mlp", False)])
+def test_learned_calls_on_several_streams(cuda_ok, arch, fused):
+    """One network used by three contexts on three streams at once (calls in
+    flight together) gives every call the rows it gives alone: the network's
+    own inference buffers are handed from call to call in stream order."""
+    import torch
+    n = 60_000
+    rec, para, _, d, feat, scale, t, v, _keep = data(0, 7, 3 * n, 72)
+    net = qlib.LearnedNet(batch=4096, seed=4, arch=arch)
+    net.train(feat[:20_000], t[:20_000], v[:20_000], epochs=2, lr=1e-3)
+    net.set_fused(fused)
+    rb = 7 * 8 * 2
+    streams = [torch.cuda.Stream() for _ in range(3)]
+    ctxs = [qlib.LocContext(para, capacity=n) for _ in range(3)]
+    alone = []
+    for j in range(3):
+        net.localize(ctxs[0], d.data_ptr() + j * n * rb, n, iters=2, bisections=6, stream=streams[0].cuda_stream)
+        alone.append(ctxs[0].read_rows(streams[0].cuda_stream)[0])
+    torch.cuda.synchronize()
+    for rep in range(2):
+        for j in range(3):
+            net.localize(ctxs[j], d.data_ptr() + j * n * rb, n, iters=2, bisections=6, stream=streams[j].cuda_stream)
+        for j in range(3):
+            got = ctxs[j].read_rows(streams[j].cuda_stream)[0]
+            np.testing.assert_array_equal(got.view(np.uint32), alone[j].view(np.uint32))
+    net.fused_status()
+    for c in ctxs:
+        c.close()
+    net.close()
