@@ -737,7 +737,11 @@ int qcs_fit_from_start_classes_device(qcs_loc_data *c, const uint16_t *d_rois, c
  * qcs_fit_from_start_device (the network's shape must be the call's:
  * QCS_ERR_ROISIZE otherwise), and, with multi-emitter fitting on (GS2D) and a
  * count threshold set, the network's emitter-count classes.  Rows in the
- * context like qcs_loc_localize_device. */
+ * context like qcs_loc_localize_device.  One network may serve several
+ * contexts on different streams at once: the inference buffers a network
+ * owns (conv networks, and the MLP with fused inference off) pass from call
+ * to call in stream order.  A CUDA graph holding such a call must not run
+ * beside another call of the same network. */
 int qcs_learned_localize_device(qcs_loc_data *c, qcs_learned_net *net, const uint16_t *d_rois, const float *d_wle,
                                 const qcs_loc_para *p, int n, int iters, int bisections, float dev_th,
                                 void *stream);
