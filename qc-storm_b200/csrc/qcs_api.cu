@@ -978,13 +978,21 @@ int qcs_loc_bfgs_mle_localization(qcs_loc_data *c, const uint16_t *h_rois, const
     if (st) return st;
     QCS_CUDA(cudaMemcpyAsync(c->h_counters, c->st.counters, qcs::kCntNum * sizeof(int), cudaMemcpyDeviceToHost, s),
              "read counters");
+    // without multi-emitter fitting every record has its row (zero when rejected): the n rows come back with the
+    // counters, one wait; with it the row count is read first
+    const bool one_pass = !p->MultiEmitterFitEn && !use_lr(c, p) && n <= c->max_rows;
+    if (one_pass)
+        QCS_CUDA(cudaMemcpyAsync(c->h_loc, c->d_loc, (size_t)n * QCS_OUT_PARA_NUM * sizeof(float),
+                                 cudaMemcpyDeviceToHost, s),
+                 "read localizations");
     QCS_CUDA(cudaStreamSynchronize(s), "localization");
     const int rows = c->h_counters[qcs::kCntValid];
-    if (rows > 0)
+    if (!one_pass && rows > 0) {
         QCS_CUDA(cudaMemcpyAsync(c->h_loc, c->d_loc, (size_t)rows * QCS_OUT_PARA_NUM * sizeof(float),
                                  cudaMemcpyDeviceToHost, s),
                  "read localizations");
-    QCS_CUDA(cudaStreamSynchronize(s), "read localizations");
+        QCS_CUDA(cudaStreamSynchronize(s), "read localizations");
+    }
     c->valid = rows;
     compute_ratios(c, p, n);
     return QCS_OK;

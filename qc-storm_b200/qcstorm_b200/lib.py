@@ -251,8 +251,9 @@ class LocContext:
         except Exception:
             pass
 
-    def localize(self, rois, wle=None, para=None, stream=0):
-        """BFGS_MLELocalization on host arrays; returns (rows[n_valid, 12], ratios[7])."""
+    def localize(self, rois, wle=None, para=None, stream=0, copy=True):
+        """BFGS_MLELocalization on host arrays; returns (rows[n_valid, 12], ratios[7]); copy=False returns a view
+        of the context's pinned row buffer (h_LocArry), valid until the next call."""
         para = para or self.para
         rois, pr = _host(rois, np.uint16)
         n = rois.shape[0]
@@ -263,11 +264,11 @@ class LocContext:
                                                      C.c_void_p(stream) if stream else None))
         nv = self.lib.qcs_loc_valid_num(self.h)
         ptr = self.lib.qcs_loc_h_loc_arry(self.h)
-        rows = np.ctypeslib.as_array((C.c_float * (12 * nv)).from_address(ptr)).reshape(nv, 12).copy() if nv else \
+        rows = np.ctypeslib.as_array((C.c_float * (12 * nv)).from_address(ptr)).reshape(nv, 12) if nv else \
             np.zeros((0, 12), np.float32)
         ratios = np.zeros(7, np.float32)
         check(self.lib.qcs_loc_fit_ratios(self.h, C.c_void_p(ratios.ctypes.data)))
-        return rows, ratios
+        return (rows.copy() if copy and nv else rows), ratios
 
     def wle(self, rois, para=None):
         """WLEParameterEstimate on host records; returns wle[n, 6]."""
